@@ -1,0 +1,165 @@
+/*
+ * vortex_b200.h — native C ABI of the B200 vortex-element step library
+ * (libvortex_b200.so).
+ *
+ * One handle (vx_sim) owns one body's resident device state: panels, the
+ * inverted panel system, structure-of-arrays particle storage and scratch.
+ * vx_step() advances it by whole time steps in the reference's per-step order
+ * (src/main.c:676-784 of grechkin-pogrebnyakov/vortex): birth, convective
+ * velocity with 3-nearest distance, vortex and wall diffusion, convection with
+ * wall absorption, force sums, compaction, collapse of opposite-sign then
+ * same-sign pairs.  A step never synchronises with the host unless the
+ * particle store has to grow.
+ *
+ * The reference's own entry points (include/unit_1.cuh:15-55) are exported
+ * by the same library; they are declared in vortex_b200_unit1.h.
+ *
+ * All functions return vx_status; VX_OK is 0.  Handles are not thread-safe;
+ * different handles may be used from different threads.
+ */
+#ifndef VORTEX_B200_H_
+#define VORTEX_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vx_status {
+    VX_OK = 0,
+    VX_ERR_CUDA = 1,        /* a CUDA call failed (message in vx_last_error) */
+    VX_ERR_ARG = 2,         /* bad argument (reference: return code 2) */
+    VX_ERR_IO = 3,          /* file could not be opened or parsed */
+    VX_ERR_SINGULAR = 4,    /* panel system pivot below 1e-12 */
+    VX_ERR_NOMEM = 5,       /* device or host allocation failed */
+    VX_ERR_DEVICE = 6,      /* a kernel reported an internal error flag */
+    VX_ERR_BUDGET = 7       /* request exceeds the server's HBM budget */
+} vx_status;
+
+enum { VX_PREC_FP64 = 0, VX_PREC_FP32 = 1 };
+/* Where a new vortex is placed: the reference's midpoint + 1e-6 n
+ * (include/kernel.cuh:109-116), the profile file's birth column, or the
+ * panel midpoint + L/2 n. */
+enum { VX_BIRTH_REF = 0, VX_BIRTH_FILE = 1, VX_BIRTH_HALF_PANEL = 2 };
+
+/* Panel record; same 120-byte layout as the reference's tPanel
+ * (include/definitions.h:82-103). */
+typedef struct vx_panel {
+    uint32_t n;
+    uint32_t pad_;
+    double left[2];
+    double right[2];
+    double contr[2];
+    double birth[2];
+    double norm[2];
+    double tang[2];
+    double length;
+    uint32_t n_of_lpanel;
+    uint32_t n_of_rpanel;
+} vx_panel;
+
+/* Run configuration.  The first block holds the reference's .conf keys
+ * (src/main.c:77-111, struct conf_t include/definitions.h:105-142); the
+ * second block holds keys this library adds.  Unknown keys in a .conf file
+ * are ignored, as in the reference. */
+typedef struct vx_conf {
+    int64_t steps, saving_step, inc_step, n_of_points, n_col, v_inf_incr_steps, tree_depth;
+    double dt, viscosity, rho, v_inf_x, v_inf_y;
+    double x_max, x_min, y_max, y_min;
+    double ve_size, h_col_x, h_col_y, rc_x, rc_y;
+    double r_col_diff_sign, r_col_same_sign, max_ve_g, rel_t, theta;
+    int32_t matrix_load, steady_flow, log_level, no_log_buf;
+    char pr_file[256];
+    char timings_file[256];
+    char kadr_file[256];
+    char second_points_file[256];
+    char log_file[256];
+    /* ---- additions ---- */
+    int32_t precision;          /* VX_PREC_FP64 (plain) or VX_PREC_FP32 (bulk) */
+    int32_t birth_offset_mode;  /* VX_BIRTH_* ; default VX_BIRTH_REF */
+    double drop_eps;            /* |G| below this is removed; default 1e-12 */
+    double diff_cutoff;         /* bulk form: vortex diffusion ignores pairs
+                                   with r > diff_cutoff * d_i (default 30) */
+    int32_t n_probes_grid;      /* >0: probes on an n x n grid (box below) */
+    int32_t pad1_;
+    double probe_box[4];        /* x0, x1, y0, y1 of the probe grid */
+} vx_conf;
+
+typedef struct vx_sim vx_sim;
+
+const char *vx_status_str(vx_status s);
+/* Last error message of the calling thread (empty string if none). */
+const char *vx_last_error(void);
+
+/* Defaults as the reference's main() leaves them (src/main.c:420-422:
+ * zeroed struct, log_level 3, v_inf_incr_steps 1) plus the additions'. */
+vx_status vx_conf_default(vx_conf *conf);
+/* Parse a .conf file ("key value" lines, prefix-matched keys, trailing
+ * comments tolerated; src/main.c:48-115) on top of *conf. */
+vx_status vx_conf_read(const char *path, vx_conf *conf);
+/* Read a profile file (src/main.c:220-256).  With out == NULL only *P is
+ * set; otherwise cap must be >= P. */
+vx_status vx_profile_read(const char *path, vx_panel *out, int64_t cap, int64_t *P);
+
+/* Create a body on CUDA device `device`: uploads panels, builds and inverts
+ * the panel system on the device.  Particle store starts empty. */
+vx_status vx_create(const vx_conf *conf, const vx_panel *panels, int64_t P, int device,
+                    vx_sim **out);
+vx_status vx_destroy(vx_sim *sim);
+
+/* Host <-> device particle state (x, y, G of the first n particles). */
+vx_status vx_set_particles(vx_sim *sim, const double *x, const double *y, const double *g,
+                           int64_t n);
+vx_status vx_get_particles(vx_sim *sim, double *x, double *y, double *g, int64_t cap,
+                           int64_t *n);
+vx_status vx_get_count(vx_sim *sim, int64_t *n);
+/* Velocity and 3-nearest distance from the last velocity evaluation. */
+vx_status vx_get_velocity(vx_sim *sim, double *vx, double *vy, double *d, int64_t cap);
+/* Absorbed circulation, force (x, y) and moment of the last step
+ * (the reference's d_g, F_p, M after summ_Kernel). */
+vx_status vx_get_forces(vx_sim *sim, double out4[4]);
+vx_status vx_set_vinf(vx_sim *sim, double vx, double vy);
+vx_status vx_set_dg(vx_sim *sim, double dg);
+/* The inverted (P+1)^2 panel system, row-major. */
+vx_status vx_get_matrix(vx_sim *sim, double *minv);
+
+/* Advance nsteps whole steps. */
+vx_status vx_step(vx_sim *sim, int64_t nsteps);
+
+/* Individual stages, in step order (for tests and custom drivers). */
+enum {
+    VX_STAGE_BIRTH = 1u << 0,
+    VX_STAGE_VELOCITY = 1u << 1,     /* Biot-Savart + 3-nearest distance */
+    VX_STAGE_DIFFUSION = 1u << 2,    /* vortex-vortex diffusive velocity */
+    VX_STAGE_WALL = 1u << 3,         /* wall diffusive velocity */
+    VX_STAGE_ADVECT = 1u << 4,       /* convection, absorption, force sums */
+    VX_STAGE_COMPACT = 1u << 5,
+    VX_STAGE_COLLAPSE1 = 1u << 6,    /* opposite signs, n_col rounds */
+    VX_STAGE_COLLAPSE2 = 1u << 7,    /* same sign, n_col rounds */
+    VX_STAGE_ALL = 0xffu
+};
+vx_status vx_stage(vx_sim *sim, unsigned stage_mask);
+
+/* Velocity at probe points (host arrays), Biot-Savart + V_inf only
+ * (src/kernel.cu:1434-1475). */
+vx_status vx_probe(vx_sim *sim, const double *px, const double *py, int64_t np,
+                   double *vx, double *vy);
+
+/* Record every step into a CUDA graph after the first call and replay it
+ * (on by default; 0 turns it off). */
+vx_status vx_set_graph(vx_sim *sim, int enable);
+
+/* Device time (ms) accumulated per stage group since the last reset:
+ * out[0] birth, [1] velocity+diffusion ("Speed"), [2] advect..collapse
+ * ("Step").  Timing adds events; off unless enabled. */
+vx_status vx_set_timing(vx_sim *sim, int enable);
+vx_status vx_get_timing(vx_sim *sim, double out3[3]);
+
+/* Number of kernels this handle has launched since creation. */
+vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VORTEX_B200_H_ */

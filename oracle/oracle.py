@@ -67,6 +67,8 @@ def lib():
 
 
 def _p(a):
+    """Pointer to a numpy array's data.  The caller must keep `a` referenced
+    until the C call returns (never pass a temporary)."""
     return C.c_void_p(a.ctypes.data) if a is not None else None
 
 
@@ -109,14 +111,16 @@ def birth_rhs(p, pan, x, y, g):
 def birth_gamma(Minv, R, dg):
     P = len(R)
     gam = np.zeros(P)
-    lib().vxo_birth_gamma(C.c_int64(P), _p(_f64(Minv)), _p(_f64(R)), C.c_double(dg), _p(gam))
+    Minv, R = _f64(Minv), _f64(R)
+    lib().vxo_birth_gamma(C.c_int64(P), _p(Minv), _p(R), C.c_double(dg), _p(gam))
     return gam
 
 
 def birth_place(p, pan, gamma):
     P = len(pan)
     x, y, g = np.zeros(P), np.zeros(P), np.zeros(P)
-    lib().vxo_birth_place(C.byref(p), _p(pan), C.c_int64(P), _p(_f64(gamma)), _p(x), _p(y), _p(g))
+    gamma = _f64(gamma)
+    lib().vxo_birth_place(C.byref(p), _p(pan), C.c_int64(P), _p(gamma), _p(x), _p(y), _p(g))
     return x, y, g
 
 
@@ -134,23 +138,25 @@ def velocity(p, x, y, g, n, s=None):
 
 def diffusion(p, x, y, g, n, d, vx, vy):
     vx, vy = _f64(vx).copy(), _f64(vy).copy()
-    lib().vxo_diffusion(C.byref(p), _p(_f64(x)), _p(_f64(y)), _p(_f64(g)), C.c_int64(n),
-                        _p(_f64(d)), _p(vx), _p(vy))
+    x, y, g, d = _f64(x), _f64(y), _f64(g), _f64(d)
+    lib().vxo_diffusion(C.byref(p), _p(x), _p(y), _p(g), C.c_int64(n), _p(d), _p(vx), _p(vy))
     return vx, vy
 
 
 def wall_diffusion(p, pan, x, y, n, d, vx, vy):
     vx, vy = _f64(vx).copy(), _f64(vy).copy()
-    lib().vxo_wall_diffusion(C.byref(p), _p(pan), C.c_int64(len(pan)), _p(_f64(x)), _p(_f64(y)),
-                             C.c_int64(n), _p(_f64(d)), _p(vx), _p(vy))
+    x, y, d = _f64(x), _f64(y), _f64(d)
+    lib().vxo_wall_diffusion(C.byref(p), _p(pan), C.c_int64(len(pan)), _p(x), _p(y),
+                             C.c_int64(n), _p(d), _p(vx), _p(vy))
     return vx, vy
 
 
 def advect(p, pan, x, y, g, vx, vy, n, n_new):
     x, y, g = _f64(x).copy(), _f64(y).copy(), _f64(g).copy()
     t = np.zeros((4, n))
+    vx, vy = _f64(vx), _f64(vy)
     lib().vxo_advect(C.byref(p), _p(pan), C.c_int64(len(pan)), _p(x), _p(y), _p(g),
-                     _p(_f64(vx)), _p(_f64(vy)), C.c_int64(n), C.c_int64(n_new),
+                     _p(vx), _p(vy), C.c_int64(n), C.c_int64(n_new),
                      _p(t[0]), _p(t[1]), _p(t[2]), _p(t[3]))
     return x, y, g, t
 
@@ -172,8 +178,8 @@ def compact(x, y, g, n, drop_eps=1e-12):
 
 def collapse_col(p, pas, x, y, g, n):
     col = np.zeros(n, dtype=np.int32)
-    lib().vxo_collapse_col(C.byref(p), C.c_int(pas), _p(_f64(x)), _p(_f64(y)), _p(_f64(g)),
-                           C.c_int64(n), _p(col))
+    x, y, g = _f64(x), _f64(y), _f64(g)
+    lib().vxo_collapse_col(C.byref(p), C.c_int(pas), _p(x), _p(y), _p(g), C.c_int64(n), _p(col))
     return col
 
 
@@ -194,7 +200,8 @@ def collapse(p, pas, x, y, g, n):
 def probe(p, x, y, g, n, px, py):
     px, py = _f64(px), _f64(py)
     vx, vy = np.zeros(len(px)), np.zeros(len(px))
-    lib().vxo_probe(C.byref(p), _p(_f64(x)), _p(_f64(y)), _p(_f64(g)), C.c_int64(n),
+    x, y, g = _f64(x), _f64(y), _f64(g)
+    lib().vxo_probe(C.byref(p), _p(x), _p(y), _p(g), C.c_int64(n),
                     _p(px), _p(py), C.c_int64(len(px)), _p(vx), _p(vy))
     return vx, vy
 

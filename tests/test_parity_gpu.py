@@ -1,0 +1,254 @@
+"""Stage-by-stage parity of the CUDA library (plain FP64 form) with the CPU
+oracle on identical seeded inputs, through the C ABI.
+
+Bit-exact: new-vortex positions, the 3-nearest distance d, convection with
+absorption and removal, compaction (every slot, dead tail included), collapse
+pairing and merge.  Tolerance (stated per test): sums whose order differs
+(velocity, diffusion, birth strengths, force totals) and values that go
+through exp/atan/log, whose last bit differs between CUDA and glibc.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import conf_kwargs, oracle_params, rel_err, wake_cloud, with_tail
+from vortex_b200 import native as N
+from vortex_b200 import profiles
+
+pytestmark = pytest.mark.gpu
+
+VEL_TOL = 1e-12      # absolute, on velocities of order |V_inf| = 1
+STRENGTH_TOL = 1e-10  # relative to max |G| of the newborns
+
+
+def make(P=200, **kw):
+    ck = conf_kwargs(P, **kw)
+    pan = profiles.circle(P)
+    sim = N.Sim(N.default_conf(**ck), pan)
+    return sim, pan, ck, oracle_params(pan, ck)
+
+
+def test_panel_matrix_matches_oracle():
+    sim, pan, ck, p = make(P=200)
+    _, M = O.panel_matrix(pan)
+    Mg = sim.matrix()
+    assert rel_err(Mg, M) < 1e-11
+    sim.close()
+
+
+@pytest.mark.parametrize("n", [0, 37, 3000])
+def test_birth(n):
+    sim, pan, ck, p = make(P=200)
+    x, y, g = with_tail(*wake_cloud(n, seed=n), extra=96)
+    sim.set_slots(x, y, g, n)
+    sim.set_dg(3.5e-3)
+    sim.stage("birth")
+    assert sim.count() == n + 200
+    gx, gy, gg = sim.get_slots(n + 200)
+    R = O.birth_rhs(p, pan, x[:n], y[:n], g[:n])
+    _, M = O.panel_matrix(pan)
+    gam = O.birth_gamma(M, R, 3.5e-3)
+    bx, by, bg = O.birth_place(p, pan, gam)
+    assert np.array_equal(gx[:n], x[:n]) and np.array_equal(gg[:n], g[:n])
+    assert np.array_equal(gx[n:], bx) and np.array_equal(gy[n:], by)
+    assert rel_err(gg[n:], bg) < STRENGTH_TOL
+    # Kelvin: the new strengths carry the absorbed circulation d_g exactly up to rounding
+    assert abs(bg.sum() - 3.5e-3) < 1e-12
+    sim.close()
+
+
+@pytest.mark.parametrize("n", [5, 333, 4000])
+def test_velocity_and_nearest(n):
+    sim, pan, ck, p = make(P=200)
+    x, y, g = with_tail(*wake_cloud(n, seed=10 + n), extra=64)
+    sim.set_slots(x, y, g, n)
+    sim.stage("velocity")
+    vx, vy, d = sim.velocity()
+    ovx, ovy, od = O.velocity(p, x, y, g, n)
+    assert np.array_equal(d, od), "3-nearest distance must be bit-exact"
+    assert np.abs(vx - ovx).max() < VEL_TOL and np.abs(vy - ovy).max() < VEL_TOL
+    sim.close()
+
+
+def test_nearest_uses_padding_slots():
+    """The reference's 3-nearest search runs over the launch padded to 32,
+    which holds dead vortices; a dead vortex close to a live one changes d."""
+    sim, pan, ck, p = make(P=200)
+    n = 40
+    x, y, g = wake_cloud(n, seed=5)
+    tx = np.full(24, 1e10)
+    ty = np.full(24, 1e10)
+    tx[0], ty[0] = x[3] + 1e-5, y[3]
+    xs, ys, gs = np.concatenate([x, tx]), np.concatenate([y, ty]), np.concatenate([g, np.zeros(24)])
+    sim.set_slots(xs, ys, gs, n)
+    sim.stage("velocity")
+    _, _, d = sim.velocity()
+    _, _, od = O.velocity(p, xs, ys, gs, n)
+    assert np.array_equal(d, od)
+    _, _, od_nopad = O.velocity(p, xs, ys, gs, n, s=n)
+    assert d[3] != od_nopad[3]
+    sim.close()
+
+
+@pytest.mark.parametrize("n", [50, 3000])
+def test_diffusion(n):
+    sim, pan, ck, p = make(P=200)
+    x, y, g = wake_cloud(n, seed=20 + n)
+    ovx, ovy, od = O.velocity(p, x, y, g, n, s=n)
+    sim.set_particles(x, y, g)
+    sim.set_velocity(ovx, ovy, od)
+    sim.stage("diffusion")
+    vx, vy, _ = sim.velocity()
+    evx, evy = O.diffusion(p, x, y, g, n, od, ovx, ovy)
+    assert np.abs(vx - evx).max() < VEL_TOL and np.abs(vy - evy).max() < VEL_TOL
+    sim.close()
+
+
+def test_wall_diffusion():
+    sim, pan, ck, p = make(P=200)
+    rng = np.random.default_rng(7)
+    n = 2000
+    th = rng.uniform(0, 2 * math.pi, n)
+    r = 0.5 + rng.uniform(0.0, 0.1, n)
+    r[:50] = 0.5 + 1e-4                # on top of birth points: the override branch
+    x, y = r * np.cos(th), r * np.sin(th)
+    g = rng.normal(0, 1e-3, n)
+    d = rng.uniform(0.002, 0.03, n)
+    vx0, vy0 = np.ones(n), np.zeros(n)
+    sim.set_particles(x, y, g)
+    sim.set_velocity(vx0, vy0, d)
+    sim.stage("wall")
+    vx, vy, _ = sim.velocity()
+    evx, evy = O.wall_diffusion(p, pan, x, y, n, d, vx0, vy0)
+    assert np.abs(vx - evx).max() < 1e-13 and np.abs(vy - evy).max() < 1e-13
+    assert np.abs(evx - 1).max() > 1e-6      # the wall term is not trivially zero
+    sim.close()
+
+
+def test_advect_absorb_and_forces():
+    sim, pan, ck, p = make(P=200)
+    rng = np.random.default_rng(3)
+    n = 5000
+    x, y, g = wake_cloud(n, seed=3)
+    # velocities: some move into the body, some leave the window
+    vx = rng.normal(0, 2.0, n)
+    vy = rng.normal(0, 2.0, n)
+    k = rng.choice(n, 300, replace=False)
+    vx[k] = -x[k] / 0.005 * 0.8
+    vy[k] = -y[k] / 0.005 * 0.8
+    x[:20] = 9.999
+    vx[:20] = 5.0
+    sim.set_particles(x, y, g)        # the last P count as newborns
+    sim.set_velocity(vx, vy, np.ones(n))
+    sim.stage("advect")
+    gx, gy, gg = sim.get_slots(n)
+    ox, oy, og, t = O.advect(p, pan, x, y, g, vx, vy, n, 200)
+    assert np.array_equal(gx, ox) and np.array_equal(gy, oy) and np.array_equal(gg, og)
+    assert (og == 0).sum() > 100
+    dg, fx, fy, m = O.sums(p, t)
+    f = sim.forces()
+    assert abs(f[0] - dg) <= 1e-13 * max(1.0, abs(dg))
+    for a, b in ((f[1], fx), (f[2], fy), (f[3], m)):
+        assert abs(a - b) <= 1e-10 * max(1.0, abs(b))
+    sim.close()
+
+
+@pytest.mark.parametrize("frac_dead", [0.0, 0.02, 0.5, 1.0])
+def test_compaction_exact(frac_dead):
+    sim, pan, ck, p = make(P=200)
+    rng = np.random.default_rng(int(frac_dead * 100))
+    n = 7001
+    x, y, g = wake_cloud(n, seed=4)
+    dead = rng.random(n) < frac_dead
+    g[dead] = 0.0
+    g[rng.random(n) < 0.01] = 1e-13     # below the 1e-12 threshold
+    xs, ys, gs = with_tail(x, y, g, extra=64)
+    sim.set_slots(xs, ys, gs, n)
+    sim.stage("compact")
+    ox, oy, og, m = O.compact(xs, ys, gs, n)
+    assert sim.count() == m
+    gx, gy, gg = sim.get_slots(len(xs))
+    assert np.array_equal(gx, ox) and np.array_equal(gy, oy) and np.array_equal(gg, og)
+    sim.close()
+
+
+@pytest.mark.parametrize("pas", [1, 2])
+def test_collapse_exact(pas):
+    kw = dict(r_col_diff_sign=0.8, r_col_same_sign=0.6, max_ve_g=3e-3, n_col=3)
+    sim, pan, ck, p = make(P=200, **kw)
+    rng = np.random.default_rng(11 + pas)
+    n = 6000
+    # clustered particles so that chains of candidates form
+    cx = rng.uniform(0.6, 2.0, 300)
+    cy = rng.normal(0, 0.3, 300)
+    idx = rng.integers(0, 300, n)
+    x = cx[idx] + rng.normal(0, 0.01, n)
+    y = cy[idx] + rng.normal(0, 0.01, n)
+    g = rng.normal(0, 1e-3, n)
+    xs, ys, gs = with_tail(x, y, g, extra=32)
+    sim.set_slots(xs, ys, gs, n)
+    sim.stage("collapse1" if pas == 1 else "collapse2")
+    ox, oy, og, m = O.collapse(p, pas, xs, ys, gs, n)
+    assert m < n - 100, "the scene must exercise merging"
+    assert sim.count() == m
+    gx, gy, gg = sim.get_slots(len(xs))
+    assert np.array_equal(gx, ox) and np.array_equal(gy, oy) and np.array_equal(gg, og)
+    sim.close()
+
+
+def test_collapse_pairing_single_round():
+    """COL (smallest qualifying j > i) and the greedy merge of one round."""
+    kw = dict(r_col_same_sign=0.9, max_ve_g=1e30, n_col=1)
+    sim, pan, ck, p = make(P=200, **kw)
+    rng = np.random.default_rng(99)
+    n = 3000
+    x = rng.uniform(1.0, 1.3, n)
+    y = rng.uniform(-0.15, 0.15, n)
+    g = np.abs(rng.normal(0, 1e-3, n)) * np.where(rng.random(n) < 0.7, 1, -1)
+    sim.set_particles(x, y, g)
+    sim.stage("collapse2")
+    col = O.collapse_col(p, 2, x, y, g, n)
+    ox, oy, og = O.collapse_merge(2, x, y, g, n, col)
+    ox, oy, og, m = O.compact(ox, oy, og, n)
+    assert sim.count() == m
+    gx, gy, gg = sim.get_slots(n)
+    assert np.array_equal(gx, ox) and np.array_equal(gy, oy) and np.array_equal(gg, og)
+    sim.close()
+
+
+def test_probe():
+    sim, pan, ck, p = make(P=200)
+    n = 2500
+    x, y, g = wake_cloud(n, seed=8)
+    sim.set_particles(x, y, g)
+    px = np.full(500, -0.15)
+    py = 0.01 + 0.002 * np.arange(500)
+    vx, vy = sim.probe(px, py)
+    ovx, ovy = O.probe(p, x, y, g, n, px, py)
+    assert np.abs(vx - ovx).max() < VEL_TOL and np.abs(vy - ovy).max() < VEL_TOL
+    sim.close()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_whole_steps_track_oracle(graph):
+    """Fresh start, 25 whole steps: the particle count follows the oracle
+    exactly and positions/strengths stay within 1e-9 (sum-order rounding
+    only; collapse decisions are exact comparisons on nearly equal inputs)."""
+    sim, pan, ck, p = make(P=200, birth_offset_mode=2)
+    sim.set_graph(graph)
+    _, M = O.panel_matrix(pan)
+    osim = O.OracleSim(p, pan, M)
+    for k in range(25):
+        sim.step(1)
+        osim.step()
+        assert sim.count() == osim.n, f"step {k}"
+    gx, gy, gg = sim.particles()
+    ox, oy, og = osim.particles()
+    assert np.abs(gx - ox).max() < 1e-9 and np.abs(gy - oy).max() < 1e-9
+    assert np.abs(gg - og).max() < 1e-9 * np.abs(og).max()
+    f = sim.forces()
+    assert abs(f[1] - osim.fx) < 1e-6 * max(1, abs(osim.fx))
+    assert abs(f[2] - osim.fy) < 1e-6 * max(1, abs(osim.fy))
+    sim.close()

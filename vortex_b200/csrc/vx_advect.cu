@@ -1,0 +1,126 @@
+// vx_advect.cu — convection r <- r + V dt, absorption of vortices that cross
+// the wall, removal of vortices that leave the window, per-particle force
+// and moment terms, and their deterministic reduction.
+//
+// Reference: step_Kernel src/kernel.cu:1090-1143, hitting :1357-1431,
+// summ_Kernel :1144-1157.  The reference sums serially in one thread; here
+// each thread of a fixed grid accumulates a fixed strided subset, blocks
+// reduce in a fixed tree and one block adds the block sums in order, so the
+// result is run-to-run identical.
+#include "vx_internal.cuh"
+
+// Segment (x2,y2)->(x1,y1) against every panel; nearest crossing wins.
+__device__ bool vx_hitting(const VxParams &p, const vx_panel *pan, double x1, double y1, double x2,
+                           double y2, int *hitpan) {
+    const double thr = 1e-12;
+    double minDist = 25.0;
+    int minN = -1;
+    bool hit = !(((x1 < p.px_min) && (x2 < p.px_min)) || ((x1 > p.px_max) && (x2 > p.px_max)) ||
+                 ((y1 < p.py_min) && (y2 < p.py_min)) || ((y1 > p.py_max) && (y2 > p.py_max)));
+    if (hit) {
+        hit = false;
+        const double A = y2 - y1, B = x1 - x2, D = y1 * x2 - x1 * y2;
+        for (int i = 0; i < p.P; ++i) {
+            const vx_panel &q = pan[i];
+            double r0 = A * q.left[0] + B * q.left[1] + D;
+            double r1 = A * q.right[0] + B * q.right[1] + D;
+            if (fabs(r0) < thr) r0 = 0.0;
+            if (fabs(r1) < thr) r1 = 0.0;
+            if (r0 * r1 <= 0) {
+                double A1 = q.right[1] - q.left[1];
+                double B1 = q.left[0] - q.right[0];
+                double D1 = q.left[1] * q.right[0] - q.left[0] * q.right[1];
+                double r2 = A1 * x1 + B1 * y1 + D1;
+                double r3 = A1 * x2 + B1 * y2 + D1;
+                if (fabs(r2) < thr) r2 = 0.0;
+                if (fabs(r3) < thr) r3 = 0.0;
+                if (r2 * r3 <= 0) {
+                    hit = true;
+                    double den = A * B1 - B * A1;
+                    double X = (B * D1 - D * B1) / den;
+                    double Y = (A1 * D - D1 * A) / den;
+                    double d2 = (x2 - X) * (x2 - X) + (y2 - Y) * (y2 - Y);
+                    if (d2 < minDist) { minDist = d2; minN = i; }
+                }
+            }
+        }
+    }
+    *hitpan = minN;
+    return hit;
+}
+
+__device__ __forceinline__ double vx_block_sum(double v, double *sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, const VxScalars *S,
+                                                       const vx_panel *pan, double *red) {
+    __shared__ double sh[VX_THREADS];
+    const long long n = S->n;
+    const long long n_new0 = S->n0;   // vortices born this step: [n0, n)
+    double sdg = 0.0, sfx = 0.0, sfy = 0.0, sm = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long k = i * v.ps;
+        double x = v.x[k], y = v.y[k], gi = v.g[k];
+        double fx = 0.0, fy = 0.0, m = 0.0;
+        if (i >= n_new0) {
+            double dx = x - p.rc_x, dy = y - p.rc_y;
+            fx = gi * (-y);
+            fy = gi * x;
+            m = gi * fma(dx, dx, dy * dy);
+        }
+        const double xn = fma(v.vx[i * v.vs], p.dt, x);
+        const double yn = fma(v.vy[i * v.vs], p.dt, y);
+        int hp = -1;
+        if (gi != 0 && vx_hitting(p, pan, xn, yn, x, y, &hp)) {
+            if (hp >= 0) {   // the reference reads panels[-1] when no crossing is nearer than 5
+                const double cx = pan[hp].contr[0], cy = pan[hp].contr[1];
+                const double dx = cx - p.rc_x, dy = cy - p.rc_y;
+                fx -= gi * (-cy);
+                fy -= gi * cx;
+                m -= gi * fma(dx, dx, dy * dy);
+            }
+            sdg += gi;
+            gi = 0.0;
+        }
+        double xo = xn, yo = yn;
+        if (gi != 0 && (xn > p.x_max || xn < p.x_min || yn > p.y_max || yn < p.y_min)) {
+            xo = -2.0e5; yo = -2.0e5; gi = 0.0;
+        }
+        v.x[k] = xo; v.y[k] = yo; v.g[k] = gi;
+        sfx += fx; sfy += fy; sm += m;
+    }
+    double t;
+    t = vx_block_sum(sdg, sh); if (threadIdx.x == 0) red[blockIdx.x * 4 + 0] = t;
+    t = vx_block_sum(sfx, sh); if (threadIdx.x == 0) red[blockIdx.x * 4 + 1] = t;
+    t = vx_block_sum(sfy, sh); if (threadIdx.x == 0) red[blockIdx.x * 4 + 2] = t;
+    t = vx_block_sum(sm, sh);  if (threadIdx.x == 0) red[blockIdx.x * 4 + 3] = t;
+}
+
+__global__ void k_sums(VxParams p, VxScalars *S, const double *red, int nblocks) {
+    if (threadIdx.x != 0) return;
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < nblocks; ++b)
+        for (int q = 0; q < 4; ++q) a[q] += red[b * 4 + q];
+    for (int q = 0; q < 4; ++q) S->raw[q] = a[q];
+    S->dg = a[0];
+    S->fx = a[1] * (p.rho / p.dt);
+    S->fy = a[2] * (p.rho / p.dt);
+    S->m = a[3] * (p.rho / (2 * p.dt));
+}
+
+cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                             VxWork &w, const vx_panel *pan) {
+    k_advect<<<VX_RED_BLOCKS, VX_THREADS, 0, L.stream>>>(p, v, S, pan, w.red); VX_COUNT(L);
+    k_sums<<<1, 32, 0, L.stream>>>(p, S, w.red, VX_RED_BLOCKS); VX_COUNT(L);
+    return cudaGetLastError();
+}

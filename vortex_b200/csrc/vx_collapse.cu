@@ -1,0 +1,373 @@
+// vx_collapse.cu — merging of close vortex pairs, two passes (opposite signs,
+// then same sign), each repeated up to n_col times while the count changes.
+//
+// Reference: first_setka_Kernel/second_setka_Kernel src/kernel.cu:1180-1235
+// (COL[i] = smallest j > i that qualifies, an O(N^2) scan per thread),
+// first_collapse_Kernel/second_collapse_Kernel src/kernel.cu:1237-1271 (one
+// thread merges in index order), pass loop src/unit_1.cu:1137-1216.
+//
+// Here:
+//  * COL comes from a uniform cell grid with cells no smaller than the merge
+//    radius (counting sort into cells, 3x3 neighbourhood query).  The distance
+//    test is the same FP64 expression as the oracle's, so COL is identical.
+//  * The serial merge is resolved in parallel.  Candidate i (COL[i] >= 0) is
+//    applied iff no applied candidate points at i; rounds decide every
+//    candidate whose in-pointing candidates are all decided.  An applied i
+//    merges with the original j only if it is the smallest applied candidate
+//    pointing at j; later ones merge with (0, 1e10) as the serial loop does,
+//    which re-rounds their position.
+//  * Compaction then runs as after convection.
+#include <limits.h>
+
+#include "vx_internal.cuh"
+
+__global__ void k_col_begin(VxScalars *S, int reset) {
+    if (reset) S->col_done = 0;
+    if (S->col_done) return;
+    S->col_n_before = S->n;
+    S->ncand = 0;
+    S->bb[0] = S->bb[1] = S->bb[2] = S->bb[3] = ~0ull;
+}
+
+__global__ void k_col_bbox(VxView v, VxScalars *S) {
+    if (S->col_done) return;
+    __shared__ unsigned long long sh[4][VX_THREADS];
+    const long long n = S->n;
+    unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double x = v.x[i * v.ps], y = v.y[i * v.ps];
+        k[0] = min(k[0], vx_dkey(x));
+        k[1] = min(k[1], vx_dkey(-x));
+        k[2] = min(k[2], vx_dkey(y));
+        k[3] = min(k[3], vx_dkey(-y));
+    }
+    for (int q = 0; q < 4; ++q) sh[q][threadIdx.x] = k[q];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int q = 0; q < 4; ++q) sh[q][threadIdx.x] = min(sh[q][threadIdx.x], sh[q][threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; ++q) atomicMin(&S->bb[q], sh[q][0]);
+}
+
+// Cell size h = r (1 + 1e-6): any pair closer than r is in neighbouring cells.
+// When the box would need more than cells_cap cells, h grows.
+__global__ void k_col_grid(VxScalars *S, double r2, long long cells_cap) {
+    if (S->col_done) return;
+    const long long n = S->n;
+    if (n == 0) { S->gncells = 0; S->gnx = S->gny = 0; return; }
+    const double x0 = vx_dunkey(S->bb[0]), x1 = -vx_dunkey(S->bb[1]);
+    const double y0 = vx_dunkey(S->bb[2]), y1 = -vx_dunkey(S->bb[3]);
+    double h = sqrt(r2) * (1.0 + 1e-6);
+    long long nx, ny;
+    for (int it = 0; it < 200; ++it) {
+        double fx = floor((x1 - x0) / h) + 1.0, fy = floor((y1 - y0) / h) + 1.0;
+        if (fx * fy <= (double)cells_cap) { nx = (long long)fx; ny = (long long)fy; break; }
+        h *= 1.25;
+        nx = ny = -1;
+    }
+    if (nx < 0) { S->err |= VX_DERR_GRID; S->gncells = 0; S->col_done = 1; return; }
+    S->gx0 = x0; S->gy0 = y0; S->gh = h;
+    S->gnx = nx; S->gny = ny; S->gncells = nx * ny;
+}
+
+__device__ __forceinline__ void vx_cell_of(const VxScalars *S, double x, double y, long long &cx,
+                                           long long &cy) {
+    cx = (long long)floor((x - S->gx0) / S->gh);
+    cy = (long long)floor((y - S->gy0) / S->gh);
+    cx = cx < 0 ? 0 : (cx >= S->gnx ? S->gnx - 1 : cx);
+    cy = cy < 0 ? 0 : (cy >= S->gny ? S->gny - 1 : cy);
+}
+
+__global__ void k_col_zero_cells(const VxScalars *S, int *cnt) {
+    if (S->col_done) return;
+    const long long nc = S->gncells;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
+         c += (long long)gridDim.x * blockDim.x)
+        cnt[c] = 0;
+}
+
+__global__ void k_col_count(VxView v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
+                            int *has_app, int *first_app) {
+    if (S->col_done) return;
+    const long long n = S->n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long cx, cy;
+        vx_cell_of(S, v.x[i * v.ps], v.y[i * v.ps], cx, cy);
+        const long long c = cy * S->gnx + cx;
+        cellid[i] = (int)c;
+        atomicAdd(&cnt[c], 1);
+        in_cnt[i] = 0;
+        has_app[i] = 0;
+        first_app[i] = INT_MAX;
+    }
+}
+
+// Exclusive scan of cnt[0, gncells) into start[], start[gncells] = total.
+__global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) {
+    if (S->col_done) return;
+    __shared__ int sh[VX_THREADS];
+    const long long nc = S->gncells;
+    const long long nch = vx_ceil_div(nc, VX_CHUNK);
+    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+        int k = 0;
+        for (long long p = c * VX_CHUNK + threadIdx.x; p < min(nc, (c + 1) * VX_CHUNK); p += blockDim.x)
+            k += cnt[p];
+        sh[threadIdx.x] = k;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) csum[c] = sh[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_cell_chunk_scan(const VxScalars *S, const int *csum, long long *coff) {
+    if (S->col_done) return;
+    __shared__ long long sh[1024];
+    __shared__ long long carry;
+    const long long nch = vx_ceil_div(S->gncells, VX_CHUNK);
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long long base = 0; base < nch; base += blockDim.x) {
+        long long c = base + threadIdx.x;
+        long long val = c < nch ? csum[c] : 0;
+        sh[threadIdx.x] = val;
+        __syncthreads();
+        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+            long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (c < nch) coff[c] = carry + sh[threadIdx.x] - val;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += sh[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(VX_THREADS) k_cell_chunk_apply(const VxScalars *S, const int *cnt,
+                                                                 const long long *coff, int *start) {
+    if (S->col_done) return;
+    constexpr int PER = VX_CHUNK / VX_THREADS;
+    __shared__ int sh[VX_THREADS];
+    const long long nc = S->gncells;
+    const long long nch = vx_ceil_div(nc, VX_CHUNK);
+    if (blockIdx.x == 0 && threadIdx.x == 0) start[nc] = (int)S->n;   // sentinel
+    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+        const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
+        int val[PER];
+        int loc = 0;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            val[q] = (b + q < nc) ? cnt[b + q] : 0;
+            loc += val[q];
+        }
+        sh[threadIdx.x] = loc;
+        __syncthreads();
+        for (int o = 1; o < VX_THREADS; o <<= 1) {
+            int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        long long run = coff[c] + sh[threadIdx.x] - loc;
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            if (b + q < nc) start[b + q] = (int)run;
+            run += val[q];
+        }
+    }
+}
+
+__global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *start, int *cnt,
+                              int *sorted) {
+    if (S->col_done) return;
+    const long long n = S->n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c = cellid[i];
+        const int k = atomicSub(&cnt[c], 1) - 1;
+        sorted[start[c] + k] = (int)i;
+    }
+}
+
+// COL[i] = smallest j > i in the 3x3 cell neighbourhood that qualifies.
+template <int PASS>
+__global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
+                            const int *sorted, int *col, int *in_cnt, int *cand) {
+    if (S->col_done) return;
+    const long long n = S->n;
+    const long long gnx = S->gnx, gny = S->gny;
+    const double rd2 = p.r_diff2, rs2 = p.r_same2, mvg = p.max_ve_g;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double xi = v.x[i * v.ps], yi = v.y[i * v.ps], gi = v.g[i * v.ps];
+        const long long c = cellid[i];
+        const long long cx = c % gnx, cy = c / gnx;
+        int best = INT_MAX;
+        for (long long yy = max(cy - 1, 0LL); yy <= min(cy + 1, gny - 1); ++yy) {
+            for (long long xx = max(cx - 1, 0LL); xx <= min(cx + 1, gnx - 1); ++xx) {
+                const long long cc = yy * gnx + xx;
+                for (int k = start[cc]; k < start[cc + 1]; ++k) {
+                    const int j = sorted[k];
+                    if (j <= i || j >= best) continue;
+                    const double gj = v.g[(long long)j * v.ps];
+                    const double dx = xi - v.x[(long long)j * v.ps], dy = yi - v.y[(long long)j * v.ps];
+                    const double r2 = fma(dx, dx, dy * dy);
+                    bool ok;
+                    if (PASS == 1) ok = (gi * gj < 0) && (r2 < rd2);
+                    else ok = (gi * gj > 0) && (r2 < rs2) && (fabs(gi + gj) < mvg);
+                    if (ok) best = j;
+                }
+            }
+        }
+        if (best != INT_MAX) {
+            col[i] = best;
+            atomicAdd(&in_cnt[best], 1);
+            const int slot = atomicAdd(&S->ncand, 1);
+            cand[slot] = (int)i;
+        } else {
+            col[i] = -1;
+        }
+    }
+}
+
+// Rounds over the candidate list (single block).  cstate: 0 undecided,
+// 1 applied, 2 consumed before its turn.
+__global__ void k_col_resolve(VxScalars *S, const int *cand, const int *col, int *in_cnt,
+                              int *has_app, int *first_app, int *cstate, int *cdec) {
+    if (S->col_done) return;
+    __shared__ int undecided;
+    const int nc = S->ncand;
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) cstate[k] = 0;
+    __syncthreads();
+    const int max_rounds = nc + 2;
+    int round = 0;
+    for (; round < max_rounds; ++round) {
+        for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+            int d = 0;
+            if (cstate[k] == 0) {
+                const int i = cand[k];
+                if (has_app[i]) d = 2;
+                else if (in_cnt[i] == 0) d = 1;
+            }
+            cdec[k] = d;
+        }
+        if (threadIdx.x == 0) undecided = 0;
+        __syncthreads();
+        for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+            if (cstate[k] != 0) continue;
+            const int d = cdec[k];
+            if (d == 0) { atomicAdd(&undecided, 1); continue; }
+            cstate[k] = d;
+            const int i = cand[k], j = col[i];
+            atomicSub(&in_cnt[j], 1);
+            if (d == 1) {
+                has_app[j] = 1;
+                atomicMin(&first_app[j], i);
+            }
+        }
+        __syncthreads();
+        if (undecided == 0) break;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && round >= max_rounds) {
+        S->err |= VX_DERR_RESOLVE;
+        S->col_done = 1;
+    }
+}
+
+template <int PASS>
+__global__ void k_col_merge(VxView v, const VxScalars *S, const int *cand, const int *col,
+                            const int *cstate, const int *first_app, double *mx, double *my,
+                            double *mg) {
+    if (S->col_done) return;
+    const int nc = S->ncand;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+        if (cstate[k] != 1) continue;
+        const long long i = cand[k], j = col[i];
+        const double xi = v.x[i * v.ps], yi = v.y[i * v.ps], gi = v.g[i * v.ps];
+        double xj = 1e10, yj = 1e10, gj = 0.0;
+        if (first_app[j] == i) { xj = v.x[j * v.ps]; yj = v.y[j * v.ps]; gj = v.g[j * v.ps]; }
+        if (PASS == 1) {
+            const double ai = fabs(gi), aj = fabs(gj);
+            const double mn = ai + aj;
+            mx[k] = (xi * ai + xj * aj) / fabs(mn);
+            my[k] = (yi * ai + yj * aj) / fabs(mn);
+            mg[k] = gi + gj;
+        } else {
+            const double ng = gi + gj;
+            mx[k] = (xi * gi + xj * gj) / ng;
+            my[k] = (yi * gi + yj * gj) / ng;
+            mg[k] = ng;
+        }
+    }
+}
+
+__global__ void k_col_apply(VxView v, const VxScalars *S, const int *cand, const int *col,
+                            const int *cstate, const double *mx, const double *my, const double *mg) {
+    if (S->col_done) return;
+    const int nc = S->ncand;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+        if (cstate[k] != 1) continue;
+        const long long i = cand[k], j = col[i];
+        v.x[i * v.ps] = mx[k]; v.y[i * v.ps] = my[k]; v.g[i * v.ps] = mg[k];
+        v.x[j * v.ps] = 1e10; v.y[j * v.ps] = 1e10; v.g[j * v.ps] = 0.0;
+    }
+}
+
+__global__ void k_col_end(VxScalars *S) {
+    if (S->col_done) return;
+    if (S->n == S->col_n_before) S->col_done = 1;
+}
+
+cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                               VxWork &w, int pass, int n_col) {
+    const double r2 = pass == 1 ? p.r_diff2 : p.r_same2;
+    if (!(r2 > 0.0) || n_col <= 0) return cudaSuccess;   // no pair can qualify
+    const int grid = L.num_sms * 4;
+    for (int cc = 0; cc < n_col; ++cc) {
+        k_col_begin<<<1, 1, 0, L.stream>>>(S, cc == 0); VX_COUNT(L);
+        k_col_bbox<<<grid, VX_THREADS, 0, L.stream>>>(v, S); VX_COUNT(L);
+        k_col_grid<<<1, 1, 0, L.stream>>>(S, r2, w.cells_cap); VX_COUNT(L);
+        k_col_zero_cells<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cell_cnt); VX_COUNT(L);
+        k_col_count<<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app,
+                                                       w.first_app); VX_COUNT(L);
+        k_cell_chunk_sum<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cell_cnt, w.cell_chunk_cnt); VX_COUNT(L);
+        k_cell_chunk_scan<<<1, 1024, 0, L.stream>>>(S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
+        k_cell_chunk_apply<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cell_cnt, w.cell_chunk_off,
+                                                              w.cell_start); VX_COUNT(L);
+        k_col_scatter<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cellid, w.cell_start, w.cell_cnt,
+                                                         w.sorted); VX_COUNT(L);
+        if (pass == 1)
+            k_col_query<1><<<grid, VX_THREADS, 0, L.stream>>>(p, v, S, w.cellid, w.cell_start, w.sorted,
+                                                              w.col, w.in_cnt, w.cand);
+        else
+            k_col_query<2><<<grid, VX_THREADS, 0, L.stream>>>(p, v, S, w.cellid, w.cell_start, w.sorted,
+                                                              w.col, w.in_cnt, w.cand);
+        VX_COUNT(L);
+        k_col_resolve<<<1, 1024, 0, L.stream>>>(S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app,
+                                                w.cstate, w.cdec); VX_COUNT(L);
+        if (pass == 1)
+            k_col_merge<1><<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cand, w.col, w.cstate, w.first_app,
+                                                              w.mx, w.my, w.mg);
+        else
+            k_col_merge<2><<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cand, w.col, w.cstate, w.first_app,
+                                                              w.mx, w.my, w.mg);
+        VX_COUNT(L);
+        k_col_apply<<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cand, w.col, w.cstate, w.mx, w.my, w.mg);
+        VX_COUNT(L);
+        vx_launch_compact_skip(L, p, v, S, w, &S->col_done);
+        k_col_end<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
+    }
+    return cudaGetLastError();
+}

@@ -1,0 +1,690 @@
+// vx_engine.cu — the vx_sim handle and the native C ABI (include/vortex_b200.h).
+//
+// A handle keeps one body resident on its device: panels, the inverted
+// panel system, SoA particle arrays (x, y, G, Vx, Vy, d) and scratch.  The
+// live count stays in device memory; the host keeps only an upper bound
+// (births add P per step, nothing else adds) and reads the true count back
+// when the store may have to grow.  A step is launched as a fixed sequence,
+// so after the first call it is recorded into a CUDA graph and replayed.
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "vx_internal.cuh"
+
+static thread_local std::string g_err;
+
+void vx_set_error(const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+extern "C" const char *vx_last_error(void) { return g_err.c_str(); }
+
+extern "C" const char *vx_status_str(vx_status s) {
+    switch (s) {
+    case VX_OK: return "ok";
+    case VX_ERR_CUDA: return "CUDA error";
+    case VX_ERR_ARG: return "bad argument";
+    case VX_ERR_IO: return "I/O error";
+    case VX_ERR_SINGULAR: return "singular panel system";
+    case VX_ERR_NOMEM: return "out of memory";
+    case VX_ERR_DEVICE: return "device error flag";
+    case VX_ERR_BUDGET: return "HBM budget exceeded";
+    }
+    return "unknown";
+}
+
+#define CU(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            vx_set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return e_ == cudaErrorMemoryAllocation ? VX_ERR_NOMEM : VX_ERR_CUDA;            \
+        }                                                                                   \
+    } while (0)
+
+struct vx_sim {
+    vx_conf conf;
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    int P = 0, P32 = 0;
+    VxParams prm;
+    vx_panel *d_pan = nullptr;
+    double *d_minv = nullptr;
+    VxScalars *d_S = nullptr;
+    VxScalars *h_S = nullptr;     // pinned mirror
+    long long cap = 0;
+    double *x = nullptr, *y = nullptr, *g = nullptr, *vx = nullptr, *vy = nullptr, *d = nullptr;
+    VxWork w;
+    std::vector<void *> work_allocs;
+    long long n_upper = 0;
+    long long launches = 0;
+    // graph
+    bool use_graph = true;
+    cudaGraphExec_t gexec = nullptr;
+    long long g_cap = -1;
+    int g_kv = -1, g_rhs = -1;
+    long long g_launches = 0;
+    // timing
+    bool timing = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double t_acc[3] = {0, 0, 0};
+    // probe scratch
+    double *d_probe = nullptr;
+    long long probe_cap = 0;
+};
+
+static VxLaunch launch_of(vx_sim *s) {
+    VxLaunch L;
+    L.stream = s->stream;
+    L.launches = &s->launches;
+    L.num_sms = s->num_sms;
+    return L;
+}
+
+static VxView view_of(vx_sim *s) {
+    VxView v;
+    v.x = s->x; v.y = s->y; v.g = s->g; v.ps = 1;
+    v.vx = s->vx; v.vy = s->vy; v.vs = 1;
+    v.d = s->d;
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// parameters (reference init_device_conf_values, src/unit_1.cu:1220-1252)
+void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams *p) {
+    memset(p, 0, sizeof(*p));
+    p->dt = c->dt;
+    p->nu = c->viscosity;
+    p->rho = c->rho;
+    p->eps = c->ve_size;
+    p->eps2 = c->ve_size * c->ve_size;
+    p->r_diff2 = c->r_col_diff_sign * c->r_col_diff_sign * p->eps2;
+    p->r_same2 = c->r_col_same_sign * c->r_col_same_sign * p->eps2;
+    p->max_ve_g = c->max_ve_g;
+    p->x_min = c->x_min; p->x_max = c->x_max; p->y_min = c->y_min; p->y_max = c->y_max;
+    // profile bbox from the left endpoints, started from the window's
+    // opposite edges (src/main.c:235-254)
+    double xmn = c->x_max, xmx = c->x_min, ymn = c->y_max, ymx = c->y_min;
+    double bx0 = 1e300, bx1 = -1e300, by0 = 1e300, by1 = -1e300, lmax = 0.0;
+    for (int i = 0; i < P; ++i) {
+        double xx = pan[i].left[0], yy = pan[i].left[1];
+        if (xx < xmn) xmn = xx;
+        if (xx > xmx) xmx = xx;
+        if (yy < ymn) ymn = yy;
+        if (yy > ymx) ymx = yy;
+        bx0 = std::min(bx0, pan[i].birth[0]); bx1 = std::max(bx1, pan[i].birth[0]);
+        by0 = std::min(by0, pan[i].birth[1]); by1 = std::max(by1, pan[i].birth[1]);
+        lmax = std::max(lmax, pan[i].length);
+    }
+    p->px_min = xmn; p->px_max = xmx; p->py_min = ymn; p->py_max = ymx;
+    // a particle farther than 5 L_max from every birth point gets no wall term
+    const double m = 5.0 * lmax * (1.0 + 1e-9) + 1e-12;
+    p->wall_x0 = bx0 - m; p->wall_x1 = bx1 + m; p->wall_y0 = by0 - m; p->wall_y1 = by1 + m;
+    p->rc_x = c->rc_x; p->rc_y = c->rc_y;
+    p->drop_eps = c->drop_eps;
+    p->diff_cutoff = c->diff_cutoff;
+    p->P = P;
+    p->n_of_points = (int)c->n_of_points;
+    p->birth_mode = c->birth_offset_mode;
+    p->prec = c->precision;
+}
+
+extern "C" vx_status vx_conf_default(vx_conf *c) {
+    if (!c) return VX_ERR_ARG;
+    memset(c, 0, sizeof(*c));
+    c->log_level = 3;
+    c->v_inf_incr_steps = 1;
+    c->precision = VX_PREC_FP64;
+    c->birth_offset_mode = VX_BIRTH_REF;
+    c->drop_eps = 1e-12;
+    c->diff_cutoff = 30.0;
+    return VX_OK;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_fill_tail(double *x, double *y, double *g, long long from, long long to) {
+    for (long long i = from + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < to;
+         i += (long long)gridDim.x * blockDim.x) {
+        x[i] = 4.0e5 + (double)i;
+        y[i] = 4.0e5 + (double)i;
+        g[i] = 0.0;
+    }
+}
+
+template <typename T>
+static vx_status dalloc(std::vector<void *> &allocs, T **p, long long count) {
+    void *q = nullptr;
+    if (count < 1) count = 1;
+    CU(cudaMalloc(&q, sizeof(T) * (size_t)count));
+    allocs.push_back(q);
+    *p = (T *)q;
+    return VX_OK;
+}
+
+void vx_work_free(VxWork &w, std::vector<void *> &allocs) {
+    for (void *q : allocs) cudaFree(q);
+    allocs.clear();
+    memset(&w, 0, sizeof(w));
+}
+
+// Scratch for a particle capacity `cap` and a panel count padded to P32.
+vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms) {
+    vx_work_free(w, allocs);
+    w.cap = cap;
+    const long long nch = cap / VX_CHUNK + 2;
+    vx_status st;
+#define A(ptr, n) if ((st = dalloc(allocs, &(ptr), (n))) != VX_OK) return st
+    A(w.cmp_cnt, nch); A(w.cmp_off, nch);
+    A(w.hole_pos, cap); A(w.hole_src, cap); A(w.tail_src, cap);
+    A(w.hx, cap); A(w.hy, cap); A(w.hg, cap); A(w.tx, cap); A(w.ty, cap);
+    w.cells_cap = std::max(4 * cap, 65536LL);
+    A(w.cellid, cap); A(w.cell_cnt, w.cells_cap); A(w.cell_start, w.cells_cap + 1); A(w.sorted, cap);
+    A(w.col, cap); A(w.in_cnt, cap); A(w.has_app, cap); A(w.first_app, cap);
+    A(w.cand, cap); A(w.cstate, cap); A(w.cdec, cap);
+    A(w.mx, cap); A(w.my, cap); A(w.mg, cap);
+    A(w.cell_chunk_cnt, w.cells_cap / VX_CHUNK + 2); A(w.cell_chunk_off, w.cells_cap / VX_CHUNK + 2);
+    // pair partials: K * n <= num_sms*8*tile + n for the split K the launchers pick
+    w.part_cap = 5LL * ((long long)num_sms * 8 * 1024 + cap + 1024);
+    A(w.part, w.part_cap);
+    A(w.src32, cap);
+    w.rhs_part_cap = (long long)num_sms * 4 * P32 * 2;
+    A(w.rhs_part, w.rhs_part_cap);
+    A(w.R, P32); A(w.gamma, P32);
+    A(w.red, VX_RED_BLOCKS * 4);
+#undef A
+    return VX_OK;
+}
+
+static void free_work(vx_sim *s) { vx_work_free(s->w, s->work_allocs); }
+
+static vx_status alloc_work(vx_sim *s, long long cap) {
+    return vx_work_alloc(s->w, s->work_allocs, cap, s->P32, s->num_sms);
+}
+
+static void drop_graph(vx_sim *s) {
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+    s->g_cap = -1;
+}
+
+// Grow the particle store to at least `need` slots, keeping every slot's
+// content (the dead tail matters: it enters the next 3-nearest search).
+static vx_status grow(vx_sim *s, long long need) {
+    long long ncap = std::max(need, s->cap + std::max<long long>(s->conf.inc_step, 8192));
+    ncap = std::max(ncap, (long long)(s->cap * 1.25));
+    ncap = vx_ceil_div(ncap, 8192) * 8192;
+    double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};
+    double *nar[6];
+    for (int k = 0; k < 6; ++k) {
+        CU(cudaMalloc(&nar[k], sizeof(double) * ncap));
+        if (s->cap > 0)
+            CU(cudaMemcpyAsync(nar[k], arr[k], sizeof(double) * s->cap, cudaMemcpyDeviceToDevice, s->stream));
+        else
+            CU(cudaMemsetAsync(nar[k], 0, sizeof(double) * ncap, s->stream));
+    }
+    k_fill_tail<<<s->num_sms * 4, 256, 0, s->stream>>>(nar[0], nar[1], nar[2], s->cap, ncap);
+    ++s->launches;
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s->stream));
+    for (int k = 0; k < 6; ++k) cudaFree(arr[k]);
+    s->x = nar[0]; s->y = nar[1]; s->g = nar[2]; s->vx = nar[3]; s->vy = nar[4]; s->d = nar[5];
+    s->cap = ncap;
+    drop_graph(s);
+    return alloc_work(s, ncap);
+}
+
+static vx_status read_scalars(vx_sim *s) {
+    CU(cudaMemcpyAsync(s->h_S, s->d_S, sizeof(VxScalars), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    s->n_upper = s->h_S->n;
+    if (s->h_S->err) {
+        vx_set_error("device error flag 0x%x", s->h_S->err);
+        return VX_ERR_DEVICE;
+    }
+    return VX_OK;
+}
+
+static long long need_for(vx_sim *s, long long n) { return vx_round32(n + s->P) + 64; }
+
+static vx_status ensure_capacity(vx_sim *s) {
+    if (need_for(s, s->n_upper) <= s->cap) return VX_OK;
+    vx_status st = read_scalars(s);
+    if (st != VX_OK) return st;
+    if (need_for(s, s->n_upper) <= s->cap) return VX_OK;
+    return grow(s, need_for(s, s->n_upper));
+}
+
+static int rhs_chunks_for(vx_sim *s) {
+    const int tiles = (s->P + 127) / 128;
+    long long want = std::max(1LL, (long long)s->num_sms * 4 / tiles);
+    long long bysrc = std::max(1LL, vx_ceil_div(s->n_upper, 2048));
+    return (int)std::min(want, bysrc);
+}
+
+static int kv_for(vx_sim *s) {
+    const int tile = s->prm.prec == VX_PREC_FP32 ? 1024 : 512;
+    return vx_pick_ksplit(s->n_upper + s->P, tile, s->num_sms);
+}
+
+// ---------------------------------------------------------------------------
+extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t P, int device,
+                               vx_sim **out) {
+    if (!conf || !pan || P < 2 || !out) { vx_set_error("vx_create: bad arguments"); return VX_ERR_ARG; }
+    if (conf->dt <= 0 || conf->ve_size <= 0 || conf->n_of_points < 1) {
+        vx_set_error("vx_create: dt, ve_size and n_of_points must be positive");
+        return VX_ERR_ARG;
+    }
+    for (int64_t i = 0; i < P; ++i) {
+        if (pan[i].n_of_rpanel >= (uint32_t)P || pan[i].n_of_lpanel >= (uint32_t)P) {
+            vx_set_error("vx_create: panel %lld has a neighbour index outside [0,%lld)", (long long)i,
+                         (long long)P);
+            return VX_ERR_ARG;
+        }
+    }
+    vx_sim *s = new vx_sim();
+    s->conf = *conf;
+    s->device = device;
+    s->P = (int)P;
+    s->P32 = (int)vx_round32(P);
+    *out = nullptr;
+    auto fail = [&](vx_status st) { vx_destroy(s); return st; };
+    if (cudaSetDevice(device) != cudaSuccess) { vx_set_error("cudaSetDevice(%d) failed", device); return fail(VX_ERR_CUDA); }
+    cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VX_ERR_CUDA);
+    vx_params_from_conf(conf, pan, (int)P, &s->prm);
+    std::vector<vx_panel> hp(s->P32);
+    memset(hp.data(), 0, sizeof(vx_panel) * s->P32);
+    memcpy(hp.data(), pan, sizeof(vx_panel) * P);
+    if (cudaMalloc(&s->d_pan, sizeof(vx_panel) * s->P32) != cudaSuccess) return fail(VX_ERR_NOMEM);
+    if (cudaMemcpy(s->d_pan, hp.data(), sizeof(vx_panel) * s->P32, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(VX_ERR_CUDA);
+    if (cudaMalloc(&s->d_S, sizeof(VxScalars)) != cudaSuccess) return fail(VX_ERR_NOMEM);
+    if (cudaMallocHost(&s->h_S, sizeof(VxScalars)) != cudaSuccess) return fail(VX_ERR_NOMEM);
+    memset(s->h_S, 0, sizeof(VxScalars));
+    // V_inf ramp (src/main.c:585-592): with a ramp the flow starts at rest
+    s->h_S->incr_steps = conf->v_inf_incr_steps;
+    if (conf->v_inf_incr_steps > 0) {
+        s->h_S->dvinf[0] = conf->v_inf_x / (double)conf->v_inf_incr_steps;
+        s->h_S->dvinf[1] = conf->v_inf_y / (double)conf->v_inf_incr_steps;
+    } else {
+        s->h_S->vinf[0] = conf->v_inf_x;
+        s->h_S->vinf[1] = conf->v_inf_y;
+    }
+    if (cudaMemcpy(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(VX_ERR_CUDA);
+    // panel system on the device
+    const long long S1 = P + 1;
+    if (cudaMalloc(&s->d_minv, sizeof(double) * S1 * S1) != cudaSuccess) return fail(VX_ERR_NOMEM);
+    double *work = nullptr;
+    int *flag = nullptr;
+    if (cudaMalloc(&work, sizeof(double) * (2 * S1 * S1 + S1)) != cudaSuccess) return fail(VX_ERR_NOMEM);
+    if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) { cudaFree(work); return fail(VX_ERR_NOMEM); }
+    VxLaunch L = launch_of(s);
+    cudaError_t e = vx_build_matrix(L, s->d_pan, (int)P, s->d_minv, work, flag, nullptr);
+    int hflag = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(work);
+    cudaFree(flag);
+    if (e != cudaSuccess) { vx_set_error("panel system: %s", cudaGetErrorString(e)); return fail(VX_ERR_CUDA); }
+    if (hflag) { vx_set_error("panel system is singular (pivot < 1e-12)"); return fail(VX_ERR_SINGULAR); }
+    vx_status st = grow(s, std::max<long long>(need_for(s, 0), conf->inc_step > 0 ? conf->inc_step : 8192));
+    if (st != VX_OK) return fail(st);
+    *out = s;
+    return VX_OK;
+}
+
+extern "C" vx_status vx_destroy(vx_sim *s) {
+    if (!s) return VX_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    drop_graph(s);
+    free_work(s);
+    double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};
+    for (double *a : arr) if (a) cudaFree(a);
+    if (s->d_pan) cudaFree(s->d_pan);
+    if (s->d_minv) cudaFree(s->d_minv);
+    if (s->d_S) cudaFree(s->d_S);
+    if (s->h_S) cudaFreeHost(s->h_S);
+    if (s->d_probe) cudaFree(s->d_probe);
+    for (auto &e : s->ev) if (e) cudaEventDestroy(e);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return VX_OK;
+}
+
+// ---------------------------------------------------------------------------
+static vx_status set_count(vx_sim *s, long long n) {
+    CU(cudaMemcpyAsync(s->h_S, s->d_S, sizeof(VxScalars), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    s->h_S->n = n;
+    s->h_S->n0 = n >= s->P ? n - s->P : 0;   // the last P count as this step's newborns
+    CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    s->n_upper = n;
+    return VX_OK;
+}
+
+extern "C" vx_status vx_set_particles(vx_sim *s, const double *x, const double *y, const double *g,
+                                      int64_t n) {
+    if (!s || n < 0 || (n > 0 && (!x || !y || !g))) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    if (need_for(s, n) > s->cap) {
+        vx_status st = grow(s, need_for(s, n));
+        if (st != VX_OK) return st;
+    }
+    if (n > 0) {
+        CU(cudaMemcpyAsync(s->x, x, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(s->y, y, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+        CU(cudaMemcpyAsync(s->g, g, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+    }
+    return set_count(s, n);
+}
+
+extern "C" vx_status vx_set_velocity(vx_sim *s, const double *vx, const double *vy, const double *d,
+                                     int64_t n) {
+    if (!s || n < 0 || n > s->cap) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    if (n > 0) {
+        if (vx) CU(cudaMemcpyAsync(s->vx, vx, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+        if (vy) CU(cudaMemcpyAsync(s->vy, vy, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+        if (d) CU(cudaMemcpyAsync(s->d, d, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+    }
+    CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}
+
+extern "C" vx_status vx_get_count(vx_sim *s, int64_t *n) {
+    if (!s || !n) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    vx_status st = read_scalars(s);
+    *n = s->h_S->n;
+    return st;
+}
+
+extern "C" vx_status vx_get_particles(vx_sim *s, double *x, double *y, double *g, int64_t cap,
+                                      int64_t *n) {
+    if (!s || !n) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    vx_status st = read_scalars(s);
+    if (st != VX_OK) return st;
+    long long m = s->h_S->n;
+    *n = m;
+    if (cap < m) return x ? VX_ERR_ARG : VX_OK;
+    if (m > 0 && x && y && g) {
+        CU(cudaMemcpyAsync(x, s->x, sizeof(double) * m, cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaMemcpyAsync(y, s->y, sizeof(double) * m, cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaMemcpyAsync(g, s->g, sizeof(double) * m, cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaStreamSynchronize(s->stream));
+    }
+    return VX_OK;
+}
+
+// Raw slots [0, count) including the dead tail (for parity tests).
+extern "C" vx_status vx_get_slots(vx_sim *s, double *x, double *y, double *g, int64_t count) {
+    if (!s || count < 0 || count > s->cap) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    CU(cudaMemcpyAsync(x, s->x, sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(y, s->y, sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(g, s->g, sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}
+
+// Write raw slots [0, count) (tail included) and set the live count.
+extern "C" vx_status vx_set_slots(vx_sim *s, const double *x, const double *y, const double *g,
+                                  int64_t count, int64_t n) {
+    if (!s || count < 0 || n < 0 || n > count) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    if (need_for(s, count) > s->cap) {
+        vx_status st = grow(s, need_for(s, count));
+        if (st != VX_OK) return st;
+    }
+    CU(cudaMemcpyAsync(s->x, x, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
+    CU(cudaMemcpyAsync(s->y, y, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
+    CU(cudaMemcpyAsync(s->g, g, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
+    return set_count(s, n);
+}
+
+extern "C" vx_status vx_get_velocity(vx_sim *s, double *vx, double *vy, double *d, int64_t cap) {
+    if (!s) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    vx_status st = read_scalars(s);
+    if (st != VX_OK) return st;
+    long long m = std::min<long long>(s->h_S->n, cap);
+    if (m > 0) {
+        if (vx) CU(cudaMemcpyAsync(vx, s->vx, sizeof(double) * m, cudaMemcpyDeviceToHost, s->stream));
+        if (vy) CU(cudaMemcpyAsync(vy, s->vy, sizeof(double) * m, cudaMemcpyDeviceToHost, s->stream));
+        if (d) CU(cudaMemcpyAsync(d, s->d, sizeof(double) * m, cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaStreamSynchronize(s->stream));
+    }
+    return VX_OK;
+}
+
+extern "C" vx_status vx_get_forces(vx_sim *s, double out4[4]) {
+    if (!s || !out4) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    vx_status st = read_scalars(s);
+    out4[0] = s->h_S->dg; out4[1] = s->h_S->fx; out4[2] = s->h_S->fy; out4[3] = s->h_S->m;
+    return st;
+}
+
+// n, n0, step, vinf x/y, dg, fx, fy, m
+extern "C" vx_status vx_get_state(vx_sim *s, double out9[9]) {
+    if (!s || !out9) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    vx_status st = read_scalars(s);
+    const VxScalars &h = *s->h_S;
+    double v[9] = {(double)h.n, (double)h.n0, (double)h.step, h.vinf[0], h.vinf[1], h.dg, h.fx, h.fy, h.m};
+    memcpy(out9, v, sizeof(v));
+    return st;
+}
+
+static vx_status patch_scalars(vx_sim *s, void (*fn)(VxScalars *, const double *), const double *a) {
+    CU(cudaMemcpyAsync(s->h_S, s->d_S, sizeof(VxScalars), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    fn(s->h_S, a);
+    CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}
+
+extern "C" vx_status vx_set_vinf(vx_sim *s, double vx, double vy) {
+    if (!s) return VX_ERR_ARG;
+    double a[2] = {vx, vy};
+    return patch_scalars(s, [](VxScalars *h, const double *q) { h->vinf[0] = q[0]; h->vinf[1] = q[1]; }, a);
+}
+
+extern "C" vx_status vx_set_dg(vx_sim *s, double dg) {
+    if (!s) return VX_ERR_ARG;
+    return patch_scalars(s, [](VxScalars *h, const double *q) { h->dg = q[0]; }, &dg);
+}
+
+// Absolute step index (restart from a KadrNNNNNN file sets it).
+extern "C" vx_status vx_set_step_index(vx_sim *s, int64_t step) {
+    if (!s || step < 0) return VX_ERR_ARG;
+    double a = (double)step;
+    return patch_scalars(s, [](VxScalars *h, const double *q) { h->step = (long long)q[0]; }, &a);
+}
+
+extern "C" vx_status vx_get_matrix(vx_sim *s, double *minv) {
+    if (!s || !minv) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    const long long S1 = s->P + 1;
+    CU(cudaMemcpy(minv, s->d_minv, sizeof(double) * S1 * S1, cudaMemcpyDeviceToHost));
+    return VX_OK;
+}
+
+// ---------------------------------------------------------------------------
+static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
+    VxLaunch L = launch_of(s);
+    VxView v = view_of(s);
+    const VxParams &p = s->prm;
+    cudaError_t e = cudaSuccess;
+    const int kv = kv_for(s);
+    auto ev = [&](int k) { if (s->timing && !whole_step) cudaEventRecord(s->ev[k], s->stream); };
+    ev(0);
+    if (mask & VX_STAGE_BIRTH) {
+        if ((e = vx_launch_step_begin(L, s->d_S)) != cudaSuccess) return e;
+        if ((e = vx_launch_birth(L, p, v, s->d_S, s->w, s->d_pan, s->d_minv, rhs_chunks_for(s))) != cudaSuccess) return e;
+    }
+    ev(1);
+    if (mask & VX_STAGE_VELOCITY)
+        if ((e = vx_launch_velocity(L, p, v, s->d_S, s->w, kv)) != cudaSuccess) return e;
+    if (mask & VX_STAGE_DIFFUSION)
+        if ((e = vx_launch_diffusion(L, p, v, s->d_S, s->w, kv)) != cudaSuccess) return e;
+    if (mask & VX_STAGE_WALL)
+        if ((e = vx_launch_wall(L, p, v, s->d_S, s->d_pan)) != cudaSuccess) return e;
+    ev(2);
+    if (mask & VX_STAGE_ADVECT)
+        if ((e = vx_launch_advect(L, p, v, s->d_S, s->w, s->d_pan)) != cudaSuccess) return e;
+    if (mask & VX_STAGE_COMPACT)
+        if ((e = vx_launch_compact(L, p, v, s->d_S, s->w)) != cudaSuccess) return e;
+    if (mask & VX_STAGE_COLLAPSE1)
+        if ((e = vx_launch_collapse(L, p, v, s->d_S, s->w, 1, (int)s->conf.n_col)) != cudaSuccess) return e;
+    if (mask & VX_STAGE_COLLAPSE2)
+        if ((e = vx_launch_collapse(L, p, v, s->d_S, s->w, 2, (int)s->conf.n_col)) != cudaSuccess) return e;
+    if (whole_step) e = vx_launch_step_end(L, s->d_S);
+    ev(3);
+    return e;
+}
+
+extern "C" vx_status vx_stage(vx_sim *s, unsigned mask) {
+    if (!s) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    vx_status st = ensure_capacity(s);
+    if (st != VX_OK) return st;
+    CU(launch_stages(s, mask, false));
+    if (mask & VX_STAGE_BIRTH) s->n_upper += s->P;
+    return read_scalars(s);
+}
+
+static vx_status step_once(vx_sim *s) {
+    vx_status st = ensure_capacity(s);
+    if (st != VX_OK) return st;
+    if (s->timing) {
+        // timed steps run eagerly so per-stage events can be recorded
+        CU(launch_stages(s, VX_STAGE_ALL, false));
+        CU(vx_launch_step_end(launch_of(s), s->d_S));
+        s->n_upper += s->P;
+        return VX_OK;
+    }
+    if (!s->use_graph) {
+        CU(launch_stages(s, VX_STAGE_ALL, true));
+        s->n_upper += s->P;
+        return VX_OK;
+    }
+    const int kv = kv_for(s), rc = rhs_chunks_for(s);
+    if (!s->gexec || s->g_cap != s->cap || s->g_kv != kv || s->g_rhs != rc) {
+        drop_graph(s);
+        cudaGraph_t graph;
+        long long before = s->launches;
+        CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = launch_stages(s, VX_STAGE_ALL, true);
+        cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            vx_set_error("graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+            return VX_ERR_CUDA;
+        }
+        s->g_launches = s->launches - before;
+        s->launches = before;
+        e = cudaGraphInstantiate(&s->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) { vx_set_error("graph instantiate: %s", cudaGetErrorString(e)); return VX_ERR_CUDA; }
+        s->g_cap = s->cap; s->g_kv = kv; s->g_rhs = rc;
+    }
+    CU(cudaGraphLaunch(s->gexec, s->stream));
+    s->launches += s->g_launches;
+    s->n_upper += s->P;
+    return VX_OK;
+}
+
+extern "C" vx_status vx_step(vx_sim *s, int64_t nsteps) {
+    if (!s || nsteps < 0) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    for (int64_t k = 0; k < nsteps; ++k) {
+        vx_status st = step_once(s);
+        if (st != VX_OK) return st;
+        if (s->timing) {
+            CU(cudaEventSynchronize(s->ev[3]));
+            float a, b, c;
+            cudaEventElapsedTime(&a, s->ev[0], s->ev[1]);
+            cudaEventElapsedTime(&b, s->ev[1], s->ev[2]);
+            cudaEventElapsedTime(&c, s->ev[2], s->ev[3]);
+            s->t_acc[0] += a; s->t_acc[1] += b; s->t_acc[2] += c;
+        }
+    }
+    CU(cudaGetLastError());
+    return VX_OK;
+}
+
+extern "C" vx_status vx_sync(vx_sim *s) {
+    if (!s) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    return read_scalars(s);
+}
+
+extern "C" vx_status vx_set_graph(vx_sim *s, int enable) {
+    if (!s) return VX_ERR_ARG;
+    s->use_graph = enable != 0;
+    if (!s->use_graph) drop_graph(s);
+    return VX_OK;
+}
+
+extern "C" vx_status vx_set_timing(vx_sim *s, int enable) {
+    if (!s) return VX_ERR_ARG;
+    s->timing = enable != 0;
+    if (s->timing && !s->ev[0])
+        for (auto &e : s->ev) CU(cudaEventCreate(&e));
+    s->t_acc[0] = s->t_acc[1] = s->t_acc[2] = 0.0;
+    return VX_OK;
+}
+
+extern "C" vx_status vx_get_timing(vx_sim *s, double out3[3]) {
+    if (!s || !out3) return VX_ERR_ARG;
+    for (int k = 0; k < 3; ++k) out3[k] = s->t_acc[k];
+    return VX_OK;
+}
+
+extern "C" vx_status vx_get_launch_count(vx_sim *s, int64_t *count) {
+    if (!s || !count) return VX_ERR_ARG;
+    *count = s->launches;
+    return VX_OK;
+}
+
+// The stream the handle launches on (for callers that time with events).
+extern "C" void *vx_get_stream(vx_sim *s) { return s ? (void *)s->stream : nullptr; }
+
+extern "C" vx_status vx_probe(vx_sim *s, const double *px, const double *py, int64_t np, double *ovx,
+                              double *ovy) {
+    if (!s || np < 0 || (np > 0 && (!px || !py || !ovx || !ovy))) return VX_ERR_ARG;
+    if (np == 0) return VX_OK;
+    CU(cudaSetDevice(s->device));
+    if (s->probe_cap < np) {
+        if (s->d_probe) cudaFree(s->d_probe);
+        s->d_probe = nullptr;
+        CU(cudaMalloc(&s->d_probe, sizeof(double) * 4 * np));
+        s->probe_cap = np;
+    }
+    double *dpx = s->d_probe, *dpy = dpx + np, *dvx = dpy + np, *dvy = dvx + np;
+    CU(cudaMemcpyAsync(dpx, px, sizeof(double) * np, cudaMemcpyHostToDevice, s->stream));
+    CU(cudaMemcpyAsync(dpy, py, sizeof(double) * np, cudaMemcpyHostToDevice, s->stream));
+    const int tile = s->prm.prec == VX_PREC_FP32 ? 1024 : 512;
+    const int K = vx_pick_ksplit(np, tile, s->num_sms);
+    CU(vx_launch_probe(launch_of(s), s->prm, view_of(s), s->d_S, s->w, dpx, dpy, 1, np, dvx, dvy, 1, K));
+    CU(cudaMemcpyAsync(ovx, dvx, sizeof(double) * np, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(ovy, dvy, sizeof(double) * np, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}

@@ -1,0 +1,185 @@
+// vx_internal.cuh — shared device structures, helpers and stage launchers of
+// libvortex_b200.  Every stage reads the live particle count from device
+// memory (VxScalars::n), so a whole step is launched without host round
+// trips and the launch shapes do not depend on the particle count.
+//
+// Floating-point contract: the library is compiled with -fmad=false; every
+// fused multiply-add is an explicit fma()/fmaf(), the same calls the CPU
+// oracle makes.  This keeps the 3-nearest distances, compaction, collapse
+// pairing and merge, and the advection bit-identical to the oracle.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/vortex_b200.h"
+
+#define VX_TWO_PI 6.283185307179586
+#define VX_PI 3.141592653589793
+
+// ---------------------------------------------------------------------------
+// Particle storage view.  Element i of x/y/g is at [i*ps], of vx/vy at
+// [i*vs]: structure-of-arrays (ps = vs = 1) for the native engine, the
+// reference's AoS Vortex/PVortex records (ps = 3, vs = 2) for the
+// unit_1.cuh-compatible entry points.
+struct VxView {
+    double *x, *y, *g;
+    long long ps;
+    double *vx, *vy;
+    long long vs;
+    double *d;
+};
+
+// Resolved run parameters (reference: __constant__ symbols filled by
+// init_device_conf_values, src/unit_1.cu:20-44,1220-1252).
+struct VxParams {
+    double dt, nu, rho;
+    double eps, eps2;
+    double r_diff2, r_same2, max_ve_g;
+    double x_min, x_max, y_min, y_max;          // wake window
+    double px_min, px_max, py_min, py_max;      // profile bbox (left endpoints)
+    double wall_x0, wall_x1, wall_y0, wall_y1;  // birth-point bbox grown by 5 L_max
+    double rc_x, rc_y;
+    double drop_eps;
+    double diff_cutoff;
+    int P;
+    int n_of_points;
+    int birth_mode;
+    int prec;
+};
+
+// Device-resident scalars of one body.
+struct VxScalars {
+    long long n;           // live particle count
+    long long n0;          // count before this step's birth
+    long long step;        // completed steps
+    long long incr_steps;  // V_inf ramp length (src/main.c:586-592,654-659)
+    double vinf[2];
+    double dvinf[2];
+    double dg;             // circulation absorbed by the last convection
+    double fx, fy, m;      // force and moment of the last step
+    double raw[4];         // unscaled sums of dg, Fx, Fy, M of the last convection
+    // compaction
+    long long c_n0, c_m, c_H, c_scan_m;
+    // collapse
+    long long col_n_before;
+    int col_done;
+    int ncand;
+    unsigned long long bb[4];  // ordered keys of x_min, -x_max, y_min, -y_max
+    double gx0, gy0, gh;
+    long long gnx, gny, gncells;
+    int err;
+    int pad_;
+};
+
+enum {
+    VX_DERR_RESOLVE = 1,     // collapse resolution did not converge
+    VX_DERR_GRID = 2,        // collapse grid did not fit its cell capacity
+};
+
+// Device scratch of one body.  Sizes are in elements.
+struct VxWork {
+    long long cap;           // particle capacity the arrays below were sized for
+    // compaction
+    int *cmp_cnt;
+    long long *cmp_off;
+    int *hole_pos, *hole_src, *tail_src;
+    double *hx, *hy, *hg, *tx, *ty;
+    // collapse
+    long long cells_cap;
+    int *cellid, *cell_cnt, *cell_start, *sorted;
+    int *col, *in_cnt, *has_app, *first_app, *cand, *cstate, *cdec;
+    double *mx, *my, *mg;
+    long long *cell_chunk_off;
+    int *cell_chunk_cnt;
+    // pair partial sums
+    double *part;
+    long long part_cap;      // doubles
+    float4 *src32;           // packed FP32 sources (bulk form)
+    // birth
+    double *rhs_part;        // [chunks][P32][2]
+    long long rhs_part_cap;
+    double *R, *gamma;
+    // reductions
+    double *red;             // [blocks][4]
+};
+
+// Compaction chunk size (elements per scan chunk).
+constexpr int VX_CHUNK = 2048;
+constexpr int VX_RED_BLOCKS = 592;   // 4 x 148 SMs: fixed, so sums are deterministic
+constexpr int VX_THREADS = 256;
+
+// ---------------------------------------------------------------------------
+// helpers
+__host__ __device__ inline long long vx_ceil_div(long long a, long long b) { return (a + b - 1) / b; }
+__host__ __device__ inline long long vx_round32(long long v) { return (v + 31) / 32 * 32; }
+
+// Keep the 3 smallest squared distances (src/kernel.cu:941-953): the result
+// is the same for any visiting order.
+template <typename T>
+__device__ __forceinline__ void vx_nn3_insert(T &d1, T &d2, T &d3, T r2) {
+    if (d3 > r2) {
+        d3 = r2;
+        T t = fmin(d3, d2); d3 = fmax(d3, d2); d2 = t;
+        t = fmin(d1, d2); d2 = fmax(d1, d2); d1 = t;
+    }
+}
+
+// Monotonic unsigned key of a double (for atomicMin on signed values).
+__device__ __forceinline__ unsigned long long vx_dkey(double v) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double vx_dunkey(unsigned long long k) {
+    unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+// ---------------------------------------------------------------------------
+// Launch context: stream + launch counter shared by all stage launchers.
+struct VxLaunch {
+    cudaStream_t stream;
+    long long *launches;   // host counter (may be null)
+    int num_sms;
+};
+#define VX_COUNT(L) do { if ((L).launches) ++*(L).launches; } while (0)
+
+// Stage launchers (each returns the first CUDA error it saw).
+cudaError_t vx_launch_step_begin(const VxLaunch &L, VxScalars *S);
+cudaError_t vx_launch_birth(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                            VxWork &w, const vx_panel *pan, const double *minv, int rhs_chunks);
+cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                               VxWork &w, int ksplit);
+cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                                VxWork &w, int ksplit);
+cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                           const vx_panel *pan);
+cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                             VxWork &w, const vx_panel *pan);
+cudaError_t vx_launch_compact(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                              VxWork &w);
+cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                               VxWork &w, int pass, int n_col);
+cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                            VxWork &w, const double *px, const double *py, long long pstride,
+                            long long np, double *out_vx, double *out_vy, long long ostride,
+                            int ksplit);
+// Panel system on the device: L (P+1)^2 then Gauss-Jordan inverse.
+// d_L_out (nullable) receives a copy of the influence matrix before elimination.
+cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, double *d_minv,
+                            double *d_work, int *d_flag, double *d_L_out);
+cudaError_t vx_launch_birth_ld(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                               VxWork &w, const vx_panel *pan, const double *minv, long long ld,
+                               int rhs_chunks);
+cudaError_t vx_launch_step_end(const VxLaunch &L, VxScalars *S);
+cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const VxView &v,
+                                   VxScalars *S, VxWork &w, const int *skip);
+void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams *p);
+void vx_set_error(const char *fmt, ...);
+#include <vector>
+vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms);
+void vx_work_free(VxWork &w, std::vector<void *> &allocs);
+
+// Split factor so that (target tiles x source chunks) fills the GPU.
+int vx_pick_ksplit(long long n_upper, int tile, int num_sms);

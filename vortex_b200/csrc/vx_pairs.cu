@@ -1,0 +1,365 @@
+// vx_pairs.cu — direct pair sums: convective (Biot-Savart) velocity with the
+// mean distance to the 3 nearest particles, vortex-vortex diffusive velocity,
+// and the probe velocity.
+//
+// Reference: shared_Kernel src/kernel.cu:875-983, diffusion_Kernel
+// src/kernel.cu:985-1029, velocity_control_Kernel src/kernel.cu:1434-1475.
+//
+// Work decomposition: a target tile (TPT targets per thread, 256 threads) x a
+// source chunk is one work item; persistent CTAs walk the items.  Sources are
+// staged through shared memory 256 at a time and read as warp-wide broadcasts.
+// Each item writes partial sums; a combine kernel adds the chunks in a fixed
+// order, so results are deterministic for a given split.
+//
+// Precision: FP64 (plain form) computes every pair in double.  FP32 (bulk
+// form) computes pairs in float and accumulates each 256-source tile in
+// float, adding tile sums into a double accumulator (blocked compensation).
+#include "vx_internal.cuh"
+
+constexpr int PT = 256;       // threads per block = sources per shared tile
+
+__host__ __device__ constexpr int pairs_tpt(bool fp32) { return fp32 ? 4 : 2; }
+
+int vx_pick_ksplit(long long n_upper, int tile, int num_sms) {
+    long long tiles = vx_ceil_div(n_upper > 0 ? n_upper : 1, tile);
+    long long want = (long long)num_sms * 8;
+    long long k = vx_ceil_div(want, tiles);
+    if (k < 1) k = 1;
+    if (k > 64) k = 64;
+    return (int)k;
+}
+
+// ---------------------------------------------------------------------------
+// Packed FP32 sources for the bulk form: (x, y, G, 0), G masked to 0 beyond n.
+__global__ void k_pack32(VxView v, const VxScalars *S, float4 *src, long long upto) {
+    const long long n = S->n;
+    const long long s = vx_round32(n);
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < s;
+         j += (long long)gridDim.x * blockDim.x) {
+        if (j >= upto) break;
+        src[j] = make_float4((float)v.x[j * v.ps], (float)v.y[j * v.ps],
+                             j < n ? (float)v.g[j * v.ps] : 0.0f, 0.0f);
+    }
+}
+
+template <typename T> struct PairMath;
+template <> struct PairMath<double> {
+    static __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+};
+template <> struct PairMath<float> {
+    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+};
+
+// Sources of one shared tile.
+template <typename T>
+struct SrcTile {
+    T x[PT], y[PT], g[PT];
+};
+
+template <typename T>
+__device__ __forceinline__ void load_src(SrcTile<T> &t, const VxView &v, const float4 *src32,
+                                         long long j, long long jend, long long nvel) {
+    if (j < jend) {
+        if (src32) {
+            float4 q = src32[j];
+            t.x[threadIdx.x] = (T)q.x; t.y[threadIdx.x] = (T)q.y; t.g[threadIdx.x] = (T)q.z;
+        } else {
+            t.x[threadIdx.x] = (T)v.x[j * v.ps];
+            t.y[threadIdx.x] = (T)v.y[j * v.ps];
+            t.g[threadIdx.x] = j < nvel ? (T)v.g[j * v.ps] : (T)0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Biot-Savart (+ 3 nearest when NN3).  Targets: particles (nt < 0 -> n) or
+// probe points (tx/ty with stride tstr).  Partials: [sc][5][tstride].
+template <typename T, bool NN3>
+__global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const VxScalars *S,
+                                                   const float4 *src32, const double *tx,
+                                                   const double *ty, long long tstr, long long nt_in,
+                                                   double *part, long long tstride, int K) {
+    constexpr int TPT = pairs_tpt(sizeof(T) == 4);
+    constexpr int NOUT = NN3 ? 5 : 2;
+    __shared__ SrcTile<T> st;
+    const long long n = S->n;
+    const long long nt = nt_in < 0 ? n : nt_in;
+    const long long srange = NN3 ? vx_round32(n) : n;
+    const long long tile = (long long)PT * TPT;
+    const long long tiles = vx_ceil_div(nt, tile);
+    const long long cs = vx_ceil_div(vx_ceil_div(srange, K), PT) * PT;
+    const long long items = tiles * K;
+    const T eps2 = (T)p.eps2;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const long long tt = it % tiles, sc = it / tiles;
+        T ax[TPT], ay[TPT];
+        long long ti[TPT];
+        double vxa[TPT], vya[TPT];
+        T d1[TPT], d2[TPT], d3[TPT];
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+            ti[k] = tt * tile + (long long)k * PT + threadIdx.x;
+            long long i = ti[k] < nt ? ti[k] : 0;
+            ax[k] = (T)tx[i * tstr];
+            ay[k] = (T)ty[i * tstr];
+            vxa[k] = 0.0; vya[k] = 0.0;
+            d1[k] = d2[k] = d3[k] = (T)1e5;
+        }
+        const long long j0 = sc * cs, j1 = min(srange, j0 + cs);
+        for (long long jt = j0; jt < j1; jt += PT) {
+            __syncthreads();
+            load_src<T>(st, v, src32, jt + threadIdx.x, j1, n);
+            __syncthreads();
+            const int cnt = (int)min((long long)PT, j1 - jt);
+            T sx[TPT], sy[TPT];
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) { sx[k] = 0; sy[k] = 0; }
+            for (int q = 0; q < cnt; ++q) {
+                const T bx = st.x[q], by = st.y[q], bg = st.g[q];
+                const long long j = jt + q;
+#pragma unroll
+                for (int k = 0; k < TPT; ++k) {
+                    T dx = ax[k] - bx, dy = ay[k] - by;
+                    T r2 = fma(dx, dx, dy * dy);
+                    if (NN3) {
+                        T r2n = (j == ti[k]) ? (T)INFINITY : r2;
+                        vx_nn3_insert<T>(d1[k], d2[k], d3[k], r2n);
+                    }
+                    T m = bg * PairMath<T>::rcp(fmax(r2, eps2));
+                    sy[k] = fma(m, dx, sy[k]);
+                    sx[k] = fma(-m, dy, sx[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) { vxa[k] += (double)sx[k]; vya[k] += (double)sy[k]; }
+        }
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+            if (ti[k] < nt) {
+                double *o = part + (long long)sc * NOUT * tstride + ti[k];
+                o[0] = vxa[k];
+                o[tstride] = vya[k];
+                if (NN3) {
+                    o[2 * tstride] = (double)d1[k];
+                    o[3 * tstride] = (double)d2[k];
+                    o[4 * tstride] = (double)d3[k];
+                }
+            }
+        }
+    }
+}
+
+// Combine: V = sum/(2 pi) + V_inf, d = mean of the 3 nearest distances.
+template <bool FP32>
+__global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, long long tstride,
+                             int K) {
+    const long long n = S->n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double sx = 0.0, sy = 0.0;
+        double d1 = 1e5, d2 = 1e5, d3 = 1e5;
+        for (int sc = 0; sc < K; ++sc) {
+            const double *o = part + (long long)sc * 5 * tstride + i;
+            sx += o[0];
+            sy += o[tstride];
+            vx_nn3_insert<double>(d1, d2, d3, o[2 * tstride]);
+            vx_nn3_insert<double>(d1, d2, d3, o[3 * tstride]);
+            vx_nn3_insert<double>(d1, d2, d3, o[4 * tstride]);
+        }
+        if (FP32)
+            v.d[i] = (double)((sqrtf((float)d1) + sqrtf((float)d2) + sqrtf((float)d3)) / 3);
+        else
+            v.d[i] = (sqrt(d1) + sqrt(d2) + sqrt(d3)) / 3;
+        v.vx[i * v.vs] = sx / VX_TWO_PI + S->vinf[0];
+        v.vy[i * v.vs] = sy / VX_TWO_PI + S->vinf[1];
+    }
+}
+
+__global__ void k_probe_combine(const VxScalars *S, const double *part, long long tstride, int K,
+                                long long np, double *ovx, double *ovy, long long ostride) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < np;
+         i += (long long)gridDim.x * blockDim.x) {
+        double sx = 0.0, sy = 0.0;
+        for (int sc = 0; sc < K; ++sc) {
+            const double *o = part + (long long)sc * 2 * tstride + i;
+            sx += o[0];
+            sy += o[tstride];
+        }
+        ovx[i * ostride] = sx / VX_TWO_PI + S->vinf[0];
+        ovy[i * ostride] = sy / VX_TWO_PI + S->vinf[1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Vortex-vortex diffusion (src/kernel.cu:985-1029).  Partials [sc][3][tstride].
+template <typename T>
+struct DiffMath;
+template <> struct DiffMath<double> {
+    // dist = sqrt(r2); 1/dist; exp(-dist/dd)
+    static __device__ __forceinline__ void eval(double r2, double ndd, double &dist, double &rd,
+                                                double &e) {
+        dist = sqrt(r2);
+        rd = __drcp_rn(dist);
+        e = exp(dist * ndd);
+    }
+};
+template <> struct DiffMath<float> {
+    static __device__ __forceinline__ void eval(float r2, float ndd, float &dist, float &rd,
+                                                float &e) {
+        rd = rsqrtf(r2);
+        dist = r2 * rd;
+        e = __expf(dist * ndd);
+    }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const VxScalars *S,
+                                                     const float4 *src32, double *part,
+                                                     long long tstride, int K) {
+    constexpr int TPT = pairs_tpt(sizeof(T) == 4);
+    __shared__ SrcTile<T> st;
+    const long long n = S->n;
+    const long long tile = (long long)PT * TPT;
+    const long long tiles = vx_ceil_div(n, tile);
+    const long long cs = vx_ceil_div(vx_ceil_div(n, K), PT) * PT;
+    const long long items = tiles * K;
+    const T thr = (T)(0.001 * p.eps);
+    const T thr2 = thr * thr;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const long long tt = it % tiles, sc = it / tiles;
+        T ax[TPT], ay[TPT], ndd[TPT];
+        long long ti[TPT];
+        double a2x[TPT], a2y[TPT], a1[TPT];
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+            ti[k] = tt * tile + (long long)k * PT + threadIdx.x;
+            long long i = ti[k] < n ? ti[k] : 0;
+            ax[k] = (T)v.x[i * v.ps];
+            ay[k] = (T)v.y[i * v.ps];
+            ndd[k] = -(T)1 / (T)v.d[i];
+            a2x[k] = a2y[k] = a1[k] = 0.0;
+        }
+        const long long j0 = sc * cs, j1 = min(n, j0 + cs);
+        for (long long jt = j0; jt < j1; jt += PT) {
+            __syncthreads();
+            load_src<T>(st, v, src32, jt + threadIdx.x, j1, n);
+            __syncthreads();
+            const int cnt = (int)min((long long)PT, j1 - jt);
+            T s2x[TPT], s2y[TPT], s1[TPT];
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) { s2x[k] = 0; s2y[k] = 0; s1[k] = 0; }
+            for (int q = 0; q < cnt; ++q) {
+                const T bx = st.x[q], by = st.y[q], bg = st.g[q];
+#pragma unroll
+                for (int k = 0; k < TPT; ++k) {
+                    T dx = ax[k] - bx, dy = ay[k] - by;
+                    T r2 = fma(dx, dx, dy * dy);
+                    T dist, rd, e;
+                    DiffMath<T>::eval(r2, ndd[k], dist, rd, e);
+                    bool use = sizeof(T) == 8 ? (dist > thr) : (r2 > thr2);
+                    T ge = use ? bg * e : (T)0;
+                    T me = use ? ge * rd : (T)0;   // r = 0 would give 0 * inf
+                    s2x[k] = fma(-me, dx, s2x[k]);
+                    s2y[k] = fma(-me, dy, s2y[k]);
+                    s1[k] += ge;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < TPT; ++k) {
+                a2x[k] += (double)s2x[k]; a2y[k] += (double)s2y[k]; a1[k] += (double)s1[k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+            if (ti[k] < n) {
+                double *o = part + (long long)sc * 3 * tstride + ti[k];
+                o[0] = a2x[k];
+                o[tstride] = a2y[k];
+                o[2 * tstride] = a1[k];
+            }
+        }
+    }
+}
+
+__global__ void k_diff_combine(VxParams p, VxView v, const VxScalars *S, const double *part,
+                               long long tstride, int K) {
+    const long long n = S->n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
+        for (int sc = 0; sc < K; ++sc) {
+            const double *o = part + (long long)sc * 3 * tstride + i;
+            I2x += o[0];
+            I2y += o[tstride];
+            I1 += o[2 * tstride];
+        }
+        if (fabs(I1) > 1e-5) {
+            const double dd = v.d[i];
+            v.vx[i * v.vs] += -p.nu * I2x / (I1 * dd);
+            v.vy[i * v.vs] += -p.nu * I2y / (I1 * dd);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+static int pair_grid(const VxLaunch &L) { return L.num_sms * 4; }
+
+static cudaError_t maybe_pack(const VxLaunch &L, const VxParams &p, const VxView &v,
+                              VxScalars *S, VxWork &w) {
+    if (p.prec != VX_PREC_FP32) return cudaSuccess;
+    k_pack32<<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.src32, w.cap);
+    VX_COUNT(L);
+    return cudaGetLastError();
+}
+
+cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                               VxWork &w, int K) {
+    const long long tstride = w.part_cap / (5LL * K);
+    if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
+    if (p.prec == VX_PREC_FP32) {
+        k_bs_partial<float, true><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, w.src32, v.x, v.y, v.ps,
+                                                                     -1, w.part, tstride, K);
+        VX_COUNT(L);
+        k_bs_combine<true><<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.part, tstride, K);
+    } else {
+        k_bs_partial<double, true><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, v.x, v.y, v.ps,
+                                                                      -1, w.part, tstride, K);
+        VX_COUNT(L);
+        k_bs_combine<false><<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.part, tstride, K);
+    }
+    VX_COUNT(L);
+    return cudaGetLastError();
+}
+
+cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                                VxWork &w, int K) {
+    const long long tstride = w.part_cap / (3LL * K);
+    if (p.prec == VX_PREC_FP32) {
+        k_diff_partial<float><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, w.src32, w.part, tstride, K);
+    } else {
+        k_diff_partial<double><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, w.part, tstride, K);
+    }
+    VX_COUNT(L);
+    k_diff_combine<<<L.num_sms * 4, 256, 0, L.stream>>>(p, v, S, w.part, tstride, K);
+    VX_COUNT(L);
+    return cudaGetLastError();
+}
+
+cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                            VxWork &w, const double *px, const double *py, long long pstride,
+                            long long np, double *ovx, double *ovy, long long ostride, int K) {
+    const long long tstride = w.part_cap / (2LL * K);
+    if (tstride < np) return cudaErrorInvalidValue;
+    if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
+    if (p.prec == VX_PREC_FP32)
+        k_bs_partial<float, false><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, w.src32, px, py, pstride,
+                                                                      np, w.part, tstride, K);
+    else
+        k_bs_partial<double, false><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, px, py, pstride,
+                                                                       np, w.part, tstride, K);
+    VX_COUNT(L);
+    k_probe_combine<<<(int)vx_ceil_div(np, 256), 256, 0, L.stream>>>(S, w.part, tstride, K, np, ovx, ovy,
+                                                                      ostride);
+    VX_COUNT(L);
+    return cudaGetLastError();
+}

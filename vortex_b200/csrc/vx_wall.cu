@@ -1,0 +1,85 @@
+// vx_wall.cu — diffusive velocity induced by the wall.
+//
+// Reference: diffusion_2_Kernel src/kernel.cu:1031-1088 with the panel
+// integral I_0_I_3 (FP64 twin src/kernel.cu:1300-1322, FP32 1324-1346).
+// A panel contributes only when the particle is within 5 L of the panel's
+// birth point, so particles outside the birth-point bounding box grown by
+// 5 L_max skip the panel loop: their contribution is exactly +0.
+#include "vx_internal.cuh"
+
+template <typename T>
+__device__ __forceinline__ T vx_exp(T x);
+template <> __device__ __forceinline__ double vx_exp<double>(double x) { return exp(x); }
+template <> __device__ __forceinline__ float vx_exp<float>(float x) { return expf(x); }
+template <typename T>
+__device__ __forceinline__ T vx_sqrt(T x);
+template <> __device__ __forceinline__ double vx_sqrt<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float vx_sqrt<float>(float x) { return sqrtf(x); }
+
+// n_of_points-point midpoint rule along the panel (same expression order as
+// the oracle's wall_integral).
+template <typename T>
+__device__ void vx_wall_integral(T Ra0, T Ra1, T Rb0, T Rb1, T N0, T N1, T Rj0, T Rj1, T dL, T d,
+                                 int N, T &R0, T &R30, T &R31) {
+    T dR0 = (Rb0 - Ra0) / (T)N, dR1 = (Rb1 - Ra1) / (T)N;
+    T delt = dL / (T)N;
+    T s0 = 0, s30 = 0, s31 = 0;
+    for (int k = 0; k < N; ++k) {
+        T Rk0 = (Ra0 + (T)k * dR0 + Ra0 + (T)(k + 1) * dR0) / 2;
+        T Rk1 = (Ra1 + (T)k * dR1 + Ra1 + (T)(k + 1) * dR1) / 2;
+        T E0 = (Rj0 - Rk0) / d, E1 = (Rj1 - Rk1) / d;
+        T e2 = fma(E0, E0, E1 * E1);
+        T me = vx_sqrt<T>(e2);
+        T ex = vx_exp<T>(-me);
+        s0 += (E0 * N0 + E1 * N1) / e2 * (me + 1) * ex * delt;
+        s30 += N0 * ex * delt;
+        s31 += N1 * ex * delt;
+    }
+    R0 = s0; R30 = s30; R31 = s31;
+}
+
+template <typename T>
+__global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel *pan) {
+    const long long n = S->n;
+    const T nu = (T)p.nu;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double xd = v.x[i * v.ps], yd = v.y[i * v.ps];
+        if (xd < p.wall_x0 || xd > p.wall_x1 || yd < p.wall_y0 || yd > p.wall_y1) continue;
+        const T a0 = (T)xd, a1 = (T)yd, dd = (T)v.d[i];
+        T I0 = (T)VX_TWO_PI * dd * dd, I30 = 0, I31 = 0;
+        for (int f = 0; f < p.P; ++f) {
+            const vx_panel &pf = pan[f];
+            const T dL = (T)pf.length;
+            T dx = a0 - (T)pf.birth[0], dy = a1 - (T)pf.birth[1];
+            T r = vx_sqrt<T>(fma(dx, dx, dy * dy));
+            if (r < 5 * dL && r > (T)0.1 * dL) {
+                T R0, R30, R31;
+                vx_wall_integral<T>((T)pf.left[0], (T)pf.left[1], (T)pf.right[0], (T)pf.right[1],
+                                    -(T)pf.norm[0], -(T)pf.norm[1], a0, a1, dL, dd, p.n_of_points,
+                                    R0, R30, R31);
+                I0 += (-dd) * R0;
+                I30 -= R30;
+                I31 -= R31;
+            } else if (r <= (T)0.1 * dL) {
+                T ex = 1 - vx_exp<T>(-dL / (2 * dd));
+                I0 = (T)VX_PI * dd * dd;
+                I30 = 2 * (T)pf.norm[0] * dd * ex;
+                I31 = 2 * (T)pf.norm[1] * dd * ex;
+                break;
+            }
+        }
+        v.vx[i * v.vs] += (double)(nu * I30 / I0);
+        v.vy[i * v.vs] += (double)(nu * I31 / I0);
+    }
+}
+
+cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                           const vx_panel *pan) {
+    if (p.prec == VX_PREC_FP32)
+        k_wall<float><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan);
+    else
+        k_wall<double><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan);
+    VX_COUNT(L);
+    return cudaGetLastError();
+}

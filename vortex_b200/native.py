@@ -1,0 +1,233 @@
+"""ctypes binding of libvortex_b200.so (include/vortex_b200.h).
+
+The library is the product; this module only marshals numpy arrays through
+its C ABI.  Importing it on a machine without the built library raises: there
+is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .profiles import PANEL_DTYPE
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvortex_b200.so")
+
+PREC_FP64, PREC_FP32 = 0, 1
+BIRTH_REF, BIRTH_FILE, BIRTH_HALF_PANEL = 0, 1, 2
+STAGE = dict(birth=1, velocity=2, diffusion=4, wall=8, advect=16, compact=32,
+             collapse1=64, collapse2=128, all=0xFF)
+
+
+class Conf(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64), ("saving_step", C.c_int64), ("inc_step", C.c_int64),
+        ("n_of_points", C.c_int64), ("n_col", C.c_int64), ("v_inf_incr_steps", C.c_int64),
+        ("tree_depth", C.c_int64),
+        ("dt", C.c_double), ("viscosity", C.c_double), ("rho", C.c_double),
+        ("v_inf_x", C.c_double), ("v_inf_y", C.c_double),
+        ("x_max", C.c_double), ("x_min", C.c_double), ("y_max", C.c_double), ("y_min", C.c_double),
+        ("ve_size", C.c_double), ("h_col_x", C.c_double), ("h_col_y", C.c_double),
+        ("rc_x", C.c_double), ("rc_y", C.c_double),
+        ("r_col_diff_sign", C.c_double), ("r_col_same_sign", C.c_double), ("max_ve_g", C.c_double),
+        ("rel_t", C.c_double), ("theta", C.c_double),
+        ("matrix_load", C.c_int32), ("steady_flow", C.c_int32), ("log_level", C.c_int32),
+        ("no_log_buf", C.c_int32),
+        ("pr_file", C.c_char * 256), ("timings_file", C.c_char * 256), ("kadr_file", C.c_char * 256),
+        ("second_points_file", C.c_char * 256), ("log_file", C.c_char * 256),
+        ("precision", C.c_int32), ("birth_offset_mode", C.c_int32),
+        ("drop_eps", C.c_double), ("diff_cutoff", C.c_double),
+        ("n_probes_grid", C.c_int32), ("pad1_", C.c_int32), ("probe_box", C.c_double * 4),
+    ]
+
+
+class VxError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise VxError(f"{LIB_PATH} is missing: build it with `python -m vortex_b200.build`")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.vx_last_error.restype = C.c_char_p
+        _lib.vx_status_str.restype = C.c_char_p
+        _lib.vx_get_stream.restype = C.c_void_p
+        _lib.vx_get_stream.argtypes = [C.c_void_p]
+        for name in ("vx_create",):
+            getattr(_lib, name).argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+    return _lib
+
+
+def _check(rc, what=""):
+    if rc != 0:
+        L = lib()
+        raise VxError(f"{what}: {L.vx_status_str(rc).decode()} ({L.vx_last_error().decode()})")
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def default_conf(**kw) -> Conf:
+    c = Conf()
+    _check(lib().vx_conf_default(C.byref(c)), "vx_conf_default")
+    base = dict(steps=400, saving_step=50, inc_step=8192, n_of_points=20, n_col=2, v_inf_incr_steps=0,
+                dt=0.005, viscosity=1e-3, rho=1.0, v_inf_x=1.0, v_inf_y=0.0,
+                x_max=10.0, x_min=-2.0, y_max=10.0, y_min=-10.0, ve_size=0.0157,
+                rc_x=0.0, rc_y=0.0, r_col_diff_sign=0.0, r_col_same_sign=0.3, max_ve_g=1e30)
+    base.update(kw)
+    for k, v in base.items():
+        if isinstance(v, str):
+            v = v.encode()
+        setattr(c, k, v)
+    return c
+
+
+def read_conf(path: str, conf: Conf | None = None) -> Conf:
+    c = conf if conf is not None else default_conf()
+    _check(lib().vx_conf_read(path.encode(), C.byref(c)), "vx_conf_read")
+    return c
+
+
+def read_profile(path: str) -> np.ndarray:
+    P = C.c_int64(0)
+    _check(lib().vx_profile_read(path.encode(), None, C.c_int64(0), C.byref(P)), "vx_profile_read")
+    pan = np.zeros(P.value, dtype=PANEL_DTYPE)
+    _check(lib().vx_profile_read(path.encode(), _p(pan), C.c_int64(P.value), C.byref(P)), "vx_profile_read")
+    return pan
+
+
+class Sim:
+    """One body resident on a GPU (vx_sim)."""
+
+    def __init__(self, conf: Conf, panels: np.ndarray, device: int = 0):
+        self.conf = conf
+        self.pan = np.ascontiguousarray(panels, dtype=PANEL_DTYPE)
+        self.P = len(self.pan)
+        self.h = C.c_void_p()
+        _check(lib().vx_create(C.byref(conf), _p(self.pan), C.c_int64(self.P), C.c_int(device),
+                               C.byref(self.h)), "vx_create")
+
+    def close(self):
+        if self.h:
+            lib().vx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- state -----------------------------------------------------------
+    def set_particles(self, x, y, g):
+        x, y, g = _f64(x), _f64(y), _f64(g)
+        _check(lib().vx_set_particles(self.h, _p(x), _p(y), _p(g), C.c_int64(len(x))), "vx_set_particles")
+
+    def set_slots(self, x, y, g, n):
+        x, y, g = _f64(x), _f64(y), _f64(g)
+        _check(lib().vx_set_slots(self.h, _p(x), _p(y), _p(g), C.c_int64(len(x)), C.c_int64(n)), "vx_set_slots")
+
+    def get_slots(self, count):
+        x, y, g = np.zeros(count), np.zeros(count), np.zeros(count)
+        _check(lib().vx_get_slots(self.h, _p(x), _p(y), _p(g), C.c_int64(count)), "vx_get_slots")
+        return x, y, g
+
+    def set_velocity(self, vx=None, vy=None, d=None):
+        n = len(vx) if vx is not None else len(d)
+        arrs = [None if a is None else _f64(a) for a in (vx, vy, d)]
+        ptrs = [None if a is None else _p(a) for a in arrs]
+        _check(lib().vx_set_velocity(self.h, *ptrs, C.c_int64(n)), "vx_set_velocity")
+
+    def count(self) -> int:
+        n = C.c_int64(0)
+        _check(lib().vx_get_count(self.h, C.byref(n)), "vx_get_count")
+        return n.value
+
+    def particles(self):
+        n = self.count()
+        x, y, g = np.zeros(n), np.zeros(n), np.zeros(n)
+        m = C.c_int64(0)
+        _check(lib().vx_get_particles(self.h, _p(x), _p(y), _p(g), C.c_int64(n), C.byref(m)), "vx_get_particles")
+        return x, y, g
+
+    def velocity(self):
+        n = self.count()
+        vx, vy, d = np.zeros(n), np.zeros(n), np.zeros(n)
+        _check(lib().vx_get_velocity(self.h, _p(vx), _p(vy), _p(d), C.c_int64(n)), "vx_get_velocity")
+        return vx, vy, d
+
+    def forces(self):
+        o = np.zeros(4)
+        _check(lib().vx_get_forces(self.h, _p(o)), "vx_get_forces")
+        return o
+
+    def state(self):
+        o = np.zeros(9)
+        _check(lib().vx_get_state(self.h, _p(o)), "vx_get_state")
+        return dict(n=int(o[0]), n0=int(o[1]), step=int(o[2]), vinf=(o[3], o[4]), dg=o[5],
+                    fx=o[6], fy=o[7], m=o[8])
+
+    def matrix(self):
+        M = np.zeros((self.P + 1, self.P + 1))
+        _check(lib().vx_get_matrix(self.h, _p(M)), "vx_get_matrix")
+        return M
+
+    def set_dg(self, dg):
+        _check(lib().vx_set_dg(self.h, C.c_double(dg)), "vx_set_dg")
+
+    def set_vinf(self, vx, vy):
+        _check(lib().vx_set_vinf(self.h, C.c_double(vx), C.c_double(vy)), "vx_set_vinf")
+
+    def set_step_index(self, k):
+        _check(lib().vx_set_step_index(self.h, C.c_int64(k)), "vx_set_step_index")
+
+    # --- running -----------------------------------------------------------
+    def step(self, nsteps: int = 1):
+        _check(lib().vx_step(self.h, C.c_int64(nsteps)), "vx_step")
+
+    def stage(self, *names):
+        mask = 0
+        for nm in names:
+            mask |= STAGE[nm]
+        _check(lib().vx_stage(self.h, C.c_uint(mask)), "vx_stage")
+
+    def sync(self):
+        _check(lib().vx_sync(self.h), "vx_sync")
+
+    def probe(self, px, py):
+        px, py = _f64(px), _f64(py)
+        vx, vy = np.zeros(len(px)), np.zeros(len(px))
+        _check(lib().vx_probe(self.h, _p(px), _p(py), C.c_int64(len(px)), _p(vx), _p(vy)), "vx_probe")
+        return vx, vy
+
+    def set_graph(self, on: bool):
+        _check(lib().vx_set_graph(self.h, C.c_int(int(on))), "vx_set_graph")
+
+    def set_timing(self, on: bool):
+        _check(lib().vx_set_timing(self.h, C.c_int(int(on))), "vx_set_timing")
+
+    def timing(self):
+        o = np.zeros(3)
+        _check(lib().vx_get_timing(self.h, _p(o)), "vx_get_timing")
+        return o
+
+    def launches(self) -> int:
+        n = C.c_int64(0)
+        _check(lib().vx_get_launch_count(self.h, C.byref(n)), "vx_get_launch_count")
+        return n.value
+
+    def stream(self) -> int:
+        return lib().vx_get_stream(self.h) or 0
