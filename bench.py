@@ -1,0 +1,377 @@
+"""Benchmark of the vortex-element time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n N0]
+
+Workload (the cylinder configuration the headline metric is quoted on): a
+circle of radius 0.5 with 1000 equal panels, U = (1, 0), Re = 2000
+(nu = 5e-4), dt = 0.002, core radius = panel length, birth half a panel off
+the wall, same-sign collapse within 0.3 eps, |G| < 1e-8 dropped, started from
+a seeded warm wake of N0 = 1e6 vortices (Gaussian in a 4 x 2 box behind the
+body, G ~ N(0, 1e-3)).  One step = birth, Biot-Savart + 3-nearest, vortex and
+wall diffusion, convection with absorption, force sums, compaction, collapse.
+
+Our arm times the FP32-bulk form (headline) and the plain FP64 form on the
+same GPU; value = whole-job steps/s.  Multi-GPU is weak scaling: each rank
+advances its own body, no collective in the step; the slowest rank's device
+time is the job time.  The reference arm (--impl reference) times the CPU
+oracle (OpenMP C transcription of the reference formulas) on the host cores
+on a bounded sample of the same step and extrapolates to a full step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "steps/sec & particle-interactions/sec FP32-bulk vs FP64 plain, same GPU; p50/p99 latency"
+P_PANELS = 1000
+FLOP_PER_PAIR_BS = 12          # Biot-Savart pair (sub x2, |r|^2 3, max 1, rcp+mul 2, 2 fma 4)
+FLOP_PER_PAIR_DIFF = 18
+
+
+def workload_conf(N, precision):
+    from vortex_b200 import native as Nt
+    eps = 2 * math.pi * 0.5 / P_PANELS
+    return Nt.default_conf(steps=1000, saving_step=100, dt=0.002, viscosity=5e-4, rho=1.0, v_inf_x=1.0,
+                           v_inf_y=0.0, x_min=-2.0, x_max=10.0, y_min=-10.0, y_max=10.0, ve_size=eps,
+                           n_of_points=20, n_col=2, r_col_diff_sign=0.0, r_col_same_sign=0.3,
+                           max_ve_g=1e30, v_inf_incr_steps=0, drop_eps=1e-8, birth_offset_mode=2,
+                           precision=precision, inc_step=8192)
+
+
+def warm_cloud(n, seed):
+    rng = np.random.default_rng(seed)
+    x = np.empty(0)
+    y = np.empty(0)
+    while len(x) < n:
+        m = 2 * (n - len(x)) + 1000
+        xx = rng.normal(2.5, 1.0, m)
+        yy = rng.normal(0.0, 0.5, m)
+        ok = (xx > 0.5) & (xx < 4.5) & (np.abs(yy) < 1.0) & (xx * xx + yy * yy > 0.51 ** 2)
+        x = np.concatenate([x, xx[ok]])
+        y = np.concatenate([y, yy[ok]])
+    g = rng.normal(0.0, 1e-3, n)
+    return x[:n].copy(), y[:n].copy(), g
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [t.strip() for t in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def pinned(n, rt):
+    p = C.c_void_p()
+    if rt.cudaHostAlloc(C.byref(p), C.c_size_t(max(8 * n, 8)), 0) != 0:
+        raise RuntimeError("cudaHostAlloc failed")
+    return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(n,)), p
+
+
+def run_ours(args, rank, world, device):
+    import torch
+    from vortex_b200 import native as Nt
+    from vortex_b200 import profiles
+
+    torch.cuda.set_device(device)
+    dist = world > 1
+    pan = profiles.circle(P_PANELS)
+    x0, y0, g0 = warm_cloud(args.n, seed=1234 + rank)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+
+    def barrier():
+        if dist:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed_steps(sim, K, W, rec_pairs):
+        """W untimed steps, then K steps each bracketed by events on the
+        handle's stream with an L2 flush between steps."""
+        stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{device}")
+        sim.step(W)
+        sim.sync()
+        sim.set_timing(True)
+        launches0 = sim.launches()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        pairs = []
+        barrier()
+        for k in range(K):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            n_before = sim.state()["n"] + P_PANELS if rec_pairs else 0
+            ev[k][0].record(stream)
+            sim.step(1)
+            ev[k][1].record(stream)
+            if rec_pairs:
+                pairs.append(n_before)
+        barrier()
+        ms = [a.elapsed_time(b) for a, b in ev]
+        t = sim.timing()
+        launches = sim.launches() - launches0
+        sim.set_timing(False)
+        return ms, t, launches, pairs
+
+    # ---- FP32 bulk (headline) ------------------------------------------
+    sim = Nt.Sim(workload_conf(args.n, Nt.PREC_FP32), pan, device=device)
+    sim.set_particles(x0, y0, g0)
+    clocks = ClockSampler(device)
+    clocks.start()
+    ms, tst, launches, nvec = timed_steps(sim, args.steps, args.warmup, True)
+    ck = clocks.stop()
+    total_ms = float(sum(ms))
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    n_end = sim.count()
+    # dominant kernel: Biot-Savart pair kernel, algorithmic FLOPs = 12 per (target, source) pair
+    pairs = [n * ((n + 31) // 32 * 32) for n in nvec]
+    bs_ms = tst[5] / args.steps
+    bs_flop = FLOP_PER_PAIR_BS * float(np.mean(pairs))
+    # ---- end to end through the C ABI with host buffers -------------------
+    rt = C.CDLL("libcudart.so.12")
+    n_now = sim.count()
+    hx, _px = pinned(n_now + 4096, rt)
+    hy, _py = pinned(n_now + 4096, rt)
+    hg, _pg = pinned(n_now + 4096, rt)
+    xs, ys, gs = sim.particles()
+    e2e_steps = max(2, min(3, args.steps))
+    e2e_t = []
+    bi = bo = 0
+    for k in range(e2e_steps):
+        m = len(xs)
+        hx[:m], hy[:m], hg[:m] = xs, ys, gs
+        t0 = time.perf_counter()
+        sim.set_particles(hx[:m], hy[:m], hg[:m])
+        sim.step(1)
+        f = sim.forces()
+        xs, ys, gs = sim.particles()
+        e2e_t.append(time.perf_counter() - t0)
+        bi += 24 * m
+        bo += 24 * len(xs) + f.nbytes
+    sim.close()
+    # ---- plain FP64 on the same workload ------------------------------------
+    fp64 = None
+    if not args.skip_fp64:
+        sim64 = Nt.Sim(workload_conf(args.n, Nt.PREC_FP64), pan, device=device)
+        sim64.set_particles(x0, y0, g0)
+        ms64, t64, _, _ = timed_steps(sim64, args.fp64_steps, 1, False)
+        sim64.close()
+        fp64 = {"steps_per_s": 1e3 * len(ms64) / sum(ms64), "ms_per_step": float(np.mean(ms64)),
+                "bs_pair_kernel_ms": t64[5] / len(ms64), "diffusion_pair_kernel_ms": t64[6] / len(ms64)}
+    peak32 = Nt.measure_peak(device, fp64=False)
+    if rank != 0:
+        return None
+    value = world * 1e3 * args.steps / total_ms
+    inter = float(np.mean(nvec)) ** 2
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        bs = tj.get("bs_pair_fp32")
+        if bs and bs.get("bytes_per_target") is not None:
+            traffic = bs["bytes_per_target"] * float(np.mean(nvec))
+    achieved = bs_flop / (bs_ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic (seeded warm wake cloud; generated circle profile)",
+        "config": {"workload": "cylinder R=0.5, 1000 panels, Re=2000 (nu=5e-4), dt=0.002, "
+                               f"warm wake N0={args.n} per GPU, FP32-bulk form",
+                   "panels": P_PANELS, "n_particles_start": args.n, "n_particles_end": int(n_end),
+                   "precision": "fp32 pair sums, fp64 panel solve/forces/positions",
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"{world} independent bodies (one per GPU)"},
+        "particle_interactions_per_s": world * inter * 1e3 * args.steps / total_ms,
+        "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+        "stage_ms": {"birth": tst[0] / args.steps, "velocity": tst[1] / args.steps,
+                     "diffusion": tst[2] / args.steps, "wall": tst[3] / args.steps,
+                     "advect_compact_collapse": tst[4] / args.steps},
+        "fp64_plain": fp64,
+        "speedup_fp32_over_fp64": (value / world) / fp64["steps_per_s"] if fp64 else None,
+        "roofline": {"kernel": "k_bs_partial<float> (Biot-Savart + 3-nearest pair kernel)",
+                     "bound": "fp32-simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                     "frac": achieved / peak32, "traffic": traffic,
+                     "peak_source": "measured FP32 FMA throughput of this GPU (vx_measure_peak)",
+                     "flop_per_pair": FLOP_PER_PAIR_BS, "launch_ms": bs_ms},
+        "e2e": {"value": e2e_steps / sum(e2e_t), "unit": "steps/s",
+                "h2d_bytes_per_step": bi // e2e_steps, "d2h_bytes_per_step": bo // e2e_steps},
+        "gpu_launches": int(launches),
+        "clocks": ck,
+    }
+    line["cpu_baseline"] = cpu_baseline(args, x0, y0, g0, pan)
+    return line
+
+
+def cpu_sample(x, y, g, pan, n_targets, n_panels):
+    """Time the oracle's plain FP64 step pieces on a sample and extrapolate
+    to a full step of len(x) particles (pair sums dominate on the CPU)."""
+    from oracle import oracle as O
+    n = len(x)
+    p = O.make_params(dt=0.002, nu=5e-4, eps=2 * math.pi * 0.5 / P_PANELS, r_col_same_sign=0.3,
+                      prof_x_min=-0.5, prof_x_max=0.5, prof_y_min=-0.5, prof_y_max=0.5, drop_eps=1e-8,
+                      birth_mode=O.BIRTH_HALF_PANEL)
+    cap = (n + 31) // 32 * 32
+    xs, ys, gs = np.zeros(cap), np.zeros(cap), np.zeros(cap)
+    xs[:n], ys[:n], gs[:n] = x, y, g
+    O.fill_tail(xs, ys, gs, n, cap)
+    T = n_targets
+    i0 = n // 2 - T // 2
+    vx, vy, d = np.zeros(T), np.zeros(T), np.zeros(T)
+    lib = O.lib()
+    ptr = [O._p(a) for a in (xs, ys, gs)]
+    t0 = time.perf_counter()
+    lib.vxo_velocity_targets(C.byref(p), *ptr, C.c_int64(n), C.c_int64(i0), C.c_int64(i0 + T),
+                             O._p(vx), O._p(vy), O._p(d))
+    t1 = time.perf_counter()
+    lib.vxo_diffusion_targets(C.byref(p), *ptr, C.c_int64(n), C.c_int64(i0), C.c_int64(i0 + T),
+                              O._p(d), O._p(vx), O._p(vy))
+    t2 = time.perf_counter()
+    sub = pan[:n_panels].copy()
+    sub["nr"] = np.minimum(sub["nr"], n_panels - 1)
+    O.birth_rhs(p, sub, xs[:n], ys[:n], gs[:n])
+    t3 = time.perf_counter()
+    step_s = (t2 - t0) * n / T + (t3 - t2) * P_PANELS / n_panels
+    return step_s, t3 - t0
+
+
+def cpu_baseline(args, x, y, g, pan):
+    from oracle import oracle as O
+    step_s, spent = cpu_sample(x, y, g, pan, args.cpu_targets, 32)
+    return {"value": 1.0 / step_s, "unit": "steps/s", "cores": O.lib().vxo_num_threads(), "kind": "port",
+            "sample": f"oracle FP64 (OpenMP): Biot-Savart+3-nearest and vortex diffusion for "
+                      f"{args.cpu_targets} of {len(x)} targets over all sources, birth RHS for 32 of "
+                      f"{P_PANELS} panels over all sources; extrapolated to one full step "
+                      f"({spent:.1f} s measured)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    from vortex_b200 import profiles
+    pan = profiles.circle(P_PANELS)
+    x, y, g = warm_cloud(args.n, seed=1234)
+    for _ in range(args.warmup):
+        cpu_sample(x, y, g, pan, args.ref_targets, 16)
+    est = []
+    for _ in range(args.steps):
+        s, _ = cpu_sample(x, y, g, pan, args.ref_targets, 16)
+        est.append(s)
+    step_s = float(np.mean(est))
+    v = 1.0 / step_s
+    return {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded warm wake cloud)",
+            "config": {"workload": "cylinder R=0.5, 1000 panels, Re=2000 (nu=5e-4), dt=0.002, "
+                                   f"warm wake N0={args.n}", "panels": P_PANELS, "n_particles_start": args.n},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": O.lib().vxo_num_threads(), "kind": "port",
+                             "sample": f"each step: oracle FP64 Biot-Savart+3-nearest for {args.ref_targets} "
+                                       f"targets over all {args.n} sources, diffusion on the same subset, "
+                                       "birth RHS for 16 panels; extrapolated to a full step"},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--cpu-targets", type=int, default=2048)
+    ap.add_argument("--ref-targets", type=int, default=1024)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        line = run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -84,6 +84,9 @@ typedef struct vx_conf {
     int32_t n_probes_grid;      /* >0: probes on an n x n grid (box below) */
     int32_t pad1_;
     double probe_box[4];        /* x0, x1, y0, y1 of the probe grid */
+    int32_t fmm;                /* bulk form: Biot-Savart by the quadtree
+                                   multipole method (default 1); 0 = direct */
+    int32_t pad2_;
 } vx_conf;
 
 typedef struct vx_sim vx_sim;
@@ -150,14 +153,40 @@ vx_status vx_probe(vx_sim *sim, const double *px, const double *py, int64_t np,
  * (on by default; 0 turns it off). */
 vx_status vx_set_graph(vx_sim *sim, int enable);
 
-/* Device time (ms) accumulated per stage group since the last reset:
- * out[0] birth, [1] velocity+diffusion ("Speed"), [2] advect..collapse
- * ("Step").  Timing adds events; off unless enabled. */
+/* Device time (ms) accumulated per stage since timing was (re)enabled:
+ * out[0] birth, [1] convective velocity, [2] vortex diffusion, [3] wall
+ * diffusion, [4] convection + compaction + collapse, [5] the Biot-Savart
+ * pair kernel alone, [6] the diffusion pair kernel alone, [7] whole steps.
+ * Timed steps run eagerly (no graph) so the events can be recorded. */
 vx_status vx_set_timing(vx_sim *sim, int enable);
-vx_status vx_get_timing(vx_sim *sim, double out3[3]);
+vx_status vx_get_timing(vx_sim *sim, double out8[8]);
 
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);
+
+/* Block until the handle's device work is done; reports device error flags. */
+vx_status vx_sync(vx_sim *sim);
+/* The CUDA stream (cudaStream_t) the handle launches on. */
+void *vx_get_stream(vx_sim *sim);
+
+/* Slot-level access for drivers that manage the padded store themselves:
+ * raw slots [0, count), dead tail included; vx_set_slots also sets the live
+ * count n (the last P live slots count as this step's newborns). */
+vx_status vx_get_slots(vx_sim *sim, double *x, double *y, double *g, int64_t count);
+vx_status vx_set_slots(vx_sim *sim, const double *x, const double *y, const double *g,
+                       int64_t count, int64_t n);
+/* Overwrite velocity / 3-nearest distance of the first n particles (any
+ * pointer may be NULL). */
+vx_status vx_set_velocity(vx_sim *sim, const double *vx, const double *vy, const double *d,
+                          int64_t n);
+/* Scalars: n, n before this step's birth, step index, V_inf x/y, d_g, Fx, Fy, M. */
+vx_status vx_get_state(vx_sim *sim, double out9[9]);
+/* Absolute step index (a restart from KadrNNNNNN.txt sets it). */
+vx_status vx_set_step_index(vx_sim *sim, int64_t step);
+
+/* Measured FMA throughput of the vector pipe of `device` (TFLOP/s, FP64 when
+ * fp64 != 0): the roofline denominator of the pair kernels. */
+vx_status vx_measure_peak(int device, int fp64, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -119,6 +119,21 @@ int init_device_conf_values(void);
 int velocity_control(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *Contr_points,
                      vxu_velocity *V, size_t n_contr);
 
+/* include/unit_1.cuh:51 — inertial tracers: carrier velocity into v_env,
+ * relaxation of v_second towards it with time constant conf.rel_t, then
+ * convection with wall absorption.  Writes output/vels/Vel<step>_4.txt and
+ * _5.txt as the reference does. */
+int second_speed(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *second_pos,
+                 vxu_velocity *v_second, vxu_velocity *v_env, size_t *n_second, vx_panel *panels);
+
+/* include/unit_1.cuh:52 — passive tracers moved with the carrier velocity. */
+int first_speed(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *second_pos,
+                vxu_velocity *v_second, size_t *n_second, vx_panel *panels);
+
+/* Kernels launched by the entry points above since the library was loaded
+ * (no counterpart in the reference; used to show which code ran). */
+int64_t vxu_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -676,3 +676,56 @@ int64_t vxo_step(const vxo_params *p, const vxo_panel *pan, int64_t P,
     st->n = n;
     return n;
 }
+
+/* Target range [i0, i1) of vxo_velocity / vxo_diffusion over all n sources
+ * (the CPU baseline times a sample of targets and extrapolates). */
+void vxo_velocity_targets(const vxo_params *p, const double *x, const double *y, const double *g,
+                          int64_t n, int64_t i0, int64_t i1, double *vx, double *vy, double *d) {
+    const double eps2 = p->eps * p->eps;
+    const int64_t s = round32(n);
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = i0; i < i1; ++i) {
+        const double a0 = x[i], a1 = y[i];
+        double d1 = 1e5, d2 = 1e5, d3 = 1e5, y0 = 0.0, y1 = 0.0;
+        for (int64_t j = 0; j < s; ++j) {
+            if (j == i) continue;
+            double dx = a0 - x[j], dy = a1 - y[j];
+            double r2 = fma(dx, dx, dy * dy);
+            NN3_INSERT(d1, d2, d3, r2, fmin, fmax);
+            if (j < n) {
+                double m = g[j] / fmax(r2, eps2);
+                y1 = fma(m, dx, y1);
+                y0 = fma(-m, dy, y0);
+            }
+        }
+        d[i - i0] = (sqrt(d1) + sqrt(d2) + sqrt(d3)) / 3;
+        vx[i - i0] = y0 / TWO_PI + p->vinf_x;
+        vy[i - i0] = y1 / TWO_PI + p->vinf_y;
+    }
+}
+
+void vxo_diffusion_targets(const vxo_params *p, const double *x, const double *y, const double *g,
+                           int64_t n, int64_t i0, int64_t i1, const double *d, double *vx, double *vy) {
+    const double thr = 0.001 * p->eps;
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = i0; i < i1; ++i) {
+        const double a0 = x[i], a1 = y[i], dd = d[i - i0];
+        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            double dx = a0 - x[j], dy = a1 - y[j];
+            double dist = sqrt(fma(dx, dx, dy * dy));
+            if (dist > thr) {
+                double m = g[j] / dist;
+                double e = exp(-dist / dd);
+                double me = m * e;
+                I2x = fma(-me, dx, I2x);
+                I2y = fma(-me, dy, I2y);
+                I1 = fma(g[j], e, I1);
+            }
+        }
+        if (fabs(I1) > 1e-5) {
+            vx[i - i0] += -p->nu * I2x / (I1 * dd);
+            vy[i - i0] += -p->nu * I2y / (I1 * dd);
+        }
+    }
+}

@@ -87,6 +87,12 @@ void vxo_birth_place(const vxo_params *p, const vxo_panel *pan, int64_t P,
 void vxo_velocity(const vxo_params *p, const double *x, const double *y, const double *g,
                   int64_t n, int64_t s, double *vx, double *vy, double *d);
 
+/* Targets [i0, i1) only, over all n sources (outputs indexed from i0). */
+void vxo_velocity_targets(const vxo_params *p, const double *x, const double *y, const double *g,
+                          int64_t n, int64_t i0, int64_t i1, double *vx, double *vy, double *d);
+void vxo_diffusion_targets(const vxo_params *p, const double *x, const double *y, const double *g,
+                           int64_t n, int64_t i0, int64_t i1, const double *d, double *vx, double *vy);
+
 /* ---- diffusive velocities (src/kernel.cu:985-1088, 1300-1346) ---- */
 void vxo_diffusion(const vxo_params *p, const double *x, const double *y, const double *g,
                    int64_t n, const double *d, double *vx, double *vy);

@@ -77,8 +77,9 @@ struct vx_sim {
     long long g_launches = 0;
     // timing
     bool timing = false;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    double t_acc[3] = {0, 0, 0};
+    cudaEvent_t ev[6] = {};     // stage boundaries
+    cudaEvent_t pev[4] = {};    // around the two pair kernels
+    double t_acc[8] = {};
     // probe scratch
     double *d_probe = nullptr;
     long long probe_cap = 0;
@@ -149,6 +150,7 @@ extern "C" vx_status vx_conf_default(vx_conf *c) {
     c->birth_offset_mode = VX_BIRTH_REF;
     c->drop_eps = 1e-12;
     c->diff_cutoff = 30.0;
+    c->fmm = 1;
     return VX_OK;
 }
 
@@ -202,6 +204,22 @@ vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, i
     A(w.rhs_part, w.rhs_part_cap);
     A(w.R, P32); A(w.gamma, P32);
     A(w.red, VX_RED_BLOCKS * 4);
+    // neighbour-list grid of the bulk form
+    A(w.key0, cap); A(w.key1, cap); A(w.val0, cap); A(w.val1, cap);
+    w.rs_tiles_cap = vx_rs_tiles_cap(cap);
+    A(w.rs_hist, 256 * w.rs_tiles_cap); A(w.rs_off, 256 * w.rs_tiles_cap);
+    A(w.cg_cnt, w.cells_cap); A(w.cg_start, w.cells_cap + 1);
+    A(w.srt, cap);
+    w.items_cap = cap / 256 + w.cells_cap + 2;
+    A(w.items, w.items_cap);
+    A(w.row_items, w.cells_cap + 1); A(w.row_item_off, w.cells_cap + 1);
+    // quadtree of the bulk-form Biot-Savart
+    w.fmm_lmax = vx_fmm_max_level(cap);
+    A(w.fmm_cnt, vx_fmm_cells(w.fmm_lmax));
+    A(w.fmm_start, (1LL << (2 * w.fmm_lmax)) + 1);
+    A(w.fmm_flags, cap);
+    A(w.fmm_M, 2LL * VX_FMM_P * vx_fmm_cells(w.fmm_lmax));
+    A(w.fmm_L, 2LL * VX_FMM_P * vx_fmm_cells(w.fmm_lmax));
 #undef A
     return VX_OK;
 }
@@ -359,6 +377,7 @@ extern "C" vx_status vx_destroy(vx_sim *s) {
     if (s->h_S) cudaFreeHost(s->h_S);
     if (s->d_probe) cudaFree(s->d_probe);
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
+    for (auto &e : s->pev) if (e) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return VX_OK;
@@ -533,20 +552,31 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
     const VxParams &p = s->prm;
     cudaError_t e = cudaSuccess;
     const int kv = kv_for(s);
-    auto ev = [&](int k) { if (s->timing && !whole_step) cudaEventRecord(s->ev[k], s->stream); };
+    const bool rec = s->timing && !whole_step;
+    if (rec)
+        for (int k = 0; k < 4; ++k) L.pair_ev[k] = s->pev[k];
+    auto ev = [&](int k) { if (rec) cudaEventRecord(s->ev[k], s->stream); };
     ev(0);
     if (mask & VX_STAGE_BIRTH) {
         if ((e = vx_launch_step_begin(L, s->d_S)) != cudaSuccess) return e;
         if ((e = vx_launch_birth(L, p, v, s->d_S, s->w, s->d_pan, s->d_minv, rhs_chunks_for(s))) != cudaSuccess) return e;
     }
     ev(1);
-    if (mask & VX_STAGE_VELOCITY)
-        if ((e = vx_launch_velocity(L, p, v, s->d_S, s->w, kv)) != cudaSuccess) return e;
+    if (mask & VX_STAGE_VELOCITY) {
+        // bulk form: quadtree FMM (vx_fmm.cu); plain form: direct sum
+        if (p.prec == VX_PREC_FP32 && s->conf.fmm)
+            e = vx_launch_velocity_fmm(L, p, v, s->d_S, s->w);
+        else
+            e = vx_launch_velocity(L, p, v, s->d_S, s->w, kv);
+        if (e != cudaSuccess) return e;
+    }
+    ev(2);
     if (mask & VX_STAGE_DIFFUSION)
         if ((e = vx_launch_diffusion(L, p, v, s->d_S, s->w, kv)) != cudaSuccess) return e;
+    ev(3);
     if (mask & VX_STAGE_WALL)
         if ((e = vx_launch_wall(L, p, v, s->d_S, s->d_pan)) != cudaSuccess) return e;
-    ev(2);
+    ev(4);
     if (mask & VX_STAGE_ADVECT)
         if ((e = vx_launch_advect(L, p, v, s->d_S, s->w, s->d_pan)) != cudaSuccess) return e;
     if (mask & VX_STAGE_COMPACT)
@@ -556,7 +586,7 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
     if (mask & VX_STAGE_COLLAPSE2)
         if ((e = vx_launch_collapse(L, p, v, s->d_S, s->w, 2, (int)s->conf.n_col)) != cudaSuccess) return e;
     if (whole_step) e = vx_launch_step_end(L, s->d_S);
-    ev(3);
+    ev(5);
     return e;
 }
 
@@ -617,12 +647,18 @@ extern "C" vx_status vx_step(vx_sim *s, int64_t nsteps) {
         vx_status st = step_once(s);
         if (st != VX_OK) return st;
         if (s->timing) {
-            CU(cudaEventSynchronize(s->ev[3]));
-            float a, b, c;
-            cudaEventElapsedTime(&a, s->ev[0], s->ev[1]);
-            cudaEventElapsedTime(&b, s->ev[1], s->ev[2]);
-            cudaEventElapsedTime(&c, s->ev[2], s->ev[3]);
-            s->t_acc[0] += a; s->t_acc[1] += b; s->t_acc[2] += c;
+            CU(cudaEventSynchronize(s->ev[5]));
+            float t;
+            for (int q = 0; q < 5; ++q) {
+                cudaEventElapsedTime(&t, s->ev[q], s->ev[q + 1]);
+                s->t_acc[q] += t;
+            }
+            cudaEventElapsedTime(&t, s->pev[0], s->pev[1]);
+            s->t_acc[5] += t;
+            cudaEventElapsedTime(&t, s->pev[2], s->pev[3]);
+            s->t_acc[6] += t;
+            cudaEventElapsedTime(&t, s->ev[0], s->ev[5]);
+            s->t_acc[7] += t;
         }
     }
     CU(cudaGetLastError());
@@ -645,15 +681,17 @@ extern "C" vx_status vx_set_graph(vx_sim *s, int enable) {
 extern "C" vx_status vx_set_timing(vx_sim *s, int enable) {
     if (!s) return VX_ERR_ARG;
     s->timing = enable != 0;
-    if (s->timing && !s->ev[0])
+    if (s->timing && !s->ev[0]) {
         for (auto &e : s->ev) CU(cudaEventCreate(&e));
-    s->t_acc[0] = s->t_acc[1] = s->t_acc[2] = 0.0;
+        for (auto &e : s->pev) CU(cudaEventCreate(&e));
+    }
+    for (double &t : s->t_acc) t = 0.0;
     return VX_OK;
 }
 
-extern "C" vx_status vx_get_timing(vx_sim *s, double out3[3]) {
-    if (!s || !out3) return VX_ERR_ARG;
-    for (int k = 0; k < 3; ++k) out3[k] = s->t_acc[k];
+extern "C" vx_status vx_get_timing(vx_sim *s, double out8[8]) {
+    if (!s || !out8) return VX_ERR_ARG;
+    for (int k = 0; k < 8; ++k) out8[k] = s->t_acc[k];
     return VX_OK;
 }
 

@@ -71,6 +71,15 @@ struct VxScalars {
     long long gnx, gny, gncells;
     int err;
     int pad_;
+    // neighbour-list grid of the bulk form (vortex diffusion)
+    unsigned long long cb[4];
+    double cx0, cy0, ch;
+    long long cnx, cny, cncells, cnitems;
+    // quadtree of the bulk-form Biot-Savart (vx_fmm.cu)
+    unsigned long long fb[4];
+    double fx0, fy0, fside;
+    long long fnleaves, fs;
+    int fL, fnflag;
 };
 
 enum {
@@ -103,6 +112,22 @@ struct VxWork {
     double *R, *gamma;
     // reductions
     double *red;             // [blocks][4]
+    // neighbour-list grid (bulk form): radix-sort buffers, cells, sorted sources
+    unsigned *key0, *key1;
+    int *val0, *val1;
+    int *rs_hist;
+    long long *rs_off;
+    long long rs_tiles_cap;
+    int *cg_cnt, *cg_start;
+    float4 *srt;
+    int2 *items;             // (row, first sorted slot) of each target segment
+    long long items_cap;
+    int *row_items;
+    long long *row_item_off;
+    // quadtree: counts and expansions of every level up to fmm_lmax
+    int fmm_lmax;
+    int *fmm_cnt, *fmm_start, *fmm_flags;
+    double *fmm_M, *fmm_L;   // complex FP64 pairs, FMM_P per cell
 };
 
 // Compaction chunk size (elements per scan chunk).
@@ -142,7 +167,11 @@ struct VxLaunch {
     cudaStream_t stream;
     long long *launches;   // host counter (may be null)
     int num_sms;
+    // optional events recorded around the Biot-Savart and diffusion pair
+    // kernels: [0,1] Biot-Savart, [2,3] diffusion (null: not recorded)
+    cudaEvent_t pair_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
+#define VX_EV(L, k) do { if ((L).pair_ev[k]) cudaEventRecord((L).pair_ev[k], (L).stream); } while (0)
 #define VX_COUNT(L) do { if ((L).launches) ++*(L).launches; } while (0)
 
 // Stage launchers (each returns the first CUDA error it saw).
@@ -179,6 +208,14 @@ void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams 
 void vx_set_error(const char *fmt, ...);
 #include <vector>
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms);
+long long vx_rs_tiles_cap(long long cap);
+int vx_fmm_max_level(long long cap);
+long long vx_fmm_cells(int lmax);         // cells of all levels 0..lmax
+constexpr int VX_FMM_P = 16;              // expansion terms (vx_fmm.cu)
+cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                                   VxWork &w);
+cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                                      VxWork &w);
 void vx_work_free(VxWork &w, std::vector<void *> &allocs);
 
 // Split factor so that (target tiles x source chunks) fills the GPU.

@@ -149,6 +149,114 @@ __global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const V
     }
 }
 
+// ---------------------------------------------------------------------------
+// Bulk-form Biot-Savart + 3 nearest, FP32.  Same decomposition as above, with
+// the inner loop cut to the arithmetic: sources come from shared memory as
+// one float4 broadcast each, the loop runs unrolled over full tiles, the
+// reciprocal is the hardware approximation (rcp.approx, 1 ulp), and the
+// self pair is excluded only in the one tile per target that can contain it
+// (a uniform branch per tile), so the hot loop has no index compare.
+__device__ __forceinline__ float vx_rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+constexpr int BS32_TPT = 4;
+
+template <bool NN3, bool CHECK_SELF>
+__device__ __forceinline__ void bs32_tile(const float4 *sm, int cnt, int jbase, const int *ti,
+                                          const float *ax, const float *ay, float eps2, float *sx,
+                                          float *sy, float *d1, float *d2, float *d3) {
+#pragma unroll 4
+    for (int q = 0; q < cnt; ++q) {
+        const float4 s = sm[q];
+#pragma unroll
+        for (int k = 0; k < BS32_TPT; ++k) {
+            const float dx = ax[k] - s.x, dy = ay[k] - s.y;
+            const float r2 = fmaf(dx, dx, dy * dy);
+            if (NN3) {
+                if (r2 < d3[k] && (!CHECK_SELF || jbase + q != ti[k])) {
+                    d3[k] = r2;
+                    float t = fminf(d3[k], d2[k]); d3[k] = fmaxf(d3[k], d2[k]); d2[k] = t;
+                    t = fminf(d1[k], d2[k]); d2[k] = fmaxf(d1[k], d2[k]); d1[k] = t;
+                }
+            }
+            const float m = s.z * vx_rcp_approx(fmaxf(r2, eps2));
+            sy[k] = fmaf(m, dx, sy[k]);
+            sx[k] = fmaf(-m, dy, sx[k]);
+        }
+    }
+}
+
+template <bool NN3>
+__global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars *S, const float4 *src32,
+                                                     const double *tx, const double *ty, long long tstr,
+                                                     long long nt_in, double *part, long long tstride,
+                                                     int K) {
+    constexpr int NOUT = NN3 ? 5 : 2;
+    __shared__ float4 sm[PT];
+    const long long n = S->n;
+    const long long nt = nt_in < 0 ? n : nt_in;
+    const long long srange = NN3 ? vx_round32(n) : n;
+    const long long tile = (long long)PT * BS32_TPT;
+    const long long tiles = vx_ceil_div(nt, tile);
+    const long long cs = vx_ceil_div(vx_ceil_div(srange, K), PT) * PT;
+    const long long items = tiles * K;
+    const float eps2 = (float)p.eps2;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const long long tt = it % tiles, sc = it / tiles;
+        const long long tlo = tt * tile, thi = min(nt, tlo + tile);
+        float ax[BS32_TPT], ay[BS32_TPT], d1[BS32_TPT], d2[BS32_TPT], d3[BS32_TPT];
+        int ti[BS32_TPT];
+        double vxa[BS32_TPT], vya[BS32_TPT];
+#pragma unroll
+        for (int k = 0; k < BS32_TPT; ++k) {
+            const long long t = tlo + (long long)k * PT + threadIdx.x;
+            ti[k] = (int)t;
+            const long long i = t < nt ? t : 0;
+            ax[k] = (float)tx[i * tstr];
+            ay[k] = (float)ty[i * tstr];
+            vxa[k] = 0.0; vya[k] = 0.0;
+            d1[k] = d2[k] = d3[k] = 1e5f;
+        }
+        const long long j0 = sc * cs, j1 = min(srange, j0 + cs);
+        for (long long jt = j0; jt < j1; jt += PT) {
+            __syncthreads();
+            if (jt + threadIdx.x < j1) {
+                float4 q = src32[jt + threadIdx.x];
+                if (!NN3 && jt + threadIdx.x >= n) q.z = 0.0f;
+                sm[threadIdx.x] = q;
+            }
+            __syncthreads();
+            const int cnt = (int)min((long long)PT, j1 - jt);
+            float sx[BS32_TPT], sy[BS32_TPT];
+#pragma unroll
+            for (int k = 0; k < BS32_TPT; ++k) { sx[k] = 0.0f; sy[k] = 0.0f; }
+            const bool self = NN3 && jt < thi && jt + cnt > tlo;   // uniform per block
+            if (self)
+                bs32_tile<NN3, true>(sm, cnt, (int)jt, ti, ax, ay, eps2, sx, sy, d1, d2, d3);
+            else
+                bs32_tile<NN3, false>(sm, cnt, (int)jt, ti, ax, ay, eps2, sx, sy, d1, d2, d3);
+#pragma unroll
+            for (int k = 0; k < BS32_TPT; ++k) { vxa[k] += (double)sx[k]; vya[k] += (double)sy[k]; }
+        }
+#pragma unroll
+        for (int k = 0; k < BS32_TPT; ++k) {
+            if (ti[k] < nt) {
+                double *o = part + (long long)sc * NOUT * tstride + ti[k];
+                o[0] = vxa[k];
+                o[tstride] = vya[k];
+                if (NN3) {
+                    o[2 * tstride] = (double)d1[k];
+                    o[3 * tstride] = (double)d2[k];
+                    o[4 * tstride] = (double)d3[k];
+                }
+            }
+        }
+    }
+}
+
 // Combine: V = sum/(2 pi) + V_inf, d = mean of the 3 nearest distances.
 template <bool FP32>
 __global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, long long tstride,
@@ -317,13 +425,17 @@ cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxVie
     const long long tstride = w.part_cap / (5LL * K);
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32) {
-        k_bs_partial<float, true><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, w.src32, v.x, v.y, v.ps,
-                                                                     -1, w.part, tstride, K);
+        VX_EV(L, 0);
+        k_bs32_partial<true><<<pair_grid(L), PT, 0, L.stream>>>(p, S, w.src32, v.x, v.y, v.ps, -1, w.part,
+                                                                tstride, K);
+        VX_EV(L, 1);
         VX_COUNT(L);
         k_bs_combine<true><<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.part, tstride, K);
     } else {
+        VX_EV(L, 0);
         k_bs_partial<double, true><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, v.x, v.y, v.ps,
                                                                       -1, w.part, tstride, K);
+        VX_EV(L, 1);
         VX_COUNT(L);
         k_bs_combine<false><<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.part, tstride, K);
     }
@@ -333,12 +445,16 @@ cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxVie
 
 cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                 VxWork &w, int K) {
+    // bulk form: neighbour lists within diff_cutoff * d_i (vx_cells.cu)
+    if (p.prec == VX_PREC_FP32 && p.diff_cutoff > 0.0) return vx_launch_diffusion_cells(L, p, v, S, w);
     const long long tstride = w.part_cap / (3LL * K);
+    VX_EV(L, 2);
     if (p.prec == VX_PREC_FP32) {
         k_diff_partial<float><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, w.src32, w.part, tstride, K);
     } else {
         k_diff_partial<double><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, w.part, tstride, K);
     }
+    VX_EV(L, 3);
     VX_COUNT(L);
     k_diff_combine<<<L.num_sms * 4, 256, 0, L.stream>>>(p, v, S, w.part, tstride, K);
     VX_COUNT(L);
@@ -352,8 +468,8 @@ cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &
     if (tstride < np) return cudaErrorInvalidValue;
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32)
-        k_bs_partial<float, false><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, w.src32, px, py, pstride,
-                                                                      np, w.part, tstride, K);
+        k_bs32_partial<false><<<pair_grid(L), PT, 0, L.stream>>>(p, S, w.src32, px, py, pstride, np, w.part,
+                                                                 tstride, K);
     else
         k_bs_partial<double, false><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, px, py, pstride,
                                                                        np, w.part, tstride, K);

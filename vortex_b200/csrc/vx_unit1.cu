@@ -29,6 +29,8 @@ static_assert(sizeof(vxu_vortex) == 24 && sizeof(vxu_velocity) == 16 && sizeof(v
 // executable that loads this library takes precedence over this one.
 extern "C" {
 struct vxu_conf_t conf;
+int current_step = 0;   // src/main.c:18-19, read by the tracer entry points
+int first_step = 0;
 }
 
 namespace {
@@ -388,6 +390,73 @@ int velocity_control(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *
                        (long long)n_contr, ov, ov + 1, 2, K));
     CK(cudaDeviceSynchronize());
     return 0;
+}
+
+// Relaxation of inertial tracers towards the carrier velocity
+// (second_speed_Kernel, src/kernel.cu:1478-1489); the previous velocity is
+// rounded to float there, and so it is here.
+__global__ void k_u_relax(const double *pos, const double *venv, double *v, long long nt, double rel_t,
+                          double dt) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nt;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (!pos[3 * i + 2]) { v[2 * i] = 0.0; v[2 * i + 1] = 0.0; continue; }
+        const float px = (float)v[2 * i], py = (float)v[2 * i + 1];
+        v[2 * i] = (venv[2 * i] - px) / rel_t * dt + px;
+        v[2 * i + 1] = (venv[2 * i + 1] - py) / rel_t * dt + py;
+    }
+}
+
+static void save_vel(const vxu_vortex *d_pos, const vxu_velocity *d_vel, size_t nt, int step, int stage) {
+    std::vector<vxu_vortex> P(nt);
+    std::vector<vxu_velocity> V(nt);
+    if (cudaMemcpy(P.data(), d_pos, nt * sizeof(vxu_vortex), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    if (cudaMemcpy(V.data(), d_vel, nt * sizeof(vxu_velocity), cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    char fname[256];
+    snprintf(fname, sizeof(fname), "output/vels/Vel%06d_%d.txt", step, stage);
+    FILE *f = fopen(fname, "w");
+    if (!f) return;
+    fprintf(f, "%zu\n", nt);
+    for (size_t i = 0; i < nt; ++i)
+        fprintf(f, "%zu %lf %lf %lf %lf\n", i, P[i].r[0], P[i].r[1], V[i].v[0], V[i].v[1]);
+    fclose(f);
+}
+
+// Tracers move with the velocity field and are absorbed by the wall and the
+// window like vortices (step_Kernel without the force terms).
+static int advect_tracers(vxu_vortex *tp, vxu_velocity *tv, size_t nt, vx_panel *panels) {
+    if (ensure_work((long long)nt)) return 1;
+    k_u_set<<<1, 1>>>(U.d_S, (long long)nt, (long long)nt, nullptr, nullptr);
+    ++U.launches;
+    CK(vx_launch_advect(launch0(), U.prm, aos_view(tp, tv, nullptr), U.d_S, U.w, panels));
+    CK(cudaDeviceSynchronize());
+    return 0;
+}
+
+// include/unit_1.cuh:52 — passive tracers (src/unit_1.cu:1271-1298).
+int first_speed(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *second_pos,
+                vxu_velocity *v_second, size_t *n_second, vx_panel *panels) {
+    if (!n_second) return 2;
+    if (velocity_control(pos, V_inf, n, second_pos, v_second, *n_second)) return 1;
+    save_vel(second_pos, v_second, *n_second, current_step, 5);
+    return advect_tracers(second_pos, v_second, *n_second, panels);
+}
+
+// include/unit_1.cuh:51 — inertial tracers relaxing towards the carrier
+// velocity with time constant rel_t (src/unit_1.cu:1300-1340).
+int second_speed(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *second_pos,
+                 vxu_velocity *v_second, vxu_velocity *v_env, size_t *n_second, vx_panel *panels) {
+    if (!n_second || !v_env) return 2;
+    if (velocity_control(pos, V_inf, n, second_pos, v_env, *n_second)) return 1;
+    if (current_step == first_step)
+        CK(cudaMemcpy(v_second, v_env, sizeof(vxu_velocity) * (*n_second), cudaMemcpyDeviceToDevice));
+    save_vel(second_pos, v_env, *n_second, current_step, 4);
+    k_u_relax<<<64, 256>>>((const double *)second_pos, (const double *)v_env, (double *)v_second,
+                           (long long)*n_second, conf.rel_t, conf.dt);
+    ++U.launches;
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    save_vel(second_pos, v_second, *n_second, current_step, 5);
+    return advect_tracers(second_pos, v_second, *n_second, panels);
 }
 
 // Kernel launches issued by the unit_1.cuh entry points since load.

@@ -41,6 +41,7 @@ class Conf(C.Structure):
         ("precision", C.c_int32), ("birth_offset_mode", C.c_int32),
         ("drop_eps", C.c_double), ("diff_cutoff", C.c_double),
         ("n_probes_grid", C.c_int32), ("pad1_", C.c_int32), ("probe_box", C.c_double * 4),
+        ("fmm", C.c_int32), ("pad2_", C.c_int32),
     ]
 
 
@@ -93,6 +94,12 @@ def default_conf(**kw) -> Conf:
             v = v.encode()
         setattr(c, k, v)
     return c
+
+
+def measure_peak(device: int = 0, fp64: bool = False) -> float:
+    t = C.c_double(0)
+    _check(lib().vx_measure_peak(C.c_int(device), C.c_int(int(fp64)), C.byref(t)), "vx_measure_peak")
+    return t.value
 
 
 def read_conf(path: str, conf: Conf | None = None) -> Conf:
@@ -220,7 +227,8 @@ class Sim:
         _check(lib().vx_set_timing(self.h, C.c_int(int(on))), "vx_set_timing")
 
     def timing(self):
-        o = np.zeros(3)
+        """ms per stage: birth, velocity, diffusion, wall, step, bs_pair, diff_pair, total."""
+        o = np.zeros(8)
         _check(lib().vx_get_timing(self.h, _p(o)), "vx_get_timing")
         return o
 
