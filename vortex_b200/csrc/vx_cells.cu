@@ -257,7 +257,7 @@ __device__ __forceinline__ float vx_ex2_approx(float x) {
 }
 
 // Vortex diffusion over the cell grid (bulk form).
-__global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, const VxScalars *S, const float4 *srt,
+__global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                      const unsigned *skey, const int *sorted, const int *start,
                                                      const int2 *items) {
     __shared__ float4 sm[CG_T];
@@ -293,8 +293,10 @@ __global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, const
         const long long c0 = max(ca - kk, 0LL), c1 = min(cbb + kk, nx - 1);
         const long long r0 = max(row - kk, 0LL), r1 = min(row + kk, ny - 1);
         double I2x = 0.0, I2y = 0.0, I1 = 0.0;
+        unsigned long long scanned = 0;
         for (long long rr = r0; rr <= r1; ++rr) {
             const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
+            scanned += (unsigned long long)(j1 - j0);
             const float oy = (float)((double)(rr - row) * (double)S->ch);
             for (long long jt = j0; jt < j1; jt += CG_T) {
                 __syncthreads();
@@ -325,6 +327,7 @@ __global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, const
                 I2x += (double)s2x; I2y += (double)s2y; I1 += (double)s1;
             }
         }
+        if (threadIdx.x == 0) atomicAdd(&S->pairs_diff, scanned * (unsigned long long)(last - item.y));
         if (valid && fabs(I1) > 1e-5) {
             const long long i = sorted[t];
             const double dd = (double)me.w;

@@ -689,6 +689,23 @@ extern "C" vx_status vx_set_timing(vx_sim *s, int enable) {
     return VX_OK;
 }
 
+// Pair evaluations executed by the bulk-form near-field (FMM) and
+// neighbour-list diffusion kernels since the last clear.
+extern "C" vx_status vx_get_pair_counts(vx_sim *s, double out2[2], int clear) {
+    if (!s || !out2) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    CU(cudaMemcpyAsync(s->h_S, s->d_S, sizeof(VxScalars), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    out2[0] = (double)s->h_S->pairs_bs;
+    out2[1] = (double)s->h_S->pairs_diff;
+    if (clear) {
+        s->h_S->pairs_bs = s->h_S->pairs_diff = 0;
+        CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
+        CU(cudaStreamSynchronize(s->stream));
+    }
+    return VX_OK;
+}
+
 extern "C" vx_status vx_get_timing(vx_sim *s, double out8[8]) {
     if (!s || !out8) return VX_ERR_ARG;
     for (int k = 0; k < 8; ++k) out8[k] = s->t_acc[k];

@@ -427,6 +427,16 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                 sx = 0.f; sy = 0.f;
             }
         }
+        {   // executed near-field pairs: sources in each target's 3x3 leaves
+            unsigned long long my = 0;
+            if (valid) {
+                const long long tc = (long long)tcol;
+                for (long long rr = max(row - 1, 0LL); rr <= min(row + 1, m - 1); ++rr)
+                    my += start[rr * m + min(tc + 1, m - 1) + 1] - start[rr * m + max(tc - 1, 0LL)];
+            }
+            for (int o = 16; o > 0; o >>= 1) my += __shfl_xor_sync(0xffffffffu, my, o);
+            if ((threadIdx.x & 31) == 0 && my) atomicAdd(&S->pairs_bs, my);
+        }
         if (valid && j_self < n) {
             // far field: f(z) = sum a_l u^l at the target's leaf (none below depth 2)
             cplx f = {0.0, 0.0};

@@ -80,6 +80,9 @@ struct VxScalars {
     double fx0, fy0, fside;
     long long fnleaves, fs;
     int fL, fnflag;
+    // pair evaluations executed by the bulk-form near-field and diffusion
+    // kernels since the counters were last cleared
+    unsigned long long pairs_bs, pairs_diff;
 };
 
 enum {

@@ -232,6 +232,12 @@ class Sim:
         _check(lib().vx_get_timing(self.h, _p(o)), "vx_get_timing")
         return o
 
+    def pair_counts(self, clear: bool = False):
+        """(near-field pairs, diffusion pairs) executed by the bulk form."""
+        o = np.zeros(2)
+        _check(lib().vx_get_pair_counts(self.h, _p(o), C.c_int(int(clear))), "vx_get_pair_counts")
+        return o
+
     def launches(self) -> int:
         n = C.c_int64(0)
         _check(lib().vx_get_launch_count(self.h, C.byref(n)), "vx_get_launch_count")
