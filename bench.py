@@ -164,6 +164,7 @@ def run_ours(args, rank, world, device):
             (tst[6] / K, pc[1] / K, FLOP_PER_PAIR_DIFF),
     }
     kname, (kms, kpairs, kflop) = max(kernels.items(), key=lambda kv: kv[1][0])
+    tree = sim.tree_info()
     # ---- end to end through the C ABI with host buffers -------------------
     rt = C.CDLL("libcudart.so.12")
     n_now = sim.count()
@@ -234,6 +235,7 @@ def run_ours(args, rank, world, device):
         "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
         "stage_ms": {"birth": tst[0] / K, "velocity": tst[1] / K, "diffusion": tst[2] / K,
                      "wall": tst[3] / K, "advect_compact_collapse": tst[4] / K},
+        "structures": tree,
         "fp64_plain": fp64,
         "speedup_fp32_over_fp64": (value / world) / fp64["steps_per_s"] if fp64 else None,
         "roofline": {"kernel": kname, "bound": "fp32-simt", "achieved": achieved, "peak": peak32,

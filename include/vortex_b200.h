@@ -163,6 +163,10 @@ vx_status vx_get_timing(vx_sim *sim, double out8[8]);
 /* Pair evaluations executed by the bulk form's near-field (FMM) and
  * neighbour-list diffusion kernels since the last clear (clear != 0 resets). */
 vx_status vx_get_pair_counts(vx_sim *sim, double out2[2], int clear);
+/* Spatial structures of the last bulk-form velocity / diffusion pass:
+ * out[0] quadtree depth, [1] leaf side, [2] targets redone by the exact
+ * 3-nearest search, [3] neighbour-grid cell side, [4] cells in x, [5] in y. */
+vx_status vx_get_tree_info(vx_sim *sim, double out6[6]);
 
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);

@@ -706,6 +706,21 @@ extern "C" vx_status vx_get_pair_counts(vx_sim *s, double out2[2], int clear) {
     return VX_OK;
 }
 
+extern "C" vx_status vx_get_tree_info(vx_sim *s, double out6[6]) {
+    if (!s || !out6) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    CU(cudaMemcpyAsync(s->h_S, s->d_S, sizeof(VxScalars), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    const VxScalars &h = *s->h_S;
+    out6[0] = (double)h.fL;
+    out6[1] = h.fL >= 0 ? h.fside / (double)(1LL << h.fL) : 0.0;
+    out6[2] = (double)h.fnflag;
+    out6[3] = h.ch;
+    out6[4] = (double)h.cnx;
+    out6[5] = (double)h.cny;
+    return VX_OK;
+}
+
 extern "C" vx_status vx_get_timing(vx_sim *s, double out8[8]) {
     if (!s || !out8) return VX_ERR_ARG;
     for (int k = 0; k < 8; ++k) out8[k] = s->t_acc[k];

@@ -25,7 +25,7 @@
 // direct FP32 with the core smoothing; the 3 nearest come from there and are
 // exact when the third distance is below the leaf side (nothing outside the
 // 3x3 block can be closer); the few targets that fail the test are redone by
-// a full scan.
+// a ring search over the leaves.
 #include <algorithm>
 
 #include "vx_internal.cuh"
@@ -456,38 +456,76 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
             v.d[j_self] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
             if (!(d3 < h2)) {   // a closer particle could lie outside the 3x3 block
                 const int slot = atomicAdd(&S->fnflag, 1);
-                flag_list[slot] = (int)j_self;
+                flag_list[slot] = (int)t;
             }
         }
     }
 }
 
 // Targets whose third-nearest distance reached the leaf side: exact 3
-// nearest by a full scan of the source slots (FP32, one warp per target).
+// nearest by a ring search over the leaves (one warp per target).  Ring k
+// holds the 8k leaves at Chebyshev distance k from the target's leaf; every
+// source outside rings 0..k lies at least k*h from the target (a source
+// clamped into an edge leaf lies farther out than that leaf), so the search
+// stops once the third distance is below (k h)^2 or the rings cover the grid.
+// Coordinates are relative to the target's leaf centre, as in the near field.
+__device__ __forceinline__ void fmm_ring_cell(int k, int q, int &dx, int &dy) {
+    if (k == 0) { dx = dy = 0; return; }
+    const int w = 2 * k + 1;
+    if (q < w) { dx = q - k; dy = -k; return; }
+    q -= w;
+    if (q < w) { dx = q - k; dy = k; return; }
+    q -= w;
+    if (q < w - 2) { dx = -k; dy = q - k + 1; return; }
+    q -= w - 2;
+    dx = k; dy = q - k + 1;
+}
+
 __global__ void k_fmm_nn3_fix(VxView v, const VxScalars *S, const float4 *srt, const int *sorted,
-                              const int *flag_list) {
+                              const int *start, const int *flag_list) {
     const int nf = S->fnflag;
-    const long long s = S->fs;
+    const long long m = 1LL << S->fL;
+    const double h = S->fside / (double)m;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < nf; f += warps) {
-        const long long i = flag_list[f];
-        const double ax = v.x[i * v.ps], ay = v.y[i * v.ps];
+        const long long t = flag_list[f];
+        const long long i = sorted[t];
+        const long long leaf = fmm_leaf(S, v.x[i * v.ps], v.y[i * v.ps]);
+        const long long cx = leaf % m, cy = leaf / m;
+        const float4 me = srt[t];
+        const long long kmax = max(max(cx, m - 1 - cx), max(cy, m - 1 - cy));
         float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
-        for (long long k = lane; k < s; k += 32) {
-            const long long j = sorted[k];
-            if (j == i) continue;
-            const float dx = (float)(ax - v.x[j * v.ps]), dy = (float)(ay - v.y[j * v.ps]);
-            const float r2 = fmaf(dx, dx, dy * dy);
-            vx_nn3_insert<float>(d1, d2, d3, r2);
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const float e1 = __shfl_xor_sync(0xffffffffu, d1, o);
-            const float e2 = __shfl_xor_sync(0xffffffffu, d2, o);
-            const float e3 = __shfl_xor_sync(0xffffffffu, d3, o);
-            vx_nn3_insert<float>(d1, d2, d3, e1);
-            vx_nn3_insert<float>(d1, d2, d3, e2);
-            vx_nn3_insert<float>(d1, d2, d3, e3);
+        for (long long k = 0; k <= kmax; ++k) {
+            const int ncell = k == 0 ? 1 : (int)(8 * k);
+            for (int q = lane; q < ncell; q += 32) {
+                int dx, dy;
+                fmm_ring_cell((int)k, q, dx, dy);
+                const long long X = cx + dx, Y = cy + dy;
+                if (X < 0 || X >= m || Y < 0 || Y >= m) continue;
+                const float ox = (float)((double)dx * h), oy = (float)((double)dy * h);
+                const long long c = Y * m + X;
+                for (long long j = start[c]; j < start[c + 1]; ++j) {
+                    if (j == t) continue;
+                    const float4 s = srt[j];
+                    const float ddx = me.x - (s.x + ox), ddy = me.y - (s.y + oy);
+                    vx_nn3_insert<float>(d1, d2, d3, fmaf(ddx, ddx, ddy * ddy));
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const float e1 = __shfl_xor_sync(0xffffffffu, d1, o);
+                const float e2 = __shfl_xor_sync(0xffffffffu, d2, o);
+                const float e3 = __shfl_xor_sync(0xffffffffu, d3, o);
+                vx_nn3_insert<float>(d1, d2, d3, e1);
+                vx_nn3_insert<float>(d1, d2, d3, e2);
+                vx_nn3_insert<float>(d1, d2, d3, e3);
+            }
+            // every lane holds the merged three; keep them in lane 0 only so
+            // that the next ring merges disjoint sets
+            const float kh = (float)((double)k * h);
+            const bool done = d3 < kh * kh;
+            if (lane != 0) d1 = d2 = d3 = 1e5f;
+            if (done) break;
         }
         if (lane == 0) v.d[i] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
     }
@@ -583,6 +621,7 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
                                                       (const cplx *)w.fmm_L, w.fmm_flags);
     VX_EV(L, 1);
     VX_COUNT(L);
-    k_fmm_nn3_fix<<<grid, FMM_T, 0, L.stream>>>(v, S, w.srt, sorted, w.fmm_flags); VX_COUNT(L);
+    k_fmm_nn3_fix<<<grid, FMM_T, 0, L.stream>>>(v, S, w.srt, sorted, w.fmm_start, w.fmm_flags);
+    VX_COUNT(L);
     return cudaGetLastError();
 }

@@ -238,6 +238,14 @@ class Sim:
         _check(lib().vx_get_pair_counts(self.h, _p(o), C.c_int(int(clear))), "vx_get_pair_counts")
         return o
 
+    def tree_info(self) -> dict:
+        """Quadtree depth / leaf side / 3-nearest fallbacks and neighbour-grid
+        geometry of the last bulk-form pass."""
+        o = np.zeros(6)
+        _check(lib().vx_get_tree_info(self.h, _p(o)), "vx_get_tree_info")
+        return {"fmm_level": int(o[0]), "leaf_side": o[1], "nn3_redone": int(o[2]), "cell_side": o[3],
+                "cells_x": int(o[4]), "cells_y": int(o[5])}
+
     def launches(self) -> int:
         n = C.c_int64(0)
         _check(lib().vx_get_launch_count(self.h, C.byref(n)), "vx_get_launch_count")
