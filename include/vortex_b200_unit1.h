@@ -134,6 +134,28 @@ int first_speed(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *secon
  * (no counterpart in the reference; used to show which code ran). */
 int64_t vxu_launch_count(void);
 
+/* Control points accepted by velocity_control_noalloc in one call. */
+#define VXU_NOALLOC_MAX_POINTS 4096
+
+/* velocity_control without any device allocation.  No counterpart in the
+ * reference: it is for host programs that cannot call cudaMalloc on their
+ * step path (device memory already held by another runtime's caching
+ * allocator, a fixed memory budget, or a loop that cannot take the device
+ * synchronisation an allocation may bring).  Its scratch is a fixed 4 MiB
+ * array inside this library, held on every GPU that loads it until exit;
+ * the caller passes the inputs and outputs as for velocity_control.
+ *   - at most VXU_NOALLOC_MAX_POINTS control points, else returns 2 and
+ *     launches nothing;
+ *   - plain FP64 form (results identical to velocity_control's when
+ *     VORTEX_B200_PRECISION is unset); core radius from conf.ve_size;
+ *   - the first call on a device, with that device current, looks up the
+ *     array's device address; make that first call before any stream
+ *     capture on the device;
+ *   - all calls on one device share the array; calls that overlap on the
+ *     same GPU race and must be serialised by the caller. */
+int velocity_control_noalloc(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *Contr_points,
+                             vxu_velocity *V, size_t n_contr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <vector>
 
@@ -463,3 +464,112 @@ int second_speed(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *seco
 int64_t vxu_launch_count(void) { return U.launches; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// velocity_control_noalloc: velocity_control for callers that must not
+// allocate device memory.  Some host programs cannot call cudaMalloc on the
+// step path: a process whose device memory is already held by another
+// runtime's caching allocator (cudaMalloc would fail or evict), a loop with a
+// fixed memory budget fixed at start-up, or a real-time loop that cannot take
+// the device-wide synchronisation cudaMalloc and cudaFree may imply.  This
+// entry point computes the same velocities with its scratch (the per-split
+// partial sums of the Biot-Savart kernel and the device scalars) in the
+// fixed file-scope array below, which every GPU that loads this library
+// holds until the process exits.
+//
+// Limits and behaviour:
+//   * at most VXU_NOALLOC_MAX_POINTS control points per call; more are
+//     rejected with return code 2 and a message (nothing is launched);
+//   * the plain FP64 form always (the FP32 form needs source scratch that
+//     grows with the vortex count); with VORTEX_B200_PRECISION unset its
+//     results are bit-identical to velocity_control's;
+//   * the core radius is read from conf.ve_size at each call;
+//   * the first call on a device, with that device current, looks up the
+//     array's device address (cudaGetSymbolAddress) and the SM count; make
+//     that first call before any stream capture on the device;
+//   * every call on a device shares the one array and finds there what the
+//     previous call left: the scalars are cleared at the start of each call
+//     and the partial sums are fully rewritten before they are read.  Calls
+//     that overlap on the same GPU (from several host threads) race on the
+//     array and must be serialised by the caller.
+namespace {
+constexpr long long NA_MAX_POINTS = 4096;   // control points per call
+constexpr int NA_MAX_SPLIT = 64;            // source splits (vx_pick_ksplit's cap)
+constexpr long long NA_HEAD = ((long long)sizeof(VxScalars) + 255) / 256 * 256 / (long long)sizeof(double);
+constexpr long long NA_PART = 2LL * NA_MAX_SPLIT * NA_MAX_POINTS;
+constexpr long long NA_WORDS = NA_HEAD + NA_PART;   // 4 MiB + the scalars
+constexpr int NA_MAX_DEVICES = 64;
+static_assert(NA_MAX_POINTS == VXU_NOALLOC_MAX_POINTS, "header limit");
+}  // namespace
+
+// File-scope scratch of velocity_control_noalloc.  In host code this name is
+// only a handle for cudaGetSymbolAddress, not a device address.
+static __device__ __align__(256) double vx_noalloc_scratch[NA_WORDS];
+
+namespace {
+struct NaDevice {
+    double *base = nullptr;   // device address of vx_noalloc_scratch
+    int num_sms = 0;
+};
+NaDevice g_na[NA_MAX_DEVICES];
+std::mutex g_na_mu;
+
+int na_device(int dev, NaDevice **out) {
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    NaDevice &d = g_na[dev];
+    if (!d.base) {
+        void *ptr = nullptr;
+        CK(cudaGetSymbolAddress(&ptr, vx_noalloc_scratch));
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        d.num_sms = sms > 0 ? sms : 1;
+        d.base = (double *)ptr;
+    }
+    *out = &d;
+    return 0;
+}
+}  // namespace
+
+extern "C" int velocity_control_noalloc(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *Contr_points,
+                                        vxu_velocity *V, size_t n_contr) {
+    if (!pos || !V_inf || !Contr_points || !V) return 2;
+    if (n_contr == 0) return 0;
+    if (n_contr > (size_t)NA_MAX_POINTS) {
+        fprintf(stderr, "vortex_b200: velocity_control_noalloc: %zu control points, at most %lld\n", n_contr,
+                NA_MAX_POINTS);
+        vx_set_error("velocity_control_noalloc: %zu control points, at most %lld", n_contr, NA_MAX_POINTS);
+        return 2;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAX_DEVICES) {
+        vx_set_error("velocity_control_noalloc: device %d beyond %d", dev, NA_MAX_DEVICES);
+        return 2;
+    }
+    NaDevice *d = nullptr;
+    if (na_device(dev, &d)) return 1;
+    VxParams prm;
+    memset(&prm, 0, sizeof(prm));
+    prm.prec = VX_PREC_FP64;
+    prm.eps = conf.ve_size;
+    prm.eps2 = conf.ve_size * conf.ve_size;
+    VxWork w;
+    memset(&w, 0, sizeof(w));
+    w.part = d->base + NA_HEAD;
+    w.part_cap = NA_PART;
+    VxScalars *S = (VxScalars *)d->base;
+    VxLaunch L;
+    L.stream = 0;
+    L.launches = &U.launches;
+    L.num_sms = d->num_sms;
+    CK(cudaMemsetAsync(S, 0, sizeof(VxScalars), 0));
+    k_u_set<<<1, 1>>>(S, (long long)n, (long long)n, (const double *)V_inf, nullptr);
+    ++U.launches;
+    const double *px = (const double *)Contr_points;
+    double *ov = (double *)V;
+    const int K = vx_pick_ksplit((long long)n_contr, 512, d->num_sms);
+    CK(vx_launch_probe(L, prm, aos_view(pos, nullptr, nullptr), S, w, px, px + 1, 3, (long long)n_contr, ov,
+                       ov + 1, 2, K));
+    CK(cudaDeviceSynchronize());
+    return 0;
+}
