@@ -9,20 +9,29 @@
 // keep index order, so every sum has a fixed order), and the cell-sorted
 // particles (x, y, G, d) are gathered into one float4 per particle.
 //
-// Work item = up to 256 cell-sorted targets of one grid row.  The item scans
-// the rows within its largest cut-off radius; in every row the columns it
-// needs are one contiguous range of the sorted array, staged through shared
-// memory 256 sources at a time.  Each target is owned by one item, so the
-// velocity is updated in place with no partial sums.
+// Cell side h = c mean(d) / 8.  Work item = one warp's 32 consecutive
+// cell-sorted targets of one grid row.  The warp scans the rows within its
+// largest cut-off radius R; in row offset dy it needs only the columns within
+// sqrt(R^2 - ((|dy|-1) h)^2) of its targets' x range (the window follows the
+// cut-off circle), and those columns are one contiguous range of the sorted
+// array, staged through the warp's shared memory 32 sources at a time.  A
+// target whose radius exceeds CG_KCAP cells (an isolated vortex with a large
+// d) would widen its warp's window for all 32 targets; it is left out of the
+// window and summed alone by one warp (k_diff_wide).  Each target is owned by
+// one warp, so the velocity is updated in place with no partial sums.
 #include "vx_internal.cuh"
 
 int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0, unsigned *k1, int *v1,
                   int nbits, int *hist, long long *off, long long tiles_cap);
 
 constexpr int CG_T = 256;
+constexpr int CG_W = 32;       // targets per work item (one warp)
+constexpr int CG_DIV = 8;      // cell side = cut-off radius at the mean d / CG_DIV
+constexpr int CG_KCAP = 16;    // widest window of a work item, in cells
 
 __global__ void k_cg_begin(VxScalars *S) {
     S->cb[0] = S->cb[1] = S->cb[2] = S->cb[3] = ~0ull;
+    S->cnwide = 0;
 }
 
 // Bounding box of the live particles and per-block sums of d (fixed grid:
@@ -58,7 +67,7 @@ __global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double
     }
 }
 
-// Cell side h = c * mean(d) / 4, grown until the grid fits cells_cap.
+// Cell side h = c * mean(d) / CG_DIV, grown until the grid fits cells_cap.
 __global__ void k_cg_params(VxScalars *S, const double *red, int nblocks, double cutoff, long long cells_cap) {
     const long long n = S->n;
     S->cnitems = 0;
@@ -67,7 +76,7 @@ __global__ void k_cg_params(VxScalars *S, const double *red, int nblocks, double
     for (int b = 0; b < nblocks; ++b) dsum += red[b];
     const double x0 = vx_dunkey(S->cb[0]), x1 = -vx_dunkey(S->cb[1]);
     const double y0 = vx_dunkey(S->cb[2]), y1 = -vx_dunkey(S->cb[3]);
-    double h = cutoff * (dsum / (double)n) / 4.0;
+    double h = cutoff * (dsum / (double)n) / (double)CG_DIV;
     if (!(h > 0.0)) h = 1e-3;
     long long nx = -1, ny = -1;
     for (int it = 0; it < 400; ++it) {
@@ -218,13 +227,13 @@ __global__ void k_cg_row_scan(const VxScalars *S, const int *in, long long *out)
     }
 }
 
-// Work items: each row's sorted range cut into segments of CG_T targets.
+// Work items: each row's sorted range cut into segments of CG_W targets.
 __global__ void k_cg_row_items(const VxScalars *S, const int *start, int *row_items) {
     const long long ny = S->cny, nx = S->cnx;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ny;
          r += (long long)gridDim.x * blockDim.x) {
         const int cnt = start[(r + 1) * nx] - start[r * nx];
-        row_items[r] = (cnt + CG_T - 1) / CG_T;
+        row_items[r] = (cnt + CG_W - 1) / CG_W;
     }
 }
 
@@ -241,7 +250,7 @@ __global__ void k_cg_items(VxScalars *S, const int *start, const int *row_items,
         const long long o = row_off[r];
         const int s0 = start[r * nx];
         for (int q = 0; q < row_items[r]; ++q)
-            if (o + q < items_cap) items[o + q] = make_int2((int)r, s0 + q * CG_T);
+            if (o + q < items_cap) items[o + q] = make_int2((int)r, s0 + q * CG_W);
     }
 }
 
@@ -256,85 +265,169 @@ __device__ __forceinline__ float vx_ex2_approx(float x) {
     return r;
 }
 
-// Vortex diffusion over the cell grid (bulk form).
+// One diffusion pair in FP32: target (relative position, 1/d folded into
+// ndd = -log2(e)/d, R2 = (c d)^2) and source (relative position, G).  Pairs
+// closer than 0.001 eps (the target itself) and beyond the cut-off add 0.
+__device__ __forceinline__ void diff_pair(float tx, float ty, float R2, float ndd, float thr2, float4 s,
+                                          float &s2x, float &s2y, float &s1) {
+    const float dx = tx - s.x, dy = ty - s.y;
+    const float r2 = fmaf(dx, dx, dy * dy);
+    const bool use = (r2 > thr2) & (r2 < R2);
+    const float rd = vx_rsqrt_approx(r2);
+    const float e = vx_ex2_approx(r2 * rd * ndd);
+    const float ge = use ? s.z * e : 0.0f;
+    const float m = use ? ge * rd : 0.0f;
+    s2x = fmaf(-m, dx, s2x);
+    s2y = fmaf(-m, dy, s2y);
+    s1 += ge;
+}
+
+// Cells of row offset dy that can hold a source within R of a target whose x
+// (relative to the centre of column `ocol`) lies in [xlo, xhi]; false if none.
+__device__ __forceinline__ bool diff_window(int dy, float R, float xlo, float xhi, float h, long long ocol,
+                                            long long nx, long long &c0, long long &c1) {
+    const float gy = (float)max(abs(dy) - 1, 0) * h;   // vertical gap to that row
+    const float hw2 = R * R - gy * gy;
+    if (!(hw2 >= 0.0f)) return false;
+    const float hw = sqrtf(hw2) * 1.0001f + 1e-3f * h;  // margin over FP32 rounding
+    c0 = max(ocol + (long long)floorf((xlo - hw) / h + 0.5f), 0LL);
+    c1 = min(ocol + (long long)floorf((xhi + hw) / h + 0.5f), nx - 1);
+    return c0 <= c1;
+}
+
+// Vortex diffusion over the cell grid (bulk form), one warp per work item.
 __global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                      const unsigned *skey, const int *sorted, const int *start,
-                                                     const int2 *items) {
+                                                     const int2 *items, int *wide) {
     __shared__ float4 sm[CG_T];
-    __shared__ float s_rmax;
+    const int lane = threadIdx.x & 31;
+    float4 *ws = sm + (threadIdx.x & ~31);
     const long long nitems = S->cnitems, nx = S->cnx, ny = S->cny;
-    const float h = (float)S->ch;
+    const double hd = S->ch;
+    const float h = (float)hd;
+    const unsigned unx = (unsigned)nx;
     const float cut = (float)p.diff_cutoff;
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
     const float log2e = 1.4426950408889634f;
-    for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const long long wpb = CG_T / 32;
+    unsigned long long pairs = 0;
+    for (long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < nitems; it += gridDim.x * wpb) {
         const int2 item = items[it];
         const long long row = item.x;
         const long long row_end = start[(row + 1) * nx];
-        const long long last = min((long long)item.y + CG_T, row_end);
-        const long long t = item.y + threadIdx.x;
+        const long long last = min((long long)item.y + CG_W, row_end);
+        const long long t = item.y + lane;
         const bool valid = t < last;
         float4 me = valid ? srt[t] : make_float4(0.f, 0.f, 0.f, 1.f);
         // coordinates relative to the centre of the item's first cell
-        const long long ocol = (long long)(skey[item.y] % (unsigned)nx);
-        if (valid) me.x += (float)((double)((long long)(skey[t] % (unsigned)nx) - ocol) * (double)S->ch);
+        const long long ocol = (long long)(skey[item.y] % unx);
+        if (valid) me.x += (float)((double)((long long)(skey[t] % unx) - ocol) * hd);
         const float R = cut * me.w;
+        const bool is_wide = valid && R > (float)CG_KCAP * h;
+        if (is_wide) wide[atomicAdd(&S->cnwide, 1)] = (int)t;
+        const bool act = valid && !is_wide;
+        float rmax = act ? R : 0.0f, xlo = act ? me.x : 3e38f, xhi = act ? me.x : -3e38f;
+        for (int o = 16; o > 0; o >>= 1) {
+            rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+            xlo = fminf(xlo, __shfl_xor_sync(0xffffffffu, xlo, o));
+            xhi = fmaxf(xhi, __shfl_xor_sync(0xffffffffu, xhi, o));
+        }
+        const int nact = __popc(__ballot_sync(0xffffffffu, act));
+        if (nact == 0) continue;
         const float R2 = R * R;
         const float ndd = -log2e / me.w;
-        __syncthreads();
-        if (threadIdx.x == 0) s_rmax = 0.0f;
-        __syncthreads();
-        if (valid) atomicMax((int *)&s_rmax, __float_as_int(R));   // R >= 0: int order = float order
-        __syncthreads();
-        const float rmax = s_rmax;
-        const long long kk = min((long long)ceilf(rmax / h), max(nx, ny));
-        const long long ca = (long long)(skey[item.y] % (unsigned)nx);
-        const long long cbb = (long long)(skey[last - 1] % (unsigned)nx);
-        const long long c0 = max(ca - kk, 0LL), c1 = min(cbb + kk, nx - 1);
-        const long long r0 = max(row - kk, 0LL), r1 = min(row + kk, ny - 1);
+        const int kk = (int)ceilf(rmax / h);
         double I2x = 0.0, I2y = 0.0, I1 = 0.0;
-        unsigned long long scanned = 0;
-        for (long long rr = r0; rr <= r1; ++rr) {
+        long long scanned = 0;
+        for (int dy = -kk; dy <= kk; ++dy) {
+            const long long rr = row + dy;
+            if (rr < 0 || rr >= ny) continue;
+            long long c0, c1;
+            if (!diff_window(dy, rmax, xlo, xhi, h, ocol, nx, c0, c1)) continue;
             const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
-            scanned += (unsigned long long)(j1 - j0);
-            const float oy = (float)((double)(rr - row) * (double)S->ch);
-            for (long long jt = j0; jt < j1; jt += CG_T) {
-                __syncthreads();
-                if (jt + threadIdx.x < j1) {
-                    float4 q = srt[jt + threadIdx.x];
-                    const long long sc = (long long)(skey[jt + threadIdx.x] % (unsigned)nx);
-                    q.x += (float)((double)(sc - ocol) * (double)S->ch);
+            scanned += j1 - j0;
+            const float oy = (float)((double)dy * hd);
+            for (long long jt = j0; jt < j1; jt += 32) {
+                if (jt + lane < j1) {
+                    float4 q = srt[jt + lane];
+                    q.x += (float)((double)((long long)(skey[jt + lane] % unx) - ocol) * hd);
                     q.y += oy;
-                    sm[threadIdx.x] = q;
+                    ws[lane] = q;
                 }
-                __syncthreads();
-                const int cnt = (int)min((long long)CG_T, j1 - jt);
+                __syncwarp();
+                const int cnt = (int)min(32LL, j1 - jt);
                 float s2x = 0.f, s2y = 0.f, s1 = 0.f;
 #pragma unroll 4
-                for (int q = 0; q < cnt; ++q) {
-                    const float4 s = sm[q];
-                    const float dx = me.x - s.x, dy = me.y - s.y;
-                    const float r2 = fmaf(dx, dx, dy * dy);
-                    const bool use = (r2 > thr2) & (r2 < R2);
-                    const float rd = vx_rsqrt_approx(r2);
-                    const float e = vx_ex2_approx(r2 * rd * ndd);
-                    const float ge = use ? s.z * e : 0.0f;
-                    const float m = use ? ge * rd : 0.0f;
-                    s2x = fmaf(-m, dx, s2x);
-                    s2y = fmaf(-m, dy, s2y);
-                    s1 += ge;
-                }
+                for (int q = 0; q < cnt; ++q) diff_pair(me.x, me.y, R2, ndd, thr2, ws[q], s2x, s2y, s1);
+                __syncwarp();
                 I2x += (double)s2x; I2y += (double)s2y; I1 += (double)s1;
             }
         }
-        if (threadIdx.x == 0) atomicAdd(&S->pairs_diff, scanned * (unsigned long long)(last - item.y));
-        if (valid && fabs(I1) > 1e-5) {
+        pairs += (unsigned long long)scanned * (unsigned long long)nact;
+        if (act && fabs(I1) > 1e-5) {
             const long long i = sorted[t];
             const double dd = (double)me.w;
             v.vx[i * v.vs] += -p.nu * I2x / (I1 * dd);
             v.vy[i * v.vs] += -p.nu * I2y / (I1 * dd);
         }
     }
+    if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);
+}
+
+// Targets left out of the work items: one warp per target, the lanes taking
+// consecutive sources of each row window; FP32 pair sums per row, FP64
+// across rows and lanes (fixed order).
+__global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                                                    const unsigned *skey, const int *sorted, const int *start,
+                                                    const int *wide) {
+    const int lane = threadIdx.x & 31;
+    const long long nx = S->cnx, ny = S->cny;
+    const double hd = S->ch;
+    const float h = (float)hd;
+    const unsigned unx = (unsigned)nx;
+    const float cut = (float)p.diff_cutoff;
+    const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
+    const float log2e = 1.4426950408889634f;
+    const int nw = S->cnwide;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long pairs = 0;
+    for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < nw; f += warps) {
+        const long long t = wide[f];
+        const float4 me = srt[t];
+        const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
+        const float R = cut * me.w, R2 = R * R, ndd = -log2e / me.w;
+        const long long kk = min((long long)ceilf(R / h), max(nx, ny));
+        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
+        for (long long dy = -kk; dy <= kk; ++dy) {
+            const long long rr = row + dy;
+            if (rr < 0 || rr >= ny) continue;
+            long long c0, c1;
+            if (!diff_window((int)dy, R, me.x, me.x, h, ocol, nx, c0, c1)) continue;
+            const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
+            pairs += j1 - j0;
+            const float oy = (float)((double)dy * hd);
+            float s2x = 0.f, s2y = 0.f, s1 = 0.f;
+            for (long long j = j0 + lane; j < j1; j += 32) {
+                float4 q = srt[j];
+                q.x += (float)((double)((long long)(skey[j] % unx) - ocol) * hd);
+                q.y += oy;
+                diff_pair(me.x, me.y, R2, ndd, thr2, q, s2x, s2y, s1);
+            }
+            I2x += (double)s2x; I2y += (double)s2y; I1 += (double)s1;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            I2x += __shfl_xor_sync(0xffffffffu, I2x, o);
+            I2y += __shfl_xor_sync(0xffffffffu, I2y, o);
+            I1 += __shfl_xor_sync(0xffffffffu, I1, o);
+        }
+        if (lane == 0 && fabs(I1) > 1e-5) {
+            const long long i = sorted[t];
+            const double dd = (double)me.w;
+            v.vx[i * v.vs] += -p.nu * I2x / (I1 * dd);
+            v.vy[i * v.vs] += -p.nu * I2y / (I1 * dd);
+        }
+    }
+    if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);   // every lane counted the same pairs
 }
 
 static int bits_for(long long cells) {
@@ -368,8 +461,11 @@ cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, cons
     k_cg_items<<<grid, CG_T, 0, L.stream>>>(S, w.cg_start, w.row_items, w.row_item_off, w.items, w.items_cap);
     VX_COUNT(L);
     VX_EV(L, 2);
-    k_diff_cells<<<L.num_sms * 8, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.items);
-    VX_EV(L, 3);
+    k_diff_cells<<<L.num_sms * 8, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.items,
+                                                       w.cg_wide);
     VX_COUNT(L);
+    k_diff_wide<<<L.num_sms * 4, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide);
+    VX_COUNT(L);
+    VX_EV(L, 3);
     return cudaGetLastError();
 }

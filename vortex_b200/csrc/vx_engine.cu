@@ -210,8 +210,9 @@ vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, i
     A(w.rs_hist, 256 * w.rs_tiles_cap); A(w.rs_off, 256 * w.rs_tiles_cap);
     A(w.cg_cnt, w.cells_cap); A(w.cg_start, w.cells_cap + 1);
     A(w.srt, cap);
-    w.items_cap = cap / 256 + w.cells_cap + 2;
+    w.items_cap = cap / 32 + w.cells_cap + 2;
     A(w.items, w.items_cap);
+    A(w.cg_wide, cap);
     A(w.row_items, w.cells_cap + 1); A(w.row_item_off, w.cells_cap + 1);
     // quadtree of the bulk-form Biot-Savart
     w.fmm_lmax = vx_fmm_max_level(cap);

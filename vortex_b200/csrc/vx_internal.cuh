@@ -70,7 +70,7 @@ struct VxScalars {
     double gx0, gy0, gh;
     long long gnx, gny, gncells;
     int err;
-    int pad_;
+    int cnwide;            // diffusion targets whose cut-off exceeds the item window
     // neighbour-list grid of the bulk form (vortex diffusion)
     unsigned long long cb[4];
     double cx0, cy0, ch;
@@ -125,6 +125,7 @@ struct VxWork {
     float4 *srt;
     int2 *items;             // (row, first sorted slot) of each target segment
     long long items_cap;
+    int *cg_wide;            // sorted slots of the diffusion targets summed one warp each
     int *row_items;
     long long *row_item_off;
     // quadtree: counts and expansions of every level up to fmm_lmax

@@ -6,8 +6,14 @@ the wall, same-sign collapse within 0.3 eps, |G| < 1e-8 dropped.  The
 reference holds about 1e6 vortices in this run after ~3000 steps; the
 stand-in for that state is a warm wake of n vortices on a jittered lattice
 in the 4 x 2 box behind the cylinder ([0.55, 4.55] x [-1, 1]), spacing
-a = sqrt(8/n), jitter +-a/4 (nearest neighbours stay farther apart than the
-collapse radius, so the count stays near n), strengths G ~ N(0, 1e-3).
+a = sqrt(8/n), jitter +-a/4 (nearest neighbours start farther apart than the
+collapse radius), carrying a smooth vorticity field sampled at the vortices
+(G = omega * a^2): a staggered street of five Gaussian vortices of
+circulation -+2 and radius 0.2 (negative above the axis, positive below,
+1.0 to 4.2 in x, 0.8 apart) over a shear background -0.5 tanh(y / 0.2).
+Neighbouring vortices carry like-signed, similar strengths, as in a wake
+that has run for some time, so the diffusion velocity stays moderate and
+the count stays near n over the timed steps.
 """
 from __future__ import annotations
 
@@ -47,5 +53,10 @@ def warm_wake(n: int, seed: int = 1234):
     pick = rng.permutation(nx * ny)[:n]
     x = x[pick] + rng.uniform(-0.25, 0.25, n) * (4.0 / nx)
     y = y[pick] + rng.uniform(-0.25, 0.25, n) * (2.0 / ny)
-    g = rng.normal(0.0, 1e-3, n)
+    omega = -0.5 * np.tanh(y / 0.2)
+    for k in range(5):
+        xc, yc = 1.0 + 0.8 * k, (0.3 if k % 2 == 0 else -0.3)
+        sign = -1.0 if k % 2 == 0 else 1.0
+        omega += sign * 2.0 / (math.pi * 0.04) * np.exp(-((x - xc) ** 2 + (y - yc) ** 2) / 0.04)
+    g = omega * (8.0 / n)
     return x, y, g
