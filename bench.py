@@ -248,6 +248,8 @@ def run_ours(args, rank, world, device):
         "clocks": ck,
     }
     line["cpu_baseline"] = cpu_baseline(args, x0, y0, g0, pan)
+    if args.ref_cuda_steps > 0 and world == 1:
+        line["reference_cuda_build"] = ref_cuda_build(args, x0, y0, g0)
     return line
 
 
@@ -293,6 +295,75 @@ def cpu_baseline(args, x, y, g, pan):
                       f"({spent:.1f} s measured)"}
 
 
+REF_CONF = """steps {steps}
+saving_step 100000
+dt 0.002
+inc_step {inc}
+pr_file circle1000.txt
+viscosity 0.0005
+rho 1.0
+v_inf_x 1.0
+v_inf_y 0.0
+v_inf_incr_steps 0
+n_of_points 20
+x_max 10.0
+x_min -2.0
+y_max 10.0
+y_min -10.0
+ve_size {eps!r}
+n_col 2
+r_col_diff_sign 0.0
+r_col_same_sign 0.3
+max_ve_g 1e30
+rc_x 0.0
+rc_y 0.0
+matrix_load 0
+timings_file output/timings.txt
+kadr_file Kadr000000.txt
+"""
+
+
+def ref_cuda_build(args, x, y, g):
+    """The reference's own CUDA program (its src/main.c + src/unit_1.cu +
+    src/kernel.cu, -DNO_TREE, sm_100a, built by oracle/build_ref.sh) on the
+    same workload, restarted from a frame holding the same warm wake; its
+    per-step device time is the Creation + Speed + Step event times it logs
+    (cumulative per step in its timings file)."""
+    import tempfile
+    from vortex_b200 import profiles
+    exe = os.path.join(ROOT, "oracle", "_ref", "vortex_ref")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/vortex_ref not built (oracle/build_ref.sh needs the reference sources)"}
+    K = args.ref_cuda_steps
+    with tempfile.TemporaryDirectory() as wd:
+        profiles.write_profile(os.path.join(wd, "circle1000.txt"), profiles.circle(P_PANELS))
+        with open(os.path.join(wd, "run.conf"), "w") as fh:
+            fh.write(REF_CONF.format(steps=K, inc=1 << 20, eps=2 * math.pi * 0.5 / P_PANELS))
+        with open(os.path.join(wd, "Kadr000000.txt"), "w") as fh:
+            fh.write(f"{len(x)}\n")
+            fh.writelines(f"{i} 0.008000 {x[i]:.17g} {y[i]:.17g} 0 0 0 {g[i]:.17g}\n" for i in range(len(x)))
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, "-c", "run.conf", "-l", "1"], cwd=wd, capture_output=True, text=True,
+                           timeout=args.ref_cuda_timeout)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            return {"unavailable": f"reference program exited {r.returncode}"}
+        rows = []
+        for line in open(os.path.join(wd, "output", "timings.txt")):
+            parts = line.strip().split("\t")
+            if len(parts) >= 5:
+                rows.append((int(parts[0]), int(parts[1].split("=")[1]),
+                             sum(float(q.split("=")[1]) for q in parts[2:5])))
+    per_step = [b[2] - a[2] for a, b in zip(rows[:-1], rows[1:]) if b[0] > a[0]]
+    if not per_step:
+        return {"unavailable": "reference timings file had no per-step lines"}
+    ms = float(np.median(per_step[1:] if len(per_step) > 1 else per_step))
+    return {"steps_per_s": 1e3 / ms, "ms_per_step": ms, "steps": len(per_step), "n_start": len(x),
+            "n_end": rows[-1][1], "wall_s": wall,
+            "source": "reference src/main.c + src/unit_1.cu + src/kernel.cu (-DNO_TREE, sm_100a) via "
+                      "oracle/build_ref.sh; median of its per-step Creation+Speed+Step CUDA-event times"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -330,6 +401,9 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--cpu-targets", type=int, default=2048)
     ap.add_argument("--ref-targets", type=int, default=1024)
+    ap.add_argument("--ref-cuda-steps", type=int, default=0,
+                    help="also time the reference's own CUDA build for this many steps (0: off)")
+    ap.add_argument("--ref-cuda-timeout", type=float, default=900.0)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -85,7 +85,11 @@ typedef struct vx_conf {
     int32_t pad1_;
     double probe_box[4];        /* x0, x1, y0, y1 of the probe grid */
     int32_t fmm;                /* bulk form: Biot-Savart by the quadtree
-                                   multipole method (default 1); 0 = direct */
+                                   multipole method, and the birth
+                                   right-hand side with the vortices beyond
+                                   twice the body radius through one local
+                                   expansion about the body (default 1);
+                                   0 = direct sums */
     int32_t pad2_;
 } vx_conf;
 

@@ -139,3 +139,33 @@ def test_bulk_steps_track_fp64():
     assert abs(np.mean(f32) - np.mean(f64)) <= 0.05 * max(abs(np.mean(f64)), 1e-6)
     s32.close()
     s64.close()
+
+
+def test_birth_far_field_vs_direct_and_fp64():
+    """Bulk birth with the far field (vortices beyond twice the body radius
+    through one 32-term expansion about the body centre) against the direct
+    FP32 and the FP64 right-hand side: born strengths within 1e-5 of the
+    largest FP64 strength, and no worse than twice the direct FP32 error."""
+    ck = conf_kwargs(1000, precision=N.PREC_FP32)
+    pan = profiles.circle(1000)
+    far = N.Sim(N.default_conf(**dict(ck, fmm=1)), pan)
+    direct = N.Sim(N.default_conf(**dict(ck, fmm=0)), pan)
+    plain = N.Sim(N.default_conf(**dict(ck, precision=N.PREC_FP64)), pan)
+    rng = np.random.default_rng(61)
+    r = np.concatenate([rng.uniform(0.505, 1.0, 4000), rng.uniform(1.0, 5.0, 30000)])
+    th = rng.uniform(0.0, 2 * math.pi, len(r))
+    x, y = r * np.cos(th), r * np.sin(th)
+    g = rng.normal(0.0, 1e-3, len(r))
+    out = []
+    for s in (far, direct, plain):
+        s.set_particles(x, y, g)
+        s.stage("birth")
+        out.append(s.particles()[2][len(r):])
+    gf, gd, g64 = out
+    assert len(gf) == len(g64) == 1000
+    scale = np.abs(g64).max()
+    ef, ed = np.abs(gf - g64).max(), np.abs(gd - g64).max()
+    assert ef <= 1e-5 * scale, (ef, scale)
+    assert ef <= 2 * ed + 1e-12 * scale, (ef, ed)
+    for s in (far, direct, plain):
+        s.close()

@@ -4,6 +4,8 @@
 //
 // Reference: matr_creation/inverse_matrix src/unit_1.cu:115-402,
 // Right_part_Kernel src/kernel.cu:779-847, birth_Kernel src/kernel.cu:849-873.
+#include <algorithm>
+
 #include "vx_internal.cuh"
 
 // ---------------------------------------------------------------------------
@@ -299,8 +301,201 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_partial(VxView v, const VxScalars
     }
 }
 
+// ---------------------------------------------------------------------------
+// Birth right-hand side of the bulk form with a far field.  The sum over
+// vortex j of the panel terms (alpha d + beta k_d) / (2 pi |d|^2) is the
+// mean velocity induced along the panel; with w(z) = u - i v and
+// dz = (tau_x + i tau_y) ds along it,
+//   mean (u, v) . tau = Re[ (1 / dz_panel) integral w dz ],
+//   integral_{za}^{zb} G / (2 pi i (z - zj)) dz.
+// For |zj - c| > 2 r_body (c: body centre) the kernel expands about c:
+//   1 / (z - zj) = sum_l a_l (z - c)^l,  a_l = -1 / (zj - c)^(l+1),
+// and the panel integral of the series is exact:
+//   sum_l a_l [(zb - c)^(l+1) - (za - c)^(l+1)] / (l + 1).
+// On the panels |z - c| <= r_body, so the terms fall as 2^-l (32 terms:
+// 2e-10 relative).  Far coefficients: FP64, fixed-order block partials.
+// Near vortices (inside 2 r_body) keep the direct FP32 panel terms, over a
+// list compacted in index order.
+constexpr int BF_T = 256;
+constexpr int BF_P = VX_BF_P;
+static_assert(BF_P == 32, "one far-field coefficient per lane");
+
+struct bcplx {
+    double r, i;
+};
+
+// Block b: sources [b cs, (b+1) cs) of the n0 pre-birth vortices.
+__device__ __forceinline__ void bf_chunk(const VxScalars *S, int nb, int b, long long &j0, long long &j1) {
+    const long long n0 = S->n0;
+    const long long cs = vx_ceil_div(vx_ceil_div(n0, (long long)nb), (long long)BF_T) * BF_T;
+    j0 = min((long long)b * cs, n0);
+    j1 = min(j0 + cs, n0);
+}
+
+__device__ __forceinline__ bool bf_near(const VxParams &p, double x, double y) {
+    const double dx = x - p.bc_x, dy = y - p.bc_y;
+    return dx * dx + dy * dy <= p.b_rfar2;
+}
+
+// Far-field coefficient partials (one per block, fixed order) and the
+// number of near sources of each block.
+__global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
+    __shared__ double sacc[BF_T / 32][BF_P][2];
+    __shared__ int snear[BF_T / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    long long j0, j1;
+    bf_chunk(S, gridDim.x, blockIdx.x, j0, j1);
+    double ar = 0.0, ai = 0.0;   // coefficient `lane` of this warp (BF_P == 32)
+    int nnear = 0;
+    for (long long jt = j0 + wid * 32; jt < j1; jt += BF_T) {
+        const long long j = jt + lane;
+        double tr = 0.0, ti = 0.0, wr = 0.0, wi = 0.0;
+        if (j < j1) {
+            const double x = v.x[j * v.ps], y = v.y[j * v.ps], g = v.g[j * v.ps];
+            if (bf_near(p, x, y)) {
+                ++nnear;
+            } else {
+                const double zr = x - p.bc_x, zi = y - p.bc_y;
+                const double q = 1.0 / (zr * zr + zi * zi);
+                wr = zr * q; wi = -zi * q;          // w = 1 / (zj - c)
+                tr = -g * wr; ti = -g * wi;         // a_0 term: -G w
+            }
+        }
+        for (int l = 0; l < BF_P; ++l) {
+            double sr = tr, si = ti;
+            for (int o = 16; o > 0; o >>= 1) {
+                sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                si += __shfl_xor_sync(0xffffffffu, si, o);
+            }
+            if (lane == l) { ar += sr; ai += si; }
+            const double nr = tr * wr - ti * wi, ni = tr * wi + ti * wr;
+            tr = nr; ti = ni;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) nnear += __shfl_xor_sync(0xffffffffu, nnear, o);
+    sacc[wid][lane][0] = ar;
+    sacc[wid][lane][1] = ai;
+    if (lane == 0) snear[wid] = nnear;
+    __syncthreads();
+    if (threadIdx.x < BF_P) {
+        double sr = 0.0, si = 0.0;
+        for (int q = 0; q < BF_T / 32; ++q) { sr += sacc[q][threadIdx.x][0]; si += sacc[q][threadIdx.x][1]; }
+        part[((long long)blockIdx.x * BF_P + threadIdx.x) * 2 + 0] = sr;
+        part[((long long)blockIdx.x * BF_P + threadIdx.x) * 2 + 1] = si;
+    }
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int q = 0; q < BF_T / 32; ++q) t += snear[q];
+        cnt[blockIdx.x] = t;
+    }
+}
+
+// Block-count offsets and the coefficient sums (block order), one block.
+__global__ void k_bf_scan(VxScalars *S, int nb, const int *cnt, long long *off, const double *part,
+                          double *coef) {
+    __shared__ long long sh[VX_BF_MAX_BLOCKS];
+    const int t = threadIdx.x;
+    for (int b = t; b < nb; b += blockDim.x) sh[b] = cnt[b];
+    __syncthreads();
+    if (t == 0) {
+        long long run = 0;
+        for (int b = 0; b < nb; ++b) { off[b] = run; run += sh[b]; }
+        off[nb] = run;
+        S->bf_nnear = run;
+    }
+    if (t < 2 * BF_P) {
+        double acc = 0.0;
+        for (int b = 0; b < nb; ++b) acc += part[(long long)b * 2 * BF_P + t];
+        coef[t] = acc;
+    }
+}
+
+// Near sources of each block in index order (block-wide ballot scan).
+__global__ void __launch_bounds__(BF_T) k_bf_scatter(VxParams p, VxView v, const VxScalars *S,
+                                                     const long long *off, float4 *near) {
+    __shared__ int swarp[BF_T / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    long long j0, j1;
+    bf_chunk(S, gridDim.x, blockIdx.x, j0, j1);
+    long long base = off[blockIdx.x];
+    for (long long jt = j0; jt < j1; jt += BF_T) {
+        const long long j = jt + threadIdx.x;
+        double x = 0.0, y = 0.0, g = 0.0;
+        bool nr = false;
+        if (j < j1) {
+            x = v.x[j * v.ps]; y = v.y[j * v.ps]; g = v.g[j * v.ps];
+            nr = bf_near(p, x, y);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, nr);
+        __syncthreads();
+        if (lane == 0) swarp[wid] = __popc(bal);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int q = 0; q < BF_T / 32; ++q) {
+            before += q < wid ? swarp[q] : 0;
+            total += swarp[q];
+        }
+        if (nr)
+            near[base + before + __popc(bal & ((1u << lane) - 1u))] = make_float4((float)x, (float)y, (float)g, 0.f);
+        base += total;
+    }
+}
+
+// Direct FP32 panel terms over the near list (chunked like k_rhs_partial).
+__global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx_panel *pan, int P, int P32,
+                                                    const float4 *near, double *part, int nchunks) {
+    __shared__ float sx[RHS_T], sy[RHS_T], sg[RHS_T];
+    const long long nn = S->bf_nnear;
+    const long long cs = vx_ceil_div(vx_ceil_div(nn, nchunks), RHS_T) * RHS_T;
+    const int tiles = (P + RHS_T - 1) / RHS_T;
+    const long long items = (long long)tiles * nchunks;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int pt = (int)(it % tiles);
+        const long long sc = it / tiles;
+        const int i = pt * RHS_T + threadIdx.x;
+        const bool valid = i < P;
+        float al0 = 0, al1 = 0, d0 = 1, d1 = 0;
+        if (valid) {
+            al0 = (float)pan[i].left[0]; al1 = (float)pan[i].left[1];
+            d0 = (float)pan[i].right[0] - al0; d1 = (float)pan[i].right[1] - al1;
+        }
+        const float kd0 = -d1, kd1 = d0;
+        const float dd2 = fmaf(d0, d0, d1 * d1);
+        float y0 = 0, y1 = 0;
+        const long long j0 = sc * cs, j1 = min(nn, j0 + cs);
+        for (long long jt = j0; jt < j1; jt += RHS_T) {
+            __syncthreads();
+            const long long j = jt + threadIdx.x;
+            if (j < j1) {
+                const float4 q = near[j];
+                sx[threadIdx.x] = q.x; sy[threadIdx.x] = q.y; sg[threadIdx.x] = q.z;
+            }
+            __syncthreads();
+            const int cnt = (int)min((long long)RHS_T, j1 - jt);
+            for (int q = 0; q < cnt; ++q) {
+                float s00 = al0 - sx[q], s01 = al1 - sy[q];
+                float s10 = s00 + d0, s11 = s01 + d1;
+                float A = fmaf(s00, d0, s01 * d1);
+                float B = fmaf(s10, d0, s11 * d1);
+                float z = fmaf(d0, s01, -(d1 * s00));
+                float alpha = atan2f(-dd2 * z, fmaf(z, z, A * B));
+                float r1 = fmaf(s10, s10, s11 * s11), r0 = fmaf(s00, s00, s01 * s01);
+                float beta = 0.5f * logf(r1 / r0);
+                y0 = fmaf(sg[q], fmaf(alpha, d0, beta * kd0), y0);
+                y1 = fmaf(sg[q], fmaf(alpha, d1, beta * kd1), y1);
+            }
+        }
+        if (valid) {
+            part[(sc * P32 + i) * 2 + 0] = (double)y0;
+            part[(sc * P32 + i) * 2 + 1] = (double)y1;
+        }
+    }
+}
+
+// R_i = -(mean velocity along panel i + V_inf) . tau_i; the far field (if
+// coef) adds Re[I_far (tau_x + i tau_y) / (2 pi i dz)] with dz = zb - za.
 __global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int P32,
-                            const double *part, int nchunks, double *R) {
+                            const double *part, int nchunks, double *R, VxParams p, const double *coef) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double y0 = 0.0, y1 = 0.0;
@@ -310,7 +505,28 @@ __global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int 
     }
     double d0 = pan[i].right[0] - pan[i].left[0], d1 = pan[i].right[1] - pan[i].left[1];
     double mnog = 1.0 / (VX_TWO_PI * (d0 * d0 + d1 * d1));
-    R[i] = -((mnog * y0 + S->vinf[0]) * pan[i].tang[0] + (mnog * y1 + S->vinf[1]) * pan[i].tang[1]);
+    double u = mnog * y0, w = mnog * y1;
+    if (coef) {
+        const double ar = pan[i].left[0] - p.bc_x, ai = pan[i].left[1] - p.bc_y;
+        const double br = pan[i].right[0] - p.bc_x, bi = pan[i].right[1] - p.bc_y;
+        double pa_r = ar, pa_i = ai, pb_r = br, pb_i = bi;   // (z - c)^(l+1)
+        double Ir = 0.0, Ii = 0.0;
+        for (int l = 0; l < BF_P; ++l) {
+            const double dr = (pb_r - pa_r) / (double)(l + 1), di = (pb_i - pa_i) / (double)(l + 1);
+            const double cr = coef[2 * l], ci = coef[2 * l + 1];
+            Ir += cr * dr - ci * di;
+            Ii += cr * di + ci * dr;
+            double t = pa_r * ar - pa_i * ai; pa_i = pa_r * ai + pa_i * ar; pa_r = t;
+            t = pb_r * br - pb_i * bi; pb_i = pb_r * bi + pb_i * br; pb_r = t;
+        }
+        // mean conjugate velocity W = I / (2 pi i dz): u = Re W, v = -Im W
+        const double qr = -VX_TWO_PI * d1, qi = VX_TWO_PI * d0;   // 2 pi i dz
+        const double qq = qr * qr + qi * qi;
+        const double Wr = (Ir * qr + Ii * qi) / qq, Wi = (Ii * qr - Ir * qi) / qq;
+        u += Wr;
+        w += -Wi;
+    }
+    R[i] = -((u + S->vinf[0]) * pan[i].tang[0] + (w + S->vinf[1]) * pan[i].tang[1]);
 }
 
 // gamma_i = sum_j M_ij R_j + M_iP dg, sequential in j with fma (as the
@@ -323,6 +539,56 @@ __global__ void k_gamma(const VxScalars *S, const double *M, long long ld, int P
     double acc = 0.0;
     for (int j = 0; j < P; ++j) acc = fma(row[j], R[j], acc);
     gamma[i] = fma(row[P], S->dg, acc);
+}
+
+// The same sums from the transposed inverse Mt (Mt[j ld + i] = M[i ld + j]):
+// the same order and fma per row, but a warp's 32 rows read 32 consecutive
+// doubles per step instead of 32 rows' worth of cache lines.
+__global__ void k_gamma_t(const VxScalars *S, const double *Mt, long long ld, int P, const double *R,
+                          double *gamma) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    double acc = 0.0;
+    for (int j = 0; j < P; ++j) acc = fma(Mt[(long long)j * ld + i], R[j], acc);
+    gamma[i] = fma(Mt[(long long)P * ld + i], S->dg, acc);
+}
+
+// Bulk form: one warp per row, lanes striding the row (coalesced), FP64
+// partial sums combined by a fixed butterfly.
+__global__ void k_gamma_w(const VxScalars *S, const double *M, long long ld, int P, const double *R,
+                          double *gamma) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= P) return;
+    const double *row = M + (long long)i * ld;
+    double acc = 0.0;
+    for (int j = lane; j < P; j += 32) acc = fma(row[j], R[j], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) gamma[i] = fma(row[P], S->dg, acc);
+}
+
+__global__ void k_transpose(const double *A, double *At, long long nr) {
+    __shared__ double t[32][33];
+    for (long long by = blockIdx.y; by * 32 < nr; by += gridDim.y)
+        for (long long bx = blockIdx.x; bx * 32 < nr; bx += gridDim.x) {
+            for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+                const long long i = by * 32 + r, j = bx * 32 + threadIdx.x;
+                if (i < nr && j < nr) t[r][threadIdx.x] = A[i * nr + j];
+            }
+            __syncthreads();
+            for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+                const long long i = bx * 32 + r, j = by * 32 + threadIdx.x;
+                if (i < nr && j < nr) At[i * nr + j] = t[threadIdx.x][r];
+            }
+            __syncthreads();
+        }
+}
+
+cudaError_t vx_transpose_square(const VxLaunch &L, const double *A, double *At, long long nr) {
+    const long long nb = vx_ceil_div(nr, 32LL);
+    const dim3 grid((unsigned)std::min(nb, 64LL), (unsigned)std::min(nb, 64LL)), block(32, 8);
+    k_transpose<<<grid, block, 0, L.stream>>>(A, At, nr); VX_COUNT(L);
+    return cudaGetLastError();
 }
 
 // One new vortex per panel at [n0, n0+P) (src/kernel.cu:862-872).
@@ -351,28 +617,54 @@ __global__ void k_place(VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
     if (i == 0) S->n = n0 + P;
 }
 
-cudaError_t vx_launch_birth_ld(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                               VxWork &w, const vx_panel *pan, const double *minv, long long ld,
-                               int rhs_chunks) {
+static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S, VxWork &w,
+                              const vx_panel *pan, const double *minv, long long ld, const double *minv_t,
+                              int rhs_chunks) {
     const int P = p.P, P32 = (int)vx_round32(P);
     const int tiles = (P + RHS_T - 1) / RHS_T;
     const int grid = (int)min((long long)tiles * rhs_chunks, (long long)L.num_sms * 8);
-    if (p.prec == VX_PREC_FP32)
+    const bool far = p.prec == VX_PREC_FP32 && p.birth_far;
+    if (far) {
+        const int nb = std::min(2 * L.num_sms, VX_BF_MAX_BLOCKS);
+        k_bf_far<<<nb, BF_T, 0, L.stream>>>(p, v, S, w.bf_part, w.bf_cnt); VX_COUNT(L);
+        k_bf_scan<<<1, 256, 0, L.stream>>>(S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef); VX_COUNT(L);
+        k_bf_scatter<<<nb, BF_T, 0, L.stream>>>(p, v, S, w.bf_off, w.bf_near); VX_COUNT(L);
+        k_rhs_near<<<grid, RHS_T, 0, L.stream>>>(S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
+    } else if (p.prec == VX_PREC_FP32) {
         k_rhs_partial<float><<<grid, RHS_T, 0, L.stream>>>(v, S, pan, P, P32, w.rhs_part, rhs_chunks);
-    else
+    } else {
         k_rhs_partial<double><<<grid, RHS_T, 0, L.stream>>>(v, S, pan, P, P32, w.rhs_part, rhs_chunks);
+    }
     VX_COUNT(L);
     const int b = (P + 127) / 128;
-    k_rhs_final<<<b, 128, 0, L.stream>>>(S, pan, P, P32, w.rhs_part, rhs_chunks, w.R); VX_COUNT(L);
-    k_gamma<<<b, 128, 0, L.stream>>>(S, minv, ld, P, w.R, w.gamma); VX_COUNT(L);
+    k_rhs_final<<<b, 128, 0, L.stream>>>(S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p,
+                                         far ? w.bf_coef : nullptr);
+    VX_COUNT(L);
+    if (minv_t && p.prec == VX_PREC_FP32)
+        k_gamma_w<<<(P + 3) / 4, 128, 0, L.stream>>>(S, minv, ld, P, w.R, w.gamma);
+    else if (minv_t)
+        k_gamma_t<<<b, 128, 0, L.stream>>>(S, minv_t, ld, P, w.R, w.gamma);
+    else
+        k_gamma<<<b, 128, 0, L.stream>>>(S, minv, ld, P, w.R, w.gamma);
+    VX_COUNT(L);
     k_place<<<b, 128, 0, L.stream>>>(p, v, S, pan, P, w.gamma); VX_COUNT(L);
     return cudaGetLastError();
 }
 
-// Native engine: the inverse is stored unpadded, row stride P+1.
+// Row-major inverse with row stride ld (the reference's padded matrix).
+cudaError_t vx_launch_birth_ld(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                               VxWork &w, const vx_panel *pan, const double *minv, long long ld,
+                               int rhs_chunks) {
+    return birth_impl(L, p, v, S, w, pan, minv, ld, nullptr, rhs_chunks);
+}
+
+// Native engine: the inverse and its transpose, unpadded, stride P+1.  The
+// plain form solves in the reference's row order from the transpose; the
+// bulk form a warp per row.
 cudaError_t vx_launch_birth(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                            VxWork &w, const vx_panel *pan, const double *minv, int rhs_chunks) {
-    return vx_launch_birth_ld(L, p, v, S, w, pan, minv, (long long)p.P + 1, rhs_chunks);
+                            VxWork &w, const vx_panel *pan, const double *minv, const double *minv_t,
+                            int rhs_chunks) {
+    return birth_impl(L, p, v, S, w, pan, minv, (long long)p.P + 1, minv_t, rhs_chunks);
 }
 
 cudaError_t vx_launch_step_end(const VxLaunch &L, VxScalars *S) {

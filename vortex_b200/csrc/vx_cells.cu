@@ -295,13 +295,58 @@ __device__ __forceinline__ bool diff_window(int dy, float R, float xlo, float xh
     return c0 <= c1;
 }
 
-// Vortex diffusion over the cell grid (bulk form), one warp per work item.
-__global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, VxScalars *S, const float4 *srt,
-                                                     const unsigned *skey, const int *sorted, const int *start,
-                                                     const int2 *items, int *wide) {
-    __shared__ float4 sm[CG_T];
+// Packed FP32 pairs (PTX f32x2, sm_100): one instruction computes the same
+// operation for the lane's two targets.  The low half is the first target.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2_pack(float a, float b) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
+    f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// Vortex diffusion over the cell grid (bulk form), one warp per work item of
+// CG_W targets, one per lane; each step of the inner loop takes two sources
+// in packed FP32 pairs.  Per pair: r^2, 1/r = rsqrt(max(r^2, thr^2)),
+// e = 2^(-log2(e) r / d_i); the pair adds G e (I1) and G e (r_i - r_j) / r
+// (I2) unless r <= 0.001 eps.  Every source of the warp's window enters (the
+// window covers all sources within c d_i of each target; the ones beyond
+// weigh below e^-c).  A chunk of 32 staged sources is padded with G = 0
+// (which adds exactly 0) so the pair loop has a fixed trip count.
+#ifndef VX_DIFF_MINB
+#define VX_DIFF_MINB 2   // minimum resident blocks per SM requested for k_diff_cells
+#endif
+__global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, VxView v, VxScalars *S,
+                                                                   const float4 *srt, const unsigned *skey,
+                                                                   const int *sorted, const int *start,
+                                                                   const int2 *items, int *wide) {
+    __shared__ float4 sxy[CG_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
+    __shared__ float2 sg[CG_T / 2];    // (G_a, G_b)
     const int lane = threadIdx.x & 31;
-    float4 *ws = sm + (threadIdx.x & ~31);
+    float4 *wxy = sxy + ((threadIdx.x & ~31) >> 1);
+    float2 *wg = sg + ((threadIdx.x & ~31) >> 1);
     const long long nitems = S->cnitems, nx = S->cnx, ny = S->cny;
     const double hd = S->ch;
     const float h = (float)hd;
@@ -334,8 +379,9 @@ __global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, VxSca
         }
         const int nact = __popc(__ballot_sync(0xffffffffu, act));
         if (nact == 0) continue;
-        const float R2 = R * R;
-        const float ndd = -log2e / me.w;
+        const f2 TX = f2_pack(me.x, me.x), TY = f2_pack(me.y, me.y);
+        const float nd = -log2e / me.w;
+        const f2 NDD = f2_pack(nd, nd);
         const int kk = (int)ceilf(rmax / h);
         double I2x = 0.0, I2y = 0.0, I1 = 0.0;
         long long scanned = 0;
@@ -348,19 +394,43 @@ __global__ void __launch_bounds__(CG_T) k_diff_cells(VxParams p, VxView v, VxSca
             scanned += j1 - j0;
             const float oy = (float)((double)dy * hd);
             for (long long jt = j0; jt < j1; jt += 32) {
+                float x = 0.f, y = 0.f, gq = 0.f;
                 if (jt + lane < j1) {
-                    float4 q = srt[jt + lane];
-                    q.x += (float)((double)((long long)(skey[jt + lane] % unx) - ocol) * hd);
-                    q.y += oy;
-                    ws[lane] = q;
+                    const float4 q = srt[jt + lane];
+                    x = q.x + (float)((double)((long long)(skey[jt + lane] % unx) - ocol) * hd);
+                    y = q.y + oy;
+                    gq = q.z;
+                }
+                float *slot = reinterpret_cast<float *>(wxy + (lane >> 1));
+                slot[lane & 1] = x;
+                slot[2 + (lane & 1)] = y;
+                reinterpret_cast<float *>(wg + (lane >> 1))[lane & 1] = gq;
+                __syncwarp();
+                f2 S2X = 0ull, S2Y = 0ull, S1 = 0ull;   // +0.0f in both halves
+#pragma unroll 8
+                for (int q = 0; q < 16; ++q) {
+                    const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(wxy + q);
+                    const f2 G = *reinterpret_cast<const f2 *>(wg + q);
+                    const f2 DX = f2_sub(TX, sq.x), DY = f2_sub(TY, sq.y);
+                    const f2 R2 = f2_fma(DX, DX, f2_mul(DY, DY));
+                    float r2a, r2b;
+                    f2_unpack(R2, r2a, r2b);
+                    const f2 RD = f2_pack(vx_rsqrt_approx(fmaxf(r2a, thr2)), vx_rsqrt_approx(fmaxf(r2b, thr2)));
+                    float aa, ab;
+                    f2_unpack(f2_mul(f2_mul(R2, RD), NDD), aa, ab);
+                    const float ea = r2a > thr2 ? vx_ex2_approx(aa) : 0.0f;
+                    const float eb = r2b > thr2 ? vx_ex2_approx(ab) : 0.0f;
+                    const f2 GE = f2_mul(G, f2_pack(ea, eb));
+                    const f2 M = f2_mul(GE, RD);
+                    S2X = f2_fma(M, DX, S2X);   // sums of +m dx, +m dy: negated below
+                    S2Y = f2_fma(M, DY, S2Y);
+                    S1 = f2_add(S1, GE);
                 }
                 __syncwarp();
-                const int cnt = (int)min(32LL, j1 - jt);
-                float s2x = 0.f, s2y = 0.f, s1 = 0.f;
-#pragma unroll 4
-                for (int q = 0; q < cnt; ++q) diff_pair(me.x, me.y, R2, ndd, thr2, ws[q], s2x, s2y, s1);
-                __syncwarp();
-                I2x += (double)s2x; I2y += (double)s2y; I1 += (double)s1;
+                float a, b;
+                f2_unpack(S2X, a, b); I2x -= (double)a + (double)b;
+                f2_unpack(S2Y, a, b); I2y -= (double)a + (double)b;
+                f2_unpack(S1, a, b); I1 += (double)a + (double)b;
             }
         }
         pairs += (unsigned long long)scanned * (unsigned long long)nact;

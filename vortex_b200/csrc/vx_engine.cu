@@ -61,6 +61,8 @@ struct vx_sim {
     VxParams prm;
     vx_panel *d_pan = nullptr;
     double *d_minv = nullptr;
+    double *d_minvT = nullptr;   // transposed copy read by the birth solve
+    int *d_wstart = nullptr, *d_widx = nullptr;   // wall panel lists per wall cell
     VxScalars *d_S = nullptr;
     VxScalars *h_S = nullptr;     // pinned mirror
     long long cap = 0;
@@ -135,6 +137,25 @@ void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams 
     p->rc_x = c->rc_x; p->rc_y = c->rc_y;
     p->drop_eps = c->drop_eps;
     p->diff_cutoff = c->diff_cutoff;
+    // body centre and radius (all endpoints) for the birth far field: the
+    // expansion about the centre converges at ratio 1/2 on the panels for
+    // vortices beyond twice the radius
+    if (P > 0) {
+        double ex0 = 1e300, ex1 = -1e300, ey0 = 1e300, ey1 = -1e300;
+        for (int i = 0; i < P; ++i)
+            for (const double *e : {pan[i].left, pan[i].right}) {
+                ex0 = std::min(ex0, e[0]); ex1 = std::max(ex1, e[0]);
+                ey0 = std::min(ey0, e[1]); ey1 = std::max(ey1, e[1]);
+            }
+        p->bc_x = 0.5 * (ex0 + ex1);
+        p->bc_y = 0.5 * (ey0 + ey1);
+        double r2 = 0.0;
+        for (int i = 0; i < P; ++i)
+            for (const double *e : {pan[i].left, pan[i].right})
+                r2 = std::max(r2, (e[0] - p->bc_x) * (e[0] - p->bc_x) + (e[1] - p->bc_y) * (e[1] - p->bc_y));
+        p->b_rfar2 = 4.0 * r2 * (1.0 + 1e-12);
+        p->birth_far = (c->precision == VX_PREC_FP32 && c->fmm) ? 1 : 0;
+    }
     p->P = P;
     p->n_of_points = (int)c->n_of_points;
     p->birth_mode = c->birth_offset_mode;
@@ -203,11 +224,13 @@ vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, i
     w.rhs_part_cap = (long long)num_sms * 4 * P32 * 2;
     A(w.rhs_part, w.rhs_part_cap);
     A(w.R, P32); A(w.gamma, P32);
+    A(w.bf_part, 2LL * VX_BF_P * VX_BF_MAX_BLOCKS); A(w.bf_cnt, VX_BF_MAX_BLOCKS);
+    A(w.bf_off, VX_BF_MAX_BLOCKS + 1); A(w.bf_near, cap); A(w.bf_coef, 2 * VX_BF_P);
     A(w.red, VX_RED_BLOCKS * 4);
     // neighbour-list grid of the bulk form
     A(w.key0, cap); A(w.key1, cap); A(w.val0, cap); A(w.val1, cap);
     w.rs_tiles_cap = vx_rs_tiles_cap(cap);
-    A(w.rs_hist, 256 * w.rs_tiles_cap); A(w.rs_off, 256 * w.rs_tiles_cap);
+    A(w.rs_hist, 256 * w.rs_tiles_cap); A(w.rs_off, 256 * (w.rs_tiles_cap + 1));
     A(w.cg_cnt, w.cells_cap); A(w.cg_start, w.cells_cap + 1);
     A(w.srt, cap);
     w.items_cap = cap / 32 + w.cells_cap + 2;
@@ -297,6 +320,44 @@ static int kv_for(vx_sim *s) {
 }
 
 // ---------------------------------------------------------------------------
+// Wall panel lists: cells of side 5 L_max (1 % margin) over the birth-point
+// box grown by 5 L_max; each panel is listed in the 3 x 3 cells around its
+// birth point, in ascending panel order.
+static vx_status build_wall_lists(vx_sim *s, const vx_panel *pan, int P) {
+    VxParams &p = s->prm;
+    double lmax = 0.0;
+    for (int i = 0; i < P; ++i) lmax = std::max(lmax, pan[i].length);
+    if (P <= 0 || !(lmax > 0.0)) { p.wall_nx = p.wall_ny = 0; return VX_OK; }
+    const double h = 5.0 * lmax * 1.01;
+    const long long nx = std::max(1LL, (long long)std::ceil((p.wall_x1 - p.wall_x0) / h));
+    const long long ny = std::max(1LL, (long long)std::ceil((p.wall_y1 - p.wall_y0) / h));
+    if (nx * ny > (1LL << 24)) { p.wall_nx = p.wall_ny = 0; return VX_OK; }   // degenerate: test all
+    std::vector<std::vector<int>> cells((size_t)(nx * ny));
+    for (int f = 0; f < P; ++f) {
+        const long long cx = std::min(std::max((long long)std::floor((pan[f].birth[0] - p.wall_x0) / h), 0LL), nx - 1);
+        const long long cy = std::min(std::max((long long)std::floor((pan[f].birth[1] - p.wall_y0) / h), 0LL), ny - 1);
+        for (long long yy = std::max(cy - 1, 0LL); yy <= std::min(cy + 1, ny - 1); ++yy)
+            for (long long xx = std::max(cx - 1, 0LL); xx <= std::min(cx + 1, nx - 1); ++xx)
+                cells[(size_t)(yy * nx + xx)].push_back(f);
+    }
+    std::vector<int> start((size_t)(nx * ny + 1), 0), idx;
+    for (size_t c = 0; c < cells.size(); ++c) {
+        start[c] = (int)idx.size();
+        idx.insert(idx.end(), cells[c].begin(), cells[c].end());
+    }
+    start[cells.size()] = (int)idx.size();
+    if (idx.empty()) idx.push_back(0);
+    if (cudaMalloc(&s->d_wstart, sizeof(int) * start.size()) != cudaSuccess) return VX_ERR_NOMEM;
+    if (cudaMalloc(&s->d_widx, sizeof(int) * idx.size()) != cudaSuccess) return VX_ERR_NOMEM;
+    if (cudaMemcpy(s->d_wstart, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->d_widx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return VX_ERR_CUDA;
+    p.wall_h = h;
+    p.wall_nx = (int)nx;
+    p.wall_ny = (int)ny;
+    return VX_OK;
+}
+
 extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t P, int device,
                                vx_sim **out) {
     if (!conf || !pan || P < 2 || !out) { vx_set_error("vx_create: bad arguments"); return VX_ERR_ARG; }
@@ -342,6 +403,7 @@ extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t
     }
     if (cudaMemcpy(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(VX_ERR_CUDA);
+    if (build_wall_lists(s, pan, (int)P) != VX_OK) return fail(VX_ERR_NOMEM);
     // panel system on the device
     const long long S1 = P + 1;
     if (cudaMalloc(&s->d_minv, sizeof(double) * S1 * S1) != cudaSuccess) return fail(VX_ERR_NOMEM);
@@ -351,6 +413,9 @@ extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t
     if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) { cudaFree(work); return fail(VX_ERR_NOMEM); }
     VxLaunch L = launch_of(s);
     cudaError_t e = vx_build_matrix(L, s->d_pan, (int)P, s->d_minv, work, flag, nullptr);
+    if (e == cudaSuccess && cudaMalloc(&s->d_minvT, sizeof(double) * S1 * S1) != cudaSuccess)
+        e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = vx_transpose_square(L, s->d_minv, s->d_minvT, S1);
     int hflag = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -374,6 +439,9 @@ extern "C" vx_status vx_destroy(vx_sim *s) {
     for (double *a : arr) if (a) cudaFree(a);
     if (s->d_pan) cudaFree(s->d_pan);
     if (s->d_minv) cudaFree(s->d_minv);
+    if (s->d_minvT) cudaFree(s->d_minvT);
+    if (s->d_wstart) cudaFree(s->d_wstart);
+    if (s->d_widx) cudaFree(s->d_widx);
     if (s->d_S) cudaFree(s->d_S);
     if (s->h_S) cudaFreeHost(s->h_S);
     if (s->d_probe) cudaFree(s->d_probe);
@@ -560,7 +628,7 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
     ev(0);
     if (mask & VX_STAGE_BIRTH) {
         if ((e = vx_launch_step_begin(L, s->d_S)) != cudaSuccess) return e;
-        if ((e = vx_launch_birth(L, p, v, s->d_S, s->w, s->d_pan, s->d_minv, rhs_chunks_for(s))) != cudaSuccess) return e;
+        if ((e = vx_launch_birth(L, p, v, s->d_S, s->w, s->d_pan, s->d_minv, s->d_minvT, rhs_chunks_for(s))) != cudaSuccess) return e;
     }
     ev(1);
     if (mask & VX_STAGE_VELOCITY) {
@@ -576,7 +644,7 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
         if ((e = vx_launch_diffusion(L, p, v, s->d_S, s->w, kv)) != cudaSuccess) return e;
     ev(3);
     if (mask & VX_STAGE_WALL)
-        if ((e = vx_launch_wall(L, p, v, s->d_S, s->d_pan)) != cudaSuccess) return e;
+        if ((e = vx_launch_wall(L, p, v, s->d_S, s->d_pan, s->d_wstart, s->d_widx)) != cudaSuccess) return e;
     ev(4);
     if (mask & VX_STAGE_ADVECT)
         if ((e = vx_launch_advect(L, p, v, s->d_S, s->w, s->d_pan)) != cudaSuccess) return e;

@@ -14,12 +14,16 @@
 //
 // Tree: uniform levels 0..L over the particles' square bounding box, dense
 // row-major cell arrays per level.  Expansions in FP64, scaled by the cell
-// side s (w = (z - c)/s keeps every coefficient O(1)):
-//   multipole  b_k  = sum_j G_j w_j^k                      (P2M)
-//   field      f(z) = sum_k b_k s^k (z - c)^-(k+1)
-//   local      f(z) = sum_l a_l u^l,  u = (z - c)/s           (M2L, L2L, L2P)
-// M2L between two cells of one level with integer offset t = (c_T - c_S)/s:
-//   a_l += (1/s) sum_k b_k C(k+l, l) (-1)^l t^-(k+l+1).
+// side s (w = (z - c)/s keeps every coefficient O(1)) and by factorials:
+//   multipole  B_k  = (1/k!) sum_j G_j w_j^k               (P2M)
+//   field      f(z) = sum_k k! B_k s^k (z - c)^-(k+1)
+//   local      f(z) = sum_l A_l u^l / l!,  u = (z - c)/s      (M2L, L2L, L2P)
+// M2L between two cells of one level with integer offset t = (c_T - c_S)/s
+// is then a Hankel product (no binomials):
+//   A_l += ((-1)^l / s) sum_k B_k H_{k+l},  H_j = j! t^-(j+1),
+// and the shifts M2M / L2L use E_p = d^p / p! for the child offset d:
+//   B_k(parent) = sum_m E_{k-m} 2^-m B_m(child),
+//   A_l(child)  = 2^-l sum_{j>=l} E_{j-l} A_j(parent).
 // Interaction list: children of the parent's 3x3 neighbours that are not
 // neighbours of the cell.  Near field: the 3x3 leaves around a target's leaf,
 // direct FP32 with the core smoothing; the 3 nearest come from there and are
@@ -48,6 +52,12 @@ __device__ __forceinline__ cplx cinv(cplx a) {
 }
 
 __host__ __device__ inline long long fmm_level_off(int l) { return ((1LL << (2 * l)) - 1) / 3; }
+
+// 1/k for k = 1..FMM_P (folded at compile time)
+__constant__ double c_fmm_inv[FMM_P + 1] = {0.0,      1.0,      1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,
+                                            1.0 / 6,  1.0 / 7,  1.0 / 8,  1.0 / 9,  1.0 / 10, 1.0 / 11,
+                                            1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15, 1.0 / 16};
+static_assert(FMM_P == 16, "reciprocal table length");
 
 // ---------------------------------------------------------------------------
 __global__ void k_fmm_begin(VxScalars *S) { S->fb[0] = S->fb[1] = S->fb[2] = S->fb[3] = ~0ull; S->fnflag = 0; }
@@ -229,11 +239,11 @@ __global__ void k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const 
             if (j >= n) continue;
             const double gj = v.g[j * v.ps];
             const cplx w = {(v.x[j * v.ps] - cx) / h, (v.y[j * v.ps] - cy) / h};
-            cplx pw = {gj, 0.0};
+            cplx pw = {gj, 0.0};   // G w^k / k!
 #pragma unroll
             for (int k = 0; k < FMM_P; ++k) {
                 b[k] = cadd(b[k], pw);
-                pw = cmul(pw, w);
+                pw = cscale(cmul(pw, w), c_fmm_inv[k + 1]);
             }
         }
 #pragma unroll
@@ -255,56 +265,75 @@ __global__ void k_fmm_count_up(const VxScalars *S, int *cnt, int l) {
     }
 }
 
-// M2M: parent at level l from its 4 children at level l+1.  Child centre
-// offset delta = (+-1 +- i) s/4; b_k = sum_m C(k,m) (delta/s)^(k-m) 2^-m b'_m.
-__global__ void k_fmm_m2m(const VxScalars *S, const int *cnt, cplx *M, int l) {
+// Shift table shared by M2M and L2L, built per block in shared memory:
+// E[q][p] = d_q^p / p! for the child offsets d_q = (+-1 +- i)/4 (in units of
+// the parent side), q = (dy > 0) * 2 + (dx > 0).
+__device__ __forceinline__ void fmm_shift_table(cplx (*se)[FMM_P]) {
+    if (threadIdx.x < 4) {
+        const int q = threadIdx.x;
+        const cplx dd = {(q & 1) ? 0.25 : -0.25, (q >> 1) ? 0.25 : -0.25};
+        cplx pw = {1.0, 0.0};
+        for (int p = 0; p < FMM_P; ++p) { se[q][p] = pw; pw = cscale(cmul(pw, dd), c_fmm_inv[p + 1]); }
+    }
+}
+
+// M2M: parent at level l from its 4 children at level l+1, one thread per
+// (parent, coefficient k).
+__global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, const int *cnt, cplx *M, int l) {
+    __shared__ cplx se[4][FMM_P];
     if (l + 1 > S->fL) return;
+    fmm_shift_table(se);
+    __syncthreads();
     const long long m = 1LL << l, m2 = 2 * m;
     cplx *Mp = M + fmm_level_off(l) * FMM_P;
     const cplx *Mc = M + fmm_level_off(l + 1) * FMM_P;
     const int *cp = cnt + fmm_level_off(l);
     const int *cc = cnt + fmm_level_off(l + 1);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < m * m;
-         c += (long long)gridDim.x * blockDim.x) {
-        cplx b[FMM_P];
-#pragma unroll
-        for (int k = 0; k < FMM_P; ++k) b[k] = {0.0, 0.0};
+    const long long tot = m * m * FMM_P;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long c = e / FMM_P;
+        const int k = (int)(e % FMM_P);
+        cplx b = {0.0, 0.0};
         if (cp[c] > 0) {
             const long long ix = c % m, iy = c / m;
             for (int q = 0; q < 4; ++q) {
-                const long long cx = 2 * ix + (q & 1), cy = 2 * iy + (q >> 1);
-                const long long child = cy * m2 + cx;
+                const long long child = (2 * iy + (q >> 1)) * m2 + 2 * ix + (q & 1);
                 if (cc[child] == 0) continue;
-                // child centre minus parent centre, in units of the parent side
-                const cplx dd = {(q & 1) ? 0.25 : -0.25, (q >> 1) ? 0.25 : -0.25};
-                cplx bc[FMM_P];
-                double sc = 1.0;
-#pragma unroll
-                for (int k = 0; k < FMM_P; ++k) { bc[k] = cscale(Mc[child * FMM_P + k], sc); sc *= 0.5; }
-                // b_k += sum_{m<=k} C(k,m) dd^(k-m) bc_m  (Horner-like by powers of dd)
-#pragma unroll
-                for (int k = 0; k < FMM_P; ++k) {
-                    cplx acc = {0.0, 0.0};
-                    cplx pw = {1.0, 0.0};
-                    double binom = 1.0;   // C(k, k-r) for r = k - mm
-                    for (int mm = k; mm >= 0; --mm) {
-                        acc = cadd(acc, cscale(cmul(pw, bc[mm]), binom));
-                        pw = cmul(pw, dd);
-                        binom = binom * (double)mm / (double)(k - mm + 1);
-                    }
-                    b[k] = cadd(b[k], acc);
+                double sc = 1.0;   // 2^-mm
+                for (int mm = 0; mm <= k; ++mm) {
+                    b = cadd(b, cscale(cmul(se[q][k - mm], Mc[child * FMM_P + mm]), sc));
+                    sc *= 0.5;
                 }
             }
         }
-#pragma unroll
-        for (int k = 0; k < FMM_P; ++k) Mp[c * FMM_P + k] = b[k];
+        Mp[e] = b;
     }
 }
 
 // M2L at level l (2 <= l <= L) plus L2L from level l-1: one thread per
-// (cell, coefficient).  Locals are stored per level.
-__global__ void k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M, cplx *Loc, int l) {
+// (cell, coefficient).  Locals are stored per level.  The Hankel entries
+// H_j = j! t^-(j+1) of the 40 integer offsets t of an interaction list are
+// tabulated per block in shared memory.
+__global__ void __launch_bounds__(128) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
+                                                     cplx *Loc, int l) {
+    __shared__ cplx sh[49][2 * FMM_P - 1];   // offset (dx, dy) in [-3, 3]^2 at (dy+3)*7 + dx+3
+    __shared__ cplx se[4][FMM_P];
     if (l > S->fL) return;
+    fmm_shift_table(se);
+    for (int q = threadIdx.x; q < 49; q += blockDim.x) {
+        const int dx = q % 7 - 3, dy = q / 7 - 3;
+        if (abs(dx) <= 1 && abs(dy) <= 1) continue;   // neighbours: never an interaction
+        const cplx ti = cinv(cplx{(double)dx, (double)dy});
+        cplx tp = ti;
+        double fact = 1.0;   // j!
+        for (int j = 0; j < 2 * FMM_P - 1; ++j) {
+            sh[q][j] = cscale(tp, fact);
+            tp = cmul(tp, ti);
+            fact *= (double)(j + 1);
+        }
+    }
+    __syncthreads();
     const long long m = 1LL << l;
     const double s = S->fside / (double)m;
     const cplx *Ml = M + fmm_level_off(l) * FMM_P;
@@ -324,35 +353,26 @@ __global__ void k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
                     if (llabs(qx - ix) <= 1 && llabs(qy - iy) <= 1) continue;   // neighbours: near field
                     const long long src = qy * m + qx;
                     if (cl[src] == 0) continue;
-                    const cplx t = {(double)(ix - qx), (double)(iy - qy)};
-                    const cplx ti = cinv(t);
-                    // t^-(l+1)
-                    cplx tp = ti;
-                    for (int r = 0; r < lc; ++r) tp = cmul(tp, ti);
-                    double binom = 1.0;   // C(k+lc, lc) at k = 0
-                    cplx acc = {0.0, 0.0};
+                    const cplx *H = sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + lc;   // H_{k+lc}
+                    const cplx *B = Ml + src * FMM_P;
+                    double ar = 0.0, ai = 0.0;
+#pragma unroll
                     for (int k = 0; k < FMM_P; ++k) {
-                        acc = cadd(acc, cscale(cmul(Ml[src * FMM_P + k], tp), binom));
-                        tp = cmul(tp, ti);
-                        binom = binom * (double)(k + 1 + lc) / (double)(k + 1);
+                        const cplx b = B[k], hh = H[k];
+                        ar = fma(b.r, hh.r, fma(-b.i, hh.i, ar));
+                        ai = fma(b.r, hh.i, fma(b.i, hh.r, ai));
                     }
-                    a = cadd(a, acc);
+                    a.r += ar;
+                    a.i += ai;
                 }
             }
             a = cscale(a, ((lc & 1) ? -1.0 : 1.0) / s);
             if (l > 2) {
-                // L2L from the parent: u_parent = u/2 + dd, dd = child centre offset / parent side
+                // L2L from the parent
                 const long long parent = py * (m >> 1) + px;
-                const cplx dd = {(ix & 1) ? 0.25 : -0.25, (iy & 1) ? 0.25 : -0.25};
-                // a'_lc = 2^-lc sum_{j>=lc} C(j, lc) dd^(j-lc) a_j
+                const int q = (int)((iy & 1) * 2 + (ix & 1));
                 cplx acc = {0.0, 0.0};
-                cplx pw = {1.0, 0.0};
-                double binom = 1.0;   // C(j, lc) at j = lc
-                for (int j = lc; j < FMM_P; ++j) {
-                    acc = cadd(acc, cscale(cmul(Lp[parent * FMM_P + j], pw), binom));
-                    pw = cmul(pw, dd);
-                    binom = binom * (double)(j + 1) / (double)(j + 1 - lc);
-                }
+                for (int j = lc; j < FMM_P; ++j) acc = cadd(acc, cmul(Lp[parent * FMM_P + j], se[q][j - lc]));
                 a = cadd(a, cscale(acc, ldexp(1.0, -lc)));
             }
         }
@@ -445,8 +465,10 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                 const double xd = v.x[j_self * v.ps], yd = v.y[j_self * v.ps];
                 const cplx u = {(xd - (S->fx0 + ((double)(leaf % m) + 0.5) * h)) / h,
                                 (yd - (S->fy0 + ((double)(leaf / m) + 0.5) * h)) / h};
+                // f = sum_l A_l u^l / l!, nested as A_0 + (u/1)(A_1 + (u/2)(A_2 + ...))
                 f = LL[leaf * FMM_P + FMM_P - 1];
-                for (int l = FMM_P - 2; l >= 0; --l) f = cadd(cmul(f, u), LL[leaf * FMM_P + l]);
+                for (int l = FMM_P - 2; l >= 0; --l)
+                    f = cadd(cmul(f, cscale(u, c_fmm_inv[l + 1])), LL[leaf * FMM_P + l]);
             }
             // u - i v = f / (2 pi i): vx = Im f / 2pi, vy = Re f / 2pi
             const double vx = (ax + f.i) / VX_TWO_PI + S->vinf[0];
@@ -604,8 +626,9 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     // of levels below the depth chosen on the device return at once
     for (int l = Lmax - 1; l >= 0; --l) {
         const int g = (int)std::min<long long>(grid, vx_ceil_div(1LL << (2 * l), 128));
+        const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));
         k_fmm_count_up<<<g, 128, 0, L.stream>>>(S, w.fmm_cnt, l); VX_COUNT(L);
-        k_fmm_m2m<<<g, 128, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
+        k_fmm_m2m<<<gm, 128, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
     }
     for (int l = 2; l <= Lmax; ++l) {
         const int g = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));

@@ -40,9 +40,16 @@ struct VxParams {
     double x_min, x_max, y_min, y_max;          // wake window
     double px_min, px_max, py_min, py_max;      // profile bbox (left endpoints)
     double wall_x0, wall_x1, wall_y0, wall_y1;  // birth-point bbox grown by 5 L_max
+    double wall_h;                              // side of the wall panel-list cells
+    int wall_nx, wall_ny;                       // wall cells (0: no lists)
     double rc_x, rc_y;
     double drop_eps;
     double diff_cutoff;
+    // birth right-hand side of the bulk form: vortices farther than
+    // sqrt(b_rfar2) from the body centre (bc_x, bc_y) enter through one
+    // local expansion about that centre (birth_far != 0)
+    double bc_x, bc_y, b_rfar2;
+    int birth_far;
     int P;
     int n_of_points;
     int birth_mode;
@@ -71,6 +78,7 @@ struct VxScalars {
     long long gnx, gny, gncells;
     int err;
     int cnwide;            // diffusion targets whose cut-off exceeds the item window
+    long long bf_nnear;    // birth sources inside the far-field radius
     // neighbour-list grid of the bulk form (vortex diffusion)
     unsigned long long cb[4];
     double cx0, cy0, ch;
@@ -113,6 +121,13 @@ struct VxWork {
     double *rhs_part;        // [chunks][P32][2]
     long long rhs_part_cap;
     double *R, *gamma;
+    // birth far field: per-block expansion partials, near-source counts /
+    // offsets, the near sources (x, y, G), the summed coefficients
+    double *bf_part;
+    int *bf_cnt;
+    long long *bf_off;
+    float4 *bf_near;
+    double *bf_coef;
     // reductions
     double *red;             // [blocks][4]
     // neighbour-list grid (bulk form): radix-sort buffers, cells, sorted sources
@@ -180,14 +195,19 @@ struct VxLaunch {
 
 // Stage launchers (each returns the first CUDA error it saw).
 cudaError_t vx_launch_step_begin(const VxLaunch &L, VxScalars *S);
+// minv / minv_t: the inverted panel system and its transpose, stride P+1
 cudaError_t vx_launch_birth(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                            VxWork &w, const vx_panel *pan, const double *minv, int rhs_chunks);
+                            VxWork &w, const vx_panel *pan, const double *minv, const double *minv_t,
+                            int rhs_chunks);
+cudaError_t vx_transpose_square(const VxLaunch &L, const double *A, double *At, long long nr);
 cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                VxWork &w, int ksplit);
 cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                 VxWork &w, int ksplit);
+// wstart/widx: per wall cell, the panels that can act on a particle in the
+// cell (CSR, ascending panel index); null: every panel is tested
 cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                           const vx_panel *pan);
+                           const vx_panel *pan, const int *wstart = nullptr, const int *widx = nullptr);
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                              VxWork &w, const vx_panel *pan);
 cudaError_t vx_launch_compact(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
@@ -215,6 +235,8 @@ vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, i
 long long vx_rs_tiles_cap(long long cap);
 int vx_fmm_max_level(long long cap);
 long long vx_fmm_cells(int lmax);         // cells of all levels 0..lmax
+constexpr int VX_BF_P = 32;          // terms of the birth far-field expansion
+constexpr int VX_BF_MAX_BLOCKS = 1024;
 constexpr int VX_FMM_P = 16;              // expansion terms (vx_fmm.cu)
 cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                    VxWork &w);

@@ -2,7 +2,7 @@
 // the element count read from device memory.
 //
 // Per 8-bit digit: (1) every tile of VX_RS_TILE elements counts its digits,
-// (2) one block scans the counts in digit-major order, (3) every tile
+// (2) one block per digit scans that digit's tile counts, (3) every tile
 // scatters its elements in their original order: the rank of an element
 // among equal digits is (elements of earlier tiles) + (earlier rounds of this
 // tile) + (earlier warps of this round) + (earlier lanes of this warp), the
@@ -33,46 +33,68 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const long long *d_n, co
     }
 }
 
-// Exclusive scan over digit-major counts [digit][tile] for tile < tiles.
-__global__ void k_rs_scan(const long long *d_n, const int *hist, long long *off, long long tiles_cap) {
-    __shared__ long long sh[1024];
-    __shared__ long long carry;
+// Exclusive scan of each digit's tile counts, one block per digit (digit-
+// local offsets in off, digit totals in dtot); the scatter adds the digit's
+// prefix over dtot.
+constexpr int RS_SCAN_T = 512;
+__global__ void __launch_bounds__(RS_SCAN_T) k_rs_scan(const long long *d_n, const int *hist, long long *off,
+                                                       long long tiles_cap, long long *dtot) {
+    __shared__ long long wsum[RS_SCAN_T / 32];
     const long long tiles = vx_ceil_div(*d_n, RS_TILE);
-    const long long total = 256 * tiles;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const long long per = vx_ceil_div(total, (long long)blockDim.x);
-    // each thread scans a contiguous run of the linearised (digit, tile) order
-    long long local = 0;
-    const long long b = threadIdx.x * per, e = min(total, b + per);
-    for (long long q = b; q < e; ++q) local += hist[(q / tiles) * tiles_cap + q % tiles];
-    sh[threadIdx.x] = local;
-    __syncthreads();
-    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-        long long v = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long d = blockIdx.x;
+    long long carry = 0;
+    for (long long t0 = 0; t0 < tiles; t0 += RS_SCAN_T) {
+        const long long t = t0 + threadIdx.x;
+        const long long c = t < tiles ? hist[d * tiles_cap + t] : 0;
+        long long inc = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) wsum[warp] = inc;
         __syncthreads();
-        sh[threadIdx.x] += v;
+        long long before = 0, total = 0;
+        for (int q = 0; q < RS_SCAN_T / 32; ++q) {
+            before += q < warp ? wsum[q] : 0;
+            total += wsum[q];
+        }
+        if (t < tiles) off[d * tiles_cap + t] = carry + before + inc - c;
+        carry += total;
         __syncthreads();
     }
-    long long run = sh[threadIdx.x] - local;
-    for (long long q = b; q < e; ++q) {
-        const long long idx = (q / tiles) * tiles_cap + q % tiles;
-        off[idx] = run;
-        run += hist[idx];
-    }
+    if (threadIdx.x == 0) dtot[d] = carry;
 }
 
 __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const long long *d_n, const unsigned *keys,
                                                            const int *vals, unsigned *okeys, int *ovals, int shift,
-                                                           const long long *off, long long tiles_cap) {
+                                                           const long long *off, long long tiles_cap,
+                                                           const long long *dtot) {
+    static_assert(RS_THREADS == 256, "one thread per digit");
     __shared__ int warp_cnt[RS_WARPS][256];
     __shared__ long long base[256];
+    __shared__ long long dpre[256];
+    __shared__ long long wtot[RS_WARPS];
     const long long n = *d_n;
     const long long tiles = vx_ceil_div(n, RS_TILE);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
+    {   // exclusive prefix of the digit totals (thread d owns digit d)
+        const long long c = dtot[threadIdx.x];
+        long long inc = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) wtot[warp] = inc;
+        __syncthreads();
+        long long before = 0;
+        for (int q = 0; q < warp; ++q) before += wtot[q];
+        dpre[threadIdx.x] = before + inc - c;
+        __syncthreads();
+    }
     for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
-        base[threadIdx.x] = off[(long long)threadIdx.x * tiles_cap + t];
+        base[threadIdx.x] = dpre[threadIdx.x] + off[(long long)threadIdx.x * tiles_cap + t];
         __syncthreads();
         for (int r = 0; r < RS_ROUNDS; ++r) {
             for (int w = 0; w < RS_WARPS; ++w) warp_cnt[w][threadIdx.x] = 0;
@@ -111,7 +133,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const long long *d_n,
 
 // Sorts keys/vals (count *d_n) by bits [0, nbits) of the key.  Buffers
 // alternate between (k0,v0) and (k1,v1); the return value tells which pair
-// holds the result (0 or 1).  hist/off hold 256 * tiles_cap entries.
+// holds the result (0 or 1).  hist holds 256 * tiles_cap entries, off
+// 256 * (tiles_cap + 1) (the digit totals follow the offsets).
 int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0, unsigned *k1, int *v1,
                   int nbits, int *hist, long long *off, long long tiles_cap) {
     const int grid = L.num_sms * 4;
@@ -120,8 +143,11 @@ int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0
         unsigned *ki = cur ? k1 : k0, *ko = cur ? k0 : k1;
         int *vi = cur ? v1 : v0, *vo = cur ? v0 : v1;
         k_rs_hist<<<grid, RS_THREADS, 0, L.stream>>>(d_n, ki, shift, hist, tiles_cap); VX_COUNT(L);
-        k_rs_scan<<<1, 1024, 0, L.stream>>>(d_n, hist, off, tiles_cap); VX_COUNT(L);
-        k_rs_scatter<<<grid, RS_THREADS, 0, L.stream>>>(d_n, ki, vi, ko, vo, shift, off, tiles_cap); VX_COUNT(L);
+        k_rs_scan<<<256, RS_SCAN_T, 0, L.stream>>>(d_n, hist, off, tiles_cap, off + 256 * tiles_cap);
+        VX_COUNT(L);
+        k_rs_scatter<<<grid, RS_THREADS, 0, L.stream>>>(d_n, ki, vi, ko, vo, shift, off, tiles_cap,
+                                                         off + 256 * tiles_cap);
+        VX_COUNT(L);
         cur ^= 1;
     }
     return cur;

@@ -4,7 +4,13 @@
 // integral I_0_I_3 (FP64 twin src/kernel.cu:1300-1322, FP32 1324-1346).
 // A panel contributes only when the particle is within 5 L of the panel's
 // birth point, so particles outside the birth-point bounding box grown by
-// 5 L_max skip the panel loop: their contribution is exactly +0.
+// 5 L_max skip the panel loop: their contribution is exactly +0.  Inside
+// that box, when panel lists are given, a particle tests only the panels of
+// its wall cell: every panel whose birth point lies within one cell (side
+// > 5 L_max) of the cell, in ascending panel order.  A panel left out is
+// farther than 5 L from the particle, so it would add nothing; the panels
+// kept are visited in the reference's order, so the sums and the first
+// r <= 0.1 L override are unchanged bit for bit.
 #include "vx_internal.cuh"
 
 template <typename T>
@@ -39,17 +45,25 @@ __device__ void vx_wall_integral(T Ra0, T Ra1, T Rb0, T Rb1, T N0, T N1, T Rj0, 
 }
 
 template <typename T>
-__global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel *pan) {
+__global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel *pan, const int *wstart,
+                       const int *widx) {
     const long long n = S->n;
     const T nu = (T)p.nu;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const double xd = v.x[i * v.ps], yd = v.y[i * v.ps];
         if (xd < p.wall_x0 || xd > p.wall_x1 || yd < p.wall_y0 || yd > p.wall_y1) continue;
+        int q0 = 0, q1 = p.P;
+        if (wstart) {
+            const int cx = min(max((int)floor((xd - p.wall_x0) / p.wall_h), 0), p.wall_nx - 1);
+            const int cy = min(max((int)floor((yd - p.wall_y0) / p.wall_h), 0), p.wall_ny - 1);
+            q0 = wstart[cy * p.wall_nx + cx];
+            q1 = wstart[cy * p.wall_nx + cx + 1];
+        }
         const T a0 = (T)xd, a1 = (T)yd, dd = (T)v.d[i];
         T I0 = (T)VX_TWO_PI * dd * dd, I30 = 0, I31 = 0;
-        for (int f = 0; f < p.P; ++f) {
-            const vx_panel &pf = pan[f];
+        for (int q = q0; q < q1; ++q) {
+            const vx_panel &pf = pan[wstart ? widx[q] : q];
             const T dL = (T)pf.length;
             T dx = a0 - (T)pf.birth[0], dy = a1 - (T)pf.birth[1];
             T r = vx_sqrt<T>(fma(dx, dx, dy * dy));
@@ -75,11 +89,12 @@ __global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel 
 }
 
 cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                           const vx_panel *pan) {
+                           const vx_panel *pan, const int *wstart, const int *widx) {
+    if (p.wall_nx <= 0 || p.wall_ny <= 0) wstart = widx = nullptr;
     if (p.prec == VX_PREC_FP32)
-        k_wall<float><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan);
+        k_wall<float><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan, wstart, widx);
     else
-        k_wall<double><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan);
+        k_wall<double><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan, wstart, widx);
     VX_COUNT(L);
     return cudaGetLastError();
 }
