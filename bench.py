@@ -328,7 +328,7 @@ def ref_cuda_build(args, x, y, g):
     src/kernel.cu, -DNO_TREE, sm_100a, built by oracle/build_ref.sh) on the
     same workload, restarted from a frame holding the same warm wake; its
     per-step device time is the Creation + Speed + Step event times it logs
-    (cumulative per step in its timings file)."""
+    (cumulative seconds per step in its timings file)."""
     import tempfile
     from vortex_b200 import profiles
     exe = os.path.join(ROOT, "oracle", "_ref", "vortex_ref")
@@ -354,7 +354,8 @@ def ref_cuda_build(args, x, y, g):
             if len(parts) >= 5:
                 rows.append((int(parts[0]), int(parts[1].split("=")[1]),
                              sum(float(q.split("=")[1]) for q in parts[2:5])))
-    per_step = [b[2] - a[2] for a, b in zip(rows[:-1], rows[1:]) if b[0] > a[0]]
+    # the reference's stop_timer returns seconds (src/unit_1.cu:604-613)
+    per_step = [1e3 * (b[2] - a[2]) for a, b in zip(rows[:-1], rows[1:]) if b[0] > a[0]]
     if not per_step:
         return {"unavailable": "reference timings file had no per-step lines"}
     ms = float(np.median(per_step[1:] if len(per_step) > 1 else per_step))
