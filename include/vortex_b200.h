@@ -90,7 +90,11 @@ typedef struct vx_conf {
                                    twice the body radius through one local
                                    expansion about the body (default 1);
                                    0 = direct sums */
-    int32_t pad2_;
+    int32_t gj_pivot;           /* panel-system inversion: 0 = the reference's
+                                   Gauss-Jordan pivot rule (a pivot below
+                                   1e-12 fails, as in the reference);
+                                   1 = partial pivoting; 2 = the reference's
+                                   rule, partial pivoting if it fails */
 } vx_conf;
 
 typedef struct vx_sim vx_sim;
@@ -171,6 +175,43 @@ vx_status vx_get_pair_counts(vx_sim *sim, double out2[2], int clear);
  * out[0] quadtree depth, [1] leaf side, [2] targets redone by the exact
  * 3-nearest search, [3] neighbour-grid cell side, [4] cells in x, [5] in y. */
 vx_status vx_get_tree_info(vx_sim *sim, double out6[6]);
+
+/* Device bytes a body with P panels will hold when its particle count
+ * reaches n_max (capacity growth included): the admission estimate of
+ * vx_server.  vx_get_device_bytes: what a handle holds now. */
+vx_status vx_estimate_bytes(const vx_conf *conf, int64_t P, int64_t n_max, int device, int64_t *bytes);
+vx_status vx_get_device_bytes(vx_sim *sim, int64_t *bytes);
+
+/* Advance `count` bodies of one device by nsteps; every step is launched on
+ * all bodies' streams before the next, so their kernels overlap.  Returns
+ * without waiting, like vx_step. */
+vx_status vx_step_many(vx_sim *const *sims, int count, int64_t nsteps);
+
+/* ---- Serving (no counterpart in the reference, which runs one body per
+ * process): a request loop with continuous batching.  Requests (one body
+ * each: conf, panels, starting vortices, step count) wait in arrival order
+ * until a slot is free and the device-byte budget holds their
+ * vx_estimate_bytes at n + P * nsteps; admitted bodies stay resident; every
+ * tick advances all resident bodies one step, launched on their own streams
+ * before any wait, and releases the finished ones.  Results do not depend
+ * on what else runs. */
+typedef struct vx_server vx_server;
+vx_status vx_server_create(int device, int64_t budget_bytes, int max_active, vx_server **out);
+vx_status vx_server_destroy(vx_server *srv);
+/* Inputs are copied; VX_ERR_BUDGET if the request alone exceeds the budget. */
+vx_status vx_server_submit(vx_server *srv, const vx_conf *conf, const vx_panel *panels, int64_t P,
+                           const double *x, const double *y, const double *g, int64_t n, int64_t nsteps,
+                           int64_t *id);
+/* Admit, step every resident body once, retire; counts after the tick. */
+vx_status vx_server_tick(vx_server *srv, int64_t *active, int64_t *queued);
+/* state: 0 queued, 1 resident, 2 done, 3 failed; forces: (dg, Fx, Fy, M)
+ * per completed step, at most cap_steps steps copied. */
+vx_status vx_server_result(vx_server *srv, int64_t id, int *state, int64_t *steps_done, double *forces,
+                           int64_t cap_steps, int64_t *n_final);
+/* out[0] finished, [1]/[2] p50/p99 body-step device ms, [3]/[4] p50/p99
+ * submit-to-finish s, [5] mean resident bodies per tick, [6] body steps,
+ * [7] particle steps, [8] bytes reserved now, [9] ticks. */
+vx_status vx_server_stats(vx_server *srv, double out10[10]);
 
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);

@@ -279,3 +279,31 @@ def test_long_run_statistics_track_oracle():
     assert abs(np.abs(gg).sum() - np.abs(og).sum()) < 0.10 * np.abs(og).sum()
     assert abs(np.mean(fg) - np.mean(fo)) < 0.10 * abs(np.mean(fo))
     sim.close()
+
+
+def test_panel_system_pivot_modes():
+    """The reference's Gauss-Jordan picks the pivot of column k+1 before
+    column k is eliminated, so a well-conditioned system (a thin rounded
+    plate, condition number ~2e3) can meet a pivot below 1e-12 and fail, as
+    the reference does (gj_pivot 0).  gj_pivot 2 retries with partial
+    pivoting and gj_pivot 1 uses it outright: both invert the same L."""
+    import ctypes as C
+    from vortex_b200 import profiles as PR
+    pan = PR.rotate(PR.rounded_plate(655), -30.0)
+    P = len(pan)
+    L = np.zeros((P + 1, P + 1))
+    M = np.zeros((P + 1, P + 1))
+    rc = O.lib().vxo_panel_matrix(C.c_void_p(pan.ctypes.data), C.c_int64(P), C.c_void_p(L.ctypes.data),
+                                  C.c_void_p(M.ctypes.data))
+    assert rc != 0                              # the oracle's reference rule fails too
+    ck = conf_kwargs(P, ve_size=float(pan["length"].mean()))
+    with pytest.raises(N.VxError, match="singular"):
+        N.Sim(N.default_conf(**dict(ck, gj_pivot=0)), pan)
+    mats = []
+    for mode in (1, 2):
+        s = N.Sim(N.default_conf(**dict(ck, gj_pivot=mode)), pan)
+        mats.append(s.matrix())
+        s.close()
+    for Minv in mats:
+        assert np.abs(Minv @ L - np.eye(P + 1)).max() < 1e-9
+    assert np.array_equal(mats[0], mats[1])

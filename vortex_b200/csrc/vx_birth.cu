@@ -123,13 +123,27 @@ __device__ void vx_block_swap_rows(double *A, long long S, long long r1, long lo
 
 // Pivot step k of src/unit_1.cu:160-227: singularity checks, choice and swap
 // of the pivot row for column k+1, then the multipliers c[i] = A[i][k]/A[k][k].
-__global__ void k_gj_pivot(double *A, double *Inv, long long S, long long k, double *c, int *flag) {
+// The reference chooses the pivot of column k+1 before column k is
+// eliminated, so a well-conditioned system can still meet a pivot below
+// 1e-12 there.  robust != 0: ordinary partial pivoting instead (the pivot of
+// column k chosen among rows k.. after the previous eliminations).
+__global__ void k_gj_pivot(double *A, double *Inv, long long S, long long k, double *c, int *flag, int robust) {
     __shared__ double s_val[1024];
     __shared__ long long s_idx[1024];
     if (*flag) return;
     const double DELT = 1e-12;
     double best;
     long long line;
+    if (robust) {
+        vx_block_argmax(A, S, k, k, s_val, s_idx, best, line);
+        if (best < DELT) { if (threadIdx.x == 0) *flag = 1; return; }
+        vx_block_swap_rows(A, S, k, line);
+        vx_block_swap_rows(Inv, S, k, line);
+        __syncthreads();
+        const double piv = A[k * S + k];
+        for (long long i = threadIdx.x; i < S; i += blockDim.x) c[i] = A[i * S + k] / piv;
+        return;
+    }
     if (k == 0 && fabs(A[0]) < DELT) {
         vx_block_argmax(A, S, 1, 0, s_val, s_idx, best, line);
         if (best > fabs(A[0])) {
@@ -192,7 +206,7 @@ __global__ void k_gj_scale(const double *A, double *Inv, long long S, const int 
 // d_work must hold 2 (P+1)^2 + (P+1) doubles.  *d_flag is set when a pivot
 // falls below 1e-12 (the reference returns NULL then).
 cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, double *d_minv,
-                            double *d_work, int *d_flag, double *d_L_out) {
+                            double *d_work, int *d_flag, double *d_L_out, int robust) {
     const long long S = P + 1;
     double *A = d_work;
     double *c = d_work + S * S;
@@ -202,7 +216,7 @@ cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, dou
     if (d_L_out) cudaMemcpyAsync(d_L_out, A, sizeof(double) * S * S, cudaMemcpyDeviceToDevice, L.stream);
     k_identity<<<grid, 256, 0, L.stream>>>(d_minv, S); VX_COUNT(L);
     for (long long k = 0; k < S - 1; ++k) {
-        k_gj_pivot<<<1, 1024, 0, L.stream>>>(A, d_minv, S, k, c, d_flag); VX_COUNT(L);
+        k_gj_pivot<<<1, 1024, 0, L.stream>>>(A, d_minv, S, k, c, d_flag, robust); VX_COUNT(L);
         k_gj_elim<<<grid, 256, 0, L.stream>>>(A, d_minv, S, k, c, d_flag); VX_COUNT(L);
     }
     k_gj_last_pivot<<<1, 1024, 0, L.stream>>>(A, S, c, d_flag); VX_COUNT(L);

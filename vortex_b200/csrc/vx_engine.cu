@@ -63,6 +63,7 @@ struct vx_sim {
     double *d_minv = nullptr;
     double *d_minvT = nullptr;   // transposed copy read by the birth solve
     int *d_wstart = nullptr, *d_widx = nullptr;   // wall panel lists per wall cell
+    long long wall_bytes = 0;
     VxScalars *d_S = nullptr;
     VxScalars *h_S = nullptr;     // pinned mirror
     long long cap = 0;
@@ -185,12 +186,16 @@ __global__ void k_fill_tail(double *x, double *y, double *g, long long from, lon
     }
 }
 
+// Device allocation of `count` elements, counted (rounded to the 256-byte
+// allocation granularity) into *bytes; with allocs == nullptr only counted.
 template <typename T>
-static vx_status dalloc(std::vector<void *> &allocs, T **p, long long count) {
+static vx_status dalloc(std::vector<void *> *allocs, long long *bytes, T **p, long long count) {
     void *q = nullptr;
     if (count < 1) count = 1;
+    *bytes += ((long long)sizeof(T) * count + 255) / 256 * 256;
+    if (!allocs) { *p = nullptr; return VX_OK; }
     CU(cudaMalloc(&q, sizeof(T) * (size_t)count));
-    allocs.push_back(q);
+    allocs->push_back(q);
     *p = (T *)q;
     return VX_OK;
 }
@@ -201,13 +206,14 @@ void vx_work_free(VxWork &w, std::vector<void *> &allocs) {
     memset(&w, 0, sizeof(w));
 }
 
-// Scratch for a particle capacity `cap` and a panel count padded to P32.
-vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms) {
-    vx_work_free(w, allocs);
+// Scratch for a particle capacity `cap` and a panel count padded to P32
+// (allocs == nullptr: only count the bytes into w.bytes).
+static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long long cap, int P32, int num_sms) {
     w.cap = cap;
+    w.bytes = 0;
     const long long nch = cap / VX_CHUNK + 2;
     vx_status st;
-#define A(ptr, n) if ((st = dalloc(allocs, &(ptr), (n))) != VX_OK) return st
+#define A(ptr, n) if ((st = dalloc(allocs, &w.bytes, &(ptr), (n))) != VX_OK) return st
     A(w.cmp_cnt, nch); A(w.cmp_off, nch);
     A(w.hole_pos, cap); A(w.hole_src, cap); A(w.tail_src, cap);
     A(w.hx, cap); A(w.hy, cap); A(w.hg, cap); A(w.tx, cap); A(w.ty, cap);
@@ -246,6 +252,18 @@ vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, i
     A(w.fmm_L, 2LL * VX_FMM_P * vx_fmm_cells(w.fmm_lmax));
 #undef A
     return VX_OK;
+}
+
+vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms) {
+    vx_work_free(w, allocs);
+    return work_alloc_impl(w, &allocs, cap, P32, num_sms);
+}
+
+long long vx_work_bytes(long long cap, int P32, int num_sms) {
+    VxWork w;
+    memset(&w, 0, sizeof(w));
+    work_alloc_impl(w, nullptr, cap, P32, num_sms);
+    return w.bytes;
 }
 
 static void free_work(vx_sim *s) { vx_work_free(s->w, s->work_allocs); }
@@ -347,6 +365,7 @@ static vx_status build_wall_lists(vx_sim *s, const vx_panel *pan, int P) {
     }
     start[cells.size()] = (int)idx.size();
     if (idx.empty()) idx.push_back(0);
+    s->wall_bytes = (long long)sizeof(int) * (long long)(start.size() + idx.size());
     if (cudaMalloc(&s->d_wstart, sizeof(int) * start.size()) != cudaSuccess) return VX_ERR_NOMEM;
     if (cudaMalloc(&s->d_widx, sizeof(int) * idx.size()) != cudaSuccess) return VX_ERR_NOMEM;
     if (cudaMemcpy(s->d_wstart, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -412,12 +431,18 @@ extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t
     if (cudaMalloc(&work, sizeof(double) * (2 * S1 * S1 + S1)) != cudaSuccess) return fail(VX_ERR_NOMEM);
     if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) { cudaFree(work); return fail(VX_ERR_NOMEM); }
     VxLaunch L = launch_of(s);
-    cudaError_t e = vx_build_matrix(L, s->d_pan, (int)P, s->d_minv, work, flag, nullptr);
+    cudaError_t e = vx_build_matrix(L, s->d_pan, (int)P, s->d_minv, work, flag, nullptr, conf->gj_pivot == 1);
+    int hflag = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess && hflag && conf->gj_pivot == 2) {   // the reference's rule failed: pivot properly
+        e = vx_build_matrix(L, s->d_pan, (int)P, s->d_minv, work, flag, nullptr, 1);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    }
     if (e == cudaSuccess && cudaMalloc(&s->d_minvT, sizeof(double) * S1 * S1) != cudaSuccess)
         e = cudaErrorMemoryAllocation;
     if (e == cudaSuccess) e = vx_transpose_square(L, s->d_minv, s->d_minvT, S1);
-    int hflag = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     cudaFree(work);
     cudaFree(flag);
@@ -799,6 +824,53 @@ extern "C" vx_status vx_get_timing(vx_sim *s, double out8[8]) {
 extern "C" vx_status vx_get_launch_count(vx_sim *s, int64_t *count) {
     if (!s || !count) return VX_ERR_ARG;
     *count = s->launches;
+    return VX_OK;
+}
+
+// Device bytes held by fixed-size parts of a body: panels, the inverted
+// system and its transpose, scalars (the Gauss-Jordan work area of vx_create
+// is transient and counted by the estimate only).
+static long long fixed_bytes(long long P) {
+    const long long P32 = vx_round32(P), S1 = P + 1;
+    return P32 * (long long)sizeof(vx_panel) + 2 * S1 * S1 * 8 + (long long)sizeof(VxScalars) + 4096;
+}
+
+static long long cap_after_growth(long long need, long long inc_step) {
+    const long long inc = std::max<long long>(inc_step, 8192);
+    return vx_ceil_div(std::max<long long>((long long)(need * 1.25), need + inc), 8192) * 8192;
+}
+
+extern "C" vx_status vx_estimate_bytes(const vx_conf *c, int64_t P, int64_t n_max, int device, int64_t *out) {
+    if (!c || !out || P < 2 || n_max < 0) return VX_ERR_ARG;
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) sms = 148;
+    const long long need = vx_round32(n_max + P) + 64;
+    const long long cap = cap_after_growth(need, c->inc_step);
+    const long long S1 = P + 1;
+    const long long transient = (2 * S1 * S1 + S1) * 8;     // Gauss-Jordan work area at creation
+    const long long wall = 4LL * (9 * P + 4096);              // wall panel lists (bound)
+    *out = 6 * 8 * cap + vx_work_bytes(cap, (int)vx_round32(P), sms) + fixed_bytes(P) + transient + wall;
+    return VX_OK;
+}
+
+extern "C" vx_status vx_get_device_bytes(vx_sim *s, int64_t *out) {
+    if (!s || !out) return VX_ERR_ARG;
+    *out = 6 * 8 * s->cap + s->w.bytes + fixed_bytes(s->P) + s->wall_bytes;
+    return VX_OK;
+}
+
+// Advance several bodies (same device) by nsteps: each step is launched on
+// every body's own stream before the next step, so the bodies' kernels
+// overlap on the device.  Asynchronous like vx_step.
+extern "C" vx_status vx_step_many(vx_sim *const *sims, int count, int64_t nsteps) {
+    if ((!sims && count > 0) || count < 0 || nsteps < 0) return VX_ERR_ARG;
+    for (int i = 0; i < count; ++i)
+        if (!sims[i]) return VX_ERR_ARG;
+    for (int64_t k = 0; k < nsteps; ++k)
+        for (int i = 0; i < count; ++i) {
+            vx_status st = vx_step(sims[i], 1);
+            if (st != VX_OK) return st;
+        }
     return VX_OK;
 }
 

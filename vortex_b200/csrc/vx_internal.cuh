@@ -101,6 +101,7 @@ enum {
 // Device scratch of one body.  Sizes are in elements.
 struct VxWork {
     long long cap;           // particle capacity the arrays below were sized for
+    long long bytes;         // device bytes the arrays below take
     // compaction
     int *cmp_cnt;
     long long *cmp_off;
@@ -221,7 +222,8 @@ cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &
 // Panel system on the device: L (P+1)^2 then Gauss-Jordan inverse.
 // d_L_out (nullable) receives a copy of the influence matrix before elimination.
 cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, double *d_minv,
-                            double *d_work, int *d_flag, double *d_L_out);
+                            double *d_work, int *d_flag, double *d_L_out,
+                            int robust = 0);
 cudaError_t vx_launch_birth_ld(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                VxWork &w, const vx_panel *pan, const double *minv, long long ld,
                                int rhs_chunks);
@@ -232,6 +234,7 @@ void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams 
 void vx_set_error(const char *fmt, ...);
 #include <vector>
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms);
+long long vx_work_bytes(long long cap, int P32, int num_sms);
 long long vx_rs_tiles_cap(long long cap);
 int vx_fmm_max_level(long long cap);
 long long vx_fmm_cells(int lmax);         // cells of all levels 0..lmax

@@ -38,7 +38,7 @@ extern "C" vx_status vx_conf_read(const char *path, vx_conf *c) {
         D(x_max) D(x_min) D(y_max) D(y_min) D(ve_size) U(n_col)
         D(h_col_x) D(h_col_y) D(rc_x) D(rc_y) D(r_col_diff_sign) D(r_col_same_sign)
         B(matrix_load) D(max_ve_g) D(rel_t) B(steady_flow) U(tree_depth) D(theta) B(no_log_buf)
-        D(drop_eps) D(diff_cutoff) B(fmm)
+        D(drop_eps) D(diff_cutoff) B(fmm) B(gj_pivot)
         else if (key_is(buf, "precision")) {
             char v[32] = {0};
             if (sscanf(buf, "%*s %31s", v) == 1)

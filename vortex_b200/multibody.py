@@ -1,0 +1,146 @@
+"""Many bodies on one GPU: the batched run and the served run.
+
+Batched: a seeded population of bodies (workloads.body_spec) advanced
+together with vx_step_many: every step is launched on all bodies' streams
+before the next, so their kernels overlap on the device.  The batched step is
+timed on the device: a start event on a main stream that every body stream
+waits for, and an end event after the main stream waited for every body.
+
+Served: requests drawn from the same population arrive as a Poisson process;
+each asks for a number of steps; the vx_server loop admits them by slot and
+device-byte budget, keeps them resident, steps all resident bodies every
+tick and releases finished ones (continuous batching).
+
+    python -m vortex_b200.multibody batch --bodies 256 --steps 20
+    python -m vortex_b200.multibody serve --requests 32
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+from . import native as N
+from . import workloads as wl
+
+
+def _event_pair():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7,
+              precision: int = N.PREC_FP32, device: int = 0) -> dict:
+    import torch
+    torch.cuda.set_device(device)
+    specs = [wl.body_spec(seed, i) for i in range(bodies)]
+    sims = []
+    t0 = time.perf_counter()
+    for sp in specs:
+        conf, pan, x, y, g = wl.make_body(sp, precision)
+        s = N.Sim(conf, pan, device=device)
+        s.set_particles(x, y, g)
+        sims.append(s)
+    setup_s = time.perf_counter() - t0
+    N.step_many(sims, warmup)
+    for s in sims:
+        s.sync()
+    streams = [torch.cuda.ExternalStream(s.stream(), device=f"cuda:{device}") for s in sims]
+    main = torch.cuda.current_stream(device)
+    counts0 = np.array([s.count() for s in sims], dtype=np.float64)
+    ms, inter = [], 0.0
+    launches0 = sum(s.launches() for s in sims)
+    for _ in range(steps):
+        a, b = _event_pair()
+        a.record(main)
+        for st in streams:
+            st.wait_event(a)
+        N.step_many(sims, 1)
+        for st in streams:
+            e = torch.cuda.Event()
+            e.record(st)
+            main.wait_event(e)
+        b.record(main)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    counts1 = np.array([s.count() for s in sims], dtype=np.float64)
+    launches = sum(s.launches() for s in sims) - launches0
+    nmean = 0.5 * (counts0 + counts1)
+    inter = float(np.sum(nmean * nmean))          # direct-sum equivalent pairs per batched step
+    total_s = sum(ms) * 1e-3
+    out = {"bodies": bodies, "steps": steps, "warmup": warmup, "seed": seed,
+           "precision": "fp32" if precision == N.PREC_FP32 else "fp64",
+           "particles_start": int(counts0.sum()), "particles_end": int(counts1.sum()),
+           "panels_total": int(sum(sp["panels"] for sp in specs)),
+           "batched_steps_per_s": steps / total_s, "body_steps_per_s": bodies * steps / total_s,
+           "ms_per_batched_step": float(np.mean(ms)), "ms_p50": float(np.percentile(ms, 50)),
+           "ms_p99": float(np.percentile(ms, 99)),
+           "particle_steps_per_s": float(nmean.sum()) * steps / total_s,
+           "interactions_per_s_effective": inter * steps / total_s,
+           "gpu_launches": int(launches), "setup_s": setup_s}
+    for s in sims:
+        s.close()
+    return out
+
+
+def run_serve(requests: int = 32, rate: float = 50.0, budget_gb: float = 160.0, max_active: int = 256,
+              seed: int = 11, precision: int = N.PREC_FP32, steps_lo: int = 50, steps_hi: int = 1000,
+              device: int = 0) -> dict:
+    """Poisson arrivals (rate per second) of `requests` bodies of the seeded
+    population, each asking for U[steps_lo, steps_hi] steps."""
+    u = wl.uniforms(seed, 2 * requests)
+    gaps = -np.log1p(-u[:requests]) / rate
+    arrive = np.cumsum(gaps)
+    nsteps = (steps_lo + np.floor(u[requests:] * (steps_hi - steps_lo + 1))).astype(int)
+    specs = [wl.body_spec(seed, i) for i in range(requests)]
+    bodies = [wl.make_body(sp, precision) for sp in specs]
+    srv = N.Server(int(budget_gb * 1e9), max_active=max_active, device=device)
+    ids = [None] * requests
+    t0 = time.perf_counter()
+    nxt = 0
+    finished = 0
+    while finished < requests:
+        now = time.perf_counter() - t0
+        while nxt < requests and arrive[nxt] <= now:
+            conf, pan, x, y, g = bodies[nxt]
+            ids[nxt] = srv.submit(conf, pan, x, y, g, int(nsteps[nxt]))
+            nxt += 1
+        resident, queued = srv.tick()
+        finished = sum(1 for i in ids if i is not None and srv.result(i)["state"] in ("done", "failed"))
+        if resident == 0 and queued == 0 and nxt < requests:
+            time.sleep(max(0.0, arrive[nxt] - (time.perf_counter() - t0)))
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    res = [srv.result(i) for i in ids]
+    srv.close()
+    return {"requests": requests, "rate_per_s": rate, "budget_gb": budget_gb, "max_active": max_active,
+            "seed": seed, "precision": "fp32" if precision == N.PREC_FP32 else "fp64",
+            "steps_requested": int(nsteps.sum()), "failed": sum(r["state"] == "failed" for r in res),
+            "wall_s": wall, "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"],
+            "ttc_s_p50": st["ttc_s_p50"], "ttc_s_p99": st["ttc_s_p99"], "mean_resident": st["mean_resident"],
+            "body_steps": st["body_steps"], "body_steps_per_s": st["body_steps"] / wall,
+            "particle_steps_per_s": st["particle_steps"] / wall, "ticks": st["ticks"]}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("mode", choices=["batch", "serve"])
+    ap.add_argument("--bodies", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--requests", type=int, default=32)
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    a = ap.parse_args()
+    prec = N.PREC_FP32 if a.precision == "fp32" else N.PREC_FP64
+    if a.mode == "batch":
+        print(json.dumps(run_batch(a.bodies, a.steps, a.warmup, precision=prec)))
+    else:
+        print(json.dumps(run_serve(a.requests, a.rate, precision=prec)))
+
+
+if __name__ == "__main__":
+    main()

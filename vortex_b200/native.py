@@ -41,7 +41,7 @@ class Conf(C.Structure):
         ("precision", C.c_int32), ("birth_offset_mode", C.c_int32),
         ("drop_eps", C.c_double), ("diff_cutoff", C.c_double),
         ("n_probes_grid", C.c_int32), ("pad1_", C.c_int32), ("probe_box", C.c_double * 4),
-        ("fmm", C.c_int32), ("pad2_", C.c_int32),
+        ("fmm", C.c_int32), ("gj_pivot", C.c_int32),
     ]
 
 
@@ -253,3 +253,76 @@ class Sim:
 
     def stream(self) -> int:
         return lib().vx_get_stream(self.h) or 0
+
+    def device_bytes(self) -> int:
+        b = C.c_int64(0)
+        _check(lib().vx_get_device_bytes(self.h, C.byref(b)), "vx_get_device_bytes")
+        return b.value
+
+
+def estimate_bytes(conf: Conf, P: int, n_max: int, device: int = 0) -> int:
+    """Device bytes a body with P panels holds once it reaches n_max vortices."""
+    b = C.c_int64(0)
+    _check(lib().vx_estimate_bytes(C.byref(conf), C.c_int64(P), C.c_int64(n_max), C.c_int(device),
+                                   C.byref(b)), "vx_estimate_bytes")
+    return b.value
+
+
+def step_many(sims, nsteps: int = 1):
+    """Advance several bodies together (their kernels overlap); asynchronous."""
+    arr = (C.c_void_p * len(sims))(*[s.h.value for s in sims])
+    _check(lib().vx_step_many(arr, C.c_int(len(sims)), C.c_int64(nsteps)), "vx_step_many")
+
+
+class Server:
+    """Continuous-batching request loop over resident bodies (vx_server)."""
+
+    STATES = ("queued", "resident", "done", "failed")
+
+    def __init__(self, budget_bytes: int, max_active: int = 64, device: int = 0):
+        self.h = C.c_void_p()
+        _check(lib().vx_server_create(C.c_int(device), C.c_int64(int(budget_bytes)), C.c_int(max_active),
+                                      C.byref(self.h)), "vx_server_create")
+
+    def close(self):
+        if self.h:
+            lib().vx_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, conf: Conf, panels, x, y, g, nsteps: int) -> int:
+        pan = np.ascontiguousarray(panels, dtype=PANEL_DTYPE)
+        x, y, g = _f64(x), _f64(y), _f64(g)
+        rid = C.c_int64(0)
+        _check(lib().vx_server_submit(self.h, C.byref(conf), _p(pan), C.c_int64(len(pan)), _p(x), _p(y), _p(g),
+                                      C.c_int64(len(x)), C.c_int64(nsteps), C.byref(rid)), "vx_server_submit")
+        return rid.value
+
+    def tick(self):
+        """One scheduling round; returns (resident, queued) after it."""
+        a, q = C.c_int64(0), C.c_int64(0)
+        _check(lib().vx_server_tick(self.h, C.byref(a), C.byref(q)), "vx_server_tick")
+        return a.value, q.value
+
+    def result(self, rid: int, cap_steps: int = 0):
+        st, done, nf = C.c_int(0), C.c_int64(0), C.c_int64(0)
+        _check(lib().vx_server_result(self.h, C.c_int64(rid), C.byref(st), C.byref(done), None, C.c_int64(0),
+                                      C.byref(nf)), "vx_server_result")
+        k = min(cap_steps, done.value) if cap_steps else done.value
+        f = np.zeros((max(k, 1), 4))
+        if k:
+            _check(lib().vx_server_result(self.h, C.c_int64(rid), C.byref(st), C.byref(done), _p(f),
+                                          C.c_int64(k), C.byref(nf)), "vx_server_result")
+        return {"state": self.STATES[st.value], "steps": done.value, "forces": f[:k], "n_final": nf.value}
+
+    def stats(self) -> dict:
+        o = np.zeros(10)
+        _check(lib().vx_server_stats(self.h, _p(o)), "vx_server_stats")
+        return {"finished": int(o[0]), "step_ms_p50": o[1], "step_ms_p99": o[2], "ttc_s_p50": o[3],
+                "ttc_s_p99": o[4], "mean_resident": o[5], "body_steps": int(o[6]), "particle_steps": o[7],
+                "bytes_reserved": int(o[8]), "ticks": int(o[9])}

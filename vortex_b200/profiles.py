@@ -68,26 +68,35 @@ def ellipse(P: int, a: float = 0.5, b: float = 0.25) -> np.ndarray:
 
 
 def rounded_plate(P: int, chord: float = 1.0, thickness: float = 0.02,
-                  n_end: int = 20) -> np.ndarray:
+                  n_end: int | None = None) -> np.ndarray:
     """Flat plate with semicircular ends (the shape of
-    profiles/Profile_file_plas_2576.txt): n_end panels per end, the rest split
-    evenly between the two flat sides.  Clockwise from the leading edge."""
+    profiles/Profile_file_plas_2576.txt): n_end panels per quarter of each
+    end circle (four quarters in all), the rest split between the two flat
+    sides (the upper side takes the odd one).  By default n_end makes the
+    end panels as long as the flat ones, as in the shipped plate (P = 2576,
+    chord 1, thickness 0.02: 20 per quarter, 1248 per side, every panel
+    pi * 0.01 / 40 long); strongly unequal panel lengths make the panel
+    system singular.  Clockwise from the leading edge."""
     r = 0.5 * thickness
-    n_flat = (P - 2 * n_end) // 2
-    if n_flat < 1 or 2 * n_end + 2 * n_flat != P:
-        raise ValueError("P must be 2*n_end + an even number of flat panels")
+    if n_end is None:
+        ell = (2.0 * (chord - 2.0 * r) + 2.0 * math.pi * r) / P
+        n_end = max(1, int(round(0.5 * math.pi * r / ell)))
+    n_rest = P - 4 * n_end
+    n_top, n_bot = (n_rest + 1) // 2, n_rest // 2
+    if n_bot < 1:
+        raise ValueError("P too small for the end panels")
     xl, xr = -0.5 * chord + r, 0.5 * chord - r
     pts = []
     for k in range(n_end):                      # leading edge, pi -> pi/2
         a = math.pi - 0.5 * math.pi * k / n_end
         pts.append((xl + r * math.cos(a), r * math.sin(a)))
-    for k in range(n_flat):                     # upper side, left -> right
-        pts.append((xl + (xr - xl) * k / n_flat, r))
+    for k in range(n_top):                      # upper side, left -> right
+        pts.append((xl + (xr - xl) * k / n_top, r))
     for k in range(2 * n_end):                  # trailing edge, pi/2 -> -pi/2
         a = 0.5 * math.pi - math.pi * k / (2 * n_end)
         pts.append((xr + r * math.cos(a), r * math.sin(a)))
-    for k in range(n_flat):                     # lower side, right -> left
-        pts.append((xr - (xr - xl) * k / n_flat, -r))
+    for k in range(n_bot):                      # lower side, right -> left
+        pts.append((xr - (xr - xl) * k / n_bot, -r))
     for k in range(n_end):                      # back to the leading edge
         a = -0.5 * math.pi - 0.5 * math.pi * k / n_end
         pts.append((xl + r * math.cos(a), r * math.sin(a)))

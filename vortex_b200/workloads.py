@@ -60,3 +60,93 @@ def warm_wake(n: int, seed: int = 1234):
         omega += sign * 2.0 / (math.pi * 0.04) * np.exp(-((x - xc) ** 2 + (y - yc) ** 2) / 0.04)
     g = omega * (8.0 / n)
     return x, y, g
+
+
+# ---------------------------------------------------------------------------
+# Seeded multi-body workloads (batched and served runs).
+#
+# Random numbers come from SplitMix64 (S. Vigna's published generator: state
+# advanced by the golden-ratio increment 0x9E3779B97F4A7C15, output mixed by
+# two xor-shift-multiply rounds), restated here.  Because the state of draw k
+# is seed + (k + 1) * increment, a whole stream is evaluated at once with
+# numpy's wrapping uint64 arithmetic.
+_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, count: int, offset: int = 0) -> np.ndarray:
+    """Draws offset .. offset+count-1 of the SplitMix64 stream of `seed`."""
+    k = np.arange(offset + 1, offset + count + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + k * _GAMMA
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+    return z ^ (z >> np.uint64(31))
+
+
+def uniforms(seed: int, count: int, offset: int = 0) -> np.ndarray:
+    """U[0, 1) doubles from the top 53 bits of each draw."""
+    return (splitmix64(seed, count, offset) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def normals(seed: int, count: int, offset: int = 0) -> np.ndarray:
+    """N(0, 1) by the Box-Muller transform of consecutive uniform pairs."""
+    m = (count + 1) // 2
+    u = uniforms(seed, 2 * m, offset)
+    r = np.sqrt(-2.0 * np.log1p(-u[0::2]))
+    t = 2.0 * math.pi * u[1::2]
+    return np.concatenate([r * np.cos(t), r * np.sin(t)])[:count]
+
+
+def _log_uniform(u: float, lo: float, hi: float) -> float:
+    return math.exp(math.log(lo) + u * (math.log(hi) - math.log(lo)))
+
+
+def body_spec(seed: int, index: int) -> dict:
+    """Parameters of body `index` of the seeded population: an ellipse
+    (a = 0.5, b ~ U[0.05, 0.5]) or a plate (chord 1, thickness 0.02, rounded
+    ends, angle ~ U[0, 45] degrees), panels log-uniform in [200, 3320],
+    Re log-uniform in [500, 2e4] (nu = 1/Re at U = 1 and unit length),
+    dt = 0.005 * 200 / panels, a warm cloud of log-uniform [1e3, 5e5]
+    vortices."""
+    u = uniforms(seed ^ 0x5EED, 8, offset=8 * index)
+    kind = "ellipse" if u[0] < 0.5 else "plate"
+    P = int(round(_log_uniform(u[1], 200, 3320)))
+    return {"index": index, "kind": kind, "panels": P,
+            "b": 0.05 + 0.45 * u[2], "angle": 45.0 * u[3],
+            "re": _log_uniform(u[4], 500.0, 2e4), "n0": int(round(_log_uniform(u[5], 1e3, 5e5))),
+            "dt": 0.005 * 200.0 / P, "cloud_seed": int(splitmix64(seed, 1, offset=index)[0])}
+
+
+def make_body(spec: dict, precision: int):
+    """(conf, panels, x, y, G) of a body_spec: Gaussian cloud in the 4 x 2 wake
+    box [0.55, 4.55] x [-1, 1] (centre (2.55, 0), sigmas 1 and 0.5, folded
+    back into the box), G ~ N(0, 1e-3); eps = mean panel length, birth half
+    a panel off the wall, same-sign collapse within 0.3 eps, |G| < 1e-8
+    dropped; the panel system is inverted with the reference's pivot rule,
+    or with partial pivoting where that rule meets a tiny pivot (thin
+    bodies)."""
+    P = spec["panels"]
+    if spec["kind"] == "ellipse":
+        pan = profiles.ellipse(P, 0.5, spec["b"])
+    else:
+        pan = profiles.rotate(profiles.rounded_plate(P, 1.0, 0.02), -spec["angle"])
+    eps = float(np.mean(pan["length"]))
+    n = spec["n0"]
+    z = normals(spec["cloud_seed"], 3 * n)
+
+    def fold(v, lo, hi):
+        w = hi - lo
+        t = np.mod(v - lo, 2 * w)
+        return lo + np.where(t > w, 2 * w - t, t)
+
+    x = fold(2.55 + 1.0 * z[:n], 0.55, 4.55)
+    y = fold(0.5 * z[n:2 * n], -1.0, 1.0)
+    g = 1e-3 * z[2 * n:]
+    conf = N.default_conf(steps=1000, dt=spec["dt"], viscosity=1.0 / spec["re"], rho=1.0, v_inf_x=1.0,
+                          v_inf_y=0.0, x_min=-2.0, x_max=10.0, y_min=-10.0, y_max=10.0, ve_size=eps,
+                          n_of_points=20, n_col=2, r_col_diff_sign=0.0, r_col_same_sign=0.3, max_ve_g=1e30,
+                          v_inf_incr_steps=0, drop_eps=1e-8, birth_offset_mode=N.BIRTH_HALF_PANEL,
+                          precision=precision, inc_step=8192, gj_pivot=2)
+    return conf, pan, x, y, g
