@@ -250,6 +250,14 @@ def run_ours(args, rank, world, device):
     line["cpu_baseline"] = cpu_baseline(args, x0, y0, g0, pan)
     if args.ref_cuda_steps > 0 and world == 1:
         line["reference_cuda_build"] = ref_cuda_build(args, x0, y0, g0)
+    if args.multibody:
+        from vortex_b200 import multibody as MB
+        batched = MB.run_batch(bodies=args.batch_bodies, steps=args.batch_steps, warmup=3, device=device)
+        sub32 = MB.run_batch(bodies=16, steps=2, warmup=1, device=device)
+        sub64 = MB.run_batch(bodies=16, steps=2, warmup=1, precision=Nt.PREC_FP64, device=device)
+        batched["fp32_vs_fp64_first16_bodies"] = sub32["body_steps_per_s"] / sub64["body_steps_per_s"]
+        line["batched"] = batched
+        line["served"] = MB.run_serve(requests=args.serve_requests, device=device)
     return line
 
 
@@ -405,6 +413,11 @@ def main():
     ap.add_argument("--ref-cuda-steps", type=int, default=0,
                     help="also time the reference's own CUDA build for this many steps (0: off)")
     ap.add_argument("--ref-cuda-timeout", type=float, default=900.0)
+    ap.add_argument("--multibody", action="store_true",
+                    help="also run the seeded multi-body population batched and served")
+    ap.add_argument("--batch-bodies", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--serve-requests", type=int, default=32)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
         float4 me = valid ? srt[t] : make_float4(0.f, 0.f, 0.f, 1.f);
         // coordinates relative to the centre of the item's first cell
         const long long ocol = (long long)(skey[item.y] % unx);
-        if (valid) me.x += (float)((double)((long long)(skey[t] % unx) - ocol) * hd);
+        if (valid) me.x += (float)((int)(skey[t] % unx) - (int)ocol) * h;   // as for the sources below
         const float R = cut * me.w;
         const bool is_wide = valid && R > (float)CG_KCAP * h;
         if (is_wide) wide[atomicAdd(&S->cnwide, 1)] = (int)t;
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
                 float x = 0.f, y = 0.f, gq = 0.f;
                 if (jt + lane < j1) {
                     const float4 q = srt[jt + lane];
-                    x = q.x + (float)((double)((long long)(skey[jt + lane] % unx) - ocol) * hd);
+                    x = q.x + (float)((int)(skey[jt + lane] % unx) - (int)ocol) * h;
                     y = q.y + oy;
                     gq = q.z;
                 }
@@ -427,10 +427,10 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
                     S1 = f2_add(S1, GE);
                 }
                 __syncwarp();
-                float a, b;
-                f2_unpack(S2X, a, b); I2x -= (double)a + (double)b;
-                f2_unpack(S2Y, a, b); I2y -= (double)a + (double)b;
-                f2_unpack(S1, a, b); I1 += (double)a + (double)b;
+                float a, b;   // the two halves are added in FP32, then carried in FP64
+                f2_unpack(S2X, a, b); I2x -= (double)(a + b);
+                f2_unpack(S2Y, a, b); I2y -= (double)(a + b);
+                f2_unpack(S1, a, b); I1 += (double)(a + b);
             }
         }
         pairs += (unsigned long long)scanned * (unsigned long long)nact;

@@ -311,14 +311,22 @@ __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, const int *
     }
 }
 
-// M2L at level l (2 <= l <= L) plus L2L from level l-1: one thread per
-// (cell, coefficient).  Locals are stored per level.  The Hankel entries
-// H_j = j! t^-(j+1) of the 40 integer offsets t of an interaction list are
-// tabulated per block in shared memory.
-__global__ void __launch_bounds__(128) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
-                                                     cplx *Loc, int l) {
+// M2L at level l (2 <= l <= L) plus L2L from level l-1.  A block takes a
+// 4 x 4 tile of target cells (two parents wide), one thread per (cell,
+// coefficient); the interaction lists of the tile draw on the 8 x 8 source
+// cells around it (children of the parents' neighbours), whose multipoles
+// are staged once in shared memory.  The Hankel entries
+// H_j = j! t^-(j+1) of the 40 integer offsets t are tabulated per block.
+constexpr int M2L_TILE = 4;
+constexpr int M2L_SRC = 2 * M2L_TILE;   // 8 x 8 staged source cells
+constexpr int M2L_T = M2L_TILE * M2L_TILE * FMM_P;
+
+__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
+                                                       cplx *Loc, int l) {
     __shared__ cplx sh[49][2 * FMM_P - 1];   // offset (dx, dy) in [-3, 3]^2 at (dy+3)*7 + dx+3
     __shared__ cplx se[4][FMM_P];
+    __shared__ cplx sm[M2L_SRC * M2L_SRC][FMM_P];
+    __shared__ int sc[M2L_SRC * M2L_SRC];
     if (l > S->fL) return;
     fmm_shift_table(se);
     for (int q = threadIdx.x; q < 49; q += blockDim.x) {
@@ -333,28 +341,42 @@ __global__ void __launch_bounds__(128) k_fmm_m2l_l2l(const VxScalars *S, const i
             fact *= (double)(j + 1);
         }
     }
-    __syncthreads();
     const long long m = 1LL << l;
+    const long long tiles1 = vx_ceil_div(m, (long long)M2L_TILE);
     const double s = S->fside / (double)m;
     const cplx *Ml = M + fmm_level_off(l) * FMM_P;
     const int *cl = cnt + fmm_level_off(l);
     cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
     const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
-    const long long tot = m * m * FMM_P;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
-         e += (long long)gridDim.x * blockDim.x) {
-        const long long c = e / FMM_P;
-        const int lc = (int)(e % FMM_P);
+    const int lc = threadIdx.x % FMM_P;
+    const int cell = threadIdx.x / FMM_P;
+    for (long long t = blockIdx.x; t < tiles1 * tiles1; t += gridDim.x) {
+        const long long tx0 = (t % tiles1) * M2L_TILE, ty0 = (t / tiles1) * M2L_TILE;
+        const long long sx0 = tx0 - 2, sy0 = ty0 - 2;   // staged region origin
+        __syncthreads();   // the previous tile is done with sm / sc; tables are built
+        for (int e = threadIdx.x; e < M2L_SRC * M2L_SRC * FMM_P; e += blockDim.x) {
+            const int q = e / FMM_P, k = e % FMM_P;
+            const long long qx = sx0 + q % M2L_SRC, qy = sy0 + q / M2L_SRC;
+            const bool in = qx >= 0 && qx < m && qy >= 0 && qy < m;
+            const long long src = qy * m + qx;
+            const int c = in ? cl[src] : 0;
+            if (k == 0) sc[q] = c;
+            sm[q][k] = c > 0 ? Ml[src * FMM_P + k] : cplx{0.0, 0.0};
+        }
+        __syncthreads();
+        const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
+        if (ix >= m || iy >= m) continue;
+        const long long c = iy * m + ix;
         cplx a = {0.0, 0.0};
         if (cl[c] > 0) {
-            const long long ix = c % m, iy = c / m, px = ix >> 1, py = iy >> 1;
+            const long long px = ix >> 1, py = iy >> 1;
             for (long long qy = max(0LL, 2 * (py - 1)); qy <= min(m - 1, 2 * (py + 1) + 1); ++qy) {
                 for (long long qx = max(0LL, 2 * (px - 1)); qx <= min(m - 1, 2 * (px + 1) + 1); ++qx) {
                     if (llabs(qx - ix) <= 1 && llabs(qy - iy) <= 1) continue;   // neighbours: near field
-                    const long long src = qy * m + qx;
-                    if (cl[src] == 0) continue;
+                    const int q = (int)((qy - sy0) * M2L_SRC + (qx - sx0));
+                    if (sc[q] == 0) continue;
                     const cplx *H = sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + lc;   // H_{k+lc}
-                    const cplx *B = Ml + src * FMM_P;
+                    const cplx *B = sm[q];
                     double ar = 0.0, ai = 0.0;
 #pragma unroll
                     for (int k = 0; k < FMM_P; ++k) {
@@ -376,7 +398,7 @@ __global__ void __launch_bounds__(128) k_fmm_m2l_l2l(const VxScalars *S, const i
                 a = cadd(a, cscale(acc, ldexp(1.0, -lc)));
             }
         }
-        Ll[e] = a;
+        Ll[c * FMM_P + lc] = a;
     }
 }
 
@@ -631,8 +653,9 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
         k_fmm_m2m<<<gm, 128, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
     }
     for (int l = 2; l <= Lmax; ++l) {
-        const int g = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));
-        k_fmm_m2l_l2l<<<g, 128, 0, L.stream>>>(S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
+        const long long t1 = vx_ceil_div(1LL << l, (long long)M2L_TILE);
+        const int g = (int)std::min<long long>(grid * 2, t1 * t1);
+        k_fmm_m2l_l2l<<<g, M2L_T, 0, L.stream>>>(S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
         VX_COUNT(L);
     }
     k_fmm_row_items<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_start, w.row_items); VX_COUNT(L);
