@@ -9,10 +9,43 @@
 // result is run-to-run identical.
 #include "vx_internal.cuh"
 
-// Segment (x2,y2)->(x1,y1) against every panel; nearest crossing wins.
-__device__ bool vx_hitting(const VxParams &p, const vx_panel *pan, double x1, double y1, double x2,
-                           double y2, int *hitpan) {
+// Segment (x2,y2)->(x1,y1) against one panel: on a crossing, sets hit and
+// keeps the crossing nearest to (x2,y2) (the lower panel index on a tie,
+// which is the reference's choice when it scans panels in index order).
+__device__ __forceinline__ void vx_hit_panel(const vx_panel &q, int i, double A, double B, double D, double x1,
+                                             double y1, double x2, double y2, bool &hit, double &minDist,
+                                             int &minN) {
     const double thr = 1e-12;
+    double r0 = A * q.left[0] + B * q.left[1] + D;
+    double r1 = A * q.right[0] + B * q.right[1] + D;
+    if (fabs(r0) < thr) r0 = 0.0;
+    if (fabs(r1) < thr) r1 = 0.0;
+    if (r0 * r1 <= 0) {
+        double A1 = q.right[1] - q.left[1];
+        double B1 = q.left[0] - q.right[0];
+        double D1 = q.left[1] * q.right[0] - q.left[0] * q.right[1];
+        double r2 = A1 * x1 + B1 * y1 + D1;
+        double r3 = A1 * x2 + B1 * y2 + D1;
+        if (fabs(r2) < thr) r2 = 0.0;
+        if (fabs(r3) < thr) r3 = 0.0;
+        if (r2 * r3 <= 0) {
+            hit = true;
+            double den = A * B1 - B * A1;
+            double X = (B * D1 - D * B1) / den;
+            double Y = (A1 * D - D1 * A) / den;
+            double d2 = (x2 - X) * (x2 - X) + (y2 - Y) * (y2 - Y);
+            if (d2 < minDist || (d2 == minDist && minN >= 0 && i < minN)) { minDist = d2; minN = i; }
+        }
+    }
+}
+
+// Segment (x2,y2)->(x1,y1) against the panels; nearest crossing wins.  With
+// hit lists (hstart/hidx: per cell of a grid over the body, every panel whose
+// bounding box touches the cell) only the panels listed in the cells under
+// the segment's bounding box are tested: a panel the segment crosses touches
+// that box, so the set of crossings, and the nearest one, are unchanged.
+__device__ bool vx_hitting(const VxParams &p, const vx_panel *pan, double x1, double y1, double x2,
+                           double y2, int *hitpan, const int *hstart = nullptr, const int *hidx = nullptr) {
     double minDist = 25.0;
     int minN = -1;
     bool hit = !(((x1 < p.px_min) && (x2 < p.px_min)) || ((x1 > p.px_max) && (x2 > p.px_max)) ||
@@ -20,30 +53,30 @@ __device__ bool vx_hitting(const VxParams &p, const vx_panel *pan, double x1, do
     if (hit) {
         hit = false;
         const double A = y2 - y1, B = x1 - x2, D = y1 * x2 - x1 * y2;
-        for (int i = 0; i < p.P; ++i) {
-            const vx_panel &q = pan[i];
-            double r0 = A * q.left[0] + B * q.left[1] + D;
-            double r1 = A * q.right[0] + B * q.right[1] + D;
-            if (fabs(r0) < thr) r0 = 0.0;
-            if (fabs(r1) < thr) r1 = 0.0;
-            if (r0 * r1 <= 0) {
-                double A1 = q.right[1] - q.left[1];
-                double B1 = q.left[0] - q.right[0];
-                double D1 = q.left[1] * q.right[0] - q.left[0] * q.right[1];
-                double r2 = A1 * x1 + B1 * y1 + D1;
-                double r3 = A1 * x2 + B1 * y2 + D1;
-                if (fabs(r2) < thr) r2 = 0.0;
-                if (fabs(r3) < thr) r3 = 0.0;
-                if (r2 * r3 <= 0) {
-                    hit = true;
-                    double den = A * B1 - B * A1;
-                    double X = (B * D1 - D * B1) / den;
-                    double Y = (A1 * D - D1 * A) / den;
-                    double d2 = (x2 - X) * (x2 - X) + (y2 - Y) * (y2 - Y);
-                    if (d2 < minDist) { minDist = d2; minN = i; }
+        bool done = false;
+        if (hstart) {
+            const double fx0 = (fmin(x1, x2) - p.hit_x0) / p.hit_h, fx1 = (fmax(x1, x2) - p.hit_x0) / p.hit_h;
+            const double fy0 = (fmin(y1, y2) - p.hit_y0) / p.hit_h, fy1 = (fmax(y1, y2) - p.hit_y0) / p.hit_h;
+            if (fx1 < 0.0 || fy1 < 0.0 || fx0 >= (double)p.hit_nx || fy0 >= (double)p.hit_ny) {
+                done = true;   // the segment misses the grid, which holds every panel
+            } else {
+                const int cx0 = max((int)floor(fx0), 0), cx1 = min((int)floor(fx1), p.hit_nx - 1);
+                const int cy0 = max((int)floor(fy0), 0), cy1 = min((int)floor(fy1), p.hit_ny - 1);
+                if ((cx1 - cx0 + 1) * (cy1 - cy0 + 1) <= 16) {
+                    for (int cy = cy0; cy <= cy1; ++cy)
+                        for (int cx = cx0; cx <= cx1; ++cx) {
+                            const int c = cy * p.hit_nx + cx;
+                            for (int q = hstart[c]; q < hstart[c + 1]; ++q) {
+                                const int i = hidx[q];
+                                vx_hit_panel(pan[i], i, A, B, D, x1, y1, x2, y2, hit, minDist, minN);
+                            }
+                        }
+                    done = true;
                 }
             }
         }
+        if (!done)
+            for (int i = 0; i < p.P; ++i) vx_hit_panel(pan[i], i, A, B, D, x1, y1, x2, y2, hit, minDist, minN);
     }
     *hitpan = minN;
     return hit;
@@ -62,7 +95,8 @@ __device__ __forceinline__ double vx_block_sum(double v, double *sh) {
 }
 
 __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, const VxScalars *S,
-                                                       const vx_panel *pan, double *red) {
+                                                       const vx_panel *pan, double *red, const int *hstart,
+                                                       const int *hidx) {
     __shared__ double sh[VX_THREADS];
     const long long n = S->n;
     const long long n_new0 = S->n0;   // vortices born this step: [n0, n)
@@ -81,7 +115,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, con
         const double xn = fma(v.vx[i * v.vs], p.dt, x);
         const double yn = fma(v.vy[i * v.vs], p.dt, y);
         int hp = -1;
-        if (gi != 0 && vx_hitting(p, pan, xn, yn, x, y, &hp)) {
+        if (gi != 0 && vx_hitting(p, pan, xn, yn, x, y, &hp, hstart, hidx)) {
             if (hp >= 0) {   // the reference reads panels[-1] when no crossing is nearer than 5
                 const double cx = pan[hp].contr[0], cy = pan[hp].contr[1];
                 const double dx = cx - p.rc_x, dy = cy - p.rc_y;
@@ -119,8 +153,9 @@ __global__ void k_sums(VxParams p, VxScalars *S, const double *red, int nblocks)
 }
 
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                             VxWork &w, const vx_panel *pan) {
-    k_advect<<<VX_RED_BLOCKS, VX_THREADS, 0, L.stream>>>(p, v, S, pan, w.red); VX_COUNT(L);
+                             VxWork &w, const vx_panel *pan, const int *hstart, const int *hidx) {
+    if (p.hit_nx <= 0 || p.hit_ny <= 0) hstart = hidx = nullptr;
+    k_advect<<<VX_RED_BLOCKS, VX_THREADS, 0, L.stream>>>(p, v, S, pan, w.red, hstart, hidx); VX_COUNT(L);
     k_sums<<<1, 32, 0, L.stream>>>(p, S, w.red, VX_RED_BLOCKS); VX_COUNT(L);
     return cudaGetLastError();
 }

@@ -63,6 +63,7 @@ struct vx_sim {
     double *d_minv = nullptr;
     double *d_minvT = nullptr;   // transposed copy read by the birth solve
     int *d_wstart = nullptr, *d_widx = nullptr;   // wall panel lists per wall cell
+    int *d_hstart = nullptr, *d_hidx = nullptr;   // hitting-test panel lists per cell
     long long wall_bytes = 0;
     VxScalars *d_S = nullptr;
     VxScalars *h_S = nullptr;     // pinned mirror
@@ -377,6 +378,59 @@ static vx_status build_wall_lists(vx_sim *s, const vx_panel *pan, int P) {
     return VX_OK;
 }
 
+// Hitting-test panel lists: a grid over the bounding box of all panel
+// endpoints (cells of side 4 L_max, at most 512 per side); each panel is
+// listed, in ascending order, in every cell its own bounding box touches.
+static vx_status build_hit_lists(vx_sim *s, const vx_panel *pan, int P) {
+    VxParams &p = s->prm;
+    p.hit_nx = p.hit_ny = 0;
+    double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300, lmax = 0.0;
+    for (int i = 0; i < P; ++i) {
+        for (const double *e : {pan[i].left, pan[i].right}) {
+            x0 = std::min(x0, e[0]); x1 = std::max(x1, e[0]);
+            y0 = std::min(y0, e[1]); y1 = std::max(y1, e[1]);
+        }
+        lmax = std::max(lmax, pan[i].length);
+    }
+    if (P <= 0 || !(lmax > 0.0)) return VX_OK;
+    double h = 4.0 * lmax;
+    h = std::max(h, std::max(x1 - x0, y1 - y0) / 512.0);
+    const double pad = 1e-9 * std::max(1.0, std::max(fabs(x0), fabs(x1)) + std::max(fabs(y0), fabs(y1)));
+    x0 -= pad; y0 -= pad;
+    const long long nx = (long long)std::floor((x1 + pad - x0) / h) + 1;
+    const long long ny = (long long)std::floor((y1 + pad - y0) / h) + 1;
+    std::vector<std::vector<int>> cells((size_t)(nx * ny));
+    for (int f = 0; f < P; ++f) {
+        const double bx0 = std::min(pan[f].left[0], pan[f].right[0]), bx1 = std::max(pan[f].left[0], pan[f].right[0]);
+        const double by0 = std::min(pan[f].left[1], pan[f].right[1]), by1 = std::max(pan[f].left[1], pan[f].right[1]);
+        const long long cx0 = std::max(0LL, (long long)std::floor((bx0 - x0) / h) - 1);
+        const long long cx1 = std::min(nx - 1, (long long)std::floor((bx1 - x0) / h) + 1);
+        const long long cy0 = std::max(0LL, (long long)std::floor((by0 - y0) / h) - 1);
+        const long long cy1 = std::min(ny - 1, (long long)std::floor((by1 - y0) / h) + 1);
+        for (long long yy = cy0; yy <= cy1; ++yy)
+            for (long long xx = cx0; xx <= cx1; ++xx) cells[(size_t)(yy * nx + xx)].push_back(f);
+    }
+    std::vector<int> start((size_t)(nx * ny + 1), 0), idx;
+    for (size_t c = 0; c < cells.size(); ++c) {
+        start[c] = (int)idx.size();
+        idx.insert(idx.end(), cells[c].begin(), cells[c].end());
+    }
+    start[cells.size()] = (int)idx.size();
+    if (idx.empty()) idx.push_back(0);
+    s->wall_bytes += (long long)sizeof(int) * (long long)(start.size() + idx.size());
+    if (cudaMalloc(&s->d_hstart, sizeof(int) * start.size()) != cudaSuccess) return VX_ERR_NOMEM;
+    if (cudaMalloc(&s->d_hidx, sizeof(int) * idx.size()) != cudaSuccess) return VX_ERR_NOMEM;
+    if (cudaMemcpy(s->d_hstart, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->d_hidx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return VX_ERR_CUDA;
+    p.hit_x0 = x0;
+    p.hit_y0 = y0;
+    p.hit_h = h;
+    p.hit_nx = (int)nx;
+    p.hit_ny = (int)ny;
+    return VX_OK;
+}
+
 extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t P, int device,
                                vx_sim **out) {
     if (!conf || !pan || P < 2 || !out) { vx_set_error("vx_create: bad arguments"); return VX_ERR_ARG; }
@@ -423,6 +477,7 @@ extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t
     if (cudaMemcpy(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(VX_ERR_CUDA);
     if (build_wall_lists(s, pan, (int)P) != VX_OK) return fail(VX_ERR_NOMEM);
+    if (build_hit_lists(s, pan, (int)P) != VX_OK) return fail(VX_ERR_NOMEM);
     // panel system on the device
     const long long S1 = P + 1;
     if (cudaMalloc(&s->d_minv, sizeof(double) * S1 * S1) != cudaSuccess) return fail(VX_ERR_NOMEM);
@@ -467,6 +522,8 @@ extern "C" vx_status vx_destroy(vx_sim *s) {
     if (s->d_minvT) cudaFree(s->d_minvT);
     if (s->d_wstart) cudaFree(s->d_wstart);
     if (s->d_widx) cudaFree(s->d_widx);
+    if (s->d_hstart) cudaFree(s->d_hstart);
+    if (s->d_hidx) cudaFree(s->d_hidx);
     if (s->d_S) cudaFree(s->d_S);
     if (s->h_S) cudaFreeHost(s->h_S);
     if (s->d_probe) cudaFree(s->d_probe);
@@ -672,7 +729,7 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
         if ((e = vx_launch_wall(L, p, v, s->d_S, s->d_pan, s->d_wstart, s->d_widx)) != cudaSuccess) return e;
     ev(4);
     if (mask & VX_STAGE_ADVECT)
-        if ((e = vx_launch_advect(L, p, v, s->d_S, s->w, s->d_pan)) != cudaSuccess) return e;
+        if ((e = vx_launch_advect(L, p, v, s->d_S, s->w, s->d_pan, s->d_hstart, s->d_hidx)) != cudaSuccess) return e;
     if (mask & VX_STAGE_COMPACT)
         if ((e = vx_launch_compact(L, p, v, s->d_S, s->w)) != cudaSuccess) return e;
     if (mask & VX_STAGE_COLLAPSE1)

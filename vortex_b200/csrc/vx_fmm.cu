@@ -39,6 +39,7 @@ int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0
 
 constexpr int FMM_P = VX_FMM_P;  // expansion terms
 constexpr int FMM_T = 256;
+constexpr int FMM_W = 32;        // targets per near-field work item (one warp)
 
 struct cplx {
     double r, i;
@@ -403,7 +404,8 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
 }
 
 // Near field (FP32, core smoothing, 3 nearest) + far field (L2P, FP64) for
-// row segments of up to FMM_T leaf-sorted targets.
+// row segments of up to FMM_W leaf-sorted targets, one warp each: the warp
+// stages the sources of its 3 rows x (its leaves +- 1) window 32 at a time.
 __device__ __forceinline__ float vx_rcp_approx2(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -414,6 +416,8 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                                                    const int *sorted, const int *start, const int2 *items,
                                                    const cplx *Loc, int *flag_list) {
     __shared__ float4 sm[FMM_T];
+    const int lane = threadIdx.x & 31;
+    float4 *ws = sm + (threadIdx.x & ~31);   // this warp's staged sources
     const long long n = S->n;
     const int L = S->fL;
     const long long m = 1LL << L;
@@ -422,12 +426,13 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
     const float eps2 = (float)p.eps2;
     const long long nitems = S->cnitems;
     const cplx *LL = Loc + fmm_level_off(L) * FMM_P;
-    for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const long long wpb = FMM_T / 32;
+    for (long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < nitems; it += gridDim.x * wpb) {
         const int2 item = items[it];
         const long long row = item.x;
         const long long row_end = start[(row + 1) * m];
-        const long long last = min((long long)item.y + FMM_T, row_end);
-        const long long t = item.y + threadIdx.x;
+        const long long last = min((long long)item.y + FMM_W, row_end);
+        const long long t = item.y + lane;
         const bool valid = t < last;
         float4 me = valid ? srt[t] : make_float4(0.f, 0.f, 0.f, 0.f);
         const long long j_self = valid ? sorted[t] : -1;
@@ -441,18 +446,17 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
         for (long long rr = max(row - 1, 0LL); rr <= min(row + 1, m - 1); ++rr) {
             const long long j0 = start[rr * m + c0], j1 = start[rr * m + c1 + 1];
             const float oy = (float)((double)(rr - row) * h);
-            for (long long jt = j0; jt < j1; jt += FMM_T) {
-                __syncthreads();
-                if (jt + threadIdx.x < j1) {
-                    float4 q = srt[jt + threadIdx.x];
+            for (long long jt = j0; jt < j1; jt += 32) {
+                if (jt + lane < j1) {
+                    float4 q = srt[jt + lane];
                     q.x += (float)(((double)q.w - (double)ca) * h);
                     q.y += oy;
-                    sm[threadIdx.x] = q;
+                    ws[lane] = q;
                 }
-                __syncthreads();
-                const int cnt = (int)min((long long)FMM_T, j1 - jt);
+                __syncwarp();
+                const int cnt = (int)min(32LL, j1 - jt);
                 for (int q = 0; q < cnt; ++q) {
-                    const float4 s = sm[q];
+                    const float4 s = ws[q];
                     if (fabsf(s.w - tcol) > 1.5f) continue;   // outside this target's 3x3 leaves
                     const float dx = me.x - s.x, dy = me.y - s.y;
                     const float r2 = fmaf(dx, dx, dy * dy);
@@ -465,6 +469,7 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                     sy = fmaf(mm, dx, sy);
                     sx = fmaf(-mm, dy, sx);
                 }
+                __syncwarp();
                 ax += (double)sx; ay += (double)sy;
                 sx = 0.f; sy = 0.f;
             }
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                     my += start[rr * m + min(tc + 1, m - 1) + 1] - start[rr * m + max(tc - 1, 0LL)];
             }
             for (int o = 16; o > 0; o >>= 1) my += __shfl_xor_sync(0xffffffffu, my, o);
-            if ((threadIdx.x & 31) == 0 && my) atomicAdd(&S->pairs_bs, my);
+            if (lane == 0 && my) atomicAdd(&S->pairs_bs, my);
         }
         if (valid && j_self < n) {
             // far field: f(z) = sum a_l u^l at the target's leaf (none below depth 2)
@@ -580,7 +585,7 @@ __global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_i
     const long long m = 1LL << S->fL;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m;
          r += (long long)gridDim.x * blockDim.x)
-        row_items[r] = (start[(r + 1) * m] - start[r * m] + FMM_T - 1) / FMM_T;
+        row_items[r] = (start[(r + 1) * m] - start[r * m] + FMM_W - 1) / FMM_W;
 }
 
 __global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
@@ -601,7 +606,7 @@ __global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long
     long long run = sh[threadIdx.x] - local;
     for (long long q = b; q < e; ++q) { out[q] = run; run += in[q]; }
     if (threadIdx.x == blockDim.x - 1) {
-        // the item buffer holds s/256 + rows items, so this never truncates
+        // the item buffer holds s/32 + rows items, so this never truncates
         if (run > items_cap) S->err |= VX_DERR_GRID;
         S->cnitems = run <= items_cap ? run : items_cap;
     }
@@ -614,7 +619,7 @@ __global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row
          r += (long long)gridDim.x * blockDim.x) {
         const int s0 = start[r * m];
         for (int q = 0; q < row_items[r]; ++q)
-            if (off[r] + q < items_cap) items[off[r] + q] = make_int2((int)r, s0 + q * FMM_T);
+            if (off[r] + q < items_cap) items[off[r] + q] = make_int2((int)r, s0 + q * FMM_W);
     }
 }
 

@@ -42,6 +42,8 @@ struct VxParams {
     double wall_x0, wall_x1, wall_y0, wall_y1;  // birth-point bbox grown by 5 L_max
     double wall_h;                              // side of the wall panel-list cells
     int wall_nx, wall_ny;                       // wall cells (0: no lists)
+    double hit_x0, hit_y0, hit_h;               // hitting-test panel lists: grid origin, cell side
+    int hit_nx, hit_ny;                         // hitting cells (0: no lists)
     double rc_x, rc_y;
     double drop_eps;
     double diff_cutoff;
@@ -210,7 +212,8 @@ cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxVi
 cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                            const vx_panel *pan, const int *wstart = nullptr, const int *widx = nullptr);
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                             VxWork &w, const vx_panel *pan);
+                             VxWork &w, const vx_panel *pan,
+                             const int *hstart = nullptr, const int *hidx = nullptr);
 cudaError_t vx_launch_compact(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                               VxWork &w);
 cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
