@@ -115,12 +115,20 @@ def run_ours(args, rank, world, device):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def timed_steps(sim, K, W):
+    def timed_steps(sim, K, W, tune=False):
         """W untimed steps, then K steps each bracketed by events on the
         handle's stream with an L2 flush between steps."""
         stream = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{device}")
         sim.step(W)
         sim.sync()
+        tuned = None
+        if tune:
+            # untimed: the autotuner picks direct or FMM and the leaf size on
+            # this state, then two more steps re-capture the step graph
+            from vortex_b200 import autotune
+            tuned = autotune.tune(sim, reps=2, device=device)["best"]
+            sim.step(2)
+            sim.sync()
         sim.set_timing(True)
         sim.pair_counts(clear=True)
         launches0 = sim.launches()
@@ -140,14 +148,14 @@ def run_ours(args, rank, world, device):
         pc = sim.pair_counts()
         launches = sim.launches() - launches0
         sim.set_timing(False)
-        return ms, t, launches, nvec, pc
+        return ms, t, launches, nvec, pc, tuned
 
     # ---- FP32 bulk (headline) ------------------------------------------
     sim = Nt.Sim(wl.cylinder_conf(Nt.PREC_FP32, P_PANELS), pan, device=device)
     sim.set_particles(x0, y0, g0)
     clocks = ClockSampler(device)
     clocks.start()
-    ms, tst, launches, nvec, pc = timed_steps(sim, args.steps, args.warmup)
+    ms, tst, launches, nvec, pc, tuned = timed_steps(sim, args.steps, args.warmup, tune=not args.no_autotune)
     ck = clocks.stop()
     total_ms = float(sum(ms))
     if dist:
@@ -192,7 +200,7 @@ def run_ours(args, rank, world, device):
     if not args.skip_fp64:
         sim64 = Nt.Sim(wl.cylinder_conf(Nt.PREC_FP64, P_PANELS), pan, device=device)
         sim64.set_particles(x0, y0, g0)
-        ms64, t64, _, _, _ = timed_steps(sim64, args.fp64_steps, 1)
+        ms64, t64, _, _, _, _ = timed_steps(sim64, args.fp64_steps, 1)
         sim64.close()
         fp64 = {"steps_per_s": 1e3 * len(ms64) / sum(ms64), "ms_per_step": float(np.mean(ms64)),
                 "bs_pair_kernel_ms": t64[5] / len(ms64), "diffusion_pair_kernel_ms": t64[6] / len(ms64),
@@ -227,6 +235,9 @@ def run_ours(args, rank, world, device):
                    "panels": P_PANELS, "n_particles_start": args.n, "n_particles_end": int(n_end),
                    "precision": "fp32 pair sums, fp64 expansions/panel solve/forces/positions",
                    "l2": "flushed between timed steps (256 MiB write)",
+                   "biot_savart": (f"autotuned before timing: {tuned['form']}"
+                                   + (f", {tuned['leaf']} vortices per leaf" if tuned and tuned['leaf'] else "")
+                                   if tuned else "FMM, 32 vortices per leaf (default)"),
                    "parallelism": f"{world} independent bodies (one per GPU)"},
         "particle_interactions_per_s": {"effective": world * eff * 1e3 * K / total_ms,
                                         "executed": world * (pc[0] + pc[1]) / (total_ms * 1e-3),
@@ -413,6 +424,7 @@ def main():
     ap.add_argument("--ref-cuda-steps", type=int, default=0,
                     help="also time the reference's own CUDA build for this many steps (0: off)")
     ap.add_argument("--ref-cuda-timeout", type=float, default=900.0)
+    ap.add_argument("--no-autotune", action="store_true", help="skip the untimed autotuning before timing")
     ap.add_argument("--multibody", action="store_true",
                     help="also run the seeded multi-body population batched and served")
     ap.add_argument("--batch-bodies", type=int, default=256)

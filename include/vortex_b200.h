@@ -80,7 +80,11 @@ typedef struct vx_conf {
     int32_t birth_offset_mode;  /* VX_BIRTH_* ; default VX_BIRTH_REF */
     double drop_eps;            /* |G| below this is removed; default 1e-12 */
     double diff_cutoff;         /* bulk form: vortex diffusion ignores pairs
-                                   with r > diff_cutoff * d_i (default 30) */
+                                   with r > diff_cutoff * d_i (default 20:
+                                   each such term weighs below e^-20 = 2e-9,
+                                   together about (c+1) e^-c = 4e-8 of the
+                                   sum in a uniform cloud, below its FP32
+                                   rounding) */
     int32_t n_probes_grid;      /* >0: probes on an n x n grid (box below) */
     int32_t pad1_;
     double probe_box[4];        /* x0, x1, y0, y1 of the probe grid */
@@ -95,6 +99,9 @@ typedef struct vx_conf {
                                    1e-12 fails, as in the reference);
                                    1 = partial pivoting; 2 = the reference's
                                    rule, partial pivoting if it fails */
+    int32_t fmm_leaf;           /* quadtree depth: mean vortices per leaf
+                                   the depth aims at (default 32) */
+    int32_t pad3_;
 } vx_conf;
 
 typedef struct vx_sim vx_sim;
@@ -212,6 +219,11 @@ vx_status vx_server_result(vx_server *srv, int64_t id, int *state, int64_t *step
  * submit-to-finish s, [5] mean resident bodies per tick, [6] body steps,
  * [7] particle steps, [8] bytes reserved now, [9] ticks. */
 vx_status vx_server_stats(vx_server *srv, double out10[10]);
+
+/* Switch the bulk form's far field (fmm: 1 quadtree FMM and birth far
+ * field, 0 direct sums) and the quadtree's target vortices per leaf at run
+ * time (the autotuner's knobs); the step graph is re-captured. */
+vx_status vx_set_fmm(vx_sim *sim, int fmm, int leaf);
 
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);

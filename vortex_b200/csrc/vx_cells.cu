@@ -2,9 +2,10 @@
 // bulk-form vortex diffusion over it.
 //
 // The diffusive velocity (reference diffusion_Kernel, src/kernel.cu:985-1029)
-// sums G_j exp(-r/d_i) terms; beyond r = c d_i (c = diff_cutoff, default 30)
-// a term is below e^-c of its strength, so the bulk form sums only those
-// pairs.  Particles are binned into square cells of side h (h tracks the
+// sums G_j exp(-r/d_i) terms; beyond r = c d_i (c = diff_cutoff, default 20)
+// a term is below e^-c of its strength, and in a uniform cloud all of them
+// together about (c+1) e^-c = 4e-8 of the sum (below its FP32 rounding), so
+// the bulk form sums only the pairs within c d_i.  Particles are binned into square cells of side h (h tracks the
 // mean 3-nearest distance), cell ids are sorted stably (radix sort: equal ids
 // keep index order, so every sum has a fixed order), and the cell-sorted
 // particles (x, y, G, d) are gathered into one float4 per particle.

@@ -158,6 +158,7 @@ void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams 
         p->b_rfar2 = 4.0 * r2 * (1.0 + 1e-12);
         p->birth_far = (c->precision == VX_PREC_FP32 && c->fmm) ? 1 : 0;
     }
+    p->fmm_leaf = c->fmm_leaf > 0 ? c->fmm_leaf : 32;
     p->P = P;
     p->n_of_points = (int)c->n_of_points;
     p->birth_mode = c->birth_offset_mode;
@@ -172,8 +173,9 @@ extern "C" vx_status vx_conf_default(vx_conf *c) {
     c->precision = VX_PREC_FP64;
     c->birth_offset_mode = VX_BIRTH_REF;
     c->drop_eps = 1e-12;
-    c->diff_cutoff = 30.0;
+    c->diff_cutoff = 20.0;
     c->fmm = 1;
+    c->fmm_leaf = 32;
     return VX_OK;
 }
 
@@ -928,6 +930,18 @@ extern "C" vx_status vx_step_many(vx_sim *const *sims, int count, int64_t nsteps
             vx_status st = vx_step(sims[i], 1);
             if (st != VX_OK) return st;
         }
+    return VX_OK;
+}
+
+extern "C" vx_status vx_set_fmm(vx_sim *s, int fmm, int leaf) {
+    if (!s || leaf < 1) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    CU(cudaStreamSynchronize(s->stream));
+    s->conf.fmm = fmm != 0;
+    s->conf.fmm_leaf = leaf;
+    s->prm.fmm_leaf = leaf;
+    s->prm.birth_far = (s->prm.prec == VX_PREC_FP32 && s->conf.fmm && s->P > 0) ? 1 : 0;
+    drop_graph(s);
     return VX_OK;
 }
 

@@ -84,16 +84,16 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
         for (int q = 0; q < 4; ++q) atomicMin(&S->fb[q], sk[q][0]);
 }
 
-// Square box, depth L = ceil(log4(n / 8)) within [2, Lmax], reduced until
+// Square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], reduced until
 // the leaf side is at least eps.
-__global__ void k_fmm_params(VxScalars *S, double eps, int Lmax) {
+__global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
     const long long n = S->n;
     const double x0 = vx_dunkey(S->fb[0]), x1 = -vx_dunkey(S->fb[1]);
     const double y0 = vx_dunkey(S->fb[2]), y1 = -vx_dunkey(S->fb[3]);
     double side = fmax(x1 - x0, y1 - y0);
     side = side * (1.0 + 1e-9) + 1e-12;
     int L = 2;
-    while (L < Lmax && (double)(1LL << (2 * L)) * 8.0 < (double)n) ++L;
+    while (L < Lmax && (double)(1LL << (2 * L)) * (double)leaf < (double)n) ++L;
     while (L > 2 && side / (double)(1LL << L) < eps) --L;
     // a box smaller than 4 eps: no pair may use an expansion, all near field
     if (side / 4.0 < eps) L = 1;
@@ -637,7 +637,7 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     const int Lmax = w.fmm_lmax;
     k_fmm_begin<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
     k_fmm_bbox<<<grid, FMM_T, 0, L.stream>>>(v, S); VX_COUNT(L);
-    k_fmm_params<<<1, 1, 0, L.stream>>>(S, p.eps, Lmax); VX_COUNT(L);
+    k_fmm_params<<<1, 1, 0, L.stream>>>(S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32); VX_COUNT(L);
     k_fmm_zero_cnt<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_cnt); VX_COUNT(L);
     k_fmm_leafid<<<grid, FMM_T, 0, L.stream>>>(v, S, w.key0, w.val0, w.fmm_cnt); VX_COUNT(L);
     k_fmm_scan_sum<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_cnt, w.cell_chunk_cnt); VX_COUNT(L);

@@ -52,6 +52,7 @@ struct VxParams {
     // local expansion about that centre (birth_far != 0)
     double bc_x, bc_y, b_rfar2;
     int birth_far;
+    int fmm_leaf;          // quadtree depth aims at this many vortices per leaf
     int P;
     int n_of_points;
     int birth_mode;

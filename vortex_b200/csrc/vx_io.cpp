@@ -39,6 +39,7 @@ extern "C" vx_status vx_conf_read(const char *path, vx_conf *c) {
         D(h_col_x) D(h_col_y) D(rc_x) D(rc_y) D(r_col_diff_sign) D(r_col_same_sign)
         B(matrix_load) D(max_ve_g) D(rel_t) B(steady_flow) U(tree_depth) D(theta) B(no_log_buf)
         D(drop_eps) D(diff_cutoff) B(fmm) B(gj_pivot)
+        else if (key_is(buf, "fmm_leaf")) { int v_ = 0; if (sscanf(buf, "%*s %d", &v_) == 1 && v_ > 0) c->fmm_leaf = v_; }
         else if (key_is(buf, "precision")) {
             char v[32] = {0};
             if (sscanf(buf, "%*s %31s", v) == 1)

@@ -41,7 +41,7 @@ class Conf(C.Structure):
         ("precision", C.c_int32), ("birth_offset_mode", C.c_int32),
         ("drop_eps", C.c_double), ("diff_cutoff", C.c_double),
         ("n_probes_grid", C.c_int32), ("pad1_", C.c_int32), ("probe_box", C.c_double * 4),
-        ("fmm", C.c_int32), ("gj_pivot", C.c_int32),
+        ("fmm", C.c_int32), ("gj_pivot", C.c_int32), ("fmm_leaf", C.c_int32), ("pad3_", C.c_int32),
     ]
 
 
@@ -253,6 +253,9 @@ class Sim:
 
     def stream(self) -> int:
         return lib().vx_get_stream(self.h) or 0
+
+    def set_fmm(self, fmm: bool, leaf: int = 8):
+        _check(lib().vx_set_fmm(self.h, C.c_int(int(fmm)), C.c_int(int(leaf))), "vx_set_fmm")
 
     def device_bytes(self) -> int:
         b = C.c_int64(0)
