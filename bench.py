@@ -243,7 +243,8 @@ def run_ours(args, rank, world, device):
                                         "executed": world * (pc[0] + pc[1]) / (total_ms * 1e-3),
                                         "effective_definition": "N_targets x N_sources per step (direct-sum equivalent)",
                                         "executed_definition": "near-field + diffusion pair evaluations"},
-        "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+        "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)),
+                       "steps": [round(float(t), 3) for t in ms]},
         "stage_ms": {"birth": tst[0] / K, "velocity": tst[1] / K, "diffusion": tst[2] / K,
                      "wall": tst[3] / K, "advect_compact_collapse": tst[4] / K},
         "structures": tree,

@@ -636,7 +636,7 @@ static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView
                               int rhs_chunks) {
     const int P = p.P, P32 = (int)vx_round32(P);
     const int tiles = (P + RHS_T - 1) / RHS_T;
-    const int grid = (int)min((long long)tiles * rhs_chunks, (long long)L.num_sms * 8);
+    const int grid = (int)min((long long)tiles * rhs_chunks, (long long)L.num_sms * 16);
     const bool far = p.prec == VX_PREC_FP32 && p.birth_far;
     if (far) {
         const int nb = std::min(2 * L.num_sms, VX_BF_MAX_BLOCKS);

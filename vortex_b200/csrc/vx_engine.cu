@@ -328,10 +328,14 @@ static vx_status ensure_capacity(vx_sim *s) {
     return grow(s, need_for(s, s->n_upper));
 }
 
+// Source chunks of the birth right-hand side: enough (panel tile, chunk)
+// items for every SM to hold several blocks, within the partial-sum buffer
+// (at most num_sms * 4 chunks).
 static int rhs_chunks_for(vx_sim *s) {
     const int tiles = (s->P + 127) / 128;
-    long long want = std::max(1LL, (long long)s->num_sms * 4 / tiles);
-    long long bysrc = std::max(1LL, vx_ceil_div(s->n_upper, 2048));
+    long long want = std::max(1LL, (long long)s->num_sms * 16 / tiles);
+    want = std::min<long long>(want, (long long)s->num_sms * 4);
+    long long bysrc = std::max(1LL, vx_ceil_div(s->n_upper, 1024));
     return (int)std::min(want, bysrc);
 }
 

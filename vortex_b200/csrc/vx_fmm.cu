@@ -403,9 +403,11 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
     }
 }
 
-// Near field (FP32, core smoothing, 3 nearest) + far field (L2P, FP64) for
-// row segments of up to FMM_W leaf-sorted targets, one warp each: the warp
-// stages the sources of its 3 rows x (its leaves +- 1) window 32 at a time.
+// Near field (FP32, core smoothing, 3 nearest) + far field (L2P, FP64): one
+// warp per work item of up to FMM_W targets of one leaf.  All of them share
+// the 3 x 3 leaves around it, whose sources the warp stages 32 at a time
+// (three contiguous runs of the leaf-sorted array), coordinates relative to
+// the item's leaf centre.
 __device__ __forceinline__ float vx_rcp_approx2(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -429,27 +431,25 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
     const long long wpb = FMM_T / 32;
     for (long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < nitems; it += gridDim.x * wpb) {
         const int2 item = items[it];
-        const long long row = item.x;
-        const long long row_end = start[(row + 1) * m];
-        const long long last = min((long long)item.y + FMM_W, row_end);
+        const long long leaf = item.x;
+        const long long row = leaf / m, col = leaf % m;
+        const long long last = min((long long)item.y + FMM_W, (long long)start[leaf + 1]);
         const long long t = item.y + lane;
         const bool valid = t < last;
-        float4 me = valid ? srt[t] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 me = valid ? srt[t] : make_float4(0.f, 0.f, 0.f, 0.f);   // relative to the leaf centre
         const long long j_self = valid ? sorted[t] : -1;
-        const float tcol = me.w;
-        const long long ca = (long long)srt[item.y].w, cb = (long long)srt[last - 1].w;
-        const long long c0 = max(ca - 1, 0LL), c1 = min(cb + 1, m - 1);
-        // coordinates relative to the centre of the item's first leaf
-        me.x += (float)(((double)tcol - (double)ca) * h);
+        const long long c0 = max(col - 1, 0LL), c1 = min(col + 1, m - 1);
         float sx = 0.f, sy = 0.f, d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
         double ax = 0.0, ay = 0.0;
+        long long scanned = 0;
         for (long long rr = max(row - 1, 0LL); rr <= min(row + 1, m - 1); ++rr) {
             const long long j0 = start[rr * m + c0], j1 = start[rr * m + c1 + 1];
+            scanned += j1 - j0;
             const float oy = (float)((double)(rr - row) * h);
             for (long long jt = j0; jt < j1; jt += 32) {
                 if (jt + lane < j1) {
                     float4 q = srt[jt + lane];
-                    q.x += (float)(((double)q.w - (double)ca) * h);
+                    q.x += (float)(((double)q.w - (double)col) * h);
                     q.y += oy;
                     ws[lane] = q;
                 }
@@ -457,7 +457,6 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                 const int cnt = (int)min(32LL, j1 - jt);
                 for (int q = 0; q < cnt; ++q) {
                     const float4 s = ws[q];
-                    if (fabsf(s.w - tcol) > 1.5f) continue;   // outside this target's 3x3 leaves
                     const float dx = me.x - s.x, dy = me.y - s.y;
                     const float r2 = fmaf(dx, dx, dy * dy);
                     if (r2 < d3 && jt + q != t) {
@@ -474,24 +473,17 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                 sx = 0.f; sy = 0.f;
             }
         }
-        {   // executed near-field pairs: sources in each target's 3x3 leaves
-            unsigned long long my = 0;
-            if (valid) {
-                const long long tc = (long long)tcol;
-                for (long long rr = max(row - 1, 0LL); rr <= min(row + 1, m - 1); ++rr)
-                    my += start[rr * m + min(tc + 1, m - 1) + 1] - start[rr * m + max(tc - 1, 0LL)];
-            }
-            for (int o = 16; o > 0; o >>= 1) my += __shfl_xor_sync(0xffffffffu, my, o);
-            if (lane == 0 && my) atomicAdd(&S->pairs_bs, my);
+        {   // executed near-field pairs: every target of the item sees the same 3x3 leaves
+            const unsigned long long nv = __popc(__ballot_sync(0xffffffffu, valid));
+            if (lane == 0) atomicAdd(&S->pairs_bs, (unsigned long long)scanned * nv);
         }
         if (valid && j_self < n) {
             // far field: f(z) = sum a_l u^l at the target's leaf (none below depth 2)
             cplx f = {0.0, 0.0};
             if (L >= 2) {
-                const long long leaf = row * m + (long long)tcol;
                 const double xd = v.x[j_self * v.ps], yd = v.y[j_self * v.ps];
-                const cplx u = {(xd - (S->fx0 + ((double)(leaf % m) + 0.5) * h)) / h,
-                                (yd - (S->fy0 + ((double)(leaf / m) + 0.5) * h)) / h};
+                const cplx u = {(xd - (S->fx0 + ((double)col + 0.5) * h)) / h,
+                                (yd - (S->fy0 + ((double)row + 0.5) * h)) / h};
                 // f = sum_l A_l u^l / l!, nested as A_0 + (u/1)(A_1 + (u/2)(A_2 + ...))
                 f = LL[leaf * FMM_P + FMM_P - 1];
                 for (int l = FMM_P - 2; l >= 0; --l)
@@ -581,11 +573,16 @@ __global__ void k_fmm_nn3_fix(VxView v, const VxScalars *S, const float4 *srt, c
 }
 
 // Row items over the leaf grid (m x m), as for the neighbour-list grid.
+// Near-field work items: every leaf's targets in chunks of FMM_W, counted per
+// leaf row (one thread per row walks its leaves).
 __global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_items) {
     const long long m = 1LL << S->fL;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m;
-         r += (long long)gridDim.x * blockDim.x)
-        row_items[r] = (start[(r + 1) * m] - start[r * m] + FMM_W - 1) / FMM_W;
+         r += (long long)gridDim.x * blockDim.x) {
+        int k = 0;
+        for (long long c = r * m; c < (r + 1) * m; ++c) k += (start[c + 1] - start[c] + FMM_W - 1) / FMM_W;
+        row_items[r] = k;
+    }
 }
 
 __global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
@@ -617,9 +614,10 @@ __global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row
     const long long m = 1LL << S->fL;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m;
          r += (long long)gridDim.x * blockDim.x) {
-        const int s0 = start[r * m];
-        for (int q = 0; q < row_items[r]; ++q)
-            if (off[r] + q < items_cap) items[off[r] + q] = make_int2((int)r, s0 + q * FMM_W);
+        long long o = off[r];
+        for (long long c = r * m; c < (r + 1) * m; ++c)
+            for (int j = start[c]; j < start[c + 1]; j += FMM_W, ++o)
+                if (o < items_cap) items[o] = make_int2((int)c, j);   // (leaf, first target slot)
     }
 }
 
