@@ -140,11 +140,15 @@ __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, con
     t = vx_block_sum(sm, sh);  if (threadIdx.x == 0) red[blockIdx.x * 4 + 3] = t;
 }
 
-__global__ void k_sums(VxParams p, VxScalars *S, const double *red, int nblocks) {
-    if (threadIdx.x != 0) return;
+// Block sums combined by one block: thread t adds blocks t, t + 256, ... in
+// order, then a fixed shared-memory tree; the result is run-to-run identical.
+__global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, const double *red, int nblocks) {
+    __shared__ double sh[VX_THREADS];
     double a[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int b = 0; b < nblocks; ++b)
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
         for (int q = 0; q < 4; ++q) a[q] += red[b * 4 + q];
+    for (int q = 0; q < 4; ++q) a[q] = vx_block_sum(a[q], sh);
+    if (threadIdx.x != 0) return;
     for (int q = 0; q < 4; ++q) S->raw[q] = a[q];
     S->dg = a[0];
     S->fx = a[1] * (p.rho / p.dt);
@@ -156,6 +160,6 @@ cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView 
                              VxWork &w, const vx_panel *pan, const int *hstart, const int *hidx) {
     if (p.hit_nx <= 0 || p.hit_ny <= 0) hstart = hidx = nullptr;
     k_advect<<<VX_RED_BLOCKS, VX_THREADS, 0, L.stream>>>(p, v, S, pan, w.red, hstart, hidx); VX_COUNT(L);
-    k_sums<<<1, 32, 0, L.stream>>>(p, S, w.red, VX_RED_BLOCKS); VX_COUNT(L);
+    k_sums<<<1, VX_THREADS, 0, L.stream>>>(p, S, w.red, VX_RED_BLOCKS); VX_COUNT(L);
     return cudaGetLastError();
 }
