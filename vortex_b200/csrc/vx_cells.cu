@@ -328,6 +328,31 @@ __device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
     return r;
 }
 
+// Two diffusion pairs (one target, sources a and b of a staged slot).  The
+// rsqrt and ex2 of every pair run on the MUFU pipe, which bounds the kernel;
+// a polynomial 2^x on the FMA pipe for a quarter of the pairs was measured
+// slower, as that pipe then limits.
+__device__ __forceinline__ void diff_pair2(const float4 *slot, const float2 *gslot, f2 TX, f2 TY, f2 NDD,
+                                           float thr2, f2 &S2X, f2 &S2Y, f2 &S1) {
+    const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(slot);
+    const f2 G = *reinterpret_cast<const f2 *>(gslot);
+    const f2 DX = f2_sub(TX, sq.x), DY = f2_sub(TY, sq.y);
+    const f2 R2 = f2_fma(DX, DX, f2_mul(DY, DY));
+    float r2a, r2b;
+    f2_unpack(R2, r2a, r2b);
+    const f2 RD = f2_pack(vx_rsqrt_approx(fmaxf(r2a, thr2)), vx_rsqrt_approx(fmaxf(r2b, thr2)));
+    const f2 ARG = f2_mul(f2_mul(R2, RD), NDD);
+    float aa, ab;
+    f2_unpack(ARG, aa, ab);
+    const float ea = r2a > thr2 ? vx_ex2_approx(aa) : 0.0f;
+    const float eb = r2b > thr2 ? vx_ex2_approx(ab) : 0.0f;
+    const f2 GE = f2_mul(G, f2_pack(ea, eb));
+    const f2 M = f2_mul(GE, RD);
+    S2X = f2_fma(M, DX, S2X);   // sums of +m dx, +m dy: negated by the caller
+    S2Y = f2_fma(M, DY, S2Y);
+    S1 = f2_add(S1, GE);
+}
+
 // Vortex diffusion over the cell grid (bulk form), one warp per work item of
 // CG_W targets, one per lane; each step of the inner loop takes two sources
 // in packed FP32 pairs.  Per pair: r^2, 1/r = rsqrt(max(r^2, thr^2)),
@@ -409,24 +434,7 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
                 __syncwarp();
                 f2 S2X = 0ull, S2Y = 0ull, S1 = 0ull;   // +0.0f in both halves
 #pragma unroll 8
-                for (int q = 0; q < 16; ++q) {
-                    const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(wxy + q);
-                    const f2 G = *reinterpret_cast<const f2 *>(wg + q);
-                    const f2 DX = f2_sub(TX, sq.x), DY = f2_sub(TY, sq.y);
-                    const f2 R2 = f2_fma(DX, DX, f2_mul(DY, DY));
-                    float r2a, r2b;
-                    f2_unpack(R2, r2a, r2b);
-                    const f2 RD = f2_pack(vx_rsqrt_approx(fmaxf(r2a, thr2)), vx_rsqrt_approx(fmaxf(r2b, thr2)));
-                    float aa, ab;
-                    f2_unpack(f2_mul(f2_mul(R2, RD), NDD), aa, ab);
-                    const float ea = r2a > thr2 ? vx_ex2_approx(aa) : 0.0f;
-                    const float eb = r2b > thr2 ? vx_ex2_approx(ab) : 0.0f;
-                    const f2 GE = f2_mul(G, f2_pack(ea, eb));
-                    const f2 M = f2_mul(GE, RD);
-                    S2X = f2_fma(M, DX, S2X);   // sums of +m dx, +m dy: negated below
-                    S2Y = f2_fma(M, DY, S2Y);
-                    S1 = f2_add(S1, GE);
-                }
+                for (int q = 0; q < 16; ++q) diff_pair2(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
                 __syncwarp();
                 float a, b;   // the two halves are added in FP32, then carried in FP64
                 f2_unpack(S2X, a, b); I2x -= (double)(a + b);

@@ -223,19 +223,25 @@ __global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, co
     }
 }
 
-// P2M at the leaves (one thread per leaf; FP64 positions).
-__global__ void k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const int *sorted, cplx *M) {
+// P2M at the leaves, one warp per leaf: each lane expands its own vortices
+// (FP64 positions), then a fixed butterfly sums the lanes.  Empty leaves are
+// not written (nothing reads their expansion).
+__global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const int *sorted,
+                                                 cplx *M) {
     const int L = S->fL;
     const long long m = 1LL << L, nl = m * m, n = S->n;
     const double h = S->fside / (double)m;
     cplx *ML = M + fmm_level_off(L) * FMM_P;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nl;
-         c += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nl; c += nw) {
+        const int j0 = start[c], j1 = start[c + 1];
+        if (j0 == j1) continue;
         cplx b[FMM_P];
 #pragma unroll
         for (int k = 0; k < FMM_P; ++k) b[k] = {0.0, 0.0};
         const double cx = S->fx0 + ((double)(c % m) + 0.5) * h, cy = S->fy0 + ((double)(c / m) + 0.5) * h;
-        for (int q = start[c]; q < start[c + 1]; ++q) {
+        for (int q = j0 + lane; q < j1; q += 32) {
             const long long j = sorted[q];
             if (j >= n) continue;
             const double gj = v.g[j * v.ps];
@@ -248,7 +254,13 @@ __global__ void k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const 
             }
         }
 #pragma unroll
-        for (int k = 0; k < FMM_P; ++k) ML[c * FMM_P + k] = b[k];
+        for (int k = 0; k < FMM_P; ++k) {
+            for (int o = 16; o > 0; o >>= 1) {
+                b[k].r += __shfl_xor_sync(0xffffffffu, b[k].r, o);
+                b[k].i += __shfl_xor_sync(0xffffffffu, b[k].i, o);
+            }
+            if (lane == k) ML[c * FMM_P + k] = b[k];
+        }
     }
 }
 
@@ -574,14 +586,16 @@ __global__ void k_fmm_nn3_fix(VxView v, const VxScalars *S, const float4 *srt, c
 
 // Row items over the leaf grid (m x m), as for the neighbour-list grid.
 // Near-field work items: every leaf's targets in chunks of FMM_W, counted per
-// leaf row (one thread per row walks its leaves).
+// leaf row (one warp per row, lanes over its leaves).
 __global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_items) {
     const long long m = 1LL << S->fL;
-    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m;
-         r += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
         int k = 0;
-        for (long long c = r * m; c < (r + 1) * m; ++c) k += (start[c + 1] - start[c] + FMM_W - 1) / FMM_W;
-        row_items[r] = k;
+        for (long long c = r * m + lane; c < (r + 1) * m; c += 32) k += (start[c + 1] - start[c] + FMM_W - 1) / FMM_W;
+        for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+        if (lane == 0) row_items[r] = k;
     }
 }
 
@@ -612,12 +626,24 @@ __global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long
 __global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row_items, const long long *off,
                             int2 *items, long long items_cap) {
     const long long m = 1LL << S->fL;
-    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m;
-         r += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
         long long o = off[r];
-        for (long long c = r * m; c < (r + 1) * m; ++c)
-            for (int j = start[c]; j < start[c + 1]; j += FMM_W, ++o)
-                if (o < items_cap) items[o] = make_int2((int)c, j);   // (leaf, first target slot)
+        for (long long c0 = r * m; c0 < (r + 1) * m; c0 += 32) {
+            const long long c = c0 + lane;
+            const int j0 = c < (r + 1) * m ? start[c] : 0, j1 = c < (r + 1) * m ? start[c + 1] : 0;
+            const int k = (j1 - j0 + FMM_W - 1) / FMM_W;
+            int inc = k;   // inclusive warp scan of the leaves' item counts
+            for (int d = 1; d < 32; d <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, inc, d);
+                if (lane >= d) inc += u;
+            }
+            long long oo = o + inc - k;
+            for (int j = j0; j < j1; j += FMM_W, ++oo)
+                if (oo < items_cap) items[oo] = make_int2((int)c, j);   // (leaf, first target slot)
+            o += __shfl_sync(0xffffffffu, inc, 31);
+        }
     }
 }
 
@@ -646,7 +672,7 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     const unsigned *skey = cur ? w.key1 : w.key0;
     const int *sorted = cur ? w.val1 : w.val0;
     k_fmm_gather<<<grid, FMM_T, 0, L.stream>>>(v, S, sorted, skey, w.srt); VX_COUNT(L);
-    k_fmm_p2m<<<grid, 128, 0, L.stream>>>(v, S, w.fmm_start, sorted, (cplx *)w.fmm_M); VX_COUNT(L);
+    k_fmm_p2m<<<grid * 4, 128, 0, L.stream>>>(v, S, w.fmm_start, sorted, (cplx *)w.fmm_M); VX_COUNT(L);
     // the level loops cover the deepest level this capacity allows; kernels
     // of levels below the depth chosen on the device return at once
     for (int l = Lmax - 1; l >= 0; --l) {
