@@ -92,6 +92,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
+def job_time_ms(local_ms: float, dist: bool, device: int = 0) -> float:
+    """The job's time: the slowest rank's device time (max over ranks)."""
+    if not dist:
+        return local_ms
+    import torch
+    on_gpu = torch.distributed.get_backend() == "nccl"
+    t = torch.tensor([local_ms], dtype=torch.float64, device=f"cuda:{device}" if on_gpu else "cpu")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def pinned(n, rt):
     p = C.c_void_p()
     if rt.cudaHostAlloc(C.byref(p), C.c_size_t(max(8 * n, 8)), 0) != 0:
@@ -157,11 +168,7 @@ def run_ours(args, rank, world, device):
     clocks.start()
     ms, tst, launches, nvec, pc, tuned = timed_steps(sim, args.steps, args.warmup, tune=not args.no_autotune)
     ck = clocks.stop()
-    total_ms = float(sum(ms))
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = job_time_ms(float(sum(ms)), dist, device)
     n_end = sim.count()
     K = args.steps
     # dominant pair kernel of the bulk step, timed by events around it
@@ -417,7 +424,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--n", "--particles", dest="n", type=int, default=1_000_000)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--cpu-targets", type=int, default=2048)
