@@ -27,8 +27,11 @@ int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0
 
 constexpr int CG_T = 256;
 constexpr int CG_W = 32;       // targets per work item (one warp)
-constexpr int CG_DIV = 8;      // cell side = cut-off radius at the mean d / CG_DIV
-constexpr int CG_KCAP = 16;    // widest window of a work item, in cells
+#ifndef VX_CG_DIV
+#define VX_CG_DIV 8
+#endif
+constexpr int CG_DIV = VX_CG_DIV;      // cell side = cut-off radius at the mean d / CG_DIV
+constexpr int CG_KCAP = 2 * CG_DIV;    // widest window of a work item, in cells (twice the mean radius)
 
 __global__ void k_cg_begin(VxScalars *S) {
     S->cb[0] = S->cb[1] = S->cb[2] = S->cb[3] = ~0ull;
