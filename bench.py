@@ -183,24 +183,33 @@ def run_ours(args, rank, world, device):
     # ---- end to end through the C ABI with host buffers -------------------
     rt = C.CDLL("libcudart.so.12")
     n_now = sim.count()
-    hx, _px = pinned(n_now + 4096, rt)
-    hy, _py = pinned(n_now + 4096, rt)
-    hg, _pg = pinned(n_now + 4096, rt)
+    room = n_now + P_PANELS * 12 + 4096      # at most P births per step
+    hx, _px = pinned(room, rt)
+    hy, _py = pinned(room, rt)
+    hg, _pg = pinned(room, rt)
     xs, ys, gs = sim.particles()
     e2e_steps = max(3, min(10, K))
     e2e_t = []
     bi = bo = 0
+    # two pinned buffer sets: a step reads its input from one and writes its
+    # result into the other, which is the next step's input
+    ox, _qx = pinned(room, rt)
+    oy, _qy = pinned(room, rt)
+    og, _qg = pinned(room, rt)
+    m = len(xs)
+    hx[:m], hy[:m], hg[:m] = xs, ys, gs
+    bufs = [(hx, hy, hg), (ox, oy, og)]
     for k in range(e2e_steps):
-        m = len(xs)
-        hx[:m], hy[:m], hg[:m] = xs, ys, gs
+        (ix, iy, ig), (wx, wy, wg) = bufs[k % 2], bufs[(k + 1) % 2]
         t0 = time.perf_counter()
-        sim.set_particles(hx[:m], hy[:m], hg[:m])
+        sim.set_particles(ix[:m], iy[:m], ig[:m])
         sim.step(1)
         f = sim.forces()
-        xs, ys, gs = sim.particles()
+        m_out = sim.particles_into(wx, wy, wg)
         e2e_t.append(time.perf_counter() - t0)
         bi += 24 * m
-        bo += 24 * len(xs) + f.nbytes
+        bo += 24 * m_out + f.nbytes
+        m = m_out
     sim.close()
     # ---- plain FP64 on the same workload ------------------------------------
     fp64 = None

@@ -459,19 +459,24 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
             scanned += j1 - j0;
             const float oy = (float)((double)(rr - row) * h);
             for (long long jt = j0; jt < j1; jt += 32) {
+                // a chunk is padded to 32 with G = 0 sources far away: they add
+                // exactly 0 and never enter the 3 nearest
+                float4 q = make_float4(1e18f, 1e18f, 0.f, 0.f);
                 if (jt + lane < j1) {
-                    float4 q = srt[jt + lane];
+                    q = srt[jt + lane];
                     q.x += (float)(((double)q.w - (double)col) * h);
                     q.y += oy;
-                    ws[lane] = q;
                 }
+                ws[lane] = q;
                 __syncwarp();
-                const int cnt = (int)min(32LL, j1 - jt);
-                for (int q = 0; q < cnt; ++q) {
+                const long long rel = t - jt;   // the target's own slot within the chunk, if any
+                const int self_q = (rel >= 0 && rel < 32) ? (int)rel : -1;
+#pragma unroll 8
+                for (int q = 0; q < 32; ++q) {
                     const float4 s = ws[q];
                     const float dx = me.x - s.x, dy = me.y - s.y;
                     const float r2 = fmaf(dx, dx, dy * dy);
-                    if (r2 < d3 && jt + q != t) {
+                    if (r2 < d3 && q != self_q) {
                         d3 = r2;
                         float tt = fminf(d3, d2); d3 = fmaxf(d3, d2); d2 = tt;
                         tt = fminf(d1, d2); d2 = fmaxf(d1, d2); d1 = tt;

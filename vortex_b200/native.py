@@ -170,6 +170,14 @@ class Sim:
         _check(lib().vx_get_particles(self.h, _p(x), _p(y), _p(g), C.c_int64(n), C.byref(m)), "vx_get_particles")
         return x, y, g
 
+    def particles_into(self, x, y, g) -> int:
+        """Live particles copied into caller arrays (float64, contiguous,
+        large enough; pinned host memory makes the copies fastest)."""
+        m = C.c_int64(0)
+        _check(lib().vx_get_particles(self.h, _p(x), _p(y), _p(g), C.c_int64(min(len(x), len(y), len(g))),
+                                      C.byref(m)), "vx_get_particles")
+        return m.value
+
     def velocity(self):
         n = self.count()
         vx, vy, d = np.zeros(n), np.zeros(n), np.zeros(n)
