@@ -141,6 +141,9 @@ vx_status vx_set_vinf(vx_sim *sim, double vx, double vy);
 vx_status vx_set_dg(vx_sim *sim, double dg);
 /* The inverted (P+1)^2 panel system, row-major. */
 vx_status vx_get_matrix(vx_sim *sim, double *minv);
+/* Replace the inverted panel system ((P+1)^2 row-major FP64), e.g. one read
+ * from a matrix file as the reference's matrix_load does. */
+vx_status vx_set_matrix(vx_sim *sim, const double *minv);
 
 /* Advance nsteps whole steps. */
 vx_status vx_step(vx_sim *sim, int64_t nsteps);
@@ -224,6 +227,10 @@ vx_status vx_server_stats(vx_server *srv, double out10[10]);
  * field, 0 direct sums) and the quadtree's target vortices per leaf at run
  * time (the autotuner's knobs); the step graph is re-captured. */
 vx_status vx_set_fmm(vx_sim *sim, int fmm, int leaf);
+
+/* Validation hook (no counterpart in the reference): the FP32 atan2 the
+ * bulk form's birth terms use, evaluated on device arrays of n floats. */
+vx_status vx_eval_bulk_atan2(const float *y, const float *x, float *out, int64_t n);
 
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);

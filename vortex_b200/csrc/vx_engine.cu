@@ -694,6 +694,18 @@ extern "C" vx_status vx_set_step_index(vx_sim *s, int64_t step) {
     return patch_scalars(s, [](VxScalars *h, const double *q) { h->step = (long long)q[0]; }, &a);
 }
 
+// Replace the inverted panel system (row-major (P+1)^2, e.g. a matrix file
+// the caller loaded) and its transposed copy.
+extern "C" vx_status vx_set_matrix(vx_sim *s, const double *minv) {
+    if (!s || !minv) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    const long long S1 = s->P + 1;
+    CU(cudaMemcpy(s->d_minv, minv, sizeof(double) * S1 * S1, cudaMemcpyHostToDevice));
+    CU(vx_transpose_square(launch_of(s), s->d_minv, s->d_minvT, S1));
+    CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}
+
 extern "C" vx_status vx_get_matrix(vx_sim *s, double *minv) {
     if (!s || !minv) return VX_ERR_ARG;
     CU(cudaSetDevice(s->device));
