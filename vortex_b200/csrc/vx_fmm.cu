@@ -426,6 +426,23 @@ __device__ __forceinline__ float vx_rcp_approx2(float x) {
     return r;
 }
 
+// One near-field pair: core-smoothed Biot-Savart term and the 3-nearest
+// insertion (skipping the target's own slot when SELF).
+template <bool SELF>
+__device__ __forceinline__ void near_pair(const float4 s, int q, int self_q, const float4 me, float eps2, float &d1,
+                                          float &d2, float &d3, float &sx, float &sy) {
+    const float dx = me.x - s.x, dy = me.y - s.y;
+    const float r2 = fmaf(dx, dx, dy * dy);
+    if (r2 < d3 && (!SELF || q != self_q)) {
+        d3 = r2;
+        float tt = fminf(d3, d2); d3 = fmaxf(d3, d2); d2 = tt;
+        tt = fminf(d1, d2); d2 = fmaxf(d1, d2); d1 = tt;
+    }
+    const float mm = s.z * vx_rcp_approx2(fmaxf(r2, eps2));
+    sy = fmaf(mm, dx, sy);
+    sx = fmaf(-mm, dy, sx);
+}
+
 __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                    const int *sorted, const int *start, const int2 *items,
                                                    const cplx *Loc, int *flag_list) {
@@ -471,19 +488,16 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
                 __syncwarp();
                 const long long rel = t - jt;   // the target's own slot within the chunk, if any
                 const int self_q = (rel >= 0 && rel < 32) ? (int)rel : -1;
+                // only chunks that hold one of the warp's own targets need the
+                // self test; the others take the loop without it
+                if (__any_sync(0xffffffffu, self_q >= 0)) {
 #pragma unroll 8
-                for (int q = 0; q < 32; ++q) {
-                    const float4 s = ws[q];
-                    const float dx = me.x - s.x, dy = me.y - s.y;
-                    const float r2 = fmaf(dx, dx, dy * dy);
-                    if (r2 < d3 && q != self_q) {
-                        d3 = r2;
-                        float tt = fminf(d3, d2); d3 = fmaxf(d3, d2); d2 = tt;
-                        tt = fminf(d1, d2); d2 = fmaxf(d1, d2); d1 = tt;
-                    }
-                    const float mm = s.z * vx_rcp_approx2(fmaxf(r2, eps2));
-                    sy = fmaf(mm, dx, sy);
-                    sx = fmaf(-mm, dy, sx);
+                    for (int q = 0; q < 32; ++q)
+                        near_pair<true>(ws[q], q, self_q, me, eps2, d1, d2, d3, sx, sy);
+                } else {
+#pragma unroll 8
+                    for (int q = 0; q < 32; ++q)
+                        near_pair<false>(ws[q], q, self_q, me, eps2, d1, d2, d3, sx, sy);
                 }
                 __syncwarp();
                 ax += (double)sx; ay += (double)sy;

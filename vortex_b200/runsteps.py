@@ -36,14 +36,16 @@ def main():
     sim.step(a.warmup)
     sim.sync()
     rt = C.CDLL("libcudart.so.12")
+    sim.pair_counts(clear=True)
     rt.cudaProfilerStart()
     t0 = time.perf_counter()
     sim.step(a.steps)
     sim.sync()
     t1 = time.perf_counter()
     rt.cudaProfilerStop()
+    pc = sim.pair_counts()
     print(json.dumps({"n_end": sim.count(), "steps": a.steps, "ms_per_step": 1e3 * (t1 - t0) / max(a.steps, 1),
-                      "precision": a.precision}))
+                      "precision": a.precision, "near_field_pairs": pc[0], "diffusion_pairs": pc[1]}))
     sim.close()
 
 
