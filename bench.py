@@ -222,6 +222,7 @@ def run_ours(args, rank, world, device):
                 "bs_pair_kernel_ms": t64[5] / len(ms64), "diffusion_pair_kernel_ms": t64[6] / len(ms64),
                 "form": "direct O(N^2) sums in FP64"}
     peak32 = Nt.measure_peak(device, fp64=False)
+    mufu = Nt.measure_peak(device, mode=3)        # 1e12 (rsqrt + ex2) units per second
     if rank != 0:
         return None
     value = world * 1e3 * K / total_ms
@@ -269,7 +270,14 @@ def run_ours(args, rank, world, device):
         "roofline": {"kernel": kname, "bound": "fp32-simt", "achieved": achieved, "peak": peak32,
                      "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": traffic,
                      "peak_source": "measured FP32 FMA throughput of this GPU (vx_measure_peak)",
-                     "flop_per_pair": kflop, "pairs_per_launch": kpairs, "launch_ms": kms},
+                     "flop_per_pair": kflop, "pairs_per_launch": kpairs, "launch_ms": kms,
+                     "mufu_ceiling": ({"bound": "special-function pipe (one rsqrt + one ex2 per pair)",
+                                       "achieved_tpairs_per_s": kpairs / (kms * 1e-3) / 1e12,
+                                       "peak_tpairs_per_s": mufu,
+                                       "frac": kpairs / (kms * 1e-3) / 1e12 / mufu,
+                                       "peak_source": "measured rsqrt+ex2 throughput of this GPU "
+                                                      "(vx_measure_peak mode 3)"}
+                                      if kname.startswith("k_diff_cells") else None)},
         "e2e": {"value": e2e_steps / sum(e2e_t), "unit": "steps/s",
                 "h2d_bytes_per_step": bi // e2e_steps, "d2h_bytes_per_step": bo // e2e_steps},
         "gpu_launches": int(launches),

@@ -255,8 +255,9 @@ vx_status vx_get_state(vx_sim *sim, double out9[9]);
 /* Absolute step index (a restart from KadrNNNNNN.txt sets it). */
 vx_status vx_set_step_index(vx_sim *sim, int64_t step);
 
-/* Measured FMA throughput of the vector pipe of `device` (TFLOP/s, FP64 when
- * fp64 != 0): the roofline denominator of the pair kernels. */
+/* Measured throughput of `device`, the roofline denominators of the pair
+ * kernels: mode 0 FP32 FMA, 1 FP64 FMA, 2 packed FP32 pairs (TFLOP/s);
+ * 3 rsqrt + ex2 units on the special-function pipe (1e12 units/s). */
 vx_status vx_measure_peak(int device, int fp64, double *tflops);
 
 #ifdef __cplusplus

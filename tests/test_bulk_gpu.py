@@ -120,7 +120,12 @@ def test_fmm_small_cloud_is_near_field_only():
 
 def test_bulk_steps_track_fp64():
     """20 whole steps from a warm cloud: counts within 2 %, total |G| within
-    5 %, force history within 5 % of the plain form."""
+    5 % of the plain form; the force history agrees per step (1e-3 of its
+    scale) over the first steps, before the first collapse or absorption
+    decision that the two precisions take differently, and its 20-step mean
+    within 5 % or 3 standard errors of the two series (after such a decision
+    the per-step force estimate moves by O(1) and the runs agree only in
+    distribution)."""
     s32, s64, pan, ck = pair(200, birth_offset_mode=2)
     x, y, g = wake_cloud(20000, seed=40, g_scale=1e-3)
     f32, f64 = [], []
@@ -136,7 +141,12 @@ def test_bulk_steps_track_fp64():
     _, _, g32 = s32.particles()
     _, _, g64 = s64.particles()
     assert abs(np.abs(g32).sum() - np.abs(g64).sum()) <= 0.05 * np.abs(g64).sum()
-    assert abs(np.mean(f32) - np.mean(f64)) <= 0.05 * max(abs(np.mean(f64)), 1e-6)
+    f32, f64 = np.array(f32), np.array(f64)
+    scale = np.abs(f64[1:]).max()
+    assert np.abs(f32[:4] - f64[:4]).max() <= 1e-3 * scale, (f32[:4], f64[:4])
+    sem = math.sqrt(f32[1:].var() / 19 + f64[1:].var() / 19)
+    tol = max(0.05 * abs(f64.mean()), 3 * sem)
+    assert abs(f32.mean() - f64.mean()) <= tol, (f32, f64, tol)
     s32.close()
     s64.close()
 

@@ -331,10 +331,11 @@ __device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
     return r;
 }
 
-// Two diffusion pairs (one target, sources a and b of a staged slot).  The
-// rsqrt and ex2 of every pair run on the MUFU pipe, which bounds the kernel;
-// a polynomial 2^x on the FMA pipe for a quarter of the pairs was measured
-// slower, as that pipe then limits.
+// Two diffusion pairs (one target, sources a and b of a staged slot).  Each
+// pair needs one rsqrt and one 2^x, both on the MUFU pipe.  A degree-5
+// polynomial 2^x on the FMA and integer pipes (round by adding 1.5 * 2^23,
+// exponent added to the bit pattern) for one or both pairs of a step was
+// measured 30 % slower on the whole kernel: those pipes then limit.
 __device__ __forceinline__ void diff_pair2(const float4 *slot, const float2 *gslot, f2 TX, f2 TY, f2 NDD,
                                            float thr2, f2 &S2X, f2 &S2Y, f2 &S1) {
     const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(slot);
@@ -362,24 +363,46 @@ __device__ __forceinline__ void diff_pair2(const float4 *slot, const float2 *gsl
 // e = 2^(-log2(e) r / d_i); the pair adds G e (I1) and G e (r_i - r_j) / r
 // (I2) unless r <= 0.001 eps.  Every source of the warp's window enters (the
 // window covers all sources within c d_i of each target; the ones beyond
-// weigh below e^-c).  A chunk of 32 staged sources is padded with G = 0
-// (which adds exactly 0) so the pair loop has a fixed trip count.
+// weigh below e^-c).
+//
+// The window is one column range per grid row.  The warp first lists the
+// rows (a lane per row: first source, x and y offsets) with an exclusive scan
+// of their lengths in shared memory, then walks the concatenated ranges in
+// chunks of 32 sources, each lane finding its source's row by advancing a
+// cursor over the scan; so a chunk spans row boundaries and only the last one
+// of the window is padded (with G = 0, which adds exactly 0) — padding every
+// row to 32 instead costs about 12 % more pair evaluations on the benchmark
+// wake.  A source's x offset is its column minus the item's first column:
+// the cell key minus (row * nx + first column), no division.
+#ifndef VX_DIFF_UNROLL
+#define VX_DIFF_UNROLL 16   // unrolled steps of the pair loop of k_diff_cells
+#endif
+#define VX_PRAGMA_(x) _Pragma(#x)
+#define VX_UNROLL(n) VX_PRAGMA_(unroll n)
 #ifndef VX_DIFF_MINB
 #define VX_DIFF_MINB 2   // minimum resident blocks per SM requested for k_diff_cells
 #endif
+struct DiffRow {
+    int j0;          // first source of the row's column range
+    int pre;         // sources of the rows before it (the entry after the last row holds the total)
+    unsigned base;   // row * nx + the item's first column (cell keys wrap modulo 2^32 alike)
+    float oy;        // row offset * h
+};
+constexpr int DIFF_ROWS = 2 * CG_KCAP + 2;   // rows of the widest window, and the total
 __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, VxView v, VxScalars *S,
                                                                    const float4 *srt, const unsigned *skey,
                                                                    const int *sorted, const int *start,
                                                                    const int2 *items, int *wide) {
     __shared__ float4 sxy[CG_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
     __shared__ float2 sg[CG_T / 2];    // (G_a, G_b)
+    __shared__ DiffRow srow[CG_T / 32][DIFF_ROWS];
     const int lane = threadIdx.x & 31;
     float4 *wxy = sxy + ((threadIdx.x & ~31) >> 1);
     float2 *wg = sg + ((threadIdx.x & ~31) >> 1);
+    DiffRow *wrow = srow[threadIdx.x >> 5];
     const long long nitems = S->cnitems, nx = S->cnx, ny = S->cny;
     const double hd = S->ch;
     const float h = (float)hd;
-    const unsigned unx = (unsigned)nx;
     const float cut = (float)p.diff_cutoff;
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
     const float log2e = 1.4426950408889634f;
@@ -394,8 +417,9 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
         const bool valid = t < last;
         float4 me = valid ? srt[t] : make_float4(0.f, 0.f, 0.f, 1.f);
         // coordinates relative to the centre of the item's first cell
-        const long long ocol = (long long)(skey[item.y] % unx);
-        if (valid) me.x += (float)((int)(skey[t] % unx) - (int)ocol) * h;   // as for the sources below
+        const unsigned key0 = skey[item.y];
+        const long long ocol = (long long)key0 - row * nx;
+        if (valid) me.x += (float)(int)(skey[t] - key0) * h;   // as for the sources below
         const float R = cut * me.w;
         const bool is_wide = valid && R > (float)CG_KCAP * h;
         if (is_wide) wide[atomicAdd(&S->cnwide, 1)] = (int)t;
@@ -411,41 +435,79 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
         const f2 TX = f2_pack(me.x, me.x), TY = f2_pack(me.y, me.y);
         const float nd = -log2e / me.w;
         const f2 NDD = f2_pack(nd, nd);
-        const int kk = (int)ceilf(rmax / h);
-        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
-        long long scanned = 0;
-        for (int dy = -kk; dy <= kk; ++dy) {
-            const long long rr = row + dy;
-            if (rr < 0 || rr >= ny) continue;
-            long long c0, c1;
-            if (!diff_window(dy, rmax, xlo, xhi, h, ocol, nx, c0, c1)) continue;
-            const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
-            scanned += j1 - j0;
-            const float oy = (float)((double)dy * hd);
-            for (long long jt = j0; jt < j1; jt += 32) {
-                float x = 0.f, y = 0.f, gq = 0.f;
-                if (jt + lane < j1) {
-                    const float4 q = srt[jt + lane];
-                    x = q.x + (float)((int)(skey[jt + lane] % unx) - (int)ocol) * h;
-                    y = q.y + oy;
-                    gq = q.z;
+        // rows -kk..kk (kk <= CG_KCAP: a non-wide target's radius is at most CG_KCAP cells)
+        const int kk = min((int)ceilf(rmax / h), CG_KCAP);
+        const int nrows = 2 * kk + 1;
+        int total = 0;
+        for (int r0 = 0; r0 < nrows; r0 += 32) {
+            const int r = r0 + lane;
+            DiffRow e = {0, 0, 0u, 0.0f};
+            int len = 0;
+            if (r < nrows) {
+                const int dy = r - kk;
+                const long long rr = row + dy;
+                long long c0, c1;
+                if (rr >= 0 && rr < ny && diff_window(dy, rmax, xlo, xhi, h, ocol, nx, c0, c1)) {
+                    e.j0 = start[rr * nx + c0];
+                    len = start[rr * nx + c1 + 1] - e.j0;
+                    e.base = (unsigned)(rr * nx + ocol);
+                    e.oy = (float)((double)dy * hd);
                 }
-                float *slot = reinterpret_cast<float *>(wxy + (lane >> 1));
-                slot[lane & 1] = x;
-                slot[2 + (lane & 1)] = y;
-                reinterpret_cast<float *>(wg + (lane >> 1))[lane & 1] = gq;
-                __syncwarp();
-                f2 S2X = 0ull, S2Y = 0ull, S1 = 0ull;   // +0.0f in both halves
-#pragma unroll 8
-                for (int q = 0; q < 16; ++q) diff_pair2(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
-                __syncwarp();
-                float a, b;   // the two halves are added in FP32, then carried in FP64
-                f2_unpack(S2X, a, b); I2x -= (double)(a + b);
-                f2_unpack(S2Y, a, b); I2y -= (double)(a + b);
-                f2_unpack(S1, a, b); I1 += (double)(a + b);
             }
+            int inc = len;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += u;
+            }
+            e.pre = total + inc - len;
+            if (r < nrows) wrow[r] = e;
+            total += __shfl_sync(0xffffffffu, inc, 31);
         }
-        pairs += (unsigned long long)scanned * (unsigned long long)nact;
+        if (lane == 0) wrow[nrows].pre = total;
+        __syncwarp();
+        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
+        int rc = 0;   // this lane's row cursor (rows only advance as the chunks do)
+        // the next chunk's source is loaded before the current chunk's pairs
+        // run, so its L2 latency overlaps them
+        float4 qn = make_float4(0.f, 0.f, 0.f, 0.f);
+        unsigned kn = 0u;
+        if (lane < total) {
+            while (rc < nrows - 1 && wrow[rc + 1].pre <= lane) ++rc;
+            const int j = wrow[rc].j0 + (lane - wrow[rc].pre);
+            qn = srt[j];
+            kn = skey[j];
+        }
+        for (int jt = 0; jt < total; jt += 32) {
+            const int f = jt + lane;
+            float x = 0.f, y = 0.f, gq = 0.f;
+            if (f < total) {
+                const DiffRow e = wrow[rc];
+                x = qn.x + (float)(int)(kn - e.base) * h;
+                y = qn.y + e.oy;
+                gq = qn.z;
+            }
+            float *slot = reinterpret_cast<float *>(wxy + (lane >> 1));
+            slot[lane & 1] = x;
+            slot[2 + (lane & 1)] = y;
+            reinterpret_cast<float *>(wg + (lane >> 1))[lane & 1] = gq;
+            __syncwarp();
+            if (f + 32 < total) {
+                while (rc < nrows - 1 && wrow[rc + 1].pre <= f + 32) ++rc;
+                const int j = wrow[rc].j0 + (f + 32 - wrow[rc].pre);
+                qn = srt[j];
+                kn = skey[j];
+            }
+            f2 S2X = 0ull, S2Y = 0ull, S1 = 0ull;   // +0.0f in both halves
+            VX_UNROLL(VX_DIFF_UNROLL)
+            for (int q = 0; q < 16; ++q) diff_pair2(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
+            __syncwarp();
+            float a, b;   // the two halves are added in FP32, then carried in FP64
+            f2_unpack(S2X, a, b); I2x -= (double)(a + b);
+            f2_unpack(S2Y, a, b); I2y -= (double)(a + b);
+            f2_unpack(S1, a, b); I1 += (double)(a + b);
+        }
+        __syncwarp();   // the row list is rewritten by the next item
+        pairs += (unsigned long long)total * (unsigned long long)nact;
         if (act && fabs(I1) > 1e-5) {
             const long long i = sorted[t];
             const double dd = (double)me.w;

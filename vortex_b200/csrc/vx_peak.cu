@@ -46,9 +46,31 @@ __global__ void __launch_bounds__(256) k_fma2_peak(float *out, int iters, float 
     if (s == 12345.678f) out[blockIdx.x] = s;
 }
 
+// Special-function pipe: one rsqrt and one ex2 per unit (the MUFU work of a
+// vortex-diffusion pair), eight independent chains per thread.
+__global__ void __launch_bounds__(256) k_mufu_peak(float *out, int iters) {
+    float r[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r[k] = 1.0f + 0.001f * (float)(threadIdx.x + k);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            float q, e;
+            asm volatile("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(q) : "f"(r[k]));
+            asm volatile("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(-0.01f * q));
+            r[k] = e;
+        }
+    }
+    float s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += r[k];
+    if (s == 12345.678f) out[blockIdx.x] = s;
+}
+
 // FLOP/s of back-to-back FMAs over the whole GPU (2 flops per FMA), best of
 // 5 timed launches after a warm-up.  fp64: 0 = FP32, 1 = FP64, 2 = packed
-// FP32 pairs (f32x2).
+// FP32 pairs (f32x2), 3 = rsqrt + ex2 units per second (in units of 1e12: the
+// special-function ceiling of the diffusion pairs).
 extern "C" vx_status vx_measure_peak(int device, int fp64, double *tflops) {
     if (!tflops) return VX_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return VX_ERR_CUDA;
@@ -65,6 +87,7 @@ extern "C" vx_status vx_measure_peak(int device, int fp64, double *tflops) {
         cudaEventRecord(e0);
         if (fp64 == 1) k_fma_peak<double><<<blocks, threads>>>((double *)out, iters, 0.999999, 1e-7);
         else if (fp64 == 2) k_fma2_peak<<<blocks, threads>>>((float *)out, iters, 0.9999f, 1e-4f);
+        else if (fp64 == 3) k_mufu_peak<<<blocks, threads>>>((float *)out, iters / 4);
         else k_fma_peak<float><<<blocks, threads>>>((float *)out, iters, 0.9999f, 1e-4f);
         cudaEventRecord(e1);
         cudaEventSynchronize(e1);
@@ -77,7 +100,8 @@ extern "C" vx_status vx_measure_peak(int device, int fp64, double *tflops) {
     cudaEventDestroy(e1);
     cudaFree(out);
     if (e != cudaSuccess) return VX_ERR_CUDA;
-    const double flops = (fp64 == 2 ? 4.0 : 2.0) * 8.0 * (double)iters * threads * blocks;
+    const double flops = fp64 == 3 ? 8.0 * (double)(iters / 4) * threads * blocks
+                                   : (fp64 == 2 ? 4.0 : 2.0) * 8.0 * (double)iters * threads * blocks;
     *tflops = flops / (best * 1e-3) / 1e12;
     return VX_OK;
 }

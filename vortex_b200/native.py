@@ -96,9 +96,11 @@ def default_conf(**kw) -> Conf:
     return c
 
 
-def measure_peak(device: int = 0, fp64: bool = False) -> float:
+def measure_peak(device: int = 0, fp64: bool = False, mode: int | None = None) -> float:
+    """TFLOP/s of the FP32 (or FP64) FMA pipe; mode 3: 1e12 rsqrt + ex2 units/s."""
     t = C.c_double(0)
-    _check(lib().vx_measure_peak(C.c_int(device), C.c_int(int(fp64)), C.byref(t)), "vx_measure_peak")
+    m = int(fp64) if mode is None else mode
+    _check(lib().vx_measure_peak(C.c_int(device), C.c_int(m), C.byref(t)), "vx_measure_peak")
     return t.value
 
 
