@@ -299,38 +299,6 @@ __device__ __forceinline__ bool diff_window(int dy, float R, float xlo, float xh
     return c0 <= c1;
 }
 
-// Packed FP32 pairs (PTX f32x2, sm_100): one instruction computes the same
-// operation for the lane's two targets.  The low half is the first target.
-typedef unsigned long long f2;
-__device__ __forceinline__ f2 f2_pack(float a, float b) {
-    f2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ void f2_unpack(f2 v, float &a, float &b) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-}
-__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
-    f2 r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
-    f2 r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
-    f2 r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
-    f2 r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
-}
-
 // Two diffusion pairs (one target, sources a and b of a staged slot).  Each
 // pair needs one rsqrt and one 2^x, both on the MUFU pipe.  A degree-5
 // polynomial 2^x on the FMA and integer pipes (round by adding 1.5 * 2^23,

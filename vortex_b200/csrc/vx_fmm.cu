@@ -426,29 +426,38 @@ __device__ __forceinline__ float vx_rcp_approx2(float x) {
     return r;
 }
 
-// One near-field pair: core-smoothed Biot-Savart term and the 3-nearest
-// insertion (skipping the target's own slot when SELF).
+// Two near-field pairs (one target, sources a and b of a staged slot) in
+// packed FP32: core-smoothed Biot-Savart terms and the branch-free 3-nearest
+// insertion (the target's own slot, when SELF, left out of the latter; its
+// Biot-Savart term is 0 as dx = dy = 0).
 template <bool SELF>
-__device__ __forceinline__ void near_pair(const float4 s, int q, int self_q, const float4 me, float eps2, float &d1,
-                                          float &d2, float &d3, float &sx, float &sy) {
-    const float dx = me.x - s.x, dy = me.y - s.y;
-    const float r2 = fmaf(dx, dx, dy * dy);
-    if (r2 < d3 && (!SELF || q != self_q)) {
-        d3 = r2;
-        float tt = fminf(d3, d2); d3 = fmaxf(d3, d2); d2 = tt;
-        tt = fminf(d1, d2); d2 = fmaxf(d1, d2); d1 = tt;
-    }
-    const float mm = s.z * vx_rcp_approx2(fmaxf(r2, eps2));
-    sy = fmaf(mm, dx, sy);
-    sx = fmaf(-mm, dy, sx);
+__device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gslot, int q2, int self_q, f2 TX,
+                                           f2 TY, float eps2, float &d1, float &d2, float &d3, f2 &SY,
+                                           f2 &SXN) {
+    const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(slot);
+    const f2 G = *reinterpret_cast<const f2 *>(gslot);
+    const f2 DX = f2_sub(TX, sq.x), DY = f2_sub(TY, sq.y);
+    const f2 R2 = f2_fma(DX, DX, f2_mul(DY, DY));
+    float r2a, r2b;
+    f2_unpack(R2, r2a, r2b);
+    vx_nn3_insert_bf(d1, d2, d3, (SELF && q2 == self_q) ? 3e38f : r2a);
+    vx_nn3_insert_bf(d1, d2, d3, (SELF && q2 + 1 == self_q) ? 3e38f : r2b);
+    const f2 MM = f2_mul(G, f2_pack(vx_rcp_approx2(fmaxf(r2a, eps2)), vx_rcp_approx2(fmaxf(r2b, eps2))));
+    SY = f2_fma(MM, DX, SY);
+    SXN = f2_fma(MM, DY, SXN);   // sum of +mm dy: negated by the caller
 }
 
-__global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+#ifndef VX_NEAR_MINB
+#define VX_NEAR_MINB 1   // minimum resident blocks per SM requested for k_fmm_near
+#endif
+__global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                    const int *sorted, const int *start, const int2 *items,
                                                    const cplx *Loc, int *flag_list) {
-    __shared__ float4 sm[FMM_T];
+    __shared__ float4 sxy[FMM_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
+    __shared__ float2 sg[FMM_T / 2];    // (G_a, G_b)
     const int lane = threadIdx.x & 31;
-    float4 *ws = sm + (threadIdx.x & ~31);   // this warp's staged sources
+    float4 *wxy = sxy + ((threadIdx.x & ~31) >> 1);
+    float2 *wg = sg + ((threadIdx.x & ~31) >> 1);
     const long long n = S->n;
     const int L = S->fL;
     const long long m = 1LL << L;
@@ -468,42 +477,69 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_near(VxParams p, VxView v, VxScal
         const float4 me = valid ? srt[t] : make_float4(0.f, 0.f, 0.f, 0.f);   // relative to the leaf centre
         const long long j_self = valid ? sorted[t] : -1;
         const long long c0 = max(col - 1, 0LL), c1 = min(col + 1, m - 1);
-        float sx = 0.f, sy = 0.f, d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
+        const f2 TX = f2_pack(me.x, me.x), TY = f2_pack(me.y, me.y);
+        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
         double ax = 0.0, ay = 0.0;
-        long long scanned = 0;
-        for (long long rr = max(row - 1, 0LL); rr <= min(row + 1, m - 1); ++rr) {
-            const long long j0 = start[rr * m + c0], j1 = start[rr * m + c1 + 1];
-            scanned += j1 - j0;
-            const float oy = (float)((double)(rr - row) * h);
-            for (long long jt = j0; jt < j1; jt += 32) {
-                // a chunk is padded to 32 with G = 0 sources far away: they add
-                // exactly 0 and never enter the 3 nearest
-                float4 q = make_float4(1e18f, 1e18f, 0.f, 0.f);
-                if (jt + lane < j1) {
-                    q = srt[jt + lane];
-                    q.x += (float)(((double)q.w - (double)col) * h);
-                    q.y += oy;
-                }
-                ws[lane] = q;
-                __syncwarp();
-                const long long rel = t - jt;   // the target's own slot within the chunk, if any
-                const int self_q = (rel >= 0 && rel < 32) ? (int)rel : -1;
-                // only chunks that hold one of the warp's own targets need the
-                // self test; the others take the loop without it
-                if (__any_sync(0xffffffffu, self_q >= 0)) {
-#pragma unroll 8
-                    for (int q = 0; q < 32; ++q)
-                        near_pair<true>(ws[q], q, self_q, me, eps2, d1, d2, d3, sx, sy);
-                } else {
-#pragma unroll 8
-                    for (int q = 0; q < 32; ++q)
-                        near_pair<false>(ws[q], q, self_q, me, eps2, d1, d2, d3, sx, sy);
-                }
-                __syncwarp();
-                ax += (double)sx; ay += (double)sy;
-                sx = 0.f; sy = 0.f;
+        // the 3 x 3 leaves are three contiguous runs (rows row-1..row+1 of
+        // columns c0..c1), walked as one stream in chunks of 32 sources, so
+        // only the stream's last chunk is padded
+        const long long r_lo = max(row - 1, 0LL), r_hi = min(row + 1, m - 1);
+        int rj0[3], rpre[4];
+        float roy[3];
+        rpre[0] = 0;
+        for (int r = 0; r < 3; ++r) {
+            const long long rr = r_lo + r;
+            int len = 0;
+            rj0[r] = 0;
+            roy[r] = 0.f;
+            if (rr <= r_hi) {
+                rj0[r] = start[rr * m + c0];
+                len = start[rr * m + c1 + 1] - rj0[r];
+                roy[r] = (float)((double)(rr - row) * h);
             }
+            rpre[r + 1] = rpre[r] + len;
         }
+        const int total = rpre[3];
+        // the target's own position in the stream (its leaf lies in row `row`)
+        const bool own1 = row > r_lo;   // the own row is run 1, else run 0 (top row of the grid)
+        const int f_self = valid ? (own1 ? rpre[1] + (int)(t - rj0[1]) : (int)(t - rj0[0])) : -1000;
+        for (int jt = 0; jt < total; jt += 32) {
+            // padding: G = 0 sources far away add exactly 0 and never enter the 3 nearest
+            float x = 1e18f, y = 1e18f, g = 0.f;
+            const int f = jt + lane;
+            if (f < total) {
+                const bool in0 = f < rpre[1], in1 = f < rpre[2];
+                const int j = in0 ? rj0[0] + f : (in1 ? rj0[1] + (f - rpre[1]) : rj0[2] + (f - rpre[2]));
+                const float4 q = srt[j];
+                x = q.x + (float)(((double)q.w - (double)col) * h);
+                y = q.y + (in0 ? roy[0] : (in1 ? roy[1] : roy[2]));
+                g = q.z;
+            }
+            float *slot = reinterpret_cast<float *>(wxy + (lane >> 1));
+            slot[lane & 1] = x;
+            slot[2 + (lane & 1)] = y;
+            reinterpret_cast<float *>(wg + (lane >> 1))[lane & 1] = g;
+            __syncwarp();
+            const int rel = f_self - jt;   // the target's own slot within the chunk, if any
+            const int self_q = (rel >= 0 && rel < 32) ? rel : -1;
+            f2 SY = 0ull, SXN = 0ull;   // +0.0f in both halves
+            // only chunks that hold one of the warp's own targets need the
+            // self test; the others take the loop without it
+            if (__any_sync(0xffffffffu, self_q >= 0)) {
+#pragma unroll 8
+                for (int q = 0; q < 16; ++q)
+                    near_pair2<true>(wxy + q, wg + q, 2 * q, self_q, TX, TY, eps2, d1, d2, d3, SY, SXN);
+            } else {
+#pragma unroll 8
+                for (int q = 0; q < 16; ++q)
+                    near_pair2<false>(wxy + q, wg + q, 2 * q, self_q, TX, TY, eps2, d1, d2, d3, SY, SXN);
+            }
+            __syncwarp();
+            float a, b;   // the two halves are added in FP32, then carried in FP64
+            f2_unpack(SXN, a, b); ax -= (double)(a + b);
+            f2_unpack(SY, a, b); ay += (double)(a + b);
+        }
+        const long long scanned = total;
         {   // executed near-field pairs: every target of the item sees the same 3x3 leaves
             const unsigned long long nv = __popc(__ballot_sync(0xffffffffu, valid));
             if (lane == 0) atomicAdd(&S->pairs_bs, (unsigned long long)scanned * nv);

@@ -174,6 +174,48 @@ __device__ __forceinline__ void vx_nn3_insert(T &d1, T &d2, T &d3, T r2) {
     }
 }
 
+// The same 3 smallest squared distances without a branch (FP32, five
+// min/max per value): the new value moves each kept one up by at most one
+// place, so the three updates read only the previous values.
+__device__ __forceinline__ void vx_nn3_insert_bf(float &d1, float &d2, float &d3, float r2) {
+    d3 = fminf(d3, fmaxf(d2, r2));
+    d2 = fminf(d2, fmaxf(d1, r2));
+    d1 = fminf(d1, r2);
+}
+
+// Packed FP32 pairs (PTX f32x2, sm_100): one instruction computes the same
+// operation on two values held in one 64-bit register; the low half is the
+// first.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2_pack(float a, float b) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
+    f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
 // Monotonic unsigned key of a double (for atomicMin on signed values).
 __device__ __forceinline__ unsigned long long vx_dkey(double v) {
     unsigned long long b = (unsigned long long)__double_as_longlong(v);
