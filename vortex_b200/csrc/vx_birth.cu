@@ -352,51 +352,74 @@ __device__ __forceinline__ bool bf_near(const VxParams &p, double x, double y) {
 }
 
 // Far-field coefficient partials (one per block, fixed order) and the
-// number of near sources of each block.
+// number of near sources of each block.  Each thread sums the terms of its
+// own sources in registers, 16 coefficients per pass (a_16..a_31 in the
+// second pass, from -G w^17 by squarings); then a reduce-scatter over the
+// warp (at each halving a lane keeps the half of its values selected by its
+// lane bit and adds the partner's copy: lane q ends with value q, i.e.
+// coefficient q/2, part q&1) and a fixed-order sum over the block's warps.
 __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
-    __shared__ double sacc[BF_T / 32][BF_P][2];
+    __shared__ double sacc[BF_T / 32][32];
     __shared__ int snear[BF_T / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     long long j0, j1;
     bf_chunk(S, gridDim.x, blockIdx.x, j0, j1);
-    double ar = 0.0, ai = 0.0;   // coefficient `lane` of this warp (BF_P == 32)
     int nnear = 0;
-    for (long long jt = j0 + wid * 32; jt < j1; jt += BF_T) {
-        const long long j = jt + lane;
-        double tr = 0.0, ti = 0.0, wr = 0.0, wi = 0.0;
-        if (j < j1) {
+    for (int pass = 0; pass < 2; ++pass) {
+        double acc[32];   // (re, im) of the pass's 16 coefficients
+#pragma unroll
+        for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+        for (long long j = j0 + threadIdx.x; j < j1; j += BF_T) {
             const double x = v.x[j * v.ps], y = v.y[j * v.ps], g = v.g[j * v.ps];
             if (bf_near(p, x, y)) {
-                ++nnear;
-            } else {
-                const double zr = x - p.bc_x, zi = y - p.bc_y;
-                const double q = 1.0 / (zr * zr + zi * zi);
-                wr = zr * q; wi = -zi * q;          // w = 1 / (zj - c)
-                tr = -g * wr; ti = -g * wi;         // a_0 term: -G w
+                nnear += pass == 0;
+                continue;
+            }
+            const double zr = x - p.bc_x, zi = y - p.bc_y;
+            const double q = 1.0 / (zr * zr + zi * zi);
+            const double wr = zr * q, wi = -zi * q;   // w = 1 / (zj - c)
+            double tr = -g * wr, ti = -g * wi;        // a_0 term: -G w
+            if (pass == 1) {                          // times w^16
+                double pr = wr, pi = wi;
+#pragma unroll
+                for (int s2 = 0; s2 < 4; ++s2) {
+                    const double nr = pr * pr - pi * pi, ni = 2.0 * pr * pi;
+                    pr = nr; pi = ni;
+                }
+                const double nr = tr * pr - ti * pi, ni = tr * pi + ti * pr;
+                tr = nr; ti = ni;
+            }
+#pragma unroll
+            for (int l = 0; l < 16; ++l) {
+                acc[2 * l] += tr;
+                acc[2 * l + 1] += ti;
+                const double nr = tr * wr - ti * wi, ni = tr * wi + ti * wr;
+                tr = nr; ti = ni;
             }
         }
-        for (int l = 0; l < BF_P; ++l) {
-            double sr = tr, si = ti;
-            for (int o = 16; o > 0; o >>= 1) {
-                sr += __shfl_xor_sync(0xffffffffu, sr, o);
-                si += __shfl_xor_sync(0xffffffffu, si, o);
+#pragma unroll
+        for (int half = 16; half > 0; half >>= 1) {
+            const bool up = (lane & half) != 0;
+#pragma unroll
+            for (int i = 0; i < half; ++i) {
+                const double send = up ? acc[i] : acc[i + half];
+                const double keep = up ? acc[i + half] : acc[i];
+                acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
             }
-            if (lane == l) { ar += sr; ai += si; }
-            const double nr = tr * wr - ti * wi, ni = tr * wi + ti * wr;
-            tr = nr; ti = ni;
         }
+        sacc[wid][lane] = acc[0];
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double sum = 0.0;
+            for (int q = 0; q < BF_T / 32; ++q) sum += sacc[q][threadIdx.x];
+            // value q of this pass: coefficient 16 pass + q/2, part q&1
+            part[((long long)blockIdx.x * BF_P + 16 * pass + (threadIdx.x >> 1)) * 2 + (threadIdx.x & 1)] = sum;
+        }
+        __syncthreads();
     }
     for (int o = 16; o > 0; o >>= 1) nnear += __shfl_xor_sync(0xffffffffu, nnear, o);
-    sacc[wid][lane][0] = ar;
-    sacc[wid][lane][1] = ai;
     if (lane == 0) snear[wid] = nnear;
     __syncthreads();
-    if (threadIdx.x < BF_P) {
-        double sr = 0.0, si = 0.0;
-        for (int q = 0; q < BF_T / 32; ++q) { sr += sacc[q][threadIdx.x][0]; si += sacc[q][threadIdx.x][1]; }
-        part[((long long)blockIdx.x * BF_P + threadIdx.x) * 2 + 0] = sr;
-        part[((long long)blockIdx.x * BF_P + threadIdx.x) * 2 + 1] = si;
-    }
     if (threadIdx.x == 0) {
         int t = 0;
         for (int q = 0; q < BF_T / 32; ++q) t += snear[q];

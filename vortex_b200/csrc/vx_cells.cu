@@ -72,12 +72,24 @@ __global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double
 }
 
 // Cell side h = c * mean(d) / CG_DIV, grown until the grid fits cells_cap.
-__global__ void k_cg_params(VxScalars *S, const double *red, int nblocks, double cutoff, long long cells_cap) {
+// One block of CG_T threads: the per-block sums of d are added in a fixed
+// tree (reproducible), then thread 0 sizes the grid.
+__global__ void __launch_bounds__(CG_T) k_cg_params(VxScalars *S, const double *red, int nblocks, double cutoff,
+                                                    long long cells_cap) {
+    __shared__ double sd[CG_T];
+    double part = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += CG_T) part += red[b];
+    sd[threadIdx.x] = part;
+    __syncthreads();
+    for (int o = CG_T / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sd[threadIdx.x] += sd[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
     const long long n = S->n;
     S->cnitems = 0;
     if (n == 0) { S->cncells = 0; S->cnx = S->cny = 0; return; }
-    double dsum = 0.0;
-    for (int b = 0; b < nblocks; ++b) dsum += red[b];
+    const double dsum = sd[0];
     const double x0 = vx_dunkey(S->cb[0]), x1 = -vx_dunkey(S->cb[1]);
     const double y0 = vx_dunkey(S->cb[2]), y1 = -vx_dunkey(S->cb[3]);
     double h = cutoff * (dsum / (double)n) / (double)CG_DIV;
@@ -555,7 +567,7 @@ cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, cons
     const int grid = L.num_sms * 4;
     k_cg_begin<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
     k_cg_bbox<<<VX_RED_BLOCKS, CG_T, 0, L.stream>>>(v, S, w.red); VX_COUNT(L);
-    k_cg_params<<<1, 1, 0, L.stream>>>(S, w.red, VX_RED_BLOCKS, p.diff_cutoff, w.cells_cap); VX_COUNT(L);
+    k_cg_params<<<1, CG_T, 0, L.stream>>>(S, w.red, VX_RED_BLOCKS, p.diff_cutoff, w.cells_cap); VX_COUNT(L);
     k_cg_zero<<<grid, CG_T, 0, L.stream>>>(S, w.cg_cnt); VX_COUNT(L);
     k_cg_cellid<<<grid, CG_T, 0, L.stream>>>(v, S, w.key0, w.val0, w.cg_cnt); VX_COUNT(L);
     k_scan_sum<<<grid, CG_T, 0, L.stream>>>(&S->cncells, w.cg_cnt, w.cell_chunk_cnt); VX_COUNT(L);

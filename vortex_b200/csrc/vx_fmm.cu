@@ -253,28 +253,24 @@ __global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, c
                 pw = cscale(cmul(pw, w), c_fmm_inv[k + 1]);
             }
         }
+        // reduce-scatter over the warp: at each halving the lane keeps the half
+        // of its values selected by its lane bit and adds the partner's copy of
+        // it (31 shuffles instead of 160 for an all-reduce of 32 values);
+        // afterwards lane q holds value q = coefficient q/2, part q&1
+        double vv[2 * FMM_P];
 #pragma unroll
-        for (int k = 0; k < FMM_P; ++k) {
-            for (int o = 16; o > 0; o >>= 1) {
-                b[k].r += __shfl_xor_sync(0xffffffffu, b[k].r, o);
-                b[k].i += __shfl_xor_sync(0xffffffffu, b[k].i, o);
+        for (int k = 0; k < FMM_P; ++k) { vv[2 * k] = b[k].r; vv[2 * k + 1] = b[k].i; }
+#pragma unroll
+        for (int half = FMM_P; half > 0; half >>= 1) {
+            const bool up = (lane & half) != 0;
+#pragma unroll
+            for (int i = 0; i < half; ++i) {
+                const double send = up ? vv[i] : vv[i + half];
+                const double keep = up ? vv[i + half] : vv[i];
+                vv[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
             }
-            if (lane == k) ML[c * FMM_P + k] = b[k];
         }
-    }
-}
-
-// Counts of the leaf level summed into every coarser level.
-__global__ void k_fmm_count_up(const VxScalars *S, int *cnt, int l) {
-    if (l + 1 > S->fL) return;   // the depth is chosen on the device
-    const long long m = 1LL << l;
-    int *cl = cnt + fmm_level_off(l);
-    const int *ch = cnt + fmm_level_off(l + 1);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < m * m;
-         c += (long long)gridDim.x * blockDim.x) {
-        const long long ix = c % m, iy = c / m, m2 = 2 * m;
-        cl[c] = ch[(2 * iy) * m2 + 2 * ix] + ch[(2 * iy) * m2 + 2 * ix + 1] + ch[(2 * iy + 1) * m2 + 2 * ix] +
-                ch[(2 * iy + 1) * m2 + 2 * ix + 1];
+        reinterpret_cast<double *>(ML + c * FMM_P)[lane] = vv[0];
     }
 }
 
@@ -291,8 +287,9 @@ __device__ __forceinline__ void fmm_shift_table(cplx (*se)[FMM_P]) {
 }
 
 // M2M: parent at level l from its 4 children at level l+1, one thread per
-// (parent, coefficient k).
-__global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, const int *cnt, cplx *M, int l) {
+// (parent, coefficient k); the thread of coefficient 0 also writes the
+// parent's vortex count (the sum of its children's).
+__global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, cplx *M, int l) {
     __shared__ cplx se[4][FMM_P];
     if (l + 1 > S->fL) return;
     fmm_shift_table(se);
@@ -300,16 +297,19 @@ __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, const int *
     const long long m = 1LL << l, m2 = 2 * m;
     cplx *Mp = M + fmm_level_off(l) * FMM_P;
     const cplx *Mc = M + fmm_level_off(l + 1) * FMM_P;
-    const int *cp = cnt + fmm_level_off(l);
+    int *cp = cnt + fmm_level_off(l);
     const int *cc = cnt + fmm_level_off(l + 1);
     const long long tot = m * m * FMM_P;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
          e += (long long)gridDim.x * blockDim.x) {
         const long long c = e / FMM_P;
         const int k = (int)(e % FMM_P);
+        const long long ix = c % m, iy = c / m;
+        const int np = cc[(2 * iy) * m2 + 2 * ix] + cc[(2 * iy) * m2 + 2 * ix + 1] +
+                       cc[(2 * iy + 1) * m2 + 2 * ix] + cc[(2 * iy + 1) * m2 + 2 * ix + 1];
+        if (k == 0) cp[c] = np;
         cplx b = {0.0, 0.0};
-        if (cp[c] > 0) {
-            const long long ix = c % m, iy = c / m;
+        if (np > 0) {
             for (int q = 0; q < 4; ++q) {
                 const long long child = (2 * iy + (q >> 1)) * m2 + 2 * ix + (q & 1);
                 if (cc[child] == 0) continue;
@@ -731,9 +731,7 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     // the level loops cover the deepest level this capacity allows; kernels
     // of levels below the depth chosen on the device return at once
     for (int l = Lmax - 1; l >= 0; --l) {
-        const int g = (int)std::min<long long>(grid, vx_ceil_div(1LL << (2 * l), 128));
         const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));
-        k_fmm_count_up<<<g, 128, 0, L.stream>>>(S, w.fmm_cnt, l); VX_COUNT(L);
         k_fmm_m2m<<<gm, 128, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
     }
     for (int l = 2; l <= Lmax; ++l) {
