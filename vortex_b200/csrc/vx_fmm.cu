@@ -361,8 +361,13 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
     const int *cl = cnt + fmm_level_off(l);
     cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
     const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
-    const int lc = threadIdx.x % FMM_P;
+    // thread (cell, coefficient group cg, part pt): coefficients 4 cg .. 4 cg + 3
+    // over the interactions u = pt, pt + 4, ... of the cell's list; the four
+    // parts (adjacent lanes) are then reduce-scattered so part pt ends with
+    // coefficient lc = 4 cg + pt
     const int cell = threadIdx.x / FMM_P;
+    const int cg = (threadIdx.x % FMM_P) >> 2, pt = threadIdx.x & 3;
+    const int lc = 4 * cg + pt;
     for (long long t = blockIdx.x; t < tiles1 * tiles1; t += gridDim.x) {
         const long long tx0 = (t % tiles1) * M2L_TILE, ty0 = (t / tiles1) * M2L_TILE;
         const long long sx0 = tx0 - 2, sy0 = ty0 - 2;   // staged region origin
@@ -378,29 +383,50 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
         }
         __syncthreads();
         const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
-        if (ix >= m || iy >= m) continue;
-        const long long c = iy * m + ix;
-        cplx a = {0.0, 0.0};
-        if (cl[c] > 0) {
-            const long long px = ix >> 1, py = iy >> 1;
-            for (long long qy = max(0LL, 2 * (py - 1)); qy <= min(m - 1, 2 * (py + 1) + 1); ++qy) {
-                for (long long qx = max(0LL, 2 * (px - 1)); qx <= min(m - 1, 2 * (px + 1) + 1); ++qx) {
-                    if (llabs(qx - ix) <= 1 && llabs(qy - iy) <= 1) continue;   // neighbours: near field
-                    const int q = (int)((qy - sy0) * M2L_SRC + (qx - sx0));
-                    if (sc[q] == 0) continue;
-                    const cplx *H = sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + lc;   // H_{k+lc}
-                    const cplx *B = sm[q];
-                    double ar = 0.0, ai = 0.0;
+        const bool live = ix < m && iy < m;
+        const long long c = live ? iy * m + ix : 0;
+        const bool busy = live && cl[c] > 0;
+        const long long px = ix >> 1, py = iy >> 1;
+        double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // (re, im) of coefficients 4 cg + j
+        if (busy) {
+            for (int u = pt; u < 36; u += 4) {
+                const long long qy = 2 * (py - 1) + u / 6, qx = 2 * (px - 1) + u % 6;
+                if (qx < 0 || qx >= m || qy < 0 || qy >= m) continue;
+                if (llabs(qx - ix) <= 1 && llabs(qy - iy) <= 1) continue;   // neighbours: near field
+                const int q = (int)((qy - sy0) * M2L_SRC + (qx - sx0));
+                if (sc[q] == 0) continue;
+                const cplx *H = sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + 4 * cg;   // H_{k + 4 cg + j}
+                const cplx *B = sm[q];
+                cplx h0 = H[0], h1 = H[1], h2 = H[2], h3 = H[3];
 #pragma unroll
-                    for (int k = 0; k < FMM_P; ++k) {
-                        const cplx b = B[k], hh = H[k];
-                        ar = fma(b.r, hh.r, fma(-b.i, hh.i, ar));
-                        ai = fma(b.r, hh.i, fma(b.i, hh.r, ai));
-                    }
-                    a.r += ar;
-                    a.i += ai;
+                for (int k = 0; k < FMM_P; ++k) {
+                    const cplx b = B[k];
+                    v[0] = fma(b.r, h0.r, fma(-b.i, h0.i, v[0]));
+                    v[1] = fma(b.r, h0.i, fma(b.i, h0.r, v[1]));
+                    v[2] = fma(b.r, h1.r, fma(-b.i, h1.i, v[2]));
+                    v[3] = fma(b.r, h1.i, fma(b.i, h1.r, v[3]));
+                    v[4] = fma(b.r, h2.r, fma(-b.i, h2.i, v[4]));
+                    v[5] = fma(b.r, h2.i, fma(b.i, h2.r, v[5]));
+                    v[6] = fma(b.r, h3.r, fma(-b.i, h3.i, v[6]));
+                    v[7] = fma(b.r, h3.i, fma(b.i, h3.r, v[7]));
+                    if (k + 1 < FMM_P) { h0 = h1; h1 = h2; h2 = h3; h3 = H[k + 4]; }
                 }
             }
+        }
+        // reduce-scatter over the four parts (all lanes take part)
+#pragma unroll
+        for (int half = 4; half >= 2; half >>= 1) {
+            const bool up = (pt & (half >> 1)) != 0;
+#pragma unroll
+            for (int i = 0; i < half; ++i) {
+                const double send = up ? v[i] : v[i + half];
+                const double keep = up ? v[i + half] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half >> 1);
+            }
+        }
+        if (!live) continue;
+        cplx a = {v[0], v[1]};
+        if (busy) {
             a = cscale(a, ((lc & 1) ? -1.0 : 1.0) / s);
             if (l > 2) {
                 // L2L from the parent
