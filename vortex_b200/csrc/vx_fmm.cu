@@ -325,23 +325,34 @@ __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, c
 }
 
 // M2L at level l (2 <= l <= L) plus L2L from level l-1.  A block takes a
-// 4 x 4 tile of target cells (two parents wide), one thread per (cell,
-// coefficient); the interaction lists of the tile draw on the 8 x 8 source
-// cells around it (children of the parents' neighbours), whose multipoles
-// are staged once in shared memory.  The Hankel entries
-// H_j = j! t^-(j+1) of the 40 integer offsets t are tabulated per block.
+// 4 x 4 tile of target cells (two parents wide); the interaction lists of the
+// tile draw on the 8 x 8 source cells around it (children of the parents'
+// neighbours), whose multipoles are staged once in shared memory.  The
+// Hankel entries H_j = j! t^-(j+1) of the 40 integer offsets t are tabulated
+// per block.  Thread (cell, coefficient group cg, part pt) sums coefficients
+// 4 cg .. 4 cg + 3 over the interactions u = pt, pt + 4, ... of the cell's
+// list, with a sliding window over the Hankel entries (one shared load per
+// term for four coefficients); the four parts (adjacent lanes) are then
+// reduce-scattered, so part pt ends with coefficient lc = 4 cg + pt.
+//
+// The levels up to M2L_SMALL have few cells each: their M2L parts are
+// independent of one another and run in one launch over all their tiles
+// (k_fmm_m2l_small), then their L2L level by level (k_fmm_l2l_small); deeper
+// levels take one launch each (k_fmm_m2l_l2l), M2L and L2L together.
 constexpr int M2L_TILE = 4;
 constexpr int M2L_SRC = 2 * M2L_TILE;   // 8 x 8 staged source cells
 constexpr int M2L_T = M2L_TILE * M2L_TILE * FMM_P;
+constexpr int M2L_SMALL = 6;
 
-__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
-                                                       cplx *Loc, int l) {
-    __shared__ cplx sh[49][2 * FMM_P - 1];   // offset (dx, dy) in [-3, 3]^2 at (dy+3)*7 + dx+3
-    __shared__ cplx se[4][FMM_P];
-    __shared__ cplx sm[M2L_SRC * M2L_SRC][FMM_P];
-    __shared__ int sc[M2L_SRC * M2L_SRC];
-    if (l > S->fL) return;
-    fmm_shift_table(se);
+struct M2LShared {
+    cplx sh[49][2 * FMM_P - 1];   // offset (dx, dy) in [-3, 3]^2 at (dy+3)*7 + dx+3
+    cplx se[4][FMM_P];
+    cplx sm[M2L_SRC * M2L_SRC][FMM_P];
+    int sc[M2L_SRC * M2L_SRC];
+};
+
+__device__ void m2l_tables(M2LShared &T) {
+    fmm_shift_table(T.se);
     for (int q = threadIdx.x; q < 49; q += blockDim.x) {
         const int dx = q % 7 - 3, dy = q / 7 - 3;
         if (abs(dx) <= 1 && abs(dy) <= 1) continue;   // neighbours: never an interaction
@@ -349,95 +360,159 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
         cplx tp = ti;
         double fact = 1.0;   // j!
         for (int j = 0; j < 2 * FMM_P - 1; ++j) {
-            sh[q][j] = cscale(tp, fact);
+            T.sh[q][j] = cscale(tp, fact);
             tp = cmul(tp, ti);
             fact *= (double)(j + 1);
         }
     }
+}
+
+// M2L of tile t of level l for this thread's (cell, lc); the block's threads
+// all take part.  Returns whether the cell exists; *c its index, *busy
+// whether it holds vortices, *a its scaled M2L coefficient lc.
+__device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int l, long long t, M2LShared &T,
+                         long long &c, bool &busy, cplx &a) {
     const long long m = 1LL << l;
     const long long tiles1 = vx_ceil_div(m, (long long)M2L_TILE);
     const double s = S->fside / (double)m;
     const cplx *Ml = M + fmm_level_off(l) * FMM_P;
     const int *cl = cnt + fmm_level_off(l);
-    cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
-    const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
-    // thread (cell, coefficient group cg, part pt): coefficients 4 cg .. 4 cg + 3
-    // over the interactions u = pt, pt + 4, ... of the cell's list; the four
-    // parts (adjacent lanes) are then reduce-scattered so part pt ends with
-    // coefficient lc = 4 cg + pt
     const int cell = threadIdx.x / FMM_P;
     const int cg = (threadIdx.x % FMM_P) >> 2, pt = threadIdx.x & 3;
     const int lc = 4 * cg + pt;
+    const long long tx0 = (t % tiles1) * M2L_TILE, ty0 = (t / tiles1) * M2L_TILE;
+    const long long sx0 = tx0 - 2, sy0 = ty0 - 2;   // staged region origin
+    __syncthreads();   // the previous tile is done with sm / sc; tables are built
+    for (int e = threadIdx.x; e < M2L_SRC * M2L_SRC * FMM_P; e += blockDim.x) {
+        const int q = e / FMM_P, k = e % FMM_P;
+        const long long qx = sx0 + q % M2L_SRC, qy = sy0 + q / M2L_SRC;
+        const bool in = qx >= 0 && qx < m && qy >= 0 && qy < m;
+        const long long src = qy * m + qx;
+        const int n = in ? cl[src] : 0;
+        if (k == 0) T.sc[q] = n;
+        T.sm[q][k] = n > 0 ? Ml[src * FMM_P + k] : cplx{0.0, 0.0};
+    }
+    __syncthreads();
+    const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
+    const bool live = ix < m && iy < m;
+    c = live ? iy * m + ix : 0;
+    busy = live && cl[c] > 0;
+    const long long px = ix >> 1, py = iy >> 1;
+    double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // (re, im) of coefficients 4 cg + j
+    if (busy) {
+        for (int u = pt; u < 36; u += 4) {
+            const long long qy = 2 * (py - 1) + u / 6, qx = 2 * (px - 1) + u % 6;
+            if (qx < 0 || qx >= m || qy < 0 || qy >= m) continue;
+            if (llabs(qx - ix) <= 1 && llabs(qy - iy) <= 1) continue;   // neighbours: near field
+            const int q = (int)((qy - sy0) * M2L_SRC + (qx - sx0));
+            if (T.sc[q] == 0) continue;
+            const cplx *H = T.sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + 4 * cg;   // H_{k + 4 cg + j}
+            const cplx *B = T.sm[q];
+            cplx h0 = H[0], h1 = H[1], h2 = H[2], h3 = H[3];
+#pragma unroll
+            for (int k = 0; k < FMM_P; ++k) {
+                const cplx b = B[k];
+                v[0] = fma(b.r, h0.r, fma(-b.i, h0.i, v[0]));
+                v[1] = fma(b.r, h0.i, fma(b.i, h0.r, v[1]));
+                v[2] = fma(b.r, h1.r, fma(-b.i, h1.i, v[2]));
+                v[3] = fma(b.r, h1.i, fma(b.i, h1.r, v[3]));
+                v[4] = fma(b.r, h2.r, fma(-b.i, h2.i, v[4]));
+                v[5] = fma(b.r, h2.i, fma(b.i, h2.r, v[5]));
+                v[6] = fma(b.r, h3.r, fma(-b.i, h3.i, v[6]));
+                v[7] = fma(b.r, h3.i, fma(b.i, h3.r, v[7]));
+                if (k + 1 < FMM_P) { h0 = h1; h1 = h2; h2 = h3; h3 = H[k + 4]; }
+            }
+        }
+    }
+    // reduce-scatter over the four parts (all lanes take part)
+#pragma unroll
+    for (int half = 4; half >= 2; half >>= 1) {
+        const bool up = (pt & (half >> 1)) != 0;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const double send = up ? v[i] : v[i + half];
+            const double keep = up ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half >> 1);
+        }
+    }
+    a = {v[0], v[1]};
+    if (busy) a = cscale(a, ((lc & 1) ? -1.0 : 1.0) / s);
+    return live;
+}
+
+// L2L of coefficient lc of cell (ix, iy) of level l from its parent's local
+// expansion Lp (level l-1).
+__device__ __forceinline__ cplx l2l_term(const cplx *Lp, const cplx (*se)[FMM_P], long long m, long long ix,
+                                         long long iy, int lc) {
+    const long long parent = (iy >> 1) * (m >> 1) + (ix >> 1);
+    const int q = (int)((iy & 1) * 2 + (ix & 1));
+    cplx acc = {0.0, 0.0};
+    for (int j = lc; j < FMM_P; ++j) acc = cadd(acc, cmul(Lp[parent * FMM_P + j], se[q][j - lc]));
+    return cscale(acc, ldexp(1.0, -lc));
+}
+
+__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
+                                                       cplx *Loc, int l) {
+    __shared__ M2LShared T;
+    if (l > S->fL) return;
+    m2l_tables(T);
+    const long long m = 1LL << l;
+    const long long tiles1 = vx_ceil_div(m, (long long)M2L_TILE);
+    cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
+    const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
+    const int lc = threadIdx.x % FMM_P;   // = 4 cg + pt
     for (long long t = blockIdx.x; t < tiles1 * tiles1; t += gridDim.x) {
-        const long long tx0 = (t % tiles1) * M2L_TILE, ty0 = (t / tiles1) * M2L_TILE;
-        const long long sx0 = tx0 - 2, sy0 = ty0 - 2;   // staged region origin
-        __syncthreads();   // the previous tile is done with sm / sc; tables are built
-        for (int e = threadIdx.x; e < M2L_SRC * M2L_SRC * FMM_P; e += blockDim.x) {
-            const int q = e / FMM_P, k = e % FMM_P;
-            const long long qx = sx0 + q % M2L_SRC, qy = sy0 + q / M2L_SRC;
-            const bool in = qx >= 0 && qx < m && qy >= 0 && qy < m;
-            const long long src = qy * m + qx;
-            const int c = in ? cl[src] : 0;
-            if (k == 0) sc[q] = c;
-            sm[q][k] = c > 0 ? Ml[src * FMM_P + k] : cplx{0.0, 0.0};
-        }
-        __syncthreads();
-        const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
-        const bool live = ix < m && iy < m;
-        const long long c = live ? iy * m + ix : 0;
-        const bool busy = live && cl[c] > 0;
-        const long long px = ix >> 1, py = iy >> 1;
-        double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // (re, im) of coefficients 4 cg + j
-        if (busy) {
-            for (int u = pt; u < 36; u += 4) {
-                const long long qy = 2 * (py - 1) + u / 6, qx = 2 * (px - 1) + u % 6;
-                if (qx < 0 || qx >= m || qy < 0 || qy >= m) continue;
-                if (llabs(qx - ix) <= 1 && llabs(qy - iy) <= 1) continue;   // neighbours: near field
-                const int q = (int)((qy - sy0) * M2L_SRC + (qx - sx0));
-                if (sc[q] == 0) continue;
-                const cplx *H = sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + 4 * cg;   // H_{k + 4 cg + j}
-                const cplx *B = sm[q];
-                cplx h0 = H[0], h1 = H[1], h2 = H[2], h3 = H[3];
-#pragma unroll
-                for (int k = 0; k < FMM_P; ++k) {
-                    const cplx b = B[k];
-                    v[0] = fma(b.r, h0.r, fma(-b.i, h0.i, v[0]));
-                    v[1] = fma(b.r, h0.i, fma(b.i, h0.r, v[1]));
-                    v[2] = fma(b.r, h1.r, fma(-b.i, h1.i, v[2]));
-                    v[3] = fma(b.r, h1.i, fma(b.i, h1.r, v[3]));
-                    v[4] = fma(b.r, h2.r, fma(-b.i, h2.i, v[4]));
-                    v[5] = fma(b.r, h2.i, fma(b.i, h2.r, v[5]));
-                    v[6] = fma(b.r, h3.r, fma(-b.i, h3.i, v[6]));
-                    v[7] = fma(b.r, h3.i, fma(b.i, h3.r, v[7]));
-                    if (k + 1 < FMM_P) { h0 = h1; h1 = h2; h2 = h3; h3 = H[k + 4]; }
-                }
-            }
-        }
-        // reduce-scatter over the four parts (all lanes take part)
-#pragma unroll
-        for (int half = 4; half >= 2; half >>= 1) {
-            const bool up = (pt & (half >> 1)) != 0;
-#pragma unroll
-            for (int i = 0; i < half; ++i) {
-                const double send = up ? v[i] : v[i + half];
-                const double keep = up ? v[i + half] : v[i];
-                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half >> 1);
-            }
-        }
-        if (!live) continue;
-        cplx a = {v[0], v[1]};
-        if (busy) {
-            a = cscale(a, ((lc & 1) ? -1.0 : 1.0) / s);
-            if (l > 2) {
-                // L2L from the parent
-                const long long parent = py * (m >> 1) + px;
-                const int q = (int)((iy & 1) * 2 + (ix & 1));
-                cplx acc = {0.0, 0.0};
-                for (int j = lc; j < FMM_P; ++j) acc = cadd(acc, cmul(Lp[parent * FMM_P + j], se[q][j - lc]));
-                a = cadd(a, cscale(acc, ldexp(1.0, -lc)));
-            }
-        }
+        long long c;
+        bool busy;
+        cplx a;
+        if (!m2l_tile(S, cnt, M, l, t, T, c, busy, a)) continue;
+        if (busy && l > 2) a = cadd(a, l2l_term(Lp, T.se, m, c % m, c / m, lc));
         Ll[c * FMM_P + lc] = a;
+    }
+}
+
+// M2L (without L2L) of levels 2 .. min(M2L_SMALL, L): blocks over the tiles
+// of all of them.
+__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
+                                                         cplx *Loc) {
+    __shared__ M2LShared T;
+    const int hi = min(S->fL, M2L_SMALL);
+    if (hi < 2) return;
+    m2l_tables(T);
+    long long total = 0;
+    for (int l = 2; l <= hi; ++l) total += vx_ceil_div(1LL << (2 * l), (long long)(M2L_TILE * M2L_TILE));
+    const int lc = threadIdx.x % FMM_P;
+    for (long long b = blockIdx.x; b < total; b += gridDim.x) {
+        int l = 2;
+        long long t = b;
+        while (t >= vx_ceil_div(1LL << (2 * l), (long long)(M2L_TILE * M2L_TILE))) {
+            t -= vx_ceil_div(1LL << (2 * l), (long long)(M2L_TILE * M2L_TILE));
+            ++l;
+        }
+        long long c;
+        bool busy;
+        cplx a;
+        if (!m2l_tile(S, cnt, M, l, t, T, c, busy, a)) continue;
+        Loc[(fmm_level_off(l) + c) * FMM_P + lc] = a;
+    }
+}
+
+// L2L into level l (3 <= l <= min(M2L_SMALL, L)) from level l-1, one thread
+// per (cell, coefficient); one launch per level.
+__global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const int *cnt, cplx *Loc, int l) {
+    __shared__ cplx se[4][FMM_P];
+    if (l > min(S->fL, M2L_SMALL)) return;
+    fmm_shift_table(se);
+    __syncthreads();
+    const long long m = 1LL << l;
+    const int *cl = cnt + fmm_level_off(l);
+    cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
+    const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m * m * FMM_P;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long c = e / FMM_P;
+        const int lc = (int)(e % FMM_P);
+        if (cl[c] > 0) Ll[e] = cadd(Ll[e], l2l_term(Lp, se, m, c % m, c / m, lc));
     }
 }
 
@@ -760,7 +835,20 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
         const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));
         k_fmm_m2m<<<gm, 128, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
     }
-    for (int l = 2; l <= Lmax; ++l) {
+    {
+        long long tiles = 0;
+        for (int l = 2; l <= std::min(Lmax, M2L_SMALL); ++l) tiles += vx_ceil_div(1LL << (2 * l), 16LL);
+        if (tiles > 0) {
+            k_fmm_m2l_small<<<(int)std::min<long long>(grid * 2, tiles), M2L_T, 0, L.stream>>>(
+                S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L);
+            VX_COUNT(L);
+            for (int l = 3; l <= std::min(Lmax, M2L_SMALL); ++l) {
+                const int g = (int)std::min<long long>(grid, vx_ceil_div((1LL << (2 * l)) * FMM_P, 256));
+                k_fmm_l2l_small<<<g, 256, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_L, l); VX_COUNT(L);
+            }
+        }
+    }
+    for (int l = M2L_SMALL + 1; l <= Lmax; ++l) {
         const long long t1 = vx_ceil_div(1LL << l, (long long)M2L_TILE);
         const int g = (int)std::min<long long>(grid * 2, t1 * t1);
         k_fmm_m2l_l2l<<<g, M2L_T, 0, L.stream>>>(S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
