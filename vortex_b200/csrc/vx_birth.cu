@@ -521,10 +521,35 @@ extern "C" vx_status vx_eval_bulk_atan2(const float *y, const float *x, float *o
     return VX_OK;
 }
 
+// beta = ln(r1 / r0) / 2 for the bulk form.  With t = (r1 - r0) / (r1 + r0),
+// ln(r1 / r0) / 2 = atanh(t); r1 - r0 = 2 A + |d|^2 comes without
+// cancellation from the panel's own terms (num).  For |t| <= 1/4 (every
+// source more than about two panel lengths away) the Taylor series of atanh,
+// t (1 + t^2/3 + t^4/5 + ... + t^10/11), truncated below t^12/13 = 5e-9
+// relative; closer sources take logf of the ratio.
+__device__ __forceinline__ float vx_half_log_ratio(float r0, float r1, float num) {
+    const float den = r0 + r1;
+    float rc;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(den));
+    rc = fmaf(rc, fmaf(-den, rc, 1.0f), rc);   // one Newton step
+    const float t = num * rc;
+    if (fabsf(t) <= 0.25f) {
+        const float t2 = t * t;
+        float q = 1.0f / 11.0f;
+        q = fmaf(q, t2, 1.0f / 9.0f);
+        q = fmaf(q, t2, 1.0f / 7.0f);
+        q = fmaf(q, t2, 1.0f / 5.0f);
+        q = fmaf(q, t2, 1.0f / 3.0f);
+        q = fmaf(q, t2, 1.0f);
+        return t * q;
+    }
+    return 0.5f * logf(r1 / r0);
+}
+
 // Direct FP32 panel terms over the near list (chunked like k_rhs_partial).
 __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx_panel *pan, int P, int P32,
                                                     const float4 *near, double *part, int nchunks) {
-    __shared__ float sx[RHS_T], sy[RHS_T], sg[RHS_T];
+    __shared__ float4 sq4[RHS_T];   // (x, y, G, unused)
     const long long nn = S->bf_nnear;
     const long long cs = vx_ceil_div(vx_ceil_div(nn, nchunks), RHS_T) * RHS_T;
     const int tiles = (P + RHS_T - 1) / RHS_T;
@@ -546,23 +571,21 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx
         for (long long jt = j0; jt < j1; jt += RHS_T) {
             __syncthreads();
             const long long j = jt + threadIdx.x;
-            if (j < j1) {
-                const float4 q = near[j];
-                sx[threadIdx.x] = q.x; sy[threadIdx.x] = q.y; sg[threadIdx.x] = q.z;
-            }
+            if (j < j1) sq4[threadIdx.x] = near[j];
             __syncthreads();
             const int cnt = (int)min((long long)RHS_T, j1 - jt);
             for (int q = 0; q < cnt; ++q) {
-                float s00 = al0 - sx[q], s01 = al1 - sy[q];
+                const float4 src = sq4[q];
+                float s00 = al0 - src.x, s01 = al1 - src.y;
                 float s10 = s00 + d0, s11 = s01 + d1;
                 float A = fmaf(s00, d0, s01 * d1);
                 float B = fmaf(s10, d0, s11 * d1);
                 float z = fmaf(d0, s01, -(d1 * s00));
                 float alpha = vx_atan2_bulk(-dd2 * z, fmaf(z, z, A * B));
                 float r1 = fmaf(s10, s10, s11 * s11), r0 = fmaf(s00, s00, s01 * s01);
-                float beta = 0.5f * logf(r1 / r0);
-                y0 = fmaf(sg[q], fmaf(alpha, d0, beta * kd0), y0);
-                y1 = fmaf(sg[q], fmaf(alpha, d1, beta * kd1), y1);
+                float beta = vx_half_log_ratio(r0, r1, fmaf(2.0f, A, dd2));
+                y0 = fmaf(src.z, fmaf(alpha, d0, beta * kd0), y0);
+                y1 = fmaf(src.z, fmaf(alpha, d1, beta * kd1), y1);
             }
         }
         if (valid) {
