@@ -200,7 +200,10 @@ __global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *
     }
 }
 
-// COL[i] = smallest j > i in the 3x3 cell neighbourhood that qualifies.
+// COL[i] = smallest j > i in the 3x3 cell neighbourhood that qualifies.  The
+// targets are taken in cell order (i = sorted[k]), so neighbouring threads
+// read the same cells and sources; each target's answer does not depend on
+// the order.
 template <int PASS>
 __global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
                             const int *sorted, int *col, int *in_cnt, int *cand) {
@@ -208,8 +211,9 @@ __global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *celli
     const long long n = S->n;
     const long long gnx = S->gnx, gny = S->gny;
     const double rd2 = p.r_diff2, rs2 = p.r_same2, mvg = p.max_ve_g;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k0 < n;
+         k0 += (long long)gridDim.x * blockDim.x) {
+        const long long i = sorted[k0];
         const double xi = v.x[i * v.ps], yi = v.y[i * v.ps], gi = v.g[i * v.ps];
         const long long c = cellid[i];
         const long long cx = c % gnx, cy = c / gnx;

@@ -10,7 +10,10 @@
 // > 5 L_max) of the cell, in ascending panel order.  A panel left out is
 // farther than 5 L from the particle, so it would add nothing; the panels
 // kept are visited in the reference's order, so the sums and the first
-// r <= 0.1 L override are unchanged bit for bit.
+// r <= 0.1 L override are unchanged bit for bit.  The FP32 (bulk) form
+// evaluates the integral with reciprocals and MUFU rsqrt / ex2
+// (vx_wall_integral_bulk); the FP64 form follows the reference's expression
+// order.
 #include "vx_internal.cuh"
 
 template <typename T>
@@ -44,6 +47,31 @@ __device__ void vx_wall_integral(T Ra0, T Ra1, T Rb0, T Rb1, T N0, T N1, T Rj0, 
     R0 = s0; R30 = s30; R31 = s31;
 }
 
+// The bulk form's integral (FP32): the same midpoint rule with the
+// divisions by d and |E|^2 taken as products with reciprocals, |E| and
+// 1/|E| from one rsqrt, and e^-|E| as 2^(-|E| log2 e), all on the MUFU pipe.
+__device__ __forceinline__ void vx_wall_integral_bulk(float Ra0, float Ra1, float Rb0, float Rb1, float N0,
+                                                      float N1, float Rj0, float Rj1, float dL, float inv_d,
+                                                      int N, float &R0, float &R30, float &R31) {
+    const float invN = 1.0f / (float)N;
+    const float dR0 = (Rb0 - Ra0) * invN, dR1 = (Rb1 - Ra1) * invN;
+    const float delt = dL * invN;
+    float s0 = 0, s30 = 0, s31 = 0;
+    for (int k = 0; k < N; ++k) {
+        const float h = (float)k + 0.5f;
+        const float E0 = (Rj0 - fmaf(h, dR0, Ra0)) * inv_d, E1 = (Rj1 - fmaf(h, dR1, Ra1)) * inv_d;
+        const float e2 = fmaf(E0, E0, E1 * E1);
+        float rs, ex;
+        asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rs) : "f"(e2));
+        const float me = e2 * rs;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ex) : "f"(-1.4426950408889634f * me));
+        s0 = fmaf(fmaf(E0, N0, E1 * N1) * (rs * rs) * (me + 1.0f), ex, s0);
+        s30 = fmaf(N0, ex, s30);
+        s31 = fmaf(N1, ex, s31);
+    }
+    R0 = s0 * delt; R30 = s30 * delt; R31 = s31 * delt;
+}
+
 template <typename T>
 __global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel *pan, const int *wstart,
                        const int *widx) {
@@ -69,9 +97,14 @@ __global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel 
             T r = vx_sqrt<T>(fma(dx, dx, dy * dy));
             if (r < 5 * dL && r > (T)0.1 * dL) {
                 T R0, R30, R31;
-                vx_wall_integral<T>((T)pf.left[0], (T)pf.left[1], (T)pf.right[0], (T)pf.right[1],
-                                    -(T)pf.norm[0], -(T)pf.norm[1], a0, a1, dL, dd, p.n_of_points,
-                                    R0, R30, R31);
+                if constexpr (sizeof(T) == 4)
+                    vx_wall_integral_bulk((T)pf.left[0], (T)pf.left[1], (T)pf.right[0], (T)pf.right[1],
+                                          -(T)pf.norm[0], -(T)pf.norm[1], a0, a1, dL, 1.0f / dd, p.n_of_points,
+                                          R0, R30, R31);
+                else
+                    vx_wall_integral<T>((T)pf.left[0], (T)pf.left[1], (T)pf.right[0], (T)pf.right[1],
+                                        -(T)pf.norm[0], -(T)pf.norm[1], a0, a1, dL, dd, p.n_of_points,
+                                        R0, R30, R31);
                 I0 += (-dd) * R0;
                 I30 -= R30;
                 I31 -= R31;
