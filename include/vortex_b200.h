@@ -91,7 +91,7 @@ typedef struct vx_conf {
     int32_t fmm;                /* bulk form: Biot-Savart by the quadtree
                                    multipole method, and the birth
                                    right-hand side with the vortices beyond
-                                   twice the body radius through one local
+                                   1.5 body radii through one local
                                    expansion about the body (default 1);
                                    0 = direct sums */
     int32_t gj_pivot;           /* panel-system inversion: 0 = the reference's

@@ -152,8 +152,8 @@ def test_bulk_steps_track_fp64():
 
 
 def test_birth_far_field_vs_direct_and_fp64():
-    """Bulk birth with the far field (vortices beyond twice the body radius
-    through one 32-term expansion about the body centre) against the direct
+    """Bulk birth with the far field (vortices beyond 1.5 body radii through
+    one 48-term expansion about the body centre) against the direct
     FP32 and the FP64 right-hand side: born strengths within 1e-5 of the
     largest FP64 strength, and no worse than twice the direct FP32 error."""
     ck = conf_kwargs(1000, precision=N.PREC_FP32)

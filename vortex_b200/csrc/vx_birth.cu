@@ -322,17 +322,17 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_partial(VxView v, const VxScalars
 // dz = (tau_x + i tau_y) ds along it,
 //   mean (u, v) . tau = Re[ (1 / dz_panel) integral w dz ],
 //   integral_{za}^{zb} G / (2 pi i (z - zj)) dz.
-// For |zj - c| > 2 r_body (c: body centre) the kernel expands about c:
+// For |zj - c| > 1.5 r_body (c: body centre) the kernel expands about c:
 //   1 / (z - zj) = sum_l a_l (z - c)^l,  a_l = -1 / (zj - c)^(l+1),
 // and the panel integral of the series is exact:
 //   sum_l a_l [(zb - c)^(l+1) - (za - c)^(l+1)] / (l + 1).
-// On the panels |z - c| <= r_body, so the terms fall as 2^-l (32 terms:
-// 2e-10 relative).  Far coefficients: FP64, fixed-order block partials.
-// Near vortices (inside 2 r_body) keep the direct FP32 panel terms, over a
-// list compacted in index order.
+// On the panels |z - c| <= r_body, so the terms fall as (2/3)^l (48 terms:
+// the remainder below 3 (2/3)^49 = 7e-9 relative).  Far coefficients: FP64,
+// fixed-order block partials.  Near vortices (inside 1.5 r_body) keep the
+// direct FP32 panel terms, over a list compacted in index order.
 constexpr int BF_T = 256;
 constexpr int BF_P = VX_BF_P;
-static_assert(BF_P == 32, "one far-field coefficient per lane");
+static_assert(BF_P % 16 == 0, "16 far-field coefficients per pass");
 
 struct bcplx {
     double r, i;
@@ -353,8 +353,8 @@ __device__ __forceinline__ bool bf_near(const VxParams &p, double x, double y) {
 
 // Far-field coefficient partials (one per block, fixed order) and the
 // number of near sources of each block.  Each thread sums the terms of its
-// own sources in registers, 16 coefficients per pass (a_16..a_31 in the
-// second pass, from -G w^17 by squarings); then a reduce-scatter over the
+// own sources in registers, 16 coefficients per pass (a_16k .. a_16k+15 in
+// pass k, from -G w^(16k+1), w^16 by squarings); then a reduce-scatter over the
 // warp (at each halving a lane keeps the half of its values selected by its
 // lane bit and adds the partner's copy: lane q ends with value q, i.e.
 // coefficient q/2, part q&1) and a fixed-order sum over the block's warps.
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxS
     long long j0, j1;
     bf_chunk(S, gridDim.x, blockIdx.x, j0, j1);
     int nnear = 0;
-    for (int pass = 0; pass < 2; ++pass) {
+    for (int pass = 0; pass < BF_P / 16; ++pass) {
         double acc[32];   // (re, im) of the pass's 16 coefficients
 #pragma unroll
         for (int k = 0; k < 32; ++k) acc[k] = 0.0;
@@ -379,15 +379,17 @@ __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxS
             const double q = 1.0 / (zr * zr + zi * zi);
             const double wr = zr * q, wi = -zi * q;   // w = 1 / (zj - c)
             double tr = -g * wr, ti = -g * wi;        // a_0 term: -G w
-            if (pass == 1) {                          // times w^16
+            if (pass > 0) {                           // times w^(16 pass)
                 double pr = wr, pi = wi;
 #pragma unroll
                 for (int s2 = 0; s2 < 4; ++s2) {
                     const double nr = pr * pr - pi * pi, ni = 2.0 * pr * pi;
                     pr = nr; pi = ni;
                 }
-                const double nr = tr * pr - ti * pi, ni = tr * pi + ti * pr;
-                tr = nr; ti = ni;
+                for (int k = 0; k < pass; ++k) {
+                    const double nr = tr * pr - ti * pi, ni = tr * pi + ti * pr;
+                    tr = nr; ti = ni;
+                }
             }
 #pragma unroll
             for (int l = 0; l < 16; ++l) {

@@ -155,7 +155,7 @@ void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams 
         for (int i = 0; i < P; ++i)
             for (const double *e : {pan[i].left, pan[i].right})
                 r2 = std::max(r2, (e[0] - p->bc_x) * (e[0] - p->bc_x) + (e[1] - p->bc_y) * (e[1] - p->bc_y));
-        p->b_rfar2 = 4.0 * r2 * (1.0 + 1e-12);
+        p->b_rfar2 = VX_BF_RHO * VX_BF_RHO * r2 * (1.0 + 1e-12);
         p->birth_far = (c->precision == VX_PREC_FP32 && c->fmm) ? 1 : 0;
     }
     p->fmm_leaf = c->fmm_leaf > 0 ? c->fmm_leaf : 32;

@@ -284,7 +284,8 @@ long long vx_work_bytes(long long cap, int P32, int num_sms);
 long long vx_rs_tiles_cap(long long cap);
 int vx_fmm_max_level(long long cap);
 long long vx_fmm_cells(int lmax);         // cells of all levels 0..lmax
-constexpr int VX_BF_P = 32;          // terms of the birth far-field expansion
+constexpr int VX_BF_P = 48;          // terms of the birth far-field expansion
+constexpr double VX_BF_RHO = 1.5;    // far-field sources lie beyond VX_BF_RHO body radii of its centre
 constexpr int VX_BF_MAX_BLOCKS = 1024;
 constexpr int VX_FMM_P = 16;              // expansion terms (vx_fmm.cu)
 cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
