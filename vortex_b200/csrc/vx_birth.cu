@@ -429,18 +429,42 @@ __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxS
     }
 }
 
-// Block-count offsets and the coefficient sums (block order), one block.
-__global__ void k_bf_scan(VxScalars *S, int nb, const int *cnt, long long *off, const double *part,
-                          double *coef) {
-    __shared__ long long sh[VX_BF_MAX_BLOCKS];
-    const int t = threadIdx.x;
-    for (int b = t; b < nb; b += blockDim.x) sh[b] = cnt[b];
+// Block-count offsets and the coefficient sums (block order), one block of
+// BF_SCAN_T threads: thread t scans the counts of blocks BF_SCAN_PER t ..,
+// then a warp and block scan of the thread totals.
+constexpr int BF_SCAN_T = 256;
+constexpr int BF_SCAN_PER = VX_BF_MAX_BLOCKS / BF_SCAN_T;
+static_assert(BF_SCAN_PER * BF_SCAN_T == VX_BF_MAX_BLOCKS, "whole blocks per scan thread");
+__global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, const int *cnt, long long *off,
+                                                       const double *part, double *coef) {
+    __shared__ long long wsum[BF_SCAN_T / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    long long c[BF_SCAN_PER], tot = 0;
+    for (int q = 0; q < BF_SCAN_PER; ++q) {
+        const int b = BF_SCAN_PER * t + q;
+        c[q] = b < nb ? cnt[b] : 0;
+        tot += c[q];
+    }
+    long long inc = tot;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) wsum[warp] = inc;
     __syncthreads();
+    long long run = inc - tot, all = 0;
+    for (int q = 0; q < BF_SCAN_T / 32; ++q) {
+        run += q < warp ? wsum[q] : 0;
+        all += wsum[q];
+    }
+    for (int q = 0; q < BF_SCAN_PER; ++q) {
+        const int b = BF_SCAN_PER * t + q;
+        if (b < nb) off[b] = run;
+        run += c[q];
+    }
     if (t == 0) {
-        long long run = 0;
-        for (int b = 0; b < nb; ++b) { off[b] = run; run += sh[b]; }
-        off[nb] = run;
-        S->bf_nnear = run;
+        off[nb] = all;
+        S->bf_nnear = all;
     }
     if (t < 2 * BF_P) {
         double acc = 0.0;
@@ -599,14 +623,30 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx
 
 // R_i = -(mean velocity along panel i + V_inf) . tau_i; the far field (if
 // coef) adds Re[I_far (tau_x + i tau_y) / (2 pi i dz)] with dz = zb - za.
+// WARP: one warp per panel, its lanes summing the chunk partials (bulk form,
+// fixed butterfly); otherwise one thread per panel in chunk order.
+template <bool WARP>
 __global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int P32,
                             const double *part, int nchunks, double *R, VxParams p, const double *coef) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = WARP ? (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) : blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double y0 = 0.0, y1 = 0.0;
-    for (int sc = 0; sc < nchunks; ++sc) {
-        y0 += part[((long long)sc * P32 + i) * 2 + 0];
-        y1 += part[((long long)sc * P32 + i) * 2 + 1];
+    if (WARP) {
+        const int lane = threadIdx.x & 31;
+        for (int sc = lane; sc < nchunks; sc += 32) {
+            y0 += part[((long long)sc * P32 + i) * 2 + 0];
+            y1 += part[((long long)sc * P32 + i) * 2 + 1];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            y0 += __shfl_xor_sync(0xffffffffu, y0, o);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, o);
+        }
+        if (lane != 0) return;
+    } else {
+        for (int sc = 0; sc < nchunks; ++sc) {
+            y0 += part[((long long)sc * P32 + i) * 2 + 0];
+            y1 += part[((long long)sc * P32 + i) * 2 + 1];
+        }
     }
     double d0 = pan[i].right[0] - pan[i].left[0], d1 = pan[i].right[1] - pan[i].left[1];
     double mnog = 1.0 / (VX_TWO_PI * (d0 * d0 + d1 * d1));
@@ -732,7 +772,7 @@ static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView
     if (far) {
         const int nb = std::min(2 * L.num_sms, VX_BF_MAX_BLOCKS);
         k_bf_far<<<nb, BF_T, 0, L.stream>>>(p, v, S, w.bf_part, w.bf_cnt); VX_COUNT(L);
-        k_bf_scan<<<1, 256, 0, L.stream>>>(S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef); VX_COUNT(L);
+        k_bf_scan<<<1, BF_SCAN_T, 0, L.stream>>>(S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef); VX_COUNT(L);
         k_bf_scatter<<<nb, BF_T, 0, L.stream>>>(p, v, S, w.bf_off, w.bf_near); VX_COUNT(L);
         k_rhs_near<<<grid, RHS_T, 0, L.stream>>>(S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
     } else if (p.prec == VX_PREC_FP32) {
@@ -742,8 +782,11 @@ static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView
     }
     VX_COUNT(L);
     const int b = (P + 127) / 128;
-    k_rhs_final<<<b, 128, 0, L.stream>>>(S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p,
-                                         far ? w.bf_coef : nullptr);
+    if (far)
+        k_rhs_final<true><<<(P + 3) / 4, 128, 0, L.stream>>>(S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p,
+                                                             w.bf_coef);
+    else
+        k_rhs_final<false><<<b, 128, 0, L.stream>>>(S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, nullptr);
     VX_COUNT(L);
     if (minv_t && p.prec == VX_PREC_FP32)
         k_gamma_w<<<(P + 3) / 4, 128, 0, L.stream>>>(S, minv, ld, P, w.R, w.gamma);
