@@ -167,6 +167,15 @@ vx_status vx_stage(vx_sim *sim, unsigned stage_mask);
 vx_status vx_probe(vx_sim *sim, const double *px, const double *py, int64_t np,
                    double *vx, double *vy);
 
+/* Tracer points moved one time step with the velocities (u, v): the
+ * convection of the tracers in first_speed / second_speed
+ * (src/unit_1.cu:1271-1340, the vortices' step kernel without force terms).
+ * A point that crosses the wall gets g = 0; one that leaves the window is
+ * moved to (-2e5, -2e5) with g = 0.  Host arrays in and out; the body's
+ * vortices and force sums are not changed. */
+vx_status vx_move_points(vx_sim *sim, double *x, double *y, double *g, const double *u,
+                         const double *v, int64_t n);
+
 /* Record every step into a CUDA graph after the first call and replay it
  * (on by default; 0 turns it off). */
 vx_status vx_set_graph(vx_sim *sim, int enable);

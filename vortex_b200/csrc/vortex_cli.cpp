@@ -19,9 +19,19 @@
 //                               matrix_load 1 the inverse is read from M.txt
 // Each step runs as three device stages (birth; velocity with both
 // diffusions; convection, compaction and collapse) with the outputs in
-// between, as the reference orders them.  Tracer runs (second_points_file,
-// steady_flow) are not driven here: they need the reference's own driver
-// linked against this library.
+// between, as the reference orders them.
+//
+// Tracers (second_points_file, with rel_t): two copies of the points file are
+// carried, inertial ("second": velocity relaxed towards the carrier velocity
+// with time constant rel_t) and passive ("first": moved with the carrier
+// velocity), each step after the outputs and before the vortices' velocity;
+// they are written to output/second and output/first on saving steps and at
+// the end, their velocities to output/vels/Vel%06d_4.txt (carrier) and
+// _5.txt (as the reference: the passive set's file replaces the inertial
+// set's), and reloaded from output/second and output/first on a restart when
+// both frames of the start step exist (src/main.c:480-505, 606-648, 731-752).
+// steady_flow: the vortices stay as loaded (no birth, velocity or
+// convection, no vortex outputs); only the tracers move.
 #include <sys/stat.h>
 
 #include <cerrno>
@@ -87,6 +97,35 @@ bool save_kadr(vx_sim *s, int step) {
     return true;
 }
 
+bool save_points(const char *folder, int step, const std::vector<double> &x, const std::vector<double> &y,
+                 const std::vector<double> &g) {
+    char name[256];
+    std::snprintf(name, sizeof(name), "output/%s/Kadr%06d.txt", folder, step);
+    FILE *f = std::fopen(name, "w");
+    if (!f) { logm(0, "cannot open %s: %s", name, std::strerror(errno)); return false; }
+    std::fprintf(f, "%zu\n", x.size());
+    for (size_t i = 0; i < x.size(); ++i)
+        std::fprintf(f, "%zu %lf %lf %lf %lf %lf %lf %lf\n", i, 0.008, x[i], y[i], 0.0, 0.0, 0.0, g[i]);
+    std::fclose(f);
+    return true;
+}
+
+void save_vel(int step, int stage, const std::vector<double> &x, const std::vector<double> &y,
+              const std::vector<double> &u, const std::vector<double> &v) {
+    char name[256];
+    std::snprintf(name, sizeof(name), "output/vels/Vel%06d_%d.txt", step, stage);
+    FILE *f = std::fopen(name, "w");
+    if (!f) return;
+    std::fprintf(f, "%zu\n", x.size());
+    for (size_t i = 0; i < x.size(); ++i) std::fprintf(f, "%zu %lf %lf %lf %lf\n", i, x[i], y[i], u[i], v[i]);
+    std::fclose(f);
+}
+
+bool file_exists(const char *name) {
+    struct stat st;
+    return stat(name, &st) == 0 && !S_ISDIR(st.st_mode);
+}
+
 bool load_kadr(const char *name, std::vector<double> &x, std::vector<double> &y, std::vector<double> &g) {
     FILE *f = std::fopen(name, "r");
     if (!f) { logm(0, "cannot open %s: %s", name, std::strerror(errno)); return false; }
@@ -124,11 +163,17 @@ int main(int argc, char **argv) {
     vx_conf c;
     vx_conf_default(&c);
     if (!check(vx_conf_read(cfg.c_str(), &c), "reading the configuration")) return 1;
-    if (c.second_points_file[0] || c.steady_flow) {
-        logm(0, "tracer runs (second_points_file, steady_flow) need the reference driver linked "
-                "against this library");
+    // tracers: inertial (second) and passive (first) copies of the points
+    std::vector<double> x2, y2, g2, x1, y1, g1;
+    if (c.second_points_file[0]) {
+        if (c.rel_t == 0.0) { logm(0, "rel_t is necessary if the second component is set"); return 1; }
+        if (!load_kadr(c.second_points_file, x2, y2, g2)) return 1;
+        x1 = x2; y1 = y2; g1 = g2;
+    } else if (c.steady_flow) {
+        logm(0, "steady_flow and no second component");
         return 1;
     }
+    const bool steady = c.steady_flow != 0;
     for (const char *d : {"output", "output/kadrs", "output/vels", "output/second", "output/first"})
         if (!ensure_dir(d)) { logm(0, "cannot create %s", d); return 1; }
 
@@ -176,6 +221,21 @@ int main(int argc, char **argv) {
         }
     }
     if (!check(vx_set_step_index(sim, first), "vx_set_step_index")) return 1;
+    if (steady && (int64_t)first < c.v_inf_incr_steps) {
+        logm(0, "steady_flow while the V_inf ramp (v_inf_incr_steps) is still running is not driven here");
+        return 1;
+    }
+    if (first && !x2.empty()) {   // restart: the tracer frames of the start step, if both were saved
+        char sname[256], fname[256];
+        std::snprintf(sname, sizeof(sname), "output/second/Kadr%06d.txt", first);
+        std::snprintf(fname, sizeof(fname), "output/first/Kadr%06d.txt", first);
+        if (file_exists(sname) && file_exists(fname)) {
+            if (!load_kadr(sname, x2, y2, g2) || !load_kadr(fname, x1, y1, g1)) return 1;
+            if (x1.size() != x2.size()) { logm(0, "%s and %s hold different counts", sname, fname); return 1; }
+        }
+    }
+    const size_t nt = x2.size();
+    std::vector<double> ue(nt), ve(nt), u2(nt, 0.0), v2(nt, 0.0), u1(nt), v1(nt);
 
     const int NC = 500;
     std::vector<double> cpx(NC), cpy(NC);
@@ -186,21 +246,23 @@ int main(int argc, char **argv) {
 
     FILE *tim = c.timings_file[0] ? std::fopen(c.timings_file, "w") : stdout;
     if (!tim) { logm(0, "cannot open %s", c.timings_file); return 1; }
-    FILE *fp = std::fopen("output/F_p.txt", "w");
-    if (!fp) { logm(0, "unable to output forces: %s", std::strerror(errno)); return 1; }
+    FILE *fp = steady ? nullptr : std::fopen("output/F_p.txt", "w");   // no forces in a steady-flow run
+    if (!steady && !fp) { logm(0, "unable to output forces: %s", std::strerror(errno)); return 1; }
 
     double t_birth = 0.0, t_speed = 0.0, t_step = 0.0;
     double f[4];
     int64_t n = 0;
     for (int k = first; k < steps; ++k) {
         double t0 = now_s();
-        if (!check(vx_stage(sim, VX_STAGE_BIRTH), "birth")) return 1;
-        t_birth += now_s() - t0;
+        if (!steady) {
+            if (!check(vx_stage(sim, VX_STAGE_BIRTH), "birth")) return 1;
+            t_birth += now_s() - t0;
+        }
         vx_get_count(sim, &n);
         std::fprintf(tim, "%d\tN = %zu\tCreation time = %f\tSpeed time = %f\tStep time = %f\n", k, (size_t)n,
                      t_birth, t_speed, t_step);
         std::fflush(tim);
-        if ((size_t)k % saving == 0) {
+        if ((size_t)k % saving == 0 && !steady) {
             char name[256];
             std::snprintf(name, sizeof(name), "output/vels/contr_Vel%06d.txt", k);
             FILE *o = std::fopen(name, "w");
@@ -211,6 +273,38 @@ int main(int argc, char **argv) {
             }
             vc_blocks = 0;
             if (!save_kadr(sim, k)) return 1;
+        }
+        if ((size_t)k % saving == 0 && nt) {
+            if (!save_points("second", k, x2, y2, g2) || !save_points("first", k, x1, y1, g1)) return 1;
+        }
+        if (nt) {
+            // inertial tracers: carrier velocity, relaxation towards it (the
+            // previous velocity taken in FP32, as the reference), convection
+            if (!check(vx_probe(sim, x2.data(), y2.data(), (int64_t)nt, ue.data(), ve.data()), "tracer velocity"))
+                return 1;
+            if (k == first) { u2 = ue; v2 = ve; }
+            save_vel(k, 4, x2, y2, ue, ve);
+            for (size_t i = 0; i < nt; ++i) {
+                if (g2[i] == 0.0) { u2[i] = 0.0; v2[i] = 0.0; continue; }
+                const float pu = (float)u2[i], pv = (float)v2[i];
+                u2[i] = (ue[i] - pu) / c.rel_t * c.dt + pu;
+                v2[i] = (ve[i] - pv) / c.rel_t * c.dt + pv;
+            }
+            save_vel(k, 5, x2, y2, u2, v2);
+            if (!check(vx_move_points(sim, x2.data(), y2.data(), g2.data(), u2.data(), v2.data(), (int64_t)nt),
+                       "tracer convection"))
+                return 1;
+            // passive tracers
+            if (!check(vx_probe(sim, x1.data(), y1.data(), (int64_t)nt, u1.data(), v1.data()), "tracer velocity"))
+                return 1;
+            save_vel(k, 5, x1, y1, u1, v1);
+            if (!check(vx_move_points(sim, x1.data(), y1.data(), g1.data(), u1.data(), v1.data(), (int64_t)nt),
+                       "tracer convection"))
+                return 1;
+        }
+        if (steady) {
+            if (!check(vx_set_step_index(sim, k + 1), "vx_set_step_index")) return 1;
+            continue;
         }
         if (vc_blocks < saving) {
             if (!check(vx_probe(sim, cpx.data(), cpy.data(), NC, &vcx[vc_blocks * NC], &vcy[vc_blocks * NC]),
@@ -234,10 +328,14 @@ int main(int argc, char **argv) {
     vx_get_count(sim, &n);
     std::fprintf(tim, "%d\tN = %zu\tCreation time = %f\tSpeed time = %f\tStep time = %f\n", (int)steps, (size_t)n,
                  t_birth, t_speed, t_step);
-    if (!save_kadr(sim, (int)steps)) return 1;
-    vx_get_forces(sim, f);
-    std::fprintf(fp, "%d %lf %lf %lf\n", (int)steps, f[1], f[2], f[3]);
-    std::fclose(fp);
+    if (!steady) {
+        if (!save_kadr(sim, (int)steps)) return 1;
+        vx_get_forces(sim, f);
+        std::fprintf(fp, "%d %lf %lf %lf\n", (int)steps, f[1], f[2], f[3]);
+    }
+    if (fp) std::fclose(fp);
+    if (nt && (!save_points("second", (int)steps, x2, y2, g2) || !save_points("first", (int)steps, x1, y1, g1)))
+        return 1;
     if (tim != stdout) std::fclose(tim);
     vx_destroy(sim);
     if (g_log) std::fclose(g_log);

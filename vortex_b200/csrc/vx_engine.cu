@@ -87,6 +87,12 @@ struct vx_sim {
     // probe scratch
     double *d_probe = nullptr;
     long long probe_cap = 0;
+    // moved-point scratch (vx_move_points): x, y, g, u, v; own scalars and
+    // block partials, so the body's force sums stay as they are
+    double *d_pts = nullptr;
+    long long pts_cap = 0;
+    VxScalars *d_St = nullptr;
+    double *d_pred = nullptr;
 };
 
 static VxLaunch launch_of(vx_sim *s) {
@@ -533,6 +539,9 @@ extern "C" vx_status vx_destroy(vx_sim *s) {
     if (s->d_S) cudaFree(s->d_S);
     if (s->h_S) cudaFreeHost(s->h_S);
     if (s->d_probe) cudaFree(s->d_probe);
+    if (s->d_pts) cudaFree(s->d_pts);
+    if (s->d_St) cudaFree(s->d_St);
+    if (s->d_pred) cudaFree(s->d_pred);
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
     for (auto &e : s->pev) if (e) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -963,6 +972,52 @@ extern "C" vx_status vx_set_fmm(vx_sim *s, int fmm, int leaf) {
 
 // The stream the handle launches on (for callers that time with events).
 extern "C" void *vx_get_stream(vx_sim *s) { return s ? (void *)s->stream : nullptr; }
+
+__global__ void k_points_begin(VxScalars *S, long long n) {
+    S->n = n;
+    S->n0 = n;   // no point counts as born this step: no force terms
+}
+
+// Passive points (tracers) moved one time step with the given velocities by
+// the vortices' convection kernel: the same wall absorption (g set to 0) and
+// window removal (moved to -2e5, g = 0), no force terms, and the body's own
+// state and force sums untouched.  Host arrays in and out.
+extern "C" vx_status vx_move_points(vx_sim *s, double *x, double *y, double *g, const double *u,
+                                    const double *v, int64_t n) {
+    if (!s || n < 0 || (n > 0 && (!x || !y || !g || !u || !v))) return VX_ERR_ARG;
+    if (n == 0) return VX_OK;
+    CU(cudaSetDevice(s->device));
+    if (!s->d_St) {
+        CU(cudaMalloc(&s->d_St, sizeof(VxScalars)));
+        CU(cudaMemset(s->d_St, 0, sizeof(VxScalars)));
+        CU(cudaMalloc(&s->d_pred, sizeof(double) * 4 * VX_RED_BLOCKS));
+    }
+    if (s->pts_cap < n) {
+        if (s->d_pts) cudaFree(s->d_pts);
+        s->d_pts = nullptr;
+        s->pts_cap = 0;
+        CU(cudaMalloc(&s->d_pts, sizeof(double) * 5 * n));
+        s->pts_cap = n;
+    }
+    double *dx = s->d_pts, *dy = dx + n, *dg = dy + n, *du = dg + n, *dv = du + n;
+    const double *src[5] = {x, y, g, u, v};
+    double *dst[5] = {dx, dy, dg, du, dv};
+    for (int q = 0; q < 5; ++q)
+        CU(cudaMemcpyAsync(dst[q], src[q], sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+    k_points_begin<<<1, 1, 0, s->stream>>>(s->d_St, (long long)n);
+    VxView pv;
+    pv.x = dx; pv.y = dy; pv.g = dg; pv.ps = 1;
+    pv.vx = du; pv.vy = dv; pv.vs = 1;
+    pv.d = nullptr;
+    VxWork tw = s->w;
+    tw.red = s->d_pred;
+    CU(vx_launch_advect(launch_of(s), s->prm, pv, s->d_St, tw, s->d_pan, s->d_hstart, s->d_hidx));
+    CU(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(g, dg, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}
 
 extern "C" vx_status vx_probe(vx_sim *s, const double *px, const double *py, int64_t np, double *ovx,
                               double *ovy) {

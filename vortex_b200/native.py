@@ -230,6 +230,15 @@ class Sim:
         _check(lib().vx_probe(self.h, _p(px), _p(py), C.c_int64(len(px)), _p(vx), _p(vy)), "vx_probe")
         return vx, vy
 
+    def move_points(self, x, y, g, u, v):
+        """Tracer points moved one step with velocities (u, v); returns new
+        (x, y, g), g = 0 for points absorbed by the wall or the window."""
+        x, y, g = _f64(x).copy(), _f64(y).copy(), _f64(g).copy()
+        u, v = _f64(u), _f64(v)
+        _check(lib().vx_move_points(self.h, _p(x), _p(y), _p(g), _p(u), _p(v), C.c_int64(len(x))),
+               "vx_move_points")
+        return x, y, g
+
     def set_graph(self, on: bool):
         _check(lib().vx_set_graph(self.h, C.c_int(int(on))), "vx_set_graph")
 
