@@ -167,6 +167,16 @@ vx_status vx_stage(vx_sim *sim, unsigned stage_mask);
 vx_status vx_probe(vx_sim *sim, const double *px, const double *py, int64_t np,
                    double *vx, double *vy);
 
+/* Binary checkpoint of a body at full precision (no counterpart in the
+ * reference, whose restart frames, src/main.c:175-188 and 558-605, keep six
+ * decimals and lose d_g, the forces and the V_inf ramp): the vortices, the
+ * step index, the current V_inf, d_g and the last forces.  A body continued
+ * from a checkpoint steps exactly as the one that wrote it.  Loading checks
+ * the panel count, the form and a hash of the panels (VX_ERR_ARG on a
+ * mismatch or a damaged file). */
+vx_status vx_checkpoint_save(vx_sim *sim, const char *path);
+vx_status vx_checkpoint_load(vx_sim *sim, const char *path);
+
 /* Tracer points moved one time step with the velocities (u, v): the
  * convection of the tracers in first_speed / second_speed
  * (src/unit_1.cu:1271-1340, the vortices' step kernel without force terms).

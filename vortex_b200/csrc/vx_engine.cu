@@ -7,6 +7,8 @@
 // when the store may have to grow.  A step is launched as a fixed sequence,
 // so after the first call it is recorded into a CUDA graph and replayed.
 #include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -711,6 +713,105 @@ extern "C" vx_status vx_set_matrix(vx_sim *s, const double *minv) {
     const long long S1 = s->P + 1;
     CU(cudaMemcpy(s->d_minv, minv, sizeof(double) * S1 * S1, cudaMemcpyHostToDevice));
     CU(vx_transpose_square(launch_of(s), s->d_minv, s->d_minvT, S1));
+    CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Binary checkpoint of a body: what the next step reads from the previous
+// ones, at full precision (the reference's text frames keep 6 decimals and
+// drop d_g, the forces and the V_inf ramp): every slot (x, y, G in FP64) up
+// to the capacity, the tail beyond the live vortices included (the plain
+// form's 3-nearest search reads the round-up slots after the live ones, as
+// the reference's does), the step index, the current V_inf, d_g and the
+// last forces with their raw sums.  The file names the body it belongs to by its panel count, its form
+// (FP64 / FP32) and a hash of its panels; loading into another body fails.
+namespace {
+struct CkptHead {
+    char magic[8];           // "VXCKPT1"
+    int32_t version, P, prec, pad;
+    int64_t n, n0, step, slots;
+    double vinf[2], dg, fx, fy, m, raw[4];
+    uint64_t panel_hash;     // FNV-1a of the panel records
+};
+const char kCkptMagic[8] = {'V', 'X', 'C', 'K', 'P', 'T', '1', 0};
+
+vx_status panel_hash(vx_sim *s, uint64_t *h) {
+    std::vector<vx_panel> pan((size_t)s->P);
+    CU(cudaMemcpy(pan.data(), s->d_pan, sizeof(vx_panel) * (size_t)s->P, cudaMemcpyDeviceToHost));
+    uint64_t v = 1469598103934665603ull;
+    const unsigned char *b = reinterpret_cast<const unsigned char *>(pan.data());
+    for (size_t i = 0; i < sizeof(vx_panel) * pan.size(); ++i) { v ^= b[i]; v *= 1099511628211ull; }
+    *h = v;
+    return VX_OK;
+}
+}  // namespace
+
+extern "C" vx_status vx_checkpoint_save(vx_sim *s, const char *path) {
+    if (!s || !path) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    vx_status st = read_scalars(s);
+    if (st != VX_OK) return st;
+    const VxScalars h = *s->h_S;
+    CkptHead hd;
+    memset(&hd, 0, sizeof(hd));
+    memcpy(hd.magic, kCkptMagic, 8);
+    hd.version = 1; hd.P = s->P; hd.prec = s->prm.prec;
+    hd.n = h.n; hd.n0 = h.n0; hd.step = h.step; hd.slots = s->cap;
+    hd.vinf[0] = h.vinf[0]; hd.vinf[1] = h.vinf[1];
+    hd.dg = h.dg; hd.fx = h.fx; hd.fy = h.fy; hd.m = h.m;
+    for (int q = 0; q < 4; ++q) hd.raw[q] = h.raw[q];
+    if ((st = panel_hash(s, &hd.panel_hash)) != VX_OK) return st;
+    const long long ns = hd.slots;
+    std::vector<double> a((size_t)(3 * ns));
+    if (ns > 0) {
+        CU(cudaMemcpy(a.data(), s->x, sizeof(double) * ns, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(a.data() + ns, s->y, sizeof(double) * ns, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(a.data() + 2 * ns, s->g, sizeof(double) * ns, cudaMemcpyDeviceToHost));
+    }
+    FILE *f = fopen(path, "wb");
+    if (!f) { vx_set_error("cannot open %s for writing", path); return VX_ERR_ARG; }
+    const bool ok = fwrite(&hd, sizeof(hd), 1, f) == 1 &&
+                    (a.empty() || fwrite(a.data(), sizeof(double), a.size(), f) == a.size());
+    if (fclose(f) != 0 || !ok) { vx_set_error("writing %s failed", path); return VX_ERR_ARG; }
+    return VX_OK;
+}
+
+extern "C" vx_status vx_checkpoint_load(vx_sim *s, const char *path) {
+    if (!s || !path) return VX_ERR_ARG;
+    CU(cudaSetDevice(s->device));
+    FILE *f = fopen(path, "rb");
+    if (!f) { vx_set_error("cannot open %s", path); return VX_ERR_ARG; }
+    CkptHead hd;
+    if (fread(&hd, sizeof(hd), 1, f) != 1 || memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1 ||
+        hd.n < 0 || hd.slots < hd.n) {
+        fclose(f);
+        vx_set_error("%s is not a checkpoint of this library", path);
+        return VX_ERR_ARG;
+    }
+    uint64_t hh = 0;
+    vx_status st = panel_hash(s, &hh);
+    if (st != VX_OK) { fclose(f); return st; }
+    if (hd.P != s->P || hd.prec != s->prm.prec || hd.panel_hash != hh) {
+        fclose(f);
+        vx_set_error("%s belongs to another body (%d panels, form %d) than this one (%d panels, form %d)", path,
+                     hd.P, hd.prec, s->P, s->prm.prec);
+        return VX_ERR_ARG;
+    }
+    const long long ns = hd.slots;
+    std::vector<double> a((size_t)(3 * ns));
+    const bool ok = a.empty() || fread(a.data(), sizeof(double), a.size(), f) == a.size();
+    fclose(f);
+    if (!ok) { vx_set_error("%s is truncated", path); return VX_ERR_ARG; }
+    if ((st = vx_set_slots(s, a.data(), a.data() + ns, a.data() + 2 * ns, ns, hd.n)) != VX_OK) return st;
+    CU(cudaMemcpyAsync(s->h_S, s->d_S, sizeof(VxScalars), cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    VxScalars *h = s->h_S;
+    h->n0 = hd.n0; h->step = hd.step;
+    h->vinf[0] = hd.vinf[0]; h->vinf[1] = hd.vinf[1];
+    h->dg = hd.dg; h->fx = hd.fx; h->fy = hd.fy; h->m = hd.m;
+    for (int q = 0; q < 4; ++q) h->raw[q] = hd.raw[q];
+    CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     return VX_OK;
 }

@@ -230,6 +230,12 @@ class Sim:
         _check(lib().vx_probe(self.h, _p(px), _p(py), C.c_int64(len(px)), _p(vx), _p(vy)), "vx_probe")
         return vx, vy
 
+    def checkpoint_save(self, path: str):
+        _check(lib().vx_checkpoint_save(self.h, os.fsencode(path)), "vx_checkpoint_save")
+
+    def checkpoint_load(self, path: str):
+        _check(lib().vx_checkpoint_load(self.h, os.fsencode(path)), "vx_checkpoint_load")
+
     def move_points(self, x, y, g, u, v):
         """Tracer points moved one step with velocities (u, v); returns new
         (x, y, g), g = 0 for points absorbed by the wall or the window."""
