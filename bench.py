@@ -223,6 +223,7 @@ def run_ours(args, rank, world, device):
                 "form": "direct O(N^2) sums in FP64"}
     peak32 = Nt.measure_peak(device, fp64=False)
     mufu = Nt.measure_peak(device, mode=3)        # 1e12 (rsqrt + ex2) units per second
+    multi = multibody_runs(args, device, rank, world) if args.multibody else None
     if rank != 0:
         return None
     value = world * 1e3 * K / total_ms
@@ -286,15 +287,33 @@ def run_ours(args, rank, world, device):
     line["cpu_baseline"] = cpu_baseline(args, x0, y0, g0, pan)
     if args.ref_cuda_steps > 0 and world == 1:
         line["reference_cuda_build"] = ref_cuda_build(args, x0, y0, g0)
-    if args.multibody:
-        from vortex_b200 import multibody as MB
-        batched = MB.run_batch(bodies=args.batch_bodies, steps=args.batch_steps, warmup=3, device=device)
-        sub32 = MB.run_batch(bodies=16, steps=2, warmup=1, device=device)
-        sub64 = MB.run_batch(bodies=16, steps=2, warmup=1, precision=Nt.PREC_FP64, device=device)
-        batched["fp32_vs_fp64_first16_bodies"] = sub32["body_steps_per_s"] / sub64["body_steps_per_s"]
-        line["batched"] = batched
-        line["served"] = MB.run_serve(requests=args.serve_requests, device=device)
+    if multi:
+        line["batched"], line["served"] = multi
     return line
+
+
+def multibody_runs(args, device, rank, world):
+    """The seeded population batched and served, partitioned by body over the
+    ranks (each rank its share on its own GPU, no exchange while stepping),
+    the ranks' records gathered and combined on the host.  Every rank takes
+    part in the gathers; rank 0 gets the combined records."""
+    from vortex_b200 import multibody as MB
+    from vortex_b200 import native as Nt
+    batched = MB.run_batch(bodies=args.batch_bodies, steps=args.batch_steps, warmup=3, device=device,
+                           rank=rank, world=world)
+    sub32 = MB.run_batch(bodies=16, steps=2, warmup=1, device=device, rank=rank, world=world)
+    sub64 = MB.run_batch(bodies=16, steps=2, warmup=1, precision=Nt.PREC_FP64, device=device, rank=rank,
+                         world=world)
+    batched["fp32_vs_fp64_first16_bodies"] = sub32["body_steps_per_s"] / sub64["body_steps_per_s"]
+    served = MB.run_serve(requests=args.serve_requests, device=device, rank=rank, world=world)
+    if world == 1:
+        return batched, served
+    import torch.distributed as D
+    parts = [None] * world
+    D.all_gather_object(parts, (batched, served))
+    b = MB.combine_batch([p[0] for p in parts])
+    b["fp32_vs_fp64_first16_bodies"] = float(np.mean([p[0]["fp32_vs_fp64_first16_bodies"] for p in parts]))
+    return b, MB.combine_serve([p[1] for p in parts])
 
 
 def cpu_sample(x, y, g, pan, n_targets, n_panels):

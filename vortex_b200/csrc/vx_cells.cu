@@ -498,13 +498,17 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
     if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);
 }
 
-// Targets left out of the work items: one warp per target, the lanes taking
-// consecutive sources of each row window; FP32 pair sums per row, FP64
-// across rows and lanes (fixed order).
+// Targets left out of the work items (radius beyond CG_KCAP cells: an
+// isolated vortex, whose window can span the whole grid): one block per
+// target, its warps taking every (CG_T / 32)-th row of the window and their
+// lanes consecutive sources of a row; FP32 pair sums per row and lane, FP64
+// across rows, lanes and warps (fixed order).
 __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                     const unsigned *skey, const int *sorted, const int *start,
                                                     const int *wide) {
-    const int lane = threadIdx.x & 31;
+    constexpr int NWARP = CG_T / 32;
+    __shared__ double sred[3][NWARP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long nx = S->cnx, ny = S->cny;
     const double hd = S->ch;
     const float h = (float)hd;
@@ -513,16 +517,15 @@ __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScal
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
     const float log2e = 1.4426950408889634f;
     const int nw = S->cnwide;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long pairs = 0;
-    for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < nw; f += warps) {
+    for (int f = blockIdx.x; f < nw; f += gridDim.x) {
         const long long t = wide[f];
         const float4 me = srt[t];
         const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
         const float R = cut * me.w, R2 = R * R, ndd = -log2e / me.w;
         const long long kk = min((long long)ceilf(R / h), max(nx, ny));
         double I2x = 0.0, I2y = 0.0, I1 = 0.0;
-        for (long long dy = -kk; dy <= kk; ++dy) {
+        for (long long dy = -kk + warp; dy <= kk; dy += NWARP) {
             const long long rr = row + dy;
             if (rr < 0 || rr >= ny) continue;
             long long c0, c1;
@@ -530,10 +533,11 @@ __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScal
             const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
             pairs += j1 - j0;
             const float oy = (float)((double)dy * hd);
+            const unsigned base = (unsigned)(rr * nx + ocol);   // cell keys wrap modulo 2^32 alike
             float s2x = 0.f, s2y = 0.f, s1 = 0.f;
             for (long long j = j0 + lane; j < j1; j += 32) {
                 float4 q = srt[j];
-                q.x += (float)((double)((long long)(skey[j] % unx) - ocol) * hd);
+                q.x += (float)(int)(skey[j] - base) * h;
                 q.y += oy;
                 diff_pair(me.x, me.y, R2, ndd, thr2, q, s2x, s2y, s1);
             }
@@ -544,14 +548,21 @@ __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScal
             I2y += __shfl_xor_sync(0xffffffffu, I2y, o);
             I1 += __shfl_xor_sync(0xffffffffu, I1, o);
         }
-        if (lane == 0 && fabs(I1) > 1e-5) {
-            const long long i = sorted[t];
-            const double dd = (double)me.w;
-            v.vx[i * v.vs] += -p.nu * I2x / (I1 * dd);
-            v.vy[i * v.vs] += -p.nu * I2y / (I1 * dd);
+        if (lane == 0) { sred[0][warp] = I2x; sred[1][warp] = I2y; sred[2][warp] = I1; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, b = 0.0, c = 0.0;
+            for (int w = 0; w < NWARP; ++w) { a += sred[0][w]; b += sred[1][w]; c += sred[2][w]; }
+            if (fabs(c) > 1e-5) {
+                const long long i = sorted[t];
+                const double dd = (double)me.w;
+                v.vx[i * v.vs] += -p.nu * a / (c * dd);
+                v.vy[i * v.vs] += -p.nu * b / (c * dd);
+            }
         }
+        __syncthreads();
     }
-    if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);   // every lane counted the same pairs
+    if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);   // a warp's lanes counted the same rows
 }
 
 static int bits_for(long long cells) {

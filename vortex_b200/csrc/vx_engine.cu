@@ -258,7 +258,7 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     w.fmm_lmax = vx_fmm_max_level(cap);
     A(w.fmm_cnt, vx_fmm_cells(w.fmm_lmax));
     A(w.fmm_start, (1LL << (2 * w.fmm_lmax)) + 1);
-    A(w.fmm_flags, cap);
+    A(w.fmm_flags, cap); A(w.fmm_brute, cap);
     A(w.fmm_M, 2LL * VX_FMM_P * vx_fmm_cells(w.fmm_lmax));
     A(w.fmm_L, 2LL * VX_FMM_P * vx_fmm_cells(w.fmm_lmax));
 #undef A

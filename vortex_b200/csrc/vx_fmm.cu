@@ -61,7 +61,11 @@ __constant__ double c_fmm_inv[FMM_P + 1] = {0.0,      1.0,      1.0 / 2,  1.0 / 
 static_assert(FMM_P == 16, "reciprocal table length");
 
 // ---------------------------------------------------------------------------
-__global__ void k_fmm_begin(VxScalars *S) { S->fb[0] = S->fb[1] = S->fb[2] = S->fb[3] = ~0ull; S->fnflag = 0; }
+__global__ void k_fmm_begin(VxScalars *S) {
+    S->fb[0] = S->fb[1] = S->fb[2] = S->fb[3] = ~0ull;
+    S->fnflag = 0;
+    S->fnbrute = 0;
+}
 
 __global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
     __shared__ unsigned long long sk[4][FMM_T];
@@ -678,6 +682,11 @@ __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, Vx
 // clamped into an edge leaf lies farther out than that leaf), so the search
 // stops once the third distance is below (k h)^2 or the rings cover the grid.
 // Coordinates are relative to the target's leaf centre, as in the near field.
+// The search stops after NN3_RINGS rings: an isolated vortex (one flung out
+// of the wake) would need rings over much of the grid, which one warp walks
+// for a millisecond or more; such targets go to k_fmm_nn3_brute instead, a
+// block scanning every source.
+constexpr int NN3_RINGS = 6;
 __device__ __forceinline__ void fmm_ring_cell(int k, int q, int &dx, int &dy) {
     if (k == 0) { dx = dy = 0; return; }
     const int w = 2 * k + 1;
@@ -690,8 +699,8 @@ __device__ __forceinline__ void fmm_ring_cell(int k, int q, int &dx, int &dy) {
     dx = k; dy = q - k + 1;
 }
 
-__global__ void k_fmm_nn3_fix(VxView v, const VxScalars *S, const float4 *srt, const int *sorted,
-                              const int *start, const int *flag_list) {
+__global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const int *sorted,
+                              const int *start, const int *flag_list, int *brute_list) {
     const int nf = S->fnflag;
     const long long m = 1LL << S->fL;
     const double h = S->fside / (double)m;
@@ -705,7 +714,8 @@ __global__ void k_fmm_nn3_fix(VxView v, const VxScalars *S, const float4 *srt, c
         const float4 me = srt[t];
         const long long kmax = max(max(cx, m - 1 - cx), max(cy, m - 1 - cy));
         float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
-        for (long long k = 0; k <= kmax; ++k) {
+        bool found = false;
+        for (long long k = 0; k <= min(kmax, (long long)NN3_RINGS); ++k) {
             const int ncell = k == 0 ? 1 : (int)(8 * k);
             for (int q = lane; q < ncell; q += 32) {
                 int dx, dy;
@@ -732,11 +742,54 @@ __global__ void k_fmm_nn3_fix(VxView v, const VxScalars *S, const float4 *srt, c
             // every lane holds the merged three; keep them in lane 0 only so
             // that the next ring merges disjoint sets
             const float kh = (float)((double)k * h);
-            const bool done = d3 < kh * kh;
+            const bool done = d3 < kh * kh || k == kmax;
             if (lane != 0) d1 = d2 = d3 = 1e5f;
-            if (done) break;
+            if (done) { found = true; break; }
         }
-        if (lane == 0) v.d[i] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
+        if (lane == 0) {
+            if (found) v.d[i] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
+            else brute_list[atomicAdd(&S->fnbrute, 1)] = (int)i;
+        }
+    }
+}
+
+// The 3 nearest of the targets the ring search left (original indices in
+// brute_list) over every source slot [0, fs): one block per target, each
+// thread keeping the three smallest of its stride, merged over the warp and
+// the block (the same set of sources as the ring search, so the same three).
+__global__ void __launch_bounds__(256) k_fmm_nn3_brute(VxView v, const VxScalars *S, const int *brute_list) {
+    __shared__ float sd[3][256 / 32];
+    const int nb = S->fnbrute;
+    const long long fs = S->fs;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = blockIdx.x; b < nb; b += gridDim.x) {
+        const long long i = brute_list[b];
+        const double xi = v.x[i * v.ps], yi = v.y[i * v.ps];
+        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
+        for (long long j = threadIdx.x; j < fs; j += blockDim.x) {
+            if (j == i) continue;
+            const double dx = xi - v.x[j * v.ps], dy = yi - v.y[j * v.ps];
+            vx_nn3_insert_bf(d1, d2, d3, (float)fma(dx, dx, dy * dy));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float e1 = __shfl_xor_sync(0xffffffffu, d1, o);
+            const float e2 = __shfl_xor_sync(0xffffffffu, d2, o);
+            const float e3 = __shfl_xor_sync(0xffffffffu, d3, o);
+            vx_nn3_insert_bf(d1, d2, d3, e1);
+            vx_nn3_insert_bf(d1, d2, d3, e2);
+            vx_nn3_insert_bf(d1, d2, d3, e3);
+        }
+        if (lane == 0) { sd[0][warp] = d1; sd[1][warp] = d2; sd[2][warp] = d3; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < 256 / 32; ++w) {
+                vx_nn3_insert_bf(d1, d2, d3, sd[0][w]);
+                vx_nn3_insert_bf(d1, d2, d3, sd[1][w]);
+                vx_nn3_insert_bf(d1, d2, d3, sd[2][w]);
+            }
+            v.d[i] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
+        }
+        __syncthreads();
     }
 }
 
@@ -863,7 +916,9 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
                                                       (const cplx *)w.fmm_L, w.fmm_flags);
     VX_EV(L, 1);
     VX_COUNT(L);
-    k_fmm_nn3_fix<<<grid, FMM_T, 0, L.stream>>>(v, S, w.srt, sorted, w.fmm_start, w.fmm_flags);
+    k_fmm_nn3_fix<<<grid, FMM_T, 0, L.stream>>>(v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
+    VX_COUNT(L);
+    k_fmm_nn3_brute<<<grid, 256, 0, L.stream>>>(v, S, w.fmm_brute);
     VX_COUNT(L);
     return cudaGetLastError();
 }

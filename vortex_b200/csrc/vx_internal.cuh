@@ -91,6 +91,7 @@ struct VxScalars {
     double fx0, fy0, fside;
     long long fnleaves, fs;
     int fL, fnflag;
+    int fnbrute;           // flagged targets left to the whole-set 3-nearest scan
     // pair evaluations executed by the bulk-form near-field and diffusion
     // kernels since the counters were last cleared
     unsigned long long pairs_bs, pairs_diff;
@@ -149,7 +150,7 @@ struct VxWork {
     long long *row_item_off;
     // quadtree: counts and expansions of every level up to fmm_lmax
     int fmm_lmax;
-    int *fmm_cnt, *fmm_start, *fmm_flags;
+    int *fmm_cnt, *fmm_start, *fmm_flags, *fmm_brute;
     double *fmm_M, *fmm_L;   // complex FP64 pairs, FMM_P per cell
 };
 

@@ -11,6 +11,12 @@ each asks for a number of steps; the vx_server loop admits them by slot and
 device-byte budget, keeps them resident, steps all resident bodies every
 tick and releases finished ones (continuous batching).
 
+On several GPUs (one process per GPU) the population is partitioned by
+body: rank r of w takes bodies / requests r, r + w, r + 2w, ... (share),
+runs them on its own GPU with no exchange on the step path, and the ranks'
+results are combined on the host afterwards (combine_batch, combine_serve:
+throughputs add, latencies take the slowest rank).
+
     python -m vortex_b200.multibody batch --bodies 256 --steps 20
     python -m vortex_b200.multibody serve --requests 32
 """
@@ -27,16 +33,53 @@ from . import native as N
 from . import workloads as wl
 
 
+def share(count: int, rank: int = 0, world: int = 1) -> list:
+    """Indices of the bodies (or requests) rank `rank` of `world` runs."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of {world}")
+    return list(range(rank, count, world))
+
+
+def combine_batch(parts: list) -> dict:
+    """One batched-run record from the ranks' records: bodies, particles
+    and throughputs add; the batched step takes the slowest rank."""
+    out = dict(parts[0])
+    for k in ("bodies", "particles_start", "particles_end", "panels_total", "body_steps_per_s",
+              "particle_steps_per_s", "interactions_per_s_effective", "gpu_launches"):
+        out[k] = sum(p[k] for p in parts)
+    for k in ("ms_per_batched_step", "ms_p50", "ms_p99", "setup_s"):
+        out[k] = max(p[k] for p in parts)
+    out["batched_steps_per_s"] = min(p["batched_steps_per_s"] for p in parts)
+    out["ranks"] = len(parts)
+    return out
+
+
+def combine_serve(parts: list) -> dict:
+    """One served-run record from the ranks' records: requests, steps and
+    throughputs add; latency percentiles and wall time take the slowest rank."""
+    out = dict(parts[0])
+    for k in ("requests", "steps_requested", "failed", "body_steps", "body_steps_per_s", "particle_steps_per_s",
+              "ticks"):
+        out[k] = sum(p[k] for p in parts)
+    for k in ("wall_s", "step_ms_p50", "step_ms_p99", "ttc_s_p50", "ttc_s_p99"):
+        out[k] = max(p[k] for p in parts)
+    out["mean_resident"] = sum(p["mean_resident"] for p in parts)
+    out["ranks"] = len(parts)
+    return out
+
+
 def _event_pair():
     import torch
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
 def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7,
-              precision: int = N.PREC_FP32, device: int = 0) -> dict:
+              precision: int = N.PREC_FP32, device: int = 0, rank: int = 0, world: int = 1) -> dict:
+    """The batched run of this rank's share of `bodies` seeded bodies."""
     import torch
     torch.cuda.set_device(device)
-    specs = [wl.body_spec(seed, i) for i in range(bodies)]
+    specs = [wl.body_spec(seed, i) for i in share(bodies, rank, world)]
+    bodies = len(specs)
     sims = []
     t0 = time.perf_counter()
     for sp in specs:
@@ -88,14 +131,17 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
 
 def run_serve(requests: int = 32, rate: float = 50.0, budget_gb: float = 160.0, max_active: int = 256,
               seed: int = 11, precision: int = N.PREC_FP32, steps_lo: int = 50, steps_hi: int = 1000,
-              device: int = 0) -> dict:
+              device: int = 0, rank: int = 0, world: int = 1) -> dict:
     """Poisson arrivals (rate per second) of `requests` bodies of the seeded
-    population, each asking for U[steps_lo, steps_hi] steps."""
+    population, each asking for U[steps_lo, steps_hi] steps; this rank serves
+    its share of them, at their arrival times."""
     u = wl.uniforms(seed, 2 * requests)
     gaps = -np.log1p(-u[:requests]) / rate
-    arrive = np.cumsum(gaps)
-    nsteps = (steps_lo + np.floor(u[requests:] * (steps_hi - steps_lo + 1))).astype(int)
-    specs = [wl.body_spec(seed, i) for i in range(requests)]
+    mine = share(requests, rank, world)
+    arrive = np.cumsum(gaps)[mine]
+    nsteps = (steps_lo + np.floor(u[requests:] * (steps_hi - steps_lo + 1))).astype(int)[mine]
+    specs = [wl.body_spec(seed, i) for i in mine]
+    requests = len(mine)
     bodies = [wl.make_body(sp, precision) for sp in specs]
     srv = N.Server(int(budget_gb * 1e9), max_active=max_active, device=device)
     ids = [None] * requests
