@@ -499,14 +499,15 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
 }
 
 // Targets left out of the work items (radius beyond CG_KCAP cells: an
-// isolated vortex, whose window can span the whole grid): one block per
-// target, its warps taking every (CG_T / 32)-th row of the window and their
-// lanes consecutive sources of a row; FP32 pair sums per row and lane, FP64
-// across rows, lanes and warps (fixed order).
-__global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
-                                                    const unsigned *skey, const int *sorted, const int *start,
-                                                    const int *wide) {
-    constexpr int NWARP = CG_T / 32;
+// isolated vortex, whose window can span the whole grid): one block of
+// WIDE_T threads per target, its warps taking every (WIDE_T / 32)-th row of
+// the window and their lanes consecutive sources of a row; FP32 pair sums
+// per row and lane, FP64 across rows, lanes and warps (fixed order).
+constexpr int WIDE_T = 512;
+__global__ void __launch_bounds__(WIDE_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                                                      const unsigned *skey, const int *sorted, const int *start,
+                                                      const int *wide) {
+    constexpr int NWARP = WIDE_T / 32;
     __shared__ double sred[3][NWARP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long nx = S->cnx, ny = S->cny;
@@ -599,7 +600,7 @@ cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, cons
     k_diff_cells<<<L.num_sms * 8, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.items,
                                                        w.cg_wide);
     VX_COUNT(L);
-    k_diff_wide<<<L.num_sms * 4, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide);
+    k_diff_wide<<<L.num_sms * 2, WIDE_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide);
     VX_COUNT(L);
     VX_EV(L, 3);
     return cudaGetLastError();
