@@ -82,6 +82,23 @@ __device__ bool vx_hitting(const VxParams &p, const vx_panel *pan, double x1, do
     return hit;
 }
 
+// True when vx_hitting would test every panel for this segment (it lies in
+// the profile box, and with hit lists its bounding box covers more than 16
+// cells of the grid).  k_advect gives such a segment to its whole warp.
+__device__ __forceinline__ bool vx_hit_all_panels(const VxParams &p, double x1, double y1, double x2, double y2,
+                                                  const int *hstart) {
+    if (((x1 < p.px_min) && (x2 < p.px_min)) || ((x1 > p.px_max) && (x2 > p.px_max)) ||
+        ((y1 < p.py_min) && (y2 < p.py_min)) || ((y1 > p.py_max) && (y2 > p.py_max)))
+        return false;
+    if (!hstart) return false;   // without lists every segment scans the panels itself
+    const double fx0 = (fmin(x1, x2) - p.hit_x0) / p.hit_h, fx1 = (fmax(x1, x2) - p.hit_x0) / p.hit_h;
+    const double fy0 = (fmin(y1, y2) - p.hit_y0) / p.hit_h, fy1 = (fmax(y1, y2) - p.hit_y0) / p.hit_h;
+    if (fx1 < 0.0 || fy1 < 0.0 || fx0 >= (double)p.hit_nx || fy0 >= (double)p.hit_ny) return false;
+    const int cx0 = max((int)floor(fx0), 0), cx1 = min((int)floor(fx1), p.hit_nx - 1);
+    const int cy0 = max((int)floor(fy0), 0), cy1 = min((int)floor(fy1), p.hit_ny - 1);
+    return (cx1 - cx0 + 1) * (cy1 - cy0 + 1) > 16;
+}
+
 __device__ __forceinline__ double vx_block_sum(double v, double *sh) {
     sh[threadIdx.x] = v;
     __syncthreads();
@@ -100,11 +117,16 @@ __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, con
     __shared__ double sh[VX_THREADS];
     const long long n = S->n;
     const long long n_new0 = S->n0;   // vortices born this step: [n0, n)
+    const int lane = threadIdx.x & 31;
     double sdg = 0.0, sfx = 0.0, sfy = 0.0, sm = 0.0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    // whole warps step together (lane i of the warp takes particle base + i),
+    // so a long segment can be handed to the warp
+    for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+         base += (long long)gridDim.x * blockDim.x) {
+        const long long i = base + lane;
+        const bool valid = i < n;
         const long long k = i * v.ps;
-        double x = v.x[k], y = v.y[k], gi = v.g[k];
+        double x = valid ? v.x[k] : 0.0, y = valid ? v.y[k] : 0.0, gi = valid ? v.g[k] : 0.0;
         double fx = 0.0, fy = 0.0, m = 0.0;
         if (i >= n_new0) {
             double dx = x - p.rc_x, dy = y - p.rc_y;
@@ -112,10 +134,39 @@ __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, con
             fy = gi * x;
             m = gi * fma(dx, dx, dy * dy);
         }
-        const double xn = fma(v.vx[i * v.vs], p.dt, x);
-        const double yn = fma(v.vy[i * v.vs], p.dt, y);
+        const double xn = valid ? fma(v.vx[i * v.vs], p.dt, x) : 0.0;
+        const double yn = valid ? fma(v.vy[i * v.vs], p.dt, y) : 0.0;
+        // segments whose box covers many hit-grid cells: every panel, tested
+        // by the whole warp (lanes over panels, then the nearest crossing,
+        // the lower index on a tie: the sequential scan's answer)
+        const bool all = valid && gi != 0 && vx_hit_all_panels(p, xn, yn, x, y, hstart);
+        unsigned want = __ballot_sync(0xffffffffu, all);
+        bool whit = false;
+        int whp = -1;
+        while (want) {
+            const int src = __ffs(want) - 1;
+            want &= want - 1;
+            const double x1 = __shfl_sync(0xffffffffu, xn, src), y1 = __shfl_sync(0xffffffffu, yn, src);
+            const double x2 = __shfl_sync(0xffffffffu, x, src), y2 = __shfl_sync(0xffffffffu, y, src);
+            const double A = y2 - y1, B = x1 - x2, D = y1 * x2 - x1 * y2;
+            bool h = false;
+            double md = 25.0;
+            int mn = -1;
+            for (int q = lane; q < p.P; q += 32) vx_hit_panel(pan[q], q, A, B, D, x1, y1, x2, y2, h, md, mn);
+            h = __any_sync(0xffffffffu, h);
+            for (int o = 16; o > 0; o >>= 1) {
+                const double od = __shfl_xor_sync(0xffffffffu, md, o);
+                const int on = __shfl_xor_sync(0xffffffffu, mn, o);
+                if (on >= 0 && (od < md || (od == md && (mn < 0 || on < mn)))) { md = od; mn = on; }
+            }
+            if (lane == src) { whit = h; whp = mn; }
+        }
         int hp = -1;
-        if (gi != 0 && vx_hitting(p, pan, xn, yn, x, y, &hp, hstart, hidx)) {
+        bool hit = false;
+        if (all) { hit = whit; hp = whp; }
+        else if (valid && gi != 0) hit = vx_hitting(p, pan, xn, yn, x, y, &hp, hstart, hidx);
+        if (!valid) continue;
+        if (hit) {
             if (hp >= 0) {   // the reference reads panels[-1] when no crossing is nearer than 5
                 const double cx = pan[hp].contr[0], cy = pan[hp].contr[1];
                 const double dx = cx - p.rc_x, dy = cy - p.rc_y;
