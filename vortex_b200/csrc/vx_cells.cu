@@ -36,6 +36,7 @@ constexpr int CG_KCAP = 2 * CG_DIV;    // widest window of a work item, in cells
 __global__ void k_cg_begin(VxScalars *S) {
     S->cb[0] = S->cb[1] = S->cb[2] = S->cb[3] = ~0ull;
     S->cnwide = 0;
+    S->cnhuge = 0;
 }
 
 // Bounding box of the live particles and per-block sums of d (fixed grid:
@@ -498,52 +499,111 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
     if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);
 }
 
-// Targets left out of the work items (radius beyond CG_KCAP cells: an
-// isolated vortex, whose window can span the whole grid): one block of
-// WIDE_T threads per target, its warps taking every (WIDE_T / 32)-th row of
-// the window and their lanes consecutive sources of a row; FP32 pair sums
-// per row and lane, FP64 across rows, lanes and warps (fixed order).
+// Targets left out of the work items (radius beyond CG_KCAP cells).  Most
+// have windows of a few thousand sources: one warp each (k_diff_wide), the
+// lanes taking consecutive sources of each row window.  An isolated vortex,
+// whose window spans more than WIDE_ROWS rows each side (up to the whole
+// grid), is passed on to k_diff_huge: one block of WIDE_T threads each, its
+// warps taking every (WIDE_T / 32)-th row.  FP32 pair sums per row and lane,
+// FP64 across rows, lanes and warps (fixed order).
+constexpr int WIDE_ROWS = 24;
 constexpr int WIDE_T = 512;
-__global__ void __launch_bounds__(WIDE_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
-                                                      const unsigned *skey, const int *sorted, const int *start,
-                                                      const int *wide) {
-    constexpr int NWARP = WIDE_T / 32;
-    __shared__ double sred[3][NWARP];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+__device__ __forceinline__ void wide_row(const VxParams &p, const VxScalars *S, const float4 *srt,
+                                         const unsigned *skey, const int *start, const float4 me, long long row,
+                                         long long ocol, float R, float R2, float ndd, float thr2, long long dy,
+                                         int lane, double &I2x, double &I2y, double &I1,
+                                         unsigned long long &pairs) {
     const long long nx = S->cnx, ny = S->cny;
     const double hd = S->ch;
     const float h = (float)hd;
+    const long long rr = row + dy;
+    if (rr < 0 || rr >= ny) return;
+    long long c0, c1;
+    if (!diff_window((int)dy, R, me.x, me.x, h, ocol, nx, c0, c1)) return;
+    const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
+    pairs += j1 - j0;
+    const float oy = (float)((double)dy * hd);
+    const unsigned base = (unsigned)(rr * nx + ocol);   // cell keys wrap modulo 2^32 alike
+    float s2x = 0.f, s2y = 0.f, s1 = 0.f;
+    for (long long j = j0 + lane; j < j1; j += 32) {
+        float4 q = srt[j];
+        q.x += (float)(int)(skey[j] - base) * h;
+        q.y += oy;
+        diff_pair(me.x, me.y, R2, ndd, thr2, q, s2x, s2y, s1);
+    }
+    I2x += (double)s2x; I2y += (double)s2y; I1 += (double)s1;
+}
+
+__device__ __forceinline__ void wide_apply(const VxParams &p, VxView v, const int *sorted, long long t, float d,
+                                           double I2x, double I2y, double I1) {
+    if (fabs(I1) > 1e-5) {
+        const long long i = sorted[t];
+        const double dd = (double)d;
+        v.vx[i * v.vs] += -p.nu * I2x / (I1 * dd);
+        v.vy[i * v.vs] += -p.nu * I2y / (I1 * dd);
+    }
+}
+
+__global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                                                    const unsigned *skey, const int *sorted, const int *start,
+                                                    const int *wide, int *huge) {
+    const int lane = threadIdx.x & 31;
+    const long long nx = S->cnx, ny = S->cny;
+    const float h = (float)S->ch;
     const unsigned unx = (unsigned)nx;
     const float cut = (float)p.diff_cutoff;
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
     const float log2e = 1.4426950408889634f;
     const int nw = S->cnwide;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long pairs = 0;
-    for (int f = blockIdx.x; f < nw; f += gridDim.x) {
+    for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < nw; f += warps) {
         const long long t = wide[f];
         const float4 me = srt[t];
         const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
         const float R = cut * me.w, R2 = R * R, ndd = -log2e / me.w;
         const long long kk = min((long long)ceilf(R / h), max(nx, ny));
-        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
-        for (long long dy = -kk + warp; dy <= kk; dy += NWARP) {
-            const long long rr = row + dy;
-            if (rr < 0 || rr >= ny) continue;
-            long long c0, c1;
-            if (!diff_window((int)dy, R, me.x, me.x, h, ocol, nx, c0, c1)) continue;
-            const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
-            pairs += j1 - j0;
-            const float oy = (float)((double)dy * hd);
-            const unsigned base = (unsigned)(rr * nx + ocol);   // cell keys wrap modulo 2^32 alike
-            float s2x = 0.f, s2y = 0.f, s1 = 0.f;
-            for (long long j = j0 + lane; j < j1; j += 32) {
-                float4 q = srt[j];
-                q.x += (float)(int)(skey[j] - base) * h;
-                q.y += oy;
-                diff_pair(me.x, me.y, R2, ndd, thr2, q, s2x, s2y, s1);
-            }
-            I2x += (double)s2x; I2y += (double)s2y; I1 += (double)s1;
+        if (kk > WIDE_ROWS) {
+            if (lane == 0) huge[atomicAdd(&S->cnhuge, 1)] = (int)t;
+            continue;
         }
+        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
+        for (long long dy = -kk; dy <= kk; ++dy)
+            wide_row(p, S, srt, skey, start, me, row, ocol, R, R2, ndd, thr2, dy, lane, I2x, I2y, I1, pairs);
+        for (int o = 16; o > 0; o >>= 1) {
+            I2x += __shfl_xor_sync(0xffffffffu, I2x, o);
+            I2y += __shfl_xor_sync(0xffffffffu, I2y, o);
+            I1 += __shfl_xor_sync(0xffffffffu, I1, o);
+        }
+        if (lane == 0) wide_apply(p, v, sorted, t, me.w, I2x, I2y, I1);
+    }
+    if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);   // every lane counted the same pairs
+}
+
+__global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                                                      const unsigned *skey, const int *sorted, const int *start,
+                                                      const int *huge) {
+    constexpr int NWARP = WIDE_T / 32;
+    __shared__ double sred[3][NWARP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long nx = S->cnx, ny = S->cny;
+    const float h = (float)S->ch;
+    const unsigned unx = (unsigned)nx;
+    const float cut = (float)p.diff_cutoff;
+    const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
+    const float log2e = 1.4426950408889634f;
+    const int nh = S->cnhuge;
+    unsigned long long pairs = 0;
+    for (int f = blockIdx.x; f < nh; f += gridDim.x) {
+        const long long t = huge[f];
+        const float4 me = srt[t];
+        const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
+        const float R = cut * me.w, R2 = R * R, ndd = -log2e / me.w;
+        const long long kk = min((long long)ceilf(R / h), max(nx, ny));
+        double I2x = 0.0, I2y = 0.0, I1 = 0.0;
+        for (long long dy = -kk + warp; dy <= kk; dy += NWARP)
+            wide_row(p, S, srt, skey, start, me, row, ocol, R, R2, ndd, thr2, dy, lane, I2x, I2y, I1, pairs);
         for (int o = 16; o > 0; o >>= 1) {
             I2x += __shfl_xor_sync(0xffffffffu, I2x, o);
             I2y += __shfl_xor_sync(0xffffffffu, I2y, o);
@@ -554,12 +614,7 @@ __global__ void __launch_bounds__(WIDE_T) k_diff_wide(VxParams p, VxView v, VxSc
         if (threadIdx.x == 0) {
             double a = 0.0, b = 0.0, c = 0.0;
             for (int w = 0; w < NWARP; ++w) { a += sred[0][w]; b += sred[1][w]; c += sred[2][w]; }
-            if (fabs(c) > 1e-5) {
-                const long long i = sorted[t];
-                const double dd = (double)me.w;
-                v.vx[i * v.vs] += -p.nu * a / (c * dd);
-                v.vy[i * v.vs] += -p.nu * b / (c * dd);
-            }
+            wide_apply(p, v, sorted, t, me.w, a, b, c);
         }
         __syncthreads();
     }
@@ -600,7 +655,10 @@ cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, cons
     k_diff_cells<<<L.num_sms * 8, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.items,
                                                        w.cg_wide);
     VX_COUNT(L);
-    k_diff_wide<<<L.num_sms * 2, WIDE_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide);
+    k_diff_wide<<<L.num_sms * 4, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide,
+                                                      w.cg_huge);
+    VX_COUNT(L);
+    k_diff_huge<<<L.num_sms * 2, WIDE_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_huge);
     VX_COUNT(L);
     VX_EV(L, 3);
     return cudaGetLastError();

@@ -252,7 +252,7 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.srt, cap);
     w.items_cap = cap / 32 + w.cells_cap + 2;
     A(w.items, w.items_cap);
-    A(w.cg_wide, cap);
+    A(w.cg_wide, cap); A(w.cg_huge, cap);
     A(w.row_items, w.cells_cap + 1); A(w.row_item_off, w.cells_cap + 1);
     // quadtree of the bulk-form Biot-Savart
     w.fmm_lmax = vx_fmm_max_level(cap);

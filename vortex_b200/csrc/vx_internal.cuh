@@ -81,6 +81,7 @@ struct VxScalars {
     long long gnx, gny, gncells;
     int err;
     int cnwide;            // diffusion targets whose cut-off exceeds the item window
+    int cnhuge;            // of those, the ones whose window spans more than WIDE_ROWS rows each side
     long long bf_nnear;    // birth sources inside the far-field radius
     // neighbour-list grid of the bulk form (vortex diffusion)
     unsigned long long cb[4];
@@ -146,6 +147,7 @@ struct VxWork {
     int2 *items;             // (row, first sorted slot) of each target segment
     long long items_cap;
     int *cg_wide;            // sorted slots of the diffusion targets summed one warp each
+    int *cg_huge;            // sorted slots of those summed one block each
     int *row_items;
     long long *row_item_off;
     // quadtree: counts and expansions of every level up to fmm_lmax
