@@ -114,6 +114,7 @@ __device__ __forceinline__ double vx_block_sum(double v, double *sh) {
 __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, const VxScalars *S,
                                                        const vx_panel *pan, double *red, const int *hstart,
                                                        const int *hidx) {
+    VX_PDL_WAIT();
     __shared__ double sh[VX_THREADS];
     const long long n = S->n;
     const long long n_new0 = S->n0;   // vortices born this step: [n0, n)
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, con
 // Block sums combined by one block: thread t adds blocks t, t + 256, ... in
 // order, then a fixed shared-memory tree; the result is run-to-run identical.
 __global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, const double *red, int nblocks) {
+    VX_PDL_WAIT();
     __shared__ double sh[VX_THREADS];
     double a[4] = {0.0, 0.0, 0.0, 0.0};
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
@@ -210,7 +212,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, c
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                              VxWork &w, const vx_panel *pan, const int *hstart, const int *hidx) {
     if (p.hit_nx <= 0 || p.hit_ny <= 0) hstart = hidx = nullptr;
-    k_advect<<<VX_RED_BLOCKS, VX_THREADS, 0, L.stream>>>(p, v, S, pan, w.red, hstart, hidx); VX_COUNT(L);
-    k_sums<<<1, VX_THREADS, 0, L.stream>>>(p, S, w.red, VX_RED_BLOCKS); VX_COUNT(L);
+    vx_launch_pdl(k_advect, VX_RED_BLOCKS, VX_THREADS, 0, L.stream, p, v, S, pan, w.red, hstart, hidx); VX_COUNT(L);
+    vx_launch_pdl(k_sums, 1, VX_THREADS, 0, L.stream, p, S, w.red, VX_RED_BLOCKS); VX_COUNT(L);
     return cudaGetLastError();
 }

@@ -16,6 +16,7 @@ __device__ __forceinline__ double vx_sp(const double a[2], const double b[2]) {
 }
 
 __global__ void k_panel_influence(const vx_panel *pan, int P, double *L) {
+    VX_PDL_WAIT();
     const long long S = P + 1;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * S;
          e += (long long)gridDim.x * blockDim.x) {
@@ -78,6 +79,7 @@ __global__ void k_panel_influence(const vx_panel *pan, int P, double *L) {
 }
 
 __global__ void k_identity(double *A, long long S) {
+    VX_PDL_WAIT();
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * S;
          e += (long long)gridDim.x * blockDim.x)
         A[e] = (e / S == e % S) ? 1.0 : 0.0;
@@ -128,6 +130,7 @@ __device__ void vx_block_swap_rows(double *A, long long S, long long r1, long lo
 // 1e-12 there.  robust != 0: ordinary partial pivoting instead (the pivot of
 // column k chosen among rows k.. after the previous eliminations).
 __global__ void k_gj_pivot(double *A, double *Inv, long long S, long long k, double *c, int *flag, int robust) {
+    VX_PDL_WAIT();
     __shared__ double s_val[1024];
     __shared__ long long s_idx[1024];
     if (*flag) return;
@@ -165,6 +168,7 @@ __global__ void k_gj_pivot(double *A, double *Inv, long long S, long long k, dou
 // Row operations of step k: every row but k loses c[i] times row k.
 __global__ void k_gj_elim(double *A, double *Inv, long long S, long long k, const double *c,
                           const int *flag) {
+    VX_PDL_WAIT();
     if (*flag) return;
     const long long W = 2 * S;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * W;
@@ -178,6 +182,7 @@ __global__ void k_gj_elim(double *A, double *Inv, long long S, long long k, cons
 }
 
 __global__ void k_gj_last_pivot(const double *A, long long S, double *c, int *flag) {
+    VX_PDL_WAIT();
     if (*flag) return;
     const long long l = S - 1;
     if (fabs(A[l * S + l]) < 1e-12) { if (threadIdx.x == 0) *flag = 1; return; }
@@ -185,6 +190,7 @@ __global__ void k_gj_last_pivot(const double *A, long long S, double *c, int *fl
 }
 
 __global__ void k_gj_last_elim(double *Inv, long long S, const double *c, const int *flag) {
+    VX_PDL_WAIT();
     if (*flag) return;
     const long long l = S - 1;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < l * S;
@@ -195,6 +201,7 @@ __global__ void k_gj_last_elim(double *Inv, long long S, const double *c, const 
 }
 
 __global__ void k_gj_scale(const double *A, double *Inv, long long S, const int *flag) {
+    VX_PDL_WAIT();
     if (*flag) return;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * S;
          e += (long long)gridDim.x * blockDim.x) {
@@ -212,22 +219,23 @@ cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, dou
     double *c = d_work + S * S;
     const int grid = L.num_sms * 4;
     cudaMemsetAsync(d_flag, 0, sizeof(int), L.stream);
-    k_panel_influence<<<grid, 256, 0, L.stream>>>(d_pan, P, A); VX_COUNT(L);
+    vx_launch_pdl(k_panel_influence, grid, 256, 0, L.stream, d_pan, P, A); VX_COUNT(L);
     if (d_L_out) cudaMemcpyAsync(d_L_out, A, sizeof(double) * S * S, cudaMemcpyDeviceToDevice, L.stream);
-    k_identity<<<grid, 256, 0, L.stream>>>(d_minv, S); VX_COUNT(L);
+    vx_launch_pdl(k_identity, grid, 256, 0, L.stream, d_minv, S); VX_COUNT(L);
     for (long long k = 0; k < S - 1; ++k) {
-        k_gj_pivot<<<1, 1024, 0, L.stream>>>(A, d_minv, S, k, c, d_flag, robust); VX_COUNT(L);
-        k_gj_elim<<<grid, 256, 0, L.stream>>>(A, d_minv, S, k, c, d_flag); VX_COUNT(L);
+        vx_launch_pdl(k_gj_pivot, 1, 1024, 0, L.stream, A, d_minv, S, k, c, d_flag, robust); VX_COUNT(L);
+        vx_launch_pdl(k_gj_elim, grid, 256, 0, L.stream, A, d_minv, S, k, c, d_flag); VX_COUNT(L);
     }
-    k_gj_last_pivot<<<1, 1024, 0, L.stream>>>(A, S, c, d_flag); VX_COUNT(L);
-    k_gj_last_elim<<<grid, 256, 0, L.stream>>>(d_minv, S, c, d_flag); VX_COUNT(L);
-    k_gj_scale<<<grid, 256, 0, L.stream>>>(A, d_minv, S, d_flag); VX_COUNT(L);
+    vx_launch_pdl(k_gj_last_pivot, 1, 1024, 0, L.stream, A, S, c, d_flag); VX_COUNT(L);
+    vx_launch_pdl(k_gj_last_elim, grid, 256, 0, L.stream, d_minv, S, c, d_flag); VX_COUNT(L);
+    vx_launch_pdl(k_gj_scale, grid, 256, 0, L.stream, A, d_minv, S, d_flag); VX_COUNT(L);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // Step begin: V_inf ramp (src/main.c:654-659) and the pre-birth count.
 __global__ void k_step_begin(VxScalars *S) {
+    VX_PDL_WAIT();
     if (S->step < S->incr_steps) {
         S->vinf[0] += S->dvinf[0];
         S->vinf[1] += S->dvinf[1];
@@ -236,11 +244,12 @@ __global__ void k_step_begin(VxScalars *S) {
 }
 
 cudaError_t vx_launch_step_begin(const VxLaunch &L, VxScalars *S) {
-    k_step_begin<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
+    vx_launch_pdl(k_step_begin, 1, 1, 0, L.stream, S); VX_COUNT(L);
     return cudaGetLastError();
 }
 
-__global__ void k_step_end(VxScalars *S) { S->step += 1; }
+__global__ void k_step_end(VxScalars *S) {
+    VX_PDL_WAIT(); S->step += 1; }
 
 // ---------------------------------------------------------------------------
 // Birth right-hand side (src/kernel.cu:779-847), partial sums per source
@@ -266,6 +275,7 @@ template <typename T>
 __global__ void __launch_bounds__(RHS_T) k_rhs_partial(VxView v, const VxScalars *S,
                                                        const vx_panel *pan, int P, int P32,
                                                        double *part, int nchunks) {
+    VX_PDL_WAIT();
     __shared__ T sx[RHS_T], sy[RHS_T], sg[RHS_T];
     const long long n0 = S->n0;
     const long long cs = vx_ceil_div(vx_ceil_div(n0, nchunks), RHS_T) * RHS_T;
@@ -359,6 +369,7 @@ __device__ __forceinline__ bool bf_near(const VxParams &p, double x, double y) {
 // lane bit and adds the partner's copy: lane q ends with value q, i.e.
 // coefficient q/2, part q&1) and a fixed-order sum over the block's warps.
 __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
+    VX_PDL_WAIT();
     __shared__ double sacc[BF_T / 32][32];
     __shared__ int snear[BF_T / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -437,6 +448,7 @@ constexpr int BF_SCAN_PER = VX_BF_MAX_BLOCKS / BF_SCAN_T;
 static_assert(BF_SCAN_PER * BF_SCAN_T == VX_BF_MAX_BLOCKS, "whole blocks per scan thread");
 __global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, const int *cnt, long long *off,
                                                        const double *part, double *coef) {
+    VX_PDL_WAIT();
     __shared__ long long wsum[BF_SCAN_T / 32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     long long c[BF_SCAN_PER], tot = 0;
@@ -476,6 +488,7 @@ __global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, con
 // Near sources of each block in index order (block-wide ballot scan).
 __global__ void __launch_bounds__(BF_T) k_bf_scatter(VxParams p, VxView v, const VxScalars *S,
                                                      const long long *off, float4 *near) {
+    VX_PDL_WAIT();
     __shared__ int swarp[BF_T / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     long long j0, j1;
@@ -533,6 +546,7 @@ __device__ __forceinline__ float vx_atan2_bulk(float y, float x) {
 }
 
 __global__ void k_eval_atan2(const float *y, const float *x, float *out, long long n) {
+    VX_PDL_WAIT();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
         out[i] = vx_atan2_bulk(y[i], x[i]);
@@ -575,6 +589,7 @@ __device__ __forceinline__ float vx_half_log_ratio(float r0, float r1, float num
 // Direct FP32 panel terms over the near list (chunked like k_rhs_partial).
 __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx_panel *pan, int P, int P32,
                                                     const float4 *near, double *part, int nchunks) {
+    VX_PDL_WAIT();
     __shared__ float4 sq4[RHS_T];   // (x, y, G, unused)
     const long long nn = S->bf_nnear;
     const long long cs = vx_ceil_div(vx_ceil_div(nn, nchunks), RHS_T) * RHS_T;
@@ -628,6 +643,7 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx
 template <bool WARP>
 __global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int P32,
                             const double *part, int nchunks, double *R, VxParams p, const double *coef) {
+    VX_PDL_WAIT();
     const int i = WARP ? (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) : blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double y0 = 0.0, y1 = 0.0;
@@ -678,6 +694,7 @@ __global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int 
 // oracle), one thread per row; ld is the matrix row stride.
 __global__ void k_gamma(const VxScalars *S, const double *M, long long ld, int P, const double *R,
                         double *gamma) {
+    VX_PDL_WAIT();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     const double *row = M + (long long)i * ld;
@@ -691,6 +708,7 @@ __global__ void k_gamma(const VxScalars *S, const double *M, long long ld, int P
 // doubles per step instead of 32 rows' worth of cache lines.
 __global__ void k_gamma_t(const VxScalars *S, const double *Mt, long long ld, int P, const double *R,
                           double *gamma) {
+    VX_PDL_WAIT();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double acc = 0.0;
@@ -702,6 +720,7 @@ __global__ void k_gamma_t(const VxScalars *S, const double *Mt, long long ld, in
 // partial sums combined by a fixed butterfly.
 __global__ void k_gamma_w(const VxScalars *S, const double *M, long long ld, int P, const double *R,
                           double *gamma) {
+    VX_PDL_WAIT();
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= P) return;
@@ -713,6 +732,7 @@ __global__ void k_gamma_w(const VxScalars *S, const double *M, long long ld, int
 }
 
 __global__ void k_transpose(const double *A, double *At, long long nr) {
+    VX_PDL_WAIT();
     __shared__ double t[32][33];
     for (long long by = blockIdx.y; by * 32 < nr; by += gridDim.y)
         for (long long bx = blockIdx.x; bx * 32 < nr; bx += gridDim.x) {
@@ -732,13 +752,14 @@ __global__ void k_transpose(const double *A, double *At, long long nr) {
 cudaError_t vx_transpose_square(const VxLaunch &L, const double *A, double *At, long long nr) {
     const long long nb = vx_ceil_div(nr, 32LL);
     const dim3 grid((unsigned)std::min(nb, 64LL), (unsigned)std::min(nb, 64LL)), block(32, 8);
-    k_transpose<<<grid, block, 0, L.stream>>>(A, At, nr); VX_COUNT(L);
+    vx_launch_pdl(k_transpose, grid, block, 0, L.stream, A, At, nr); VX_COUNT(L);
     return cudaGetLastError();
 }
 
 // One new vortex per panel at [n0, n0+P) (src/kernel.cu:862-872).
 __global__ void k_place(VxParams p, VxView v, VxScalars *S, const vx_panel *pan, int P,
                         const double *gamma) {
+    VX_PDL_WAIT();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const long long n0 = S->n0;
     if (i < P) {
@@ -771,31 +792,31 @@ static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView
     const bool far = p.prec == VX_PREC_FP32 && p.birth_far;
     if (far) {
         const int nb = std::min(2 * L.num_sms, VX_BF_MAX_BLOCKS);
-        k_bf_far<<<nb, BF_T, 0, L.stream>>>(p, v, S, w.bf_part, w.bf_cnt); VX_COUNT(L);
-        k_bf_scan<<<1, BF_SCAN_T, 0, L.stream>>>(S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef); VX_COUNT(L);
-        k_bf_scatter<<<nb, BF_T, 0, L.stream>>>(p, v, S, w.bf_off, w.bf_near); VX_COUNT(L);
-        k_rhs_near<<<grid, RHS_T, 0, L.stream>>>(S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
+        vx_launch_pdl(k_bf_far, nb, BF_T, 0, L.stream, p, v, S, w.bf_part, w.bf_cnt); VX_COUNT(L);
+        vx_launch_pdl(k_bf_scan, 1, BF_SCAN_T, 0, L.stream, S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef); VX_COUNT(L);
+        vx_launch_pdl(k_bf_scatter, nb, BF_T, 0, L.stream, p, v, S, w.bf_off, w.bf_near); VX_COUNT(L);
+        vx_launch_pdl(k_rhs_near, grid, RHS_T, 0, L.stream, S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
     } else if (p.prec == VX_PREC_FP32) {
-        k_rhs_partial<float><<<grid, RHS_T, 0, L.stream>>>(v, S, pan, P, P32, w.rhs_part, rhs_chunks);
+        vx_launch_pdl(k_rhs_partial<float>, grid, RHS_T, 0, L.stream, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
     } else {
-        k_rhs_partial<double><<<grid, RHS_T, 0, L.stream>>>(v, S, pan, P, P32, w.rhs_part, rhs_chunks);
+        vx_launch_pdl(k_rhs_partial<double>, grid, RHS_T, 0, L.stream, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
     }
     VX_COUNT(L);
     const int b = (P + 127) / 128;
     if (far)
-        k_rhs_final<true><<<(P + 3) / 4, 128, 0, L.stream>>>(S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p,
+        vx_launch_pdl(k_rhs_final<true>, (P + 3) / 4, 128, 0, L.stream, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p,
                                                              w.bf_coef);
     else
-        k_rhs_final<false><<<b, 128, 0, L.stream>>>(S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, nullptr);
+        vx_launch_pdl(k_rhs_final<false>, b, 128, 0, L.stream, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, nullptr);
     VX_COUNT(L);
     if (minv_t && p.prec == VX_PREC_FP32)
-        k_gamma_w<<<(P + 3) / 4, 128, 0, L.stream>>>(S, minv, ld, P, w.R, w.gamma);
+        vx_launch_pdl(k_gamma_w, (P + 3) / 4, 128, 0, L.stream, S, minv, ld, P, w.R, w.gamma);
     else if (minv_t)
-        k_gamma_t<<<b, 128, 0, L.stream>>>(S, minv_t, ld, P, w.R, w.gamma);
+        vx_launch_pdl(k_gamma_t, b, 128, 0, L.stream, S, minv_t, ld, P, w.R, w.gamma);
     else
-        k_gamma<<<b, 128, 0, L.stream>>>(S, minv, ld, P, w.R, w.gamma);
+        vx_launch_pdl(k_gamma, b, 128, 0, L.stream, S, minv, ld, P, w.R, w.gamma);
     VX_COUNT(L);
-    k_place<<<b, 128, 0, L.stream>>>(p, v, S, pan, P, w.gamma); VX_COUNT(L);
+    vx_launch_pdl(k_place, b, 128, 0, L.stream, p, v, S, pan, P, w.gamma); VX_COUNT(L);
     return cudaGetLastError();
 }
 
@@ -816,6 +837,6 @@ cudaError_t vx_launch_birth(const VxLaunch &L, const VxParams &p, const VxView &
 }
 
 cudaError_t vx_launch_step_end(const VxLaunch &L, VxScalars *S) {
-    k_step_end<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
+    vx_launch_pdl(k_step_end, 1, 1, 0, L.stream, S); VX_COUNT(L);
     return cudaGetLastError();
 }

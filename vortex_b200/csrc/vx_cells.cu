@@ -34,6 +34,7 @@ constexpr int CG_DIV = VX_CG_DIV;      // cell side = cut-off radius at the mean
 constexpr int CG_KCAP = 2 * CG_DIV;    // widest window of a work item, in cells (twice the mean radius)
 
 __global__ void k_cg_begin(VxScalars *S) {
+    VX_PDL_WAIT();
     S->cb[0] = S->cb[1] = S->cb[2] = S->cb[3] = ~0ull;
     S->cnwide = 0;
     S->cnhuge = 0;
@@ -42,6 +43,7 @@ __global__ void k_cg_begin(VxScalars *S) {
 // Bounding box of the live particles and per-block sums of d (fixed grid:
 // the mean below is reproducible).
 __global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double *red) {
+    VX_PDL_WAIT();
     __shared__ unsigned long long sk[4][CG_T];
     __shared__ double sd[CG_T];
     const long long n = S->n;
@@ -77,6 +79,7 @@ __global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double
 // tree (reproducible), then thread 0 sizes the grid.
 __global__ void __launch_bounds__(CG_T) k_cg_params(VxScalars *S, const double *red, int nblocks, double cutoff,
                                                     long long cells_cap) {
+    VX_PDL_WAIT();
     __shared__ double sd[CG_T];
     double part = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += CG_T) part += red[b];
@@ -115,6 +118,7 @@ __device__ __forceinline__ long long cg_cell(const VxScalars *S, double x, doubl
 }
 
 __global__ void k_cg_zero(const VxScalars *S, int *cnt) {
+    VX_PDL_WAIT();
     const long long nc = S->cncells;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
          c += (long long)gridDim.x * blockDim.x)
@@ -122,6 +126,7 @@ __global__ void k_cg_zero(const VxScalars *S, int *cnt) {
 }
 
 __global__ void k_cg_cellid(VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
+    VX_PDL_WAIT();
     const long long n = S->n;
     if (S->cncells == 0) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -136,6 +141,7 @@ __global__ void k_cg_cellid(VxView v, const VxScalars *S, unsigned *key, int *va
 // Exclusive scan of cnt[0, len) into start[], start[len] = total: chunk
 // sums, one-block scan of the chunk sums, per-chunk apply.
 __global__ void __launch_bounds__(CG_T) k_scan_sum(const long long *len_p, const int *cnt, int *csum) {
+    VX_PDL_WAIT();
     __shared__ int sh[CG_T];
     const long long len = *len_p, nch = vx_ceil_div(len, VX_CHUNK);
     for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
@@ -153,6 +159,7 @@ __global__ void __launch_bounds__(CG_T) k_scan_sum(const long long *len_p, const
 }
 
 __global__ void k_scan_top(const long long *len_p, const int *csum, long long *coff) {
+    VX_PDL_WAIT();
     __shared__ long long sh[1024];
     __shared__ long long carry;
     const long long nch = vx_ceil_div(*len_p, VX_CHUNK);
@@ -178,6 +185,7 @@ __global__ void k_scan_top(const long long *len_p, const int *csum, long long *c
 
 __global__ void __launch_bounds__(CG_T) k_scan_apply(const long long *len_p, const int *cnt, const long long *coff,
                                                      int *start, const long long *total_p) {
+    VX_PDL_WAIT();
     constexpr int PER = VX_CHUNK / CG_T;
     __shared__ int sh[CG_T];
     const long long len = *len_p, nch = vx_ceil_div(len, VX_CHUNK);
@@ -209,6 +217,7 @@ __global__ void __launch_bounds__(CG_T) k_scan_apply(const long long *len_p, con
 // FP32 positions relative to the cell keeps the pair differences accurate to
 // FP32 rounding of the local spacing rather than of the absolute position.
 __global__ void k_cg_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
+    VX_PDL_WAIT();
     const long long n = S->n, nx = S->cnx;
     const double h = S->ch;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
@@ -223,6 +232,7 @@ __global__ void k_cg_gather(VxView v, const VxScalars *S, const int *sorted, con
 
 // Exclusive scan of the per-row item counts (single block, runs per thread).
 __global__ void k_cg_row_scan(const VxScalars *S, const int *in, long long *out) {
+    VX_PDL_WAIT();
     __shared__ long long sh[1024];
     const long long len = S->cny;
     const long long per = vx_ceil_div(len, (long long)blockDim.x);
@@ -246,6 +256,7 @@ __global__ void k_cg_row_scan(const VxScalars *S, const int *in, long long *out)
 
 // Work items: each row's sorted range cut into segments of CG_W targets.
 __global__ void k_cg_row_items(const VxScalars *S, const int *start, int *row_items) {
+    VX_PDL_WAIT();
     const long long ny = S->cny, nx = S->cnx;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ny;
          r += (long long)gridDim.x * blockDim.x) {
@@ -256,6 +267,7 @@ __global__ void k_cg_row_items(const VxScalars *S, const int *start, int *row_it
 
 __global__ void k_cg_items(VxScalars *S, const int *start, const int *row_items, const long long *row_off,
                            int2 *items, long long items_cap) {
+    VX_PDL_WAIT();
     const long long ny = S->cny, nx = S->cnx;
     if (blockIdx.x == 0 && threadIdx.x == 0 && ny > 0) {
         const long long tot = row_off[ny - 1] + row_items[ny - 1];
@@ -374,6 +386,7 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
                                                                    const float4 *srt, const unsigned *skey,
                                                                    const int *sorted, const int *start,
                                                                    const int2 *items, int *wide) {
+    VX_PDL_WAIT();
     __shared__ float4 sxy[CG_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
     __shared__ float2 sg[CG_T / 2];    // (G_a, G_b)
     __shared__ DiffRow srow[CG_T / 32][DIFF_ROWS];
@@ -548,6 +561,7 @@ __device__ __forceinline__ void wide_apply(const VxParams &p, VxView v, const in
 __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                     const unsigned *skey, const int *sorted, const int *start,
                                                     const int *wide, int *huge) {
+    VX_PDL_WAIT();
     const int lane = threadIdx.x & 31;
     const long long nx = S->cnx, ny = S->cny;
     const float h = (float)S->ch;
@@ -584,6 +598,7 @@ __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScal
 __global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                       const unsigned *skey, const int *sorted, const int *start,
                                                       const int *huge) {
+    VX_PDL_WAIT();
     constexpr int NWARP = WIDE_T / 32;
     __shared__ double sred[3][NWARP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -632,33 +647,33 @@ static int bits_for(long long cells) {
 cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                       VxWork &w) {
     const int grid = L.num_sms * 4;
-    k_cg_begin<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
-    k_cg_bbox<<<VX_RED_BLOCKS, CG_T, 0, L.stream>>>(v, S, w.red); VX_COUNT(L);
-    k_cg_params<<<1, CG_T, 0, L.stream>>>(S, w.red, VX_RED_BLOCKS, p.diff_cutoff, w.cells_cap); VX_COUNT(L);
-    k_cg_zero<<<grid, CG_T, 0, L.stream>>>(S, w.cg_cnt); VX_COUNT(L);
-    k_cg_cellid<<<grid, CG_T, 0, L.stream>>>(v, S, w.key0, w.val0, w.cg_cnt); VX_COUNT(L);
-    k_scan_sum<<<grid, CG_T, 0, L.stream>>>(&S->cncells, w.cg_cnt, w.cell_chunk_cnt); VX_COUNT(L);
-    k_scan_top<<<1, 1024, 0, L.stream>>>(&S->cncells, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
-    k_scan_apply<<<grid, CG_T, 0, L.stream>>>(&S->cncells, w.cg_cnt, w.cell_chunk_off, w.cg_start, &S->n);
+    vx_launch_pdl(k_cg_begin, 1, 1, 0, L.stream, S); VX_COUNT(L);
+    vx_launch_pdl(k_cg_bbox, VX_RED_BLOCKS, CG_T, 0, L.stream, v, S, w.red); VX_COUNT(L);
+    vx_launch_pdl(k_cg_params, 1, CG_T, 0, L.stream, S, w.red, VX_RED_BLOCKS, p.diff_cutoff, w.cells_cap); VX_COUNT(L);
+    vx_launch_pdl(k_cg_zero, grid, CG_T, 0, L.stream, S, w.cg_cnt); VX_COUNT(L);
+    vx_launch_pdl(k_cg_cellid, grid, CG_T, 0, L.stream, v, S, w.key0, w.val0, w.cg_cnt); VX_COUNT(L);
+    vx_launch_pdl(k_scan_sum, grid, CG_T, 0, L.stream, &S->cncells, w.cg_cnt, w.cell_chunk_cnt); VX_COUNT(L);
+    vx_launch_pdl(k_scan_top, 1, 1024, 0, L.stream, &S->cncells, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
+    vx_launch_pdl(k_scan_apply, grid, CG_T, 0, L.stream, &S->cncells, w.cg_cnt, w.cell_chunk_off, w.cg_start, &S->n);
     VX_COUNT(L);
     const int nb = bits_for(w.cells_cap);
     const int cur = vx_radix_sort(L, &S->n, w.key0, w.val0, w.key1, w.val1, nb, w.rs_hist, w.rs_off,
                                   w.rs_tiles_cap);
     const unsigned *skey = cur ? w.key1 : w.key0;
     const int *sorted = cur ? w.val1 : w.val0;
-    k_cg_gather<<<grid, CG_T, 0, L.stream>>>(v, S, sorted, skey, w.srt); VX_COUNT(L);
-    k_cg_row_items<<<grid, CG_T, 0, L.stream>>>(S, w.cg_start, w.row_items); VX_COUNT(L);
-    k_cg_row_scan<<<1, 1024, 0, L.stream>>>(S, w.row_items, w.row_item_off); VX_COUNT(L);
-    k_cg_items<<<grid, CG_T, 0, L.stream>>>(S, w.cg_start, w.row_items, w.row_item_off, w.items, w.items_cap);
+    vx_launch_pdl(k_cg_gather, grid, CG_T, 0, L.stream, v, S, sorted, skey, w.srt); VX_COUNT(L);
+    vx_launch_pdl(k_cg_row_items, grid, CG_T, 0, L.stream, S, w.cg_start, w.row_items); VX_COUNT(L);
+    vx_launch_pdl(k_cg_row_scan, 1, 1024, 0, L.stream, S, w.row_items, w.row_item_off); VX_COUNT(L);
+    vx_launch_pdl(k_cg_items, grid, CG_T, 0, L.stream, S, w.cg_start, w.row_items, w.row_item_off, w.items, w.items_cap);
     VX_COUNT(L);
     VX_EV(L, 2);
-    k_diff_cells<<<L.num_sms * 8, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.items,
+    vx_launch_pdl(k_diff_cells, L.num_sms * 8, CG_T, 0, L.stream, p, v, S, w.srt, skey, sorted, w.cg_start, w.items,
                                                        w.cg_wide);
     VX_COUNT(L);
-    k_diff_wide<<<L.num_sms * 4, CG_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide,
+    vx_launch_pdl(k_diff_wide, L.num_sms * 4, CG_T, 0, L.stream, p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide,
                                                       w.cg_huge);
     VX_COUNT(L);
-    k_diff_huge<<<L.num_sms * 2, WIDE_T, 0, L.stream>>>(p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_huge);
+    vx_launch_pdl(k_diff_huge, L.num_sms * 2, WIDE_T, 0, L.stream, p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_huge);
     VX_COUNT(L);
     VX_EV(L, 3);
     return cudaGetLastError();

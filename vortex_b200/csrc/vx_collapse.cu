@@ -22,6 +22,7 @@
 #include "vx_internal.cuh"
 
 __global__ void k_col_begin(VxScalars *S, int reset) {
+    VX_PDL_WAIT();
     if (reset) S->col_done = 0;
     if (S->col_done) return;
     S->col_n_before = S->n;
@@ -30,6 +31,7 @@ __global__ void k_col_begin(VxScalars *S, int reset) {
 }
 
 __global__ void k_col_bbox(VxView v, VxScalars *S) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     __shared__ unsigned long long sh[4][VX_THREADS];
     const long long n = S->n;
@@ -56,6 +58,7 @@ __global__ void k_col_bbox(VxView v, VxScalars *S) {
 // Cell size h = r (1 + 1e-6): any pair closer than r is in neighbouring cells.
 // When the box would need more than cells_cap cells, h grows.
 __global__ void k_col_grid(VxScalars *S, double r2, long long cells_cap) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     const long long n = S->n;
     if (n == 0) { S->gncells = 0; S->gnx = S->gny = 0; return; }
@@ -86,6 +89,7 @@ __device__ __forceinline__ void vx_cell_of(const VxScalars *S, double x, double 
 }
 
 __global__ void k_col_zero_cells(const VxScalars *S, int *cnt) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     const long long nc = S->gncells;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
@@ -95,6 +99,7 @@ __global__ void k_col_zero_cells(const VxScalars *S, int *cnt) {
 
 __global__ void k_col_count(VxView v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
                             int *has_app, int *first_app) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     const long long n = S->n;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -112,6 +117,7 @@ __global__ void k_col_count(VxView v, const VxScalars *S, int *cellid, int *cnt,
 
 // Exclusive scan of cnt[0, gncells) into start[], start[gncells] = total.
 __global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     __shared__ int sh[VX_THREADS];
     const long long nc = S->gncells;
@@ -132,6 +138,7 @@ __global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) 
 }
 
 __global__ void k_cell_chunk_scan(const VxScalars *S, const int *csum, long long *coff) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     __shared__ long long sh[1024];
     __shared__ long long carry;
@@ -158,6 +165,7 @@ __global__ void k_cell_chunk_scan(const VxScalars *S, const int *csum, long long
 
 __global__ void __launch_bounds__(VX_THREADS) k_cell_chunk_apply(const VxScalars *S, const int *cnt,
                                                                  const long long *coff, int *start) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     constexpr int PER = VX_CHUNK / VX_THREADS;
     __shared__ int sh[VX_THREADS];
@@ -193,6 +201,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_cell_chunk_apply(const VxScalars
 
 __global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *start, int *cnt,
                               int *sorted) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     const long long n = S->n;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -210,6 +219,7 @@ __global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *
 template <int PASS>
 __global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
                             const int *sorted, int *col, int *in_cnt, int *cand) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     const long long n = S->n;
     const long long gnx = S->gnx, gny = S->gny;
@@ -252,6 +262,7 @@ __global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *celli
 // 1 applied, 2 consumed before its turn.
 __global__ void k_col_resolve(VxScalars *S, const int *cand, const int *col, int *in_cnt,
                               int *has_app, int *first_app, int *cstate, int *cdec) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     __shared__ int undecided;
     const int nc = S->ncand;
@@ -297,6 +308,7 @@ template <int PASS>
 __global__ void k_col_merge(VxView v, const VxScalars *S, const int *cand, const int *col,
                             const int *cstate, const int *first_app, double *mx, double *my,
                             double *mg) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     const int nc = S->ncand;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
@@ -322,6 +334,7 @@ __global__ void k_col_merge(VxView v, const VxScalars *S, const int *cand, const
 
 __global__ void k_col_apply(VxView v, const VxScalars *S, const int *cand, const int *col,
                             const int *cstate, const double *mx, const double *my, const double *mg) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     const int nc = S->ncand;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
@@ -333,6 +346,7 @@ __global__ void k_col_apply(VxView v, const VxScalars *S, const int *cand, const
 }
 
 __global__ void k_col_end(VxScalars *S) {
+    VX_PDL_WAIT();
     if (S->col_done) return;
     if (S->n == S->col_n_before) S->col_done = 1;
 }
@@ -343,38 +357,38 @@ cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxVie
     if (!(r2 > 0.0) || n_col <= 0) return cudaSuccess;   // no pair can qualify
     const int grid = L.num_sms * 4;
     for (int cc = 0; cc < n_col; ++cc) {
-        k_col_begin<<<1, 1, 0, L.stream>>>(S, cc == 0); VX_COUNT(L);
-        k_col_bbox<<<grid, VX_THREADS, 0, L.stream>>>(v, S); VX_COUNT(L);
-        k_col_grid<<<1, 1, 0, L.stream>>>(S, r2, w.cells_cap); VX_COUNT(L);
-        k_col_zero_cells<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cell_cnt); VX_COUNT(L);
-        k_col_count<<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app,
+        vx_launch_pdl(k_col_begin, 1, 1, 0, L.stream, S, cc == 0); VX_COUNT(L);
+        vx_launch_pdl(k_col_bbox, grid, VX_THREADS, 0, L.stream, v, S); VX_COUNT(L);
+        vx_launch_pdl(k_col_grid, 1, 1, 0, L.stream, S, r2, w.cells_cap); VX_COUNT(L);
+        vx_launch_pdl(k_col_zero_cells, grid, VX_THREADS, 0, L.stream, S, w.cell_cnt); VX_COUNT(L);
+        vx_launch_pdl(k_col_count, grid, VX_THREADS, 0, L.stream, v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app,
                                                        w.first_app); VX_COUNT(L);
-        k_cell_chunk_sum<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cell_cnt, w.cell_chunk_cnt); VX_COUNT(L);
-        k_cell_chunk_scan<<<1, 1024, 0, L.stream>>>(S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
-        k_cell_chunk_apply<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cell_cnt, w.cell_chunk_off,
+        vx_launch_pdl(k_cell_chunk_sum, grid, VX_THREADS, 0, L.stream, S, w.cell_cnt, w.cell_chunk_cnt); VX_COUNT(L);
+        vx_launch_pdl(k_cell_chunk_scan, 1, 1024, 0, L.stream, S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
+        vx_launch_pdl(k_cell_chunk_apply, grid, VX_THREADS, 0, L.stream, S, w.cell_cnt, w.cell_chunk_off,
                                                               w.cell_start); VX_COUNT(L);
-        k_col_scatter<<<grid, VX_THREADS, 0, L.stream>>>(S, w.cellid, w.cell_start, w.cell_cnt,
+        vx_launch_pdl(k_col_scatter, grid, VX_THREADS, 0, L.stream, S, w.cellid, w.cell_start, w.cell_cnt,
                                                          w.sorted); VX_COUNT(L);
         if (pass == 1)
-            k_col_query<1><<<grid, VX_THREADS, 0, L.stream>>>(p, v, S, w.cellid, w.cell_start, w.sorted,
+            vx_launch_pdl(k_col_query<1>, grid, VX_THREADS, 0, L.stream, p, v, S, w.cellid, w.cell_start, w.sorted,
                                                               w.col, w.in_cnt, w.cand);
         else
-            k_col_query<2><<<grid, VX_THREADS, 0, L.stream>>>(p, v, S, w.cellid, w.cell_start, w.sorted,
+            vx_launch_pdl(k_col_query<2>, grid, VX_THREADS, 0, L.stream, p, v, S, w.cellid, w.cell_start, w.sorted,
                                                               w.col, w.in_cnt, w.cand);
         VX_COUNT(L);
-        k_col_resolve<<<1, 1024, 0, L.stream>>>(S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app,
+        vx_launch_pdl(k_col_resolve, 1, 1024, 0, L.stream, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app,
                                                 w.cstate, w.cdec); VX_COUNT(L);
         if (pass == 1)
-            k_col_merge<1><<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cand, w.col, w.cstate, w.first_app,
+            vx_launch_pdl(k_col_merge<1>, grid, VX_THREADS, 0, L.stream, v, S, w.cand, w.col, w.cstate, w.first_app,
                                                               w.mx, w.my, w.mg);
         else
-            k_col_merge<2><<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cand, w.col, w.cstate, w.first_app,
+            vx_launch_pdl(k_col_merge<2>, grid, VX_THREADS, 0, L.stream, v, S, w.cand, w.col, w.cstate, w.first_app,
                                                               w.mx, w.my, w.mg);
         VX_COUNT(L);
-        k_col_apply<<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.cand, w.col, w.cstate, w.mx, w.my, w.mg);
+        vx_launch_pdl(k_col_apply, grid, VX_THREADS, 0, L.stream, v, S, w.cand, w.col, w.cstate, w.mx, w.my, w.mg);
         VX_COUNT(L);
         vx_launch_compact_skip(L, p, v, S, w, &S->col_done);
-        k_col_end<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
+        vx_launch_pdl(k_col_end, 1, 1, 0, L.stream, S); VX_COUNT(L);
     }
     return cudaGetLastError();
 }

@@ -23,6 +23,7 @@ __device__ __forceinline__ bool vx_live(const VxView &v, long long p, double eps
 }
 
 __global__ void k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt, const int *skip) {
+    VX_PDL_WAIT();
     if (skip && *skip) return;
     __shared__ int sh[VX_THREADS];
     const long long n0 = S->n;
@@ -45,6 +46,7 @@ __global__ void k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt, const 
 // Single block: exclusive scan of the chunk counts, m, scan[m] and H.
 __global__ void k_cmp_scan(VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
                            const int *skip) {
+    VX_PDL_WAIT();
     if (skip && *skip) return;
     __shared__ long long sh[1024];
     __shared__ long long carry;
@@ -98,6 +100,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_cmp_classify(VxView v, const VxS
                                                              const long long *off, int *hole_pos,
                                                              int *hole_src, int *tail_src,
                                                              const int *skip) {
+    VX_PDL_WAIT();
     if (skip && *skip) return;
     constexpr int PER = VX_CHUNK / VX_THREADS;
     __shared__ int sh[VX_THREADS];
@@ -150,6 +153,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_cmp_classify(VxView v, const VxS
 __global__ void k_cmp_gather(VxView v, const VxScalars *S, const int *hole_pos, const int *hole_src,
                              const int *tail_src, double *hx, double *hy, double *hg, double *tx,
                              double *ty, const int *skip) {
+    VX_PDL_WAIT();
     if (skip && *skip) return;
     const long long n0 = S->c_n0, m = S->c_m, H = S->c_H;
     if (m == n0) return;
@@ -172,6 +176,7 @@ __global__ void k_cmp_gather(VxView v, const VxScalars *S, const int *hole_pos, 
 __global__ void k_cmp_scatter(VxView v, VxScalars *S, const int *hole_pos, const double *hx,
                               const double *hy, const double *hg, const double *tx, const double *ty,
                               const int *skip) {
+    VX_PDL_WAIT();
     if (skip && *skip) return;
     const long long n0 = S->c_n0, m = S->c_m, H = S->c_H;
     if (m != n0) {
@@ -194,13 +199,13 @@ __global__ void k_cmp_scatter(VxView v, VxScalars *S, const int *hole_pos, const
 cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const VxView &v,
                                    VxScalars *S, VxWork &w, const int *skip) {
     const int grid = L.num_sms * 4;
-    k_cmp_count<<<grid, VX_THREADS, 0, L.stream>>>(v, S, p.drop_eps, w.cmp_cnt, skip); VX_COUNT(L);
-    k_cmp_scan<<<1, 1024, 0, L.stream>>>(v, S, p.drop_eps, w.cmp_cnt, w.cmp_off, skip); VX_COUNT(L);
-    k_cmp_classify<<<grid, VX_THREADS, 0, L.stream>>>(v, S, p.drop_eps, w.cmp_off, w.hole_pos,
+    vx_launch_pdl(k_cmp_count, grid, VX_THREADS, 0, L.stream, v, S, p.drop_eps, w.cmp_cnt, skip); VX_COUNT(L);
+    vx_launch_pdl(k_cmp_scan, 1, 1024, 0, L.stream, v, S, p.drop_eps, w.cmp_cnt, w.cmp_off, skip); VX_COUNT(L);
+    vx_launch_pdl(k_cmp_classify, grid, VX_THREADS, 0, L.stream, v, S, p.drop_eps, w.cmp_off, w.hole_pos,
                                                       w.hole_src, w.tail_src, skip); VX_COUNT(L);
-    k_cmp_gather<<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.hole_pos, w.hole_src, w.tail_src,
+    vx_launch_pdl(k_cmp_gather, grid, VX_THREADS, 0, L.stream, v, S, w.hole_pos, w.hole_src, w.tail_src,
                                                     w.hx, w.hy, w.hg, w.tx, w.ty, skip); VX_COUNT(L);
-    k_cmp_scatter<<<grid, VX_THREADS, 0, L.stream>>>(v, S, w.hole_pos, w.hx, w.hy, w.hg, w.tx, w.ty,
+    vx_launch_pdl(k_cmp_scatter, grid, VX_THREADS, 0, L.stream, v, S, w.hole_pos, w.hx, w.hy, w.hg, w.tx, w.ty,
                                                      skip);
     VX_COUNT(L);
     return cudaGetLastError();

@@ -189,6 +189,7 @@ extern "C" vx_status vx_conf_default(vx_conf *c) {
 
 // ---------------------------------------------------------------------------
 __global__ void k_fill_tail(double *x, double *y, double *g, long long from, long long to) {
+    VX_PDL_WAIT();
     for (long long i = from + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < to;
          i += (long long)gridDim.x * blockDim.x) {
         x[i] = 4.0e5 + (double)i;
@@ -1075,6 +1076,7 @@ extern "C" vx_status vx_set_fmm(vx_sim *s, int fmm, int leaf) {
 extern "C" void *vx_get_stream(vx_sim *s) { return s ? (void *)s->stream : nullptr; }
 
 __global__ void k_points_begin(VxScalars *S, long long n) {
+    VX_PDL_WAIT();
     S->n = n;
     S->n0 = n;   // no point counts as born this step: no force terms
 }
@@ -1105,7 +1107,7 @@ extern "C" vx_status vx_move_points(vx_sim *s, double *x, double *y, double *g, 
     double *dst[5] = {dx, dy, dg, du, dv};
     for (int q = 0; q < 5; ++q)
         CU(cudaMemcpyAsync(dst[q], src[q], sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
-    k_points_begin<<<1, 1, 0, s->stream>>>(s->d_St, (long long)n);
+    vx_launch_pdl(k_points_begin, 1, 1, 0, s->stream, s->d_St, (long long)n);
     VxView pv;
     pv.x = dx; pv.y = dy; pv.g = dg; pv.ps = 1;
     pv.vx = du; pv.vy = dv; pv.vs = 1;

@@ -62,12 +62,14 @@ static_assert(FMM_P == 16, "reciprocal table length");
 
 // ---------------------------------------------------------------------------
 __global__ void k_fmm_begin(VxScalars *S) {
+    VX_PDL_WAIT();
     S->fb[0] = S->fb[1] = S->fb[2] = S->fb[3] = ~0ull;
     S->fnflag = 0;
     S->fnbrute = 0;
 }
 
 __global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
+    VX_PDL_WAIT();
     __shared__ unsigned long long sk[4][FMM_T];
     const long long n = S->n;
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
@@ -91,6 +93,7 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
 // Square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], reduced until
 // the leaf side is at least eps.
 __global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
+    VX_PDL_WAIT();
     const long long n = S->n;
     const double x0 = vx_dunkey(S->fb[0]), x1 = -vx_dunkey(S->fb[1]);
     const double y0 = vx_dunkey(S->fb[2]), y1 = -vx_dunkey(S->fb[3]);
@@ -110,6 +113,7 @@ __global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
 }
 
 __global__ void k_fmm_zero_cnt(const VxScalars *S, int *cnt) {
+    VX_PDL_WAIT();
     const long long tot = fmm_level_off(S->fL + 1);
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < tot;
          c += (long long)gridDim.x * blockDim.x)
@@ -127,6 +131,7 @@ __device__ __forceinline__ long long fmm_leaf(const VxScalars *S, double x, doub
 
 // Leaf of every source slot [0, s); counts at the leaf level.
 __global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
+    VX_PDL_WAIT();
     const long long s = S->fs;
     int *leafcnt = cnt + fmm_level_off(S->fL);
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < s;
@@ -140,6 +145,7 @@ __global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *v
 
 // Leaf starts: exclusive scan of the leaf counts (chunked, device length).
 __global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, const int *cnt, int *csum) {
+    VX_PDL_WAIT();
     __shared__ int sh[FMM_T];
     const long long len = S->fnleaves, nch = vx_ceil_div(len, VX_CHUNK);
     const int *c0 = cnt + fmm_level_off(S->fL);
@@ -158,6 +164,7 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, cons
 }
 
 __global__ void k_fmm_scan_top(const VxScalars *S, const int *csum, long long *coff) {
+    VX_PDL_WAIT();
     __shared__ long long sh[1024];
     __shared__ long long carry;
     const long long nch = vx_ceil_div(S->fnleaves, VX_CHUNK);
@@ -183,6 +190,7 @@ __global__ void k_fmm_scan_top(const VxScalars *S, const int *csum, long long *c
 
 __global__ void __launch_bounds__(FMM_T) k_fmm_scan_apply(const VxScalars *S, const int *cnt, const long long *coff,
                                                           int *start) {
+    VX_PDL_WAIT();
     constexpr int PER = VX_CHUNK / FMM_T;
     __shared__ int sh[FMM_T];
     const long long len = S->fnleaves, nch = vx_ceil_div(len, VX_CHUNK);
@@ -214,6 +222,7 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_scan_apply(const VxScalars *S, co
 // Leaf-sorted sources: position relative to the leaf centre (FP32 keeps the
 // local spacing accurate), G masked beyond n, leaf column.
 __global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
+    VX_PDL_WAIT();
     const long long s = S->fs, n = S->n;
     const unsigned m = 1u << S->fL;
     const double h = S->fside / (double)m;
@@ -232,6 +241,7 @@ __global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, co
 // not written (nothing reads their expansion).
 __global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const int *sorted,
                                                  cplx *M) {
+    VX_PDL_WAIT();
     const int L = S->fL;
     const long long m = 1LL << L, nl = m * m, n = S->n;
     const double h = S->fside / (double)m;
@@ -294,6 +304,7 @@ __device__ __forceinline__ void fmm_shift_table(cplx (*se)[FMM_P]) {
 // (parent, coefficient k); the thread of coefficient 0 also writes the
 // parent's vortex count (the sum of its children's).
 __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, cplx *M, int l) {
+    VX_PDL_WAIT();
     __shared__ cplx se[4][FMM_P];
     if (l + 1 > S->fL) return;
     fmm_shift_table(se);
@@ -457,6 +468,7 @@ __device__ __forceinline__ cplx l2l_term(const cplx *Lp, const cplx (*se)[FMM_P]
 
 __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
                                                        cplx *Loc, int l) {
+    VX_PDL_WAIT();
     __shared__ M2LShared T;
     if (l > S->fL) return;
     m2l_tables(T);
@@ -479,6 +491,7 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
 // of all of them.
 __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
                                                          cplx *Loc) {
+    VX_PDL_WAIT();
     __shared__ M2LShared T;
     const int hi = min(S->fL, M2L_SMALL);
     if (hi < 2) return;
@@ -504,6 +517,7 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, con
 // L2L into level l (3 <= l <= min(M2L_SMALL, L)) from level l-1, one thread
 // per (cell, coefficient); one launch per level.
 __global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const int *cnt, cplx *Loc, int l) {
+    VX_PDL_WAIT();
     __shared__ cplx se[4][FMM_P];
     if (l > min(S->fL, M2L_SMALL)) return;
     fmm_shift_table(se);
@@ -558,6 +572,7 @@ __device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gsl
 __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                    const int *sorted, const int *start, const int2 *items,
                                                    const cplx *Loc, int *flag_list) {
+    VX_PDL_WAIT();
     __shared__ float4 sxy[FMM_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
     __shared__ float2 sg[FMM_T / 2];    // (G_a, G_b)
     const int lane = threadIdx.x & 31;
@@ -701,6 +716,7 @@ __device__ __forceinline__ void fmm_ring_cell(int k, int q, int &dx, int &dy) {
 
 __global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const int *sorted,
                               const int *start, const int *flag_list, int *brute_list) {
+    VX_PDL_WAIT();
     const int nf = S->fnflag;
     const long long m = 1LL << S->fL;
     const double h = S->fside / (double)m;
@@ -758,6 +774,7 @@ __global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const i
 // thread keeping the three smallest of its stride, merged over the warp and
 // the block (the same set of sources as the ring search, so the same three).
 __global__ void __launch_bounds__(256) k_fmm_nn3_brute(VxView v, const VxScalars *S, const int *brute_list) {
+    VX_PDL_WAIT();
     __shared__ float sd[3][256 / 32];
     const int nb = S->fnbrute;
     const long long fs = S->fs;
@@ -797,6 +814,7 @@ __global__ void __launch_bounds__(256) k_fmm_nn3_brute(VxView v, const VxScalars
 // Near-field work items: every leaf's targets in chunks of FMM_W, counted per
 // leaf row (one warp per row, lanes over its leaves).
 __global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_items) {
+    VX_PDL_WAIT();
     const long long m = 1LL << S->fL;
     const int lane = threadIdx.x & 31;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -809,6 +827,7 @@ __global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_i
 }
 
 __global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
+    VX_PDL_WAIT();
     __shared__ long long sh[1024];
     const long long len = 1LL << S->fL;
     const long long per = vx_ceil_div(len, (long long)blockDim.x);
@@ -834,6 +853,7 @@ __global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long
 
 __global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row_items, const long long *off,
                             int2 *items, long long items_cap) {
+    VX_PDL_WAIT();
     const long long m = 1LL << S->fL;
     const int lane = threadIdx.x & 31;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -868,57 +888,57 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
                                    VxWork &w) {
     const int grid = L.num_sms * 4;
     const int Lmax = w.fmm_lmax;
-    k_fmm_begin<<<1, 1, 0, L.stream>>>(S); VX_COUNT(L);
-    k_fmm_bbox<<<grid, FMM_T, 0, L.stream>>>(v, S); VX_COUNT(L);
-    k_fmm_params<<<1, 1, 0, L.stream>>>(S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32); VX_COUNT(L);
-    k_fmm_zero_cnt<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_cnt); VX_COUNT(L);
-    k_fmm_leafid<<<grid, FMM_T, 0, L.stream>>>(v, S, w.key0, w.val0, w.fmm_cnt); VX_COUNT(L);
-    k_fmm_scan_sum<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_cnt, w.cell_chunk_cnt); VX_COUNT(L);
-    k_fmm_scan_top<<<1, 1024, 0, L.stream>>>(S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
-    k_fmm_scan_apply<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_cnt, w.cell_chunk_off, w.fmm_start); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_begin, 1, 1, 0, L.stream, S); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_bbox, grid, FMM_T, 0, L.stream, v, S); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_params, 1, 1, 0, L.stream, S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_zero_cnt, grid, FMM_T, 0, L.stream, S, w.fmm_cnt); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_leafid, grid, FMM_T, 0, L.stream, v, S, w.key0, w.val0, w.fmm_cnt); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_scan_sum, grid, FMM_T, 0, L.stream, S, w.fmm_cnt, w.cell_chunk_cnt); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_scan_top, 1, 1024, 0, L.stream, S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_scan_apply, grid, FMM_T, 0, L.stream, S, w.fmm_cnt, w.cell_chunk_off, w.fmm_start); VX_COUNT(L);
     const int cur = vx_radix_sort(L, &S->fs, w.key0, w.val0, w.key1, w.val1, 2 * Lmax <= 16 ? 16 : 24,
                                   w.rs_hist, w.rs_off, w.rs_tiles_cap);
     const unsigned *skey = cur ? w.key1 : w.key0;
     const int *sorted = cur ? w.val1 : w.val0;
-    k_fmm_gather<<<grid, FMM_T, 0, L.stream>>>(v, S, sorted, skey, w.srt); VX_COUNT(L);
-    k_fmm_p2m<<<grid * 4, 128, 0, L.stream>>>(v, S, w.fmm_start, sorted, (cplx *)w.fmm_M); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_gather, grid, FMM_T, 0, L.stream, v, S, sorted, skey, w.srt); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_p2m, grid * 4, 128, 0, L.stream, v, S, w.fmm_start, sorted, (cplx *)w.fmm_M); VX_COUNT(L);
     // the level loops cover the deepest level this capacity allows; kernels
     // of levels below the depth chosen on the device return at once
     for (int l = Lmax - 1; l >= 0; --l) {
         const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));
-        k_fmm_m2m<<<gm, 128, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
+        vx_launch_pdl(k_fmm_m2m, gm, 128, 0, L.stream, S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
     }
     {
         long long tiles = 0;
         for (int l = 2; l <= std::min(Lmax, M2L_SMALL); ++l) tiles += vx_ceil_div(1LL << (2 * l), 16LL);
         if (tiles > 0) {
-            k_fmm_m2l_small<<<(int)std::min<long long>(grid * 2, tiles), M2L_T, 0, L.stream>>>(
+            vx_launch_pdl(k_fmm_m2l_small, (int)std::min<long long>(grid * 2, tiles), M2L_T, 0, L.stream, 
                 S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L);
             VX_COUNT(L);
             for (int l = 3; l <= std::min(Lmax, M2L_SMALL); ++l) {
                 const int g = (int)std::min<long long>(grid, vx_ceil_div((1LL << (2 * l)) * FMM_P, 256));
-                k_fmm_l2l_small<<<g, 256, 0, L.stream>>>(S, w.fmm_cnt, (cplx *)w.fmm_L, l); VX_COUNT(L);
+                vx_launch_pdl(k_fmm_l2l_small, g, 256, 0, L.stream, S, w.fmm_cnt, (cplx *)w.fmm_L, l); VX_COUNT(L);
             }
         }
     }
     for (int l = M2L_SMALL + 1; l <= Lmax; ++l) {
         const long long t1 = vx_ceil_div(1LL << l, (long long)M2L_TILE);
         const int g = (int)std::min<long long>(grid * 2, t1 * t1);
-        k_fmm_m2l_l2l<<<g, M2L_T, 0, L.stream>>>(S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
+        vx_launch_pdl(k_fmm_m2l_l2l, g, M2L_T, 0, L.stream, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
         VX_COUNT(L);
     }
-    k_fmm_row_items<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_start, w.row_items); VX_COUNT(L);
-    k_fmm_row_scan<<<1, 1024, 0, L.stream>>>(S, w.row_items, w.row_item_off, w.items_cap); VX_COUNT(L);
-    k_fmm_items<<<grid, FMM_T, 0, L.stream>>>(S, w.fmm_start, w.row_items, w.row_item_off, w.items, w.items_cap);
+    vx_launch_pdl(k_fmm_row_items, grid, FMM_T, 0, L.stream, S, w.fmm_start, w.row_items); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_row_scan, 1, 1024, 0, L.stream, S, w.row_items, w.row_item_off, w.items_cap); VX_COUNT(L);
+    vx_launch_pdl(k_fmm_items, grid, FMM_T, 0, L.stream, S, w.fmm_start, w.row_items, w.row_item_off, w.items, w.items_cap);
     VX_COUNT(L);
     VX_EV(L, 0);
-    k_fmm_near<<<L.num_sms * 8, FMM_T, 0, L.stream>>>(p, v, S, w.srt, sorted, w.fmm_start, w.items,
+    vx_launch_pdl(k_fmm_near, L.num_sms * 8, FMM_T, 0, L.stream, p, v, S, w.srt, sorted, w.fmm_start, w.items,
                                                       (const cplx *)w.fmm_L, w.fmm_flags);
     VX_EV(L, 1);
     VX_COUNT(L);
-    k_fmm_nn3_fix<<<grid, FMM_T, 0, L.stream>>>(v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
+    vx_launch_pdl(k_fmm_nn3_fix, grid, FMM_T, 0, L.stream, v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
     VX_COUNT(L);
-    k_fmm_nn3_brute<<<grid, 256, 0, L.stream>>>(v, S, w.fmm_brute);
+    vx_launch_pdl(k_fmm_nn3_brute, grid, 256, 0, L.stream, v, S, w.fmm_brute);
     VX_COUNT(L);
     return cudaGetLastError();
 }

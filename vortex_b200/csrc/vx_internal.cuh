@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <utility>
 #include <stdint.h>
 #include <stdio.h>
 
@@ -240,6 +241,29 @@ struct VxLaunch {
     cudaEvent_t pair_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 #define VX_EV(L, k) do { if ((L).pair_ev[k]) cudaEventRecord((L).pair_ev[k], (L).stream); } while (0)
+
+// Programmatic dependent launch (sm_90+): a kernel launched by vx_launch_pdl
+// may be scheduled while its predecessor on the stream is still finishing,
+// which hides the launch gap between the many short kernels of a step.  Every
+// such kernel starts with VX_PDL_WAIT(), which returns once the predecessor
+// has completed and its writes are visible; nothing is read or written before
+// it.  (In a kernel launched the ordinary way the wait returns at once.)
+#define VX_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+template <typename... K, typename... A>
+inline cudaError_t vx_launch_pdl(void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                                 A &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 #define VX_COUNT(L) do { if ((L).launches) ++*(L).launches; } while (0)
 
 // Stage launchers (each returns the first CUDA error it saw).

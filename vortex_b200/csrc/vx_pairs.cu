@@ -32,6 +32,7 @@ int vx_pick_ksplit(long long n_upper, int tile, int num_sms) {
 // ---------------------------------------------------------------------------
 // Packed FP32 sources for the bulk form: (x, y, G, 0), G masked to 0 beyond n.
 __global__ void k_pack32(VxView v, const VxScalars *S, float4 *src, long long upto) {
+    VX_PDL_WAIT();
     const long long n = S->n;
     const long long s = vx_round32(n);
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < s;
@@ -79,6 +80,7 @@ __global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const V
                                                    const float4 *src32, const double *tx,
                                                    const double *ty, long long tstr, long long nt_in,
                                                    double *part, long long tstride, int K) {
+    VX_PDL_WAIT();
     constexpr int TPT = pairs_tpt(sizeof(T) == 4);
     constexpr int NOUT = NN3 ? 5 : 2;
     __shared__ SrcTile<T> st;
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars
                                                      const double *tx, const double *ty, long long tstr,
                                                      long long nt_in, double *part, long long tstride,
                                                      int K) {
+    VX_PDL_WAIT();
     constexpr int NOUT = NN3 ? 5 : 2;
     __shared__ float4 sm[PT];
     const long long n = S->n;
@@ -261,6 +264,7 @@ __global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars
 template <bool FP32>
 __global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, long long tstride,
                              int K) {
+    VX_PDL_WAIT();
     const long long n = S->n;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
@@ -285,6 +289,7 @@ __global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, l
 
 __global__ void k_probe_combine(const VxScalars *S, const double *part, long long tstride, int K,
                                 long long np, double *ovx, double *ovy, long long ostride) {
+    VX_PDL_WAIT();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < np;
          i += (long long)gridDim.x * blockDim.x) {
         double sx = 0.0, sy = 0.0;
@@ -324,6 +329,7 @@ template <typename T>
 __global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const VxScalars *S,
                                                      const float4 *src32, double *part,
                                                      long long tstride, int K) {
+    VX_PDL_WAIT();
     constexpr int TPT = pairs_tpt(sizeof(T) == 4);
     __shared__ SrcTile<T> st;
     const long long n = S->n;
@@ -391,6 +397,7 @@ __global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const
 
 __global__ void k_diff_combine(VxParams p, VxView v, const VxScalars *S, const double *part,
                                long long tstride, int K) {
+    VX_PDL_WAIT();
     const long long n = S->n;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
@@ -415,7 +422,7 @@ static int pair_grid(const VxLaunch &L) { return L.num_sms * 4; }
 static cudaError_t maybe_pack(const VxLaunch &L, const VxParams &p, const VxView &v,
                               VxScalars *S, VxWork &w) {
     if (p.prec != VX_PREC_FP32) return cudaSuccess;
-    k_pack32<<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.src32, w.cap);
+    vx_launch_pdl(k_pack32, L.num_sms * 4, 256, 0, L.stream, v, S, w.src32, w.cap);
     VX_COUNT(L);
     return cudaGetLastError();
 }
@@ -426,18 +433,18 @@ cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxVie
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32) {
         VX_EV(L, 0);
-        k_bs32_partial<true><<<pair_grid(L), PT, 0, L.stream>>>(p, S, w.src32, v.x, v.y, v.ps, -1, w.part,
+        vx_launch_pdl(k_bs32_partial<true>, pair_grid(L), PT, 0, L.stream, p, S, w.src32, v.x, v.y, v.ps, -1, w.part,
                                                                 tstride, K);
         VX_EV(L, 1);
         VX_COUNT(L);
-        k_bs_combine<true><<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.part, tstride, K);
+        vx_launch_pdl(k_bs_combine<true>, L.num_sms * 4, 256, 0, L.stream, v, S, w.part, tstride, K);
     } else {
         VX_EV(L, 0);
-        k_bs_partial<double, true><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, v.x, v.y, v.ps,
+        vx_launch_pdl(k_bs_partial<double, true>, pair_grid(L), PT, 0, L.stream, p, v, S, nullptr, v.x, v.y, v.ps,
                                                                       -1, w.part, tstride, K);
         VX_EV(L, 1);
         VX_COUNT(L);
-        k_bs_combine<false><<<L.num_sms * 4, 256, 0, L.stream>>>(v, S, w.part, tstride, K);
+        vx_launch_pdl(k_bs_combine<false>, L.num_sms * 4, 256, 0, L.stream, v, S, w.part, tstride, K);
     }
     VX_COUNT(L);
     return cudaGetLastError();
@@ -450,13 +457,13 @@ cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxVi
     const long long tstride = w.part_cap / (3LL * K);
     VX_EV(L, 2);
     if (p.prec == VX_PREC_FP32) {
-        k_diff_partial<float><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, w.src32, w.part, tstride, K);
+        vx_launch_pdl(k_diff_partial<float>, pair_grid(L), PT, 0, L.stream, p, v, S, w.src32, w.part, tstride, K);
     } else {
-        k_diff_partial<double><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, w.part, tstride, K);
+        vx_launch_pdl(k_diff_partial<double>, pair_grid(L), PT, 0, L.stream, p, v, S, nullptr, w.part, tstride, K);
     }
     VX_EV(L, 3);
     VX_COUNT(L);
-    k_diff_combine<<<L.num_sms * 4, 256, 0, L.stream>>>(p, v, S, w.part, tstride, K);
+    vx_launch_pdl(k_diff_combine, L.num_sms * 4, 256, 0, L.stream, p, v, S, w.part, tstride, K);
     VX_COUNT(L);
     return cudaGetLastError();
 }
@@ -468,13 +475,13 @@ cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &
     if (tstride < np) return cudaErrorInvalidValue;
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32)
-        k_bs32_partial<false><<<pair_grid(L), PT, 0, L.stream>>>(p, S, w.src32, px, py, pstride, np, w.part,
+        vx_launch_pdl(k_bs32_partial<false>, pair_grid(L), PT, 0, L.stream, p, S, w.src32, px, py, pstride, np, w.part,
                                                                  tstride, K);
     else
-        k_bs_partial<double, false><<<pair_grid(L), PT, 0, L.stream>>>(p, v, S, nullptr, px, py, pstride,
+        vx_launch_pdl(k_bs_partial<double, false>, pair_grid(L), PT, 0, L.stream, p, v, S, nullptr, px, py, pstride,
                                                                        np, w.part, tstride, K);
     VX_COUNT(L);
-    k_probe_combine<<<(int)vx_ceil_div(np, 256), 256, 0, L.stream>>>(S, w.part, tstride, K, np, ovx, ovy,
+    vx_launch_pdl(k_probe_combine, (int)vx_ceil_div(np, 256), 256, 0, L.stream, S, w.part, tstride, K, np, ovx, ovy,
                                                                       ostride);
     VX_COUNT(L);
     return cudaGetLastError();

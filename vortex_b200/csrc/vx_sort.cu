@@ -17,6 +17,7 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 
 __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const long long *d_n, const unsigned *keys, int shift,
                                                         int *hist, long long tiles_cap) {
+    VX_PDL_WAIT();
     __shared__ int cnt[256];
     const long long n = *d_n;
     const long long tiles = vx_ceil_div(n, RS_TILE);
@@ -39,6 +40,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const long long *d_n, co
 constexpr int RS_SCAN_T = 512;
 __global__ void __launch_bounds__(RS_SCAN_T) k_rs_scan(const long long *d_n, const int *hist, long long *off,
                                                        long long tiles_cap, long long *dtot) {
+    VX_PDL_WAIT();
     __shared__ long long wsum[RS_SCAN_T / 32];
     const long long tiles = vx_ceil_div(*d_n, RS_TILE);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -70,6 +72,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const long long *d_n,
                                                            const int *vals, unsigned *okeys, int *ovals, int shift,
                                                            const long long *off, long long tiles_cap,
                                                            const long long *dtot) {
+    VX_PDL_WAIT();
     static_assert(RS_THREADS == 256, "one thread per digit");
     __shared__ int warp_cnt[RS_WARPS][256];
     __shared__ long long base[256];
@@ -142,10 +145,10 @@ int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0
     for (int shift = 0; shift < nbits; shift += 8) {
         unsigned *ki = cur ? k1 : k0, *ko = cur ? k0 : k1;
         int *vi = cur ? v1 : v0, *vo = cur ? v0 : v1;
-        k_rs_hist<<<grid, RS_THREADS, 0, L.stream>>>(d_n, ki, shift, hist, tiles_cap); VX_COUNT(L);
-        k_rs_scan<<<256, RS_SCAN_T, 0, L.stream>>>(d_n, hist, off, tiles_cap, off + 256 * tiles_cap);
+        vx_launch_pdl(k_rs_hist, grid, RS_THREADS, 0, L.stream, d_n, ki, shift, hist, tiles_cap); VX_COUNT(L);
+        vx_launch_pdl(k_rs_scan, 256, RS_SCAN_T, 0, L.stream, d_n, hist, off, tiles_cap, off + 256 * tiles_cap);
         VX_COUNT(L);
-        k_rs_scatter<<<grid, RS_THREADS, 0, L.stream>>>(d_n, ki, vi, ko, vo, shift, off, tiles_cap,
+        vx_launch_pdl(k_rs_scatter, grid, RS_THREADS, 0, L.stream, d_n, ki, vi, ko, vo, shift, off, tiles_cap,
                                                          off + 256 * tiles_cap);
         VX_COUNT(L);
         cur ^= 1;

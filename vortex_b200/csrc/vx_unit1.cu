@@ -135,6 +135,7 @@ int ensure_wall_box(const vx_panel *d_pan) {
 }
 
 __global__ void k_u_set(VxScalars *S, long long n, long long n0, const double *vinf, const double *dg) {
+    VX_PDL_WAIT();
     S->n = n;
     S->n0 = n0;
     if (vinf) { S->vinf[0] = vinf[0]; S->vinf[1] = vinf[1]; }
@@ -144,6 +145,7 @@ __global__ void k_u_set(VxScalars *S, long long n, long long n0, const double *v
 // summ_Kernel (src/kernel.cu:1144-1157): d_g overwritten, F and M accumulated
 // onto the caller's values and then scaled.
 __global__ void k_u_sums(VxParams p, const VxScalars *S, double *d_g, double *F, double *M) {
+    VX_PDL_WAIT();
     if (d_g) d_g[0] = S->raw[0];
     if (F) {
         F[0] = (F[0] + S->raw[1]) * (p.rho / p.dt);
@@ -153,6 +155,7 @@ __global__ void k_u_sums(VxParams p, const VxScalars *S, double *d_g, double *F,
 }
 
 __global__ void k_u_tail(double *pos, long long from, long long to) {
+    VX_PDL_WAIT();
     for (long long i = from + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < to;
          i += (long long)gridDim.x * blockDim.x) {
         pos[3 * i] = 4.0e5 + (double)i;
@@ -398,6 +401,7 @@ int velocity_control(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *
 // rounded to float there, and so it is here.
 __global__ void k_u_relax(const double *pos, const double *venv, double *v, long long nt, double rel_t,
                           double dt) {
+    VX_PDL_WAIT();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nt;
          i += (long long)gridDim.x * blockDim.x) {
         if (!pos[3 * i + 2]) { v[2 * i] = 0.0; v[2 * i + 1] = 0.0; continue; }

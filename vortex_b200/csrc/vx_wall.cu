@@ -75,6 +75,7 @@ __device__ __forceinline__ void vx_wall_integral_bulk(float Ra0, float Ra1, floa
 template <typename T>
 __global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel *pan, const int *wstart,
                        const int *widx) {
+    VX_PDL_WAIT();
     const long long n = S->n;
     const T nu = (T)p.nu;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -125,9 +126,9 @@ cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v
                            const vx_panel *pan, const int *wstart, const int *widx) {
     if (p.wall_nx <= 0 || p.wall_ny <= 0) wstart = widx = nullptr;
     if (p.prec == VX_PREC_FP32)
-        k_wall<float><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan, wstart, widx);
+        vx_launch_pdl(k_wall<float>, L.num_sms * 8, 128, 0, L.stream, p, v, S, pan, wstart, widx);
     else
-        k_wall<double><<<L.num_sms * 8, 128, 0, L.stream>>>(p, v, S, pan, wstart, widx);
+        vx_launch_pdl(k_wall<double>, L.num_sms * 8, 128, 0, L.stream, p, v, S, pan, wstart, widx);
     VX_COUNT(L);
     return cudaGetLastError();
 }
