@@ -5,10 +5,11 @@
 // sums G_j exp(-r/d_i) terms; beyond r = c d_i (c = diff_cutoff, default 20)
 // a term is below e^-c of its strength, and in a uniform cloud all of them
 // together about (c+1) e^-c = 4e-8 of the sum (below its FP32 rounding), so
-// the bulk form sums only the pairs within c d_i.  Particles are binned into square cells of side h (h tracks the
-// mean 3-nearest distance), cell ids are sorted stably (radix sort: equal ids
-// keep index order, so every sum has a fixed order), and the cell-sorted
-// particles (x, y, G, d) are gathered into one float4 per particle.
+// the bulk form sums only the pairs within c d_i.  Particles are binned into
+// square cells of side h (h tracks the mean 3-nearest distance), put in cell
+// order with each cell's particles in index order (vx_bucket_order: every
+// sum then has a fixed order), and gathered into one float4 per particle
+// (x, y, G, d).
 //
 // Cell side h = c mean(d) / 8.  Work item = one warp's 32 consecutive
 // cell-sorted targets of one grid row.  The warp scans the rows within its
@@ -21,9 +22,6 @@
 // window and summed alone by one warp (k_diff_wide).  Each target is owned by
 // one warp, so the velocity is updated in place with no partial sums.
 #include "vx_internal.cuh"
-
-int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0, unsigned *k1, int *v1,
-                  int nbits, int *hist, long long *off, long long tiles_cap);
 
 constexpr int CG_T = 256;
 constexpr int CG_W = 32;       // targets per work item (one warp)
@@ -38,6 +36,7 @@ __global__ void k_cg_begin(VxScalars *S) {
     S->cb[0] = S->cb[1] = S->cb[2] = S->cb[3] = ~0ull;
     S->cnwide = 0;
     S->cnhuge = 0;
+    S->bk_nmid = S->bk_nbig = 0;
 }
 
 // Bounding box of the live particles and per-block sums of d (fixed grid:
@@ -636,12 +635,6 @@ __global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxSc
     if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);   // a warp's lanes counted the same rows
 }
 
-static int bits_for(long long cells) {
-    int b = 1;
-    while ((1LL << b) < cells && b < 32) ++b;
-    return ((b + 7) / 8) * 8;
-}
-
 // Build the grid and run the bulk diffusion.  Scratch from w; the collapse
 // chunk arrays are reused (the passes run one after the other on one stream).
 cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
@@ -656,11 +649,11 @@ cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, cons
     vx_launch_pdl(k_scan_top, 1, 1024, 0, L.stream, &S->cncells, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
     vx_launch_pdl(k_scan_apply, grid, CG_T, 0, L.stream, &S->cncells, w.cg_cnt, w.cell_chunk_off, w.cg_start, &S->n);
     VX_COUNT(L);
-    const int nb = bits_for(w.cells_cap);
-    const int cur = vx_radix_sort(L, &S->n, w.key0, w.val0, w.key1, w.val1, nb, w.rs_hist, w.rs_off,
-                                  w.rs_tiles_cap);
-    const unsigned *skey = cur ? w.key1 : w.key0;
-    const int *sorted = cur ? w.val1 : w.val0;
+    // cell order: each cell's vortices in index order (a stable sort by cell)
+    vx_bucket_order(L, S, &S->n, &S->cncells, w.key0, w.cg_start, w.cg_cnt, nullptr, w.key1, w.val1, w.bk_mid, w.bk_big,
+                    w.val0);
+    const unsigned *skey = w.key1;
+    const int *sorted = w.val1;
     vx_launch_pdl(k_cg_gather, grid, CG_T, 0, L.stream, v, S, sorted, skey, w.srt); VX_COUNT(L);
     vx_launch_pdl(k_cg_row_items, grid, CG_T, 0, L.stream, S, w.cg_start, w.row_items); VX_COUNT(L);
     vx_launch_pdl(k_cg_row_scan, 1, 1024, 0, L.stream, S, w.row_items, w.row_item_off); VX_COUNT(L);

@@ -247,13 +247,11 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.red, VX_RED_BLOCKS * 4);
     // neighbour-list grid of the bulk form
     A(w.key0, cap); A(w.key1, cap); A(w.val0, cap); A(w.val1, cap);
-    w.rs_tiles_cap = vx_rs_tiles_cap(cap);
-    A(w.rs_hist, 256 * w.rs_tiles_cap); A(w.rs_off, 256 * (w.rs_tiles_cap + 1));
     A(w.cg_cnt, w.cells_cap); A(w.cg_start, w.cells_cap + 1);
     A(w.srt, cap);
     w.items_cap = cap / 32 + w.cells_cap + 2;
     A(w.items, w.items_cap);
-    A(w.cg_wide, cap); A(w.cg_huge, cap);
+    A(w.cg_wide, cap); A(w.cg_huge, cap); A(w.bk_mid, cap / 16 + 2); A(w.bk_big, cap / 128 + 2);
     A(w.row_items, w.cells_cap + 1); A(w.row_item_off, w.cells_cap + 1);
     // quadtree of the bulk-form Biot-Savart
     w.fmm_lmax = vx_fmm_max_level(cap);

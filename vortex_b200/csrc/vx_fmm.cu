@@ -34,9 +34,6 @@
 
 #include "vx_internal.cuh"
 
-int vx_radix_sort(const VxLaunch &L, const long long *d_n, unsigned *k0, int *v0, unsigned *k1, int *v1,
-                  int nbits, int *hist, long long *off, long long tiles_cap);
-
 constexpr int FMM_P = VX_FMM_P;  // expansion terms
 constexpr int FMM_T = 256;
 constexpr int FMM_W = 32;        // targets per near-field work item (one warp)
@@ -66,6 +63,7 @@ __global__ void k_fmm_begin(VxScalars *S) {
     S->fb[0] = S->fb[1] = S->fb[2] = S->fb[3] = ~0ull;
     S->fnflag = 0;
     S->fnbrute = 0;
+    S->bk_nmid = S->bk_nbig = 0;
 }
 
 __global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
@@ -108,6 +106,7 @@ __global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
     S->fy0 = 0.5 * (y0 + y1) - 0.5 * side;
     S->fside = side;
     S->fL = L;
+    S->fcnt_off = fmm_level_off(L);
     S->fnleaves = 1LL << (2 * L);
     S->fs = vx_round32(n);   // sources include the round-32 padding (3-nearest)
 }
@@ -896,10 +895,11 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     vx_launch_pdl(k_fmm_scan_sum, grid, FMM_T, 0, L.stream, S, w.fmm_cnt, w.cell_chunk_cnt); VX_COUNT(L);
     vx_launch_pdl(k_fmm_scan_top, 1, 1024, 0, L.stream, S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
     vx_launch_pdl(k_fmm_scan_apply, grid, FMM_T, 0, L.stream, S, w.fmm_cnt, w.cell_chunk_off, w.fmm_start); VX_COUNT(L);
-    const int cur = vx_radix_sort(L, &S->fs, w.key0, w.val0, w.key1, w.val1, 2 * Lmax <= 16 ? 16 : 24,
-                                  w.rs_hist, w.rs_off, w.rs_tiles_cap);
-    const unsigned *skey = cur ? w.key1 : w.key0;
-    const int *sorted = cur ? w.val1 : w.val0;
+    // leaf order: each leaf's sources in index order (a stable sort by leaf)
+    vx_bucket_order(L, S, &S->fs, &S->fnleaves, w.key0, w.fmm_start, w.fmm_cnt, &S->fcnt_off, w.key1, w.val1,
+                    w.bk_mid, w.bk_big, w.val0);
+    const unsigned *skey = w.key1;
+    const int *sorted = w.val1;
     vx_launch_pdl(k_fmm_gather, grid, FMM_T, 0, L.stream, v, S, sorted, skey, w.srt); VX_COUNT(L);
     vx_launch_pdl(k_fmm_p2m, grid * 4, 128, 0, L.stream, v, S, w.fmm_start, sorted, (cplx *)w.fmm_M); VX_COUNT(L);
     // the level loops cover the deepest level this capacity allows; kernels

@@ -94,6 +94,8 @@ struct VxScalars {
     long long fnleaves, fs;
     int fL, fnflag;
     int fnbrute;           // flagged targets left to the whole-set 3-nearest scan
+    int bk_nmid, bk_nbig;  // buckets of 17..128 / more elements in the running bucket order (vx_sort.cu)
+    long long fcnt_off;    // offset of the leaf level in the quadtree's count array
     // pair evaluations executed by the bulk-form near-field and diffusion
     // kernels since the counters were last cleared
     unsigned long long pairs_bs, pairs_diff;
@@ -140,15 +142,13 @@ struct VxWork {
     // neighbour-list grid (bulk form): radix-sort buffers, cells, sorted sources
     unsigned *key0, *key1;
     int *val0, *val1;
-    int *rs_hist;
-    long long *rs_off;
-    long long rs_tiles_cap;
     int *cg_cnt, *cg_start;
     float4 *srt;
     int2 *items;             // (row, first sorted slot) of each target segment
     long long items_cap;
     int *cg_wide;            // sorted slots of the diffusion targets summed one warp each
     int *cg_huge;            // sorted slots of those summed one block each
+    int *bk_mid, *bk_big;    // buckets of 17..128 / more than 128 elements (vx_bucket_order)
     int *row_items;
     long long *row_item_off;
     // quadtree: counts and expansions of every level up to fmm_lmax
@@ -308,7 +308,12 @@ void vx_set_error(const char *fmt, ...);
 #include <vector>
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms);
 long long vx_work_bytes(long long cap, int P32, int num_sms);
-long long vx_rs_tiles_cap(long long cap);
+// Stable order by bucket from bucket counts (used up, then restored) and
+// starts: (okey, oval) = keys and element indices in bucket order, elements
+// of a bucket in index order (vx_sort.cu).
+cudaError_t vx_bucket_order(const VxLaunch &L, VxScalars *S, const long long *d_n, const long long *d_nbuckets,
+                            const unsigned *key, const int *start, int *cnt, const long long *d_cnt_off,
+                            unsigned *okey, int *oval, int *mid, int *big, int *scratch);
 int vx_fmm_max_level(long long cap);
 long long vx_fmm_cells(int lmax);         // cells of all levels 0..lmax
 constexpr int VX_BF_P = 48;          // terms of the birth far-field expansion
