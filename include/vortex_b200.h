@@ -251,6 +251,12 @@ vx_status vx_set_fmm(vx_sim *sim, int fmm, int leaf);
  * bulk form's birth terms use, evaluated on device arrays of n floats. */
 vx_status vx_eval_bulk_atan2(const float *y, const float *x, float *out, int64_t n);
 
+/* Validation hook (no counterpart in the reference): the order the particle
+ * grids use, for n keys below nb (device arrays): element indices by key,
+ * equal keys in index order (a stable sort by key), written to `order`.
+ * Allocates its own scratch. */
+vx_status vx_eval_bucket_order(const unsigned *key, int64_t n, int64_t nb, int *order);
+
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);
 

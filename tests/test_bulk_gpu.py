@@ -305,3 +305,24 @@ def test_bulk_atan2_against_float64():
     assert np.max(np.abs(got - ref)[small] / np.abs(ref[small])) <= 2.5e-7
     assert np.all(got[ref == 0] == 0)
     assert np.array_equal(np.signbit(got[:4]), np.signbit(ref[:4]))
+
+
+def test_bucket_order_is_the_stable_sort():
+    """The grids' bucket order (slots from the counts, then each bucket in
+    index order by rank counting: a thread up to 16, a warp up to 128, a
+    block beyond, through scratch above 4096) against numpy's stable argsort,
+    on buckets of every size class, twice (the counts are used up and must
+    come back)."""
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(5)
+    sizes = [0, 1, 2, 16, 17, 31, 32, 33, 128, 129, 700, 4096, 4097, 9000] + list(rng.integers(0, 40, 3000))
+    keys = np.concatenate([np.full(s, b, dtype=np.uint32) for b, s in enumerate(sizes)])
+    keys = keys[rng.permutation(len(keys))]
+    nb = len(sizes)
+    dk = torch.from_numpy(keys.view(np.int32)).cuda()
+    for _ in range(2):
+        out = torch.empty(len(keys), dtype=torch.int32, device="cuda")
+        assert N.lib().vx_eval_bucket_order(C.c_void_p(dk.data_ptr()), C.c_int64(len(keys)), C.c_int64(nb),
+                                            C.c_void_p(out.data_ptr())) == 0
+        assert np.array_equal(out.cpu().numpy(), np.argsort(keys, kind="stable"))

@@ -5,6 +5,7 @@
 // Equal keys keep their input order, so sorting particle indices by cell gives
 // a deterministic order inside every cell.
 #include <climits>
+#include <vector>
 
 #include "vx_internal.cuh"
 
@@ -135,4 +136,55 @@ cudaError_t vx_bucket_order(const VxLaunch &L, VxScalars *S, const long long *d_
     vx_launch_pdl(k_bk_order_big, L.num_sms, BK_T, 0, L.stream, S, start, big, oval, scratch);
     VX_COUNT(L);
     return cudaGetLastError();
+}
+
+// Validation hook: the bucket order of n keys (device array, each below nb)
+// into `order` (device array of n element indices), with counts and starts
+// computed on the host.  Allocates its own scratch; not for the step path.
+extern "C" vx_status vx_eval_bucket_order(const unsigned *key, int64_t n, int64_t nb, int *order) {
+    if (n < 0 || nb < 1 || n > INT_MAX || (n > 0 && (!key || !order))) return VX_ERR_ARG;
+    if (n == 0) return VX_OK;
+    std::vector<unsigned> hk((size_t)n);
+    if (cudaMemcpy(hk.data(), key, sizeof(unsigned) * n, cudaMemcpyDeviceToHost) != cudaSuccess) return VX_ERR_CUDA;
+    std::vector<int> cnt((size_t)nb, 0), start((size_t)nb + 1, 0);
+    for (unsigned k : hk) {
+        if ((int64_t)k >= nb) return VX_ERR_ARG;
+        ++cnt[k];
+    }
+    for (int64_t b = 0; b < nb; ++b) start[b + 1] = start[b] + cnt[b];
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    void *mem[8] = {};
+    const size_t sz[8] = {sizeof(VxScalars), 2 * sizeof(long long), sizeof(int) * (nb + 1), sizeof(int) * nb,
+                          sizeof(unsigned) * n, sizeof(int) * (n / 16 + 2), sizeof(int) * (n / 128 + 2),
+                          sizeof(int) * n};
+    vx_status st = VX_OK;
+    for (int q = 0; q < 8 && st == VX_OK; ++q)
+        if (cudaMalloc(&mem[q], sz[q]) != cudaSuccess) st = VX_ERR_NOMEM;
+    if (st == VX_OK) {
+        VxScalars *S = (VxScalars *)mem[0];
+        long long *dn = (long long *)mem[1];
+        const long long hn[2] = {(long long)n, (long long)nb};
+        int *dstart = (int *)mem[2], *dcnt = (int *)mem[3];
+        bool ok = cudaMemset(S, 0, sizeof(VxScalars)) == cudaSuccess &&
+                  cudaMemcpy(dn, hn, sizeof(hn), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(dstart, start.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(dcnt, cnt.data(), sizeof(int) * nb, cudaMemcpyHostToDevice) == cudaSuccess;
+        if (ok) {
+            VxLaunch L;
+            L.stream = 0;
+            L.launches = nullptr;
+            L.num_sms = sms;
+            ok = vx_bucket_order(L, S, dn, dn + 1, key, dstart, dcnt, nullptr, (unsigned *)mem[4], order,
+                                 (int *)mem[5], (int *)mem[6], (int *)mem[7]) == cudaSuccess &&
+                 cudaDeviceSynchronize() == cudaSuccess;
+        }
+        std::vector<int> back((size_t)nb);
+        if (ok) ok = cudaMemcpy(back.data(), dcnt, sizeof(int) * nb, cudaMemcpyDeviceToHost) == cudaSuccess;
+        if (ok && back != cnt) st = VX_ERR_DEVICE;   // the counts must come back as they went in
+        if (!ok) st = VX_ERR_CUDA;
+    }
+    for (void *p : mem) if (p) cudaFree(p);
+    return st;
 }
