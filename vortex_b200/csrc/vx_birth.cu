@@ -791,7 +791,7 @@ static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView
     const int grid = (int)min((long long)tiles * rhs_chunks, (long long)L.num_sms * 16);
     const bool far = p.prec == VX_PREC_FP32 && p.birth_far;
     if (far) {
-        const int nb = std::min(2 * L.num_sms, VX_BF_MAX_BLOCKS);
+        const int nb = std::min(2 * vx_full_sms(L), VX_BF_MAX_BLOCKS);
         vx_launch_pdl(k_bf_far, nb, BF_T, 0, L.stream, p, v, S, w.bf_part, w.bf_cnt); VX_COUNT(L);
         vx_launch_pdl(k_bf_scan, 1, BF_SCAN_T, 0, L.stream, S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef); VX_COUNT(L);
         vx_launch_pdl(k_bf_scatter, nb, BF_T, 0, L.stream, p, v, S, w.bf_off, w.bf_near); VX_COUNT(L);

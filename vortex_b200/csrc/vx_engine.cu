@@ -75,12 +75,17 @@ struct vx_sim {
     std::vector<void *> work_allocs;
     long long n_upper = 0;
     long long launches = 0;
-    // graph
+    // step graphs: a few instantiated shapes, least recently used evicted
+    // (the source count moves a shape key back and forth across a power of
+    // two; capacity growth drops them all)
     bool use_graph = true;
-    cudaGraphExec_t gexec = nullptr;
-    long long g_cap = -1;
-    int g_kv = -1, g_rhs = -1;
-    long long g_launches = 0;
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        int kv = -1, rhs = -1, sms = -1;
+        long long launches = 0, used = 0;
+    };
+    StepGraph graphs[4];
+    long long graph_clock = 0;
     // timing
     bool timing = false;
     cudaEvent_t ev[6] = {};     // stage boundaries
@@ -283,9 +288,10 @@ static vx_status alloc_work(vx_sim *s, long long cap) {
 }
 
 static void drop_graph(vx_sim *s) {
-    if (s->gexec) cudaGraphExecDestroy(s->gexec);
-    s->gexec = nullptr;
-    s->g_cap = -1;
+    for (auto &g : s->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = vx_sim::StepGraph();
+    }
 }
 
 // Grow the particle store to at least `need` slots, keeping every slot's
@@ -338,17 +344,33 @@ static vx_status ensure_capacity(vx_sim *s) {
 // Source chunks of the birth right-hand side: enough (panel tile, chunk)
 // items for every SM to hold several blocks, within the partial-sum buffer
 // (at most num_sms * 4 chunks).
+// The launch shapes below follow the host's upper bound of the source count
+// rounded up to a power of two, so that they (and the step graph holding
+// them) change only when that bound crosses one, not every few steps.
+static long long pow2_ceil(long long n) {
+    long long q = 1;
+    while (q < n) q <<= 1;
+    return q;
+}
+
 static int rhs_chunks_for(vx_sim *s) {
     const int tiles = (s->P + 127) / 128;
     long long want = std::max(1LL, (long long)s->num_sms * 16 / tiles);
     want = std::min<long long>(want, (long long)s->num_sms * 4);
-    long long bysrc = std::max(1LL, vx_ceil_div(s->n_upper, 1024));
+    long long bysrc = std::max(1LL, vx_ceil_div(pow2_ceil(s->n_upper), 1024));
     return (int)std::min(want, bysrc);
+}
+
+// SMs a step's grid-stride launches are sized for: one per 2048 sources of
+// the rounded bound, at least 4, at most the device's.
+static int step_sms_for(vx_sim *s) {
+    const long long q = pow2_ceil(s->n_upper + s->P) / 2048;
+    return (int)std::max(4LL, std::min((long long)s->num_sms, q));
 }
 
 static int kv_for(vx_sim *s) {
     const int tile = s->prm.prec == VX_PREC_FP32 ? 1024 : 512;
-    return vx_pick_ksplit(s->n_upper + s->P, tile, s->num_sms);
+    return vx_pick_ksplit(pow2_ceil(s->n_upper + s->P), tile, s->num_sms);
 }
 
 // ---------------------------------------------------------------------------
@@ -826,6 +848,8 @@ extern "C" vx_status vx_get_matrix(vx_sim *s, double *minv) {
 // ---------------------------------------------------------------------------
 static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
     VxLaunch L = launch_of(s);
+    L.num_sms = step_sms_for(s);
+    L.full_sms = s->num_sms;
     VxView v = view_of(s);
     const VxParams &p = s->prm;
     cudaError_t e = cudaSuccess;
@@ -893,9 +917,16 @@ static vx_status step_once(vx_sim *s) {
         s->n_upper += s->P;
         return VX_OK;
     }
-    const int kv = kv_for(s), rc = rhs_chunks_for(s);
-    if (!s->gexec || s->g_cap != s->cap || s->g_kv != kv || s->g_rhs != rc) {
-        drop_graph(s);
+    const int kv = kv_for(s), rc = rhs_chunks_for(s), sms = step_sms_for(s);
+    vx_sim::StepGraph *sg = nullptr;
+    for (auto &g : s->graphs)
+        if (g.exec && g.kv == kv && g.rhs == rc && g.sms == sms) sg = &g;
+    if (!sg) {
+        sg = &s->graphs[0];
+        for (auto &g : s->graphs)
+            if (!g.exec || (sg->exec && g.used < sg->used)) sg = &g;
+        if (sg->exec) cudaGraphExecDestroy(sg->exec);
+        *sg = vx_sim::StepGraph();
         cudaGraph_t graph;
         long long before = s->launches;
         CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -905,15 +936,22 @@ static vx_status step_once(vx_sim *s) {
             vx_set_error("graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
             return VX_ERR_CUDA;
         }
-        s->g_launches = s->launches - before;
+        sg->launches = s->launches - before;
         s->launches = before;
-        e = cudaGraphInstantiate(&s->gexec, graph, 0);
+        e = cudaGraphInstantiate(&sg->exec, graph, 0);
         cudaGraphDestroy(graph);
-        if (e != cudaSuccess) { vx_set_error("graph instantiate: %s", cudaGetErrorString(e)); return VX_ERR_CUDA; }
-        s->g_cap = s->cap; s->g_kv = kv; s->g_rhs = rc;
+        if (e != cudaSuccess) {
+            sg->exec = nullptr;
+            vx_set_error("graph instantiate: %s", cudaGetErrorString(e));
+            return VX_ERR_CUDA;
+        }
+        sg->kv = kv;
+        sg->rhs = rc;
+        sg->sms = sms;
     }
-    CU(cudaGraphLaunch(s->gexec, s->stream));
-    s->launches += s->g_launches;
+    sg->used = ++s->graph_clock;
+    CU(cudaGraphLaunch(sg->exec, s->stream));
+    s->launches += sg->launches;
     s->n_upper += s->P;
     return VX_OK;
 }

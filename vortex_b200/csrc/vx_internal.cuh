@@ -235,11 +235,20 @@ __device__ __forceinline__ double vx_dunkey(unsigned long long k) {
 struct VxLaunch {
     cudaStream_t stream;
     long long *launches;   // host counter (may be null)
+    // SMs the launch grids are sized for.  A step of a small body sizes them
+    // for a share of the GPU that follows its source count (grid-stride
+    // kernels: same results, fewer idle blocks, so the kernels of many
+    // small bodies on concurrent streams overlap); full_sms (0: num_sms)
+    // stays the device's count for the kernels whose work does not scale
+    // with the count (the all-pairs sums) or whose results depend on the
+    // grid (the birth far field's per-block partials).
     int num_sms;
+    int full_sms = 0;
     // optional events recorded around the Biot-Savart and diffusion pair
     // kernels: [0,1] Biot-Savart, [2,3] diffusion (null: not recorded)
     cudaEvent_t pair_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
+inline int vx_full_sms(const VxLaunch &L) { return L.full_sms > 0 ? L.full_sms : L.num_sms; }
 #define VX_EV(L, k) do { if ((L).pair_ev[k]) cudaEventRecord((L).pair_ev[k], (L).stream); } while (0)
 
 // Programmatic dependent launch (sm_90+): a kernel launched by vx_launch_pdl

@@ -417,7 +417,7 @@ __global__ void k_diff_combine(VxParams p, VxView v, const VxScalars *S, const d
 }
 
 // ---------------------------------------------------------------------------
-static int pair_grid(const VxLaunch &L) { return L.num_sms * 4; }
+static int pair_grid(const VxLaunch &L) { return vx_full_sms(L) * 4; }
 
 static cudaError_t maybe_pack(const VxLaunch &L, const VxParams &p, const VxView &v,
                               VxScalars *S, VxWork &w) {
