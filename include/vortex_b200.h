@@ -220,10 +220,12 @@ vx_status vx_step_many(vx_sim *const *sims, int count, int64_t nsteps);
  * process): a request loop with continuous batching.  Requests (one body
  * each: conf, panels, starting vortices, step count) wait in arrival order
  * until a slot is free and the device-byte budget holds their
- * vx_estimate_bytes at n + P * nsteps; admitted bodies stay resident; every
- * tick advances all resident bodies one step, launched on their own streams
- * before any wait, and releases the finished ones.  Results do not depend
- * on what else runs. */
+ * vx_estimate_bytes at n + P * nsteps; admitted bodies stay resident, each
+ * with at most one step in flight on its own stream; a tick launches the
+ * next step of every resident body with none in flight, waits until at
+ * least one step has finished, collects every finished step and launches
+ * that body's next one, and releases the finished bodies.  Results do not
+ * depend on what else runs. */
 typedef struct vx_server vx_server;
 vx_status vx_server_create(int device, int64_t budget_bytes, int max_active, vx_server **out);
 vx_status vx_server_destroy(vx_server *srv);
@@ -231,7 +233,8 @@ vx_status vx_server_destroy(vx_server *srv);
 vx_status vx_server_submit(vx_server *srv, const vx_conf *conf, const vx_panel *panels, int64_t P,
                            const double *x, const double *y, const double *g, int64_t n, int64_t nsteps,
                            int64_t *id);
-/* Admit, step every resident body once, retire; counts after the tick. */
+/* Admit, launch, collect at least one finished step, retire; counts after
+ * the tick. */
 vx_status vx_server_tick(vx_server *srv, int64_t *active, int64_t *queued);
 /* state: 0 queued, 1 resident, 2 done, 3 failed; forces: (dg, Fx, Fy, M)
  * per completed step, at most cap_steps steps copied. */

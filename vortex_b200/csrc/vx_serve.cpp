@@ -4,12 +4,16 @@
 // steps).  Requests wait in arrival order until a slot is free and the
 // device-byte budget holds their estimate (vx_estimate_bytes at the largest
 // particle count the run can reach: start + P per step); then the body is
-// created and stays resident until its last step.  Every tick advances every
-// resident body by one step: all steps are launched on the bodies' own
-// streams before any is waited for, so bodies of different sizes overlap on
-// the device.  Finished bodies are released at once, which frees their slot
-// and budget for the next arrivals.  Each body runs in its own handle with
-// deterministic kernels, so its results do not depend on what else runs.
+// created and stays resident until its last step.  Each body has at most one
+// step in flight on its own stream; a tick launches the next step of every
+// resident body that has none in flight, waits until at least one step has
+// finished, collects every finished step (forces, count) and launches that
+// body's next step at once.  So no body waits for the slowest one: bodies of
+// different sizes overlap on the device and a small body takes many steps
+// while a large one takes one.  Finished bodies are released at once, which
+// frees their slot and budget for the next arrivals.  Each body runs in its
+// own handle with deterministic kernels, so its results do not depend on what
+// else runs.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -41,6 +45,8 @@ struct Request {
     int state = 0;            // 0 queued, 1 resident, 2 done, 3 failed
     vx_sim *sim = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool inflight = false;    // a step launched and not yet collected
+    int64_t launch_seq = 0;   // order of that launch (the oldest is waited for)
     int64_t done_steps = 0;
     std::vector<double> forces;   // 4 per step: dg, Fx, Fy, M
     int64_t n_final = 0;
@@ -68,9 +74,44 @@ struct vx_server {
     std::vector<double> step_ms;      // device time of every body step
     std::vector<double> ttc_s;        // submit -> finish of every finished request
     double active_sum = 0.0;
-    int64_t ticks = 0, body_steps = 0;
+    int64_t ticks = 0, body_steps = 0, launch_seq = 0;
     double particle_steps = 0.0;      // sum over body steps of the particle count
 };
+
+// Launch the next step of resident body r on its stream, between its events.
+static void launch_step(vx_server *S, Request *r) {
+    cudaStream_t st = (cudaStream_t)vx_get_stream(r->sim);
+    cudaEventRecord(r->e0, st);
+    if (vx_step(r->sim, 1) != VX_OK) {
+        r->state = 3;
+        return;
+    }
+    cudaEventRecord(r->e1, st);
+    r->inflight = true;
+    r->launch_seq = ++S->launch_seq;
+}
+
+// Collect r's finished step: its device time, forces and count.
+static void collect_step(vx_server *S, Request *r) {
+    r->inflight = false;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->e0, r->e1);
+    double st9[9];
+    if (vx_get_state(r->sim, st9) != VX_OK) {
+        r->state = 3;
+        return;
+    }
+    const int64_t n = (int64_t)st9[0];
+    S->step_ms.push_back(ms);
+    S->body_steps += 1;
+    S->particle_steps += (double)n;
+    r->forces.insert(r->forces.end(), st9 + 5, st9 + 9);
+    r->done_steps += 1;
+    if (r->done_steps == r->steps) {
+        r->n_final = n;
+        r->state = 2;
+    }
+}
 
 static vx_status release(vx_server *S, Request *r) {
     if (r->sim) vx_destroy(r->sim);
@@ -133,7 +174,7 @@ extern "C" vx_status vx_server_submit(vx_server *S, const vx_conf *conf, const v
     return VX_OK;
 }
 
-// Admit what fits, advance every resident body by one step, retire the
+// Admit what fits, launch and collect steps as above, retire the
 // finished ones.  *active: bodies resident after the tick; *queued: waiting.
 extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queued) {
     if (!S) return VX_ERR_ARG;
@@ -162,36 +203,38 @@ extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queu
         r->t_admit = now_s();
         S->active.push_back(r);
     }
-    // one step of every resident body, launched before any wait
+    // the next step of every resident body with none in flight
+    for (Request *r : S->active)
+        if (r->state == 1 && !r->inflight) launch_step(S, r);
+    // wait for the oldest step in flight unless some step has finished already
+    Request *oldest = nullptr;
+    bool any = false;
     for (Request *r : S->active) {
-        cudaStream_t st = (cudaStream_t)vx_get_stream(r->sim);
-        cudaEventRecord(r->e0, st);
-        if (vx_step(r->sim, 1) != VX_OK) r->state = 3;
-        cudaEventRecord(r->e1, st);
+        if (!r->inflight) continue;
+        if (cudaEventQuery(r->e1) == cudaSuccess) any = true;
+        if (!oldest || r->launch_seq < oldest->launch_seq) oldest = r;
     }
+    if (!any && oldest && cudaEventSynchronize(oldest->e1) != cudaSuccess) {
+        oldest->inflight = false;
+        oldest->state = 3;
+    }
+    // collect every finished step; launch that body's next one at once
     std::vector<Request *> keep;
     for (Request *r : S->active) {
-        if (cudaEventSynchronize(r->e1) != cudaSuccess) r->state = 3;
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, r->e0, r->e1);
-        double f[4] = {0, 0, 0, 0};
-        int64_t n = 0;
-        if (r->state == 1 && (vx_get_forces(r->sim, f) != VX_OK || vx_get_count(r->sim, &n) != VX_OK))
-            r->state = 3;
-        if (r->state == 1) {
-            S->step_ms.push_back(ms);
-            S->body_steps += 1;
-            S->particle_steps += (double)n;
-            r->forces.insert(r->forces.end(), f, f + 4);
-            r->done_steps += 1;
-            if (r->done_steps == r->steps) {
-                r->n_final = n;
-                r->state = 2;
+        if (r->inflight && r->state == 1) {
+            const cudaError_t q = cudaEventQuery(r->e1);
+            if (q == cudaSuccess) {
+                collect_step(S, r);
+                if (r->state == 1) launch_step(S, r);
+            } else if (q != cudaErrorNotReady) {
+                r->inflight = false;
+                r->state = 3;
             }
         }
         if (r->state == 1) {
             keep.push_back(r);
         } else {
+            if (r->inflight) cudaEventSynchronize(r->e1);   // nothing of it may run on after release
             r->t_finish = now_s();
             if (r->state == 2) S->ttc_s.push_back(r->t_finish - r->t_submit);
             release(S, r);

@@ -147,16 +147,16 @@ def run_serve(requests: int = 32, rate: float = 50.0, budget_gb: float = 160.0, 
     ids = [None] * requests
     t0 = time.perf_counter()
     nxt = 0
-    finished = 0
-    while finished < requests:
+    while True:
         now = time.perf_counter() - t0
         while nxt < requests and arrive[nxt] <= now:
             conf, pan, x, y, g = bodies[nxt]
             ids[nxt] = srv.submit(conf, pan, x, y, g, int(nsteps[nxt]))
             nxt += 1
         resident, queued = srv.tick()
-        finished = sum(1 for i in ids if i is not None and srv.result(i)["state"] in ("done", "failed"))
-        if resident == 0 and queued == 0 and nxt < requests:
+        if resident == 0 and queued == 0:
+            if nxt == requests:
+                break            # every request submitted has finished or failed
             time.sleep(max(0.0, arrive[nxt] - (time.perf_counter() - t0)))
     wall = time.perf_counter() - t0
     st = srv.stats()
