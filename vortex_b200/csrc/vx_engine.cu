@@ -205,32 +205,45 @@ __global__ void k_fill_tail(double *x, double *y, double *g, long long from, lon
 
 // Device allocation of `count` elements, counted (rounded to the 256-byte
 // allocation granularity) into *bytes; with allocs == nullptr only counted.
+// With a stream the allocation is stream-ordered (cudaMallocAsync): growing
+// one body's store then never waits for the other bodies' streams, as a
+// cudaFree would.
 template <typename T>
-static vx_status dalloc(std::vector<void *> *allocs, long long *bytes, T **p, long long count) {
+static vx_status dalloc(std::vector<void *> *allocs, long long *bytes, T **p, long long count,
+                        cudaStream_t stream) {
     void *q = nullptr;
     if (count < 1) count = 1;
     *bytes += ((long long)sizeof(T) * count + 255) / 256 * 256;
     if (!allocs) { *p = nullptr; return VX_OK; }
-    CU(cudaMalloc(&q, sizeof(T) * (size_t)count));
+    if (stream)
+        CU(cudaMallocAsync(&q, sizeof(T) * (size_t)count, stream));
+    else
+        CU(cudaMalloc(&q, sizeof(T) * (size_t)count));
     allocs->push_back(q);
     *p = (T *)q;
     return VX_OK;
 }
 
-void vx_work_free(VxWork &w, std::vector<void *> &allocs) {
-    for (void *q : allocs) cudaFree(q);
+void vx_work_free(VxWork &w, std::vector<void *> &allocs, cudaStream_t stream) {
+    for (void *q : allocs) {
+        if (stream)
+            cudaFreeAsync(q, stream);
+        else
+            cudaFree(q);
+    }
     allocs.clear();
     memset(&w, 0, sizeof(w));
 }
 
 // Scratch for a particle capacity `cap` and a panel count padded to P32
 // (allocs == nullptr: only count the bytes into w.bytes).
-static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long long cap, int P32, int num_sms) {
+static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long long cap, int P32, int num_sms,
+                                 cudaStream_t stream) {
     w.cap = cap;
     w.bytes = 0;
     const long long nch = cap / VX_CHUNK + 2;
     vx_status st;
-#define A(ptr, n) if ((st = dalloc(allocs, &w.bytes, &(ptr), (n))) != VX_OK) return st
+#define A(ptr, n) if ((st = dalloc(allocs, &w.bytes, &(ptr), (n), stream)) != VX_OK) return st
     A(w.cmp_cnt, nch); A(w.cmp_off, nch);
     A(w.hole_pos, cap); A(w.hole_src, cap); A(w.tail_src, cap);
     A(w.hx, cap); A(w.hy, cap); A(w.hg, cap); A(w.tx, cap); A(w.ty, cap);
@@ -269,22 +282,23 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     return VX_OK;
 }
 
-vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms) {
-    vx_work_free(w, allocs);
-    return work_alloc_impl(w, &allocs, cap, P32, num_sms);
+vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
+                        cudaStream_t stream) {
+    vx_work_free(w, allocs, stream);
+    return work_alloc_impl(w, &allocs, cap, P32, num_sms, stream);
 }
 
 long long vx_work_bytes(long long cap, int P32, int num_sms) {
     VxWork w;
     memset(&w, 0, sizeof(w));
-    work_alloc_impl(w, nullptr, cap, P32, num_sms);
+    work_alloc_impl(w, nullptr, cap, P32, num_sms, nullptr);
     return w.bytes;
 }
 
-static void free_work(vx_sim *s) { vx_work_free(s->w, s->work_allocs); }
+static void free_work(vx_sim *s) { vx_work_free(s->w, s->work_allocs, s->stream); }
 
 static vx_status alloc_work(vx_sim *s, long long cap) {
-    return vx_work_alloc(s->w, s->work_allocs, cap, s->P32, s->num_sms);
+    return vx_work_alloc(s->w, s->work_allocs, cap, s->P32, s->num_sms, s->stream);
 }
 
 static void drop_graph(vx_sim *s) {
@@ -303,7 +317,7 @@ static vx_status grow(vx_sim *s, long long need) {
     double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};
     double *nar[6];
     for (int k = 0; k < 6; ++k) {
-        CU(cudaMalloc(&nar[k], sizeof(double) * ncap));
+        CU(cudaMallocAsync(&nar[k], sizeof(double) * ncap, s->stream));   // stream-ordered: see dalloc
         if (s->cap > 0)
             CU(cudaMemcpyAsync(nar[k], arr[k], sizeof(double) * s->cap, cudaMemcpyDeviceToDevice, s->stream));
         else
@@ -312,8 +326,8 @@ static vx_status grow(vx_sim *s, long long need) {
     k_fill_tail<<<s->num_sms * 4, 256, 0, s->stream>>>(nar[0], nar[1], nar[2], s->cap, ncap);
     ++s->launches;
     CU(cudaGetLastError());
-    CU(cudaStreamSynchronize(s->stream));
-    for (int k = 0; k < 6; ++k) cudaFree(arr[k]);
+    for (int k = 0; k < 6; ++k)
+        if (arr[k]) CU(cudaFreeAsync(arr[k], s->stream));
     s->x = nar[0]; s->y = nar[1]; s->g = nar[2]; s->vx = nar[3]; s->vy = nar[4]; s->d = nar[5];
     s->cap = ncap;
     drop_graph(s);
@@ -549,9 +563,10 @@ extern "C" vx_status vx_destroy(vx_sim *s) {
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     drop_graph(s);
-    free_work(s);
+    free_work(s);   // stream-ordered, as allocated
     double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};
-    for (double *a : arr) if (a) cudaFree(a);
+    for (double *a : arr) if (a) cudaFreeAsync(a, s->stream);
+    if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->d_pan) cudaFree(s->d_pan);
     if (s->d_minv) cudaFree(s->d_minv);
     if (s->d_minvT) cudaFree(s->d_minvT);

@@ -315,7 +315,8 @@ cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const V
 void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams *p);
 void vx_set_error(const char *fmt, ...);
 #include <vector>
-vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms);
+vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
+                        cudaStream_t stream = nullptr);
 long long vx_work_bytes(long long cap, int P32, int num_sms);
 // Stable order by bucket from bucket counts (used up, then restored) and
 // starts: (okey, oval) = keys and element indices in bucket order, elements
@@ -333,7 +334,7 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
                                    VxWork &w);
 cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                       VxWork &w);
-void vx_work_free(VxWork &w, std::vector<void *> &allocs);
+void vx_work_free(VxWork &w, std::vector<void *> &allocs, cudaStream_t stream = nullptr);
 
 // Split factor so that (target tiles x source chunks) fills the GPU.
 int vx_pick_ksplit(long long n_upper, int tile, int num_sms);
