@@ -74,6 +74,27 @@ def test_result_same_alone_and_in_mix():
     assert st["mean_resident"] > 1.0        # the bodies did overlap
 
 
+def test_small_body_is_not_held_back_by_a_large_one():
+    """Each body is relaunched as soon as its own step is collected: a small
+    body finishes its steps while a large one submitted with it, asking for
+    as many steps, is still running."""
+    big = small_body(0, n0=300000, panels=400)
+    small = small_body(1, n0=1000, panels=100)
+    srv = N.Server(int(16e9), max_active=4)
+    ib = srv.submit(*big, 12)
+    isml = srv.submit(*small, 12)
+    seen = False
+    for _ in range(500):
+        res, q = srv.tick()
+        if srv.result(isml)["state"] == "done" and srv.result(ib)["state"] == "resident":
+            seen = True
+        if res == 0 and q == 0:
+            break
+    assert srv.result(ib)["state"] == srv.result(isml)["state"] == "done"
+    assert seen
+    srv.close()
+
+
 def test_admission_by_slots_and_budget():
     body = small_body(0)
     c, p = body[0], body[1]

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -46,7 +47,6 @@ struct Request {
     vx_sim *sim = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     bool inflight = false;    // a step launched and not yet collected
-    int64_t launch_seq = 0;   // order of that launch (the oldest is waited for)
     int64_t done_steps = 0;
     std::vector<double> forces;   // 4 per step: dg, Fx, Fy, M
     int64_t n_final = 0;
@@ -74,7 +74,7 @@ struct vx_server {
     std::vector<double> step_ms;      // device time of every body step
     std::vector<double> ttc_s;        // submit -> finish of every finished request
     double active_sum = 0.0;
-    int64_t ticks = 0, body_steps = 0, launch_seq = 0;
+    int64_t ticks = 0, body_steps = 0;
     double particle_steps = 0.0;      // sum over body steps of the particle count
 };
 
@@ -88,7 +88,6 @@ static void launch_step(vx_server *S, Request *r) {
     }
     cudaEventRecord(r->e1, st);
     r->inflight = true;
-    r->launch_seq = ++S->launch_seq;
 }
 
 // Collect r's finished step: its device time, forces and count.
@@ -206,17 +205,17 @@ extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queu
     // the next step of every resident body with none in flight
     for (Request *r : S->active)
         if (r->state == 1 && !r->inflight) launch_step(S, r);
-    // wait for the oldest step in flight unless some step has finished already
-    Request *oldest = nullptr;
-    bool any = false;
-    for (Request *r : S->active) {
-        if (!r->inflight) continue;
-        if (cudaEventQuery(r->e1) == cudaSuccess) any = true;
-        if (!oldest || r->launch_seq < oldest->launch_seq) oldest = r;
-    }
-    if (!any && oldest && cudaEventSynchronize(oldest->e1) != cudaSuccess) {
-        oldest->inflight = false;
-        oldest->state = 3;
+    // wait until some step in flight has finished (whichever comes first:
+    // a small body's step is not held back by a large one's)
+    for (;;) {
+        bool pending = false, any = false;
+        for (Request *r : S->active) {
+            if (!r->inflight) continue;
+            pending = true;
+            if (cudaEventQuery(r->e1) != cudaErrorNotReady) any = true;
+        }
+        if (any || !pending) break;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
     // collect every finished step; launch that body's next one at once
     std::vector<Request *> keep;
