@@ -78,7 +78,7 @@ def test_small_body_is_not_held_back_by_a_large_one():
     """Each body is relaunched as soon as its own step is collected: a small
     body finishes its steps while a large one submitted with it, asking for
     as many steps, is still running."""
-    big = small_body(0, n0=300000, panels=400)
+    big = small_body(0, n0=600000, panels=400)
     small = small_body(1, n0=1000, panels=100)
     srv = N.Server(int(16e9), max_active=4)
     ib = srv.submit(*big, 12)

@@ -4,7 +4,9 @@
 // steps).  Requests wait in arrival order until a slot is free and the
 // device-byte budget holds their estimate (vx_estimate_bytes at the largest
 // particle count the run can reach: start + P per step); then the body is
-// created and stays resident until its last step.  Each body has at most one
+// created (on worker threads: building a body's panel system takes tens of
+// milliseconds, during which the loop keeps relaunching the resident bodies)
+// and stays resident until its last step.  Each body has at most one
 // step in flight on its own stream; a tick launches the next step of every
 // resident body that has none in flight, waits until at least one step has
 // finished, collects every finished step (forces, count) and launches that
@@ -19,7 +21,9 @@
 #include <cmath>
 #include <cstring>
 #include <deque>
+#include <condition_variable>
 #include <map>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -47,6 +51,7 @@ struct Request {
     vx_sim *sim = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     bool inflight = false;    // a step launched and not yet collected
+    vx_status create_st = VX_OK;   // set by the worker thread
     int64_t done_steps = 0;
     std::vector<double> forces;   // 4 per step: dg, Fx, Fy, M
     int64_t n_final = 0;
@@ -70,6 +75,15 @@ struct vx_server {
     int64_t next_id = 1;
     std::deque<Request *> queue;
     std::vector<Request *> active;
+    // body creation on worker threads: admitted requests go to to_create,
+    // come back in created; `creating` (loop thread only) counts those away
+    std::vector<std::thread> workers;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Request *> to_create;
+    std::vector<Request *> created;
+    bool stop = false;
+    int creating = 0;
     std::map<int64_t, Request *> all;
     std::vector<double> step_ms;      // device time of every body step
     std::vector<double> ttc_s;        // submit -> finish of every finished request
@@ -132,9 +146,50 @@ extern "C" vx_status vx_server_create(int device, int64_t budget_bytes, int max_
     return VX_OK;
 }
 
+constexpr int CREATE_THREADS = 4;
+
+// Worker thread: create admitted bodies, taken in admission order.
+static void create_loop(vx_server *S) {
+    cudaSetDevice(S->device);
+    for (;;) {
+        Request *r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv.wait(lk, [S] { return S->stop || !S->to_create.empty(); });
+            if (S->to_create.empty()) return;   // stop, nothing left
+            r = S->to_create.front();
+            S->to_create.pop_front();
+        }
+        vx_status st = vx_create(&r->conf, r->pan.data(), (int64_t)r->pan.size(), S->device, &r->sim);
+        if (st == VX_OK && !r->x.empty())
+            st = vx_set_particles(r->sim, r->x.data(), r->y.data(), r->g.data(), (int64_t)r->x.size());
+        if (st == VX_OK && (cudaEventCreate(&r->e0) != cudaSuccess || cudaEventCreate(&r->e1) != cudaSuccess))
+            st = VX_ERR_CUDA;
+        if (st == VX_OK && r->sim && vx_sync(r->sim) != VX_OK) st = VX_ERR_CUDA;
+        r->create_st = st;
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->created.push_back(r);
+    }
+}
+
+static void stop_worker(vx_server *S) {
+    if (S->workers.empty()) return;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        for (Request *r : S->to_create) r->create_st = VX_ERR_ARG;   // never created
+        for (Request *r : S->to_create) S->created.push_back(r);
+        S->to_create.clear();
+    }
+    S->cv.notify_all();
+    for (auto &t : S->workers) t.join();
+    S->workers.clear();
+}
+
 extern "C" vx_status vx_server_destroy(vx_server *S) {
     if (!S) return VX_OK;
     cudaSetDevice(S->device);
+    stop_worker(S);
     for (auto &kv : S->all) {
         if (kv.second->state == 1) release(S, kv.second);
         delete kv.second;
@@ -173,42 +228,62 @@ extern "C" vx_status vx_server_submit(vx_server *S, const vx_conf *conf, const v
     return VX_OK;
 }
 
-// Admit what fits, launch and collect steps as above, retire the
-// finished ones.  *active: bodies resident after the tick; *queued: waiting.
-extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queued) {
-    if (!S) return VX_ERR_ARG;
-    if (cudaSetDevice(S->device) != cudaSuccess) return VX_ERR_CUDA;
-    // admission in arrival order
-    while (!S->queue.empty() && (int)S->active.size() < S->max_active &&
-           S->used + S->queue.front()->est_bytes <= S->budget) {
-        Request *r = S->queue.front();
-        S->queue.pop_front();
-        vx_status st = vx_create(&r->conf, r->pan.data(), (int64_t)r->pan.size(), S->device, &r->sim);
-        if (st == VX_OK && !r->x.empty())
-            st = vx_set_particles(r->sim, r->x.data(), r->y.data(), r->g.data(), (int64_t)r->x.size());
-        if (st == VX_OK && (cudaEventCreate(&r->e0) != cudaSuccess || cudaEventCreate(&r->e1) != cudaSuccess))
-            st = VX_ERR_CUDA;
-        S->used += r->est_bytes;
-        if (st != VX_OK) {
+// Bodies the worker has finished creating join the resident set (or fail).
+static void take_created(vx_server *S) {
+    std::vector<Request *> got;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        got.swap(S->created);
+    }
+    for (Request *r : got) {
+        --S->creating;
+        if (r->create_st != VX_OK) {
             release(S, r);
             r->state = 3;
+            r->t_finish = now_s();
             continue;
         }
         std::vector<double>().swap(r->x);
         std::vector<double>().swap(r->y);
         std::vector<double>().swap(r->g);
         r->forces.reserve((size_t)(4 * r->steps));
-        r->state = 1;
         r->t_admit = now_s();
         S->active.push_back(r);
     }
+}
+
+// Admit what fits, launch and collect steps as above, retire the
+// finished ones.  *active: bodies resident after the tick; *queued: waiting.
+extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queued) {
+    if (!S) return VX_ERR_ARG;
+    if (cudaSetDevice(S->device) != cudaSuccess) return VX_ERR_CUDA;
+    // admission in arrival order (slots and budget are held from here on)
+    while (!S->queue.empty() && (int)S->active.size() + S->creating < S->max_active &&
+           S->used + S->queue.front()->est_bytes <= S->budget) {
+        Request *r = S->queue.front();
+        S->queue.pop_front();
+        S->used += r->est_bytes;
+        r->state = 1;
+        ++S->creating;
+        if ((int)S->workers.size() < std::min(CREATE_THREADS, S->creating)) S->workers.emplace_back(create_loop, S);
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->to_create.push_back(r);
+        }
+        S->cv.notify_one();
+    }
+    take_created(S);
     // the next step of every resident body with none in flight
     for (Request *r : S->active)
         if (r->state == 1 && !r->inflight) launch_step(S, r);
     // wait until some step in flight has finished (whichever comes first:
     // a small body's step is not held back by a large one's)
     for (;;) {
-        bool pending = false, any = false;
+        bool pending = S->creating > 0, any = false;
+        if (pending) {
+            std::lock_guard<std::mutex> lk(S->mu);
+            any = !S->created.empty();
+        }
         for (Request *r : S->active) {
             if (!r->inflight) continue;
             pending = true;
@@ -240,9 +315,12 @@ extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queu
         }
     }
     S->active.swap(keep);
+    take_created(S);
+    for (Request *r : S->active)
+        if (r->state == 1 && !r->inflight) launch_step(S, r);
     S->ticks += 1;
     S->active_sum += (double)S->active.size();
-    if (active) *active = (int64_t)S->active.size();
+    if (active) *active = (int64_t)S->active.size() + S->creating;
     if (queued) *queued = (int64_t)S->queue.size();
     return VX_OK;
 }
