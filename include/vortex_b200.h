@@ -220,7 +220,8 @@ vx_status vx_step_many(vx_sim *const *sims, int count, int64_t nsteps);
  * process): a request loop with continuous batching.  Requests (one body
  * each: conf, panels, starting vortices, step count) wait in arrival order
  * until a slot is free and the device-byte budget holds their
- * vx_estimate_bytes at n + P * nsteps; admitted bodies stay resident, each
+ * vx_estimate_bytes at n + P * nsteps; admitted bodies are created on worker
+ * threads (state 1 from admission on) and stay resident, each
  * with at most one step in flight on its own stream; a tick launches the
  * next step of every resident body with none in flight, waits until at
  * least one step has finished, collects every finished step and launches
