@@ -95,6 +95,30 @@ def test_small_body_is_not_held_back_by_a_large_one():
     srv.close()
 
 
+def test_failed_creation_is_reported_and_the_rest_run():
+    """A body whose panel system the reference's pivot rule cannot invert
+    (thin rounded plate, gj_pivot 0) fails at creation on the worker thread:
+    its request reports "failed", frees its slot and budget, and the request
+    submitted with it runs to the end."""
+    from tests.helpers import conf_kwargs
+    from vortex_b200 import profiles as PR
+    pan = PR.rotate(PR.rounded_plate(655), -30.0)
+    ck = conf_kwargs(len(pan), ve_size=float(pan["length"].mean()))
+    bad = N.default_conf(**dict(ck, gj_pivot=0))
+    x, y, g = np.linspace(1.0, 2.0, 10), np.zeros(10), np.full(10, 1e-3)
+    srv = N.Server(int(8e9), max_active=4)
+    ib = srv.submit(bad, pan, x, y, g, 3)
+    ig = srv.submit(*small_body(0), 4)
+    for _ in range(200):
+        res, q = srv.tick()
+        if res == 0 and q == 0:
+            break
+    assert srv.result(ib)["state"] == "failed"
+    assert srv.result(ig)["state"] == "done" and srv.result(ig)["steps"] == 4
+    assert srv.stats()["bytes_reserved"] == 0
+    srv.close()
+
+
 def test_admission_by_slots_and_budget():
     body = small_body(0)
     c, p = body[0], body[1]
