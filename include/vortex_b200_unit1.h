@@ -138,19 +138,22 @@ int64_t vxu_launch_count(void);
 #define VXU_NOALLOC_MAX_POINTS 4096
 
 /* velocity_control without any device allocation.  No counterpart in the
- * reference: it is for host programs that cannot call cudaMalloc on their
- * step path (device memory already held by another runtime's caching
- * allocator, a fixed memory budget, or a loop that cannot take the device
- * synchronisation an allocation may bring).  Its scratch is a fixed 4 MiB
- * array inside this library, held on every GPU that loads it until exit;
- * the caller passes the inputs and outputs as for velocity_control.
+ * reference: it is for host programs that cannot call cudaMalloc where they
+ * sample the flow (device memory already held by another runtime's caching
+ * allocator, or a device-memory budget fixed at start-up).  Its scratch is a
+ * fixed 4 MiB array inside this library, held on every GPU that loads it
+ * until exit; the caller passes the inputs and outputs as for
+ * velocity_control.
  *   - at most VXU_NOALLOC_MAX_POINTS control points, else returns 2 and
  *     launches nothing;
  *   - plain FP64 form (results identical to velocity_control's when
- *     VORTEX_B200_PRECISION is unset); core radius from conf.ve_size;
+ *     VORTEX_B200_PRECISION is unset); the core radius is velocity_control's:
+ *     the one fixed by init_device_conf_values, or conf.ve_size before it;
+ *   - each call launches on the legacy default stream and synchronises the
+ *     device, like the reference's entry points: do not call it while any
+ *     stream on the device is being captured;
  *   - the first call on a device, with that device current, looks up the
- *     array's device address; make that first call before any stream
- *     capture on the device;
+ *     array's device address;
  *   - all calls on one device share the array; calls that overlap on the
  *     same GPU race and must be serialised by the caller. */
 int velocity_control_noalloc(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *Contr_points,

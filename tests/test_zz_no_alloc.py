@@ -9,6 +9,9 @@ the one the unit_1 tests use for FP64 against FP64: 1e-12 relative.
 import ctypes as C
 import math
 import os
+import subprocess
+import sys
+import textwrap
 
 import numpy as np
 import pytest
@@ -74,3 +77,55 @@ def test_noalloc_matches_velocity_control_on_consecutive_calls():
     finally:
         if saved is not None:
             os.environ["VORTEX_B200_PRECISION"] = saved
+
+
+# Run in a fresh process with every module of the library loaded when the
+# context is created (CUDA_MODULE_LOADING=EAGER), so that the 4 MiB array is
+# already resident and lazy module loading cannot be mistaken for an
+# allocation.  The first call on the device and a second one must leave the
+# device's free memory exactly as it was.
+_FRESH = textwrap.dedent("""
+    import ctypes as C, sys
+    import numpy as np
+    sys.path.insert(0, {root!r})
+    from tests.test_zz_no_alloc import _setup, _bind
+    from tests.test_unit1_gpu import Dev, rt
+    from vortex_b200 import native as N
+    L = N.lib()
+    assert rt().cudaFree(C.c_void_p(0)) == 0
+    _setup(L)
+    _bind(L)
+    rng = np.random.default_rng(3)
+    n, npts = 30000, 4096
+    pos = np.zeros((n, 3))
+    pos[:, 0] = rng.uniform(0.55, 3.0, n)
+    pos[:, 1] = rng.uniform(-1.0, 1.0, n)
+    pos[:, 2] = rng.normal(0.0, 1e-3, n)
+    cp = np.zeros((npts, 3))
+    cp[:, 0] = rng.uniform(0.0, 3.5, npts)
+    cp[:, 1] = rng.uniform(-1.2, 1.2, npts)
+    d_pos, d_cp, d_vinf, d_out = Dev(pos.nbytes), Dev(cp.nbytes), Dev(16), Dev(npts * 16)
+    d_pos.put(pos); d_cp.put(cp); d_vinf.put(np.array([1.0, 0.0]))
+    free, total = C.c_size_t(), C.c_size_t()
+    def free_bytes():
+        assert rt().cudaDeviceSynchronize() == 0
+        assert rt().cudaMemGetInfo(C.byref(free), C.byref(total)) == 0
+        return free.value
+    f0 = free_bytes()
+    assert L.velocity_control_noalloc(d_pos.p, d_vinf.p, n, d_cp.p, d_out.p, npts) == 0   # first call
+    f1 = free_bytes()
+    assert L.velocity_control_noalloc(d_pos.p, d_vinf.p, n, d_cp.p, d_out.p, npts) == 0
+    f2 = free_bytes()
+    print("free bytes", f0, f1, f2)
+    assert f0 == f1 == f2, (f0, f1, f2)
+    assert np.isfinite(d_out.get((npts, 2))).all()
+""")
+
+
+def test_noalloc_allocates_nothing_from_the_first_call():
+    root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+    env.pop("VORTEX_B200_PRECISION", None)
+    r = subprocess.run([sys.executable, "-c", _FRESH.format(root=root)], env=env, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]

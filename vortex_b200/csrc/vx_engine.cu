@@ -315,13 +315,20 @@ static vx_status grow(vx_sim *s, long long need) {
     ncap = std::max(ncap, (long long)(s->cap * 1.25));
     ncap = vx_ceil_div(ncap, 8192) * 8192;
     double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};
-    double *nar[6];
+    double *nar[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     for (int k = 0; k < 6; ++k) {
-        CU(cudaMallocAsync(&nar[k], sizeof(double) * ncap, s->stream));   // stream-ordered: see dalloc
-        if (s->cap > 0)
-            CU(cudaMemcpyAsync(nar[k], arr[k], sizeof(double) * s->cap, cudaMemcpyDeviceToDevice, s->stream));
-        else
-            CU(cudaMemsetAsync(nar[k], 0, sizeof(double) * ncap, s->stream));
+        cudaError_t e = cudaMallocAsync(&nar[k], sizeof(double) * ncap, s->stream);   // stream-ordered: see dalloc
+        if (e == cudaSuccess)
+            e = s->cap > 0 ? cudaMemcpyAsync(nar[k], arr[k], sizeof(double) * s->cap, cudaMemcpyDeviceToDevice,
+                                             s->stream)
+                           : cudaMemsetAsync(nar[k], 0, sizeof(double) * ncap, s->stream);
+        if (e != cudaSuccess) {
+            // the store stays as it was: release the new arrays made so far
+            for (int q = 0; q <= k; ++q)
+                if (nar[q]) cudaFreeAsync(nar[q], s->stream);
+            vx_set_error("growing the particle store to %lld slots: %s", ncap, cudaGetErrorString(e));
+            return e == cudaErrorMemoryAllocation ? VX_ERR_NOMEM : VX_ERR_CUDA;
+        }
     }
     k_fill_tail<<<s->num_sms * 4, 256, 0, s->stream>>>(nar[0], nar[1], nar[2], s->cap, ncap);
     ++s->launches;

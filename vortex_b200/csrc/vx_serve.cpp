@@ -24,6 +24,7 @@
 #include <condition_variable>
 #include <map>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -52,6 +53,7 @@ struct Request {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     bool inflight = false;    // a step launched and not yet collected
     vx_status create_st = VX_OK;   // set by the worker thread
+    std::string create_err;        // the worker's error text when create_st != VX_OK
     int64_t done_steps = 0;
     std::vector<double> forces;   // 4 per step: dg, Fx, Fy, M
     int64_t n_final = 0;
@@ -167,6 +169,8 @@ static void create_loop(vx_server *S) {
             st = VX_ERR_CUDA;
         if (st == VX_OK && r->sim && vx_sync(r->sim) != VX_OK) st = VX_ERR_CUDA;
         r->create_st = st;
+        // the error text is thread-local: keep the worker's for the loop thread
+        if (st != VX_OK) r->create_err = vx_last_error();
         std::lock_guard<std::mutex> lk(S->mu);
         S->created.push_back(r);
     }
@@ -238,6 +242,9 @@ static void take_created(vx_server *S) {
     for (Request *r : got) {
         --S->creating;
         if (r->create_st != VX_OK) {
+            // the caller of the tick reads the reason through vx_last_error
+            vx_set_error("request %lld: body creation failed: %s", (long long)r->id,
+                         r->create_err.empty() ? vx_status_str(r->create_st) : r->create_err.c_str());
             release(S, r);
             r->state = 3;
             r->t_finish = now_s();

@@ -471,15 +471,15 @@ int64_t vxu_launch_count(void) { return U.launches; }
 
 // ---------------------------------------------------------------------------
 // velocity_control_noalloc: velocity_control for callers that must not
-// allocate device memory.  Some host programs cannot call cudaMalloc on the
-// step path: a process whose device memory is already held by another
-// runtime's caching allocator (cudaMalloc would fail or evict), a loop with a
-// fixed memory budget fixed at start-up, or a real-time loop that cannot take
-// the device-wide synchronisation cudaMalloc and cudaFree may imply.  This
-// entry point computes the same velocities with its scratch (the per-split
-// partial sums of the Biot-Savart kernel and the device scalars) in the
-// fixed file-scope array below, which every GPU that loads this library
-// holds until the process exits.
+// allocate device memory.  Some host programs cannot call cudaMalloc where
+// they sample the flow: a process whose device memory is already held by
+// another runtime's caching allocator (a cudaMalloc there fails, or forces
+// that allocator to release its cache), or a program that reserves a fixed
+// device-memory budget at start-up and may not grow past it.  This entry
+// point computes the same velocities with its scratch (the per-split partial
+// sums of the Biot-Savart kernel and the device scalars) in the fixed
+// file-scope array below, which every GPU that loads this library holds
+// until the process exits.
 //
 // Limits and behaviour:
 //   * at most VXU_NOALLOC_MAX_POINTS control points per call; more are
@@ -487,10 +487,14 @@ int64_t vxu_launch_count(void) { return U.launches; }
 //   * the plain FP64 form always (the FP32 form needs source scratch that
 //     grows with the vortex count); with VORTEX_B200_PRECISION unset its
 //     results are bit-identical to velocity_control's;
-//   * the core radius is read from conf.ve_size at each call;
+//   * the core radius is the one velocity_control uses: the value fixed when
+//     init_device_conf_values (or the first entry point) ran, or, before
+//     that, conf.ve_size at the call;
+//   * each call launches on the legacy default stream and ends with a
+//     device-wide synchronisation, like the reference's entry points: it
+//     must not run while any stream on the device is being captured;
 //   * the first call on a device, with that device current, looks up the
-//     array's device address (cudaGetSymbolAddress) and the SM count; make
-//     that first call before any stream capture on the device;
+//     array's device address (cudaGetSymbolAddress) and the SM count;
 //   * every call on a device shares the one array and finds there what the
 //     previous call left: the scalars are cleared at the start of each call
 //     and the partial sums are fully rewritten before they are read.  Calls
@@ -555,8 +559,8 @@ extern "C" int velocity_control_noalloc(vxu_vortex *pos, double (*V_inf)[2], siz
     VxParams prm;
     memset(&prm, 0, sizeof(prm));
     prm.prec = VX_PREC_FP64;
-    prm.eps = conf.ve_size;
-    prm.eps2 = conf.ve_size * conf.ve_size;
+    prm.eps = U.ready ? U.prm.eps : conf.ve_size;
+    prm.eps2 = U.ready ? U.prm.eps2 : conf.ve_size * conf.ve_size;
     VxWork w;
     memset(&w, 0, sizeof(w));
     w.part = d->base + NA_HEAD;
