@@ -111,10 +111,9 @@ __device__ __forceinline__ double vx_block_sum(double v, double *sh) {
     return r;
 }
 
-__global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, const VxScalars *S,
-                                                       const vx_panel *pan, double *red, const int *hstart,
-                                                       const int *hidx) {
-    VX_PDL_WAIT();
+VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, const VxScalars *S,
+                           const vx_panel *pan, double *red, const int *hstart,
+                           const int *hidx) {
     __shared__ double sh[VX_THREADS];
     const long long n = S->n;
     const long long n_new0 = S->n0;   // vortices born this step: [n0, n)
@@ -122,8 +121,8 @@ __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, con
     double sdg = 0.0, sfx = 0.0, sfy = 0.0, sm = 0.0;
     // whole warps step together (lane i of the warp takes particle base + i),
     // so a long segment can be handed to the warp
-    for (long long base = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
-         base += (long long)gridDim.x * blockDim.x) {
+    for (long long base = vb.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+         base += (long long)vb.n * blockDim.x) {
         const long long i = base + lane;
         const bool valid = i < n;
         const long long k = i * v.ps;
@@ -186,16 +185,21 @@ __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, con
         sfx += fx; sfy += fy; sm += m;
     }
     double t;
-    t = vx_block_sum(sdg, sh); if (threadIdx.x == 0) red[blockIdx.x * 4 + 0] = t;
-    t = vx_block_sum(sfx, sh); if (threadIdx.x == 0) red[blockIdx.x * 4 + 1] = t;
-    t = vx_block_sum(sfy, sh); if (threadIdx.x == 0) red[blockIdx.x * 4 + 2] = t;
-    t = vx_block_sum(sm, sh);  if (threadIdx.x == 0) red[blockIdx.x * 4 + 3] = t;
+    t = vx_block_sum(sdg, sh); if (threadIdx.x == 0) red[vb.x * 4 + 0] = t;
+    t = vx_block_sum(sfx, sh); if (threadIdx.x == 0) red[vb.x * 4 + 1] = t;
+    t = vx_block_sum(sfy, sh); if (threadIdx.x == 0) red[vb.x * 4 + 2] = t;
+    t = vx_block_sum(sm, sh);  if (threadIdx.x == 0) red[vb.x * 4 + 3] = t;
+}
+__global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, const VxScalars *S,
+                                                       const vx_panel *pan, double *red, const int *hstart,
+                                                       const int *hidx) {
+    VX_PDL_WAIT();
+    k_advect_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, red, hstart, hidx);
 }
 
 // Block sums combined by one block: thread t adds blocks t, t + 256, ... in
 // order, then a fixed shared-memory tree; the result is run-to-run identical.
-__global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, const double *red, int nblocks) {
-    VX_PDL_WAIT();
+VX_DEVK void k_sums_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxScalars *S, const double *red, int nblocks) {
     __shared__ double sh[VX_THREADS];
     double a[4] = {0.0, 0.0, 0.0, 0.0};
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
@@ -208,11 +212,15 @@ __global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, c
     S->fy = a[2] * (p.rho / p.dt);
     S->m = a[3] * (p.rho / (2 * p.dt));
 }
+__global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, const double *red, int nblocks) {
+    VX_PDL_WAIT();
+    k_sums_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, p, S, red, nblocks);
+}
 
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                              VxWork &w, const vx_panel *pan, const int *hstart, const int *hidx) {
     if (p.hit_nx <= 0 || p.hit_ny <= 0) hstart = hidx = nullptr;
-    vx_launch_pdl(k_advect, VX_RED_BLOCKS, VX_THREADS, 0, L.stream, p, v, S, pan, w.red, hstart, hidx); VX_COUNT(L);
-    vx_launch_pdl(k_sums, 1, VX_THREADS, 0, L.stream, p, S, w.red, VX_RED_BLOCKS); VX_COUNT(L);
+    vx_launch<k_advect, k_advect_body>(L, VX_RED_BLOCKS, VX_THREADS, 0, p, v, S, pan, w.red, hstart, hidx);
+    vx_launch<k_sums, k_sums_body>(L, 1, VX_THREADS, 0, p, S, w.red, VX_RED_BLOCKS);
     return cudaGetLastError();
 }

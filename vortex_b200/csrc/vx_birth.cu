@@ -15,11 +15,10 @@ __device__ __forceinline__ double vx_sp(const double a[2], const double b[2]) {
     return a[0] * b[0] + a[1] * b[1];
 }
 
-__global__ void k_panel_influence(const vx_panel *pan, int P, double *L) {
-    VX_PDL_WAIT();
+VX_DEVK void k_panel_influence_body(VxBlkB<0, 0> vb, const vx_panel *pan, int P, double *L) {
     const long long S = P + 1;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * S;
-         e += (long long)gridDim.x * blockDim.x) {
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < S * S;
+         e += (long long)vb.n * blockDim.x) {
         int i = (int)(e / S), j = (int)(e % S);
         double val;
         if (i == P) {
@@ -77,12 +76,19 @@ __global__ void k_panel_influence(const vx_panel *pan, int P, double *L) {
         L[e] = val;
     }
 }
+__global__ void k_panel_influence(const vx_panel *pan, int P, double *L) {
+    VX_PDL_WAIT();
+    k_panel_influence_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, pan, P, L);
+}
 
+VX_DEVK void k_identity_body(VxBlkB<0, 0> vb, double *A, long long S) {
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < S * S;
+         e += (long long)vb.n * blockDim.x)
+        A[e] = (e / S == e % S) ? 1.0 : 0.0;
+}
 __global__ void k_identity(double *A, long long S) {
     VX_PDL_WAIT();
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * S;
-         e += (long long)gridDim.x * blockDim.x)
-        A[e] = (e / S == e % S) ? 1.0 : 0.0;
+    k_identity_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, A, S);
 }
 
 // Block-wide arg-max of |A[i][col]| over i in [lo, S): the first row that
@@ -129,8 +135,7 @@ __device__ void vx_block_swap_rows(double *A, long long S, long long r1, long lo
 // eliminated, so a well-conditioned system can still meet a pivot below
 // 1e-12 there.  robust != 0: ordinary partial pivoting instead (the pivot of
 // column k chosen among rows k.. after the previous eliminations).
-__global__ void k_gj_pivot(double *A, double *Inv, long long S, long long k, double *c, int *flag, int robust) {
-    VX_PDL_WAIT();
+VX_DEVK void k_gj_pivot_body(VxBlkB<0, 0> vb, double *A, double *Inv, long long S, long long k, double *c, int *flag, int robust) {
     __shared__ double s_val[1024];
     __shared__ long long s_idx[1024];
     if (*flag) return;
@@ -164,15 +169,18 @@ __global__ void k_gj_pivot(double *A, double *Inv, long long S, long long k, dou
     const double piv = A[k * S + k];
     for (long long i = threadIdx.x; i < S; i += blockDim.x) c[i] = A[i * S + k] / piv;
 }
+__global__ void k_gj_pivot(double *A, double *Inv, long long S, long long k, double *c, int *flag, int robust) {
+    VX_PDL_WAIT();
+    k_gj_pivot_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, A, Inv, S, k, c, flag, robust);
+}
 
 // Row operations of step k: every row but k loses c[i] times row k.
-__global__ void k_gj_elim(double *A, double *Inv, long long S, long long k, const double *c,
-                          const int *flag) {
-    VX_PDL_WAIT();
+VX_DEVK void k_gj_elim_body(VxBlkB<0, 0> vb, double *A, double *Inv, long long S, long long k, const double *c,
+                            const int *flag) {
     if (*flag) return;
     const long long W = 2 * S;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * W;
-         e += (long long)gridDim.x * blockDim.x) {
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < S * W;
+         e += (long long)vb.n * blockDim.x) {
         long long i = e / W, j = e % W;
         if (i == k) continue;
         double ci = c[i];
@@ -180,34 +188,48 @@ __global__ void k_gj_elim(double *A, double *Inv, long long S, long long k, cons
         else { j -= S; Inv[i * S + j] = Inv[i * S + j] - ci * Inv[k * S + j]; }
     }
 }
-
-__global__ void k_gj_last_pivot(const double *A, long long S, double *c, int *flag) {
+__global__ void k_gj_elim(double *A, double *Inv, long long S, long long k, const double *c,
+                          const int *flag) {
     VX_PDL_WAIT();
+    k_gj_elim_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, A, Inv, S, k, c, flag);
+}
+
+VX_DEVK void k_gj_last_pivot_body(VxBlkB<0, 0> vb, const double *A, long long S, double *c, int *flag) {
     if (*flag) return;
     const long long l = S - 1;
     if (fabs(A[l * S + l]) < 1e-12) { if (threadIdx.x == 0) *flag = 1; return; }
     for (long long i = threadIdx.x; i < l; i += blockDim.x) c[i] = A[i * S + l] / A[l * S + l];
 }
-
-__global__ void k_gj_last_elim(double *Inv, long long S, const double *c, const int *flag) {
+__global__ void k_gj_last_pivot(const double *A, long long S, double *c, int *flag) {
     VX_PDL_WAIT();
+    k_gj_last_pivot_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, A, S, c, flag);
+}
+
+VX_DEVK void k_gj_last_elim_body(VxBlkB<0, 0> vb, double *Inv, long long S, const double *c, const int *flag) {
     if (*flag) return;
     const long long l = S - 1;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < l * S;
-         e += (long long)gridDim.x * blockDim.x) {
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < l * S;
+         e += (long long)vb.n * blockDim.x) {
         long long i = e / S, j = e % S;
         Inv[i * S + j] = Inv[i * S + j] - c[i] * Inv[l * S + j];
     }
 }
-
-__global__ void k_gj_scale(const double *A, double *Inv, long long S, const int *flag) {
+__global__ void k_gj_last_elim(double *Inv, long long S, const double *c, const int *flag) {
     VX_PDL_WAIT();
+    k_gj_last_elim_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, Inv, S, c, flag);
+}
+
+VX_DEVK void k_gj_scale_body(VxBlkB<0, 0> vb, const double *A, double *Inv, long long S, const int *flag) {
     if (*flag) return;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * S;
-         e += (long long)gridDim.x * blockDim.x) {
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < S * S;
+         e += (long long)vb.n * blockDim.x) {
         long long i = e / S;
         Inv[e] = Inv[e] / A[i * S + i];
     }
+}
+__global__ void k_gj_scale(const double *A, double *Inv, long long S, const int *flag) {
+    VX_PDL_WAIT();
+    k_gj_scale_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, A, Inv, S, flag);
 }
 
 // d_work must hold 2 (P+1)^2 + (P+1) doubles.  *d_flag is set when a pivot
@@ -219,37 +241,44 @@ cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, dou
     double *c = d_work + S * S;
     const int grid = L.num_sms * 4;
     cudaMemsetAsync(d_flag, 0, sizeof(int), L.stream);
-    vx_launch_pdl(k_panel_influence, grid, 256, 0, L.stream, d_pan, P, A); VX_COUNT(L);
+    vx_launch<k_panel_influence, k_panel_influence_body>(L, grid, 256, 0, d_pan, P, A);
     if (d_L_out) cudaMemcpyAsync(d_L_out, A, sizeof(double) * S * S, cudaMemcpyDeviceToDevice, L.stream);
-    vx_launch_pdl(k_identity, grid, 256, 0, L.stream, d_minv, S); VX_COUNT(L);
+    vx_launch<k_identity, k_identity_body>(L, grid, 256, 0, d_minv, S);
     for (long long k = 0; k < S - 1; ++k) {
-        vx_launch_pdl(k_gj_pivot, 1, 1024, 0, L.stream, A, d_minv, S, k, c, d_flag, robust); VX_COUNT(L);
-        vx_launch_pdl(k_gj_elim, grid, 256, 0, L.stream, A, d_minv, S, k, c, d_flag); VX_COUNT(L);
+        vx_launch<k_gj_pivot, k_gj_pivot_body>(L, 1, 1024, 0, A, d_minv, S, k, c, d_flag, robust);
+        vx_launch<k_gj_elim, k_gj_elim_body>(L, grid, 256, 0, A, d_minv, S, k, c, d_flag);
     }
-    vx_launch_pdl(k_gj_last_pivot, 1, 1024, 0, L.stream, A, S, c, d_flag); VX_COUNT(L);
-    vx_launch_pdl(k_gj_last_elim, grid, 256, 0, L.stream, d_minv, S, c, d_flag); VX_COUNT(L);
-    vx_launch_pdl(k_gj_scale, grid, 256, 0, L.stream, A, d_minv, S, d_flag); VX_COUNT(L);
+    vx_launch<k_gj_last_pivot, k_gj_last_pivot_body>(L, 1, 1024, 0, A, S, c, d_flag);
+    vx_launch<k_gj_last_elim, k_gj_last_elim_body>(L, grid, 256, 0, d_minv, S, c, d_flag);
+    vx_launch<k_gj_scale, k_gj_scale_body>(L, grid, 256, 0, A, d_minv, S, d_flag);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // Step begin: V_inf ramp (src/main.c:654-659) and the pre-birth count.
-__global__ void k_step_begin(VxScalars *S) {
-    VX_PDL_WAIT();
+VX_DEVK void k_step_begin_body(VxBlkB<0, 0> vb, VxScalars *S) {
     if (S->step < S->incr_steps) {
         S->vinf[0] += S->dvinf[0];
         S->vinf[1] += S->dvinf[1];
     }
     S->n0 = S->n;
 }
+__global__ void k_step_begin(VxScalars *S) {
+    VX_PDL_WAIT();
+    k_step_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
+}
 
 cudaError_t vx_launch_step_begin(const VxLaunch &L, VxScalars *S) {
-    vx_launch_pdl(k_step_begin, 1, 1, 0, L.stream, S); VX_COUNT(L);
+    vx_launch<k_step_begin, k_step_begin_body>(L, 1, 1, 0, S);
     return cudaGetLastError();
 }
 
+VX_DEVK void k_step_end_body(VxBlkB<0, 0> vb, VxScalars *S) {
+S->step += 1; }
 __global__ void k_step_end(VxScalars *S) {
-    VX_PDL_WAIT(); S->step += 1; }
+    VX_PDL_WAIT();
+    k_step_end_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
+}
 
 // ---------------------------------------------------------------------------
 // Birth right-hand side (src/kernel.cu:779-847), partial sums per source
@@ -272,16 +301,15 @@ struct RhsMath<float> {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(RHS_T) k_rhs_partial(VxView v, const VxScalars *S,
-                                                       const vx_panel *pan, int P, int P32,
-                                                       double *part, int nchunks) {
-    VX_PDL_WAIT();
+VX_DEVK void k_rhs_partial_body(VxBlkB<RHS_T, 0> vb, VxView v, const VxScalars *S,
+                                const vx_panel *pan, int P, int P32,
+                                double *part, int nchunks) {
     __shared__ T sx[RHS_T], sy[RHS_T], sg[RHS_T];
     const long long n0 = S->n0;
     const long long cs = vx_ceil_div(vx_ceil_div(n0, nchunks), RHS_T) * RHS_T;
     const int tiles = (P + RHS_T - 1) / RHS_T;
     const long long items = (long long)tiles * nchunks;
-    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    for (long long it = vb.x; it < items; it += vb.n) {
         const int pt = (int)(it % tiles);
         const long long sc = it / tiles;
         const int i = pt * RHS_T + threadIdx.x;
@@ -323,6 +351,13 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_partial(VxView v, const VxScalars
             part[(sc * P32 + i) * 2 + 1] = (double)y1;
         }
     }
+}
+template <typename T>
+__global__ void __launch_bounds__(RHS_T) k_rhs_partial(VxView v, const VxScalars *S,
+                                                       const vx_panel *pan, int P, int P32,
+                                                       double *part, int nchunks) {
+    VX_PDL_WAIT();
+    k_rhs_partial_body<T>(VxBlkB<RHS_T, 0>{blockIdx.x, gridDim.x}, v, S, pan, P, P32, part, nchunks);
 }
 
 // ---------------------------------------------------------------------------
@@ -368,13 +403,12 @@ __device__ __forceinline__ bool bf_near(const VxParams &p, double x, double y) {
 // warp (at each halving a lane keeps the half of its values selected by its
 // lane bit and adds the partner's copy: lane q ends with value q, i.e.
 // coefficient q/2, part q&1) and a fixed-order sum over the block's warps.
-__global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
     __shared__ double sacc[BF_T / 32][32];
     __shared__ int snear[BF_T / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     long long j0, j1;
-    bf_chunk(S, gridDim.x, blockIdx.x, j0, j1);
+    bf_chunk(S, vb.n, vb.x, j0, j1);
     int nnear = 0;
     for (int pass = 0; pass < BF_P / 16; ++pass) {
         double acc[32];   // (re, im) of the pass's 16 coefficients
@@ -426,7 +460,7 @@ __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxS
             double sum = 0.0;
             for (int q = 0; q < BF_T / 32; ++q) sum += sacc[q][threadIdx.x];
             // value q of this pass: coefficient 16 pass + q/2, part q&1
-            part[((long long)blockIdx.x * BF_P + 16 * pass + (threadIdx.x >> 1)) * 2 + (threadIdx.x & 1)] = sum;
+            part[((long long)vb.x * BF_P + 16 * pass + (threadIdx.x >> 1)) * 2 + (threadIdx.x & 1)] = sum;
         }
         __syncthreads();
     }
@@ -436,8 +470,12 @@ __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxS
     if (threadIdx.x == 0) {
         int t = 0;
         for (int q = 0; q < BF_T / 32; ++q) t += snear[q];
-        cnt[blockIdx.x] = t;
+        cnt[vb.x] = t;
     }
+}
+__global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
+    VX_PDL_WAIT();
+    k_bf_far_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, part, cnt);
 }
 
 // Block-count offsets and the coefficient sums (block order), one block of
@@ -446,9 +484,8 @@ __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxS
 constexpr int BF_SCAN_T = 256;
 constexpr int BF_SCAN_PER = VX_BF_MAX_BLOCKS / BF_SCAN_T;
 static_assert(BF_SCAN_PER * BF_SCAN_T == VX_BF_MAX_BLOCKS, "whole blocks per scan thread");
-__global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, const int *cnt, long long *off,
-                                                       const double *part, double *coef) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bf_scan_body(VxBlkB<BF_SCAN_T, 0> vb, VxScalars *S, int nb, const int *cnt, long long *off,
+                            const double *part, double *coef) {
     __shared__ long long wsum[BF_SCAN_T / 32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     long long c[BF_SCAN_PER], tot = 0;
@@ -484,16 +521,20 @@ __global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, con
         coef[t] = acc;
     }
 }
+__global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, const int *cnt, long long *off,
+                                                       const double *part, double *coef) {
+    VX_PDL_WAIT();
+    k_bf_scan_body(VxBlkB<BF_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, nb, cnt, off, part, coef);
+}
 
 // Near sources of each block in index order (block-wide ballot scan).
-__global__ void __launch_bounds__(BF_T) k_bf_scatter(VxParams p, VxView v, const VxScalars *S,
-                                                     const long long *off, float4 *near) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bf_scatter_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S,
+                               const long long *off, float4 *near) {
     __shared__ int swarp[BF_T / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     long long j0, j1;
-    bf_chunk(S, gridDim.x, blockIdx.x, j0, j1);
-    long long base = off[blockIdx.x];
+    bf_chunk(S, vb.n, vb.x, j0, j1);
+    long long base = off[vb.x];
     for (long long jt = j0; jt < j1; jt += BF_T) {
         const long long j = jt + threadIdx.x;
         double x = 0.0, y = 0.0, g = 0.0;
@@ -515,6 +556,11 @@ __global__ void __launch_bounds__(BF_T) k_bf_scatter(VxParams p, VxView v, const
             near[base + before + __popc(bal & ((1u << lane) - 1u))] = make_float4((float)x, (float)y, (float)g, 0.f);
         base += total;
     }
+}
+__global__ void __launch_bounds__(BF_T) k_bf_scatter(VxParams p, VxView v, const VxScalars *S,
+                                                     const long long *off, float4 *near) {
+    VX_PDL_WAIT();
+    k_bf_scatter_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, off, near);
 }
 
 // atan2 in FP32 for the bulk form's near panel terms: the octant reduction
@@ -587,15 +633,14 @@ __device__ __forceinline__ float vx_half_log_ratio(float r0, float r1, float num
 }
 
 // Direct FP32 panel terms over the near list (chunked like k_rhs_partial).
-__global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx_panel *pan, int P, int P32,
-                                                    const float4 *near, double *part, int nchunks) {
-    VX_PDL_WAIT();
+VX_DEVK void k_rhs_near_body(VxBlkB<RHS_T, 0> vb, const VxScalars *S, const vx_panel *pan, int P, int P32,
+                             const float4 *near, double *part, int nchunks) {
     __shared__ float4 sq4[RHS_T];   // (x, y, G, unused)
     const long long nn = S->bf_nnear;
     const long long cs = vx_ceil_div(vx_ceil_div(nn, nchunks), RHS_T) * RHS_T;
     const int tiles = (P + RHS_T - 1) / RHS_T;
     const long long items = (long long)tiles * nchunks;
-    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    for (long long it = vb.x; it < items; it += vb.n) {
         const int pt = (int)(it % tiles);
         const long long sc = it / tiles;
         const int i = pt * RHS_T + threadIdx.x;
@@ -635,16 +680,20 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx
         }
     }
 }
+__global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx_panel *pan, int P, int P32,
+                                                    const float4 *near, double *part, int nchunks) {
+    VX_PDL_WAIT();
+    k_rhs_near_body(VxBlkB<RHS_T, 0>{blockIdx.x, gridDim.x}, S, pan, P, P32, near, part, nchunks);
+}
 
 // R_i = -(mean velocity along panel i + V_inf) . tau_i; the far field (if
 // coef) adds Re[I_far (tau_x + i tau_y) / (2 pi i dz)] with dz = zb - za.
 // WARP: one warp per panel, its lanes summing the chunk partials (bulk form,
 // fixed butterfly); otherwise one thread per panel in chunk order.
 template <bool WARP>
-__global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int P32,
-                            const double *part, int nchunks, double *R, VxParams p, const double *coef) {
-    VX_PDL_WAIT();
-    const int i = WARP ? (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) : blockIdx.x * blockDim.x + threadIdx.x;
+VX_DEVK void k_rhs_final_body(VxBlkB<0, 0> vb, const VxScalars *S, const vx_panel *pan, int P, int P32,
+                              const double *part, int nchunks, double *R, VxParams p, const double *coef) {
+    const int i = WARP ? (int)((vb.x * blockDim.x + threadIdx.x) >> 5) : vb.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double y0 = 0.0, y1 = 0.0;
     if (WARP) {
@@ -689,40 +738,53 @@ __global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int 
     }
     R[i] = -((u + S->vinf[0]) * pan[i].tang[0] + (w + S->vinf[1]) * pan[i].tang[1]);
 }
+template <bool WARP>
+__global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int P32,
+                            const double *part, int nchunks, double *R, VxParams p, const double *coef) {
+    VX_PDL_WAIT();
+    k_rhs_final_body<WARP>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, pan, P, P32, part, nchunks, R, p, coef);
+}
 
 // gamma_i = sum_j M_ij R_j + M_iP dg, sequential in j with fma (as the
 // oracle), one thread per row; ld is the matrix row stride.
-__global__ void k_gamma(const VxScalars *S, const double *M, long long ld, int P, const double *R,
-                        double *gamma) {
-    VX_PDL_WAIT();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+VX_DEVK void k_gamma_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *M, long long ld, int P, const double *R,
+                          double *gamma) {
+    int i = vb.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     const double *row = M + (long long)i * ld;
     double acc = 0.0;
     for (int j = 0; j < P; ++j) acc = fma(row[j], R[j], acc);
     gamma[i] = fma(row[P], S->dg, acc);
 }
+__global__ void k_gamma(const VxScalars *S, const double *M, long long ld, int P, const double *R,
+                        double *gamma) {
+    VX_PDL_WAIT();
+    k_gamma_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, M, ld, P, R, gamma);
+}
 
 // The same sums from the transposed inverse Mt (Mt[j ld + i] = M[i ld + j]):
 // the same order and fma per row, but a warp's 32 rows read 32 consecutive
 // doubles per step instead of 32 rows' worth of cache lines.
-__global__ void k_gamma_t(const VxScalars *S, const double *Mt, long long ld, int P, const double *R,
-                          double *gamma) {
-    VX_PDL_WAIT();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+VX_DEVK void k_gamma_t_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *Mt, long long ld, int P, const double *R,
+                            double *gamma) {
+    int i = vb.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double acc = 0.0;
     for (int j = 0; j < P; ++j) acc = fma(Mt[(long long)j * ld + i], R[j], acc);
     gamma[i] = fma(Mt[(long long)P * ld + i], S->dg, acc);
 }
+__global__ void k_gamma_t(const VxScalars *S, const double *Mt, long long ld, int P, const double *R,
+                          double *gamma) {
+    VX_PDL_WAIT();
+    k_gamma_t_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, Mt, ld, P, R, gamma);
+}
 
 // Bulk form: one warp per row, lanes striding the row (coalesced), FP64
 // partial sums combined by a fixed butterfly.
-__global__ void k_gamma_w(const VxScalars *S, const double *M, long long ld, int P, const double *R,
-                          double *gamma) {
-    VX_PDL_WAIT();
+VX_DEVK void k_gamma_w_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *M, long long ld, int P, const double *R,
+                            double *gamma) {
     const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = (vb.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= P) return;
     const double *row = M + (long long)i * ld;
     double acc = 0.0;
@@ -730,12 +792,16 @@ __global__ void k_gamma_w(const VxScalars *S, const double *M, long long ld, int
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) gamma[i] = fma(row[P], S->dg, acc);
 }
-
-__global__ void k_transpose(const double *A, double *At, long long nr) {
+__global__ void k_gamma_w(const VxScalars *S, const double *M, long long ld, int P, const double *R,
+                          double *gamma) {
     VX_PDL_WAIT();
+    k_gamma_w_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, M, ld, P, R, gamma);
+}
+
+VX_DEVK void k_transpose_body(VxBlkB<0, 0> vb, const double *A, double *At, long long nr) {
     __shared__ double t[32][33];
     for (long long by = blockIdx.y; by * 32 < nr; by += gridDim.y)
-        for (long long bx = blockIdx.x; bx * 32 < nr; bx += gridDim.x) {
+        for (long long bx = vb.x; bx * 32 < nr; bx += vb.n) {
             for (int r = threadIdx.y; r < 32; r += blockDim.y) {
                 const long long i = by * 32 + r, j = bx * 32 + threadIdx.x;
                 if (i < nr && j < nr) t[r][threadIdx.x] = A[i * nr + j];
@@ -748,19 +814,22 @@ __global__ void k_transpose(const double *A, double *At, long long nr) {
             __syncthreads();
         }
 }
+__global__ void k_transpose(const double *A, double *At, long long nr) {
+    VX_PDL_WAIT();
+    k_transpose_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, A, At, nr);
+}
 
 cudaError_t vx_transpose_square(const VxLaunch &L, const double *A, double *At, long long nr) {
     const long long nb = vx_ceil_div(nr, 32LL);
     const dim3 grid((unsigned)std::min(nb, 64LL), (unsigned)std::min(nb, 64LL)), block(32, 8);
-    vx_launch_pdl(k_transpose, grid, block, 0, L.stream, A, At, nr); VX_COUNT(L);
+    vx_launch<k_transpose, k_transpose_body>(L, grid, block, 0, A, At, nr);
     return cudaGetLastError();
 }
 
 // One new vortex per panel at [n0, n0+P) (src/kernel.cu:862-872).
-__global__ void k_place(VxParams p, VxView v, VxScalars *S, const vx_panel *pan, int P,
-                        const double *gamma) {
-    VX_PDL_WAIT();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+VX_DEVK void k_place_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan, int P,
+                          const double *gamma) {
+    int i = vb.x * blockDim.x + threadIdx.x;
     const long long n0 = S->n0;
     if (i < P) {
         int in = (int)pan[i].n_of_rpanel;
@@ -782,6 +851,11 @@ __global__ void k_place(VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
     }
     if (i == 0) S->n = n0 + P;
 }
+__global__ void k_place(VxParams p, VxView v, VxScalars *S, const vx_panel *pan, int P,
+                        const double *gamma) {
+    VX_PDL_WAIT();
+    k_place_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, P, gamma);
+}
 
 static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S, VxWork &w,
                               const vx_panel *pan, const double *minv, long long ld, const double *minv_t,
@@ -792,31 +866,30 @@ static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView
     const bool far = p.prec == VX_PREC_FP32 && p.birth_far;
     if (far) {
         const int nb = std::min(2 * vx_full_sms(L), VX_BF_MAX_BLOCKS);
-        vx_launch_pdl(k_bf_far, nb, BF_T, 0, L.stream, p, v, S, w.bf_part, w.bf_cnt); VX_COUNT(L);
-        vx_launch_pdl(k_bf_scan, 1, BF_SCAN_T, 0, L.stream, S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef); VX_COUNT(L);
-        vx_launch_pdl(k_bf_scatter, nb, BF_T, 0, L.stream, p, v, S, w.bf_off, w.bf_near); VX_COUNT(L);
-        vx_launch_pdl(k_rhs_near, grid, RHS_T, 0, L.stream, S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
+        vx_launch<k_bf_far, k_bf_far_body>(L, nb, BF_T, 0, p, v, S, w.bf_part, w.bf_cnt);
+        vx_launch<k_bf_scan, k_bf_scan_body>(L, 1, BF_SCAN_T, 0, S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef);
+        vx_launch<k_bf_scatter, k_bf_scatter_body>(L, nb, BF_T, 0, p, v, S, w.bf_off, w.bf_near);
+        vx_launch<k_rhs_near, k_rhs_near_body>(L, grid, RHS_T, 0, S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
     } else if (p.prec == VX_PREC_FP32) {
-        vx_launch_pdl(k_rhs_partial<float>, grid, RHS_T, 0, L.stream, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
+        vx_launch<k_rhs_partial<float>, k_rhs_partial_body<float>>(L, grid, RHS_T, 0, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
     } else {
-        vx_launch_pdl(k_rhs_partial<double>, grid, RHS_T, 0, L.stream, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
+        vx_launch<k_rhs_partial<double>, k_rhs_partial_body<double>>(L, grid, RHS_T, 0, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
     }
-    VX_COUNT(L);
+
     const int b = (P + 127) / 128;
     if (far)
-        vx_launch_pdl(k_rhs_final<true>, (P + 3) / 4, 128, 0, L.stream, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p,
-                                                             w.bf_coef);
+        vx_launch<k_rhs_final<true>, k_rhs_final_body<true>>(L, (P + 3) / 4, 128, 0, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, w.bf_coef);
     else
-        vx_launch_pdl(k_rhs_final<false>, b, 128, 0, L.stream, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, nullptr);
-    VX_COUNT(L);
+        vx_launch<k_rhs_final<false>, k_rhs_final_body<false>>(L, b, 128, 0, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, nullptr);
+
     if (minv_t && p.prec == VX_PREC_FP32)
-        vx_launch_pdl(k_gamma_w, (P + 3) / 4, 128, 0, L.stream, S, minv, ld, P, w.R, w.gamma);
+        vx_launch<k_gamma_w, k_gamma_w_body>(L, (P + 3) / 4, 128, 0, S, minv, ld, P, w.R, w.gamma);
     else if (minv_t)
-        vx_launch_pdl(k_gamma_t, b, 128, 0, L.stream, S, minv_t, ld, P, w.R, w.gamma);
+        vx_launch<k_gamma_t, k_gamma_t_body>(L, b, 128, 0, S, minv_t, ld, P, w.R, w.gamma);
     else
-        vx_launch_pdl(k_gamma, b, 128, 0, L.stream, S, minv, ld, P, w.R, w.gamma);
-    VX_COUNT(L);
-    vx_launch_pdl(k_place, b, 128, 0, L.stream, p, v, S, pan, P, w.gamma); VX_COUNT(L);
+        vx_launch<k_gamma, k_gamma_body>(L, b, 128, 0, S, minv, ld, P, w.R, w.gamma);
+
+    vx_launch<k_place, k_place_body>(L, b, 128, 0, p, v, S, pan, P, w.gamma);
     return cudaGetLastError();
 }
 
@@ -837,6 +910,6 @@ cudaError_t vx_launch_birth(const VxLaunch &L, const VxParams &p, const VxView &
 }
 
 cudaError_t vx_launch_step_end(const VxLaunch &L, VxScalars *S) {
-    vx_launch_pdl(k_step_end, 1, 1, 0, L.stream, S); VX_COUNT(L);
+    vx_launch<k_step_end, k_step_end_body>(L, 1, 1, 0, S);
     return cudaGetLastError();
 }

@@ -31,25 +31,27 @@ constexpr int CG_W = 32;       // targets per work item (one warp)
 constexpr int CG_DIV = VX_CG_DIV;      // cell side = cut-off radius at the mean d / CG_DIV
 constexpr int CG_KCAP = 2 * CG_DIV;    // widest window of a work item, in cells (twice the mean radius)
 
-__global__ void k_cg_begin(VxScalars *S) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cg_begin_body(VxBlkB<0, 0> vb, VxScalars *S) {
     S->cb[0] = S->cb[1] = S->cb[2] = S->cb[3] = ~0ull;
     S->cnwide = 0;
     S->cnhuge = 0;
     S->bk_nmid = S->bk_nbig = 0;
 }
+__global__ void k_cg_begin(VxScalars *S) {
+    VX_PDL_WAIT();
+    k_cg_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
+}
 
 // Bounding box of the live particles and per-block sums of d (fixed grid:
 // the mean below is reproducible).
-__global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double *red) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cg_bbox_body(VxBlkB<CG_T, 0> vb, VxView v, VxScalars *S, double *red) {
     __shared__ unsigned long long sk[4][CG_T];
     __shared__ double sd[CG_T];
     const long long n = S->n;
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
     double dsum = 0.0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         const double x = v.x[i * v.ps], y = v.y[i * v.ps];
         k[0] = min(k[0], vx_dkey(x));
         k[1] = min(k[1], vx_dkey(-x));
@@ -69,16 +71,19 @@ __global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double
     }
     if (threadIdx.x == 0) {
         for (int q = 0; q < 4; ++q) atomicMin(&S->cb[q], sk[q][0]);
-        red[blockIdx.x] = sd[0];
+        red[vb.x] = sd[0];
     }
+}
+__global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double *red) {
+    VX_PDL_WAIT();
+    k_cg_bbox_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, v, S, red);
 }
 
 // Cell side h = c * mean(d) / CG_DIV, grown until the grid fits cells_cap.
 // One block of CG_T threads: the per-block sums of d are added in a fixed
 // tree (reproducible), then thread 0 sizes the grid.
-__global__ void __launch_bounds__(CG_T) k_cg_params(VxScalars *S, const double *red, int nblocks, double cutoff,
-                                                    long long cells_cap) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cg_params_body(VxBlkB<CG_T, 0> vb, VxScalars *S, const double *red, int nblocks, double cutoff,
+                              long long cells_cap) {
     __shared__ double sd[CG_T];
     double part = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += CG_T) part += red[b];
@@ -107,6 +112,11 @@ __global__ void __launch_bounds__(CG_T) k_cg_params(VxScalars *S, const double *
     S->cx0 = x0; S->cy0 = y0; S->ch = h;
     S->cnx = nx; S->cny = ny; S->cncells = nx * ny;
 }
+__global__ void __launch_bounds__(CG_T) k_cg_params(VxScalars *S, const double *red, int nblocks, double cutoff,
+                                                    long long cells_cap) {
+    VX_PDL_WAIT();
+    k_cg_params_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, S, red, nblocks, cutoff, cells_cap);
+}
 
 __device__ __forceinline__ long long cg_cell(const VxScalars *S, double x, double y) {
     long long cx = (long long)floor((x - S->cx0) / S->ch);
@@ -116,34 +126,39 @@ __device__ __forceinline__ long long cg_cell(const VxScalars *S, double x, doubl
     return cy * S->cnx + cx;
 }
 
-__global__ void k_cg_zero(const VxScalars *S, int *cnt) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cg_zero_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt) {
     const long long nc = S->cncells;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
-         c += (long long)gridDim.x * blockDim.x)
+    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < nc;
+         c += (long long)vb.n * blockDim.x)
         cnt[c] = 0;
 }
-
-__global__ void k_cg_cellid(VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
+__global__ void k_cg_zero(const VxScalars *S, int *cnt) {
     VX_PDL_WAIT();
+    k_cg_zero_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt);
+}
+
+VX_DEVK void k_cg_cellid_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
     const long long n = S->n;
     if (S->cncells == 0) return;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         const long long c = cg_cell(S, v.x[i * v.ps], v.y[i * v.ps]);
         key[i] = (unsigned)c;
         val[i] = (int)i;
         atomicAdd(&cnt[c], 1);
     }
 }
+__global__ void k_cg_cellid(VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
+    VX_PDL_WAIT();
+    k_cg_cellid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, key, val, cnt);
+}
 
 // Exclusive scan of cnt[0, len) into start[], start[len] = total: chunk
 // sums, one-block scan of the chunk sums, per-chunk apply.
-__global__ void __launch_bounds__(CG_T) k_scan_sum(const long long *len_p, const int *cnt, int *csum) {
-    VX_PDL_WAIT();
+VX_DEVK void k_scan_sum_body(VxBlkB<CG_T, 0> vb, const long long *len_p, const int *cnt, int *csum) {
     __shared__ int sh[CG_T];
     const long long len = *len_p, nch = vx_ceil_div(len, VX_CHUNK);
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    for (long long c = vb.x; c < nch; c += vb.n) {
         int k = 0;
         for (long long q = c * VX_CHUNK + threadIdx.x; q < min(len, (c + 1) * VX_CHUNK); q += blockDim.x) k += cnt[q];
         sh[threadIdx.x] = k;
@@ -156,9 +171,12 @@ __global__ void __launch_bounds__(CG_T) k_scan_sum(const long long *len_p, const
         __syncthreads();
     }
 }
-
-__global__ void k_scan_top(const long long *len_p, const int *csum, long long *coff) {
+__global__ void __launch_bounds__(CG_T) k_scan_sum(const long long *len_p, const int *cnt, int *csum) {
     VX_PDL_WAIT();
+    k_scan_sum_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, len_p, cnt, csum);
+}
+
+VX_DEVK void k_scan_top_body(VxBlkB<0, 0> vb, const long long *len_p, const int *csum, long long *coff) {
     __shared__ long long sh[1024];
     __shared__ long long carry;
     const long long nch = vx_ceil_div(*len_p, VX_CHUNK);
@@ -181,15 +199,18 @@ __global__ void k_scan_top(const long long *len_p, const int *csum, long long *c
         __syncthreads();
     }
 }
-
-__global__ void __launch_bounds__(CG_T) k_scan_apply(const long long *len_p, const int *cnt, const long long *coff,
-                                                     int *start, const long long *total_p) {
+__global__ void k_scan_top(const long long *len_p, const int *csum, long long *coff) {
     VX_PDL_WAIT();
+    k_scan_top_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, len_p, csum, coff);
+}
+
+VX_DEVK void k_scan_apply_body(VxBlkB<CG_T, 0> vb, const long long *len_p, const int *cnt, const long long *coff,
+                               int *start, const long long *total_p) {
     constexpr int PER = VX_CHUNK / CG_T;
     __shared__ int sh[CG_T];
     const long long len = *len_p, nch = vx_ceil_div(len, VX_CHUNK);
-    if (blockIdx.x == 0 && threadIdx.x == 0) start[len] = (int)*total_p;
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    if (vb.x == 0 && threadIdx.x == 0) start[len] = (int)*total_p;
+    for (long long c = vb.x; c < nch; c += vb.n) {
         const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
         int val[PER], loc = 0;
 #pragma unroll
@@ -211,16 +232,20 @@ __global__ void __launch_bounds__(CG_T) k_scan_apply(const long long *len_p, con
         }
     }
 }
+__global__ void __launch_bounds__(CG_T) k_scan_apply(const long long *len_p, const int *cnt, const long long *coff,
+                                                     int *start, const long long *total_p) {
+    VX_PDL_WAIT();
+    k_scan_apply_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, len_p, cnt, coff, start, total_p);
+}
 
 // Cell-sorted particles (x, y relative to their cell centre, G, d).  Keeping
 // FP32 positions relative to the cell keeps the pair differences accurate to
 // FP32 rounding of the local spacing rather than of the absolute position.
-__global__ void k_cg_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cg_gather_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
     const long long n = S->n, nx = S->cnx;
     const double h = S->ch;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x) {
+    for (long long k = vb.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)vb.n * blockDim.x) {
         const long long i = sorted[k];
         const long long c = skey[k];
         const double ccx = S->cx0 + ((double)(c % nx) + 0.5) * h, ccy = S->cy0 + ((double)(c / nx) + 0.5) * h;
@@ -228,10 +253,13 @@ __global__ void k_cg_gather(VxView v, const VxScalars *S, const int *sorted, con
                              (float)v.d[i]);
     }
 }
+__global__ void k_cg_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
+    VX_PDL_WAIT();
+    k_cg_gather_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, sorted, skey, srt);
+}
 
 // Exclusive scan of the per-row item counts (single block, runs per thread).
-__global__ void k_cg_row_scan(const VxScalars *S, const int *in, long long *out) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cg_row_scan_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *in, long long *out) {
     __shared__ long long sh[1024];
     const long long len = S->cny;
     const long long per = vx_ceil_div(len, (long long)blockDim.x);
@@ -252,34 +280,45 @@ __global__ void k_cg_row_scan(const VxScalars *S, const int *in, long long *out)
         run += in[q];
     }
 }
+__global__ void k_cg_row_scan(const VxScalars *S, const int *in, long long *out) {
+    VX_PDL_WAIT();
+    k_cg_row_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, in, out);
+}
 
 // Work items: each row's sorted range cut into segments of CG_W targets.
-__global__ void k_cg_row_items(const VxScalars *S, const int *start, int *row_items) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cg_row_items_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, int *row_items) {
     const long long ny = S->cny, nx = S->cnx;
-    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ny;
-         r += (long long)gridDim.x * blockDim.x) {
+    for (long long r = vb.x * (long long)blockDim.x + threadIdx.x; r < ny;
+         r += (long long)vb.n * blockDim.x) {
         const int cnt = start[(r + 1) * nx] - start[r * nx];
         row_items[r] = (cnt + CG_W - 1) / CG_W;
     }
 }
-
-__global__ void k_cg_items(VxScalars *S, const int *start, const int *row_items, const long long *row_off,
-                           int2 *items, long long items_cap) {
+__global__ void k_cg_row_items(const VxScalars *S, const int *start, int *row_items) {
     VX_PDL_WAIT();
+    k_cg_row_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items);
+}
+
+VX_DEVK void k_cg_items_body(VxBlkB<0, 0> vb, VxScalars *S, const int *start, const int *row_items, const long long *row_off,
+                             int2 *items, long long items_cap) {
     const long long ny = S->cny, nx = S->cnx;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && ny > 0) {
+    if (vb.x == 0 && threadIdx.x == 0 && ny > 0) {
         const long long tot = row_off[ny - 1] + row_items[ny - 1];
         S->cnitems = tot <= items_cap ? tot : 0;
         if (tot > items_cap) S->err |= VX_DERR_GRID;
     }
-    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ny;
-         r += (long long)gridDim.x * blockDim.x) {
+    for (long long r = vb.x * (long long)blockDim.x + threadIdx.x; r < ny;
+         r += (long long)vb.n * blockDim.x) {
         const long long o = row_off[r];
         const int s0 = start[r * nx];
         for (int q = 0; q < row_items[r]; ++q)
             if (o + q < items_cap) items[o + q] = make_int2((int)r, s0 + q * CG_W);
     }
+}
+__global__ void k_cg_items(VxScalars *S, const int *start, const int *row_items, const long long *row_off,
+                           int2 *items, long long items_cap) {
+    VX_PDL_WAIT();
+    k_cg_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items, row_off, items, items_cap);
 }
 
 __device__ __forceinline__ float vx_rsqrt_approx(float x) {
@@ -381,11 +420,10 @@ struct DiffRow {
     float oy;        // row offset * h
 };
 constexpr int DIFF_ROWS = 2 * CG_KCAP + 2;   // rows of the widest window, and the total
-__global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, VxView v, VxScalars *S,
-                                                                   const float4 *srt, const unsigned *skey,
-                                                                   const int *sorted, const int *start,
-                                                                   const int2 *items, int *wide) {
-    VX_PDL_WAIT();
+VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView v, VxScalars *S,
+                               const float4 *srt, const unsigned *skey,
+                               const int *sorted, const int *start,
+                               const int2 *items, int *wide) {
     __shared__ float4 sxy[CG_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
     __shared__ float2 sg[CG_T / 2];    // (G_a, G_b)
     __shared__ DiffRow srow[CG_T / 32][DIFF_ROWS];
@@ -401,7 +439,7 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
     const float log2e = 1.4426950408889634f;
     const long long wpb = CG_T / 32;
     unsigned long long pairs = 0;
-    for (long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < nitems; it += gridDim.x * wpb) {
+    for (long long it = vb.x * wpb + (threadIdx.x >> 5); it < nitems; it += vb.n * wpb) {
         const int2 item = items[it];
         const long long row = item.x;
         const long long row_end = start[(row + 1) * nx];
@@ -510,6 +548,13 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
     }
     if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);
 }
+__global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, VxView v, VxScalars *S,
+                                                                   const float4 *srt, const unsigned *skey,
+                                                                   const int *sorted, const int *start,
+                                                                   const int2 *items, int *wide) {
+    VX_PDL_WAIT();
+    k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB>{blockIdx.x, gridDim.x}, p, v, S, srt, skey, sorted, start, items, wide);
+}
 
 // Targets left out of the work items (radius beyond CG_KCAP cells).  Most
 // have windows of a few thousand sources: one warp each (k_diff_wide), the
@@ -557,10 +602,9 @@ __device__ __forceinline__ void wide_apply(const VxParams &p, VxView v, const in
     }
 }
 
-__global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
-                                                    const unsigned *skey, const int *sorted, const int *start,
-                                                    const int *wide, int *huge) {
-    VX_PDL_WAIT();
+VX_DEVK void k_diff_wide_body(VxBlkB<CG_T, 0> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                              const unsigned *skey, const int *sorted, const int *start,
+                              const int *wide, int *huge) {
     const int lane = threadIdx.x & 31;
     const long long nx = S->cnx, ny = S->cny;
     const float h = (float)S->ch;
@@ -569,9 +613,9 @@ __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScal
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
     const float log2e = 1.4426950408889634f;
     const int nw = S->cnwide;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const int warps = (vb.n * blockDim.x) >> 5;
     unsigned long long pairs = 0;
-    for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < nw; f += warps) {
+    for (int f = (vb.x * blockDim.x + threadIdx.x) >> 5; f < nw; f += warps) {
         const long long t = wide[f];
         const float4 me = srt[t];
         const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
@@ -593,11 +637,16 @@ __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScal
     }
     if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);   // every lane counted the same pairs
 }
-
-__global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxScalars *S, const float4 *srt,
-                                                      const unsigned *skey, const int *sorted, const int *start,
-                                                      const int *huge) {
+__global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                                                    const unsigned *skey, const int *sorted, const int *start,
+                                                    const int *wide, int *huge) {
     VX_PDL_WAIT();
+    k_diff_wide_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, p, v, S, srt, skey, sorted, start, wide, huge);
+}
+
+VX_DEVK void k_diff_huge_body(VxBlkB<WIDE_T, 0> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                              const unsigned *skey, const int *sorted, const int *start,
+                              const int *huge) {
     constexpr int NWARP = WIDE_T / 32;
     __shared__ double sred[3][NWARP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -609,7 +658,7 @@ __global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxSc
     const float log2e = 1.4426950408889634f;
     const int nh = S->cnhuge;
     unsigned long long pairs = 0;
-    for (int f = blockIdx.x; f < nh; f += gridDim.x) {
+    for (int f = vb.x; f < nh; f += vb.n) {
         const long long t = huge[f];
         const float4 me = srt[t];
         const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
@@ -634,40 +683,44 @@ __global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxSc
     }
     if (lane == 0 && pairs) atomicAdd(&S->pairs_diff, pairs);   // a warp's lanes counted the same rows
 }
+__global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                                                      const unsigned *skey, const int *sorted, const int *start,
+                                                      const int *huge) {
+    VX_PDL_WAIT();
+    k_diff_huge_body(VxBlkB<WIDE_T, 0>{blockIdx.x, gridDim.x}, p, v, S, srt, skey, sorted, start, huge);
+}
 
 // Build the grid and run the bulk diffusion.  Scratch from w; the collapse
 // chunk arrays are reused (the passes run one after the other on one stream).
 cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                       VxWork &w) {
     const int grid = L.num_sms * 4;
-    vx_launch_pdl(k_cg_begin, 1, 1, 0, L.stream, S); VX_COUNT(L);
-    vx_launch_pdl(k_cg_bbox, VX_RED_BLOCKS, CG_T, 0, L.stream, v, S, w.red); VX_COUNT(L);
-    vx_launch_pdl(k_cg_params, 1, CG_T, 0, L.stream, S, w.red, VX_RED_BLOCKS, p.diff_cutoff, w.cells_cap); VX_COUNT(L);
-    vx_launch_pdl(k_cg_zero, grid, CG_T, 0, L.stream, S, w.cg_cnt); VX_COUNT(L);
-    vx_launch_pdl(k_cg_cellid, grid, CG_T, 0, L.stream, v, S, w.key0, w.val0, w.cg_cnt); VX_COUNT(L);
-    vx_launch_pdl(k_scan_sum, grid, CG_T, 0, L.stream, &S->cncells, w.cg_cnt, w.cell_chunk_cnt); VX_COUNT(L);
-    vx_launch_pdl(k_scan_top, 1, 1024, 0, L.stream, &S->cncells, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
-    vx_launch_pdl(k_scan_apply, grid, CG_T, 0, L.stream, &S->cncells, w.cg_cnt, w.cell_chunk_off, w.cg_start, &S->n);
-    VX_COUNT(L);
+    vx_launch<k_cg_begin, k_cg_begin_body>(L, 1, 1, 0, S);
+    vx_launch<k_cg_bbox, k_cg_bbox_body>(L, VX_RED_BLOCKS, CG_T, 0, v, S, w.red);
+    vx_launch<k_cg_params, k_cg_params_body>(L, 1, CG_T, 0, S, w.red, VX_RED_BLOCKS, p.diff_cutoff, w.cells_cap);
+    vx_launch<k_cg_zero, k_cg_zero_body>(L, grid, CG_T, 0, S, w.cg_cnt);
+    vx_launch<k_cg_cellid, k_cg_cellid_body>(L, grid, CG_T, 0, v, S, w.key0, w.val0, w.cg_cnt);
+    vx_launch<k_scan_sum, k_scan_sum_body>(L, grid, CG_T, 0, &S->cncells, w.cg_cnt, w.cell_chunk_cnt);
+    vx_launch<k_scan_top, k_scan_top_body>(L, 1, 1024, 0, &S->cncells, w.cell_chunk_cnt, w.cell_chunk_off);
+    vx_launch<k_scan_apply, k_scan_apply_body>(L, grid, CG_T, 0, &S->cncells, w.cg_cnt, w.cell_chunk_off, w.cg_start, &S->n);
+
     // cell order: each cell's vortices in index order (a stable sort by cell)
     vx_bucket_order(L, S, &S->n, &S->cncells, w.key0, w.cg_start, w.cg_cnt, nullptr, w.key1, w.val1, w.bk_mid, w.bk_big,
                     w.val0);
     const unsigned *skey = w.key1;
     const int *sorted = w.val1;
-    vx_launch_pdl(k_cg_gather, grid, CG_T, 0, L.stream, v, S, sorted, skey, w.srt); VX_COUNT(L);
-    vx_launch_pdl(k_cg_row_items, grid, CG_T, 0, L.stream, S, w.cg_start, w.row_items); VX_COUNT(L);
-    vx_launch_pdl(k_cg_row_scan, 1, 1024, 0, L.stream, S, w.row_items, w.row_item_off); VX_COUNT(L);
-    vx_launch_pdl(k_cg_items, grid, CG_T, 0, L.stream, S, w.cg_start, w.row_items, w.row_item_off, w.items, w.items_cap);
-    VX_COUNT(L);
+    vx_launch<k_cg_gather, k_cg_gather_body>(L, grid, CG_T, 0, v, S, sorted, skey, w.srt);
+    vx_launch<k_cg_row_items, k_cg_row_items_body>(L, grid, CG_T, 0, S, w.cg_start, w.row_items);
+    vx_launch<k_cg_row_scan, k_cg_row_scan_body>(L, 1, 1024, 0, S, w.row_items, w.row_item_off);
+    vx_launch<k_cg_items, k_cg_items_body>(L, grid, CG_T, 0, S, w.cg_start, w.row_items, w.row_item_off, w.items, w.items_cap);
+
     VX_EV(L, 2);
-    vx_launch_pdl(k_diff_cells, L.num_sms * 8, CG_T, 0, L.stream, p, v, S, w.srt, skey, sorted, w.cg_start, w.items,
-                                                       w.cg_wide);
-    VX_COUNT(L);
-    vx_launch_pdl(k_diff_wide, L.num_sms * 4, CG_T, 0, L.stream, p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide,
-                                                      w.cg_huge);
-    VX_COUNT(L);
-    vx_launch_pdl(k_diff_huge, L.num_sms * 2, WIDE_T, 0, L.stream, p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_huge);
-    VX_COUNT(L);
+    vx_launch<k_diff_cells, k_diff_cells_body>(L, L.num_sms * 8, CG_T, 0, p, v, S, w.srt, skey, sorted, w.cg_start, w.items, w.cg_wide);
+
+    vx_launch<k_diff_wide, k_diff_wide_body>(L, L.num_sms * 4, CG_T, 0, p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_wide, w.cg_huge);
+
+    vx_launch<k_diff_huge, k_diff_huge_body>(L, L.num_sms * 2, WIDE_T, 0, p, v, S, w.srt, skey, sorted, w.cg_start, w.cg_huge);
+
     VX_EV(L, 3);
     return cudaGetLastError();
 }

@@ -21,23 +21,25 @@
 
 #include "vx_internal.cuh"
 
-__global__ void k_col_begin(VxScalars *S, int reset) {
-    VX_PDL_WAIT();
+VX_DEVK void k_col_begin_body(VxBlkB<0, 0> vb, VxScalars *S, int reset) {
     if (reset) S->col_done = 0;
     if (S->col_done) return;
     S->col_n_before = S->n;
     S->ncand = 0;
     S->bb[0] = S->bb[1] = S->bb[2] = S->bb[3] = ~0ull;
 }
-
-__global__ void k_col_bbox(VxView v, VxScalars *S) {
+__global__ void k_col_begin(VxScalars *S, int reset) {
     VX_PDL_WAIT();
+    k_col_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, reset);
+}
+
+VX_DEVK void k_col_bbox_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S) {
     if (S->col_done) return;
     __shared__ unsigned long long sh[4][VX_THREADS];
     const long long n = S->n;
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         const double x = v.x[i * v.ps], y = v.y[i * v.ps];
         k[0] = min(k[0], vx_dkey(x));
         k[1] = min(k[1], vx_dkey(-x));
@@ -54,11 +56,14 @@ __global__ void k_col_bbox(VxView v, VxScalars *S) {
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) atomicMin(&S->bb[q], sh[q][0]);
 }
+__global__ void k_col_bbox(VxView v, VxScalars *S) {
+    VX_PDL_WAIT();
+    k_col_bbox_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S);
+}
 
 // Cell size h = r (1 + 1e-6): any pair closer than r is in neighbouring cells.
 // When the box would need more than cells_cap cells, h grows.
-__global__ void k_col_grid(VxScalars *S, double r2, long long cells_cap) {
-    VX_PDL_WAIT();
+VX_DEVK void k_col_grid_body(VxBlkB<0, 0> vb, VxScalars *S, double r2, long long cells_cap) {
     if (S->col_done) return;
     const long long n = S->n;
     if (n == 0) { S->gncells = 0; S->gnx = S->gny = 0; return; }
@@ -79,6 +84,10 @@ __global__ void k_col_grid(VxScalars *S, double r2, long long cells_cap) {
     S->gx0 = x0; S->gy0 = y0; S->gh = h;
     S->gnx = nx; S->gny = ny; S->gncells = nx * ny;
 }
+__global__ void k_col_grid(VxScalars *S, double r2, long long cells_cap) {
+    VX_PDL_WAIT();
+    k_col_grid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, r2, cells_cap);
+}
 
 __device__ __forceinline__ void vx_cell_of(const VxScalars *S, double x, double y, long long &cx,
                                            long long &cy) {
@@ -88,22 +97,24 @@ __device__ __forceinline__ void vx_cell_of(const VxScalars *S, double x, double 
     cy = cy < 0 ? 0 : (cy >= S->gny ? S->gny - 1 : cy);
 }
 
-__global__ void k_col_zero_cells(const VxScalars *S, int *cnt) {
-    VX_PDL_WAIT();
+VX_DEVK void k_col_zero_cells_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt) {
     if (S->col_done) return;
     const long long nc = S->gncells;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
-         c += (long long)gridDim.x * blockDim.x)
+    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < nc;
+         c += (long long)vb.n * blockDim.x)
         cnt[c] = 0;
 }
-
-__global__ void k_col_count(VxView v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
-                            int *has_app, int *first_app) {
+__global__ void k_col_zero_cells(const VxScalars *S, int *cnt) {
     VX_PDL_WAIT();
+    k_col_zero_cells_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt);
+}
+
+VX_DEVK void k_col_count_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
+                              int *has_app, int *first_app) {
     if (S->col_done) return;
     const long long n = S->n;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         long long cx, cy;
         vx_cell_of(S, v.x[i * v.ps], v.y[i * v.ps], cx, cy);
         const long long c = cy * S->gnx + cx;
@@ -114,15 +125,19 @@ __global__ void k_col_count(VxView v, const VxScalars *S, int *cellid, int *cnt,
         first_app[i] = INT_MAX;
     }
 }
+__global__ void k_col_count(VxView v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
+                            int *has_app, int *first_app) {
+    VX_PDL_WAIT();
+    k_col_count_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cellid, cnt, in_cnt, has_app, first_app);
+}
 
 // Exclusive scan of cnt[0, gncells) into start[], start[gncells] = total.
-__global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cell_chunk_sum_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *cnt, int *csum) {
     if (S->col_done) return;
     __shared__ int sh[VX_THREADS];
     const long long nc = S->gncells;
     const long long nch = vx_ceil_div(nc, VX_CHUNK);
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    for (long long c = vb.x; c < nch; c += vb.n) {
         int k = 0;
         for (long long p = c * VX_CHUNK + threadIdx.x; p < min(nc, (c + 1) * VX_CHUNK); p += blockDim.x)
             k += cnt[p];
@@ -136,9 +151,12 @@ __global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) 
         __syncthreads();
     }
 }
-
-__global__ void k_cell_chunk_scan(const VxScalars *S, const int *csum, long long *coff) {
+__global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) {
     VX_PDL_WAIT();
+    k_cell_chunk_sum_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt, csum);
+}
+
+VX_DEVK void k_cell_chunk_scan_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
     if (S->col_done) return;
     __shared__ long long sh[1024];
     __shared__ long long carry;
@@ -162,17 +180,20 @@ __global__ void k_cell_chunk_scan(const VxScalars *S, const int *csum, long long
         __syncthreads();
     }
 }
-
-__global__ void __launch_bounds__(VX_THREADS) k_cell_chunk_apply(const VxScalars *S, const int *cnt,
-                                                                 const long long *coff, int *start) {
+__global__ void k_cell_chunk_scan(const VxScalars *S, const int *csum, long long *coff) {
     VX_PDL_WAIT();
+    k_cell_chunk_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
+}
+
+VX_DEVK void k_cell_chunk_apply_body(VxBlkB<VX_THREADS, 0> vb, const VxScalars *S, const int *cnt,
+                                     const long long *coff, int *start) {
     if (S->col_done) return;
     constexpr int PER = VX_CHUNK / VX_THREADS;
     __shared__ int sh[VX_THREADS];
     const long long nc = S->gncells;
     const long long nch = vx_ceil_div(nc, VX_CHUNK);
-    if (blockIdx.x == 0 && threadIdx.x == 0) start[nc] = (int)S->n;   // sentinel
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    if (vb.x == 0 && threadIdx.x == 0) start[nc] = (int)S->n;   // sentinel
+    for (long long c = vb.x; c < nch; c += vb.n) {
         const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
         int val[PER];
         int loc = 0;
@@ -198,18 +219,27 @@ __global__ void __launch_bounds__(VX_THREADS) k_cell_chunk_apply(const VxScalars
         }
     }
 }
-
-__global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *start, int *cnt,
-                              int *sorted) {
+__global__ void __launch_bounds__(VX_THREADS) k_cell_chunk_apply(const VxScalars *S, const int *cnt,
+                                                                 const long long *coff, int *start) {
     VX_PDL_WAIT();
+    k_cell_chunk_apply_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, S, cnt, coff, start);
+}
+
+VX_DEVK void k_col_scatter_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *cellid, const int *start, int *cnt,
+                                int *sorted) {
     if (S->col_done) return;
     const long long n = S->n;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         const int c = cellid[i];
         const int k = atomicSub(&cnt[c], 1) - 1;
         sorted[start[c] + k] = (int)i;
     }
+}
+__global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *start, int *cnt,
+                              int *sorted) {
+    VX_PDL_WAIT();
+    k_col_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cellid, start, cnt, sorted);
 }
 
 // COL[i] = smallest j > i in the 3x3 cell neighbourhood that qualifies.  The
@@ -217,15 +247,14 @@ __global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *
 // read the same cells and sources; each target's answer does not depend on
 // the order.
 template <int PASS>
-__global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
-                            const int *sorted, int *col, int *in_cnt, int *cand) {
-    VX_PDL_WAIT();
+VX_DEVK void k_col_query_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
+                              const int *sorted, int *col, int *in_cnt, int *cand) {
     if (S->col_done) return;
     const long long n = S->n;
     const long long gnx = S->gnx, gny = S->gny;
     const double rd2 = p.r_diff2, rs2 = p.r_same2, mvg = p.max_ve_g;
-    for (long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k0 < n;
-         k0 += (long long)gridDim.x * blockDim.x) {
+    for (long long k0 = vb.x * (long long)blockDim.x + threadIdx.x; k0 < n;
+         k0 += (long long)vb.n * blockDim.x) {
         const long long i = sorted[k0];
         const double xi = v.x[i * v.ps], yi = v.y[i * v.ps], gi = v.g[i * v.ps];
         const long long c = cellid[i];
@@ -257,12 +286,17 @@ __global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *celli
         }
     }
 }
+template <int PASS>
+__global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
+                            const int *sorted, int *col, int *in_cnt, int *cand) {
+    VX_PDL_WAIT();
+    k_col_query_body<PASS>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, cellid, start, sorted, col, in_cnt, cand);
+}
 
 // Rounds over the candidate list (single block).  cstate: 0 undecided,
 // 1 applied, 2 consumed before its turn.
-__global__ void k_col_resolve(VxScalars *S, const int *cand, const int *col, int *in_cnt,
-                              int *has_app, int *first_app, int *cstate, int *cdec) {
-    VX_PDL_WAIT();
+VX_DEVK void k_col_resolve_body(VxBlkB<0, 0> vb, VxScalars *S, const int *cand, const int *col, int *in_cnt,
+                                int *has_app, int *first_app, int *cstate, int *cdec) {
     if (S->col_done) return;
     __shared__ int undecided;
     const int nc = S->ncand;
@@ -303,15 +337,19 @@ __global__ void k_col_resolve(VxScalars *S, const int *cand, const int *col, int
         S->col_done = 1;
     }
 }
+__global__ void k_col_resolve(VxScalars *S, const int *cand, const int *col, int *in_cnt,
+                              int *has_app, int *first_app, int *cstate, int *cdec) {
+    VX_PDL_WAIT();
+    k_col_resolve_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cand, col, in_cnt, has_app, first_app, cstate, cdec);
+}
 
 template <int PASS>
-__global__ void k_col_merge(VxView v, const VxScalars *S, const int *cand, const int *col,
-                            const int *cstate, const int *first_app, double *mx, double *my,
-                            double *mg) {
-    VX_PDL_WAIT();
+VX_DEVK void k_col_merge_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *cand, const int *col,
+                              const int *cstate, const int *first_app, double *mx, double *my,
+                              double *mg) {
     if (S->col_done) return;
     const int nc = S->ncand;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+    for (int k = vb.x * blockDim.x + threadIdx.x; k < nc; k += vb.n * blockDim.x) {
         if (cstate[k] != 1) continue;
         const long long i = cand[k], j = col[i];
         const double xi = v.x[i * v.ps], yi = v.y[i * v.ps], gi = v.g[i * v.ps];
@@ -331,24 +369,38 @@ __global__ void k_col_merge(VxView v, const VxScalars *S, const int *cand, const
         }
     }
 }
-
-__global__ void k_col_apply(VxView v, const VxScalars *S, const int *cand, const int *col,
-                            const int *cstate, const double *mx, const double *my, const double *mg) {
+template <int PASS>
+__global__ void k_col_merge(VxView v, const VxScalars *S, const int *cand, const int *col,
+                            const int *cstate, const int *first_app, double *mx, double *my,
+                            double *mg) {
     VX_PDL_WAIT();
+    k_col_merge_body<PASS>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cand, col, cstate, first_app, mx, my, mg);
+}
+
+VX_DEVK void k_col_apply_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *cand, const int *col,
+                              const int *cstate, const double *mx, const double *my, const double *mg) {
     if (S->col_done) return;
     const int nc = S->ncand;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+    for (int k = vb.x * blockDim.x + threadIdx.x; k < nc; k += vb.n * blockDim.x) {
         if (cstate[k] != 1) continue;
         const long long i = cand[k], j = col[i];
         v.x[i * v.ps] = mx[k]; v.y[i * v.ps] = my[k]; v.g[i * v.ps] = mg[k];
         v.x[j * v.ps] = 1e10; v.y[j * v.ps] = 1e10; v.g[j * v.ps] = 0.0;
     }
 }
-
-__global__ void k_col_end(VxScalars *S) {
+__global__ void k_col_apply(VxView v, const VxScalars *S, const int *cand, const int *col,
+                            const int *cstate, const double *mx, const double *my, const double *mg) {
     VX_PDL_WAIT();
+    k_col_apply_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cand, col, cstate, mx, my, mg);
+}
+
+VX_DEVK void k_col_end_body(VxBlkB<0, 0> vb, VxScalars *S) {
     if (S->col_done) return;
     if (S->n == S->col_n_before) S->col_done = 1;
+}
+__global__ void k_col_end(VxScalars *S) {
+    VX_PDL_WAIT();
+    k_col_end_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
 }
 
 cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
@@ -357,38 +409,30 @@ cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxVie
     if (!(r2 > 0.0) || n_col <= 0) return cudaSuccess;   // no pair can qualify
     const int grid = L.num_sms * 4;
     for (int cc = 0; cc < n_col; ++cc) {
-        vx_launch_pdl(k_col_begin, 1, 1, 0, L.stream, S, cc == 0); VX_COUNT(L);
-        vx_launch_pdl(k_col_bbox, grid, VX_THREADS, 0, L.stream, v, S); VX_COUNT(L);
-        vx_launch_pdl(k_col_grid, 1, 1, 0, L.stream, S, r2, w.cells_cap); VX_COUNT(L);
-        vx_launch_pdl(k_col_zero_cells, grid, VX_THREADS, 0, L.stream, S, w.cell_cnt); VX_COUNT(L);
-        vx_launch_pdl(k_col_count, grid, VX_THREADS, 0, L.stream, v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app,
-                                                       w.first_app); VX_COUNT(L);
-        vx_launch_pdl(k_cell_chunk_sum, grid, VX_THREADS, 0, L.stream, S, w.cell_cnt, w.cell_chunk_cnt); VX_COUNT(L);
-        vx_launch_pdl(k_cell_chunk_scan, 1, 1024, 0, L.stream, S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
-        vx_launch_pdl(k_cell_chunk_apply, grid, VX_THREADS, 0, L.stream, S, w.cell_cnt, w.cell_chunk_off,
-                                                              w.cell_start); VX_COUNT(L);
-        vx_launch_pdl(k_col_scatter, grid, VX_THREADS, 0, L.stream, S, w.cellid, w.cell_start, w.cell_cnt,
-                                                         w.sorted); VX_COUNT(L);
+        vx_launch<k_col_begin, k_col_begin_body>(L, 1, 1, 0, S, cc == 0);
+        vx_launch<k_col_bbox, k_col_bbox_body>(L, grid, VX_THREADS, 0, v, S);
+        vx_launch<k_col_grid, k_col_grid_body>(L, 1, 1, 0, S, r2, w.cells_cap);
+        vx_launch<k_col_zero_cells, k_col_zero_cells_body>(L, grid, VX_THREADS, 0, S, w.cell_cnt);
+        vx_launch<k_col_count, k_col_count_body>(L, grid, VX_THREADS, 0, v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app, w.first_app);
+        vx_launch<k_cell_chunk_sum, k_cell_chunk_sum_body>(L, grid, VX_THREADS, 0, S, w.cell_cnt, w.cell_chunk_cnt);
+        vx_launch<k_cell_chunk_scan, k_cell_chunk_scan_body>(L, 1, 1024, 0, S, w.cell_chunk_cnt, w.cell_chunk_off);
+        vx_launch<k_cell_chunk_apply, k_cell_chunk_apply_body>(L, grid, VX_THREADS, 0, S, w.cell_cnt, w.cell_chunk_off, w.cell_start);
+        vx_launch<k_col_scatter, k_col_scatter_body>(L, grid, VX_THREADS, 0, S, w.cellid, w.cell_start, w.cell_cnt, w.sorted);
         if (pass == 1)
-            vx_launch_pdl(k_col_query<1>, grid, VX_THREADS, 0, L.stream, p, v, S, w.cellid, w.cell_start, w.sorted,
-                                                              w.col, w.in_cnt, w.cand);
+            vx_launch<k_col_query<1>, k_col_query_body<1>>(L, grid, VX_THREADS, 0, p, v, S, w.cellid, w.cell_start, w.sorted, w.col, w.in_cnt, w.cand);
         else
-            vx_launch_pdl(k_col_query<2>, grid, VX_THREADS, 0, L.stream, p, v, S, w.cellid, w.cell_start, w.sorted,
-                                                              w.col, w.in_cnt, w.cand);
-        VX_COUNT(L);
-        vx_launch_pdl(k_col_resolve, 1, 1024, 0, L.stream, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app,
-                                                w.cstate, w.cdec); VX_COUNT(L);
+            vx_launch<k_col_query<2>, k_col_query_body<2>>(L, grid, VX_THREADS, 0, p, v, S, w.cellid, w.cell_start, w.sorted, w.col, w.in_cnt, w.cand);
+
+        vx_launch<k_col_resolve, k_col_resolve_body>(L, 1, 1024, 0, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec);
         if (pass == 1)
-            vx_launch_pdl(k_col_merge<1>, grid, VX_THREADS, 0, L.stream, v, S, w.cand, w.col, w.cstate, w.first_app,
-                                                              w.mx, w.my, w.mg);
+            vx_launch<k_col_merge<1>, k_col_merge_body<1>>(L, grid, VX_THREADS, 0, v, S, w.cand, w.col, w.cstate, w.first_app, w.mx, w.my, w.mg);
         else
-            vx_launch_pdl(k_col_merge<2>, grid, VX_THREADS, 0, L.stream, v, S, w.cand, w.col, w.cstate, w.first_app,
-                                                              w.mx, w.my, w.mg);
-        VX_COUNT(L);
-        vx_launch_pdl(k_col_apply, grid, VX_THREADS, 0, L.stream, v, S, w.cand, w.col, w.cstate, w.mx, w.my, w.mg);
-        VX_COUNT(L);
+            vx_launch<k_col_merge<2>, k_col_merge_body<2>>(L, grid, VX_THREADS, 0, v, S, w.cand, w.col, w.cstate, w.first_app, w.mx, w.my, w.mg);
+
+        vx_launch<k_col_apply, k_col_apply_body>(L, grid, VX_THREADS, 0, v, S, w.cand, w.col, w.cstate, w.mx, w.my, w.mg);
+
         vx_launch_compact_skip(L, p, v, S, w, &S->col_done);
-        vx_launch_pdl(k_col_end, 1, 1, 0, L.stream, S); VX_COUNT(L);
+        vx_launch<k_col_end, k_col_end_body>(L, 1, 1, 0, S);
     }
     return cudaGetLastError();
 }

@@ -22,13 +22,12 @@ __device__ __forceinline__ bool vx_live(const VxView &v, long long p, double eps
     return fabs(v.g[p * v.ps]) >= eps;
 }
 
-__global__ void k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt, const int *skip) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cmp_count_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, double eps, int *cnt, const int *skip) {
     if (skip && *skip) return;
     __shared__ int sh[VX_THREADS];
     const long long n0 = S->n;
     const long long nch = vx_ceil_div(n0, VX_CHUNK);
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    for (long long c = vb.x; c < nch; c += vb.n) {
         int k = 0;
         const long long b = c * VX_CHUNK, e = min(n0, b + VX_CHUNK);
         for (long long p = b + threadIdx.x; p < e; p += blockDim.x) k += vx_live(v, p, eps);
@@ -42,11 +41,14 @@ __global__ void k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt, const 
         __syncthreads();
     }
 }
+__global__ void k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt, const int *skip) {
+    VX_PDL_WAIT();
+    k_cmp_count_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, eps, cnt, skip);
+}
 
 // Single block: exclusive scan of the chunk counts, m, scan[m] and H.
-__global__ void k_cmp_scan(VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
-                           const int *skip) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cmp_scan_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
+                             const int *skip) {
     if (skip && *skip) return;
     __shared__ long long sh[1024];
     __shared__ long long carry;
@@ -93,21 +95,25 @@ __global__ void k_cmp_scan(VxView v, VxScalars *S, double eps, const int *cnt, l
         S->c_H = m - scan_m;
     }
 }
+__global__ void k_cmp_scan(VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
+                           const int *skip) {
+    VX_PDL_WAIT();
+    k_cmp_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, eps, cnt, off, skip);
+}
 
 // Per chunk: local scan, then hole positions, hole sources and tail sources.
 // tail_src < 0 encodes "the position of hole -(value+1)".
-__global__ void __launch_bounds__(VX_THREADS) k_cmp_classify(VxView v, const VxScalars *S, double eps,
-                                                             const long long *off, int *hole_pos,
-                                                             int *hole_src, int *tail_src,
-                                                             const int *skip) {
-    VX_PDL_WAIT();
+VX_DEVK void k_cmp_classify_body(VxBlkB<VX_THREADS, 0> vb, VxView v, const VxScalars *S, double eps,
+                                 const long long *off, int *hole_pos,
+                                 int *hole_src, int *tail_src,
+                                 const int *skip) {
     if (skip && *skip) return;
     constexpr int PER = VX_CHUNK / VX_THREADS;
     __shared__ int sh[VX_THREADS];
     const long long n0 = S->c_n0, m = S->c_m, H = S->c_H, scan_m = S->c_scan_m;
     if (m == n0) return;
     const long long nch = vx_ceil_div(n0, VX_CHUNK);
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    for (long long c = vb.x; c < nch; c += vb.n) {
         const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
         bool lv[PER];
         int loc = 0;
@@ -149,17 +155,23 @@ __global__ void __launch_bounds__(VX_THREADS) k_cmp_classify(VxView v, const VxS
         }
     }
 }
-
-__global__ void k_cmp_gather(VxView v, const VxScalars *S, const int *hole_pos, const int *hole_src,
-                             const int *tail_src, double *hx, double *hy, double *hg, double *tx,
-                             double *ty, const int *skip) {
+__global__ void __launch_bounds__(VX_THREADS) k_cmp_classify(VxView v, const VxScalars *S, double eps,
+                                                             const long long *off, int *hole_pos,
+                                                             int *hole_src, int *tail_src,
+                                                             const int *skip) {
     VX_PDL_WAIT();
+    k_cmp_classify_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, v, S, eps, off, hole_pos, hole_src, tail_src, skip);
+}
+
+VX_DEVK void k_cmp_gather_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *hole_pos, const int *hole_src,
+                               const int *tail_src, double *hx, double *hy, double *hg, double *tx,
+                               double *ty, const int *skip) {
     if (skip && *skip) return;
     const long long n0 = S->c_n0, m = S->c_m, H = S->c_H;
     if (m == n0) return;
     const long long T = n0 - m;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < H + T;
-         k += (long long)gridDim.x * blockDim.x) {
+    for (long long k = vb.x * (long long)blockDim.x + threadIdx.x; k < H + T;
+         k += (long long)vb.n * blockDim.x) {
         if (k < H) {
             const long long s = (long long)hole_src[k] * v.ps;
             hx[k] = v.x[s]; hy[k] = v.y[s]; hg[k] = v.g[s];
@@ -172,17 +184,22 @@ __global__ void k_cmp_gather(VxView v, const VxScalars *S, const int *hole_pos, 
         }
     }
 }
-
-__global__ void k_cmp_scatter(VxView v, VxScalars *S, const int *hole_pos, const double *hx,
-                              const double *hy, const double *hg, const double *tx, const double *ty,
-                              const int *skip) {
+__global__ void k_cmp_gather(VxView v, const VxScalars *S, const int *hole_pos, const int *hole_src,
+                             const int *tail_src, double *hx, double *hy, double *hg, double *tx,
+                             double *ty, const int *skip) {
     VX_PDL_WAIT();
+    k_cmp_gather_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, hole_pos, hole_src, tail_src, hx, hy, hg, tx, ty, skip);
+}
+
+VX_DEVK void k_cmp_scatter_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const int *hole_pos, const double *hx,
+                                const double *hy, const double *hg, const double *tx, const double *ty,
+                                const int *skip) {
     if (skip && *skip) return;
     const long long n0 = S->c_n0, m = S->c_m, H = S->c_H;
     if (m != n0) {
         const long long T = n0 - m;
-        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < H + T;
-             k += (long long)gridDim.x * blockDim.x) {
+        for (long long k = vb.x * (long long)blockDim.x + threadIdx.x; k < H + T;
+             k += (long long)vb.n * blockDim.x) {
             if (k < H) {
                 const long long d = (long long)hole_pos[k] * v.ps;
                 v.x[d] = hx[k]; v.y[d] = hy[k]; v.g[d] = hg[k];
@@ -193,21 +210,24 @@ __global__ void k_cmp_scatter(VxView v, VxScalars *S, const int *hole_pos, const
             }
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->n = m;
+    if (vb.x == 0 && threadIdx.x == 0) S->n = m;
+}
+__global__ void k_cmp_scatter(VxView v, VxScalars *S, const int *hole_pos, const double *hx,
+                              const double *hy, const double *hg, const double *tx, const double *ty,
+                              const int *skip) {
+    VX_PDL_WAIT();
+    k_cmp_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, hole_pos, hx, hy, hg, tx, ty, skip);
 }
 
 cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const VxView &v,
                                    VxScalars *S, VxWork &w, const int *skip) {
     const int grid = L.num_sms * 4;
-    vx_launch_pdl(k_cmp_count, grid, VX_THREADS, 0, L.stream, v, S, p.drop_eps, w.cmp_cnt, skip); VX_COUNT(L);
-    vx_launch_pdl(k_cmp_scan, 1, 1024, 0, L.stream, v, S, p.drop_eps, w.cmp_cnt, w.cmp_off, skip); VX_COUNT(L);
-    vx_launch_pdl(k_cmp_classify, grid, VX_THREADS, 0, L.stream, v, S, p.drop_eps, w.cmp_off, w.hole_pos,
-                                                      w.hole_src, w.tail_src, skip); VX_COUNT(L);
-    vx_launch_pdl(k_cmp_gather, grid, VX_THREADS, 0, L.stream, v, S, w.hole_pos, w.hole_src, w.tail_src,
-                                                    w.hx, w.hy, w.hg, w.tx, w.ty, skip); VX_COUNT(L);
-    vx_launch_pdl(k_cmp_scatter, grid, VX_THREADS, 0, L.stream, v, S, w.hole_pos, w.hx, w.hy, w.hg, w.tx, w.ty,
-                                                     skip);
-    VX_COUNT(L);
+    vx_launch<k_cmp_count, k_cmp_count_body>(L, grid, VX_THREADS, 0, v, S, p.drop_eps, w.cmp_cnt, skip);
+    vx_launch<k_cmp_scan, k_cmp_scan_body>(L, 1, 1024, 0, v, S, p.drop_eps, w.cmp_cnt, w.cmp_off, skip);
+    vx_launch<k_cmp_classify, k_cmp_classify_body>(L, grid, VX_THREADS, 0, v, S, p.drop_eps, w.cmp_off, w.hole_pos, w.hole_src, w.tail_src, skip);
+    vx_launch<k_cmp_gather, k_cmp_gather_body>(L, grid, VX_THREADS, 0, v, S, w.hole_pos, w.hole_src, w.tail_src, w.hx, w.hy, w.hg, w.tx, w.ty, skip);
+    vx_launch<k_cmp_scatter, k_cmp_scatter_body>(L, grid, VX_THREADS, 0, v, S, w.hole_pos, w.hx, w.hy, w.hg, w.tx, w.ty, skip);
+
     return cudaGetLastError();
 }
 

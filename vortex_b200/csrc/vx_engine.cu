@@ -1133,10 +1133,13 @@ extern "C" vx_status vx_set_fmm(vx_sim *s, int fmm, int leaf) {
 // The stream the handle launches on (for callers that time with events).
 extern "C" void *vx_get_stream(vx_sim *s) { return s ? (void *)s->stream : nullptr; }
 
-__global__ void k_points_begin(VxScalars *S, long long n) {
-    VX_PDL_WAIT();
+VX_DEVK void k_points_begin_body(VxBlkB<0, 0> vb, VxScalars *S, long long n) {
     S->n = n;
     S->n0 = n;   // no point counts as born this step: no force terms
+}
+__global__ void k_points_begin(VxScalars *S, long long n) {
+    VX_PDL_WAIT();
+    k_points_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, n);
 }
 
 // Passive points (tracers) moved one time step with the given velocities by

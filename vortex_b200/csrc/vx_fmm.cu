@@ -58,21 +58,23 @@ __constant__ double c_fmm_inv[FMM_P + 1] = {0.0,      1.0,      1.0 / 2,  1.0 / 
 static_assert(FMM_P == 16, "reciprocal table length");
 
 // ---------------------------------------------------------------------------
-__global__ void k_fmm_begin(VxScalars *S) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_begin_body(VxBlkB<0, 0> vb, VxScalars *S) {
     S->fb[0] = S->fb[1] = S->fb[2] = S->fb[3] = ~0ull;
     S->fnflag = 0;
     S->fnbrute = 0;
     S->bk_nmid = S->bk_nbig = 0;
 }
-
-__global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
+__global__ void k_fmm_begin(VxScalars *S) {
     VX_PDL_WAIT();
+    k_fmm_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
+}
+
+VX_DEVK void k_fmm_bbox_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S) {
     __shared__ unsigned long long sk[4][FMM_T];
     const long long n = S->n;
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         const double x = v.x[i * v.ps], y = v.y[i * v.ps];
         k[0] = min(k[0], vx_dkey(x)); k[1] = min(k[1], vx_dkey(-x));
         k[2] = min(k[2], vx_dkey(y)); k[3] = min(k[3], vx_dkey(-y));
@@ -87,11 +89,14 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) atomicMin(&S->fb[q], sk[q][0]);
 }
+__global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
+    VX_PDL_WAIT();
+    k_fmm_bbox_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, v, S);
+}
 
 // Square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], reduced until
 // the leaf side is at least eps.
-__global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_params_body(VxBlkB<0, 0> vb, VxScalars *S, double eps, int Lmax, int leaf) {
     const long long n = S->n;
     const double x0 = vx_dunkey(S->fb[0]), x1 = -vx_dunkey(S->fb[1]);
     const double y0 = vx_dunkey(S->fb[2]), y1 = -vx_dunkey(S->fb[3]);
@@ -110,13 +115,20 @@ __global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
     S->fnleaves = 1LL << (2 * L);
     S->fs = vx_round32(n);   // sources include the round-32 padding (3-nearest)
 }
+__global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
+    VX_PDL_WAIT();
+    k_fmm_params_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, eps, Lmax, leaf);
+}
 
+VX_DEVK void k_fmm_zero_cnt_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt) {
+    const long long tot = fmm_level_off(S->fL + 1);
+    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < tot;
+         c += (long long)vb.n * blockDim.x)
+        cnt[c] = 0;
+}
 __global__ void k_fmm_zero_cnt(const VxScalars *S, int *cnt) {
     VX_PDL_WAIT();
-    const long long tot = fmm_level_off(S->fL + 1);
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < tot;
-         c += (long long)gridDim.x * blockDim.x)
-        cnt[c] = 0;
+    k_fmm_zero_cnt_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt);
 }
 
 __device__ __forceinline__ long long fmm_leaf(const VxScalars *S, double x, double y) {
@@ -129,26 +141,28 @@ __device__ __forceinline__ long long fmm_leaf(const VxScalars *S, double x, doub
 }
 
 // Leaf of every source slot [0, s); counts at the leaf level.
-__global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_leafid_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
     const long long s = S->fs;
     int *leafcnt = cnt + fmm_level_off(S->fL);
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < s;
-         j += (long long)gridDim.x * blockDim.x) {
+    for (long long j = vb.x * (long long)blockDim.x + threadIdx.x; j < s;
+         j += (long long)vb.n * blockDim.x) {
         const long long c = fmm_leaf(S, v.x[j * v.ps], v.y[j * v.ps]);
         key[j] = (unsigned)c;
         val[j] = (int)j;
         atomicAdd(&leafcnt[c], 1);
     }
 }
+__global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
+    VX_PDL_WAIT();
+    k_fmm_leafid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, key, val, cnt);
+}
 
 // Leaf starts: exclusive scan of the leaf counts (chunked, device length).
-__global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, const int *cnt, int *csum) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_scan_sum_body(VxBlkB<FMM_T, 0> vb, const VxScalars *S, const int *cnt, int *csum) {
     __shared__ int sh[FMM_T];
     const long long len = S->fnleaves, nch = vx_ceil_div(len, VX_CHUNK);
     const int *c0 = cnt + fmm_level_off(S->fL);
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    for (long long c = vb.x; c < nch; c += vb.n) {
         int k = 0;
         for (long long q = c * VX_CHUNK + threadIdx.x; q < min(len, (c + 1) * VX_CHUNK); q += blockDim.x) k += c0[q];
         sh[threadIdx.x] = k;
@@ -161,9 +175,12 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, cons
         __syncthreads();
     }
 }
-
-__global__ void k_fmm_scan_top(const VxScalars *S, const int *csum, long long *coff) {
+__global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, const int *cnt, int *csum) {
     VX_PDL_WAIT();
+    k_fmm_scan_sum_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, S, cnt, csum);
+}
+
+VX_DEVK void k_fmm_scan_top_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
     __shared__ long long sh[1024];
     __shared__ long long carry;
     const long long nch = vx_ceil_div(S->fnleaves, VX_CHUNK);
@@ -186,16 +203,19 @@ __global__ void k_fmm_scan_top(const VxScalars *S, const int *csum, long long *c
         __syncthreads();
     }
 }
-
-__global__ void __launch_bounds__(FMM_T) k_fmm_scan_apply(const VxScalars *S, const int *cnt, const long long *coff,
-                                                          int *start) {
+__global__ void k_fmm_scan_top(const VxScalars *S, const int *csum, long long *coff) {
     VX_PDL_WAIT();
+    k_fmm_scan_top_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
+}
+
+VX_DEVK void k_fmm_scan_apply_body(VxBlkB<FMM_T, 0> vb, const VxScalars *S, const int *cnt, const long long *coff,
+                                   int *start) {
     constexpr int PER = VX_CHUNK / FMM_T;
     __shared__ int sh[FMM_T];
     const long long len = S->fnleaves, nch = vx_ceil_div(len, VX_CHUNK);
     const int *c0 = cnt + fmm_level_off(S->fL);
-    if (blockIdx.x == 0 && threadIdx.x == 0) start[len] = (int)S->fs;
-    for (long long c = blockIdx.x; c < nch; c += gridDim.x) {
+    if (vb.x == 0 && threadIdx.x == 0) start[len] = (int)S->fs;
+    for (long long c = vb.x; c < nch; c += vb.n) {
         const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
         int val[PER], loc = 0;
 #pragma unroll
@@ -217,16 +237,20 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_scan_apply(const VxScalars *S, co
         }
     }
 }
+__global__ void __launch_bounds__(FMM_T) k_fmm_scan_apply(const VxScalars *S, const int *cnt, const long long *coff,
+                                                          int *start) {
+    VX_PDL_WAIT();
+    k_fmm_scan_apply_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, S, cnt, coff, start);
+}
 
 // Leaf-sorted sources: position relative to the leaf centre (FP32 keeps the
 // local spacing accurate), G masked beyond n, leaf column.
-__global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_gather_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
     const long long s = S->fs, n = S->n;
     const unsigned m = 1u << S->fL;
     const double h = S->fside / (double)m;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < s;
-         k += (long long)gridDim.x * blockDim.x) {
+    for (long long k = vb.x * (long long)blockDim.x + threadIdx.x; k < s;
+         k += (long long)vb.n * blockDim.x) {
         const long long j = sorted[k];
         const unsigned col = skey[k] % m, row = skey[k] / m;
         const double ccx = S->fx0 + ((double)col + 0.5) * h, ccy = S->fy0 + ((double)row + 0.5) * h;
@@ -234,20 +258,23 @@ __global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, co
                              j < n ? (float)v.g[j * v.ps] : 0.0f, (float)col);
     }
 }
+__global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
+    VX_PDL_WAIT();
+    k_fmm_gather_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, sorted, skey, srt);
+}
 
 // P2M at the leaves, one warp per leaf: each lane expands its own vortices
 // (FP64 positions), then a fixed butterfly sums the lanes.  Empty leaves are
 // not written (nothing reads their expansion).
-__global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const int *sorted,
-                                                 cplx *M) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_p2m_body(VxBlkB<128, 0> vb, VxView v, const VxScalars *S, const int *start, const int *sorted,
+                            cplx *M) {
     const int L = S->fL;
     const long long m = 1LL << L, nl = m * m, n = S->n;
     const double h = S->fside / (double)m;
     cplx *ML = M + fmm_level_off(L) * FMM_P;
     const int lane = threadIdx.x & 31;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nl; c += nw) {
+    const long long nw = ((long long)vb.n * blockDim.x) >> 5;
+    for (long long c = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5; c < nl; c += nw) {
         const int j0 = start[c], j1 = start[c + 1];
         if (j0 == j1) continue;
         cplx b[FMM_P];
@@ -286,6 +313,11 @@ __global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, c
         reinterpret_cast<double *>(ML + c * FMM_P)[lane] = vv[0];
     }
 }
+__global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const int *sorted,
+                                                 cplx *M) {
+    VX_PDL_WAIT();
+    k_fmm_p2m_body(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, v, S, start, sorted, M);
+}
 
 // Shift table shared by M2M and L2L, built per block in shared memory:
 // E[q][p] = d_q^p / p! for the child offsets d_q = (+-1 +- i)/4 (in units of
@@ -302,8 +334,7 @@ __device__ __forceinline__ void fmm_shift_table(cplx (*se)[FMM_P]) {
 // M2M: parent at level l from its 4 children at level l+1, one thread per
 // (parent, coefficient k); the thread of coefficient 0 also writes the
 // parent's vortex count (the sum of its children's).
-__global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, cplx *M, int l) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_m2m_body(VxBlkB<128, 0> vb, const VxScalars *S, int *cnt, cplx *M, int l) {
     __shared__ cplx se[4][FMM_P];
     if (l + 1 > S->fL) return;
     fmm_shift_table(se);
@@ -314,8 +345,8 @@ __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, c
     int *cp = cnt + fmm_level_off(l);
     const int *cc = cnt + fmm_level_off(l + 1);
     const long long tot = m * m * FMM_P;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
-         e += (long long)gridDim.x * blockDim.x) {
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)vb.n * blockDim.x) {
         const long long c = e / FMM_P;
         const int k = (int)(e % FMM_P);
         const long long ix = c % m, iy = c / m;
@@ -336,6 +367,10 @@ __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, c
         }
         Mp[e] = b;
     }
+}
+__global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, cplx *M, int l) {
+    VX_PDL_WAIT();
+    k_fmm_m2m_body(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, S, cnt, M, l);
 }
 
 // M2L at level l (2 <= l <= L) plus L2L from level l-1.  A block takes a
@@ -465,9 +500,8 @@ __device__ __forceinline__ cplx l2l_term(const cplx *Lp, const cplx (*se)[FMM_P]
     return cscale(acc, ldexp(1.0, -lc));
 }
 
-__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
-                                                       cplx *Loc, int l) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_m2l_l2l_body(VxBlkB<M2L_T, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
+                                cplx *Loc, int l) {
     __shared__ M2LShared T;
     if (l > S->fL) return;
     m2l_tables(T);
@@ -476,7 +510,7 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
     cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
     const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
     const int lc = threadIdx.x % FMM_P;   // = 4 cg + pt
-    for (long long t = blockIdx.x; t < tiles1 * tiles1; t += gridDim.x) {
+    for (long long t = vb.x; t < tiles1 * tiles1; t += vb.n) {
         long long c;
         bool busy;
         cplx a;
@@ -485,12 +519,16 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const
         Ll[c * FMM_P + lc] = a;
     }
 }
+__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
+                                                       cplx *Loc, int l) {
+    VX_PDL_WAIT();
+    k_fmm_m2l_l2l_body(VxBlkB<M2L_T, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc, l);
+}
 
 // M2L (without L2L) of levels 2 .. min(M2L_SMALL, L): blocks over the tiles
 // of all of them.
-__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
-                                                         cplx *Loc) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_m2l_small_body(VxBlkB<M2L_T, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
+                                  cplx *Loc) {
     __shared__ M2LShared T;
     const int hi = min(S->fL, M2L_SMALL);
     if (hi < 2) return;
@@ -498,7 +536,7 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, con
     long long total = 0;
     for (int l = 2; l <= hi; ++l) total += vx_ceil_div(1LL << (2 * l), (long long)(M2L_TILE * M2L_TILE));
     const int lc = threadIdx.x % FMM_P;
-    for (long long b = blockIdx.x; b < total; b += gridDim.x) {
+    for (long long b = vb.x; b < total; b += vb.n) {
         int l = 2;
         long long t = b;
         while (t >= vx_ceil_div(1LL << (2 * l), (long long)(M2L_TILE * M2L_TILE))) {
@@ -512,11 +550,15 @@ __global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, con
         Loc[(fmm_level_off(l) + c) * FMM_P + lc] = a;
     }
 }
+__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
+                                                         cplx *Loc) {
+    VX_PDL_WAIT();
+    k_fmm_m2l_small_body(VxBlkB<M2L_T, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc);
+}
 
 // L2L into level l (3 <= l <= min(M2L_SMALL, L)) from level l-1, one thread
 // per (cell, coefficient); one launch per level.
-__global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const int *cnt, cplx *Loc, int l) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_l2l_small_body(VxBlkB<256, 0> vb, const VxScalars *S, const int *cnt, cplx *Loc, int l) {
     __shared__ cplx se[4][FMM_P];
     if (l > min(S->fL, M2L_SMALL)) return;
     fmm_shift_table(se);
@@ -525,12 +567,16 @@ __global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const
     const int *cl = cnt + fmm_level_off(l);
     cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
     const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m * m * FMM_P;
-         e += (long long)gridDim.x * blockDim.x) {
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < m * m * FMM_P;
+         e += (long long)vb.n * blockDim.x) {
         const long long c = e / FMM_P;
         const int lc = (int)(e % FMM_P);
         if (cl[c] > 0) Ll[e] = cadd(Ll[e], l2l_term(Lp, se, m, c % m, c / m, lc));
     }
+}
+__global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const int *cnt, cplx *Loc, int l) {
+    VX_PDL_WAIT();
+    k_fmm_l2l_small_body(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, S, cnt, Loc, l);
 }
 
 // Near field (FP32, core smoothing, 3 nearest) + far field (L2P, FP64): one
@@ -568,10 +614,9 @@ __device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gsl
 #ifndef VX_NEAR_MINB
 #define VX_NEAR_MINB 1   // minimum resident blocks per SM requested for k_fmm_near
 #endif
-__global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
-                                                   const int *sorted, const int *start, const int2 *items,
-                                                   const cplx *Loc, int *flag_list) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                             const int *sorted, const int *start, const int2 *items,
+                             const cplx *Loc, int *flag_list) {
     __shared__ float4 sxy[FMM_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
     __shared__ float2 sg[FMM_T / 2];    // (G_a, G_b)
     const int lane = threadIdx.x & 31;
@@ -586,7 +631,7 @@ __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, Vx
     const long long nitems = S->cnitems;
     const cplx *LL = Loc + fmm_level_off(L) * FMM_P;
     const long long wpb = FMM_T / 32;
-    for (long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < nitems; it += gridDim.x * wpb) {
+    for (long long it = vb.x * wpb + (threadIdx.x >> 5); it < nitems; it += vb.n * wpb) {
         const int2 item = items[it];
         const long long leaf = item.x;
         const long long row = leaf / m, col = leaf % m;
@@ -688,6 +733,12 @@ __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, Vx
         }
     }
 }
+__global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
+                                                   const int *sorted, const int *start, const int2 *items,
+                                                   const cplx *Loc, int *flag_list) {
+    VX_PDL_WAIT();
+    k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB>{blockIdx.x, gridDim.x}, p, v, S, srt, sorted, start, items, Loc, flag_list);
+}
 
 // Targets whose third-nearest distance reached the leaf side: exact 3
 // nearest by a ring search over the leaves (one warp per target).  Ring k
@@ -713,15 +764,14 @@ __device__ __forceinline__ void fmm_ring_cell(int k, int q, int &dx, int &dy) {
     dx = k; dy = q - k + 1;
 }
 
-__global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const int *sorted,
-                              const int *start, const int *flag_list, int *brute_list) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_nn3_fix_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const float4 *srt, const int *sorted,
+                                const int *start, const int *flag_list, int *brute_list) {
     const int nf = S->fnflag;
     const long long m = 1LL << S->fL;
     const double h = S->fside / (double)m;
     const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < nf; f += warps) {
+    const int warps = (vb.n * blockDim.x) >> 5;
+    for (int f = (vb.x * blockDim.x + threadIdx.x) >> 5; f < nf; f += warps) {
         const long long t = flag_list[f];
         const long long i = sorted[t];
         const long long leaf = fmm_leaf(S, v.x[i * v.ps], v.y[i * v.ps]);
@@ -767,18 +817,22 @@ __global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const i
         }
     }
 }
+__global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const int *sorted,
+                              const int *start, const int *flag_list, int *brute_list) {
+    VX_PDL_WAIT();
+    k_fmm_nn3_fix_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, srt, sorted, start, flag_list, brute_list);
+}
 
 // The 3 nearest of the targets the ring search left (original indices in
 // brute_list) over every source slot [0, fs): one block per target, each
 // thread keeping the three smallest of its stride, merged over the warp and
 // the block (the same set of sources as the ring search, so the same three).
-__global__ void __launch_bounds__(256) k_fmm_nn3_brute(VxView v, const VxScalars *S, const int *brute_list) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_nn3_brute_body(VxBlkB<256, 0> vb, VxView v, const VxScalars *S, const int *brute_list) {
     __shared__ float sd[3][256 / 32];
     const int nb = S->fnbrute;
     const long long fs = S->fs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int b = blockIdx.x; b < nb; b += gridDim.x) {
+    for (int b = vb.x; b < nb; b += vb.n) {
         const long long i = brute_list[b];
         const double xi = v.x[i * v.ps], yi = v.y[i * v.ps];
         float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
@@ -808,25 +862,31 @@ __global__ void __launch_bounds__(256) k_fmm_nn3_brute(VxView v, const VxScalars
         __syncthreads();
     }
 }
+__global__ void __launch_bounds__(256) k_fmm_nn3_brute(VxView v, const VxScalars *S, const int *brute_list) {
+    VX_PDL_WAIT();
+    k_fmm_nn3_brute_body(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, v, S, brute_list);
+}
 
 // Row items over the leaf grid (m x m), as for the neighbour-list grid.
 // Near-field work items: every leaf's targets in chunks of FMM_W, counted per
 // leaf row (one warp per row, lanes over its leaves).
-__global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_items) {
-    VX_PDL_WAIT();
+VX_DEVK void k_fmm_row_items_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, int *row_items) {
     const long long m = 1LL << S->fL;
     const int lane = threadIdx.x & 31;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    const long long nw = ((long long)vb.n * blockDim.x) >> 5;
+    for (long long r = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
         int k = 0;
         for (long long c = r * m + lane; c < (r + 1) * m; c += 32) k += (start[c + 1] - start[c] + FMM_W - 1) / FMM_W;
         for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
         if (lane == 0) row_items[r] = k;
     }
 }
-
-__global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
+__global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_items) {
     VX_PDL_WAIT();
+    k_fmm_row_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items);
+}
+
+VX_DEVK void k_fmm_row_scan_body(VxBlkB<0, 0> vb, VxScalars *S, const int *in, long long *out, long long items_cap) {
     __shared__ long long sh[1024];
     const long long len = 1LL << S->fL;
     const long long per = vx_ceil_div(len, (long long)blockDim.x);
@@ -849,14 +909,17 @@ __global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long
         S->cnitems = run <= items_cap ? run : items_cap;
     }
 }
-
-__global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row_items, const long long *off,
-                            int2 *items, long long items_cap) {
+__global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
     VX_PDL_WAIT();
+    k_fmm_row_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, in, out, items_cap);
+}
+
+VX_DEVK void k_fmm_items_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, const int *row_items, const long long *off,
+                              int2 *items, long long items_cap) {
     const long long m = 1LL << S->fL;
     const int lane = threadIdx.x & 31;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    const long long nw = ((long long)vb.n * blockDim.x) >> 5;
+    for (long long r = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
         long long o = off[r];
         for (long long c0 = r * m; c0 < (r + 1) * m; c0 += 32) {
             const long long c = c0 + lane;
@@ -874,6 +937,11 @@ __global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row
         }
     }
 }
+__global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row_items, const long long *off,
+                            int2 *items, long long items_cap) {
+    VX_PDL_WAIT();
+    k_fmm_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items, off, items, items_cap);
+}
 
 long long vx_fmm_cells(int lmax) { return fmm_level_off(lmax + 1); }
 
@@ -887,58 +955,56 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
                                    VxWork &w) {
     const int grid = L.num_sms * 4;
     const int Lmax = w.fmm_lmax;
-    vx_launch_pdl(k_fmm_begin, 1, 1, 0, L.stream, S); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_bbox, grid, FMM_T, 0, L.stream, v, S); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_params, 1, 1, 0, L.stream, S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_zero_cnt, grid, FMM_T, 0, L.stream, S, w.fmm_cnt); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_leafid, grid, FMM_T, 0, L.stream, v, S, w.key0, w.val0, w.fmm_cnt); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_scan_sum, grid, FMM_T, 0, L.stream, S, w.fmm_cnt, w.cell_chunk_cnt); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_scan_top, 1, 1024, 0, L.stream, S, w.cell_chunk_cnt, w.cell_chunk_off); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_scan_apply, grid, FMM_T, 0, L.stream, S, w.fmm_cnt, w.cell_chunk_off, w.fmm_start); VX_COUNT(L);
+    vx_launch<k_fmm_begin, k_fmm_begin_body>(L, 1, 1, 0, S);
+    vx_launch<k_fmm_bbox, k_fmm_bbox_body>(L, grid, FMM_T, 0, v, S);
+    vx_launch<k_fmm_params, k_fmm_params_body>(L, 1, 1, 0, S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32);
+    vx_launch<k_fmm_zero_cnt, k_fmm_zero_cnt_body>(L, grid, FMM_T, 0, S, w.fmm_cnt);
+    vx_launch<k_fmm_leafid, k_fmm_leafid_body>(L, grid, FMM_T, 0, v, S, w.key0, w.val0, w.fmm_cnt);
+    vx_launch<k_fmm_scan_sum, k_fmm_scan_sum_body>(L, grid, FMM_T, 0, S, w.fmm_cnt, w.cell_chunk_cnt);
+    vx_launch<k_fmm_scan_top, k_fmm_scan_top_body>(L, 1, 1024, 0, S, w.cell_chunk_cnt, w.cell_chunk_off);
+    vx_launch<k_fmm_scan_apply, k_fmm_scan_apply_body>(L, grid, FMM_T, 0, S, w.fmm_cnt, w.cell_chunk_off, w.fmm_start);
     // leaf order: each leaf's sources in index order (a stable sort by leaf)
     vx_bucket_order(L, S, &S->fs, &S->fnleaves, w.key0, w.fmm_start, w.fmm_cnt, &S->fcnt_off, w.key1, w.val1,
                     w.bk_mid, w.bk_big, w.val0);
     const unsigned *skey = w.key1;
     const int *sorted = w.val1;
-    vx_launch_pdl(k_fmm_gather, grid, FMM_T, 0, L.stream, v, S, sorted, skey, w.srt); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_p2m, grid * 4, 128, 0, L.stream, v, S, w.fmm_start, sorted, (cplx *)w.fmm_M); VX_COUNT(L);
+    vx_launch<k_fmm_gather, k_fmm_gather_body>(L, grid, FMM_T, 0, v, S, sorted, skey, w.srt);
+    vx_launch<k_fmm_p2m, k_fmm_p2m_body>(L, grid * 4, 128, 0, v, S, w.fmm_start, sorted, (cplx *)w.fmm_M);
     // the level loops cover the deepest level this capacity allows; kernels
     // of levels below the depth chosen on the device return at once
     for (int l = Lmax - 1; l >= 0; --l) {
         const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));
-        vx_launch_pdl(k_fmm_m2m, gm, 128, 0, L.stream, S, w.fmm_cnt, (cplx *)w.fmm_M, l); VX_COUNT(L);
+        vx_launch<k_fmm_m2m, k_fmm_m2m_body>(L, gm, 128, 0, S, w.fmm_cnt, (cplx *)w.fmm_M, l);
     }
     {
         long long tiles = 0;
         for (int l = 2; l <= std::min(Lmax, M2L_SMALL); ++l) tiles += vx_ceil_div(1LL << (2 * l), 16LL);
         if (tiles > 0) {
-            vx_launch_pdl(k_fmm_m2l_small, (int)std::min<long long>(grid * 2, tiles), M2L_T, 0, L.stream, 
-                S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L);
-            VX_COUNT(L);
+            vx_launch<k_fmm_m2l_small, k_fmm_m2l_small_body>(L, (int)std::min<long long>(grid * 2, tiles), M2L_T, 0, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L);
+
             for (int l = 3; l <= std::min(Lmax, M2L_SMALL); ++l) {
                 const int g = (int)std::min<long long>(grid, vx_ceil_div((1LL << (2 * l)) * FMM_P, 256));
-                vx_launch_pdl(k_fmm_l2l_small, g, 256, 0, L.stream, S, w.fmm_cnt, (cplx *)w.fmm_L, l); VX_COUNT(L);
+                vx_launch<k_fmm_l2l_small, k_fmm_l2l_small_body>(L, g, 256, 0, S, w.fmm_cnt, (cplx *)w.fmm_L, l);
             }
         }
     }
     for (int l = M2L_SMALL + 1; l <= Lmax; ++l) {
         const long long t1 = vx_ceil_div(1LL << l, (long long)M2L_TILE);
         const int g = (int)std::min<long long>(grid * 2, t1 * t1);
-        vx_launch_pdl(k_fmm_m2l_l2l, g, M2L_T, 0, L.stream, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
-        VX_COUNT(L);
+        vx_launch<k_fmm_m2l_l2l, k_fmm_m2l_l2l_body>(L, g, M2L_T, 0, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
+
     }
-    vx_launch_pdl(k_fmm_row_items, grid, FMM_T, 0, L.stream, S, w.fmm_start, w.row_items); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_row_scan, 1, 1024, 0, L.stream, S, w.row_items, w.row_item_off, w.items_cap); VX_COUNT(L);
-    vx_launch_pdl(k_fmm_items, grid, FMM_T, 0, L.stream, S, w.fmm_start, w.row_items, w.row_item_off, w.items, w.items_cap);
-    VX_COUNT(L);
+    vx_launch<k_fmm_row_items, k_fmm_row_items_body>(L, grid, FMM_T, 0, S, w.fmm_start, w.row_items);
+    vx_launch<k_fmm_row_scan, k_fmm_row_scan_body>(L, 1, 1024, 0, S, w.row_items, w.row_item_off, w.items_cap);
+    vx_launch<k_fmm_items, k_fmm_items_body>(L, grid, FMM_T, 0, S, w.fmm_start, w.row_items, w.row_item_off, w.items, w.items_cap);
+
     VX_EV(L, 0);
-    vx_launch_pdl(k_fmm_near, L.num_sms * 8, FMM_T, 0, L.stream, p, v, S, w.srt, sorted, w.fmm_start, w.items,
-                                                      (const cplx *)w.fmm_L, w.fmm_flags);
+    vx_launch<k_fmm_near, k_fmm_near_body>(L, L.num_sms * 8, FMM_T, 0, p, v, S, w.srt, sorted, w.fmm_start, w.items, (const cplx *)w.fmm_L, w.fmm_flags);
     VX_EV(L, 1);
-    VX_COUNT(L);
-    vx_launch_pdl(k_fmm_nn3_fix, grid, FMM_T, 0, L.stream, v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
-    VX_COUNT(L);
-    vx_launch_pdl(k_fmm_nn3_brute, grid, 256, 0, L.stream, v, S, w.fmm_brute);
-    VX_COUNT(L);
+
+    vx_launch<k_fmm_nn3_fix, k_fmm_nn3_fix_body>(L, grid, FMM_T, 0, v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
+
+    vx_launch<k_fmm_nn3_brute, k_fmm_nn3_brute_body>(L, grid, 256, 0, v, S, w.fmm_brute);
+
     return cudaGetLastError();
 }

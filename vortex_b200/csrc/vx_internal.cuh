@@ -13,6 +13,9 @@
 #include <utility>
 #include <stdint.h>
 #include <stdio.h>
+#include <string.h>
+
+#include <vector>
 
 #include "../../include/vortex_b200.h"
 
@@ -230,33 +233,13 @@ __device__ __forceinline__ double vx_dunkey(unsigned long long k) {
     return __longlong_as_double((long long)b);
 }
 
-// ---------------------------------------------------------------------------
-// Launch context: stream + launch counter shared by all stage launchers.
-struct VxLaunch {
-    cudaStream_t stream;
-    long long *launches;   // host counter (may be null)
-    // SMs the launch grids are sized for.  A step of a small body sizes them
-    // for a share of the GPU that follows its source count (grid-stride
-    // kernels: same results, fewer idle blocks, so the kernels of many
-    // small bodies on concurrent streams overlap); full_sms (0: num_sms)
-    // stays the device's count for the kernels whose work does not scale
-    // with the count (the all-pairs sums) or whose results depend on the
-    // grid (the birth far field's per-block partials).
-    int num_sms;
-    int full_sms = 0;
-    // optional events recorded around the Biot-Savart and diffusion pair
-    // kernels: [0,1] Biot-Savart, [2,3] diffusion (null: not recorded)
-    cudaEvent_t pair_ev[4] = {nullptr, nullptr, nullptr, nullptr};
-};
-inline int vx_full_sms(const VxLaunch &L) { return L.full_sms > 0 ? L.full_sms : L.num_sms; }
-#define VX_EV(L, k) do { if ((L).pair_ev[k]) cudaEventRecord((L).pair_ev[k], (L).stream); } while (0)
-
 // Programmatic dependent launch (sm_90+): a kernel launched by vx_launch_pdl
-// may be scheduled while its predecessor on the stream is still finishing,
-// which hides the launch gap between the many short kernels of a step.  Every
-// such kernel starts with VX_PDL_WAIT(), which returns once the predecessor
-// has completed and its writes are visible; nothing is read or written before
-// it.  (In a kernel launched the ordinary way the wait returns at once.)
+// or vx_launch may be scheduled while its predecessor on the stream is still
+// finishing, which hides the launch gap between the many short kernels of a
+// step.  Every such kernel starts with VX_PDL_WAIT(), which returns once the
+// predecessor has completed and its writes are visible; nothing is read or
+// written before it.  (In a kernel launched the ordinary way the wait returns
+// at once.)
 #define VX_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
 template <typename... K, typename... A>
 inline cudaError_t vx_launch_pdl(void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
@@ -274,6 +257,212 @@ inline cudaError_t vx_launch_pdl(void (*kernel)(K...), dim3 grid, dim3 block, si
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 #define VX_COUNT(L) do { if ((L).launches) ++*(L).launches; } while (0)
+
+// ---------------------------------------------------------------------------
+// Kernel bodies and the two ways they are launched.
+//
+// A step kernel is written as a device function `k_name_body(VxBlkB<T,B> vb,
+// args...)` that uses vb.x / vb.n where a kernel would use blockIdx.x /
+// gridDim.x (T, B: its launch bounds, 0 for none).  Two kernels run it:
+//  * `k_name(args...)`, the body's own __global__ wrapper (vb = blockIdx.x,
+//    gridDim.x): one body, arguments as kernel parameters;
+//  * `k_many<body>(slot)`: many bodies in one launch.  The slot (device
+//    memory) holds, per body, the first block of its range and its argument
+//    pack; block b of the launch finds its body by a binary search over the
+//    block ranges and runs the body with vb = (b - first, count).  Each body
+//    sees exactly the blocks and arguments it would see launched alone, so
+//    its results are the same.
+template <int MAXT, int MINB>
+struct VxBlkB {
+    unsigned x, n;   // block index within this body's launch, blocks of this body's launch
+};
+using VxBlk = VxBlkB<0, 0>;
+#define VX_DEVK __device__ __forceinline__
+
+// Argument pack: a plain nested struct (the same layout in host and device
+// code), built on the host and read on the device.
+template <typename... A>
+struct VxPack {};
+template <typename H, typename... T>
+struct VxPack<H, T...> {
+    H h;
+    VxPack<T...> t;
+};
+template <typename... A>
+struct VxPackMake;
+template <>
+struct VxPackMake<> {
+    static VxPack<> make() { return {}; }
+};
+template <typename H, typename... T>
+struct VxPackMake<H, T...> {
+    static VxPack<H, T...> make(const H &h, const T &...t) {
+        VxPack<H, T...> p;
+        p.h = h;
+        p.t = VxPackMake<T...>::make(t...);
+        return p;
+    }
+};
+template <auto DEV, typename BK, typename... Done>
+__device__ __forceinline__ void vx_apply(BK vb, const VxPack<> &, const Done &...d) {
+    DEV(vb, d...);
+}
+template <auto DEV, typename BK, typename H, typename... T, typename... Done>
+__device__ __forceinline__ void vx_apply(BK vb, const VxPack<H, T...> &p, const Done &...d) {
+    vx_apply<DEV>(vb, p.t, d..., p.h);
+}
+
+// One multi-body launch (device memory): nb bodies, body i owns blocks
+// [first[i], first[i+1]), its arguments at packs + i * stride.
+struct VxSlot {
+    int nb;
+    int pad;
+    long long stride;
+    const int *first;
+    const unsigned char *packs;
+};
+
+template <auto DEV, int MAXT, int MINB, typename... A>
+__device__ __forceinline__ void vx_many_body(const VxSlot *sd) {
+    VX_PDL_WAIT();
+    const int nb = sd->nb;
+    const int *first = sd->first;
+    const unsigned bid = blockIdx.x;
+    if (bid >= (unsigned)first[nb]) return;
+    int lo = 0, hi = nb;
+    while (hi - lo > 1) {
+        const int m = (lo + hi) >> 1;
+        if ((unsigned)first[m] <= bid) lo = m; else hi = m;
+    }
+    const VxBlkB<MAXT, MINB> vb{bid - (unsigned)first[lo], (unsigned)(first[lo + 1] - first[lo])};
+    const VxPack<A...> &p = *reinterpret_cast<const VxPack<A...> *>(sd->packs + (long long)lo * sd->stride);
+    vx_apply<DEV>(vb, p);
+}
+template <auto DEV, typename... A>
+__global__ void k_many(const VxSlot *sd) { vx_many_body<DEV, 0, 0, A...>(sd); }
+template <auto DEV, int MAXT, typename... A>
+__global__ void __launch_bounds__(MAXT) k_many_t(const VxSlot *sd) { vx_many_body<DEV, MAXT, 0, A...>(sd); }
+template <auto DEV, int MAXT, int MINB, typename... A>
+__global__ void __launch_bounds__(MAXT, MINB) k_many_tb(const VxSlot *sd) {
+    vx_many_body<DEV, MAXT, MINB, A...>(sd);
+}
+
+// A launch recorded instead of issued (building a multi-body step): the
+// single-body kernel (identity), its multi-body kernel, the shape and the
+// argument pack (bytes in the recorder's arena).
+struct VxRecLaunch {
+    const void *key;
+    const void *many;
+    dim3 grid, block;
+    size_t smem;
+    size_t off, size;
+};
+struct VxRecorder {
+    std::vector<VxRecLaunch> launches;
+    std::vector<unsigned char> arena;
+    void add(const void *key, const void *many, dim3 grid, dim3 block, size_t smem, const void *pack,
+             size_t size) {
+        const size_t off = (arena.size() + 15) / 16 * 16;
+        arena.resize(off + size);
+        memcpy(arena.data() + off, pack, size);
+        launches.push_back(VxRecLaunch{key, many, grid, block, smem, off, size});
+    }
+};
+
+// Per-kernel device times: events around every launch, read back by kernel
+// once the work has finished.
+struct VxKernelTimer {
+    struct Rec {
+        const void *key;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get() {
+        cudaEvent_t e = nullptr;
+        if (!pool.empty()) {
+            e = pool.back();
+            pool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Launch context: stream + launch counter shared by all stage launchers.
+struct VxLaunch {
+    cudaStream_t stream;
+    long long *launches;   // host counter (may be null)
+    // SMs the launch grids are sized for.  A step of a small body sizes them
+    // for a share of the GPU that follows its source count (grid-stride
+    // kernels: same results, fewer idle blocks, so the kernels of many
+    // small bodies on concurrent streams overlap); full_sms (0: num_sms)
+    // stays the device's count for the kernels whose work does not scale
+    // with the count (the all-pairs sums) or whose results depend on the
+    // grid (the birth far field's per-block partials).
+    int num_sms;
+    int full_sms = 0;
+    // optional events recorded around the Biot-Savart and diffusion pair
+    // kernels: [0,1] Biot-Savart, [2,3] diffusion (null: not recorded)
+    cudaEvent_t pair_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // recording instead of launching (multi-body steps), per-kernel timing
+    VxRecorder *rec = nullptr;
+    VxKernelTimer *kt = nullptr;
+};
+inline int vx_full_sms(const VxLaunch &L) { return L.full_sms > 0 ? L.full_sms : L.num_sms; }
+#define VX_EV(L, k) do { if ((L).pair_ev[k] && !(L).rec) cudaEventRecord((L).pair_ev[k], (L).stream); } while (0)
+
+// Launch kernel K (the __global__ wrapper of body DEV) for one body: with
+// programmatic dependent launch, or recorded into L.rec, or bracketed by
+// timing events into L.kt.
+template <auto K, auto DEV, typename SigD = decltype(DEV)>
+struct VxLauncher;
+template <auto K, auto DEV, int MAXT, int MINB, typename... A>
+struct VxLauncher<K, DEV, void (*)(VxBlkB<MAXT, MINB>, A...)> {
+    static const void *many() {
+        if constexpr (MAXT > 0 && MINB > 0) return (const void *)&k_many_tb<DEV, MAXT, MINB, A...>;
+        else if constexpr (MAXT > 0) return (const void *)&k_many_t<DEV, MAXT, A...>;
+        else return (const void *)&k_many<DEV, A...>;
+    }
+    template <typename... Args>
+    static cudaError_t go(const VxLaunch &L, dim3 grid, dim3 block, size_t smem, Args &&...args) {
+        if (L.launches) ++*L.launches;
+        if (L.rec) {
+            const VxPack<A...> p = VxPackMake<A...>::make(static_cast<A>(args)...);
+            L.rec->add((const void *)K, many(), grid, block, smem, &p, sizeof(p));
+            return cudaSuccess;
+        }
+        cudaEvent_t ea = nullptr, eb = nullptr;
+        if (L.kt) {
+            ea = L.kt->get();
+            eb = L.kt->get();
+            cudaEventRecord(ea, L.stream);
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = L.stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(&cfg, K, static_cast<A>(args)...);
+        if (L.kt) {
+            cudaEventRecord(eb, L.stream);
+            L.kt->recs.push_back(VxKernelTimer::Rec{(const void *)K, ea, eb});
+        }
+        return e;
+    }
+};
+template <auto K, auto DEV, typename... Args>
+inline cudaError_t vx_launch(const VxLaunch &L, dim3 grid, dim3 block, size_t smem, Args &&...args) {
+    return VxLauncher<K, DEV>::go(L, grid, block, smem, std::forward<Args>(args)...);
+}
+
 
 // Stage launchers (each returns the first CUDA error it saw).
 cudaError_t vx_launch_step_begin(const VxLaunch &L, VxScalars *S);
@@ -314,7 +503,6 @@ cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const V
                                    VxScalars *S, VxWork &w, const int *skip);
 void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams *p);
 void vx_set_error(const char *fmt, ...);
-#include <vector>
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
                         cudaStream_t stream = nullptr);
 long long vx_work_bytes(long long cap, int P32, int num_sms);

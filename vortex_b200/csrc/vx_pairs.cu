@@ -31,16 +31,19 @@ int vx_pick_ksplit(long long n_upper, int tile, int num_sms) {
 
 // ---------------------------------------------------------------------------
 // Packed FP32 sources for the bulk form: (x, y, G, 0), G masked to 0 beyond n.
-__global__ void k_pack32(VxView v, const VxScalars *S, float4 *src, long long upto) {
-    VX_PDL_WAIT();
+VX_DEVK void k_pack32_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, float4 *src, long long upto) {
     const long long n = S->n;
     const long long s = vx_round32(n);
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < s;
-         j += (long long)gridDim.x * blockDim.x) {
+    for (long long j = vb.x * (long long)blockDim.x + threadIdx.x; j < s;
+         j += (long long)vb.n * blockDim.x) {
         if (j >= upto) break;
         src[j] = make_float4((float)v.x[j * v.ps], (float)v.y[j * v.ps],
                              j < n ? (float)v.g[j * v.ps] : 0.0f, 0.0f);
     }
+}
+__global__ void k_pack32(VxView v, const VxScalars *S, float4 *src, long long upto) {
+    VX_PDL_WAIT();
+    k_pack32_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, src, upto);
 }
 
 template <typename T> struct PairMath;
@@ -76,11 +79,10 @@ __device__ __forceinline__ void load_src(SrcTile<T> &t, const VxView &v, const f
 // Biot-Savart (+ 3 nearest when NN3).  Targets: particles (nt < 0 -> n) or
 // probe points (tx/ty with stride tstr).  Partials: [sc][5][tstride].
 template <typename T, bool NN3>
-__global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const VxScalars *S,
-                                                   const float4 *src32, const double *tx,
-                                                   const double *ty, long long tstr, long long nt_in,
-                                                   double *part, long long tstride, int K) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bs_partial_body(VxBlkB<PT, 0> vb, VxParams p, VxView v, const VxScalars *S,
+                               const float4 *src32, const double *tx,
+                               const double *ty, long long tstr, long long nt_in,
+                               double *part, long long tstride, int K) {
     constexpr int TPT = pairs_tpt(sizeof(T) == 4);
     constexpr int NOUT = NN3 ? 5 : 2;
     __shared__ SrcTile<T> st;
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const V
     const long long cs = vx_ceil_div(vx_ceil_div(srange, K), PT) * PT;
     const long long items = tiles * K;
     const T eps2 = (T)p.eps2;
-    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    for (long long it = vb.x; it < items; it += vb.n) {
         const long long tt = it % tiles, sc = it / tiles;
         T ax[TPT], ay[TPT];
         long long ti[TPT];
@@ -150,6 +152,14 @@ __global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const V
         }
     }
 }
+template <typename T, bool NN3>
+__global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const VxScalars *S,
+                                                   const float4 *src32, const double *tx,
+                                                   const double *ty, long long tstr, long long nt_in,
+                                                   double *part, long long tstride, int K) {
+    VX_PDL_WAIT();
+    k_bs_partial_body<T, NN3>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, v, S, src32, tx, ty, tstr, nt_in, part, tstride, K);
+}
 
 // ---------------------------------------------------------------------------
 // Bulk-form Biot-Savart + 3 nearest, FP32.  Same decomposition as above, with
@@ -192,11 +202,10 @@ __device__ __forceinline__ void bs32_tile(const float4 *sm, int cnt, int jbase, 
 }
 
 template <bool NN3>
-__global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars *S, const float4 *src32,
-                                                     const double *tx, const double *ty, long long tstr,
-                                                     long long nt_in, double *part, long long tstride,
-                                                     int K) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bs32_partial_body(VxBlkB<PT, 0> vb, VxParams p, const VxScalars *S, const float4 *src32,
+                                 const double *tx, const double *ty, long long tstr,
+                                 long long nt_in, double *part, long long tstride,
+                                 int K) {
     constexpr int NOUT = NN3 ? 5 : 2;
     __shared__ float4 sm[PT];
     const long long n = S->n;
@@ -207,7 +216,7 @@ __global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars
     const long long cs = vx_ceil_div(vx_ceil_div(srange, K), PT) * PT;
     const long long items = tiles * K;
     const float eps2 = (float)p.eps2;
-    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    for (long long it = vb.x; it < items; it += vb.n) {
         const long long tt = it % tiles, sc = it / tiles;
         const long long tlo = tt * tile, thi = min(nt, tlo + tile);
         float ax[BS32_TPT], ay[BS32_TPT], d1[BS32_TPT], d2[BS32_TPT], d3[BS32_TPT];
@@ -259,15 +268,22 @@ __global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars
         }
     }
 }
+template <bool NN3>
+__global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars *S, const float4 *src32,
+                                                     const double *tx, const double *ty, long long tstr,
+                                                     long long nt_in, double *part, long long tstride,
+                                                     int K) {
+    VX_PDL_WAIT();
+    k_bs32_partial_body<NN3>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, S, src32, tx, ty, tstr, nt_in, part, tstride, K);
+}
 
 // Combine: V = sum/(2 pi) + V_inf, d = mean of the 3 nearest distances.
 template <bool FP32>
-__global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, long long tstride,
-                             int K) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bs_combine_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const double *part, long long tstride,
+                               int K) {
     const long long n = S->n;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         double sx = 0.0, sy = 0.0;
         double d1 = 1e5, d2 = 1e5, d3 = 1e5;
         for (int sc = 0; sc < K; ++sc) {
@@ -286,12 +302,17 @@ __global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, l
         v.vy[i * v.vs] = sy / VX_TWO_PI + S->vinf[1];
     }
 }
-
-__global__ void k_probe_combine(const VxScalars *S, const double *part, long long tstride, int K,
-                                long long np, double *ovx, double *ovy, long long ostride) {
+template <bool FP32>
+__global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, long long tstride,
+                             int K) {
     VX_PDL_WAIT();
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < np;
-         i += (long long)gridDim.x * blockDim.x) {
+    k_bs_combine_body<FP32>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, part, tstride, K);
+}
+
+VX_DEVK void k_probe_combine_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *part, long long tstride, int K,
+                                  long long np, double *ovx, double *ovy, long long ostride) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < np;
+         i += (long long)vb.n * blockDim.x) {
         double sx = 0.0, sy = 0.0;
         for (int sc = 0; sc < K; ++sc) {
             const double *o = part + (long long)sc * 2 * tstride + i;
@@ -301,6 +322,11 @@ __global__ void k_probe_combine(const VxScalars *S, const double *part, long lon
         ovx[i * ostride] = sx / VX_TWO_PI + S->vinf[0];
         ovy[i * ostride] = sy / VX_TWO_PI + S->vinf[1];
     }
+}
+__global__ void k_probe_combine(const VxScalars *S, const double *part, long long tstride, int K,
+                                long long np, double *ovx, double *ovy, long long ostride) {
+    VX_PDL_WAIT();
+    k_probe_combine_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, part, tstride, K, np, ovx, ovy, ostride);
 }
 
 // ---------------------------------------------------------------------------
@@ -326,10 +352,9 @@ template <> struct DiffMath<float> {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const VxScalars *S,
-                                                     const float4 *src32, double *part,
-                                                     long long tstride, int K) {
-    VX_PDL_WAIT();
+VX_DEVK void k_diff_partial_body(VxBlkB<PT, 0> vb, VxParams p, VxView v, const VxScalars *S,
+                                 const float4 *src32, double *part,
+                                 long long tstride, int K) {
     constexpr int TPT = pairs_tpt(sizeof(T) == 4);
     __shared__ SrcTile<T> st;
     const long long n = S->n;
@@ -339,7 +364,7 @@ __global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const
     const long long items = tiles * K;
     const T thr = (T)(0.001 * p.eps);
     const T thr2 = thr * thr;
-    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    for (long long it = vb.x; it < items; it += vb.n) {
         const long long tt = it % tiles, sc = it / tiles;
         T ax[TPT], ay[TPT], ndd[TPT];
         long long ti[TPT];
@@ -394,13 +419,19 @@ __global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const
         }
     }
 }
-
-__global__ void k_diff_combine(VxParams p, VxView v, const VxScalars *S, const double *part,
-                               long long tstride, int K) {
+template <typename T>
+__global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const VxScalars *S,
+                                                     const float4 *src32, double *part,
+                                                     long long tstride, int K) {
     VX_PDL_WAIT();
+    k_diff_partial_body<T>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, v, S, src32, part, tstride, K);
+}
+
+VX_DEVK void k_diff_combine_body(VxBlkB<0, 0> vb, VxParams p, VxView v, const VxScalars *S, const double *part,
+                                 long long tstride, int K) {
     const long long n = S->n;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         double I2x = 0.0, I2y = 0.0, I1 = 0.0;
         for (int sc = 0; sc < K; ++sc) {
             const double *o = part + (long long)sc * 3 * tstride + i;
@@ -415,6 +446,11 @@ __global__ void k_diff_combine(VxParams p, VxView v, const VxScalars *S, const d
         }
     }
 }
+__global__ void k_diff_combine(VxParams p, VxView v, const VxScalars *S, const double *part,
+                               long long tstride, int K) {
+    VX_PDL_WAIT();
+    k_diff_combine_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, part, tstride, K);
+}
 
 // ---------------------------------------------------------------------------
 static int pair_grid(const VxLaunch &L) { return vx_full_sms(L) * 4; }
@@ -422,8 +458,8 @@ static int pair_grid(const VxLaunch &L) { return vx_full_sms(L) * 4; }
 static cudaError_t maybe_pack(const VxLaunch &L, const VxParams &p, const VxView &v,
                               VxScalars *S, VxWork &w) {
     if (p.prec != VX_PREC_FP32) return cudaSuccess;
-    vx_launch_pdl(k_pack32, L.num_sms * 4, 256, 0, L.stream, v, S, w.src32, w.cap);
-    VX_COUNT(L);
+    vx_launch<k_pack32, k_pack32_body>(L, L.num_sms * 4, 256, 0, v, S, w.src32, w.cap);
+
     return cudaGetLastError();
 }
 
@@ -433,20 +469,18 @@ cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxVie
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32) {
         VX_EV(L, 0);
-        vx_launch_pdl(k_bs32_partial<true>, pair_grid(L), PT, 0, L.stream, p, S, w.src32, v.x, v.y, v.ps, -1, w.part,
-                                                                tstride, K);
+        vx_launch<k_bs32_partial<true>, k_bs32_partial_body<true>>(L, pair_grid(L), PT, 0, p, S, w.src32, v.x, v.y, v.ps, -1, w.part, tstride, K);
         VX_EV(L, 1);
-        VX_COUNT(L);
-        vx_launch_pdl(k_bs_combine<true>, L.num_sms * 4, 256, 0, L.stream, v, S, w.part, tstride, K);
+
+        vx_launch<k_bs_combine<true>, k_bs_combine_body<true>>(L, L.num_sms * 4, 256, 0, v, S, w.part, tstride, K);
     } else {
         VX_EV(L, 0);
-        vx_launch_pdl(k_bs_partial<double, true>, pair_grid(L), PT, 0, L.stream, p, v, S, nullptr, v.x, v.y, v.ps,
-                                                                      -1, w.part, tstride, K);
+        vx_launch<k_bs_partial<double, true>, k_bs_partial_body<double, true>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, v.x, v.y, v.ps, -1, w.part, tstride, K);
         VX_EV(L, 1);
-        VX_COUNT(L);
-        vx_launch_pdl(k_bs_combine<false>, L.num_sms * 4, 256, 0, L.stream, v, S, w.part, tstride, K);
+
+        vx_launch<k_bs_combine<false>, k_bs_combine_body<false>>(L, L.num_sms * 4, 256, 0, v, S, w.part, tstride, K);
     }
-    VX_COUNT(L);
+
     return cudaGetLastError();
 }
 
@@ -457,14 +491,14 @@ cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxVi
     const long long tstride = w.part_cap / (3LL * K);
     VX_EV(L, 2);
     if (p.prec == VX_PREC_FP32) {
-        vx_launch_pdl(k_diff_partial<float>, pair_grid(L), PT, 0, L.stream, p, v, S, w.src32, w.part, tstride, K);
+        vx_launch<k_diff_partial<float>, k_diff_partial_body<float>>(L, pair_grid(L), PT, 0, p, v, S, w.src32, w.part, tstride, K);
     } else {
-        vx_launch_pdl(k_diff_partial<double>, pair_grid(L), PT, 0, L.stream, p, v, S, nullptr, w.part, tstride, K);
+        vx_launch<k_diff_partial<double>, k_diff_partial_body<double>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, w.part, tstride, K);
     }
     VX_EV(L, 3);
-    VX_COUNT(L);
-    vx_launch_pdl(k_diff_combine, L.num_sms * 4, 256, 0, L.stream, p, v, S, w.part, tstride, K);
-    VX_COUNT(L);
+
+    vx_launch<k_diff_combine, k_diff_combine_body>(L, L.num_sms * 4, 256, 0, p, v, S, w.part, tstride, K);
+
     return cudaGetLastError();
 }
 
@@ -475,14 +509,11 @@ cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &
     if (tstride < np) return cudaErrorInvalidValue;
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32)
-        vx_launch_pdl(k_bs32_partial<false>, pair_grid(L), PT, 0, L.stream, p, S, w.src32, px, py, pstride, np, w.part,
-                                                                 tstride, K);
+        vx_launch<k_bs32_partial<false>, k_bs32_partial_body<false>>(L, pair_grid(L), PT, 0, p, S, w.src32, px, py, pstride, np, w.part, tstride, K);
     else
-        vx_launch_pdl(k_bs_partial<double, false>, pair_grid(L), PT, 0, L.stream, p, v, S, nullptr, px, py, pstride,
-                                                                       np, w.part, tstride, K);
-    VX_COUNT(L);
-    vx_launch_pdl(k_probe_combine, (int)vx_ceil_div(np, 256), 256, 0, L.stream, S, w.part, tstride, K, np, ovx, ovy,
-                                                                      ostride);
-    VX_COUNT(L);
+        vx_launch<k_bs_partial<double, false>, k_bs_partial_body<double, false>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, px, py, pstride, np, w.part, tstride, K);
+
+    vx_launch<k_probe_combine, k_probe_combine_body>(L, (int)vx_ceil_div(np, 256), 256, 0, S, w.part, tstride, K, np, ovx, ovy, ostride);
+
     return cudaGetLastError();
 }

@@ -17,18 +17,22 @@
 // the bucket's elements with a lower index).  A bucket of up to 16 elements
 // takes one thread, one of up to 128 a warp, a larger one a block.  The
 // counts are used up by the placement and written back by the ordering.
-__global__ void k_bk_place(const long long *d_n, const unsigned *key, const int *start, int *cnt0,
-                           const long long *d_off, unsigned *okey, int *oval) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bk_place_body(VxBlkB<0, 0> vb, const long long *d_n, const unsigned *key, const int *start, int *cnt0,
+                             const long long *d_off, unsigned *okey, int *oval) {
     const long long n = *d_n;
     int *cnt = cnt0 + (d_off ? *d_off : 0);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         const unsigned c = key[i];
         const int pos = start[c] + atomicSub(&cnt[c], 1) - 1;
         okey[pos] = c;
         oval[pos] = (int)i;
     }
+}
+__global__ void k_bk_place(const long long *d_n, const unsigned *key, const int *start, int *cnt0,
+                           const long long *d_off, unsigned *okey, int *oval) {
+    VX_PDL_WAIT();
+    k_bk_place_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, d_n, key, start, cnt0, d_off, okey, oval);
 }
 
 constexpr int BK_S = 16;  // a thread orders buckets of up to BK_S elements
@@ -37,13 +41,12 @@ constexpr int BK_E = 4;   // elements per lane: a warp orders buckets of up to 3
 // One thread per bucket: writes the count back, orders a bucket of up to
 // BK_S elements itself (ranks by counting, in registers) and lists larger
 // ones for a warp (mid) or a block (big).
-__global__ void k_bk_order(VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
-                           int *oval, int *mid, int *big) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bk_order_body(VxBlkB<0, 0> vb, VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
+                             int *oval, int *mid, int *big) {
     const long long nb = *d_nb;
     int *cnt = cnt0 + (d_off ? *d_off : 0);
-    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
-         b += (long long)gridDim.x * blockDim.x) {
+    for (long long b = vb.x * (long long)blockDim.x + threadIdx.x; b < nb;
+         b += (long long)vb.n * blockDim.x) {
         const int a = start[b], m = start[b + 1] - a;
         cnt[b] = m;
         if (m <= 1) continue;
@@ -64,15 +67,19 @@ __global__ void k_bk_order(VxScalars *S, const long long *d_nb, const int *start
         }
     }
 }
+__global__ void k_bk_order(VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
+                           int *oval, int *mid, int *big) {
+    VX_PDL_WAIT();
+    k_bk_order_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, d_nb, start, cnt0, d_off, oval, mid, big);
+}
 
 // One warp per listed bucket of BK_S < m <= 32 BK_E elements: lane holds
 // elements lane, lane + 32, ...; each counts the smaller ones.
-__global__ void k_bk_order_mid(const VxScalars *S, const int *start, const int *mid, int *oval) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bk_order_mid_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, const int *mid, int *oval) {
     const int nmid = S->bk_nmid;
     const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nmid; q += nw) {
+    const int nw = (vb.n * blockDim.x) >> 5;
+    for (int q = (vb.x * blockDim.x + threadIdx.x) >> 5; q < nmid; q += nw) {
         const int b = mid[q];
         const int a = start[b], m = start[b + 1] - a;
         int v[BK_E], r[BK_E];
@@ -98,15 +105,18 @@ __global__ void k_bk_order_mid(const VxScalars *S, const int *start, const int *
             if (lane + 32 * e < m) oval[a + r[e]] = v[e];
     }
 }
+__global__ void k_bk_order_mid(const VxScalars *S, const int *start, const int *mid, int *oval) {
+    VX_PDL_WAIT();
+    k_bk_order_mid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, mid, oval);
+}
 
 constexpr int BK_T = 512;
 constexpr int BK_SH = 4096;   // elements of a bucket held in shared memory; larger ones go through scratch
-__global__ void __launch_bounds__(BK_T) k_bk_order_big(const VxScalars *S, const int *start, const int *big,
-                                                       int *oval, int *scratch) {
-    VX_PDL_WAIT();
+VX_DEVK void k_bk_order_big_body(VxBlkB<BK_T, 0> vb, const VxScalars *S, const int *start, const int *big,
+                                 int *oval, int *scratch) {
     __shared__ int sv[BK_SH];
     const int nbig = S->bk_nbig;
-    for (int q = blockIdx.x; q < nbig; q += gridDim.x) {
+    for (int q = vb.x; q < nbig; q += vb.n) {
         const int b = big[q];
         const int a = start[b], m = start[b + 1] - a;
         const bool sh = m <= BK_SH;
@@ -122,19 +132,23 @@ __global__ void __launch_bounds__(BK_T) k_bk_order_big(const VxScalars *S, const
         __syncthreads();
     }
 }
+__global__ void __launch_bounds__(BK_T) k_bk_order_big(const VxScalars *S, const int *start, const int *big,
+                                                       int *oval, int *scratch) {
+    VX_PDL_WAIT();
+    k_bk_order_big_body(VxBlkB<BK_T, 0>{blockIdx.x, gridDim.x}, S, start, big, oval, scratch);
+}
 
 cudaError_t vx_bucket_order(const VxLaunch &L, VxScalars *S, const long long *d_n, const long long *d_nbuckets,
                             const unsigned *key, const int *start, int *cnt, const long long *d_cnt_off,
                             unsigned *okey, int *oval, int *mid, int *big, int *scratch) {
-    vx_launch_pdl(k_bk_place, L.num_sms * 4, 256, 0, L.stream, d_n, key, start, cnt, d_cnt_off, okey, oval);
-    VX_COUNT(L);
-    vx_launch_pdl(k_bk_order, L.num_sms * 4, 256, 0, L.stream, S, d_nbuckets, start, cnt, d_cnt_off, oval, mid,
-                  big);
-    VX_COUNT(L);
-    vx_launch_pdl(k_bk_order_mid, L.num_sms * 8, 256, 0, L.stream, S, start, mid, oval);
-    VX_COUNT(L);
-    vx_launch_pdl(k_bk_order_big, L.num_sms, BK_T, 0, L.stream, S, start, big, oval, scratch);
-    VX_COUNT(L);
+    vx_launch<k_bk_place, k_bk_place_body>(L, L.num_sms * 4, 256, 0, d_n, key, start, cnt, d_cnt_off, okey, oval);
+
+    vx_launch<k_bk_order, k_bk_order_body>(L, L.num_sms * 4, 256, 0, S, d_nbuckets, start, cnt, d_cnt_off, oval, mid, big);
+
+    vx_launch<k_bk_order_mid, k_bk_order_mid_body>(L, L.num_sms * 8, 256, 0, S, start, mid, oval);
+
+    vx_launch<k_bk_order_big, k_bk_order_big_body>(L, L.num_sms, BK_T, 0, S, start, big, oval, scratch);
+
     return cudaGetLastError();
 }
 

@@ -73,13 +73,12 @@ __device__ __forceinline__ void vx_wall_integral_bulk(float Ra0, float Ra1, floa
 }
 
 template <typename T>
-__global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel *pan, const int *wstart,
-                       const int *widx) {
-    VX_PDL_WAIT();
+VX_DEVK void k_wall_body(VxBlkB<0, 0> vb, VxParams p, VxView v, const VxScalars *S, const vx_panel *pan, const int *wstart,
+                         const int *widx) {
     const long long n = S->n;
     const T nu = (T)p.nu;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)vb.n * blockDim.x) {
         const double xd = v.x[i * v.ps], yd = v.y[i * v.ps];
         if (xd < p.wall_x0 || xd > p.wall_x1 || yd < p.wall_y0 || yd > p.wall_y1) continue;
         int q0 = 0, q1 = p.P;
@@ -121,14 +120,20 @@ __global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel 
         v.vy[i * v.vs] += (double)(nu * I31 / I0);
     }
 }
+template <typename T>
+__global__ void k_wall(VxParams p, VxView v, const VxScalars *S, const vx_panel *pan, const int *wstart,
+                       const int *widx) {
+    VX_PDL_WAIT();
+    k_wall_body<T>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, wstart, widx);
+}
 
 cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                            const vx_panel *pan, const int *wstart, const int *widx) {
     if (p.wall_nx <= 0 || p.wall_ny <= 0) wstart = widx = nullptr;
     if (p.prec == VX_PREC_FP32)
-        vx_launch_pdl(k_wall<float>, L.num_sms * 8, 128, 0, L.stream, p, v, S, pan, wstart, widx);
+        vx_launch<k_wall<float>, k_wall_body<float>>(L, L.num_sms * 8, 128, 0, p, v, S, pan, wstart, widx);
     else
-        vx_launch_pdl(k_wall<double>, L.num_sms * 8, 128, 0, L.stream, p, v, S, pan, wstart, widx);
-    VX_COUNT(L);
+        vx_launch<k_wall<double>, k_wall_body<double>>(L, L.num_sms * 8, 128, 0, p, v, S, pan, wstart, widx);
+
     return cudaGetLastError();
 }
