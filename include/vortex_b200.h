@@ -246,6 +246,32 @@ vx_status vx_server_result(vx_server *srv, int64_t id, int *state, int64_t *step
  * [7] particle steps, [8] bytes reserved now, [9] ticks. */
 vx_status vx_server_stats(vx_server *srv, double out10[10]);
 
+/* Batched steps (no counterpart in the reference, which runs one body per
+ * process; its step loop is src/main.c:652-785).  A batch advances bodies
+ * of one device together: each kernel of the step runs once for all of them
+ * (its blocks laid out body after body, each block given its body's
+ * arguments), and the whole batched step is one CUDA graph, so a step of
+ * the batch takes one launch per kernel of the step, not one per body.
+ * Each body's results are bit-identical to stepping it alone with vx_step.
+ * While a body belongs to a batch it launches on the batch's stream and is
+ * stepped only through vx_batch_step (vx_step and vx_stage refuse it); the
+ * other calls on the body work and are ordered after the batch's steps.
+ * Destroy the batch before any of its bodies. */
+typedef struct vx_batch vx_batch;
+vx_status vx_batch_create(vx_sim *const *sims, int count, vx_batch **out);
+/* Asynchronous like vx_step; bodies grow their stores as needed. */
+vx_status vx_batch_step(vx_batch *batch, int64_t nsteps);
+/* Wait for the batch's steps; reports the bodies' device error flags. */
+vx_status vx_batch_sync(vx_batch *batch);
+/* out[0] batched steps, [1] kernels they launched, [2] kernels per batched
+ * step now, [3] slot-table rebuilds, [4] graph instantiations, [5] bodies. */
+vx_status vx_batch_info(vx_batch *batch, double out6[6]);
+/* The CUDA stream (cudaStream_t) the batch launches on. */
+void *vx_batch_stream(vx_batch *batch);
+/* Ends the batch (waits for its steps); the bodies return to their own
+ * streams and can be stepped alone again. */
+vx_status vx_batch_destroy(vx_batch *batch);
+
 /* Switch the bulk form's far field (fmm: 1 quadtree FMM and birth far
  * field, 0 direct sums) and the quadtree's target vortices per leaf at run
  * time (the autotuner's knobs); the step graph is re-captured. */

@@ -21,18 +21,17 @@ LEAVES = (8, 16, 32, 64, 128, 256)
 
 
 def time_velocity(sim: N.Sim, reps: int = 3, device: int = 0) -> float:
-    """Median device ms of the velocity stage on the sim's stream."""
-    import torch
-    st = torch.cuda.ExternalStream(sim.stream(), device=f"cuda:{device}")
+    """Median device ms of the velocity stage, timed with CUDA events on the
+    sim's own stream."""
+    st = sim.stream()
     sim.stage("velocity")      # warm (graph-free stage path, buffers sized)
     ms = []
     for _ in range(reps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a, b = N.Event(), N.Event()
         a.record(st)
         sim.stage("velocity")
         b.record(st)
-        b.synchronize()
-        ms.append(a.elapsed_time(b))
+        ms.append(a.elapsed_ms(b))
     ms.sort()
     return ms[len(ms) // 2]
 

@@ -7,6 +7,8 @@
 // each thread of a fixed grid accumulates a fixed strided subset, blocks
 // reduce in a fixed tree and one block adds the block sums in order, so the
 // result is run-to-run identical.
+#include <algorithm>
+
 #include "vx_internal.cuh"
 
 // Segment (x2,y2)->(x1,y1) against one panel: on a crossing, sets hit and
@@ -111,9 +113,11 @@ __device__ __forceinline__ double vx_block_sum(double v, double *sh) {
     return r;
 }
 
-VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, const VxScalars *S,
-                           const vx_panel *pan, double *red, const int *hstart,
-                           const int *hidx) {
+// Partition `part` of `nparts` (the particles a block of a grid of nparts
+// blocks would take) and its four block sums into red[4 part ..].
+__device__ __forceinline__ void advect_part(unsigned part, unsigned nparts, const VxParams &p, const VxView &v,
+                                            const VxScalars *S, const vx_panel *pan, double *red,
+                                            const int *hstart, const int *hidx) {
     __shared__ double sh[VX_THREADS];
     const long long n = S->n;
     const long long n_new0 = S->n0;   // vortices born this step: [n0, n)
@@ -121,8 +125,8 @@ VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, const
     double sdg = 0.0, sfx = 0.0, sfy = 0.0, sm = 0.0;
     // whole warps step together (lane i of the warp takes particle base + i),
     // so a long segment can be handed to the warp
-    for (long long base = vb.x * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
-         base += (long long)vb.n * blockDim.x) {
+    for (long long base = part * (long long)blockDim.x + (threadIdx.x & ~31); base < n;
+         base += (long long)nparts * blockDim.x) {
         const long long i = base + lane;
         const bool valid = i < n;
         const long long k = i * v.ps;
@@ -185,16 +189,32 @@ VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, const
         sfx += fx; sfy += fy; sm += m;
     }
     double t;
-    t = vx_block_sum(sdg, sh); if (threadIdx.x == 0) red[vb.x * 4 + 0] = t;
-    t = vx_block_sum(sfx, sh); if (threadIdx.x == 0) red[vb.x * 4 + 1] = t;
-    t = vx_block_sum(sfy, sh); if (threadIdx.x == 0) red[vb.x * 4 + 2] = t;
-    t = vx_block_sum(sm, sh);  if (threadIdx.x == 0) red[vb.x * 4 + 3] = t;
+    t = vx_block_sum(sdg, sh); if (threadIdx.x == 0) red[part * 4 + 0] = t;
+    t = vx_block_sum(sfx, sh); if (threadIdx.x == 0) red[part * 4 + 1] = t;
+    t = vx_block_sum(sfy, sh); if (threadIdx.x == 0) red[part * 4 + 2] = t;
+    t = vx_block_sum(sm, sh);  if (threadIdx.x == 0) red[part * 4 + 3] = t;
+}
+// The particles are split into nparts fixed partitions (block-strided, as a
+// grid of nparts blocks would take them) whatever the grid: each block takes
+// partitions blockIdx, blockIdx + grid, ...; a partition past the last
+// particle has zero sums.  The partial sums, and so the totals, do not depend
+// on the grid the kernel runs with.
+VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, const VxScalars *S,
+                           const vx_panel *pan, double *red, const int *hstart, const int *hidx, int nparts) {
+    const long long n = S->n;
+    for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) {
+        if ((long long)q * blockDim.x >= n) {
+            if (threadIdx.x < 4) red[q * 4 + threadIdx.x] = 0.0;
+            continue;
+        }
+        advect_part(q, (unsigned)nparts, p, v, S, pan, red, hstart, hidx);
+    }
 }
 __global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, const VxScalars *S,
                                                        const vx_panel *pan, double *red, const int *hstart,
-                                                       const int *hidx) {
+                                                       const int *hidx, int nparts) {
     VX_PDL_WAIT();
-    k_advect_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, red, hstart, hidx);
+    k_advect_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, red, hstart, hidx, nparts);
 }
 
 // Block sums combined by one block: thread t adds blocks t, t + 256, ... in
@@ -220,7 +240,11 @@ __global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, c
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                              VxWork &w, const vx_panel *pan, const int *hstart, const int *hidx) {
     if (p.hit_nx <= 0 || p.hit_ny <= 0) hstart = hidx = nullptr;
-    vx_launch<k_advect, k_advect_body>(L, VX_RED_BLOCKS, VX_THREADS, 0, p, v, S, pan, w.red, hstart, hidx);
-    vx_launch<k_sums, k_sums_body>(L, 1, VX_THREADS, 0, p, S, w.red, VX_RED_BLOCKS);
+    // partitions of the force sums follow the body's size (vx_part_sms), the
+    // grid follows the SMs this launch is given
+    const int nparts = std::min(vx_part_sms(L) * 4, VX_RED_BLOCKS);
+    const int grid = std::min(nparts, L.num_sms * 4);
+    vx_launch<k_advect, k_advect_body>(L, grid, VX_THREADS, 0, p, v, S, pan, w.red, hstart, hidx, nparts);
+    vx_launch<k_sums, k_sums_body>(L, 1, VX_THREADS, 0, p, S, w.red, nparts);
     return cudaGetLastError();
 }

@@ -1,0 +1,556 @@
+// vx_batch.cu — many bodies advanced together: every kernel of the step runs
+// once for all bodies (k_many over the bodies' argument packs), and the whole
+// batched step is one CUDA graph.
+//
+// Each body's step is recorded, not launched: the same stage launchers the
+// single-body path runs (vx_sim_launch_stages) append (kernel, grid, block,
+// argument pack) to the body's recording.  The recordings are merged into one
+// sequence of slots, each one kernel with the bodies that run it at that
+// point: a greedy merge that keeps every body's own order (bodies whose
+// quadtrees have more levels run their extra level kernels in slots of their
+// own).  A slot's bodies share one launch: its blocks are the bodies' own
+// grids laid end to end, and k_many gives each block its body's arguments
+// and block coordinates, so a body computes exactly what its own launches
+// would have computed.  The grids of the scaled grid-stride launches are
+// sized for a share of the GPU proportional to the body's size; the
+// partitions that fix summation orders follow the body's own size
+// (VxLaunch::part_sms), so results are bit-identical to vx_step's.
+//
+// The slot tables (block ranges and packs) live in one device arena that the
+// graph's kernels read; when a body's recording changes (its store grew, a
+// launch shape followed its size across a power of two) the arena is
+// rewritten by a stream-ordered copy and the graph is re-instantiated only if
+// the slot sequence or a grid bound changed.  Capacity: the host keeps an
+// upper bound of each body's count (births add P per step) and, when a body
+// may outgrow its store, tightens it with the counts of the step before the
+// one in flight (copied back after every step), so the pipeline is not
+// drained for it; growth is stream-ordered after the steps in flight.
+//
+// Reference: the step loop this batches is src/main.c:652-785 with Speed /
+// Step / vort_creation (src/unit_1.cu:963-1218); the reference runs one body
+// per process.
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "vx_sim.cuh"
+
+#define BCU(call)                                                                           \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            vx_set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return e_ == cudaErrorMemoryAllocation ? VX_ERR_NOMEM : VX_ERR_CUDA;            \
+        }                                                                                   \
+    } while (0)
+
+namespace {
+
+// What a body's recording depends on besides its (unchanging) parameters.
+struct BodyKey {
+    long long cap;
+    int kv, rhs, sms, share, fmm, leaf, lmax;
+    bool operator==(const BodyKey &o) const {
+        return cap == o.cap && kv == o.kv && rhs == o.rhs && sms == o.sms && share == o.share && fmm == o.fmm &&
+               leaf == o.leaf && lmax == o.lmax;
+    }
+};
+
+struct Body {
+    vx_sim *s = nullptr;
+    VxRecorder rec;
+    BodyKey key{};
+    bool recorded = false;
+};
+
+struct Slot {
+    const void *key = nullptr;    // the single-body kernel (identity)
+    const void *many = nullptr;   // its multi-body kernel
+    dim3 block;
+    size_t smem = 0;
+    std::vector<int> bodies;      // batch indices
+    std::vector<int> launch;      // index of the launch in each body's recording
+    long long total = 0;          // blocks of all bodies
+    size_t pack = 0;              // bytes of one argument pack
+};
+
+// What the instantiated graph holds for a slot.
+struct SlotSig {
+    const void *many;
+    unsigned bx;
+    size_t smem;
+    long long bound;
+};
+
+__global__ void k_batch_counts(const VxScalars *const *S, long long *out, int nb) {
+    VX_PDL_WAIT();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) out[i] = S[i]->n;
+}
+
+long long pow2_at_least(long long v) {
+    long long q = 1;
+    while (q < v) q <<= 1;
+    return q;
+}
+
+}  // namespace
+
+struct vx_batch {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<Body> bodies;
+    int share_div = 1;
+    std::vector<Slot> slots;
+    // device arena: VxSlot[ns] | scalar pointers [nb] | per slot: first[] | packs
+    unsigned char *d_arena = nullptr;
+    size_t arena_cap = 0;
+    std::vector<unsigned char> h_arena;
+    unsigned char *h_stage[2] = {nullptr, nullptr};
+    size_t stage_cap[2] = {0, 0};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    int stage_idx = 0;
+    // graph
+    cudaGraphExec_t exec = nullptr;
+    std::vector<SlotSig> sig;
+    const unsigned char *sig_arena = nullptr;
+    // counts after each step, copied back (two steps kept)
+    long long *d_counts = nullptr;
+    long long *h_counts[2] = {nullptr, nullptr};
+    cudaEvent_t cnt_ev[2] = {nullptr, nullptr};
+    long long cnt_step[2] = {-1, -1};
+    long long launched = 0;       // batched steps launched
+    long long kernels = 0;        // kernels launched by the batched steps
+    long long rebuilds = 0, reinstantiations = 0;
+    bool dirty = true;
+};
+
+static vx_status free_graph(vx_batch *b) {
+    if (b->exec) {
+        cudaStreamSynchronize(b->stream);   // no launch of it still running
+        cudaGraphExecDestroy(b->exec);
+    }
+    b->exec = nullptr;
+    b->sig.clear();
+    return VX_OK;
+}
+
+// Greedy merge of the bodies' launch sequences into slots: repeatedly take
+// the (kernel, block) pair at the head of the most sequences (ties: the one
+// heading the longest remaining sequence) and advance those sequences.
+static vx_status merge(vx_batch *b) {
+    const int nb = (int)b->bodies.size();
+    std::vector<size_t> head((size_t)nb, 0);
+    b->slots.clear();
+    for (;;) {
+        std::map<std::pair<const void *, unsigned>, int> count;
+        std::pair<const void *, unsigned> best{nullptr, 0};
+        int best_n = 0;
+        size_t best_left = 0;
+        for (int i = 0; i < nb; ++i) {
+            const auto &L = b->bodies[(size_t)i].rec.launches;
+            if (head[(size_t)i] >= L.size()) continue;
+            const VxRecLaunch &r = L[head[(size_t)i]];
+            const auto k = std::make_pair(r.key, r.block.x);
+            count[k] += 1;
+        }
+        if (count.empty()) break;
+        for (int i = 0; i < nb; ++i) {
+            const auto &L = b->bodies[(size_t)i].rec.launches;
+            if (head[(size_t)i] >= L.size()) continue;
+            const VxRecLaunch &r = L[head[(size_t)i]];
+            const auto k = std::make_pair(r.key, r.block.x);
+            const int c = count[k];
+            const size_t left = L.size() - head[(size_t)i];
+            if (c > best_n || (c == best_n && left > best_left)) {
+                best = k;
+                best_n = c;
+                best_left = left;
+            }
+        }
+        Slot sl;
+        sl.key = best.first;
+        for (int i = 0; i < nb; ++i) {
+            const auto &L = b->bodies[(size_t)i].rec.launches;
+            if (head[(size_t)i] >= L.size()) continue;
+            const VxRecLaunch &r = L[head[(size_t)i]];
+            if (r.key != best.first || r.block.x != best.second) continue;
+            if (r.grid.y != 1 || r.grid.z != 1 || r.block.y != 1 || r.block.z != 1) {
+                vx_set_error("batch: a step kernel with a multi-dimensional launch cannot be batched");
+                return VX_ERR_ARG;
+            }
+            if (sl.bodies.empty()) {
+                sl.many = r.many;
+                sl.block = r.block;
+                sl.pack = r.size;
+            } else if (r.size != sl.pack || r.many != sl.many) {
+                vx_set_error("batch: one kernel recorded with different argument packs");
+                return VX_ERR_ARG;
+            }
+            sl.smem = std::max(sl.smem, r.smem);
+            sl.bodies.push_back(i);
+            sl.launch.push_back((int)head[(size_t)i]);
+            sl.total += r.grid.x;
+            head[(size_t)i] += 1;
+        }
+        b->slots.push_back(std::move(sl));
+    }
+    return VX_OK;
+}
+
+static size_t align16(size_t v) { return (v + 15) / 16 * 16; }
+
+// Lay out the arena for the current slots on the host (device addresses from
+// `base`); returns its size.
+static size_t layout(vx_batch *b, unsigned char *base) {
+    const size_t ns = b->slots.size(), nb = b->bodies.size();
+    size_t off = align16(ns * sizeof(VxSlot));
+    const size_t s_off = off;
+    off = align16(off + nb * sizeof(VxScalars *));
+    std::vector<size_t> first_off(ns), pack_off(ns);
+    for (size_t j = 0; j < ns; ++j) {
+        first_off[j] = off;
+        off = align16(off + (b->slots[j].bodies.size() + 1) * sizeof(int));
+    }
+    for (size_t j = 0; j < ns; ++j) {
+        pack_off[j] = off;
+        off = align16(off + b->slots[j].bodies.size() * align16(b->slots[j].pack));
+    }
+    const size_t size = off;
+    b->h_arena.assign(size, 0);
+    unsigned char *h = b->h_arena.data();
+    VxSlot *hs = reinterpret_cast<VxSlot *>(h);
+    for (size_t j = 0; j < ns; ++j) {
+        const Slot &sl = b->slots[j];
+        VxSlot d;
+        d.nb = (int)sl.bodies.size();
+        d.pad = 0;
+        d.stride = (long long)align16(sl.pack);
+        d.first = reinterpret_cast<const int *>(base + first_off[j]);
+        d.packs = base + pack_off[j];
+        hs[j] = d;
+        int *first = reinterpret_cast<int *>(h + first_off[j]);
+        long long acc = 0;
+        for (size_t q = 0; q < sl.bodies.size(); ++q) {
+            const Body &bd = b->bodies[(size_t)sl.bodies[q]];
+            const VxRecLaunch &r = bd.rec.launches[(size_t)sl.launch[q]];
+            first[q] = (int)acc;
+            acc += r.grid.x;
+            memcpy(h + pack_off[j] + q * align16(sl.pack), bd.rec.arena.data() + r.off, r.size);
+        }
+        first[sl.bodies.size()] = (int)acc;
+    }
+    VxScalars **sp = reinterpret_cast<VxScalars **>(h + s_off);
+    for (size_t i = 0; i < nb; ++i) sp[i] = b->bodies[i].s->d_S;
+    return size;
+}
+
+static const VxScalars *const *scalars_list(vx_batch *b) {
+    const size_t ns = b->slots.size();
+    return reinterpret_cast<const VxScalars *const *>(b->d_arena + align16(ns * sizeof(VxSlot)));
+}
+
+static vx_status build_graph(vx_batch *b) {
+    free_graph(b);
+    for (const Slot &sl : b->slots) {
+        if (sl.smem > 48 * 1024)
+            BCU(cudaFuncSetAttribute(sl.many, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sl.smem));
+        cudaFuncAttributes fa;
+        BCU(cudaFuncGetAttributes(&fa, sl.many));
+        if ((int)sl.block.x > fa.maxThreadsPerBlock) {
+            vx_set_error("batch: a multi-body kernel takes at most %d threads per block, %u recorded",
+                         fa.maxThreadsPerBlock, sl.block.x);
+            return VX_ERR_CUDA;
+        }
+    }
+    cudaGraph_t graph;
+    BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (size_t j = 0; j < b->slots.size() && e == cudaSuccess; ++j) {
+        const Slot &sl = b->slots[j];
+        SlotSig g{sl.many, sl.block.x, sl.smem, std::max<long long>(1, pow2_at_least(sl.total))};
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)g.bound);
+        cfg.blockDim = sl.block;
+        cfg.dynamicSmemBytes = sl.smem;
+        cfg.stream = b->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const VxSlot *slot = reinterpret_cast<const VxSlot *>(b->d_arena) + j;
+        void *args[1] = {&slot};
+        e = cudaLaunchKernelExC(&cfg, sl.many, args);
+        b->sig.push_back(g);
+    }
+    if (e == cudaSuccess) {
+        const int nb = (int)b->bodies.size();
+        vx_launch_pdl(k_batch_counts, std::max(1, std::min(64, (nb + 255) / 256)), 256, 0, b->stream,
+                      scalars_list(b), b->d_counts, nb);
+        e = cudaGetLastError();
+    }
+    cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        b->sig.clear();
+        vx_set_error("batch graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        return VX_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&b->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        b->exec = nullptr;
+        b->sig.clear();
+        vx_set_error("batch graph instantiate: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    b->sig_arena = b->d_arena;
+    b->reinstantiations += 1;
+    return VX_OK;
+}
+
+static bool graph_fits(const vx_batch *b) {
+    if (!b->exec || b->sig_arena != b->d_arena || b->sig.size() != b->slots.size()) return false;
+    for (size_t j = 0; j < b->slots.size(); ++j) {
+        const SlotSig &g = b->sig[j];
+        const Slot &sl = b->slots[j];
+        if (g.many != sl.many || g.bx != sl.block.x || sl.smem > g.smem || sl.total > g.bound) return false;
+    }
+    return true;
+}
+
+// Copy the host arena into the device one: a pinned staging buffer (two,
+// used in turn, each reused only after its previous copy finished) and a
+// copy ordered on the batch stream after the steps already launched.
+static vx_status upload(vx_batch *b) {
+    const size_t size = b->h_arena.size();
+    const int k = b->stage_idx;
+    b->stage_idx ^= 1;
+    BCU(cudaEventSynchronize(b->stage_ev[k]));
+    if (b->stage_cap[k] < size) {
+        if (b->h_stage[k]) cudaFreeHost(b->h_stage[k]);
+        b->h_stage[k] = nullptr;
+        b->stage_cap[k] = 0;
+        BCU(cudaMallocHost(&b->h_stage[k], size));
+        b->stage_cap[k] = size;
+    }
+    memcpy(b->h_stage[k], b->h_arena.data(), size);
+    BCU(cudaMemcpyAsync(b->d_arena, b->h_stage[k], size, cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaEventRecord(b->stage_ev[k], b->stream));
+    return VX_OK;
+}
+
+static BodyKey key_of(vx_batch *b, vx_sim *s) {
+    BodyKey k;
+    k.cap = s->cap;
+    k.kv = vx_sim_kv(s);
+    k.rhs = vx_sim_rhs_chunks(s);
+    k.sms = vx_sim_step_sms(s);
+    k.share = std::max(1, (k.sms + b->share_div - 1) / b->share_div);
+    k.fmm = s->conf.fmm;
+    k.leaf = s->prm.fmm_leaf;
+    k.lmax = s->w.fmm_lmax;
+    return k;
+}
+
+// Re-record the bodies whose recordings are stale, then merge, lay out,
+// upload and (if needed) re-instantiate.
+static vx_status refresh(vx_batch *b) {
+    bool changed = b->dirty;
+    for (Body &bd : b->bodies) {
+        const BodyKey k = key_of(b, bd.s);
+        if (bd.recorded && k == bd.key) continue;
+        bd.rec.launches.clear();
+        bd.rec.arena.clear();
+        const cudaError_t e = vx_sim_launch_stages(bd.s, VX_STAGE_ALL, true, &bd.rec, k.share);
+        if (e != cudaSuccess) {
+            vx_set_error("batch: recording a body's step: %s", cudaGetErrorString(e));
+            return VX_ERR_CUDA;
+        }
+        bd.key = k;
+        bd.recorded = true;
+        changed = true;
+    }
+    if (!changed) return VX_OK;
+    vx_status st = merge(b);
+    if (st != VX_OK) return st;
+    size_t need = layout(b, b->d_arena);
+    if (need > b->arena_cap) {
+        if (b->d_arena) BCU(cudaFreeAsync(b->d_arena, b->stream));   // after the steps in flight
+        b->d_arena = nullptr;
+        b->arena_cap = 0;
+        const size_t cap = std::max(need + need / 2, (size_t)1 << 16);
+        BCU(cudaMallocAsync((void **)&b->d_arena, cap, b->stream));
+        b->arena_cap = cap;
+        need = layout(b, b->d_arena);
+    }
+    if ((st = upload(b)) != VX_OK) return st;
+    if (!graph_fits(b) && (st = build_graph(b)) != VX_OK) return st;
+    b->rebuilds += 1;
+    b->dirty = false;
+    return VX_OK;
+}
+
+// Upper bounds of the counts before the next step, from the counts copied
+// back after step `launched - 2` (the step before the one in flight);
+// bodies that may outgrow their stores grow (stream-ordered).
+static vx_status ensure_capacities(vx_batch *b) {
+    bool need_counts = false;
+    for (Body &bd : b->bodies)
+        if (vx_sim_need(bd.s, bd.s->n_upper) > bd.s->cap) need_counts = true;
+    if (!need_counts) return VX_OK;
+    const long long want = b->launched - 2;
+    int k = -1;
+    for (int q = 0; q < 2; ++q)
+        if (b->cnt_step[q] >= 0 && b->cnt_step[q] >= want && (k < 0 || b->cnt_step[q] < b->cnt_step[k])) k = q;
+    if (k < 0)
+        for (int q = 0; q < 2; ++q)
+            if (b->cnt_step[q] >= 0 && (k < 0 || b->cnt_step[q] > b->cnt_step[k])) k = q;
+    if (k >= 0) {
+        BCU(cudaEventSynchronize(b->cnt_ev[k]));
+        const long long after = b->launched - 1 - b->cnt_step[k];   // steps launched after those counts
+        for (size_t i = 0; i < b->bodies.size(); ++i) {
+            vx_sim *s = b->bodies[i].s;
+            const long long bound = b->h_counts[k][i] + after * s->P;
+            if (bound < s->n_upper) s->n_upper = bound;
+        }
+    }
+    for (Body &bd : b->bodies) {
+        vx_sim *s = bd.s;
+        const long long need = vx_sim_need(s, s->n_upper);
+        if (need > s->cap) {
+            const vx_status st = vx_sim_grow(s, need);
+            if (st != VX_OK) return st;
+        }
+    }
+    return VX_OK;
+}
+
+static void release(vx_batch *b) {
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    free_graph(b);
+    for (Body &bd : b->bodies) {
+        vx_sim *s = bd.s;
+        if (!s || !s->in_batch) continue;
+        s->stream = s->own_stream;
+        s->own_stream = nullptr;
+        s->in_batch = false;
+        vx_sim_read_scalars(s);   // the true count again
+    }
+    if (b->d_arena) cudaFree(b->d_arena);
+    if (b->d_counts) cudaFree(b->d_counts);
+    for (int k = 0; k < 2; ++k) {
+        if (b->h_stage[k]) cudaFreeHost(b->h_stage[k]);
+        if (b->h_counts[k]) cudaFreeHost(b->h_counts[k]);
+        if (b->stage_ev[k]) cudaEventDestroy(b->stage_ev[k]);
+        if (b->cnt_ev[k]) cudaEventDestroy(b->cnt_ev[k]);
+    }
+    if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+extern "C" vx_status vx_batch_create(vx_sim *const *sims, int count, vx_batch **out) {
+    if (!sims || count < 1 || !out) return VX_ERR_ARG;
+    *out = nullptr;
+    const int dev = sims[0] ? sims[0]->device : 0;
+    for (int i = 0; i < count; ++i) {
+        if (!sims[i] || sims[i]->device != dev || sims[i]->in_batch) {
+            vx_set_error("vx_batch_create: body %d is null, on another device or already in a batch", i);
+            return VX_ERR_ARG;
+        }
+        for (int j = 0; j < i; ++j)
+            if (sims[j] == sims[i]) {
+                vx_set_error("vx_batch_create: body %d is listed twice", i);
+                return VX_ERR_ARG;
+            }
+    }
+    BCU(cudaSetDevice(dev));
+    vx_batch *b = new vx_batch();
+    b->device = dev;
+    auto fail = [&](vx_status st) {
+        release(b);
+        delete b;
+        return st;
+    };
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VX_ERR_CUDA);
+    for (int k = 0; k < 2; ++k) {
+        if (cudaEventCreateWithFlags(&b->stage_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->cnt_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost(&b->h_counts[k], sizeof(long long) * (size_t)count) != cudaSuccess)
+            return fail(VX_ERR_CUDA);
+    }
+    if (cudaMalloc(&b->d_counts, sizeof(long long) * (size_t)count) != cudaSuccess) return fail(VX_ERR_NOMEM);
+    // every body's own work first, then the bodies launch on the batch stream
+    long long demand = 0;
+    for (int i = 0; i < count; ++i) {
+        vx_sim *s = sims[i];
+        if (cudaStreamSynchronize(s->stream) != cudaSuccess) return fail(VX_ERR_CUDA);
+        Body bd;
+        bd.s = s;
+        b->bodies.push_back(std::move(bd));
+        s->own_stream = s->stream;
+        s->stream = b->stream;
+        s->in_batch = true;
+        demand += vx_sim_step_sms(s);
+    }
+    // shares: the scaled launches of all bodies together about fill the GPU twice
+    b->share_div = (int)std::max(1LL, demand / (2LL * b->num_sms));
+    *out = b;
+    return VX_OK;
+}
+
+extern "C" vx_status vx_batch_step(vx_batch *b, int64_t nsteps) {
+    if (!b || nsteps < 0) return VX_ERR_ARG;
+    BCU(cudaSetDevice(b->device));
+    for (int64_t t = 0; t < nsteps; ++t) {
+        vx_status st = ensure_capacities(b);
+        if (st != VX_OK) return st;
+        if ((st = refresh(b)) != VX_OK) return st;
+        BCU(cudaGraphLaunch(b->exec, b->stream));
+        const int k = (int)(b->launched & 1);
+        BCU(cudaMemcpyAsync(b->h_counts[k], b->d_counts, sizeof(long long) * b->bodies.size(),
+                            cudaMemcpyDeviceToHost, b->stream));
+        BCU(cudaEventRecord(b->cnt_ev[k], b->stream));
+        b->cnt_step[k] = b->launched;
+        b->launched += 1;
+        b->kernels += (long long)b->slots.size() + 1;
+        for (Body &bd : b->bodies) bd.s->n_upper += bd.s->P;
+    }
+    return VX_OK;
+}
+
+extern "C" vx_status vx_batch_sync(vx_batch *b) {
+    if (!b) return VX_ERR_ARG;
+    BCU(cudaSetDevice(b->device));
+    BCU(cudaStreamSynchronize(b->stream));
+    for (Body &bd : b->bodies) {
+        const vx_status st = vx_sim_read_scalars(bd.s);
+        if (st != VX_OK) return st;
+    }
+    return VX_OK;
+}
+
+// out[0] batched steps, [1] kernels launched by them, [2] kernels per step
+// now (slots + the count gather), [3] slot-table rebuilds, [4] graph
+// instantiations, [5] bodies.
+extern "C" vx_status vx_batch_info(vx_batch *b, double out6[6]) {
+    if (!b || !out6) return VX_ERR_ARG;
+    out6[0] = (double)b->launched;
+    out6[1] = (double)b->kernels;
+    out6[2] = (double)b->slots.size() + 1;
+    out6[3] = (double)b->rebuilds;
+    out6[4] = (double)b->reinstantiations;
+    out6[5] = (double)b->bodies.size();
+    return VX_OK;
+}
+
+extern "C" void *vx_batch_stream(vx_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+extern "C" vx_status vx_batch_destroy(vx_batch *b) {
+    if (!b) return VX_OK;
+    cudaSetDevice(b->device);
+    release(b);
+    delete b;
+    return VX_OK;
+}

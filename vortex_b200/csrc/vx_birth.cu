@@ -403,12 +403,13 @@ __device__ __forceinline__ bool bf_near(const VxParams &p, double x, double y) {
 // warp (at each halving a lane keeps the half of its values selected by its
 // lane bit and adds the partner's copy: lane q ends with value q, i.e.
 // coefficient q/2, part q&1) and a fixed-order sum over the block's warps.
-VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
+// Partition q of nparts: sources [j0, j1) (bf_chunk).
+__device__ __forceinline__ void bf_far_part(unsigned q, unsigned nparts, const VxParams &p, const VxView &v,
+                                            const VxScalars *S, double *part, int *cnt, long long j0,
+                                            long long j1) {
     __shared__ double sacc[BF_T / 32][32];
     __shared__ int snear[BF_T / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    long long j0, j1;
-    bf_chunk(S, vb.n, vb.x, j0, j1);
     int nnear = 0;
     for (int pass = 0; pass < BF_P / 16; ++pass) {
         double acc[32];   // (re, im) of the pass's 16 coefficients
@@ -460,7 +461,7 @@ VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxSca
             double sum = 0.0;
             for (int q = 0; q < BF_T / 32; ++q) sum += sacc[q][threadIdx.x];
             // value q of this pass: coefficient 16 pass + q/2, part q&1
-            part[((long long)vb.x * BF_P + 16 * pass + (threadIdx.x >> 1)) * 2 + (threadIdx.x & 1)] = sum;
+            part[((long long)q * BF_P + 16 * pass + (threadIdx.x >> 1)) * 2 + (threadIdx.x & 1)] = sum;
         }
         __syncthreads();
     }
@@ -470,12 +471,29 @@ VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxSca
     if (threadIdx.x == 0) {
         int t = 0;
         for (int q = 0; q < BF_T / 32; ++q) t += snear[q];
-        cnt[vb.x] = t;
+        cnt[q] = t;
     }
 }
-__global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt) {
+// The sources are split into nparts fixed chunks whatever the grid; each
+// block takes chunks blockIdx, blockIdx + grid, ...; an empty chunk has zero
+// partials.  The summed coefficients do not depend on the launch's grid.
+VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S, double *part, int *cnt,
+                           int nparts) {
+    for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) {
+        long long j0, j1;
+        bf_chunk(S, nparts, q, j0, j1);
+        if (j0 >= j1) {
+            for (int t = threadIdx.x; t < 2 * BF_P; t += blockDim.x) part[(long long)q * 2 * BF_P + t] = 0.0;
+            if (threadIdx.x == 0) cnt[q] = 0;
+            continue;
+        }
+        bf_far_part(q, (unsigned)nparts, p, v, S, part, cnt, j0, j1);
+    }
+}
+__global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt,
+                                                 int nparts) {
     VX_PDL_WAIT();
-    k_bf_far_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, part, cnt);
+    k_bf_far_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, part, cnt, nparts);
 }
 
 // Block-count offsets and the coefficient sums (block order), one block of
@@ -528,13 +546,13 @@ __global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, con
 }
 
 // Near sources of each block in index order (block-wide ballot scan).
-VX_DEVK void k_bf_scatter_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S,
-                               const long long *off, float4 *near) {
+__device__ __forceinline__ void bf_scatter_part(unsigned q, unsigned nparts, const VxParams &p, const VxView &v,
+                                                const VxScalars *S, const long long *off, float4 *near) {
     __shared__ int swarp[BF_T / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     long long j0, j1;
-    bf_chunk(S, vb.n, vb.x, j0, j1);
-    long long base = off[vb.x];
+    bf_chunk(S, nparts, q, j0, j1);
+    long long base = off[q];
     for (long long jt = j0; jt < j1; jt += BF_T) {
         const long long j = jt + threadIdx.x;
         double x = 0.0, y = 0.0, g = 0.0;
@@ -557,10 +575,14 @@ VX_DEVK void k_bf_scatter_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const V
         base += total;
     }
 }
+VX_DEVK void k_bf_scatter_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S,
+                               const long long *off, float4 *near, int nparts) {
+    for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) bf_scatter_part(q, (unsigned)nparts, p, v, S, off, near);
+}
 __global__ void __launch_bounds__(BF_T) k_bf_scatter(VxParams p, VxView v, const VxScalars *S,
-                                                     const long long *off, float4 *near) {
+                                                     const long long *off, float4 *near, int nparts) {
     VX_PDL_WAIT();
-    k_bf_scatter_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, off, near);
+    k_bf_scatter_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, off, near, nparts);
 }
 
 // atan2 in FP32 for the bulk form's near panel terms: the octant reduction
@@ -865,10 +887,13 @@ static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView
     const int grid = (int)min((long long)tiles * rhs_chunks, (long long)L.num_sms * 16);
     const bool far = p.prec == VX_PREC_FP32 && p.birth_far;
     if (far) {
-        const int nb = std::min(2 * vx_full_sms(L), VX_BF_MAX_BLOCKS);
-        vx_launch<k_bf_far, k_bf_far_body>(L, nb, BF_T, 0, p, v, S, w.bf_part, w.bf_cnt);
+        // source chunks follow the body's size (vx_part_sms), the grid the
+        // SMs this launch is given
+        const int nb = std::min(2 * vx_part_sms(L), VX_BF_MAX_BLOCKS);
+        const int gb = std::min(nb, 2 * L.num_sms);
+        vx_launch<k_bf_far, k_bf_far_body>(L, gb, BF_T, 0, p, v, S, w.bf_part, w.bf_cnt, nb);
         vx_launch<k_bf_scan, k_bf_scan_body>(L, 1, BF_SCAN_T, 0, S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef);
-        vx_launch<k_bf_scatter, k_bf_scatter_body>(L, nb, BF_T, 0, p, v, S, w.bf_off, w.bf_near);
+        vx_launch<k_bf_scatter, k_bf_scatter_body>(L, gb, BF_T, 0, p, v, S, w.bf_off, w.bf_near, nb);
         vx_launch<k_rhs_near, k_rhs_near_body>(L, grid, RHS_T, 0, S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
     } else if (p.prec == VX_PREC_FP32) {
         vx_launch<k_rhs_partial<float>, k_rhs_partial_body<float>>(L, grid, RHS_T, 0, v, S, pan, P, P32, w.rhs_part, rhs_chunks);

@@ -44,14 +44,17 @@ __global__ void k_cg_begin(VxScalars *S) {
 
 // Bounding box of the live particles and per-block sums of d (fixed grid:
 // the mean below is reproducible).
-VX_DEVK void k_cg_bbox_body(VxBlkB<CG_T, 0> vb, VxView v, VxScalars *S, double *red) {
+// Partition `part` of `nparts` (block-strided): its box into the running
+// minimum, its sum of d into red[part].
+__device__ __forceinline__ void cg_bbox_part(unsigned part, unsigned nparts, const VxView &v, VxScalars *S,
+                                             double *red) {
     __shared__ unsigned long long sk[4][CG_T];
     __shared__ double sd[CG_T];
     const long long n = S->n;
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
     double dsum = 0.0;
-    for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)vb.n * blockDim.x) {
+    for (long long i = part * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)nparts * blockDim.x) {
         const double x = v.x[i * v.ps], y = v.y[i * v.ps];
         k[0] = min(k[0], vx_dkey(x));
         k[1] = min(k[1], vx_dkey(-x));
@@ -71,12 +74,25 @@ VX_DEVK void k_cg_bbox_body(VxBlkB<CG_T, 0> vb, VxView v, VxScalars *S, double *
     }
     if (threadIdx.x == 0) {
         for (int q = 0; q < 4; ++q) atomicMin(&S->cb[q], sk[q][0]);
-        red[vb.x] = sd[0];
+        red[part] = sd[0];
     }
 }
-__global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double *red) {
+// The sum of d is split into nparts fixed partitions whatever the grid (a
+// partition past the last particle adds 0), so the mean spacing, and the
+// grid built from it, do not depend on the launch's grid.
+VX_DEVK void k_cg_bbox_body(VxBlkB<CG_T, 0> vb, VxView v, VxScalars *S, double *red, int nparts) {
+    const long long n = S->n;
+    for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) {
+        if ((long long)q * blockDim.x >= n) {
+            if (threadIdx.x == 0) red[q] = 0.0;
+            continue;
+        }
+        cg_bbox_part(q, (unsigned)nparts, v, S, red);
+    }
+}
+__global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double *red, int nparts) {
     VX_PDL_WAIT();
-    k_cg_bbox_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, v, S, red);
+    k_cg_bbox_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, v, S, red, nparts);
 }
 
 // Cell side h = c * mean(d) / CG_DIV, grown until the grid fits cells_cap.
@@ -176,7 +192,7 @@ __global__ void __launch_bounds__(CG_T) k_scan_sum(const long long *len_p, const
     k_scan_sum_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, len_p, cnt, csum);
 }
 
-VX_DEVK void k_scan_top_body(VxBlkB<0, 0> vb, const long long *len_p, const int *csum, long long *coff) {
+VX_DEVK void k_scan_top_body(VxBlkB<1024, 0> vb, const long long *len_p, const int *csum, long long *coff) {
     __shared__ long long sh[1024];
     __shared__ long long carry;
     const long long nch = vx_ceil_div(*len_p, VX_CHUNK);
@@ -199,9 +215,9 @@ VX_DEVK void k_scan_top_body(VxBlkB<0, 0> vb, const long long *len_p, const int 
         __syncthreads();
     }
 }
-__global__ void k_scan_top(const long long *len_p, const int *csum, long long *coff) {
+__global__ void __launch_bounds__(1024) k_scan_top(const long long *len_p, const int *csum, long long *coff) {
     VX_PDL_WAIT();
-    k_scan_top_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, len_p, csum, coff);
+    k_scan_top_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, len_p, csum, coff);
 }
 
 VX_DEVK void k_scan_apply_body(VxBlkB<CG_T, 0> vb, const long long *len_p, const int *cnt, const long long *coff,
@@ -259,7 +275,7 @@ __global__ void k_cg_gather(VxView v, const VxScalars *S, const int *sorted, con
 }
 
 // Exclusive scan of the per-row item counts (single block, runs per thread).
-VX_DEVK void k_cg_row_scan_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *in, long long *out) {
+VX_DEVK void k_cg_row_scan_body(VxBlkB<1024, 0> vb, const VxScalars *S, const int *in, long long *out) {
     __shared__ long long sh[1024];
     const long long len = S->cny;
     const long long per = vx_ceil_div(len, (long long)blockDim.x);
@@ -280,9 +296,9 @@ VX_DEVK void k_cg_row_scan_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *
         run += in[q];
     }
 }
-__global__ void k_cg_row_scan(const VxScalars *S, const int *in, long long *out) {
+__global__ void __launch_bounds__(1024) k_cg_row_scan(const VxScalars *S, const int *in, long long *out) {
     VX_PDL_WAIT();
-    k_cg_row_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, in, out);
+    k_cg_row_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, in, out);
 }
 
 // Work items: each row's sorted range cut into segments of CG_W targets.
@@ -696,8 +712,9 @@ cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, cons
                                       VxWork &w) {
     const int grid = L.num_sms * 4;
     vx_launch<k_cg_begin, k_cg_begin_body>(L, 1, 1, 0, S);
-    vx_launch<k_cg_bbox, k_cg_bbox_body>(L, VX_RED_BLOCKS, CG_T, 0, v, S, w.red);
-    vx_launch<k_cg_params, k_cg_params_body>(L, 1, CG_T, 0, S, w.red, VX_RED_BLOCKS, p.diff_cutoff, w.cells_cap);
+    const int nparts = std::min(vx_part_sms(L) * 4, VX_RED_BLOCKS);
+    vx_launch<k_cg_bbox, k_cg_bbox_body>(L, std::min(nparts, L.num_sms * 4), CG_T, 0, v, S, w.red, nparts);
+    vx_launch<k_cg_params, k_cg_params_body>(L, 1, CG_T, 0, S, w.red, nparts, p.diff_cutoff, w.cells_cap);
     vx_launch<k_cg_zero, k_cg_zero_body>(L, grid, CG_T, 0, S, w.cg_cnt);
     vx_launch<k_cg_cellid, k_cg_cellid_body>(L, grid, CG_T, 0, v, S, w.key0, w.val0, w.cg_cnt);
     vx_launch<k_scan_sum, k_scan_sum_body>(L, grid, CG_T, 0, &S->cncells, w.cg_cnt, w.cell_chunk_cnt);

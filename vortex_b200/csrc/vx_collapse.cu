@@ -156,7 +156,7 @@ __global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) 
     k_cell_chunk_sum_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt, csum);
 }
 
-VX_DEVK void k_cell_chunk_scan_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
+VX_DEVK void k_cell_chunk_scan_body(VxBlkB<1024, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
     if (S->col_done) return;
     __shared__ long long sh[1024];
     __shared__ long long carry;
@@ -180,9 +180,9 @@ VX_DEVK void k_cell_chunk_scan_body(VxBlkB<0, 0> vb, const VxScalars *S, const i
         __syncthreads();
     }
 }
-__global__ void k_cell_chunk_scan(const VxScalars *S, const int *csum, long long *coff) {
+__global__ void __launch_bounds__(1024) k_cell_chunk_scan(const VxScalars *S, const int *csum, long long *coff) {
     VX_PDL_WAIT();
-    k_cell_chunk_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
+    k_cell_chunk_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
 }
 
 VX_DEVK void k_cell_chunk_apply_body(VxBlkB<VX_THREADS, 0> vb, const VxScalars *S, const int *cnt,
@@ -295,7 +295,7 @@ __global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *celli
 
 // Rounds over the candidate list (single block).  cstate: 0 undecided,
 // 1 applied, 2 consumed before its turn.
-VX_DEVK void k_col_resolve_body(VxBlkB<0, 0> vb, VxScalars *S, const int *cand, const int *col, int *in_cnt,
+VX_DEVK void k_col_resolve_body(VxBlkB<1024, 0> vb, VxScalars *S, const int *cand, const int *col, int *in_cnt,
                                 int *has_app, int *first_app, int *cstate, int *cdec) {
     if (S->col_done) return;
     __shared__ int undecided;
@@ -337,10 +337,10 @@ VX_DEVK void k_col_resolve_body(VxBlkB<0, 0> vb, VxScalars *S, const int *cand, 
         S->col_done = 1;
     }
 }
-__global__ void k_col_resolve(VxScalars *S, const int *cand, const int *col, int *in_cnt,
+__global__ void __launch_bounds__(1024) k_col_resolve(VxScalars *S, const int *cand, const int *col, int *in_cnt,
                               int *has_app, int *first_app, int *cstate, int *cdec) {
     VX_PDL_WAIT();
-    k_col_resolve_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cand, col, in_cnt, has_app, first_app, cstate, cdec);
+    k_col_resolve_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, cand, col, in_cnt, has_app, first_app, cstate, cdec);
 }
 
 template <int PASS>

@@ -47,7 +47,7 @@ __global__ void k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt, const 
 }
 
 // Single block: exclusive scan of the chunk counts, m, scan[m] and H.
-VX_DEVK void k_cmp_scan_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
+VX_DEVK void k_cmp_scan_body(VxBlkB<1024, 0> vb, VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
                              const int *skip) {
     if (skip && *skip) return;
     __shared__ long long sh[1024];
@@ -95,10 +95,10 @@ VX_DEVK void k_cmp_scan_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, double eps
         S->c_H = m - scan_m;
     }
 }
-__global__ void k_cmp_scan(VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
+__global__ void __launch_bounds__(1024) k_cmp_scan(VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
                            const int *skip) {
     VX_PDL_WAIT();
-    k_cmp_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, eps, cnt, off, skip);
+    k_cmp_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, v, S, eps, cnt, off, skip);
 }
 
 // Per chunk: local scan, then hole positions, hole sources and tail sources.

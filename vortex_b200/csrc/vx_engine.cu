@@ -16,7 +16,7 @@
 #include <string>
 #include <vector>
 
-#include "vx_internal.cuh"
+#include "vx_sim.cuh"
 
 static thread_local std::string g_err;
 
@@ -53,54 +53,6 @@ extern "C" const char *vx_status_str(vx_status s) {
             return e_ == cudaErrorMemoryAllocation ? VX_ERR_NOMEM : VX_ERR_CUDA;            \
         }                                                                                   \
     } while (0)
-
-struct vx_sim {
-    vx_conf conf;
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t stream = nullptr;
-    int P = 0, P32 = 0;
-    VxParams prm;
-    vx_panel *d_pan = nullptr;
-    double *d_minv = nullptr;
-    double *d_minvT = nullptr;   // transposed copy read by the birth solve
-    int *d_wstart = nullptr, *d_widx = nullptr;   // wall panel lists per wall cell
-    int *d_hstart = nullptr, *d_hidx = nullptr;   // hitting-test panel lists per cell
-    long long wall_bytes = 0;
-    VxScalars *d_S = nullptr;
-    VxScalars *h_S = nullptr;     // pinned mirror
-    long long cap = 0;
-    double *x = nullptr, *y = nullptr, *g = nullptr, *vx = nullptr, *vy = nullptr, *d = nullptr;
-    VxWork w;
-    std::vector<void *> work_allocs;
-    long long n_upper = 0;
-    long long launches = 0;
-    // step graphs: a few instantiated shapes, least recently used evicted
-    // (the source count moves a shape key back and forth across a power of
-    // two; capacity growth drops them all)
-    bool use_graph = true;
-    struct StepGraph {
-        cudaGraphExec_t exec = nullptr;
-        int kv = -1, rhs = -1, sms = -1;
-        long long launches = 0, used = 0;
-    };
-    StepGraph graphs[4];
-    long long graph_clock = 0;
-    // timing
-    bool timing = false;
-    cudaEvent_t ev[6] = {};     // stage boundaries
-    cudaEvent_t pev[4] = {};    // around the two pair kernels
-    double t_acc[8] = {};
-    // probe scratch
-    double *d_probe = nullptr;
-    long long probe_cap = 0;
-    // moved-point scratch (vx_move_points): x, y, g, u, v; own scalars and
-    // block partials, so the body's force sums stay as they are
-    double *d_pts = nullptr;
-    long long pts_cap = 0;
-    VxScalars *d_St = nullptr;
-    double *d_pred = nullptr;
-};
 
 static VxLaunch launch_of(vx_sim *s) {
     VxLaunch L;
@@ -393,6 +345,14 @@ static int kv_for(vx_sim *s) {
     const int tile = s->prm.prec == VX_PREC_FP32 ? 1024 : 512;
     return vx_pick_ksplit(pow2_ceil(s->n_upper + s->P), tile, s->num_sms);
 }
+
+VxLaunch vx_sim_launch(vx_sim *s) { return launch_of(s); }
+long long vx_sim_need(vx_sim *s, long long n) { return need_for(s, n); }
+vx_status vx_sim_grow(vx_sim *s, long long need) { return grow(s, need); }
+vx_status vx_sim_read_scalars(vx_sim *s) { return read_scalars(s); }
+int vx_sim_step_sms(vx_sim *s) { return step_sms_for(s); }
+int vx_sim_kv(vx_sim *s) { return kv_for(s); }
+int vx_sim_rhs_chunks(vx_sim *s) { return rhs_chunks_for(s); }
 
 // ---------------------------------------------------------------------------
 // Wall panel lists: cells of side 5 L_max (1 % margin) over the birth-point
@@ -868,18 +828,23 @@ extern "C" vx_status vx_get_matrix(vx_sim *s, double *minv) {
 }
 
 // ---------------------------------------------------------------------------
-static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
+static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step, VxRecorder *rec = nullptr,
+                                 int share = 0) {
     VxLaunch L = launch_of(s);
     L.num_sms = step_sms_for(s);
+    L.part_sms = L.num_sms;     // result-defining partitions: the body's own size
+    if (share > 0) L.num_sms = std::min(share, L.num_sms);
     L.full_sms = s->num_sms;
+    L.rec = rec;
+    if (rec) L.launches = nullptr;
     VxView v = view_of(s);
     const VxParams &p = s->prm;
     cudaError_t e = cudaSuccess;
     const int kv = kv_for(s);
-    const bool rec = s->timing && !whole_step;
-    if (rec)
+    const bool timed = s->timing && !whole_step && !rec;
+    if (timed)
         for (int k = 0; k < 4; ++k) L.pair_ev[k] = s->pev[k];
-    auto ev = [&](int k) { if (rec) cudaEventRecord(s->ev[k], s->stream); };
+    auto ev = [&](int k) { if (timed) cudaEventRecord(s->ev[k], s->stream); };
     ev(0);
     if (mask & VX_STAGE_BIRTH) {
         if ((e = vx_launch_step_begin(L, s->d_S)) != cudaSuccess) return e;
@@ -914,8 +879,13 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step) {
     return e;
 }
 
+cudaError_t vx_sim_launch_stages(vx_sim *s, unsigned mask, bool whole_step, VxRecorder *rec, int share) {
+    return launch_stages(s, mask, whole_step, rec, share);
+}
+
 extern "C" vx_status vx_stage(vx_sim *s, unsigned mask) {
     if (!s) return VX_ERR_ARG;
+    if (s->in_batch) { vx_set_error("vx_stage: the body belongs to a batch (step it with vx_batch_step)"); return VX_ERR_ARG; }
     CU(cudaSetDevice(s->device));
     vx_status st = ensure_capacity(s);
     if (st != VX_OK) return st;
@@ -980,6 +950,7 @@ static vx_status step_once(vx_sim *s) {
 
 extern "C" vx_status vx_step(vx_sim *s, int64_t nsteps) {
     if (!s || nsteps < 0) return VX_ERR_ARG;
+    if (s->in_batch) { vx_set_error("vx_step: the body belongs to a batch (step it with vx_batch_step)"); return VX_ERR_ARG; }
     CU(cudaSetDevice(s->device));
     for (int64_t k = 0; k < nsteps; ++k) {
         vx_status st = step_once(s);

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, cons
     k_fmm_scan_sum_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, S, cnt, csum);
 }
 
-VX_DEVK void k_fmm_scan_top_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
+VX_DEVK void k_fmm_scan_top_body(VxBlkB<1024, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
     __shared__ long long sh[1024];
     __shared__ long long carry;
     const long long nch = vx_ceil_div(S->fnleaves, VX_CHUNK);
@@ -203,9 +203,9 @@ VX_DEVK void k_fmm_scan_top_body(VxBlkB<0, 0> vb, const VxScalars *S, const int 
         __syncthreads();
     }
 }
-__global__ void k_fmm_scan_top(const VxScalars *S, const int *csum, long long *coff) {
+__global__ void __launch_bounds__(1024) k_fmm_scan_top(const VxScalars *S, const int *csum, long long *coff) {
     VX_PDL_WAIT();
-    k_fmm_scan_top_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
+    k_fmm_scan_top_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
 }
 
 VX_DEVK void k_fmm_scan_apply_body(VxBlkB<FMM_T, 0> vb, const VxScalars *S, const int *cnt, const long long *coff,
@@ -886,7 +886,7 @@ __global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_i
     k_fmm_row_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items);
 }
 
-VX_DEVK void k_fmm_row_scan_body(VxBlkB<0, 0> vb, VxScalars *S, const int *in, long long *out, long long items_cap) {
+VX_DEVK void k_fmm_row_scan_body(VxBlkB<1024, 0> vb, VxScalars *S, const int *in, long long *out, long long items_cap) {
     __shared__ long long sh[1024];
     const long long len = 1LL << S->fL;
     const long long per = vx_ceil_div(len, (long long)blockDim.x);
@@ -909,9 +909,9 @@ VX_DEVK void k_fmm_row_scan_body(VxBlkB<0, 0> vb, VxScalars *S, const int *in, l
         S->cnitems = run <= items_cap ? run : items_cap;
     }
 }
-__global__ void k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
+__global__ void __launch_bounds__(1024) k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
     VX_PDL_WAIT();
-    k_fmm_row_scan_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, in, out, items_cap);
+    k_fmm_row_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, in, out, items_cap);
 }
 
 VX_DEVK void k_fmm_items_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, const int *row_items, const long long *off,

@@ -404,6 +404,12 @@ struct VxLaunch {
     // grid (the birth far field's per-block partials).
     int num_sms;
     int full_sms = 0;
+    // SMs the result-defining partitions of a body are sized for (0:
+    // num_sms): the force sums, the diffusion grid's mean spacing and the
+    // birth far field's partial sums split the particles into partitions
+    // whose number follows the body's size, not the grid of the launch, so
+    // a body gets the same results whatever share of the GPU it runs on.
+    int part_sms = 0;
     // optional events recorded around the Biot-Savart and diffusion pair
     // kernels: [0,1] Biot-Savart, [2,3] diffusion (null: not recorded)
     cudaEvent_t pair_ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -412,6 +418,7 @@ struct VxLaunch {
     VxKernelTimer *kt = nullptr;
 };
 inline int vx_full_sms(const VxLaunch &L) { return L.full_sms > 0 ? L.full_sms : L.num_sms; }
+inline int vx_part_sms(const VxLaunch &L) { return L.part_sms > 0 ? L.part_sms : L.num_sms; }
 #define VX_EV(L, k) do { if ((L).pair_ev[k] && !(L).rec) cudaEventRecord((L).pair_ev[k], (L).stream); } while (0)
 
 // Launch kernel K (the __global__ wrapper of body DEV) for one body: with

@@ -1,10 +1,12 @@
 """Many bodies on one GPU: the batched run and the served run.
 
 Batched: a seeded population of bodies (workloads.body_spec) advanced
-together with vx_step_many: every step is launched on all bodies' streams
-before the next, so their kernels overlap on the device.  The batched step is
-timed on the device: a start event on a main stream that every body stream
-waits for, and an end event after the main stream waited for every body.
+together.  Default form (mode "graph", vx_batch): each kernel of the step
+runs once for all bodies and the batched step is one CUDA graph; the step is
+timed by events on the batch's stream.  Mode "streams" (vx_step_many): every
+body's own step graph launched on its own stream before the next step, timed
+from a start event every body stream waits for to an end event after the
+main stream waited for every body.
 
 Served: requests drawn from the same population arrive as a Poisson process;
 each asks for a number of steps; the vx_server loop admits them by slot and
@@ -68,16 +70,10 @@ def combine_serve(parts: list) -> dict:
     return out
 
 
-def _event_pair():
-    import torch
-    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-
 def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7,
-              precision: int = N.PREC_FP32, device: int = 0, rank: int = 0, world: int = 1) -> dict:
+              precision: int = N.PREC_FP32, device: int = 0, rank: int = 0, world: int = 1,
+              mode: str = "graph") -> dict:
     """The batched run of this rank's share of `bodies` seeded bodies."""
-    import torch
-    torch.cuda.set_device(device)
     specs = [wl.body_spec(seed, i) for i in share(bodies, rank, world)]
     bodies = len(specs)
     sims = []
@@ -88,34 +84,48 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
         s.set_particles(x, y, g)
         sims.append(s)
     setup_s = time.perf_counter() - t0
-    N.step_many(sims, warmup)
-    for s in sims:
-        s.sync()
-    streams = [torch.cuda.ExternalStream(s.stream(), device=f"cuda:{device}") for s in sims]
-    main = torch.cuda.current_stream(device)
+    batch = N.Batch(sims) if mode == "graph" else None
+    if batch:
+        batch.step(warmup)
+        batch.sync()
+        stream = batch.stream()
+    else:
+        N.step_many(sims, warmup)
+        for s in sims:
+            s.sync()
+        stream = 0
     counts0 = np.array([s.count() for s in sims], dtype=np.float64)
-    ms, inter = [], 0.0
-    launches0 = sum(s.launches() for s in sims)
+    ms = []
+    launches0 = batch.info()["kernels"] if batch else sum(s.launches() for s in sims)
     for _ in range(steps):
-        a, b = _event_pair()
-        a.record(main)
-        for st in streams:
-            st.wait_event(a)
-        N.step_many(sims, 1)
-        for st in streams:
-            e = torch.cuda.Event()
-            e.record(st)
-            main.wait_event(e)
-        b.record(main)
-        b.synchronize()
-        ms.append(a.elapsed_time(b))
+        a, b = N.Event(), N.Event()
+        if batch:
+            a.record(stream)
+            batch.step(1)
+            b.record(stream)
+        else:
+            a.record(stream)
+            for s in sims:
+                N.wait_event(s.stream(), a)
+            N.step_many(sims, 1)
+            for s in sims:
+                e = N.Event()
+                e.record(s.stream())
+                N.wait_event(stream, e)
+            b.record(stream)
+        ms.append(a.elapsed_ms(b))
+    if batch:
+        batch.sync()
     counts1 = np.array([s.count() for s in sims], dtype=np.float64)
-    launches = sum(s.launches() for s in sims) - launches0
+    launches = (batch.info()["kernels"] if batch else sum(s.launches() for s in sims)) - launches0
+    info = batch.info() if batch else None
     nmean = 0.5 * (counts0 + counts1)
     inter = float(np.sum(nmean * nmean))          # direct-sum equivalent pairs per batched step
     total_s = sum(ms) * 1e-3
     out = {"bodies": bodies, "steps": steps, "warmup": warmup, "seed": seed,
            "precision": "fp32" if precision == N.PREC_FP32 else "fp64",
+           "mode": ("one launch per kernel of the step for all bodies, the batched step one CUDA graph (vx_batch)"
+                    if batch else "every body's own step graph on its own stream (vx_step_many)"),
            "particles_start": int(counts0.sum()), "particles_end": int(counts1.sum()),
            "panels_total": int(sum(sp["panels"] for sp in specs)),
            "batched_steps_per_s": steps / total_s, "body_steps_per_s": bodies * steps / total_s,
@@ -123,7 +133,11 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
            "ms_p99": float(np.percentile(ms, 99)),
            "particle_steps_per_s": float(nmean.sum()) * steps / total_s,
            "interactions_per_s_effective": inter * steps / total_s,
-           "gpu_launches": int(launches), "setup_s": setup_s}
+           "gpu_launches": int(launches), "kernels_per_batched_step": launches / steps, "setup_s": setup_s}
+    if info:
+        out["graph_instantiations"] = info["graph_instantiations"]
+        out["slot_table_rebuilds"] = info["rebuilds"]
+        batch.close()
     for s in sims:
         s.close()
     return out
@@ -180,10 +194,11 @@ def main():
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--mode", default="graph", choices=["graph", "streams"])
     a = ap.parse_args()
     prec = N.PREC_FP32 if a.precision == "fp32" else N.PREC_FP64
     if a.mode == "batch":
-        print(json.dumps(run_batch(a.bodies, a.steps, a.warmup, precision=prec)))
+        print(json.dumps(run_batch(a.bodies, a.steps, a.warmup, precision=prec, mode=a.mode)))
     else:
         print(json.dumps(run_serve(a.requests, a.rate, precision=prec)))
 

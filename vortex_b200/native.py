@@ -62,6 +62,8 @@ def lib():
         _lib.vx_status_str.restype = C.c_char_p
         _lib.vx_get_stream.restype = C.c_void_p
         _lib.vx_get_stream.argtypes = [C.c_void_p]
+        _lib.vx_batch_stream.restype = C.c_void_p
+        _lib.vx_batch_stream.argtypes = [C.c_void_p]
         for name in ("vx_create",):
             getattr(_lib, name).argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
     return _lib
@@ -300,6 +302,103 @@ def step_many(sims, nsteps: int = 1):
     """Advance several bodies together (their kernels overlap); asynchronous."""
     arr = (C.c_void_p * len(sims))(*[s.h.value for s in sims])
     _check(lib().vx_step_many(arr, C.c_int(len(sims)), C.c_int64(nsteps)), "vx_step_many")
+
+
+_rt = None
+
+
+def cudart():
+    """The CUDA runtime the library itself links (for events and streams)."""
+    global _rt
+    if _rt is None:
+        lib()
+        _rt = C.CDLL("libcudart.so.12")
+        _rt.cudaEventCreate.argtypes = [C.POINTER(C.c_void_p)]
+        _rt.cudaEventRecord.argtypes = [C.c_void_p, C.c_void_p]
+        _rt.cudaEventSynchronize.argtypes = [C.c_void_p]
+        _rt.cudaEventElapsedTime.argtypes = [C.POINTER(C.c_float), C.c_void_p, C.c_void_p]
+        _rt.cudaEventDestroy.argtypes = [C.c_void_p]
+        _rt.cudaStreamWaitEvent.argtypes = [C.c_void_p, C.c_void_p, C.c_uint]
+    return _rt
+
+
+class Event:
+    """A CUDA event with timing (device time between two records)."""
+
+    def __init__(self):
+        self.e = C.c_void_p()
+        if cudart().cudaEventCreate(C.byref(self.e)) != 0:
+            raise VxError("cudaEventCreate failed")
+
+    def record(self, stream: int = 0):
+        if cudart().cudaEventRecord(self.e, C.c_void_p(stream)) != 0:
+            raise VxError("cudaEventRecord failed")
+
+    def synchronize(self):
+        if cudart().cudaEventSynchronize(self.e) != 0:
+            raise VxError("cudaEventSynchronize failed")
+
+    def elapsed_ms(self, end: "Event") -> float:
+        end.synchronize()
+        t = C.c_float(0.0)
+        if cudart().cudaEventElapsedTime(C.byref(t), self.e, end.e) != 0:
+            raise VxError("cudaEventElapsedTime failed")
+        return float(t.value)
+
+    def __del__(self):
+        try:
+            if self.e:
+                cudart().cudaEventDestroy(self.e)
+        except Exception:
+            pass
+
+
+def wait_event(stream: int, ev: Event):
+    if cudart().cudaStreamWaitEvent(C.c_void_p(stream), ev.e, 0) != 0:
+        raise VxError("cudaStreamWaitEvent failed")
+
+
+class Batch:
+    """Bodies of one device advanced together (vx_batch): one launch per
+    kernel of the step for all bodies, the batched step one CUDA graph."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (C.c_void_p * len(self.sims))(*[s.h.value for s in self.sims])
+        self.h = C.c_void_p()
+        _check(lib().vx_batch_create(arr, C.c_int(len(self.sims)), C.byref(self.h)), "vx_batch_create")
+
+    def step(self, nsteps: int = 1):
+        _check(lib().vx_batch_step(self.h, C.c_int64(nsteps)), "vx_batch_step")
+
+    def sync(self):
+        _check(lib().vx_batch_sync(self.h), "vx_batch_sync")
+
+    def stream(self) -> int:
+        return lib().vx_batch_stream(self.h) or 0
+
+    def info(self) -> dict:
+        o = np.zeros(6)
+        _check(lib().vx_batch_info(self.h, _p(o)), "vx_batch_info")
+        return {"steps": int(o[0]), "kernels": int(o[1]), "kernels_per_step": int(o[2]), "rebuilds": int(o[3]),
+                "graph_instantiations": int(o[4]), "bodies": int(o[5])}
+
+    def close(self):
+        if self.h:
+            lib().vx_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class Server:
