@@ -103,6 +103,64 @@ def job_time_ms(local_ms: float, dist: bool, device: int = 0) -> float:
     return float(t.item())
 
 
+def workload_config(args, world: int) -> dict:
+    """The workload both arms run (identical in both JSON lines)."""
+    return {"workload": "cylinder R=0.5, 1000 panels, Re=2000 (nu=5e-4), dt=0.002, core radius = panel length, "
+                        f"seeded warm wake N0={args.n} vortices per GPU; one step = birth, Biot-Savart + "
+                        "3-nearest, vortex and wall diffusion, convection with absorption, force sums, compaction, "
+                        "collapse",
+            "panels": P_PANELS, "n_particles_start": args.n,
+            "l2": "our arm: flushed between timed steps (256 MiB write); reference arm: host caches",
+            "parallelism": f"{world} independent bodies (one per GPU)"}
+
+
+# Algorithmic DRAM bytes per particle of the memory-bound kernels of a step
+# (FP64 SoA state, 4-byte keys and indices, float4 sorted copies); the
+# pair kernels are compute-bound and reported in `roofline`.
+HBM_BYTES = {
+    "k_advect": (64, "read x, y, G, Vx, Vy; write x, y, G"),
+    "k_fmm_bbox": (16, "read x, y"),
+    "k_fmm_leafid": (24, "read x, y; write leaf key and index"),
+    "k_cg_bbox": (24, "read x, y, d"),
+    "k_cg_cellid": (24, "read x, y; write cell key and index"),
+    "k_bk_place": (12, "read key; write key and index at the bucket slot"),
+    "k_bk_order": (8, "read and write the bucket's indices"),
+    "k_fmm_gather": (48, "read order index and key, x, y, G; write float4"),
+    "k_cg_gather": (56, "read order index and key, x, y, G, d; write float4"),
+    "k_fmm_p2m": (16, "read float4 source"),
+    "k_col_query<2>": (28, "read x, y, G; write COL"),
+    "k_col_query<1>": (28, "read x, y, G; write COL"),
+    "k_cmp_count": (8, "read G"),
+    "k_cmp_classify": (8, "read G"),
+}
+
+
+def roofline_hbm(kt: dict, steps: int, n: float, peak_gbs: float) -> list:
+    """Per-kernel achieved DRAM bandwidth of the memory-bound passes from the
+    per-kernel event times of `steps` instrumented steps at about n vortices."""
+    out = []
+    for name, (ms, launches) in kt.items():
+        if name not in HBM_BYTES or ms <= 0:
+            continue
+        bpp, what = HBM_BYTES[name]
+        b = bpp * n * launches / steps
+        t = ms / steps
+        gbs = b / (t * 1e-3) / 1e9
+        out.append({"kernel": name, "launches_per_step": launches / steps, "ms_per_step": t,
+                    "bytes_per_step": b, "bytes_per_particle": bpp, "bytes_counted": what,
+                    "achieved_gbs": gbs, "frac": gbs / peak_gbs})
+    out.sort(key=lambda r: -r["ms_per_step"])
+    return out
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except (OSError, ValueError):
+        return {}
+
+
 def pinned(n, rt):
     p = C.c_void_p()
     if rt.cudaHostAlloc(C.byref(p), C.c_size_t(max(8 * n, 8)), 0) != 0:
@@ -195,6 +253,10 @@ def run_ours(args, rank, world, device):
     }
     kname, (kms, kpairs, kflop) = max(kernels.items(), key=lambda kv: kv[1][0])
     tree = sim.tree_info()
+    # per-kernel device times of three further instrumented steps (the
+    # memory-bound passes' bandwidth)
+    n_kt = sim.count()
+    kt = sim.kernel_times(3)
     # ---- end to end through the C ABI with host buffers -------------------
     rt = C.CDLL("libcudart.so.12")
     n_now = sim.count()
@@ -236,12 +298,18 @@ def run_ours(args, rank, world, device):
         fp64 = {"steps_per_s": 1e3 * len(ms64) / sum(ms64), "ms_per_step": float(np.mean(ms64)),
                 "bs_pair_kernel_ms": t64[5] / len(ms64), "diffusion_pair_kernel_ms": t64[6] / len(ms64),
                 "form": "direct O(N^2) sums in FP64"}
-    peak32 = Nt.measure_peak(device, fp64=False)
+    peak32_scalar = Nt.measure_peak(device, fp64=False)
+    peak32_packed = Nt.measure_peak(device, mode=2)   # fma.rn.f32x2, two FMAs per instruction
+    peak32 = max(peak32_scalar, peak32_packed)
     mufu = Nt.measure_peak(device, mode=3)        # 1e12 (rsqrt + ex2) units per second
     multi = multibody_runs(args, device, rank, world) if args.multibody else None
     if rank != 0:
         return None
     value = world * 1e3 * K / total_ms
+    mp = measured_peaks()
+    hbm_peak = float(mp.get("hbm_gbs") or 6650.0)
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (copy bandwidth measured on this pool)" if mp.get("hbm_gbs") else \
+        "fallback 6.65 TB/s (earlier measurement on this pool)"
     eff = float(np.mean([n * ((n + 31) // 32 * 32) for n in nvec]))
     achieved = kflop * kpairs / (kms * 1e-3) / 1e12
     traffic = None
@@ -263,16 +331,14 @@ def run_ours(args, rank, world, device):
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic (seeded warm wake on a jittered lattice; generated circle profile)",
-        "config": {"workload": "cylinder R=0.5, 1000 panels, Re=2000 (nu=5e-4), dt=0.002, "
-                               f"warm wake N0={args.n} per GPU, FP32-bulk form",
-                   "panels": P_PANELS, "n_particles_start": args.n, "n_particles_end": int(n_end),
-                   "precision": "fp32 pair sums, fp64 expansions/panel solve/forces/positions",
-                   "l2": "flushed between timed steps (256 MiB write)",
-                   "launch": "each timed step replays the step's CUDA graph (vx_step, as a user's call does)",
-                   "biot_savart": (f"autotuned before timing: {tuned['form']}"
-                                   + (f", {tuned['leaf']} vortices per leaf" if tuned and tuned['leaf'] else "")
-                                   if tuned else "FMM, 32 vortices per leaf (default)"),
-                   "parallelism": f"{world} independent bodies (one per GPU)"},
+        "config": workload_config(args, world),
+        "run": {"n_particles_end": int(n_end),
+                "form": "FP32-bulk: FP32 pair sums with FP64 accumulation, FP64 expansions, panel solve, forces "
+                        "and positions",
+                "launch": "each timed step replays the step's CUDA graph (vx_step, as a user's call does)",
+                "biot_savart": (f"autotuned before timing: {tuned['form']}"
+                                + (f", {tuned['leaf']} vortices per leaf" if tuned and tuned['leaf'] else "")
+                                if tuned else "FMM, 32 vortices per leaf (default)")},
         "particle_interactions_per_s": {"effective": world * eff * 1e3 * K / total_ms,
                                         "executed": world * (pc[0] + pc[1]) / (total_ms * 1e-3),
                                         "effective_definition": "N_targets x N_sources per step (direct-sum equivalent)",
@@ -287,7 +353,9 @@ def run_ours(args, rank, world, device):
         "speedup_fp32_over_fp64": (value / world) / fp64["steps_per_s"] if fp64 else None,
         "roofline": {"kernel": kname, "bound": "fp32-simt", "achieved": achieved, "peak": peak32,
                      "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": traffic,
-                     "peak_source": "measured FP32 FMA throughput of this GPU (vx_measure_peak)",
+                     "peak_source": "measured FP32 FMA throughput of this GPU (vx_measure_peak), the larger of "
+                                    "scalar FMA and packed f32x2 FMA",
+                     "peak_fp32_scalar": peak32_scalar, "peak_fp32_packed": peak32_packed,
                      "flop_per_pair": kflop, "pairs_per_launch": kpairs, "launch_ms": kms,
                      "mufu_ceiling": ({"bound": "special-function pipe (one rsqrt + one ex2 per pair)",
                                        "achieved_tpairs_per_s": kpairs / (kms * 1e-3) / 1e12,
@@ -296,6 +364,11 @@ def run_ours(args, rank, world, device):
                                        "peak_source": "measured rsqrt+ex2 throughput of this GPU "
                                                       "(vx_measure_peak mode 3)"}
                                       if kname.startswith("k_diff_cells") else None)},
+        "roofline_hbm": {"peak_gbs": hbm_peak, "peak_source": hbm_src,
+                         "n_particles": n_kt,
+                         "timing": "3 instrumented steps, an event pair around every kernel (about 1 us of event "
+                                   "overhead in each time)",
+                         "kernels": roofline_hbm(kt, 3, n_kt, hbm_peak)},
         "e2e": {"value": e2e_steps / sum(e2e_t), "unit": "steps/s",
                 "h2d_bytes_per_step": bi // e2e_steps, "d2h_bytes_per_step": bo // e2e_steps},
         "gpu_launches": int(launches),
@@ -317,7 +390,12 @@ def multibody_runs(args, device, rank, world):
     from vortex_b200 import multibody as MB
     from vortex_b200 import native as Nt
     batched = MB.run_batch(bodies=args.batch_bodies, steps=args.batch_steps, warmup=3, device=device,
-                           rank=rank, world=world)
+                           rank=rank, world=world, mode="graph")
+    # the same population as concurrent per-body step graphs, for comparison
+    streams = MB.run_batch(bodies=args.batch_bodies, steps=3, warmup=2, device=device, rank=rank, world=world,
+                           mode="streams")
+    batched["per_body_streams"] = {k: streams[k] for k in ("mode", "ms_per_batched_step", "body_steps_per_s",
+                                                           "particle_steps_per_s", "kernels_per_batched_step")}
     sub32 = MB.run_batch(bodies=16, steps=2, warmup=1, device=device, rank=rank, world=world)
     sub64 = MB.run_batch(bodies=16, steps=2, warmup=1, precision=Nt.PREC_FP64, device=device, rank=rank,
                          world=world)
@@ -454,16 +532,23 @@ def run_reference(args, rank, world):
     x, y, g = wl.warm_wake(args.n, seed=1234)
     for _ in range(args.warmup):
         cpu_sample(x, y, g, pan, args.ref_targets, 16)
+    t0 = time.perf_counter()
     est = [cpu_sample(x, y, g, pan, args.ref_targets, 16)[0] for _ in range(args.steps)]
+    measured_s = time.perf_counter() - t0
     step_s = float(np.mean(est))
+    # each timed "step" is a bounded sample of one step: the sampled targets'
+    # pair sums and 16 panels' birth sums, extrapolated to the full step
+    frac = measured_s / args.steps / step_s
     v = 1.0 / step_s
     return {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded warm wake on a jittered lattice)",
-            "config": {"workload": "cylinder R=0.5, 1000 panels, Re=2000 (nu=5e-4), dt=0.002, "
-                                   f"warm wake N0={args.n} per GPU, FP32-bulk form",
-                       "panels": P_PANELS, "n_particles_start": args.n},
+            "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic (seeded warm wake on a jittered lattice; generated circle profile)",
+            "config": workload_config(args, world),
             "impl": "reference",
+            "extrapolated": True,
+            "measured_s": measured_s,
+            "sample_fraction_of_step": frac,
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": O.lib().vxo_num_threads(), "kind": "port",
                              "sample": f"each step: oracle FP64 (OpenMP) Biot-Savart+3-nearest and diffusion "
                                        f"for {args.ref_targets} targets over all {args.n} sources, birth RHS "
@@ -482,14 +567,14 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--cpu-targets", type=int, default=2048)
     ap.add_argument("--ref-targets", type=int, default=1024)
-    ap.add_argument("--ref-cuda-steps", type=int, default=0,
+    ap.add_argument("--ref-cuda-steps", type=int, default=3,
                     help="also time the reference's own CUDA build for this many steps (0: off)")
     ap.add_argument("--ref-cuda-timeout", type=float, default=900.0)
     ap.add_argument("--no-autotune", action="store_true", help="skip the untimed autotuning before timing")
-    ap.add_argument("--multibody", action="store_true",
-                    help="also run the seeded multi-body population batched and served")
+    ap.add_argument("--no-multibody", dest="multibody", action="store_false",
+                    help="skip the seeded multi-body population batched and served")
     ap.add_argument("--batch-bodies", type=int, default=256)
-    ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--serve-requests", type=int, default=32)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

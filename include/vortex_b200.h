@@ -101,7 +101,8 @@ typedef struct vx_conf {
                                    rule, partial pivoting if it fails */
     int32_t fmm_leaf;           /* quadtree depth: mean vortices per leaf
                                    the depth aims at (default 32) */
-    int32_t pad3_;
+    int32_t fmm_p;              /* expansion terms of the quadtree FMM: 8, 12, 16
+                                   or 20 (0: 16) */
 } vx_conf;
 
 typedef struct vx_sim vx_sim;
@@ -290,8 +291,21 @@ vx_status vx_eval_bucket_order(const unsigned *key, int64_t n, int64_t nb, int *
 /* Number of kernels this handle has launched since creation. */
 vx_status vx_get_launch_count(vx_sim *sim, int64_t *count);
 
+/* Instrumentation (no counterpart in the reference): run nsteps steps
+ * stage by stage with an event pair around every kernel launch and report
+ * each kernel's total device time and launches.  names receives the
+ * kernels' names, '\n'-separated (names_cap bytes, NUL-terminated); ms[k] and
+ * counts[k] belong to the k-th name; *nkernels is the number of distinct
+ * kernels (at most cap are written).  The events keep consecutive kernels
+ * from overlapping and add about a microsecond to each time. */
+vx_status vx_kernel_times(vx_sim *sim, int64_t nsteps, char *names, int64_t names_cap, double *ms,
+                          int64_t *counts, int64_t cap, int64_t *nkernels);
+
 /* Block until the handle's device work is done; reports device error flags. */
 vx_status vx_sync(vx_sim *sim);
+/* Expansion terms of the bulk form's quadtree FMM (8, 12, 16 or 20; the
+ * autotuner's third knob); the step graph is re-captured. */
+vx_status vx_set_fmm_order(vx_sim *sim, int p);
 /* The CUDA stream (cudaStream_t) the handle launches on. */
 void *vx_get_stream(vx_sim *sim);
 

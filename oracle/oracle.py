@@ -143,6 +143,14 @@ def diffusion(p, x, y, g, n, d, vx, vy):
     return vx, vy
 
 
+def diffusion_sums(p, x, y, g, n, d):
+    """(I1, A1) of every target: the diffusion sum and its magnitude sum."""
+    x, y, g, d = _f64(x), _f64(y), _f64(g), _f64(d)
+    I1, A1 = np.zeros(n), np.zeros(n)
+    lib().vxo_diffusion_sums(C.byref(p), _p(x), _p(y), _p(g), C.c_int64(n), _p(d), _p(I1), _p(A1))
+    return I1, A1
+
+
 def wall_diffusion(p, pan, x, y, n, d, vx, vy):
     vx, vy = _f64(vx).copy(), _f64(vy).copy()
     x, y, d = _f64(x), _f64(y), _f64(d)

@@ -383,6 +383,31 @@ static void wall_integral_f(float Ra0, float Ra1, float Rb0, float Rb1, float N0
     *R0 = s0; *R30 = s30; *R31 = s31;
 }
 
+/* The vortex-diffusion sums of each target in FP64 (the loop of
+ * vxo_diffusion, src/kernel.cu:985-1029): I1 = sum G_j e^(-r/d_i) and its
+ * magnitude sum A1 = sum |G_j| e^(-r/d_i).  A1 / |I1| is the cancellation
+ * factor of I1, |I1| against 1e-5 the reference's switch of the term. */
+void vxo_diffusion_sums(const vxo_params *p, const double *x, const double *y, const double *g,
+                        int64_t n, const double *d, double *I1o, double *A1o) {
+    const double thr = 0.001 * p->eps;
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < n; ++i) {
+        const double a0 = x[i], a1 = y[i], dd = d[i];
+        double I1 = 0.0, A1 = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            double dx = a0 - x[j], dy = a1 - y[j];
+            double dist = sqrt(fma(dx, dx, dy * dy));
+            if (dist > thr) {
+                double e = exp(-dist / dd);
+                I1 = fma(g[j], e, I1);
+                A1 = fma(fabs(g[j]), e, A1);
+            }
+        }
+        I1o[i] = I1;
+        A1o[i] = A1;
+    }
+}
+
 /* Wall diffusive velocity: src/kernel.cu:1031-1088 (diffusion_2_Kernel). */
 void vxo_wall_diffusion(const vxo_params *p, const vxo_panel *pan, int64_t P,
                         const double *x, const double *y, int64_t n, const double *d,

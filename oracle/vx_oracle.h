@@ -96,6 +96,8 @@ void vxo_diffusion_targets(const vxo_params *p, const double *x, const double *y
 /* ---- diffusive velocities (src/kernel.cu:985-1088, 1300-1346) ---- */
 void vxo_diffusion(const vxo_params *p, const double *x, const double *y, const double *g,
                    int64_t n, const double *d, double *vx, double *vy);
+void vxo_diffusion_sums(const vxo_params *p, const double *x, const double *y, const double *g,
+                        int64_t n, const double *d, double *I1, double *A1);
 void vxo_wall_diffusion(const vxo_params *p, const vxo_panel *pan, int64_t P,
                         const double *x, const double *y, int64_t n, const double *d,
                         double *vx, double *vy);

@@ -11,7 +11,10 @@ Workloads: the 200-panel circle of radius 0.5 (generated by
 vortex_b200.profiles.circle), core radius = panel length, U = (1, 0),
 nu = 1e-3, dt = 0.005, with the reference's own birth placement and 1e-12
 removal threshold; "cfg1" has same-sign collapse only (ratio 0.3), "mixed"
-also merges opposite signs (ratio 0.5) and caps merged strength at 0.05.
+also merges opposite signs (ratio 0.5) and caps merged strength at 0.05;
+"krug1000" is the 1000-panel circle of the cylinder benchmark (the layout of
+the reference's profiles/Profile_file_krug_1000.txt), nu = 5e-4, dt = 0.002,
+same-sign collapse only.
 Per recorded step k the file holds pre_pos, born_pos, vel, d, post_pos
 (slots [0, s), s = n rounded up to 32 after birth), pre/post counts and the
 post-step (d_g, Fx, Fy, M), plus probe velocities at 500 points.
@@ -31,21 +34,21 @@ sys.path.insert(0, ROOT)
 from oracle import refdrv  # noqa: E402
 from vortex_b200 import profiles  # noqa: E402
 
-P = 200
-EPS = 2 * math.pi * 0.5 / P
 BASE = dict(dt=0.005, viscosity=1e-3, rho=1.0, v_inf_x=1.0, v_inf_y=0.0, x_min=-2.0, x_max=10.0,
-            y_min=-10.0, y_max=10.0, ve_size=EPS, n_of_points=20, n_col=2, rc_x=0.0, rc_y=0.0,
+            y_min=-10.0, y_max=10.0, n_of_points=20, n_col=2, rc_x=0.0, rc_y=0.0,
             inc_step=8192)
-RUNS = {
-    "cfg1": (dict(r_col_diff_sign=0.0, r_col_same_sign=0.3, max_ve_g=1e30), 30, (1, 4, 30)),
-    "mixed": (dict(r_col_diff_sign=0.5, r_col_same_sign=0.3, max_ve_g=0.05), 20, (2, 20)),
+RUNS = {   # panels, conf overrides, steps, recorded steps
+    "cfg1": (200, dict(r_col_diff_sign=0.0, r_col_same_sign=0.3, max_ve_g=1e30), 30, (1, 4, 30)),
+    "mixed": (200, dict(r_col_diff_sign=0.5, r_col_same_sign=0.3, max_ve_g=0.05), 20, (2, 20)),
+    "krug1000": (1000, dict(dt=0.002, viscosity=5e-4, r_col_diff_sign=0.0, r_col_same_sign=0.3, max_ve_g=1e30),
+                 6, (2, 6)),
 }
 
 
 def run(name, out_dir):
-    extra, steps, rec = RUNS[name]
+    P, extra, steps, rec = RUNS[name]
     pan = profiles.circle(P)
-    conf = dict(BASE, **extra)
+    conf = dict(BASE, ve_size=2 * math.pi * 0.5 / P, **extra)
     bb = profiles.profile_bbox(pan, (conf["x_min"], conf["x_max"], conf["y_min"], conf["y_max"]))
     conf.update(profile_x_min=bb[0], profile_x_max=bb[1], profile_y_min=bb[2], profile_y_max=bb[3])
     cap = refdrv.round32(P * steps + P) + 256

@@ -62,3 +62,57 @@ def rel_err(a, b, scale=None):
     a, b = np.asarray(a), np.asarray(b)
     s = scale if scale is not None else max(np.abs(b).max(), 1e-300)
     return float(np.abs(a - b).max() / s) if a.size else 0.0
+
+
+def inside_polygon(px, py, pan):
+    """Even-odd test of points against the closed polygon of the panels'
+    left endpoints."""
+    x0, y0 = pan["left"][:, 0], pan["left"][:, 1]
+    x1, y1 = pan["right"][:, 0], pan["right"][:, 1]
+    inside = np.zeros(len(px), dtype=bool)
+    for a in range(0, len(px), 4096):
+        X = px[a:a + 4096, None]
+        Y = py[a:a + 4096, None]
+        crosses = (y0[None, :] > Y) != (y1[None, :] > Y)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            xc = x0[None, :] + (Y - y0[None, :]) * (x1 - x0)[None, :] / (y1 - y0)[None, :]
+        inside[a:a + 4096] = np.logical_xor.reduce(crosses & (X < xc), axis=1)
+    return inside
+
+
+def scale_body(name):
+    """The configurations' own bodies: the 1000-panel cylinder (the
+    benchmark's; Re 2000, dt 0.002) and the 2576-panel rounded plate of
+    chord 1 turned to 20 degrees of incidence (Re 1e4, dt 0.001); core
+    radius = mean panel length, same-sign collapse within 0.3 eps."""
+    if name == "circle1000":
+        pan = profiles.circle(1000)
+        ck = conf_kwargs(1000, dt=0.002, viscosity=5e-4)
+    elif name == "plate2576":
+        pan = profiles.rotate(profiles.rounded_plate(2576), 20.0)
+        ck = conf_kwargs(2576, dt=0.001, viscosity=1e-4, ve_size=float(pan["length"].mean()))
+    else:
+        raise ValueError(name)
+    return pan, ck
+
+
+def body_cloud(pan, n, seed=0, g_scale=2e-3):
+    """A wake-like cloud around and behind any body, none inside it: half
+    near the wall (off the panels' control points along their normals, an
+    exponential distance), half in a box behind the body."""
+    rng = np.random.default_rng(seed)
+    n1 = n // 2
+    k = rng.integers(0, len(pan), n1)
+    off = rng.exponential(0.03, n1) + 1e-4
+    t = rng.uniform(-0.5, 0.5, n1) * pan["length"][k]
+    x1 = pan["contr"][k, 0] + off * pan["norm"][k, 0] + t * pan["tang"][k, 0]
+    y1 = pan["contr"][k, 1] + off * pan["norm"][k, 1] + t * pan["tang"][k, 1]
+    xmin, xmax = pan["left"][:, 0].min(), pan["left"][:, 0].max()
+    ymin, ymax = pan["left"][:, 1].min(), pan["left"][:, 1].max()
+    x2 = rng.uniform(xmin, xmax + 2.5, n - n1)
+    y2 = rng.normal(0.5 * (ymin + ymax), 0.3 + 0.5 * (ymax - ymin), n - n1)
+    x, y = np.concatenate([x1, x2]), np.concatenate([y1, y2])
+    bad = inside_polygon(x, y, pan)
+    x[bad] += (xmax - xmin) + 0.5      # moved downstream, clear of the body
+    g = rng.normal(0.0, g_scale, n)
+    return x, y, g

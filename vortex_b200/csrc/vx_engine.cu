@@ -12,7 +12,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <cxxabi.h>
+
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -124,6 +127,7 @@ void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams 
         p->birth_far = (c->precision == VX_PREC_FP32 && c->fmm) ? 1 : 0;
     }
     p->fmm_leaf = c->fmm_leaf > 0 ? c->fmm_leaf : 32;
+    p->fmm_p = vx_fmm_order_ok(c->fmm_p) ? c->fmm_p : VX_FMM_P;
     p->P = P;
     p->n_of_points = (int)c->n_of_points;
     p->birth_mode = c->birth_offset_mode;
@@ -190,8 +194,9 @@ void vx_work_free(VxWork &w, std::vector<void *> &allocs, cudaStream_t stream) {
 // Scratch for a particle capacity `cap` and a panel count padded to P32
 // (allocs == nullptr: only count the bytes into w.bytes).
 static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long long cap, int P32, int num_sms,
-                                 cudaStream_t stream) {
+                                 cudaStream_t stream, int fmm_p) {
     w.cap = cap;
+    w.fmm_p = fmm_p;
     w.bytes = 0;
     const long long nch = cap / VX_CHUNK + 2;
     vx_status st;
@@ -228,29 +233,29 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.fmm_cnt, vx_fmm_cells(w.fmm_lmax));
     A(w.fmm_start, (1LL << (2 * w.fmm_lmax)) + 1);
     A(w.fmm_flags, cap); A(w.fmm_brute, cap);
-    A(w.fmm_M, 2LL * VX_FMM_P * vx_fmm_cells(w.fmm_lmax));
-    A(w.fmm_L, 2LL * VX_FMM_P * vx_fmm_cells(w.fmm_lmax));
+    A(w.fmm_M, 2LL * fmm_p * vx_fmm_cells(w.fmm_lmax));
+    A(w.fmm_L, 2LL * fmm_p * vx_fmm_cells(w.fmm_lmax));
 #undef A
     return VX_OK;
 }
 
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int fmm_p) {
     vx_work_free(w, allocs, stream);
-    return work_alloc_impl(w, &allocs, cap, P32, num_sms, stream);
+    return work_alloc_impl(w, &allocs, cap, P32, num_sms, stream, fmm_p);
 }
 
-long long vx_work_bytes(long long cap, int P32, int num_sms) {
+long long vx_work_bytes(long long cap, int P32, int num_sms, int fmm_p) {
     VxWork w;
     memset(&w, 0, sizeof(w));
-    work_alloc_impl(w, nullptr, cap, P32, num_sms, nullptr);
+    work_alloc_impl(w, nullptr, cap, P32, num_sms, nullptr, fmm_p);
     return w.bytes;
 }
 
 static void free_work(vx_sim *s) { vx_work_free(s->w, s->work_allocs, s->stream); }
 
 static vx_status alloc_work(vx_sim *s, long long cap) {
-    return vx_work_alloc(s->w, s->work_allocs, cap, s->P32, s->num_sms, s->stream);
+    return vx_work_alloc(s->w, s->work_allocs, cap, s->P32, s->num_sms, s->stream, s->prm.fmm_p);
 }
 
 static void drop_graph(vx_sim *s) {
@@ -837,6 +842,7 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step, VxRe
     L.full_sms = s->num_sms;
     L.rec = rec;
     if (rec) L.launches = nullptr;
+    if (!rec) L.kt = s->kt;
     VxView v = view_of(s);
     const VxParams &p = s->prm;
     cudaError_t e = cudaSuccess;
@@ -1064,7 +1070,8 @@ extern "C" vx_status vx_estimate_bytes(const vx_conf *c, int64_t P, int64_t n_ma
     const long long S1 = P + 1;
     const long long transient = (2 * S1 * S1 + S1) * 8;     // Gauss-Jordan work area at creation
     const long long wall = 4LL * (9 * P + 4096);              // wall panel lists (bound)
-    *out = 6 * 8 * cap + vx_work_bytes(cap, (int)vx_round32(P), sms) + fixed_bytes(P) + transient + wall;
+    const int fp = vx_fmm_order_ok(c->fmm_p) ? c->fmm_p : VX_FMM_P;
+    *out = 6 * 8 * cap + vx_work_bytes(cap, (int)vx_round32(P), sms, fp) + fixed_bytes(P) + transient + wall;
     return VX_OK;
 }
 
@@ -1099,6 +1106,22 @@ extern "C" vx_status vx_set_fmm(vx_sim *s, int fmm, int leaf) {
     s->prm.birth_far = (s->prm.prec == VX_PREC_FP32 && s->conf.fmm && s->P > 0) ? 1 : 0;
     drop_graph(s);
     return VX_OK;
+}
+
+// Expansion terms of the bulk form's quadtree FMM (8, 12, 16 or 20); the
+// expansion arrays are re-sized and the step graph re-captured.
+extern "C" vx_status vx_set_fmm_order(vx_sim *s, int p) {
+    if (!s || !vx_fmm_order_ok(p)) {
+        vx_set_error("vx_set_fmm_order: %d terms (8, 12, 16 or 20)", p);
+        return VX_ERR_ARG;
+    }
+    CU(cudaSetDevice(s->device));
+    CU(cudaStreamSynchronize(s->stream));
+    if (p == s->prm.fmm_p) return VX_OK;
+    s->conf.fmm_p = p;
+    s->prm.fmm_p = p;
+    drop_graph(s);
+    return alloc_work(s, s->cap);
 }
 
 // The stream the handle launches on (for callers that time with events).
@@ -1174,5 +1197,79 @@ extern "C" vx_status vx_probe(vx_sim *s, const double *px, const double *py, int
     CU(cudaMemcpyAsync(ovx, dvx, sizeof(double) * np, cudaMemcpyDeviceToHost, s->stream));
     CU(cudaMemcpyAsync(ovy, dvy, sizeof(double) * np, cudaMemcpyDeviceToHost, s->stream));
     CU(cudaStreamSynchronize(s->stream));
+    return VX_OK;
+}
+
+// Device time of every kernel of `nsteps` steps launched stage by stage with
+// an event pair around each launch (instrumentation: the events keep
+// consecutive kernels from overlapping, and each time includes the event
+// overhead, about a microsecond).  Kernels are named by their demangled
+// names without parameters; names: '\n'-separated into a buffer of
+// names_cap bytes; ms[k], counts[k]: total time and launches of kernel k;
+// *nk: kernels found (at most cap are written).
+extern "C" vx_status vx_kernel_times(vx_sim *s, int64_t nsteps, char *names, int64_t names_cap, double *ms,
+                                     int64_t *counts, int64_t cap, int64_t *nk) {
+    if (!s || nsteps < 1 || !names || names_cap < 1 || !ms || !counts || cap < 0 || !nk) return VX_ERR_ARG;
+    if (s->in_batch) { vx_set_error("vx_kernel_times: the body belongs to a batch"); return VX_ERR_ARG; }
+    CU(cudaSetDevice(s->device));
+    VxKernelTimer kt;
+    s->kt = &kt;
+    vx_status st = VX_OK;
+    for (int64_t k = 0; k < nsteps && st == VX_OK; ++k) {
+        if ((st = ensure_capacity(s)) != VX_OK) break;
+        const cudaError_t e = launch_stages(s, VX_STAGE_ALL, true);
+        if (e != cudaSuccess) { vx_set_error("vx_kernel_times: %s", cudaGetErrorString(e)); st = VX_ERR_CUDA; }
+        s->n_upper += s->P;
+    }
+    s->kt = nullptr;
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    std::map<std::string, std::pair<double, long long>> acc;
+    std::vector<std::string> order;
+    std::map<const void *, std::string> name_of;
+    for (const auto &r : kt.recs) {
+        auto it = name_of.find(r.key);
+        if (it == name_of.end()) {
+            const char *raw = nullptr;
+            std::string nm = "?";
+            if (cudaFuncGetName(&raw, r.key) == cudaSuccess && raw) {
+                int ok = -1;
+                char *dm = abi::__cxa_demangle(raw, nullptr, nullptr, &ok);
+                nm = (ok == 0 && dm) ? std::string(dm) : std::string(raw);
+                free(dm);
+                const size_t par = nm.find('(');
+                if (par != std::string::npos) nm = nm.substr(0, par);
+                if (nm.rfind("void ", 0) == 0) nm = nm.substr(5);
+            }
+            it = name_of.emplace(r.key, nm).first;
+        }
+        float t = 0.f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&t, r.a, r.b);
+        auto a = acc.find(it->second);
+        if (a == acc.end()) {
+            order.push_back(it->second);
+            a = acc.emplace(it->second, std::make_pair(0.0, 0LL)).first;
+        }
+        a->second.first += t;
+        a->second.second += 1;
+    }
+    for (const auto &r : kt.recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (cudaEvent_t ev : kt.pool) cudaEventDestroy(ev);
+    if (st != VX_OK) return st;
+    CU(e);
+    std::string all;
+    int64_t k = 0;
+    for (const std::string &nm : order) {
+        if (k < cap) {
+            ms[k] = acc[nm].first;
+            counts[k] = acc[nm].second;
+            all += nm;
+            all += '\n';
+        }
+        ++k;
+    }
+    *nk = k;
+    const size_t nb = std::min<size_t>(all.size(), (size_t)names_cap - 1);
+    memcpy(names, all.data(), nb);
+    names[nb] = 0;
     return VX_OK;
 }

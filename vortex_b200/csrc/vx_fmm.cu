@@ -34,7 +34,9 @@
 
 #include "vx_internal.cuh"
 
-constexpr int FMM_P = VX_FMM_P;  // expansion terms
+// Expansion terms P: a template parameter of the kernels that hold
+// expansions, one of VX_FMM_ORDERS (run-time choice, VxParams::fmm_p).
+constexpr int FMM_PMAX = 20;
 constexpr int FMM_T = 256;
 constexpr int FMM_W = 32;        // targets per near-field work item (one warp)
 
@@ -51,11 +53,13 @@ __device__ __forceinline__ cplx cinv(cplx a) {
 
 __host__ __device__ inline long long fmm_level_off(int l) { return ((1LL << (2 * l)) - 1) / 3; }
 
-// 1/k for k = 1..FMM_P (folded at compile time)
-__constant__ double c_fmm_inv[FMM_P + 1] = {0.0,      1.0,      1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,
-                                            1.0 / 6,  1.0 / 7,  1.0 / 8,  1.0 / 9,  1.0 / 10, 1.0 / 11,
-                                            1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15, 1.0 / 16};
-static_assert(FMM_P == 16, "reciprocal table length");
+// 1/k for k = 1..FMM_PMAX (folded at compile time)
+__constant__ double c_fmm_inv[FMM_PMAX + 1] = {0.0,      1.0,      1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,
+                                               1.0 / 6,  1.0 / 7,  1.0 / 8,  1.0 / 9,  1.0 / 10, 1.0 / 11,
+                                               1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15, 1.0 / 16, 1.0 / 17,
+                                               1.0 / 18, 1.0 / 19, 1.0 / 20};
+// M2L blocks stage their tables in dynamic shared memory (over 48 KB at P = 20)
+extern __shared__ __align__(16) unsigned char vx_fmm_dyn[];
 
 // ---------------------------------------------------------------------------
 VX_DEVK void k_fmm_begin_body(VxBlkB<0, 0> vb, VxScalars *S) {
@@ -266,20 +270,21 @@ __global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, co
 // P2M at the leaves, one warp per leaf: each lane expands its own vortices
 // (FP64 positions), then a fixed butterfly sums the lanes.  Empty leaves are
 // not written (nothing reads their expansion).
+template <int P>
 VX_DEVK void k_fmm_p2m_body(VxBlkB<128, 0> vb, VxView v, const VxScalars *S, const int *start, const int *sorted,
                             cplx *M) {
     const int L = S->fL;
     const long long m = 1LL << L, nl = m * m, n = S->n;
     const double h = S->fside / (double)m;
-    cplx *ML = M + fmm_level_off(L) * FMM_P;
+    cplx *ML = M + fmm_level_off(L) * P;
     const int lane = threadIdx.x & 31;
     const long long nw = ((long long)vb.n * blockDim.x) >> 5;
     for (long long c = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5; c < nl; c += nw) {
         const int j0 = start[c], j1 = start[c + 1];
         if (j0 == j1) continue;
-        cplx b[FMM_P];
+        cplx b[P];
 #pragma unroll
-        for (int k = 0; k < FMM_P; ++k) b[k] = {0.0, 0.0};
+        for (int k = 0; k < P; ++k) b[k] = {0.0, 0.0};
         const double cx = S->fx0 + ((double)(c % m) + 0.5) * h, cy = S->fy0 + ((double)(c / m) + 0.5) * h;
         for (int q = j0 + lane; q < j1; q += 32) {
             const long long j = sorted[q];
@@ -288,7 +293,7 @@ VX_DEVK void k_fmm_p2m_body(VxBlkB<128, 0> vb, VxView v, const VxScalars *S, con
             const cplx w = {(v.x[j * v.ps] - cx) / h, (v.y[j * v.ps] - cy) / h};
             cplx pw = {gj, 0.0};   // G w^k / k!
 #pragma unroll
-            for (int k = 0; k < FMM_P; ++k) {
+            for (int k = 0; k < P; ++k) {
                 b[k] = cadd(b[k], pw);
                 pw = cscale(cmul(pw, w), c_fmm_inv[k + 1]);
             }
@@ -297,58 +302,69 @@ VX_DEVK void k_fmm_p2m_body(VxBlkB<128, 0> vb, VxView v, const VxScalars *S, con
         // of its values selected by its lane bit and adds the partner's copy of
         // it (31 shuffles instead of 160 for an all-reduce of 32 values);
         // afterwards lane q holds value q = coefficient q/2, part q&1
-        double vv[2 * FMM_P];
+        // (in groups of 16 coefficients, the last one padded with zeros)
 #pragma unroll
-        for (int k = 0; k < FMM_P; ++k) { vv[2 * k] = b[k].r; vv[2 * k + 1] = b[k].i; }
+        for (int g0 = 0; g0 < P; g0 += 16) {
+            double vv[32];
 #pragma unroll
-        for (int half = FMM_P; half > 0; half >>= 1) {
-            const bool up = (lane & half) != 0;
-#pragma unroll
-            for (int i = 0; i < half; ++i) {
-                const double send = up ? vv[i] : vv[i + half];
-                const double keep = up ? vv[i + half] : vv[i];
-                vv[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+            for (int k = 0; k < 16; ++k) {
+                const int kk = min(g0 + k, P - 1);
+                vv[2 * k] = g0 + k < P ? b[kk].r : 0.0;
+                vv[2 * k + 1] = g0 + k < P ? b[kk].i : 0.0;
             }
+#pragma unroll
+            for (int half = 16; half > 0; half >>= 1) {
+                const bool up = (lane & half) != 0;
+#pragma unroll
+                for (int i = 0; i < half; ++i) {
+                    const double send = up ? vv[i] : vv[i + half];
+                    const double keep = up ? vv[i + half] : vv[i];
+                    vv[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+                }
+            }
+            if (g0 + (lane >> 1) < P) reinterpret_cast<double *>(ML + c * P)[2 * g0 + lane] = vv[0];
         }
-        reinterpret_cast<double *>(ML + c * FMM_P)[lane] = vv[0];
     }
 }
+template <int P>
 __global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const int *sorted,
                                                  cplx *M) {
     VX_PDL_WAIT();
-    k_fmm_p2m_body(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, v, S, start, sorted, M);
+    k_fmm_p2m_body<P>(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, v, S, start, sorted, M);
 }
 
 // Shift table shared by M2M and L2L, built per block in shared memory:
 // E[q][p] = d_q^p / p! for the child offsets d_q = (+-1 +- i)/4 (in units of
 // the parent side), q = (dy > 0) * 2 + (dx > 0).
-__device__ __forceinline__ void fmm_shift_table(cplx (*se)[FMM_P]) {
+template <int P>
+__device__ __forceinline__ void fmm_shift_table(cplx (*se)[P]) {
     if (threadIdx.x < 4) {
         const int q = threadIdx.x;
         const cplx dd = {(q & 1) ? 0.25 : -0.25, (q >> 1) ? 0.25 : -0.25};
         cplx pw = {1.0, 0.0};
-        for (int p = 0; p < FMM_P; ++p) { se[q][p] = pw; pw = cscale(cmul(pw, dd), c_fmm_inv[p + 1]); }
+        for (int p = 0; p < P; ++p) { se[q][p] = pw; pw = cscale(cmul(pw, dd), c_fmm_inv[p + 1]); }
     }
 }
 
 // M2M: parent at level l from its 4 children at level l+1, one thread per
 // (parent, coefficient k); the thread of coefficient 0 also writes the
 // parent's vortex count (the sum of its children's).
+template <int P>
 VX_DEVK void k_fmm_m2m_body(VxBlkB<128, 0> vb, const VxScalars *S, int *cnt, cplx *M, int l) {
-    __shared__ cplx se[4][FMM_P];
+    __shared__ cplx se[4][P];
     if (l + 1 > S->fL) return;
-    fmm_shift_table(se);
+    fmm_shift_table<P>(se);
     __syncthreads();
     const long long m = 1LL << l, m2 = 2 * m;
-    cplx *Mp = M + fmm_level_off(l) * FMM_P;
-    const cplx *Mc = M + fmm_level_off(l + 1) * FMM_P;
+    cplx *Mp = M + fmm_level_off(l) * P;
+    const cplx *Mc = M + fmm_level_off(l + 1) * P;
     int *cp = cnt + fmm_level_off(l);
     const int *cc = cnt + fmm_level_off(l + 1);
-    const long long tot = m * m * FMM_P;
+    const long long tot = m * m * P;
     for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < tot;
          e += (long long)vb.n * blockDim.x) {
-        const long long c = e / FMM_P;
-        const int k = (int)(e % FMM_P);
+        const long long c = e / P;
+        const int k = (int)(e % P);
         const long long ix = c % m, iy = c / m;
         const int np = cc[(2 * iy) * m2 + 2 * ix] + cc[(2 * iy) * m2 + 2 * ix + 1] +
                        cc[(2 * iy + 1) * m2 + 2 * ix] + cc[(2 * iy + 1) * m2 + 2 * ix + 1];
@@ -360,7 +376,7 @@ VX_DEVK void k_fmm_m2m_body(VxBlkB<128, 0> vb, const VxScalars *S, int *cnt, cpl
                 if (cc[child] == 0) continue;
                 double sc = 1.0;   // 2^-mm
                 for (int mm = 0; mm <= k; ++mm) {
-                    b = cadd(b, cscale(cmul(se[q][k - mm], Mc[child * FMM_P + mm]), sc));
+                    b = cadd(b, cscale(cmul(se[q][k - mm], Mc[child * P + mm]), sc));
                     sc *= 0.5;
                 }
             }
@@ -368,9 +384,10 @@ VX_DEVK void k_fmm_m2m_body(VxBlkB<128, 0> vb, const VxScalars *S, int *cnt, cpl
         Mp[e] = b;
     }
 }
+template <int P>
 __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, cplx *M, int l) {
     VX_PDL_WAIT();
-    k_fmm_m2m_body(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, S, cnt, M, l);
+    k_fmm_m2m_body<P>(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, S, cnt, M, l);
 }
 
 // M2L at level l (2 <= l <= L) plus L2L from level l-1.  A block takes a
@@ -390,25 +407,26 @@ __global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, c
 // levels take one launch each (k_fmm_m2l_l2l), M2L and L2L together.
 constexpr int M2L_TILE = 4;
 constexpr int M2L_SRC = 2 * M2L_TILE;   // 8 x 8 staged source cells
-constexpr int M2L_T = M2L_TILE * M2L_TILE * FMM_P;
 constexpr int M2L_SMALL = 6;
 
+template <int P>
 struct M2LShared {
-    cplx sh[49][2 * FMM_P - 1];   // offset (dx, dy) in [-3, 3]^2 at (dy+3)*7 + dx+3
-    cplx se[4][FMM_P];
-    cplx sm[M2L_SRC * M2L_SRC][FMM_P];
+    cplx sh[49][2 * P - 1];   // offset (dx, dy) in [-3, 3]^2 at (dy+3)*7 + dx+3
+    cplx se[4][P];
+    cplx sm[M2L_SRC * M2L_SRC][P];
     int sc[M2L_SRC * M2L_SRC];
 };
 
-__device__ void m2l_tables(M2LShared &T) {
-    fmm_shift_table(T.se);
+template <int P>
+__device__ void m2l_tables(M2LShared<P> &T) {
+    fmm_shift_table<P>(T.se);
     for (int q = threadIdx.x; q < 49; q += blockDim.x) {
         const int dx = q % 7 - 3, dy = q / 7 - 3;
         if (abs(dx) <= 1 && abs(dy) <= 1) continue;   // neighbours: never an interaction
         const cplx ti = cinv(cplx{(double)dx, (double)dy});
         cplx tp = ti;
         double fact = 1.0;   // j!
-        for (int j = 0; j < 2 * FMM_P - 1; ++j) {
+        for (int j = 0; j < 2 * P - 1; ++j) {
             T.sh[q][j] = cscale(tp, fact);
             tp = cmul(tp, ti);
             fact *= (double)(j + 1);
@@ -419,27 +437,28 @@ __device__ void m2l_tables(M2LShared &T) {
 // M2L of tile t of level l for this thread's (cell, lc); the block's threads
 // all take part.  Returns whether the cell exists; *c its index, *busy
 // whether it holds vortices, *a its scaled M2L coefficient lc.
-__device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int l, long long t, M2LShared &T,
+template <int P>
+__device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int l, long long t, M2LShared<P> &T,
                          long long &c, bool &busy, cplx &a) {
     const long long m = 1LL << l;
     const long long tiles1 = vx_ceil_div(m, (long long)M2L_TILE);
     const double s = S->fside / (double)m;
-    const cplx *Ml = M + fmm_level_off(l) * FMM_P;
+    const cplx *Ml = M + fmm_level_off(l) * P;
     const int *cl = cnt + fmm_level_off(l);
-    const int cell = threadIdx.x / FMM_P;
-    const int cg = (threadIdx.x % FMM_P) >> 2, pt = threadIdx.x & 3;
+    const int cell = threadIdx.x / P;
+    const int cg = (threadIdx.x % P) >> 2, pt = threadIdx.x & 3;
     const int lc = 4 * cg + pt;
     const long long tx0 = (t % tiles1) * M2L_TILE, ty0 = (t / tiles1) * M2L_TILE;
     const long long sx0 = tx0 - 2, sy0 = ty0 - 2;   // staged region origin
     __syncthreads();   // the previous tile is done with sm / sc; tables are built
-    for (int e = threadIdx.x; e < M2L_SRC * M2L_SRC * FMM_P; e += blockDim.x) {
-        const int q = e / FMM_P, k = e % FMM_P;
+    for (int e = threadIdx.x; e < M2L_SRC * M2L_SRC * P; e += blockDim.x) {
+        const int q = e / P, k = e % P;
         const long long qx = sx0 + q % M2L_SRC, qy = sy0 + q / M2L_SRC;
         const bool in = qx >= 0 && qx < m && qy >= 0 && qy < m;
         const long long src = qy * m + qx;
         const int n = in ? cl[src] : 0;
         if (k == 0) T.sc[q] = n;
-        T.sm[q][k] = n > 0 ? Ml[src * FMM_P + k] : cplx{0.0, 0.0};
+        T.sm[q][k] = n > 0 ? Ml[src * P + k] : cplx{0.0, 0.0};
     }
     __syncthreads();
     const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
@@ -459,7 +478,7 @@ __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int 
             const cplx *B = T.sm[q];
             cplx h0 = H[0], h1 = H[1], h2 = H[2], h3 = H[3];
 #pragma unroll
-            for (int k = 0; k < FMM_P; ++k) {
+            for (int k = 0; k < P; ++k) {
                 const cplx b = B[k];
                 v[0] = fma(b.r, h0.r, fma(-b.i, h0.i, v[0]));
                 v[1] = fma(b.r, h0.i, fma(b.i, h0.r, v[1]));
@@ -469,7 +488,7 @@ __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int 
                 v[5] = fma(b.r, h2.i, fma(b.i, h2.r, v[5]));
                 v[6] = fma(b.r, h3.r, fma(-b.i, h3.i, v[6]));
                 v[7] = fma(b.r, h3.i, fma(b.i, h3.r, v[7]));
-                if (k + 1 < FMM_P) { h0 = h1; h1 = h2; h2 = h3; h3 = H[k + 4]; }
+                if (k + 1 < P) { h0 = h1; h1 = h2; h2 = h3; h3 = H[k + 4]; }
             }
         }
     }
@@ -491,51 +510,55 @@ __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int 
 
 // L2L of coefficient lc of cell (ix, iy) of level l from its parent's local
 // expansion Lp (level l-1).
-__device__ __forceinline__ cplx l2l_term(const cplx *Lp, const cplx (*se)[FMM_P], long long m, long long ix,
+template <int P>
+__device__ __forceinline__ cplx l2l_term(const cplx *Lp, const cplx (*se)[P], long long m, long long ix,
                                          long long iy, int lc) {
     const long long parent = (iy >> 1) * (m >> 1) + (ix >> 1);
     const int q = (int)((iy & 1) * 2 + (ix & 1));
     cplx acc = {0.0, 0.0};
-    for (int j = lc; j < FMM_P; ++j) acc = cadd(acc, cmul(Lp[parent * FMM_P + j], se[q][j - lc]));
+    for (int j = lc; j < P; ++j) acc = cadd(acc, cmul(Lp[parent * P + j], se[q][j - lc]));
     return cscale(acc, ldexp(1.0, -lc));
 }
 
-VX_DEVK void k_fmm_m2l_l2l_body(VxBlkB<M2L_T, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
+template <int P>
+VX_DEVK void k_fmm_m2l_l2l_body(VxBlkB<M2L_TILE * M2L_TILE * P, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
                                 cplx *Loc, int l) {
-    __shared__ M2LShared T;
+    M2LShared<P> &T = *reinterpret_cast<M2LShared<P> *>(vx_fmm_dyn);
     if (l > S->fL) return;
-    m2l_tables(T);
+    m2l_tables<P>(T);
     const long long m = 1LL << l;
     const long long tiles1 = vx_ceil_div(m, (long long)M2L_TILE);
-    cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
-    const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
-    const int lc = threadIdx.x % FMM_P;   // = 4 cg + pt
+    cplx *Ll = Loc + fmm_level_off(l) * P;
+    const cplx *Lp = Loc + fmm_level_off(l - 1) * P;
+    const int lc = threadIdx.x % P;   // = 4 cg + pt
     for (long long t = vb.x; t < tiles1 * tiles1; t += vb.n) {
         long long c;
         bool busy;
         cplx a;
-        if (!m2l_tile(S, cnt, M, l, t, T, c, busy, a)) continue;
-        if (busy && l > 2) a = cadd(a, l2l_term(Lp, T.se, m, c % m, c / m, lc));
-        Ll[c * FMM_P + lc] = a;
+        if (!m2l_tile<P>(S, cnt, M, l, t, T, c, busy, a)) continue;
+        if (busy && l > 2) a = cadd(a, l2l_term<P>(Lp, T.se, m, c % m, c / m, lc));
+        Ll[c * P + lc] = a;
     }
 }
-__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
+template <int P>
+__global__ void __launch_bounds__(M2L_TILE * M2L_TILE * P) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
                                                        cplx *Loc, int l) {
     VX_PDL_WAIT();
-    k_fmm_m2l_l2l_body(VxBlkB<M2L_T, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc, l);
+    k_fmm_m2l_l2l_body<P>(VxBlkB<M2L_TILE * M2L_TILE * P, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc, l);
 }
 
 // M2L (without L2L) of levels 2 .. min(M2L_SMALL, L): blocks over the tiles
 // of all of them.
-VX_DEVK void k_fmm_m2l_small_body(VxBlkB<M2L_T, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
+template <int P>
+VX_DEVK void k_fmm_m2l_small_body(VxBlkB<M2L_TILE * M2L_TILE * P, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
                                   cplx *Loc) {
-    __shared__ M2LShared T;
+    M2LShared<P> &T = *reinterpret_cast<M2LShared<P> *>(vx_fmm_dyn);
     const int hi = min(S->fL, M2L_SMALL);
     if (hi < 2) return;
-    m2l_tables(T);
+    m2l_tables<P>(T);
     long long total = 0;
     for (int l = 2; l <= hi; ++l) total += vx_ceil_div(1LL << (2 * l), (long long)(M2L_TILE * M2L_TILE));
-    const int lc = threadIdx.x % FMM_P;
+    const int lc = threadIdx.x % P;
     for (long long b = vb.x; b < total; b += vb.n) {
         int l = 2;
         long long t = b;
@@ -546,37 +569,40 @@ VX_DEVK void k_fmm_m2l_small_body(VxBlkB<M2L_T, 0> vb, const VxScalars *S, const
         long long c;
         bool busy;
         cplx a;
-        if (!m2l_tile(S, cnt, M, l, t, T, c, busy, a)) continue;
-        Loc[(fmm_level_off(l) + c) * FMM_P + lc] = a;
+        if (!m2l_tile<P>(S, cnt, M, l, t, T, c, busy, a)) continue;
+        Loc[(fmm_level_off(l) + c) * P + lc] = a;
     }
 }
-__global__ void __launch_bounds__(M2L_T) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
+template <int P>
+__global__ void __launch_bounds__(M2L_TILE * M2L_TILE * P) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
                                                          cplx *Loc) {
     VX_PDL_WAIT();
-    k_fmm_m2l_small_body(VxBlkB<M2L_T, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc);
+    k_fmm_m2l_small_body<P>(VxBlkB<M2L_TILE * M2L_TILE * P, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc);
 }
 
 // L2L into level l (3 <= l <= min(M2L_SMALL, L)) from level l-1, one thread
 // per (cell, coefficient); one launch per level.
+template <int P>
 VX_DEVK void k_fmm_l2l_small_body(VxBlkB<256, 0> vb, const VxScalars *S, const int *cnt, cplx *Loc, int l) {
-    __shared__ cplx se[4][FMM_P];
+    __shared__ cplx se[4][P];
     if (l > min(S->fL, M2L_SMALL)) return;
-    fmm_shift_table(se);
+    fmm_shift_table<P>(se);
     __syncthreads();
     const long long m = 1LL << l;
     const int *cl = cnt + fmm_level_off(l);
-    cplx *Ll = Loc + fmm_level_off(l) * FMM_P;
-    const cplx *Lp = Loc + fmm_level_off(l - 1) * FMM_P;
-    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < m * m * FMM_P;
+    cplx *Ll = Loc + fmm_level_off(l) * P;
+    const cplx *Lp = Loc + fmm_level_off(l - 1) * P;
+    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < m * m * P;
          e += (long long)vb.n * blockDim.x) {
-        const long long c = e / FMM_P;
-        const int lc = (int)(e % FMM_P);
-        if (cl[c] > 0) Ll[e] = cadd(Ll[e], l2l_term(Lp, se, m, c % m, c / m, lc));
+        const long long c = e / P;
+        const int lc = (int)(e % P);
+        if (cl[c] > 0) Ll[e] = cadd(Ll[e], l2l_term<P>(Lp, se, m, c % m, c / m, lc));
     }
 }
+template <int P>
 __global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const int *cnt, cplx *Loc, int l) {
     VX_PDL_WAIT();
-    k_fmm_l2l_small_body(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, S, cnt, Loc, l);
+    k_fmm_l2l_small_body<P>(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, S, cnt, Loc, l);
 }
 
 // Near field (FP32, core smoothing, 3 nearest) + far field (L2P, FP64): one
@@ -614,6 +640,7 @@ __device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gsl
 #ifndef VX_NEAR_MINB
 #define VX_NEAR_MINB 1   // minimum resident blocks per SM requested for k_fmm_near
 #endif
+template <int P>
 VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
                              const int *sorted, const int *start, const int2 *items,
                              const cplx *Loc, int *flag_list) {
@@ -629,7 +656,7 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
     const float h2 = (float)(h * h);
     const float eps2 = (float)p.eps2;
     const long long nitems = S->cnitems;
-    const cplx *LL = Loc + fmm_level_off(L) * FMM_P;
+    const cplx *LL = Loc + fmm_level_off(L) * P;
     const long long wpb = FMM_T / 32;
     for (long long it = vb.x * wpb + (threadIdx.x >> 5); it < nitems; it += vb.n * wpb) {
         const int2 item = items[it];
@@ -716,9 +743,9 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
                 const cplx u = {(xd - (S->fx0 + ((double)col + 0.5) * h)) / h,
                                 (yd - (S->fy0 + ((double)row + 0.5) * h)) / h};
                 // f = sum_l A_l u^l / l!, nested as A_0 + (u/1)(A_1 + (u/2)(A_2 + ...))
-                f = LL[leaf * FMM_P + FMM_P - 1];
-                for (int l = FMM_P - 2; l >= 0; --l)
-                    f = cadd(cmul(f, cscale(u, c_fmm_inv[l + 1])), LL[leaf * FMM_P + l]);
+                f = LL[leaf * P + P - 1];
+                for (int l = P - 2; l >= 0; --l)
+                    f = cadd(cmul(f, cscale(u, c_fmm_inv[l + 1])), LL[leaf * P + l]);
             }
             // u - i v = f / (2 pi i): vx = Im f / 2pi, vy = Re f / 2pi
             const double vx = (ax + f.i) / VX_TWO_PI + S->vinf[0];
@@ -733,11 +760,12 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
         }
     }
 }
+template <int P>
 __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                    const int *sorted, const int *start, const int2 *items,
                                                    const cplx *Loc, int *flag_list) {
     VX_PDL_WAIT();
-    k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB>{blockIdx.x, gridDim.x}, p, v, S, srt, sorted, start, items, Loc, flag_list);
+    k_fmm_near_body<P>(VxBlkB<FMM_T, VX_NEAR_MINB>{blockIdx.x, gridDim.x}, p, v, S, srt, sorted, start, items, Loc, flag_list);
 }
 
 // Targets whose third-nearest distance reached the leaf side: exact 3
@@ -951,8 +979,20 @@ int vx_fmm_max_level(long long cap) {
     return L;
 }
 
-cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                                   VxWork &w) {
+template <int P>
+static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S, VxWork &w) {
+    constexpr int M2L_T = M2L_TILE * M2L_TILE * P;
+    constexpr size_t M2L_SMEM = sizeof(M2LShared<P>);
+    if (M2L_SMEM > 48 * 1024 && !L.rec) {   // opt in to more than 48 KB of shared memory (once per device)
+        static bool done[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < 64 && !done[dev]) {
+            cudaFuncSetAttribute(k_fmm_m2l_l2l<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M2L_SMEM);
+            cudaFuncSetAttribute(k_fmm_m2l_small<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M2L_SMEM);
+            done[dev] = true;
+        }
+    }
     const int grid = L.num_sms * 4;
     const int Lmax = w.fmm_lmax;
     vx_launch<k_fmm_begin, k_fmm_begin_body>(L, 1, 1, 0, S);
@@ -969,29 +1009,29 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     const unsigned *skey = w.key1;
     const int *sorted = w.val1;
     vx_launch<k_fmm_gather, k_fmm_gather_body>(L, grid, FMM_T, 0, v, S, sorted, skey, w.srt);
-    vx_launch<k_fmm_p2m, k_fmm_p2m_body>(L, grid * 4, 128, 0, v, S, w.fmm_start, sorted, (cplx *)w.fmm_M);
+    vx_launch<k_fmm_p2m<P>, k_fmm_p2m_body<P>>(L, grid * 4, 128, 0, v, S, w.fmm_start, sorted, (cplx *)w.fmm_M);
     // the level loops cover the deepest level this capacity allows; kernels
     // of levels below the depth chosen on the device return at once
     for (int l = Lmax - 1; l >= 0; --l) {
-        const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * FMM_P, 128));
-        vx_launch<k_fmm_m2m, k_fmm_m2m_body>(L, gm, 128, 0, S, w.fmm_cnt, (cplx *)w.fmm_M, l);
+        const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * P, 128));
+        vx_launch<k_fmm_m2m<P>, k_fmm_m2m_body<P>>(L, gm, 128, 0, S, w.fmm_cnt, (cplx *)w.fmm_M, l);
     }
     {
         long long tiles = 0;
         for (int l = 2; l <= std::min(Lmax, M2L_SMALL); ++l) tiles += vx_ceil_div(1LL << (2 * l), 16LL);
         if (tiles > 0) {
-            vx_launch<k_fmm_m2l_small, k_fmm_m2l_small_body>(L, (int)std::min<long long>(grid * 2, tiles), M2L_T, 0, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L);
+            vx_launch<k_fmm_m2l_small<P>, k_fmm_m2l_small_body<P>>(L, (int)std::min<long long>(grid * 2, tiles), M2L_T, M2L_SMEM, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L);
 
             for (int l = 3; l <= std::min(Lmax, M2L_SMALL); ++l) {
-                const int g = (int)std::min<long long>(grid, vx_ceil_div((1LL << (2 * l)) * FMM_P, 256));
-                vx_launch<k_fmm_l2l_small, k_fmm_l2l_small_body>(L, g, 256, 0, S, w.fmm_cnt, (cplx *)w.fmm_L, l);
+                const int g = (int)std::min<long long>(grid, vx_ceil_div((1LL << (2 * l)) * P, 256));
+                vx_launch<k_fmm_l2l_small<P>, k_fmm_l2l_small_body<P>>(L, g, 256, 0, S, w.fmm_cnt, (cplx *)w.fmm_L, l);
             }
         }
     }
     for (int l = M2L_SMALL + 1; l <= Lmax; ++l) {
         const long long t1 = vx_ceil_div(1LL << l, (long long)M2L_TILE);
         const int g = (int)std::min<long long>(grid * 2, t1 * t1);
-        vx_launch<k_fmm_m2l_l2l, k_fmm_m2l_l2l_body>(L, g, M2L_T, 0, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
+        vx_launch<k_fmm_m2l_l2l<P>, k_fmm_m2l_l2l_body<P>>(L, g, M2L_T, M2L_SMEM, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
 
     }
     vx_launch<k_fmm_row_items, k_fmm_row_items_body>(L, grid, FMM_T, 0, S, w.fmm_start, w.row_items);
@@ -999,7 +1039,7 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     vx_launch<k_fmm_items, k_fmm_items_body>(L, grid, FMM_T, 0, S, w.fmm_start, w.row_items, w.row_item_off, w.items, w.items_cap);
 
     VX_EV(L, 0);
-    vx_launch<k_fmm_near, k_fmm_near_body>(L, L.num_sms * 8, FMM_T, 0, p, v, S, w.srt, sorted, w.fmm_start, w.items, (const cplx *)w.fmm_L, w.fmm_flags);
+    vx_launch<k_fmm_near<P>, k_fmm_near_body<P>>(L, L.num_sms * 8, FMM_T, 0, p, v, S, w.srt, sorted, w.fmm_start, w.items, (const cplx *)w.fmm_L, w.fmm_flags);
     VX_EV(L, 1);
 
     vx_launch<k_fmm_nn3_fix, k_fmm_nn3_fix_body>(L, grid, FMM_T, 0, v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
@@ -1007,4 +1047,14 @@ cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const V
     vx_launch<k_fmm_nn3_brute, k_fmm_nn3_brute_body>(L, grid, 256, 0, v, S, w.fmm_brute);
 
     return cudaGetLastError();
+}
+
+cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
+                                   VxWork &w) {
+    switch (p.fmm_p) {
+    case 8: return velocity_fmm<8>(L, p, v, S, w);
+    case 12: return velocity_fmm<12>(L, p, v, S, w);
+    case 20: return velocity_fmm<20>(L, p, v, S, w);
+    default: return velocity_fmm<16>(L, p, v, S, w);
+    }
 }

@@ -57,6 +57,7 @@ struct VxParams {
     double bc_x, bc_y, b_rfar2;
     int birth_far;
     int fmm_leaf;          // quadtree depth aims at this many vortices per leaf
+    int fmm_p;             // expansion terms of the quadtree FMM (8, 12, 16 or 20)
     int P;
     int n_of_points;
     int birth_mode;
@@ -157,8 +158,12 @@ struct VxWork {
     // quadtree: counts and expansions of every level up to fmm_lmax
     int fmm_lmax;
     int *fmm_cnt, *fmm_start, *fmm_flags, *fmm_brute;
-    double *fmm_M, *fmm_L;   // complex FP64 pairs, FMM_P per cell
+    int fmm_p;               // expansion terms the two arrays below were sized for
+    double *fmm_M, *fmm_L;   // complex FP64 pairs, fmm_p per cell
 };
+
+constexpr int VX_FMM_P = 16;              // default expansion terms of the quadtree FMM (vx_fmm.cu)
+inline bool vx_fmm_order_ok(int p) { return p == 8 || p == 12 || p == 16 || p == 20; }
 
 // Compaction chunk size (elements per scan chunk).
 constexpr int VX_CHUNK = 2048;
@@ -511,8 +516,8 @@ cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const V
 void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams *p);
 void vx_set_error(const char *fmt, ...);
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
-                        cudaStream_t stream = nullptr);
-long long vx_work_bytes(long long cap, int P32, int num_sms);
+                        cudaStream_t stream = nullptr, int fmm_p = VX_FMM_P);
+long long vx_work_bytes(long long cap, int P32, int num_sms, int fmm_p = VX_FMM_P);
 // Stable order by bucket from bucket counts (used up, then restored) and
 // starts: (okey, oval) = keys and element indices in bucket order, elements
 // of a bucket in index order (vx_sort.cu).
@@ -524,7 +529,6 @@ long long vx_fmm_cells(int lmax);         // cells of all levels 0..lmax
 constexpr int VX_BF_P = 48;          // terms of the birth far-field expansion
 constexpr double VX_BF_RHO = 1.5;    // far-field sources lie beyond VX_BF_RHO body radii of its centre
 constexpr int VX_BF_MAX_BLOCKS = 1024;
-constexpr int VX_FMM_P = 16;              // expansion terms (vx_fmm.cu)
 cudaError_t vx_launch_velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                    VxWork &w);
 cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,

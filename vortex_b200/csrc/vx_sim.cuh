@@ -54,6 +54,8 @@ struct vx_sim {
     // batch's stream meanwhile (own_stream kept), and steps only through it
     bool in_batch = false;
     cudaStream_t own_stream = nullptr;
+    // per-kernel timing of eagerly launched steps (vx_kernel_times)
+    VxKernelTimer *kt = nullptr;
 };
 
 

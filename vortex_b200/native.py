@@ -41,7 +41,7 @@ class Conf(C.Structure):
         ("precision", C.c_int32), ("birth_offset_mode", C.c_int32),
         ("drop_eps", C.c_double), ("diff_cutoff", C.c_double),
         ("n_probes_grid", C.c_int32), ("pad1_", C.c_int32), ("probe_box", C.c_double * 4),
-        ("fmm", C.c_int32), ("gj_pivot", C.c_int32), ("fmm_leaf", C.c_int32), ("pad3_", C.c_int32),
+        ("fmm", C.c_int32), ("gj_pivot", C.c_int32), ("fmm_leaf", C.c_int32), ("fmm_p", C.c_int32),
     ]
 
 
@@ -281,8 +281,24 @@ class Sim:
     def stream(self) -> int:
         return lib().vx_get_stream(self.h) or 0
 
-    def set_fmm(self, fmm: bool, leaf: int = 8):
+    def set_fmm(self, fmm: bool, leaf: int = 8, p: int = None):
         _check(lib().vx_set_fmm(self.h, C.c_int(int(fmm)), C.c_int(int(leaf))), "vx_set_fmm")
+        if p is not None:
+            _check(lib().vx_set_fmm_order(self.h, C.c_int(int(p))), "vx_set_fmm_order")
+
+    def kernel_times(self, nsteps: int = 3) -> dict:
+        """{kernel name: (total ms, launches)} over nsteps instrumented steps
+        (an event pair around every launch)."""
+        cap = 512
+        names = C.create_string_buffer(64 * cap)
+        ms = np.zeros(cap)
+        cnt = np.zeros(cap, dtype=np.int64)
+        nk = C.c_int64(0)
+        _check(lib().vx_kernel_times(self.h, C.c_int64(nsteps), names, C.c_int64(len(names)), _p(ms), _p(cnt),
+                                     C.c_int64(cap), C.byref(nk)), "vx_kernel_times")
+        nm = names.value.decode().split("\n")
+        k = min(nk.value, cap)
+        return {nm[i]: (float(ms[i]), int(cnt[i])) for i in range(k)}
 
     def device_bytes(self) -> int:
         b = C.c_int64(0)
