@@ -153,6 +153,16 @@ def roofline_hbm(kt: dict, steps: int, n: float, peak_gbs: float) -> list:
     return out
 
 
+def autotune_leaves():
+    from vortex_b200 import autotune
+    return autotune.LEAVES
+
+
+def autotune_orders():
+    from vortex_b200 import autotune
+    return autotune.ORDERS
+
+
 def measured_peaks() -> dict:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -199,7 +209,10 @@ def run_ours(args, rank, world, device):
             # untimed: the autotuner picks direct or FMM and the leaf size on
             # this state, then two more steps re-capture the step graph
             from vortex_b200 import autotune
-            tuned = autotune.tune(sim, reps=2, device=device)["best"]
+            tres = autotune.tune(sim, reps=2, device=device)
+            tuned = tres["best"]
+            tuned["rejected"] = sum(1 for r in tres["table"] if "rejected" in r)
+            tuned["candidates"] = len(tres["table"])
             sim.step(2)
             sim.sync()
         sim.set_timing(instrumented == 0)
@@ -303,6 +316,10 @@ def run_ours(args, rank, world, device):
     peak32 = max(peak32_scalar, peak32_packed)
     mufu = Nt.measure_peak(device, mode=3)        # 1e12 (rsqrt + ex2) units per second
     multi = multibody_runs(args, device, rank, world) if args.multibody else None
+    cross = None
+    if args.crossover and rank == 0:
+        from vortex_b200 import autotune
+        cross = autotune.crossover(device=device)
     if rank != 0:
         return None
     value = world * 1e3 * K / total_ms
@@ -336,9 +353,12 @@ def run_ours(args, rank, world, device):
                 "form": "FP32-bulk: FP32 pair sums with FP64 accumulation, FP64 expansions, panel solve, forces "
                         "and positions",
                 "launch": "each timed step replays the step's CUDA graph (vx_step, as a user's call does)",
-                "biot_savart": (f"autotuned before timing: {tuned['form']}"
-                                + (f", {tuned['leaf']} vortices per leaf" if tuned and tuned['leaf'] else "")
-                                if tuned else "FMM, 32 vortices per leaf (default)")},
+                "biot_savart": (f"autotuned before timing over direct and FMM (leaf {list(autotune_leaves())}, "
+                                f"p {list(autotune_orders())}; {tuned['rejected']} of {tuned['candidates']} "
+                                f"settings rejected by the 2e-5 max|V| check): {tuned['form']}"
+                                + (f", {tuned['leaf']} vortices per leaf, {tuned['p']} terms"
+                                   if tuned['form'] == 'fmm' else "")
+                                if tuned else "FMM, 32 vortices per leaf, 16 terms (default)")},
         "particle_interactions_per_s": {"effective": world * eff * 1e3 * K / total_ms,
                                         "executed": world * (pc[0] + pc[1]) / (total_ms * 1e-3),
                                         "effective_definition": "N_targets x N_sources per step (direct-sum equivalent)",
@@ -379,6 +399,9 @@ def run_ours(args, rank, world, device):
         line["reference_cuda_build"] = ref_cuda_build(args, x0, y0, g0)
     if multi:
         line["batched"], line["served"] = multi
+    if cross:
+        line["crossover"] = {"what": "velocity stage (FP32) on the benchmark wake: direct sum against the best "
+                                     "accurate FMM setting, ms", "rows": cross}
     return line
 
 
@@ -389,11 +412,15 @@ def multibody_runs(args, device, rank, world):
     part in the gathers; rank 0 gets the combined records."""
     from vortex_b200 import multibody as MB
     from vortex_b200 import native as Nt
-    batched = MB.run_batch(bodies=args.batch_bodies, steps=args.batch_steps, warmup=3, device=device,
-                           rank=rank, world=world, mode="graph")
-    # the same population as concurrent per-body step graphs, for comparison
-    streams = MB.run_batch(bodies=args.batch_bodies, steps=3, warmup=2, device=device, rank=rank, world=world,
-                           mode="streams")
+    pop = MB.make_population(args.batch_bodies, device=device, rank=rank, world=world)
+    batched = MB.run_batch(steps=args.batch_steps, warmup=3, device=device, rank=rank, world=world, mode="graph",
+                           population=pop)
+    # the same bodies (a few steps later) as concurrent per-body step graphs,
+    # for comparison
+    streams = MB.run_batch(steps=3, warmup=1, device=device, rank=rank, world=world, mode="streams",
+                           population=pop)
+    for s in pop[1]:
+        s.close()
     batched["per_body_streams"] = {k: streams[k] for k in ("mode", "ms_per_batched_step", "body_steps_per_s",
                                                            "particle_steps_per_s", "kernels_per_batched_step")}
     sub32 = MB.run_batch(bodies=16, steps=2, warmup=1, device=device, rank=rank, world=world)
@@ -571,6 +598,8 @@ def main():
                     help="also time the reference's own CUDA build for this many steps (0: off)")
     ap.add_argument("--ref-cuda-timeout", type=float, default=900.0)
     ap.add_argument("--no-autotune", action="store_true", help="skip the untimed autotuning before timing")
+    ap.add_argument("--no-crossover", dest="crossover", action="store_false",
+                    help="skip the direct-vs-FMM crossover table (untimed)")
     ap.add_argument("--no-multibody", dest="multibody", action="store_false",
                     help="skip the seeded multi-body population batched and served")
     ap.add_argument("--batch-bodies", type=int, default=256)

@@ -246,6 +246,11 @@ vx_status vx_server_result(vx_server *srv, int64_t id, int *state, int64_t *step
  * submit-to-finish s, [5] mean resident bodies per tick, [6] body steps,
  * [7] particle steps, [8] bytes reserved now, [9] ticks. */
 vx_status vx_server_stats(vx_server *srv, double out10[10]);
+/* How the resident bodies are stepped: 1 (default) as the members of one
+ * batch (vx_batch: each kernel of the step once for all of them, joining
+ * at the step after their creation, leaving after their last step), 0 each
+ * on its own stream.  Only while no body is resident. */
+vx_status vx_server_set_batched(vx_server *srv, int on);
 
 /* Batched steps (no counterpart in the reference, which runs one body per
  * process; its step loop is src/main.c:652-785).  A batch advances bodies
@@ -260,6 +265,22 @@ vx_status vx_server_stats(vx_server *srv, double out10[10]);
  * Destroy the batch before any of its bodies. */
 typedef struct vx_batch vx_batch;
 vx_status vx_batch_create(vx_sim *const *sims, int count, vx_batch **out);
+/* An empty batch on `device`; members join with vx_batch_add. */
+vx_status vx_batch_new(int device, vx_batch **out);
+/* Membership changes between batched steps: a body joins at the next step
+ * (after the work already queued on its own stream), or leaves after the
+ * steps already launched and returns to its own stream.  No host wait. */
+vx_status vx_batch_add(vx_batch *batch, vx_sim *sim);
+vx_status vx_batch_remove(vx_batch *batch, vx_sim *sim);
+/* Wait for the last batched step; for each body that took part in it (in
+ * the batch's order at that step, *count of them, at most cap written):
+ * the body and 5 values, its vortex count, d_g, Fx, Fy and M after the
+ * step (gathered on the device and copied back once per step). */
+vx_status vx_batch_last_results(vx_batch *batch, vx_sim **members, double *out5, int cap, int *count);
+/* The same for batched step `step` (0-based among the batch's steps; the
+ * last two launched are kept, so a caller can launch the next step before
+ * collecting the previous one). */
+vx_status vx_batch_results(vx_batch *batch, int64_t step, vx_sim **members, double *out5, int cap, int *count);
 /* Asynchronous like vx_step; bodies grow their stores as needed. */
 vx_status vx_batch_step(vx_batch *batch, int64_t nsteps);
 /* Wait for the batch's steps; reports the bodies' device error flags. */

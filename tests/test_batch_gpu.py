@@ -115,3 +115,39 @@ def test_batch_of_the_seeded_population_steps_and_reports_launches():
     assert info["kernels_per_step"] < 300
     for s in sims:
         s.close()
+
+
+def test_members_join_and_leave_between_steps():
+    """Continuous membership: A runs alone in the batch for 3 steps, B joins
+    for 4, then A leaves and C joins for 5 more.  Each body ends exactly as
+    its twin stepped alone for its own number of steps (7, 9, 5), and the
+    results gathered after the last batched step are the members' own
+    counts and force sums."""
+    specs = _bodies()[:3]
+    alone = [_make(sp) for sp in specs]
+    mine = [_make(sp) for sp in specs]
+    for s, k in zip(alone, (7, 9, 5)):
+        s.step(k)
+        s.sync()
+    A, B, C = mine
+    b = N.Batch([A])
+    b.step(3)
+    b.add(B)
+    b.step(4)
+    b.remove(A)
+    b.add(C)
+    b.step(5)
+    res = b.last_results()
+    assert set(res) == {B.h.value, C.h.value}
+    for m in (B, C):
+        n, dg, fx, fy, mm = res[m.h.value]
+        f = m.forces()
+        assert n == m.count() and dg == f[0] and fx == f[1] and fy == f[2] and mm == f[3]
+    b.close()
+    for k, (a, m) in enumerate(zip(alone, mine)):
+        sa, sm = _state(a), _state(m)
+        assert sa[0] == sm[0], f"body {k}: count {sa[0]} alone, {sm[0]} batched"
+        for q, name in enumerate(("x", "y", "g", "vx", "vy", "d", "forces"), start=1):
+            assert np.array_equal(sa[q], sm[q]), f"body {k}: {name} differs"
+    for s in alone + mine:
+        s.close()

@@ -256,10 +256,13 @@ def test_bulk_force_statistics_vs_fp64_config1():
     assert abs(a[-1, 2] - b[-1, 2]) <= 0.05 * b[-1, 2]
 
 
-def test_fmm_leaf_sizes_and_autotune():
-    """Every leaf size the autotuner may pick keeps the FMM velocity within
-    2e-5 max|V| of FP64; the tuner times each candidate and leaves the body
-    on the fastest."""
+def test_fmm_leaf_sizes_orders_and_autotune():
+    """Every expansion order (8, 12, 16, 20 terms) at every leaf size the
+    autotuner may pick: the FMM velocity's error against FP64 falls as the
+    order rises, 16 and 20 terms keep it within 2e-5 max|V| at every leaf
+    size; the tuner checks each setting against the direct sum at sampled
+    vortices, rejects the inaccurate ones, times the rest and leaves the body
+    on the fastest (form, leaf, order)."""
     from vortex_b200 import autotune
     ck = conf_kwargs(1000, precision=N.PREC_FP32)
     pan = profiles.circle(1000)
@@ -271,14 +274,22 @@ def test_fmm_leaf_sizes_and_autotune():
     vmax = np.abs(np.stack([c[0], c[1]])).max()
     s = N.Sim(N.default_conf(**ck), pan)
     s.set_particles(x, y, g)
+    err = {}
+    for p in autotune.ORDERS:
+        for leaf in autotune.LEAVES:
+            s.set_fmm(True, leaf, p)
+            s.stage("velocity")
+            a = s.velocity()
+            err[p, leaf] = max(np.abs(a[0] - c[0]).max(), np.abs(a[1] - c[1]).max()) / vmax
     for leaf in autotune.LEAVES:
-        s.set_fmm(True, leaf)
-        s.stage("velocity")
-        a = s.velocity()
-        assert np.abs(a[0] - c[0]).max() <= 2e-5 * vmax and np.abs(a[1] - c[1]).max() <= 2e-5 * vmax, leaf
+        assert err[16, leaf] <= 2e-5 and err[20, leaf] <= 2e-5, (leaf, err[16, leaf], err[20, leaf])
+        assert err[8, leaf] > err[16, leaf]
     r = autotune.tune(s, reps=2)
-    assert len(r["table"]) == 1 + len(autotune.LEAVES) and all(t["ms"] > 0 for t in r["table"])
-    assert r["best"]["ms"] == min(t["ms"] for t in r["table"])
+    assert len(r["table"]) == 1 + len(autotune.LEAVES) * len(autotune.ORDERS)
+    timed = [t for t in r["table"] if "ms" in t]
+    assert all(t["ms"] > 0 for t in timed) and all(t["error"] <= 2e-5 for t in timed if t["form"] == "fmm")
+    assert r["best"]["ms"] == min(t["ms"] for t in timed)
+    assert r["best"]["form"] == "direct" or r["best"]["p"] in autotune.ORDERS
     s.step(2)   # runs with the chosen setting
     s.close()
     plain.close()

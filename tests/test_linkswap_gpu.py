@@ -72,11 +72,11 @@ def start_frame(path, n=3000, seed=5):
             fh.write(f"{i} 0.008000 {x[i]:f} {y[i]:f} 0.000000 0.000000 0.000000 {g[i]:f}\n")
 
 
-def run(exe, wd):
+def run(exe, wd, inc=65536):
     os.makedirs(wd, exist_ok=True)
     profiles.write_profile(os.path.join(wd, "circle200.txt"), profiles.circle(200))
     with open(os.path.join(wd, "run.conf"), "w") as fh:
-        fh.write(CONF.format(eps=2 * math.pi * 0.5 / 200))
+        fh.write(CONF.format(eps=2 * math.pi * 0.5 / 200).replace("inc_step 65536", f"inc_step {inc}"))
     start_frame(os.path.join(wd, "Kadr000012.txt"))
     r = subprocess.run([exe, "-c", "run.conf", "-l", "1"], cwd=wd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
@@ -116,3 +116,24 @@ def test_reference_driver_runs_on_this_library(tmp_path):
     for f in ("Kadr000018.txt", "Kadr000024.txt"):
         assert os.path.exists(os.path.join(b, "output", "kadrs", f))
     assert os.path.exists(os.path.join(b, "output", "vels", "contr_Vel000018.txt"))
+
+
+@pytest.mark.skipif(not os.path.exists(SWAP), reason="oracle/_ref binaries not built")
+def test_reference_driver_grows_the_store_through_this_library(tmp_path):
+    """The reference's driver with inc_step 512: its step loop calls
+    incr_vort_quant (allocate_arrays, randomize_tail) whenever the padded
+    count outgrows the store, here on the first step and several times
+    after (3000 restart vortices, 200 born per step).  Growth keeps every
+    slot and fills the new tail far from every vortex, so the run writes
+    the same frames, forces and counts, to the last printed digit, as the
+    run whose store never grows (inc_step 65536).  (The reference's own
+    randomize_tail returns no value, which its driver takes as a failure at
+    the first growth, so only the library is run here.)"""
+    a, b = str(tmp_path / "big"), str(tmp_path / "grow")
+    run(SWAP, a, inc=65536)
+    run(SWAP, b, inc=512)
+    for f in ("M.txt", os.path.join("output", "kadrs", "Kadr000018.txt"),
+              os.path.join("output", "kadrs", "Kadr000024.txt"), os.path.join("output", "F_p.txt")):
+        fa, fb = numbers(os.path.join(a, f)), numbers(os.path.join(b, f))
+        assert fa.shape == fb.shape and np.array_equal(fa, fb), f
+    assert counts(a) == counts(b)

@@ -42,9 +42,10 @@ def test_step_many_matches_individual_steps():
         s.close()
 
 
-def run_requests(subs, budget=int(8e9), max_active=8):
+def run_requests(subs, budget=int(8e9), max_active=8, batched=True):
     """subs: (tick at which to submit, body, steps); returns results by index."""
     srv = N.Server(budget, max_active=max_active)
+    srv.set_batched(batched)
     ids = {}
     tick = 0
     while True:
@@ -62,25 +63,34 @@ def run_requests(subs, budget=int(8e9), max_active=8):
     return out, stats
 
 
-def test_result_same_alone_and_in_mix():
+@pytest.mark.parametrize("batched", [True, False])
+def test_result_same_alone_and_in_mix(batched):
+    """A request's result is the same alone and in a mix that arrives before
+    and after it, stepped in one batch with the others (batched) or on its
+    own stream beside them; the two ways give the same bits too."""
     A = small_body(0)
-    alone, _ = run_requests([(0, A, 12)])
-    mix, st = run_requests([(0, small_body(1), 20), (2, A, 12), (3, small_body(2), 5), (7, small_body(3), 9)])
+    alone, _ = run_requests([(0, A, 12)], batched=batched)
+    mix, st = run_requests([(0, small_body(1), 20), (2, A, 12), (3, small_body(2), 5), (7, small_body(3), 9)],
+                           batched=batched)
     a, m = alone[0], mix[1]
     assert a["state"] == m["state"] == "done" and a["steps"] == m["steps"] == 12
     assert np.array_equal(a["forces"], m["forces"])
     assert a["n_final"] == m["n_final"]
     assert st["finished"] == 4 and st["step_ms_p99"] >= st["step_ms_p50"] > 0
     assert st["mean_resident"] > 1.0        # the bodies did overlap
+    other, _ = run_requests([(0, A, 12)], batched=not batched)
+    assert np.array_equal(a["forces"], other[0]["forces"]) and a["n_final"] == other[0]["n_final"]
 
 
 def test_small_body_is_not_held_back_by_a_large_one():
-    """Each body is relaunched as soon as its own step is collected: a small
+    """Per-body streams: each body is relaunched as soon as its own step is
+    collected: a small
     body finishes its steps while a large one submitted with it, asking for
     as many steps, is still running."""
     big = small_body(0, n0=600000, panels=400)
     small = small_body(1, n0=1000, panels=100)
     srv = N.Server(int(16e9), max_active=4)
+    srv.set_batched(False)          # per-body streams (a batch steps its members together)
     ib = srv.submit(*big, 12)
     isml = srv.submit(*small, 12)
     seen = False

@@ -21,6 +21,9 @@ class FakeServer:
         self.body_steps = 0
         FakeServer.instances.append(self)
 
+    def set_batched(self, on):
+        self.batched = bool(on)
+
     def submit(self, conf, pan, x, y, g, nsteps):
         rid = len(self.res) + 1
         self.res[rid] = {"state": "queued", "steps": 0, "want": nsteps}

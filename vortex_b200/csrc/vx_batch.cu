@@ -83,9 +83,20 @@ struct SlotSig {
     long long bound;
 };
 
-__global__ void k_batch_counts(const VxScalars *const *S, long long *out, int nb) {
+// What a batched step leaves of each member, gathered into one array that
+// is copied back after the step: count, d_g, Fx, Fy, M.
+constexpr int GATHER = 5;
+__global__ void k_batch_gather(const VxScalars *const *S, double *out, int nb) {
     VX_PDL_WAIT();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) out[i] = S[i]->n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+        const VxScalars *q = S[i];
+        double *o = out + (long long)GATHER * i;
+        o[0] = (double)q->n;
+        o[1] = q->dg;
+        o[2] = q->fx;
+        o[3] = q->fy;
+        o[4] = q->m;
+    }
 }
 
 long long pow2_at_least(long long v) {
@@ -115,11 +126,16 @@ struct vx_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<SlotSig> sig;
     const unsigned char *sig_arena = nullptr;
-    // counts after each step, copied back (two steps kept)
-    long long *d_counts = nullptr;
-    long long *h_counts[2] = {nullptr, nullptr};
+    const double *sig_gather = nullptr;
+    size_t sig_nb = 0;
+    // what each step left of its members (GATHER values each), copied back
+    // after the step (two steps kept), with the members of that step
+    double *d_gather = nullptr;
+    double *h_gather[2] = {nullptr, nullptr};
+    size_t gather_cap = 0;                  // members the buffers hold
     cudaEvent_t cnt_ev[2] = {nullptr, nullptr};
     long long cnt_step[2] = {-1, -1};
+    std::vector<vx_sim *> cnt_members[2];
     long long launched = 0;       // batched steps launched
     long long kernels = 0;        // kernels launched by the batched steps
     long long rebuilds = 0, reinstantiations = 0;
@@ -287,8 +303,8 @@ static vx_status build_graph(vx_batch *b) {
     }
     if (e == cudaSuccess) {
         const int nb = (int)b->bodies.size();
-        vx_launch_pdl(k_batch_counts, std::max(1, std::min(64, (nb + 255) / 256)), 256, 0, b->stream,
-                      scalars_list(b), b->d_counts, nb);
+        vx_launch_pdl(k_batch_gather, std::max(1, std::min(64, (nb + 255) / 256)), 256, 0, b->stream,
+                      scalars_list(b), b->d_gather, nb);
         e = cudaGetLastError();
     }
     cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
@@ -306,12 +322,16 @@ static vx_status build_graph(vx_batch *b) {
         return VX_ERR_CUDA;
     }
     b->sig_arena = b->d_arena;
+    b->sig_gather = b->d_gather;
+    b->sig_nb = b->bodies.size();
     b->reinstantiations += 1;
     return VX_OK;
 }
 
 static bool graph_fits(const vx_batch *b) {
-    if (!b->exec || b->sig_arena != b->d_arena || b->sig.size() != b->slots.size()) return false;
+    if (!b->exec || b->sig_arena != b->d_arena || b->sig_gather != b->d_gather || b->sig_nb != b->bodies.size() ||
+        b->sig.size() != b->slots.size())
+        return false;
     for (size_t j = 0; j < b->slots.size(); ++j) {
         const SlotSig &g = b->sig[j];
         const Slot &sl = b->slots[j];
@@ -410,9 +430,11 @@ static vx_status ensure_capacities(vx_batch *b) {
     if (k >= 0) {
         BCU(cudaEventSynchronize(b->cnt_ev[k]));
         const long long after = b->launched - 1 - b->cnt_step[k];   // steps launched after those counts
-        for (size_t i = 0; i < b->bodies.size(); ++i) {
-            vx_sim *s = b->bodies[i].s;
-            const long long bound = b->h_counts[k][i] + after * s->P;
+        const std::vector<vx_sim *> &mem = b->cnt_members[k];
+        for (size_t i = 0; i < mem.size(); ++i) {
+            vx_sim *s = mem[i];
+            if (!s->in_batch || s->stream != b->stream) continue;   // left the batch since
+            const long long bound = (long long)b->h_gather[k][GATHER * i] + after * s->P;
             if (bound < s->n_upper) s->n_upper = bound;
         }
     }
@@ -439,22 +461,129 @@ static void release(vx_batch *b) {
         vx_sim_read_scalars(s);   // the true count again
     }
     if (b->d_arena) cudaFree(b->d_arena);
-    if (b->d_counts) cudaFree(b->d_counts);
+    if (b->d_gather) cudaFree(b->d_gather);
     for (int k = 0; k < 2; ++k) {
         if (b->h_stage[k]) cudaFreeHost(b->h_stage[k]);
-        if (b->h_counts[k]) cudaFreeHost(b->h_counts[k]);
+        if (b->h_gather[k]) cudaFreeHost(b->h_gather[k]);
         if (b->stage_ev[k]) cudaEventDestroy(b->stage_ev[k]);
         if (b->cnt_ev[k]) cudaEventDestroy(b->cnt_ev[k]);
     }
     if (b->stream) cudaStreamDestroy(b->stream);
 }
 
+// Members' shares of the GPU: the scaled launches of all members together
+// fill it about twice; the divisor is kept while the total demand stays
+// within a factor of two of the one it was set for (a new divisor changes
+// every member's launch shapes, so all are recorded again).
+static void update_share(vx_batch *b) {
+    long long demand = 0;
+    for (const Body &bd : b->bodies) demand += vx_sim_step_sms(bd.s);
+    const int want = (int)std::max(1LL, demand / (2LL * b->num_sms));
+    if (want > 2 * b->share_div || 2 * want < b->share_div) b->share_div = want;
+}
+
+// Room for `nb` members in the gathered results (the device array is
+// stream-ordered: steps in flight still write the old one).
+static vx_status gather_room(vx_batch *b, size_t nb) {
+    if (nb <= b->gather_cap && b->d_gather) return VX_OK;
+    size_t cap = std::max<size_t>(std::max<size_t>(nb, 2 * b->gather_cap), 16);
+    for (int k = 0; k < 2; ++k) {
+        BCU(cudaEventSynchronize(b->cnt_ev[k]));   // its last copy has landed
+        if (b->h_gather[k]) cudaFreeHost(b->h_gather[k]);
+        b->h_gather[k] = nullptr;
+        b->cnt_step[k] = -1;
+        b->cnt_members[k].clear();
+        BCU(cudaMallocHost(&b->h_gather[k], sizeof(double) * GATHER * cap));
+    }
+    if (b->d_gather) BCU(cudaFreeAsync(b->d_gather, b->stream));
+    b->d_gather = nullptr;
+    BCU(cudaMallocAsync((void **)&b->d_gather, sizeof(double) * GATHER * cap, b->stream));
+    b->gather_cap = cap;
+    return VX_OK;
+}
+
+extern "C" vx_status vx_batch_new(int device, vx_batch **out) {
+    if (!out) return VX_ERR_ARG;
+    *out = nullptr;
+    BCU(cudaSetDevice(device));
+    vx_batch *b = new vx_batch();
+    b->device = device;
+    auto fail = [&](vx_status st) {
+        release(b);
+        delete b;
+        return st;
+    };
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VX_ERR_CUDA);
+    for (int k = 0; k < 2; ++k)
+        if (cudaEventCreateWithFlags(&b->stage_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->cnt_ev[k], cudaEventDisableTiming) != cudaSuccess)
+            return fail(VX_ERR_CUDA);
+    vx_status st = gather_room(b, 16);
+    if (st != VX_OK) return fail(st);
+    *out = b;
+    return VX_OK;
+}
+
+// A body joins at the next batched step: the batch's stream waits for the
+// work already queued on the body's own stream (no host wait).
+extern "C" vx_status vx_batch_add(vx_batch *b, vx_sim *s) {
+    if (!b || !s) return VX_ERR_ARG;
+    if (s->device != b->device || s->in_batch) {
+        vx_set_error("vx_batch_add: the body is on another device or already in a batch");
+        return VX_ERR_ARG;
+    }
+    BCU(cudaSetDevice(b->device));
+    cudaEvent_t e;
+    BCU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaError_t err = cudaEventRecord(e, s->stream);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(b->stream, e, 0);
+    cudaEventDestroy(e);
+    BCU(err);
+    Body bd;
+    bd.s = s;
+    b->bodies.push_back(std::move(bd));
+    s->own_stream = s->stream;
+    s->stream = b->stream;
+    s->in_batch = true;
+    vx_status st = gather_room(b, b->bodies.size());
+    if (st != VX_OK) return st;
+    update_share(b);
+    b->dirty = true;
+    return VX_OK;
+}
+
+// A body leaves after the batched steps already launched: its own stream
+// waits for them (no host wait) and it can be stepped alone again.
+extern "C" vx_status vx_batch_remove(vx_batch *b, vx_sim *s) {
+    if (!b || !s) return VX_ERR_ARG;
+    size_t i = 0;
+    while (i < b->bodies.size() && b->bodies[i].s != s) ++i;
+    if (i == b->bodies.size()) {
+        vx_set_error("vx_batch_remove: the body is not in this batch");
+        return VX_ERR_ARG;
+    }
+    BCU(cudaSetDevice(b->device));
+    cudaEvent_t e;
+    BCU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaError_t err = cudaEventRecord(e, b->stream);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(s->own_stream, e, 0);
+    cudaEventDestroy(e);
+    BCU(err);
+    s->stream = s->own_stream;
+    s->own_stream = nullptr;
+    s->in_batch = false;
+    b->bodies.erase(b->bodies.begin() + (long)i);
+    update_share(b);
+    b->dirty = true;
+    return VX_OK;
+}
+
 extern "C" vx_status vx_batch_create(vx_sim *const *sims, int count, vx_batch **out) {
     if (!sims || count < 1 || !out) return VX_ERR_ARG;
     *out = nullptr;
-    const int dev = sims[0] ? sims[0]->device : 0;
     for (int i = 0; i < count; ++i) {
-        if (!sims[i] || sims[i]->device != dev || sims[i]->in_batch) {
+        if (!sims[i] || sims[i]->device != sims[0]->device || sims[i]->in_batch) {
             vx_set_error("vx_batch_create: body %d is null, on another device or already in a batch", i);
             return VX_ERR_ARG;
         }
@@ -464,38 +593,14 @@ extern "C" vx_status vx_batch_create(vx_sim *const *sims, int count, vx_batch **
                 return VX_ERR_ARG;
             }
     }
-    BCU(cudaSetDevice(dev));
-    vx_batch *b = new vx_batch();
-    b->device = dev;
-    auto fail = [&](vx_status st) {
-        release(b);
-        delete b;
+    vx_batch *b = nullptr;
+    vx_status st = vx_batch_new(sims[0]->device, &b);
+    if (st != VX_OK) return st;
+    for (int i = 0; i < count && st == VX_OK; ++i) st = vx_batch_add(b, sims[i]);
+    if (st != VX_OK) {
+        vx_batch_destroy(b);
         return st;
-    };
-    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VX_ERR_CUDA);
-    for (int k = 0; k < 2; ++k) {
-        if (cudaEventCreateWithFlags(&b->stage_ev[k], cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&b->cnt_ev[k], cudaEventDisableTiming) != cudaSuccess ||
-            cudaMallocHost(&b->h_counts[k], sizeof(long long) * (size_t)count) != cudaSuccess)
-            return fail(VX_ERR_CUDA);
     }
-    if (cudaMalloc(&b->d_counts, sizeof(long long) * (size_t)count) != cudaSuccess) return fail(VX_ERR_NOMEM);
-    // every body's own work first, then the bodies launch on the batch stream
-    long long demand = 0;
-    for (int i = 0; i < count; ++i) {
-        vx_sim *s = sims[i];
-        if (cudaStreamSynchronize(s->stream) != cudaSuccess) return fail(VX_ERR_CUDA);
-        Body bd;
-        bd.s = s;
-        b->bodies.push_back(std::move(bd));
-        s->own_stream = s->stream;
-        s->stream = b->stream;
-        s->in_batch = true;
-        demand += vx_sim_step_sms(s);
-    }
-    // shares: the scaled launches of all bodies together about fill the GPU twice
-    b->share_div = (int)std::max(1LL, demand / (2LL * b->num_sms));
     *out = b;
     return VX_OK;
 }
@@ -503,21 +608,57 @@ extern "C" vx_status vx_batch_create(vx_sim *const *sims, int count, vx_batch **
 extern "C" vx_status vx_batch_step(vx_batch *b, int64_t nsteps) {
     if (!b || nsteps < 0) return VX_ERR_ARG;
     BCU(cudaSetDevice(b->device));
+    if (b->bodies.empty()) return VX_OK;
     for (int64_t t = 0; t < nsteps; ++t) {
         vx_status st = ensure_capacities(b);
         if (st != VX_OK) return st;
         if ((st = refresh(b)) != VX_OK) return st;
-        BCU(cudaGraphLaunch(b->exec, b->stream));
         const int k = (int)(b->launched & 1);
-        BCU(cudaMemcpyAsync(b->h_counts[k], b->d_counts, sizeof(long long) * b->bodies.size(),
+        BCU(cudaEventSynchronize(b->cnt_ev[k]));   // the host buffer of two steps ago has been read
+        BCU(cudaGraphLaunch(b->exec, b->stream));
+        BCU(cudaMemcpyAsync(b->h_gather[k], b->d_gather, sizeof(double) * GATHER * b->bodies.size(),
                             cudaMemcpyDeviceToHost, b->stream));
         BCU(cudaEventRecord(b->cnt_ev[k], b->stream));
         b->cnt_step[k] = b->launched;
+        b->cnt_members[k].clear();
+        for (const Body &bd : b->bodies) b->cnt_members[k].push_back(bd.s);
         b->launched += 1;
         b->kernels += (long long)b->slots.size() + 1;
         for (Body &bd : b->bodies) bd.s->n_upper += bd.s->P;
     }
     return VX_OK;
+}
+
+// Waits for batched step `step` (the index among the batch's steps; the
+// last two launched are kept) and reports, for each body that took part in
+// it (in the batch's order at that step), the count and the force sums it
+// left: 5 values per body (count, d_g, Fx, Fy, M).
+extern "C" vx_status vx_batch_results(vx_batch *b, int64_t step, vx_sim **members, double *out5, int cap,
+                                      int *count) {
+    if (!b || !count || cap < 0) return VX_ERR_ARG;
+    *count = 0;
+    const int k = (int)(step & 1);
+    if (step < 0 || b->cnt_step[k] != step) {
+        vx_set_error("vx_batch_results: step %lld is not one of the last two launched", (long long)step);
+        return VX_ERR_ARG;
+    }
+    BCU(cudaSetDevice(b->device));
+    BCU(cudaEventSynchronize(b->cnt_ev[k]));
+    const std::vector<vx_sim *> &mem = b->cnt_members[k];
+    const int n = (int)std::min<size_t>(mem.size(), (size_t)cap);
+    for (int i = 0; i < n; ++i) {
+        if (members) members[i] = mem[(size_t)i];
+        if (out5) memcpy(out5 + GATHER * i, b->h_gather[k] + GATHER * i, sizeof(double) * GATHER);
+    }
+    *count = (int)mem.size();
+    return VX_OK;
+}
+
+extern "C" vx_status vx_batch_last_results(vx_batch *b, vx_sim **members, double *out5, int cap, int *count) {
+    if (!b || !count) return VX_ERR_ARG;
+    *count = 0;
+    if (b->launched == 0) return VX_OK;
+    return vx_batch_results(b, b->launched - 1, members, out5, cap, count);
 }
 
 extern "C" vx_status vx_batch_sync(vx_batch *b) {

@@ -5,17 +5,26 @@
 // device-byte budget holds their estimate (vx_estimate_bytes at the largest
 // particle count the run can reach: start + P per step); then the body is
 // created (on worker threads: building a body's panel system takes tens of
-// milliseconds, during which the loop keeps relaunching the resident bodies)
-// and stays resident until its last step.  Each body has at most one
-// step in flight on its own stream; a tick launches the next step of every
-// resident body that has none in flight, waits until at least one step has
-// finished, collects every finished step (forces, count) and launches that
-// body's next step at once.  So no body waits for the slowest one: bodies of
-// different sizes overlap on the device and a small body takes many steps
-// while a large one takes one.  Finished bodies are released at once, which
-// frees their slot and budget for the next arrivals.  Each body runs in its
-// own handle with deterministic kernels, so its results do not depend on what
-// else runs.
+// milliseconds, during which the loop keeps stepping the resident bodies)
+// and stays resident until its last step.  Finished bodies are released at
+// once, which frees their slot and budget for the next arrivals.
+//
+// Two ways to step the resident bodies:
+//  * batched (default): the resident bodies are the members of one vx_batch,
+//    so each batched step runs every kernel of the step once for all of them
+//    (one CUDA graph).  Bodies join the batch at the step after their
+//    creation and leave it after their last step, so requests that arrive
+//    while others run are batched with them step by step (iteration-level
+//    continuous batching).  The next batched step is launched before the
+//    previous one is collected (its results come back in one copy), so the
+//    device does not wait for the host between steps.
+//  * per-body streams: each body has at most one step in flight on its own
+//    stream; a tick launches the next step of every resident body that has
+//    none in flight, waits until at least one has finished, collects every
+//    finished step and launches that body's next one at once.
+// Either way each body runs in its own handle with deterministic kernels, so
+// its results do not depend on what else runs (bit-identical alone and in
+// the mix).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -55,6 +64,8 @@ struct Request {
     vx_status create_st = VX_OK;   // set by the worker thread
     std::string create_err;        // the worker's error text when create_st != VX_OK
     int64_t done_steps = 0;
+    int64_t launched = 0;     // steps launched (batched form)
+    bool in_batch = false;
     std::vector<double> forces;   // 4 per step: dg, Fx, Fy, M
     int64_t n_final = 0;
     double t_submit = 0, t_admit = 0, t_finish = 0;
@@ -92,6 +103,17 @@ struct vx_server {
     double active_sum = 0.0;
     int64_t ticks = 0, body_steps = 0;
     double particle_steps = 0.0;      // sum over body steps of the particle count
+    // batched form
+    bool batched = true;
+    vx_batch *batch = nullptr;
+    struct Flight {
+        int64_t step;                     // the batch's step index
+        std::vector<Request *> members;
+        cudaEvent_t e0, e1;
+    };
+    std::deque<Flight> flight;
+    std::vector<cudaEvent_t> ev_pool;
+    int64_t batch_steps = 0;
 };
 
 // Launch the next step of resident body r on its stream, between its events.
@@ -129,7 +151,9 @@ static void collect_step(vx_server *S, Request *r) {
 }
 
 static vx_status release(vx_server *S, Request *r) {
-    if (r->sim) vx_destroy(r->sim);
+    if (r->in_batch && S->batch && r->sim) vx_batch_remove(S->batch, r->sim);
+    r->in_batch = false;
+    if (r->sim) vx_destroy(r->sim);   // waits for the steps it took part in
     r->sim = nullptr;
     if (r->e0) cudaEventDestroy(r->e0);
     if (r->e1) cudaEventDestroy(r->e1);
@@ -198,6 +222,12 @@ extern "C" vx_status vx_server_destroy(vx_server *S) {
         if (kv.second->state == 1) release(S, kv.second);
         delete kv.second;
     }
+    if (S->batch) vx_batch_destroy(S->batch);
+    for (auto &f : S->flight) {
+        cudaEventDestroy(f.e0);
+        cudaEventDestroy(f.e1);
+    }
+    for (cudaEvent_t e : S->ev_pool) cudaEventDestroy(e);
     delete S;
     return VX_OK;
 }
@@ -259,12 +289,9 @@ static void take_created(vx_server *S) {
     }
 }
 
-// Admit what fits, launch and collect steps as above, retire the
-// finished ones.  *active: bodies resident after the tick; *queued: waiting.
-extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queued) {
-    if (!S) return VX_ERR_ARG;
-    if (cudaSetDevice(S->device) != cudaSuccess) return VX_ERR_CUDA;
-    // admission in arrival order (slots and budget are held from here on)
+// Admission in arrival order (slots and budget are held from here on); the
+// admitted bodies are created on the worker threads.
+static void admit(vx_server *S) {
     while (!S->queue.empty() && (int)S->active.size() + S->creating < S->max_active &&
            S->used + S->queue.front()->est_bytes <= S->budget) {
         Request *r = S->queue.front();
@@ -279,18 +306,39 @@ extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queu
         }
         S->cv.notify_one();
     }
-    take_created(S);
-    // the next step of every resident body with none in flight
+}
+
+static bool created_waiting(vx_server *S) {
+    if (S->creating == 0) return false;
+    std::lock_guard<std::mutex> lk(S->mu);
+    return !S->created.empty();
+}
+
+// Release every body that is no longer resident (done or failed).
+static void retire(vx_server *S) {
+    std::vector<Request *> keep;
+    for (Request *r : S->active) {
+        if (r->state == 1) {
+            keep.push_back(r);
+            continue;
+        }
+        if (r->inflight) cudaEventSynchronize(r->e1);   // nothing of it may run on after release
+        r->t_finish = now_s();
+        if (r->state == 2) S->ttc_s.push_back(r->t_finish - r->t_submit);
+        release(S, r);
+    }
+    S->active.swap(keep);
+}
+
+// Per-body streams: launch the next step of every resident body with none
+// in flight, wait until some step has finished (whichever comes first: a
+// small body's step is not held back by a large one's), collect every
+// finished step and launch that body's next one at once.
+static void tick_streams(vx_server *S) {
     for (Request *r : S->active)
         if (r->state == 1 && !r->inflight) launch_step(S, r);
-    // wait until some step in flight has finished (whichever comes first:
-    // a small body's step is not held back by a large one's)
     for (;;) {
-        bool pending = S->creating > 0, any = false;
-        if (pending) {
-            std::lock_guard<std::mutex> lk(S->mu);
-            any = !S->created.empty();
-        }
+        bool pending = S->creating > 0, any = created_waiting(S);
         for (Request *r : S->active) {
             if (!r->inflight) continue;
             pending = true;
@@ -299,8 +347,6 @@ extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queu
         if (any || !pending) break;
         std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
-    // collect every finished step; launch that body's next one at once
-    std::vector<Request *> keep;
     for (Request *r : S->active) {
         if (r->inflight && r->state == 1) {
             const cudaError_t q = cudaEventQuery(r->e1);
@@ -312,23 +358,172 @@ extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queu
                 r->state = 3;
             }
         }
-        if (r->state == 1) {
-            keep.push_back(r);
-        } else {
-            if (r->inflight) cudaEventSynchronize(r->e1);   // nothing of it may run on after release
-            r->t_finish = now_s();
-            if (r->state == 2) S->ttc_s.push_back(r->t_finish - r->t_submit);
-            release(S, r);
-        }
     }
-    S->active.swap(keep);
+    retire(S);
     take_created(S);
     for (Request *r : S->active)
         if (r->state == 1 && !r->inflight) launch_step(S, r);
+}
+
+static cudaEvent_t pool_event(vx_server *S) {
+    cudaEvent_t e = nullptr;
+    if (!S->ev_pool.empty()) {
+        e = S->ev_pool.back();
+        S->ev_pool.pop_back();
+    } else {
+        cudaEventCreate(&e);
+    }
+    return e;
+}
+
+// Collect the oldest batched step in flight: per member its count and
+// force sums (one copy for all), its step time, completion.
+static void collect_flight(vx_server *S) {
+    vx_server::Flight f = S->flight.front();
+    S->flight.pop_front();
+    cudaEventSynchronize(f.e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, f.e0, f.e1);
+    S->ev_pool.push_back(f.e0);
+    S->ev_pool.push_back(f.e1);
+    std::vector<vx_sim *> mem(f.members.size());
+    std::vector<double> out(5 * f.members.size());
+    int cnt = 0;
+    const vx_status st = vx_batch_results(S->batch, f.step, mem.data(), out.data(), (int)mem.size(), &cnt);
+    for (size_t i = 0; i < f.members.size(); ++i) {
+        Request *r = f.members[i];
+        if (r->state != 1) continue;
+        if (st != VX_OK || (int)i >= cnt || mem[i] != r->sim) {
+            r->state = 3;
+            continue;
+        }
+        const double *o = out.data() + 5 * i;
+        S->step_ms.push_back(ms);
+        S->body_steps += 1;
+        S->particle_steps += o[0];
+        r->forces.insert(r->forces.end(), o + 1, o + 5);
+        r->done_steps += 1;
+        if (r->done_steps == r->steps) {
+            r->n_final = (int64_t)o[0];
+            r->state = 2;
+        }
+    }
+}
+
+// Batched: new bodies join the batch, bodies that have launched all their
+// steps leave it, the next batched step is launched (at most two in flight),
+// then the oldest step in flight is collected once it has finished (or a
+// created body is waiting to join).
+static vx_status tick_batched(vx_server *S) {
+    if (!S->batch) {
+        const vx_status st = vx_batch_new(S->device, &S->batch);
+        if (st != VX_OK) return st;
+    }
+    // keep two batched steps in flight: the host collects one while the
+    // device runs the next
+    while (S->flight.size() < 2) {
+        for (Request *r : S->active) {
+            if (r->state == 1 && !r->in_batch && r->launched < r->steps) {
+                if (vx_batch_add(S->batch, r->sim) != VX_OK) { r->state = 3; continue; }
+                r->in_batch = true;
+            }
+            if (r->in_batch && (r->launched >= r->steps || r->state != 1)) {
+                vx_batch_remove(S->batch, r->sim);   // after the steps in flight
+                r->in_batch = false;
+            }
+        }
+        vx_server::Flight f;
+        for (Request *r : S->active)
+            if (r->in_batch) f.members.push_back(r);
+        if (f.members.empty()) break;
+        cudaStream_t st = (cudaStream_t)vx_batch_stream(S->batch);
+        f.e0 = pool_event(S);
+        f.e1 = pool_event(S);
+        cudaEventRecord(f.e0, st);
+        double info[6];
+        vx_batch_info(S->batch, info);
+        f.step = (int64_t)info[0];
+        if (vx_batch_step(S->batch, 1) != VX_OK) {
+            for (Request *r : f.members) r->state = 3;
+            S->ev_pool.push_back(f.e0);
+            S->ev_pool.push_back(f.e1);
+            break;
+        }
+        cudaEventRecord(f.e1, st);
+        for (Request *r : f.members) r->launched += 1;
+        S->flight.push_back(f);
+        S->batch_steps += 1;
+    }
+    // collect the oldest step once it has finished; with fewer than two in
+    // flight and a body waiting to join, do not wait for it
+    while (!S->flight.empty()) {
+        const bool full = S->flight.size() >= 2;
+        if (cudaEventQuery(S->flight.front().e1) == cudaSuccess || full) {
+            collect_flight(S);
+            break;
+        }
+        if (created_waiting(S)) break;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    if (S->flight.empty() && S->active.empty() && S->creating > 0) {
+        // nothing to step: wait for a body to be created
+        while (!created_waiting(S)) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+    // a body leaves before its release; its last step has been collected
+    for (Request *r : S->active)
+        if (r->state != 1 && r->in_batch) {
+            vx_batch_remove(S->batch, r->sim);
+            r->in_batch = false;
+        }
+    bool referenced = false;
+    std::vector<Request *> keep;
+    for (Request *r : S->active) {
+        referenced = false;
+        for (const auto &fl : S->flight)
+            for (Request *q : fl.members) referenced |= (q == r);
+        if (r->state == 1 || referenced) {
+            keep.push_back(r);
+            continue;
+        }
+        r->t_finish = now_s();
+        if (r->state == 2) S->ttc_s.push_back(r->t_finish - r->t_submit);
+        release(S, r);
+    }
+    S->active.swap(keep);
+    take_created(S);
+    return VX_OK;
+}
+
+// Admit what fits, step the resident bodies (batched or per-body streams, as
+// above), retire the finished ones.  *active: bodies resident after the
+// tick; *queued: waiting.
+extern "C" vx_status vx_server_tick(vx_server *S, int64_t *active, int64_t *queued) {
+    if (!S) return VX_ERR_ARG;
+    if (cudaSetDevice(S->device) != cudaSuccess) return VX_ERR_CUDA;
+    admit(S);
+    take_created(S);
+    if (S->batched) {
+        const vx_status st = tick_batched(S);
+        if (st != VX_OK) return st;
+    } else {
+        tick_streams(S);
+    }
     S->ticks += 1;
     S->active_sum += (double)S->active.size();
     if (active) *active = (int64_t)S->active.size() + S->creating;
     if (queued) *queued = (int64_t)S->queue.size();
+    return VX_OK;
+}
+
+// 1: batched steps (default); 0: per-body streams.  Only while nothing is
+// resident.
+extern "C" vx_status vx_server_set_batched(vx_server *S, int on) {
+    if (!S) return VX_ERR_ARG;
+    if (!S->active.empty() || S->creating > 0) {
+        vx_set_error("vx_server_set_batched: bodies are resident");
+        return VX_ERR_ARG;
+    }
+    S->batched = on != 0;
     return VX_OK;
 }
 

@@ -70,12 +70,11 @@ def combine_serve(parts: list) -> dict:
     return out
 
 
-def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7,
-              precision: int = N.PREC_FP32, device: int = 0, rank: int = 0, world: int = 1,
-              mode: str = "graph") -> dict:
-    """The batched run of this rank's share of `bodies` seeded bodies."""
+def make_population(bodies: int = 256, seed: int = 7, precision: int = N.PREC_FP32, device: int = 0,
+                    rank: int = 0, world: int = 1):
+    """This rank's share of the seeded population, created on `device`:
+    (specs, sims, setup seconds)."""
     specs = [wl.body_spec(seed, i) for i in share(bodies, rank, world)]
-    bodies = len(specs)
     sims = []
     t0 = time.perf_counter()
     for sp in specs:
@@ -83,7 +82,18 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
         s = N.Sim(conf, pan, device=device)
         s.set_particles(x, y, g)
         sims.append(s)
-    setup_s = time.perf_counter() - t0
+    return specs, sims, time.perf_counter() - t0
+
+
+def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7,
+              precision: int = N.PREC_FP32, device: int = 0, rank: int = 0, world: int = 1,
+              mode: str = "graph", population=None) -> dict:
+    """The batched run of this rank's share of `bodies` seeded bodies (or of
+    an existing population from make_population, which is left open)."""
+    own = population is None
+    specs, sims, setup_s = population if population else make_population(bodies, seed, precision, device,
+                                                                           rank, world)
+    bodies = len(specs)
     batch = N.Batch(sims) if mode == "graph" else None
     if batch:
         batch.step(warmup)
@@ -138,14 +148,15 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
         out["graph_instantiations"] = info["graph_instantiations"]
         out["slot_table_rebuilds"] = info["rebuilds"]
         batch.close()
-    for s in sims:
-        s.close()
+    if own:
+        for s in sims:
+            s.close()
     return out
 
 
 def run_serve(requests: int = 32, rate: float = 50.0, budget_gb: float = 160.0, max_active: int = 256,
               seed: int = 11, precision: int = N.PREC_FP32, steps_lo: int = 50, steps_hi: int = 1000,
-              device: int = 0, rank: int = 0, world: int = 1) -> dict:
+              device: int = 0, rank: int = 0, world: int = 1, batched: bool = True) -> dict:
     """Poisson arrivals (rate per second) of `requests` bodies of the seeded
     population, each asking for U[steps_lo, steps_hi] steps; this rank serves
     its share of them, at their arrival times."""
@@ -158,6 +169,7 @@ def run_serve(requests: int = 32, rate: float = 50.0, budget_gb: float = 160.0, 
     requests = len(mine)
     bodies = [wl.make_body(sp, precision) for sp in specs]
     srv = N.Server(int(budget_gb * 1e9), max_active=max_active, device=device)
+    srv.set_batched(batched)
     ids = [None] * requests
     t0 = time.perf_counter()
     nxt = 0
@@ -177,6 +189,8 @@ def run_serve(requests: int = 32, rate: float = 50.0, budget_gb: float = 160.0, 
     res = [srv.result(i) for i in ids]
     srv.close()
     return {"requests": requests, "rate_per_s": rate, "budget_gb": budget_gb, "max_active": max_active,
+            "stepping": ("resident bodies batched step by step (vx_batch: one launch per kernel of the step)"
+                         if batched else "each resident body on its own stream"),
             "seed": seed, "precision": "fp32" if precision == N.PREC_FP32 else "fp64",
             "steps_requested": int(nsteps.sum()), "failed": sum(r["state"] == "failed" for r in res),
             "wall_s": wall, "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"],

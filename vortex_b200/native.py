@@ -387,6 +387,24 @@ class Batch:
     def step(self, nsteps: int = 1):
         _check(lib().vx_batch_step(self.h, C.c_int64(nsteps)), "vx_batch_step")
 
+    def add(self, sim):
+        _check(lib().vx_batch_add(self.h, sim.h), "vx_batch_add")
+        self.sims.append(sim)
+
+    def remove(self, sim):
+        _check(lib().vx_batch_remove(self.h, sim.h), "vx_batch_remove")
+        self.sims.remove(sim)
+
+    def last_results(self) -> dict:
+        """{sim handle value: (count, d_g, Fx, Fy, M)} after the last batched step."""
+        cap = max(len(self.sims), 1) + 64
+        mem = (C.c_void_p * cap)()
+        out = np.zeros(5 * cap)
+        cnt = C.c_int(0)
+        _check(lib().vx_batch_last_results(self.h, mem, _p(out), C.c_int(cap), C.byref(cnt)),
+               "vx_batch_last_results")
+        return {mem[i]: tuple(out[5 * i:5 * i + 5]) for i in range(min(cnt.value, cap))}
+
     def sync(self):
         _check(lib().vx_batch_sync(self.h), "vx_batch_sync")
 
@@ -445,6 +463,9 @@ class Server:
         _check(lib().vx_server_submit(self.h, C.byref(conf), _p(pan), C.c_int64(len(pan)), _p(x), _p(y), _p(g),
                                       C.c_int64(len(x)), C.c_int64(nsteps), C.byref(rid)), "vx_server_submit")
         return rid.value
+
+    def set_batched(self, on: bool):
+        _check(lib().vx_server_set_batched(self.h, C.c_int(int(on))), "vx_server_set_batched")
 
     def tick(self):
         """One scheduling round; returns (resident, queued) after it."""
