@@ -98,7 +98,10 @@ typedef struct vx_conf {
                                    Gauss-Jordan pivot rule (a pivot below
                                    1e-12 fails, as in the reference);
                                    1 = partial pivoting; 2 = the reference's
-                                   rule, partial pivoting if it fails */
+                                   rule, partial pivoting if it fails;
+                                   3 = blocked LU with partial pivoting
+                                   (fastest to build, about 20 kernels
+                                   per 32 columns) */
     int32_t fmm_leaf;           /* quadtree depth: mean vortices per leaf
                                    the depth aims at (default 32) */
     int32_t fmm_p;              /* expansion terms of the quadtree FMM: 8, 12, 16

@@ -243,6 +243,8 @@ cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, dou
     cudaMemsetAsync(d_flag, 0, sizeof(int), L.stream);
     vx_launch<k_panel_influence, k_panel_influence_body>(L, grid, 256, 0, d_pan, P, A);
     if (d_L_out) cudaMemcpyAsync(d_L_out, A, sizeof(double) * S * S, cudaMemcpyDeviceToDevice, L.stream);
+    if (robust == 3)   // blocked LU with partial pivoting (vx_lu.cu)
+        return vx_invert_lu(L, A, d_minv, S, reinterpret_cast<int *>(c), d_flag);
     vx_launch<k_identity, k_identity_body>(L, grid, 256, 0, d_minv, S);
     for (long long k = 0; k < S - 1; ++k) {
         vx_launch<k_gj_pivot, k_gj_pivot_body>(L, 1, 1024, 0, A, d_minv, S, k, c, d_flag, robust);

@@ -507,7 +507,8 @@ extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t
     if (cudaMalloc(&work, sizeof(double) * (2 * S1 * S1 + S1)) != cudaSuccess) return fail(VX_ERR_NOMEM);
     if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) { cudaFree(work); return fail(VX_ERR_NOMEM); }
     VxLaunch L = launch_of(s);
-    cudaError_t e = vx_build_matrix(L, s->d_pan, (int)P, s->d_minv, work, flag, nullptr, conf->gj_pivot == 1);
+    const int mode = conf->gj_pivot == 1 ? 1 : (conf->gj_pivot == 3 ? 3 : 0);
+    cudaError_t e = vx_build_matrix(L, s->d_pan, (int)P, s->d_minv, work, flag, nullptr, mode);
     int hflag = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);

@@ -507,6 +507,11 @@ cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &
 cudaError_t vx_build_matrix(const VxLaunch &L, const vx_panel *d_pan, int P, double *d_minv,
                             double *d_work, int *d_flag, double *d_L_out,
                             int robust = 0);
+// robust: 0 the reference's pivot rule, 1 Gauss-Jordan with partial
+// pivoting, 3 blocked LU with partial pivoting (vx_invert_lu).
+// A (n x n) -> Inv = A^-1 by blocked LU with partial pivoting; A is
+// overwritten, piv holds n ints; *flag set on a pivot below 1e-12.
+cudaError_t vx_invert_lu(const VxLaunch &L, double *A, double *Inv, long long n, int *piv, int *flag);
 cudaError_t vx_launch_birth_ld(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                VxWork &w, const vx_panel *pan, const double *minv, long long ld,
                                int rhs_chunks);
