@@ -233,6 +233,8 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.fmm_cnt, vx_fmm_cells(w.fmm_lmax));
     A(w.fmm_start, (1LL << (2 * w.fmm_lmax)) + 1);
     A(w.fmm_flags, cap); A(w.fmm_brute, cap);
+    A(w.fmm_sub_cnt, 1LL << (2 * (w.fmm_lmax + 1)));
+    A(w.fmm_sub_start, (1LL << (2 * (w.fmm_lmax + 1))) + 1);
     A(w.fmm_M, 2LL * fmm_p * vx_fmm_cells(w.fmm_lmax));
     A(w.fmm_L, 2LL * fmm_p * vx_fmm_cells(w.fmm_lmax));
 #undef A

@@ -117,6 +117,7 @@ VX_DEVK void k_fmm_params_body(VxBlkB<0, 0> vb, VxScalars *S, double eps, int Lm
     S->fL = L;
     S->fcnt_off = fmm_level_off(L);
     S->fnleaves = 1LL << (2 * L);
+    S->fnsub = 4 * S->fnleaves;
     S->fs = vx_round32(n);   // sources include the round-32 padding (3-nearest)
 }
 __global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
@@ -124,15 +125,17 @@ __global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
     k_fmm_params_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, eps, Lmax, leaf);
 }
 
-VX_DEVK void k_fmm_zero_cnt_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt) {
-    const long long tot = fmm_level_off(S->fL + 1);
-    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < tot;
-         c += (long long)vb.n * blockDim.x)
-        cnt[c] = 0;
+VX_DEVK void k_fmm_zero_cnt_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt, int *subcnt) {
+    const long long tot = fmm_level_off(S->fL + 1), nsub = S->fnsub;
+    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < tot + nsub;
+         c += (long long)vb.n * blockDim.x) {
+        if (c < tot) cnt[c] = 0;
+        else subcnt[c - tot] = 0;
+    }
 }
-__global__ void k_fmm_zero_cnt(const VxScalars *S, int *cnt) {
+__global__ void k_fmm_zero_cnt(const VxScalars *S, int *cnt, int *subcnt) {
     VX_PDL_WAIT();
-    k_fmm_zero_cnt_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt);
+    k_fmm_zero_cnt_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt, subcnt);
 }
 
 __device__ __forceinline__ long long fmm_leaf(const VxScalars *S, double x, double y) {
@@ -144,28 +147,62 @@ __device__ __forceinline__ long long fmm_leaf(const VxScalars *S, double x, doub
     return iy * m + ix;
 }
 
-// Leaf of every source slot [0, s); counts at the leaf level.
-VX_DEVK void k_fmm_leafid_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
-    const long long s = S->fs;
-    int *leafcnt = cnt + fmm_level_off(S->fL);
-    for (long long j = vb.x * (long long)blockDim.x + threadIdx.x; j < s;
-         j += (long long)vb.n * blockDim.x) {
-        const long long c = fmm_leaf(S, v.x[j * v.ps], v.y[j * v.ps]);
-        key[j] = (unsigned)c;
-        val[j] = (int)j;
-        atomicAdd(&leafcnt[c], 1);
-    }
-}
-__global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
-    VX_PDL_WAIT();
-    k_fmm_leafid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, key, val, cnt);
+// Cell of the level below the leaves of every source slot [0, s), as the
+// key 4 leaf + child (child = 2 (row & 1) + (column & 1) at that level), so
+// that sorting by it keeps each leaf's sources contiguous, its four quarters
+// one after the other; counts per key.  The leaf of the key is the one
+// fmm_leaf gives (x / (h/2) is exactly 2 (x / h)).
+__device__ __forceinline__ unsigned fmm_subkey(const VxScalars *S, double x, double y) {
+    const long long m2 = 2LL << S->fL;
+    const double h2 = 0.5 * (S->fside / (double)(m2 >> 1));
+    long long ix = (long long)floor((x - S->fx0) / h2), iy = (long long)floor((y - S->fy0) / h2);
+    ix = ix < 0 ? 0 : (ix >= m2 ? m2 - 1 : ix);
+    iy = iy < 0 ? 0 : (iy >= m2 ? m2 - 1 : iy);
+    const long long leaf = (iy >> 1) * (m2 >> 1) + (ix >> 1);
+    return (unsigned)(4 * leaf + 2 * (iy & 1) + (ix & 1));
 }
 
-// Leaf starts: exclusive scan of the leaf counts (chunked, device length).
+VX_DEVK void k_fmm_leafid_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, unsigned *key, int *val, int *subcnt) {
+    const long long s = S->fs;
+    for (long long j = vb.x * (long long)blockDim.x + threadIdx.x; j < s;
+         j += (long long)vb.n * blockDim.x) {
+        const unsigned k = fmm_subkey(S, v.x[j * v.ps], v.y[j * v.ps]);
+        key[j] = k;
+        val[j] = (int)j;
+        atomicAdd(&subcnt[k], 1);
+    }
+}
+__global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *val, int *subcnt) {
+    VX_PDL_WAIT();
+    k_fmm_leafid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, key, val, subcnt);
+}
+
+// Leaf counts (the tree's leaf level) and leaf starts from the quarters'.
+VX_DEVK void k_fmm_leaf_from_sub_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *subcnt, const int *substart,
+                                      int *cnt, int *start) {
+    const long long nl = S->fnleaves;
+    int *leafcnt = cnt + fmm_level_off(S->fL);
+    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c <= nl; c += (long long)vb.n * blockDim.x) {
+        if (c == nl) {
+            start[nl] = substart[4 * nl];
+            continue;
+        }
+        leafcnt[c] = subcnt[4 * c] + subcnt[4 * c + 1] + subcnt[4 * c + 2] + subcnt[4 * c + 3];
+        start[c] = substart[4 * c];
+    }
+}
+__global__ void k_fmm_leaf_from_sub(const VxScalars *S, const int *subcnt, const int *substart, int *cnt,
+                                    int *start) {
+    VX_PDL_WAIT();
+    k_fmm_leaf_from_sub_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, subcnt, substart, cnt, start);
+}
+
+// Starts of the quarters: exclusive scan of their counts (chunked, device
+// length).
 VX_DEVK void k_fmm_scan_sum_body(VxBlkB<FMM_T, 0> vb, const VxScalars *S, const int *cnt, int *csum) {
     __shared__ int sh[FMM_T];
-    const long long len = S->fnleaves, nch = vx_ceil_div(len, VX_CHUNK);
-    const int *c0 = cnt + fmm_level_off(S->fL);
+    const long long len = S->fnsub, nch = vx_ceil_div(len, VX_CHUNK);
+    const int *c0 = cnt;
     for (long long c = vb.x; c < nch; c += vb.n) {
         int k = 0;
         for (long long q = c * VX_CHUNK + threadIdx.x; q < min(len, (c + 1) * VX_CHUNK); q += blockDim.x) k += c0[q];
@@ -187,7 +224,7 @@ __global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, cons
 VX_DEVK void k_fmm_scan_top_body(VxBlkB<1024, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
     __shared__ long long sh[1024];
     __shared__ long long carry;
-    const long long nch = vx_ceil_div(S->fnleaves, VX_CHUNK);
+    const long long nch = vx_ceil_div(S->fnsub, VX_CHUNK);
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (long long base = 0; base < nch; base += blockDim.x) {
@@ -216,8 +253,8 @@ VX_DEVK void k_fmm_scan_apply_body(VxBlkB<FMM_T, 0> vb, const VxScalars *S, cons
                                    int *start) {
     constexpr int PER = VX_CHUNK / FMM_T;
     __shared__ int sh[FMM_T];
-    const long long len = S->fnleaves, nch = vx_ceil_div(len, VX_CHUNK);
-    const int *c0 = cnt + fmm_level_off(S->fL);
+    const long long len = S->fnsub, nch = vx_ceil_div(len, VX_CHUNK);
+    const int *c0 = cnt;
     if (vb.x == 0 && threadIdx.x == 0) start[len] = (int)S->fs;
     for (long long c = vb.x; c < nch; c += vb.n) {
         const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
@@ -256,7 +293,7 @@ VX_DEVK void k_fmm_gather_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, co
     for (long long k = vb.x * (long long)blockDim.x + threadIdx.x; k < s;
          k += (long long)vb.n * blockDim.x) {
         const long long j = sorted[k];
-        const unsigned col = skey[k] % m, row = skey[k] / m;
+        const unsigned leaf = skey[k] >> 2, col = leaf % m, row = leaf / m;
         const double ccx = S->fx0 + ((double)col + 0.5) * h, ccy = S->fy0 + ((double)row + 0.5) * h;
         srt[k] = make_float4((float)(v.x[j * v.ps] - ccx), (float)(v.y[j * v.ps] - ccy),
                              j < n ? (float)v.g[j * v.ps] : 0.0f, (float)col);
@@ -605,11 +642,12 @@ __global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const
     k_fmm_l2l_small_body<P>(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, S, cnt, Loc, l);
 }
 
-// Near field (FP32, core smoothing, 3 nearest) + far field (L2P, FP64): one
-// warp per work item of up to FMM_W targets of one leaf.  All of them share
-// the 3 x 3 leaves around it, whose sources the warp stages 32 at a time
-// (three contiguous runs of the leaf-sorted array), coordinates relative to
-// the item's leaf centre.
+// Near field (FP32, core smoothing) + far field (L2P, FP64): one warp per
+// work item of up to FMM_W targets of one leaf.  All of them share the 3 x 3
+// leaves around it, whose sources the warp stages 32 at a time (three
+// contiguous runs of the leaf-sorted array), coordinates relative to the
+// item's leaf centre.  The 3 nearest come from their own pass
+// (k_fmm_nn3_sub) over the finer grid of quarter leaves.
 __device__ __forceinline__ float vx_rcp_approx2(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -617,22 +655,21 @@ __device__ __forceinline__ float vx_rcp_approx2(float x) {
 }
 
 // Two near-field pairs (one target, sources a and b of a staged slot) in
-// packed FP32: core-smoothed Biot-Savart terms and the branch-free 3-nearest
-// insertion (the target's own slot, when SELF, left out of the latter; its
-// Biot-Savart term is 0 as dx = dy = 0).
-template <bool SELF>
-__device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gslot, int q2, int self_q, f2 TX,
-                                           f2 TY, float eps2, float &d1, float &d2, float &d3, f2 &SY,
-                                           f2 &SXN) {
+// packed FP32: core-smoothed Biot-Savart terms.  The target's own slot adds
+// 0 (dx = dy = 0), so no pair is skipped.  One reciprocal serves both pairs:
+// 1/a = b (1/(a b)), 1/b = a (1/(a b)) (a b stays within FP32 range: padding
+// sources sit 1e12 away, and both padded gives 1/inf = 0, G = 0).
+__device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gslot, f2 TX, f2 TY, float eps2,
+                                           f2 &SY, f2 &SXN) {
     const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(slot);
     const f2 G = *reinterpret_cast<const f2 *>(gslot);
     const f2 DX = f2_sub(TX, sq.x), DY = f2_sub(TY, sq.y);
     const f2 R2 = f2_fma(DX, DX, f2_mul(DY, DY));
     float r2a, r2b;
     f2_unpack(R2, r2a, r2b);
-    vx_nn3_insert_bf(d1, d2, d3, (SELF && q2 == self_q) ? 3e38f : r2a);
-    vx_nn3_insert_bf(d1, d2, d3, (SELF && q2 + 1 == self_q) ? 3e38f : r2b);
-    const f2 MM = f2_mul(G, f2_pack(vx_rcp_approx2(fmaxf(r2a, eps2)), vx_rcp_approx2(fmaxf(r2b, eps2))));
+    const float ra = fmaxf(r2a, eps2), rb = fmaxf(r2b, eps2);
+    const float q = vx_rcp_approx2(ra * rb);
+    const f2 MM = f2_mul(G, f2_mul(f2_pack(rb, ra), f2_pack(q, q)));
     SY = f2_fma(MM, DX, SY);
     SXN = f2_fma(MM, DY, SXN);   // sum of +mm dy: negated by the caller
 }
@@ -642,8 +679,7 @@ __device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gsl
 #endif
 template <int P>
 VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
-                             const int *sorted, const int *start, const int2 *items,
-                             const cplx *Loc, int *flag_list) {
+                             const int *sorted, const int *start, const int2 *items, const cplx *Loc) {
     __shared__ float4 sxy[FMM_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
     __shared__ float2 sg[FMM_T / 2];    // (G_a, G_b)
     const int lane = threadIdx.x & 31;
@@ -653,7 +689,6 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
     const int L = S->fL;
     const long long m = 1LL << L;
     const double h = S->fside / (double)m;
-    const float h2 = (float)(h * h);
     const float eps2 = (float)p.eps2;
     const long long nitems = S->cnitems;
     const cplx *LL = Loc + fmm_level_off(L) * P;
@@ -669,7 +704,6 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
         const long long j_self = valid ? sorted[t] : -1;
         const long long c0 = max(col - 1, 0LL), c1 = min(col + 1, m - 1);
         const f2 TX = f2_pack(me.x, me.x), TY = f2_pack(me.y, me.y);
-        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
         double ax = 0.0, ay = 0.0;
         // the 3 x 3 leaves are three contiguous runs (rows row-1..row+1 of
         // columns c0..c1), walked as one stream in chunks of 32 sources, so
@@ -691,12 +725,9 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
             rpre[r + 1] = rpre[r] + len;
         }
         const int total = rpre[3];
-        // the target's own position in the stream (its leaf lies in row `row`)
-        const bool own1 = row > r_lo;   // the own row is run 1, else run 0 (top row of the grid)
-        const int f_self = valid ? (own1 ? rpre[1] + (int)(t - rj0[1]) : (int)(t - rj0[0])) : -1000;
         for (int jt = 0; jt < total; jt += 32) {
-            // padding: G = 0 sources far away add exactly 0 and never enter the 3 nearest
-            float x = 1e18f, y = 1e18f, g = 0.f;
+            // padding: G = 0 sources far away add exactly 0
+            float x = 1e12f, y = 1e12f, g = 0.f;
             const int f = jt + lane;
             if (f < total) {
                 const bool in0 = f < rpre[1], in1 = f < rpre[2];
@@ -711,29 +742,17 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
             slot[2 + (lane & 1)] = y;
             reinterpret_cast<float *>(wg + (lane >> 1))[lane & 1] = g;
             __syncwarp();
-            const int rel = f_self - jt;   // the target's own slot within the chunk, if any
-            const int self_q = (rel >= 0 && rel < 32) ? rel : -1;
             f2 SY = 0ull, SXN = 0ull;   // +0.0f in both halves
-            // only chunks that hold one of the warp's own targets need the
-            // self test; the others take the loop without it
-            if (__any_sync(0xffffffffu, self_q >= 0)) {
-#pragma unroll 8
-                for (int q = 0; q < 16; ++q)
-                    near_pair2<true>(wxy + q, wg + q, 2 * q, self_q, TX, TY, eps2, d1, d2, d3, SY, SXN);
-            } else {
-#pragma unroll 8
-                for (int q = 0; q < 16; ++q)
-                    near_pair2<false>(wxy + q, wg + q, 2 * q, self_q, TX, TY, eps2, d1, d2, d3, SY, SXN);
-            }
+#pragma unroll 16
+            for (int q = 0; q < 16; ++q) near_pair2(wxy + q, wg + q, TX, TY, eps2, SY, SXN);
             __syncwarp();
             float a, b;   // the two halves are added in FP32, then carried in FP64
             f2_unpack(SXN, a, b); ax -= (double)(a + b);
             f2_unpack(SY, a, b); ay += (double)(a + b);
         }
-        const long long scanned = total;
         {   // executed near-field pairs: every target of the item sees the same 3x3 leaves
             const unsigned long long nv = __popc(__ballot_sync(0xffffffffu, valid));
-            if (lane == 0) atomicAdd(&S->pairs_bs, (unsigned long long)scanned * nv);
+            if (lane == 0) atomicAdd(&S->pairs_bs, (unsigned long long)total * nv);
         }
         if (valid && j_self < n) {
             // far field: f(z) = sum a_l u^l at the target's leaf (none below depth 2)
@@ -748,24 +767,69 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
                     f = cadd(cmul(f, cscale(u, c_fmm_inv[l + 1])), LL[leaf * P + l]);
             }
             // u - i v = f / (2 pi i): vx = Im f / 2pi, vy = Re f / 2pi
-            const double vx = (ax + f.i) / VX_TWO_PI + S->vinf[0];
-            const double vy = (ay + f.r) / VX_TWO_PI + S->vinf[1];
-            v.vx[j_self * v.vs] = vx;
-            v.vy[j_self * v.vs] = vy;
-            v.d[j_self] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
-            if (!(d3 < h2)) {   // a closer particle could lie outside the 3x3 block
-                const int slot = atomicAdd(&S->fnflag, 1);
-                flag_list[slot] = (int)t;
-            }
+            v.vx[j_self * v.vs] = (ax + f.i) / VX_TWO_PI + S->vinf[0];
+            v.vy[j_self * v.vs] = (ay + f.r) / VX_TWO_PI + S->vinf[1];
         }
     }
 }
 template <int P>
 __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, VxView v, VxScalars *S, const float4 *srt,
                                                    const int *sorted, const int *start, const int2 *items,
-                                                   const cplx *Loc, int *flag_list) {
+                                                   const cplx *Loc) {
     VX_PDL_WAIT();
-    k_fmm_near_body<P>(VxBlkB<FMM_T, VX_NEAR_MINB>{blockIdx.x, gridDim.x}, p, v, S, srt, sorted, start, items, Loc, flag_list);
+    k_fmm_near_body<P>(VxBlkB<FMM_T, VX_NEAR_MINB>{blockIdx.x, gridDim.x}, p, v, S, srt, sorted, start, items, Loc);
+}
+
+// The 3 nearest sources of every live target (the reference's padded
+// launch: sources include the round-32 slots after the live ones; the
+// target itself excluded), one thread per target, over the 3 x 3 quarter
+// leaves around its own quarter (each quarter a contiguous run of the
+// sorted sources; coordinates relative to the target's leaf centre,
+// computed as the near field computes them).  Exact when the third distance
+// is below the quarter's side (every source outside the 3 x 3 block is
+// farther); the others go to the ring search over leaves (k_fmm_nn3_fix).
+VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S, const float4 *srt, const unsigned *skey,
+                                const int *sorted, const int *substart, int *flag_list) {
+    const long long s = S->fs, n = S->n;
+    const long long m = 1LL << S->fL, m2 = 2 * m;
+    const double h = S->fside / (double)m;
+    const float sq2 = (float)(0.25 * h * h);   // (quarter side)^2
+    for (long long t = vb.x * (long long)blockDim.x + threadIdx.x; t < s; t += (long long)vb.n * blockDim.x) {
+        const long long j = sorted[t];
+        if (j >= n) continue;
+        const unsigned key = skey[t];
+        const long long leaf = key >> 2, col = leaf % m, row = leaf / m;
+        const long long ix2 = 2 * col + (key & 1), iy2 = 2 * row + ((key >> 1) & 1);
+        const float4 me = srt[t];
+        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
+        for (long long Y2 = max(iy2 - 1, 0LL); Y2 <= min(iy2 + 1, m2 - 1); ++Y2) {
+            const long long lr = Y2 >> 1;
+            const float oy = (float)((double)(lr - row) * h);
+            for (long long X2 = max(ix2 - 1, 0LL); X2 <= min(ix2 + 1, m2 - 1); ++X2) {
+                const long long lc = X2 >> 1;
+                const long long k = 4 * (lr * m + lc) + 2 * (Y2 & 1) + (X2 & 1);
+                const int q0 = substart[k], q1 = substart[k + 1];
+                for (int qq = q0; qq < q1; ++qq) {
+                    if (qq == t) continue;
+                    const float4 q = srt[qq];
+                    const float x = q.x + (float)(((double)q.w - (double)col) * h);
+                    const float y = q.y + oy;
+                    const float dx = me.x - x, dy = me.y - y;
+                    vx_nn3_insert_bf(d1, d2, d3, fmaf(dx, dx, dy * dy));
+                }
+            }
+        }
+        v.d[j] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
+        if (!(d3 < sq2)) {   // a closer source could lie outside the 3x3 quarters
+            const int slot = atomicAdd(&S->fnflag, 1);
+            flag_list[slot] = (int)t;
+        }
+    }
+}
+__global__ void __launch_bounds__(FMM_T) k_fmm_nn3_sub(VxView v, VxScalars *S, const float4 *srt, const unsigned *skey,
+                                                      const int *sorted, const int *substart, int *flag_list) {
+    VX_PDL_WAIT();
+    k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, v, S, srt, skey, sorted, substart, flag_list);
 }
 
 // Targets whose third-nearest distance reached the leaf side: exact 3
@@ -998,13 +1062,18 @@ static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxVi
     vx_launch<k_fmm_begin, k_fmm_begin_body>(L, 1, 1, 0, S);
     vx_launch<k_fmm_bbox, k_fmm_bbox_body>(L, grid, FMM_T, 0, v, S);
     vx_launch<k_fmm_params, k_fmm_params_body>(L, 1, 1, 0, S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32);
-    vx_launch<k_fmm_zero_cnt, k_fmm_zero_cnt_body>(L, grid, FMM_T, 0, S, w.fmm_cnt);
-    vx_launch<k_fmm_leafid, k_fmm_leafid_body>(L, grid, FMM_T, 0, v, S, w.key0, w.val0, w.fmm_cnt);
-    vx_launch<k_fmm_scan_sum, k_fmm_scan_sum_body>(L, grid, FMM_T, 0, S, w.fmm_cnt, w.cell_chunk_cnt);
+    vx_launch<k_fmm_zero_cnt, k_fmm_zero_cnt_body>(L, grid, FMM_T, 0, S, w.fmm_cnt, w.fmm_sub_cnt);
+    vx_launch<k_fmm_leafid, k_fmm_leafid_body>(L, grid, FMM_T, 0, v, S, w.key0, w.val0, w.fmm_sub_cnt);
+    vx_launch<k_fmm_scan_sum, k_fmm_scan_sum_body>(L, grid, FMM_T, 0, S, (const int *)w.fmm_sub_cnt, w.cell_chunk_cnt);
     vx_launch<k_fmm_scan_top, k_fmm_scan_top_body>(L, 1, 1024, 0, S, w.cell_chunk_cnt, w.cell_chunk_off);
-    vx_launch<k_fmm_scan_apply, k_fmm_scan_apply_body>(L, grid, FMM_T, 0, S, w.fmm_cnt, w.cell_chunk_off, w.fmm_start);
+    vx_launch<k_fmm_scan_apply, k_fmm_scan_apply_body>(L, grid, FMM_T, 0, S, (const int *)w.fmm_sub_cnt, w.cell_chunk_off,
+                                                       w.fmm_sub_start);
+    vx_launch<k_fmm_leaf_from_sub, k_fmm_leaf_from_sub_body>(L, grid, FMM_T, 0, S, (const int *)w.fmm_sub_cnt,
+                                                             (const int *)w.fmm_sub_start, w.fmm_cnt, w.fmm_start);
     // leaf order: each leaf's sources in index order (a stable sort by leaf)
-    vx_bucket_order(L, S, &S->fs, &S->fnleaves, w.key0, w.fmm_start, w.fmm_cnt, &S->fcnt_off, w.key1, w.val1,
+    // source order: by quarter-leaf, each quarter's sources in index order
+    // (a stable sort by the key 4 leaf + child; each leaf stays contiguous)
+    vx_bucket_order(L, S, &S->fs, &S->fnsub, w.key0, w.fmm_sub_start, w.fmm_sub_cnt, nullptr, w.key1, w.val1,
                     w.bk_mid, w.bk_big, w.val0);
     const unsigned *skey = w.key1;
     const int *sorted = w.val1;
@@ -1039,8 +1108,11 @@ static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxVi
     vx_launch<k_fmm_items, k_fmm_items_body>(L, grid, FMM_T, 0, S, w.fmm_start, w.row_items, w.row_item_off, w.items, w.items_cap);
 
     VX_EV(L, 0);
-    vx_launch<k_fmm_near<P>, k_fmm_near_body<P>>(L, L.num_sms * 8, FMM_T, 0, p, v, S, w.srt, sorted, w.fmm_start, w.items, (const cplx *)w.fmm_L, w.fmm_flags);
+    vx_launch<k_fmm_near<P>, k_fmm_near_body<P>>(L, L.num_sms * 8, FMM_T, 0, p, v, S, w.srt, sorted, w.fmm_start,
+                                                 w.items, (const cplx *)w.fmm_L);
     VX_EV(L, 1);
+    vx_launch<k_fmm_nn3_sub, k_fmm_nn3_sub_body>(L, grid, FMM_T, 0, v, S, w.srt, skey, sorted,
+                                                 (const int *)w.fmm_sub_start, w.fmm_flags);
 
     vx_launch<k_fmm_nn3_fix, k_fmm_nn3_fix_body>(L, grid, FMM_T, 0, v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
 

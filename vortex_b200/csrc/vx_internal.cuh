@@ -96,6 +96,7 @@ struct VxScalars {
     unsigned long long fb[4];
     double fx0, fy0, fside;
     long long fnleaves, fs;
+    long long fnsub;       // cells of the level below the leaves (4 per leaf): the 3-nearest grid
     int fL, fnflag;
     int fnbrute;           // flagged targets left to the whole-set 3-nearest scan
     int bk_nmid, bk_nbig;  // buckets of 17..128 / more elements in the running bucket order (vx_sort.cu)
@@ -158,6 +159,7 @@ struct VxWork {
     // quadtree: counts and expansions of every level up to fmm_lmax
     int fmm_lmax;
     int *fmm_cnt, *fmm_start, *fmm_flags, *fmm_brute;
+    int *fmm_sub_cnt, *fmm_sub_start;   // counts / starts of the level below the leaves
     int fmm_p;               // expansion terms the two arrays below were sized for
     double *fmm_M, *fmm_L;   // complex FP64 pairs, fmm_p per cell
 };
