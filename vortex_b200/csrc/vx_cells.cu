@@ -383,6 +383,35 @@ __device__ __forceinline__ bool diff_window(int dy, float R, float xlo, float xh
 // polynomial 2^x on the FMA and integer pipes (round by adding 1.5 * 2^23,
 // exponent added to the bit pattern) for one or both pairs of a step was
 // measured 30 % slower on the whole kernel: those pipes then limit.
+// 2^x of both halves on the FMA pipe (Cody-Waite reduction to the nearest
+// integer k by adding 1.5 * 2^23, f = x - k in [-1/2, 1/2], then a degree-5
+// polynomial p(f) ~ 2^f whose coefficients were fitted here for least
+// relative error on [-1/2, 1/2] (7.5e-8; 2.3e-7 after FP32 rounding, as
+// ex2.approx), and k added to p's exponent field by one integer
+// multiply-add).  The halves are clamped to -125 first, so the exponent
+// stays normal; for x that low the value is below 3e-38 either way.
+__device__ __forceinline__ f2 diff_exp2_fma(float xa, float xb) {
+    const f2 X = f2_pack(fmaxf(xa, -125.0f), fmaxf(xb, -125.0f));
+    const f2 MAGIC = f2_pack(12582912.0f, 12582912.0f);
+    const f2 T = f2_add(X, MAGIC);
+    const f2 F = f2_sub(X, f2_sub(T, MAGIC));
+    f2 P = f2_pack(1.3276184150891887e-3f, 1.3276184150891887e-3f);
+    P = f2_fma(P, F, f2_pack(9.675540302623352e-3f, 9.675540302623352e-3f));
+    P = f2_fma(P, F, f2_pack(5.5507141714826916e-2f, 5.5507141714826916e-2f));
+    P = f2_fma(P, F, f2_pack(2.402211974958503e-1f, 2.402211974958503e-1f));
+    P = f2_fma(P, F, f2_pack(6.931469665054077e-1f, 6.931469665054077e-1f));
+    P = f2_fma(P, F, f2_pack(1.000000071646687f, 1.000000071646687f));
+    float pa, pb, ta, tb;
+    f2_unpack(P, pa, pb);
+    f2_unpack(T, ta, tb);
+    return f2_pack(__uint_as_float(__float_as_uint(pa) + (__float_as_uint(ta) << 23)),
+                   __uint_as_float(__float_as_uint(pb) + (__float_as_uint(tb) << 23)));
+}
+
+#ifndef VX_DIFF_POLY_EVERY
+#define VX_DIFF_POLY_EVERY 0   // every k-th pair step takes its 2^x on the FMA pipe (0: none)
+#endif
+template <bool POLY = false>
 __device__ __forceinline__ void diff_pair2(const float4 *slot, const float2 *gslot, f2 TX, f2 TY, f2 NDD,
                                            float thr2, f2 &S2X, f2 &S2Y, f2 &S1) {
     const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(slot);
@@ -395,8 +424,15 @@ __device__ __forceinline__ void diff_pair2(const float4 *slot, const float2 *gsl
     const f2 ARG = f2_mul(f2_mul(R2, RD), NDD);
     float aa, ab;
     f2_unpack(ARG, aa, ab);
-    const float ea = r2a > thr2 ? vx_ex2_approx(aa) : 0.0f;
-    const float eb = r2b > thr2 ? vx_ex2_approx(ab) : 0.0f;
+    float ea, eb;
+    if (POLY) {
+        f2_unpack(diff_exp2_fma(aa, ab), ea, eb);
+    } else {
+        ea = vx_ex2_approx(aa);
+        eb = vx_ex2_approx(ab);
+    }
+    ea = r2a > thr2 ? ea : 0.0f;
+    eb = r2b > thr2 ? eb : 0.0f;
     const f2 GE = f2_mul(G, f2_pack(ea, eb));
     const f2 M = f2_mul(GE, RD);
     S2X = f2_fma(M, DX, S2X);   // sums of +m dx, +m dy: negated by the caller
@@ -546,7 +582,13 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
             }
             f2 S2X = 0ull, S2Y = 0ull, S1 = 0ull;   // +0.0f in both halves
             VX_UNROLL(VX_DIFF_UNROLL)
-            for (int q = 0; q < 16; ++q) diff_pair2(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
+            for (int q = 0; q < 16; ++q) {
+                if (VX_DIFF_POLY_EVERY > 0 && q % (VX_DIFF_POLY_EVERY > 0 ? VX_DIFF_POLY_EVERY : 1) ==
+                                                  VX_DIFF_POLY_EVERY - 1)
+                    diff_pair2<true>(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
+                else
+                    diff_pair2<false>(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
+            }
             __syncwarp();
             float a, b;   // the two halves are added in FP32, then carried in FP64
             f2_unpack(S2X, a, b); I2x -= (double)(a + b);
