@@ -320,6 +320,7 @@ def run_ours(args, rank, world, device):
     if args.crossover and rank == 0:
         from vortex_b200 import autotune
         cross = autotune.crossover(device=device)
+    plate = plate_leg(args, device) if args.plate_steps > 0 and rank == 0 else None
     if rank != 0:
         return None
     value = world * 1e3 * K / total_ms
@@ -399,10 +400,44 @@ def run_ours(args, rank, world, device):
         line["reference_cuda_build"] = ref_cuda_build(args, x0, y0, g0)
     if multi:
         line["batched"], line["served"] = multi
+    if plate:
+        line["plate_config"] = plate
     if cross:
         line["crossover"] = {"what": "velocity stage (FP32) on the benchmark wake: direct sum against the best "
                                      "accurate FMM setting, ms", "rows": cross}
     return line
+
+
+def plate_leg(args, device):
+    """The plate configuration at its scale: the 2576-panel rounded plate at
+    20 degrees of incidence, Re 1e4, dt 0.001, FP32 bulk, from a seeded warm
+    wake of args.plate_n vortices: steps/s over args.plate_steps event-timed
+    steps (graph replay) and the 64 x 64 probe grid against the plain FP64
+    direct sum over the same vortices.  (The 5000-step run with its Cd/Cl
+    statistics is `python -m vortex_b200.runs config3`.)"""
+    from vortex_b200 import native as Nt
+    from vortex_b200 import profiles
+    from vortex_b200 import runs
+    from vortex_b200 import workloads as wl
+    pan = profiles.rotate(profiles.rounded_plate(2576), -20.0)
+    sim = Nt.Sim(runs.plate_conf(Nt.PREC_FP32, pan), pan, device=device)
+    sim.set_particles(*wl.warm_wake(args.plate_n, seed=4321))
+    sim.step(2)
+    sim.sync()
+    st = sim.stream()
+    ms = []
+    for _ in range(args.plate_steps):
+        a, b = Nt.Event(), Nt.Event()
+        a.record(st)
+        sim.step(1)
+        b.record(st)
+        ms.append(a.elapsed_ms(b))
+    rec = {"workload": "rounded plate chord 1, thickness 0.02, 2576 panels, 20 deg incidence, Re 1e4, dt 0.001, "
+                       f"FP32 bulk, seeded warm wake of {args.plate_n} vortices",
+           "steps": args.plate_steps, "steps_per_s": 1e3 * len(ms) / sum(ms), "ms_p50": float(np.percentile(ms, 50)),
+           "n_particles_end": sim.count(), "probe_grid_vs_fp64_direct": runs.probe_error(sim, pan, device)}
+    sim.close()
+    return rec
 
 
 def multibody_runs(args, device, rank, world):
@@ -598,6 +633,8 @@ def main():
                     help="also time the reference's own CUDA build for this many steps (0: off)")
     ap.add_argument("--ref-cuda-timeout", type=float, default=900.0)
     ap.add_argument("--no-autotune", action="store_true", help="skip the untimed autotuning before timing")
+    ap.add_argument("--plate-steps", type=int, default=10, help="steps of the plate leg (0: skip)")
+    ap.add_argument("--plate-n", type=int, default=3_000_000)
     ap.add_argument("--no-crossover", dest="crossover", action="store_false",
                     help="skip the direct-vs-FMM crossover table (untimed)")
     ap.add_argument("--no-multibody", dest="multibody", action="store_false",
