@@ -791,25 +791,26 @@ __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, Vx
 VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S, const float4 *srt, const unsigned *skey,
                                 const int *sorted, const int *substart, int *flag_list) {
     const long long s = S->fs, n = S->n;
-    const long long m = 1LL << S->fL, m2 = 2 * m;
+    const int m = 1 << S->fL, m2 = 2 * m;
     const double h = S->fside / (double)m;
     const float sq2 = (float)(0.25 * h * h);   // (quarter side)^2
     for (long long t = vb.x * (long long)blockDim.x + threadIdx.x; t < s; t += (long long)vb.n * blockDim.x) {
-        const long long j = sorted[t];
+        const int j = sorted[t];
         if (j >= n) continue;
         const unsigned key = skey[t];
-        const long long leaf = key >> 2, col = leaf % m, row = leaf / m;
-        const long long ix2 = 2 * col + (key & 1), iy2 = 2 * row + ((key >> 1) & 1);
+        const int leaf = (int)(key >> 2), col = leaf % m, row = leaf / m;
+        const int ix2 = 2 * col + (int)(key & 1), iy2 = 2 * row + (int)((key >> 1) & 1);
         const float4 me = srt[t];
         float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
-        for (long long Y2 = max(iy2 - 1, 0LL); Y2 <= min(iy2 + 1, m2 - 1); ++Y2) {
-            const long long lr = Y2 >> 1;
+        const int y0 = max(iy2 - 1, 0), y1 = min(iy2 + 1, m2 - 1);
+        const int x0 = max(ix2 - 1, 0), x1 = min(ix2 + 1, m2 - 1);
+        for (int Y2 = y0; Y2 <= y1; ++Y2) {
+            const int lr = Y2 >> 1;
             const float oy = (float)((double)(lr - row) * h);
-            for (long long X2 = max(ix2 - 1, 0LL); X2 <= min(ix2 + 1, m2 - 1); ++X2) {
-                const long long lc = X2 >> 1;
-                const long long k = 4 * (lr * m + lc) + 2 * (Y2 & 1) + (X2 & 1);
-                const int q0 = substart[k], q1 = substart[k + 1];
-                for (int qq = q0; qq < q1; ++qq) {
+            for (int X2 = x0; X2 <= x1; ++X2) {
+                const int k = 4 * (lr * m + (X2 >> 1)) + 2 * (Y2 & 1) + (X2 & 1);
+                const int q1 = substart[k + 1];
+                for (int qq = substart[k]; qq < q1; ++qq) {
                     if (qq == t) continue;
                     const float4 q = srt[qq];
                     const float x = q.x + (float)(((double)q.w - (double)col) * h);
