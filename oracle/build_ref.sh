@@ -6,10 +6,12 @@
 # reference's src/main.c would otherwise provide.  Outputs go only to
 # oracle/_ref/, which git ignores; the .so travels to the GPU machine.
 #
-#   REF=<reference checkout> oracle/build_ref.sh
+#   VX_REFERENCE_DIR=<reference checkout> oracle/build_ref.sh
+# (default: the checkout this repository was built beside, /root/reference).
+# Exits 3 when the reference sources are not there.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${REF:-/root/reference}"
+REF="${VX_REFERENCE_DIR:-${REF:-/root/reference}}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-nvcc}"
 if [ ! -f "$REF/src/unit_1.cu" ] || [ ! -f "$REF/src/kernel.cu" ]; then

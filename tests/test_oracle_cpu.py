@@ -45,12 +45,14 @@ def test_singular_panel_system_is_reported():
         O.panel_matrix(pan)
 
 
-REF_PROFILE = "/root/reference/profiles/Profile_file_krug_1000.txt"
+GOLDEN_PROFILE = os.path.join(os.path.dirname(__file__), "golden", "krug_1000_profile.npz")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_PROFILE), reason="reference checkout absent")
 def test_circle_generator_matches_shipped_profile():
-    ref = profiles.read_profile(REF_PROFILE)
+    """The generated 1000-panel circle against the reference's shipped
+    profiles/Profile_file_krug_1000.txt (recorded as a fixture by
+    tests/golden/make_profile_golden.py)."""
+    ref = np.load(GOLDEN_PROFILE)
     mine = profiles.circle(1000)
     for f in ("left", "right", "contr", "birth", "norm", "tang"):
         assert np.abs(ref[f] - mine[f]).max() < 1e-6    # the file prints 6 digits
