@@ -65,10 +65,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs = list(ex.map(lambda s: _compile(s, force, hm, verbose), srcs))
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC, "-shared", "--cudart", "shared", *ARCH, "-o", LIB, *objs]
+        tmp = LIB + ".tmp"          # linked aside, then renamed: the library is never seen half written
+        cmd = [NVCC, "-shared", "--cudart", "shared", *ARCH, "-o", tmp, *objs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stderr)
+        os.replace(tmp, LIB)
     cli_src = os.path.join(CSRC, "vortex_cli.cpp")
     if os.path.exists(cli_src):
         os.makedirs(os.path.dirname(CLI), exist_ok=True)
