@@ -171,6 +171,17 @@ def measured_peaks() -> dict:
         return {}
 
 
+def guarded(what, fn, *a, **kw):
+    """An optional leg of the line: its record, or the error it raised (the
+    headline keys never depend on it)."""
+    try:
+        return fn(*a, **kw)
+    except Exception as e:   # noqa: BLE001 - reported in the line
+        import traceback
+        traceback.print_exc(file=sys.stderr)
+        return {"error": f"{what}: {type(e).__name__}: {e}"[:500]}
+
+
 def pinned(n, rt):
     p = C.c_void_p()
     if rt.cudaHostAlloc(C.byref(p), C.c_size_t(max(8 * n, 8)), 0) != 0:
@@ -319,8 +330,8 @@ def run_ours(args, rank, world, device):
     cross = None
     if args.crossover and rank == 0:
         from vortex_b200 import autotune
-        cross = autotune.crossover(device=device)
-    plate = plate_leg(args, device) if args.plate_steps > 0 and rank == 0 else None
+        cross = guarded("crossover", autotune.crossover, device=device)
+    plate = guarded("plate leg", plate_leg, args, device) if args.plate_steps > 0 and rank == 0 else None
     if rank != 0:
         return None
     value = world * 1e3 * K / total_ms
@@ -395,16 +406,17 @@ def run_ours(args, rank, world, device):
         "gpu_launches": int(launches),
         "clocks": ck,
     }
-    line["cpu_baseline"] = cpu_baseline(args, x0, y0, g0, pan)
+    line["cpu_baseline"] = guarded("cpu baseline", cpu_baseline, args, x0, y0, g0, pan)
     if args.ref_cuda_steps > 0 and world == 1:
-        line["reference_cuda_build"] = ref_cuda_build(args, x0, y0, g0)
+        line["reference_cuda_build"] = guarded("reference CUDA build", ref_cuda_build, args, x0, y0, g0)
     if multi:
         line["batched"], line["served"] = multi
     if plate:
         line["plate_config"] = plate
     if cross:
-        line["crossover"] = {"what": "velocity stage (FP32) on the benchmark wake: direct sum against the best "
-                                     "accurate FMM setting, ms", "rows": cross}
+        line["crossover"] = (cross if isinstance(cross, dict) else
+                             {"what": "velocity stage (FP32) on the benchmark wake: direct sum against the best "
+                                      "accurate FMM setting, ms", "rows": cross})
     return line
 
 
@@ -444,33 +456,47 @@ def multibody_runs(args, device, rank, world):
     """The seeded population batched and served, partitioned by body over the
     ranks (each rank its share on its own GPU, no exchange while stepping),
     the ranks' records gathered and combined on the host.  Every rank takes
-    part in the gathers; rank 0 gets the combined records."""
+    part in the gathers (also when its own part failed); rank 0 gets the
+    combined records."""
     from vortex_b200 import multibody as MB
     from vortex_b200 import native as Nt
-    pop = MB.make_population(args.batch_bodies, device=device, rank=rank, world=world)
-    batched = MB.run_batch(steps=args.batch_steps, warmup=3, device=device, rank=rank, world=world, mode="graph",
-                           population=pop)
-    # the same bodies (a few steps later) as concurrent per-body step graphs,
-    # for comparison
-    streams = MB.run_batch(steps=3, warmup=1, device=device, rank=rank, world=world, mode="streams",
-                           population=pop)
-    for s in pop[1]:
-        s.close()
-    batched["per_body_streams"] = {k: streams[k] for k in ("mode", "ms_per_batched_step", "body_steps_per_s",
-                                                           "particle_steps_per_s", "kernels_per_batched_step")}
-    sub32 = MB.run_batch(bodies=16, steps=2, warmup=1, device=device, rank=rank, world=world)
-    sub64 = MB.run_batch(bodies=16, steps=2, warmup=1, precision=Nt.PREC_FP64, device=device, rank=rank,
-                         world=world)
-    batched["fp32_vs_fp64_first16_bodies"] = sub32["body_steps_per_s"] / sub64["body_steps_per_s"]
-    served = MB.run_serve(requests=args.serve_requests, device=device, rank=rank, world=world)
+
+    def batched_part():
+        pop = MB.make_population(args.batch_bodies, device=device, rank=rank, world=world)
+        try:
+            batched = MB.run_batch(steps=args.batch_steps, warmup=3, device=device, rank=rank, world=world,
+                                   mode="graph", population=pop)
+            # the same bodies (a few steps later) as concurrent per-body step
+            # graphs, for comparison
+            streams = MB.run_batch(steps=3, warmup=1, device=device, rank=rank, world=world, mode="streams",
+                                   population=pop)
+        finally:
+            for s in pop[1]:
+                s.close()
+        batched["per_body_streams"] = {k: streams[k] for k in ("mode", "ms_per_batched_step", "body_steps_per_s",
+                                                               "particle_steps_per_s", "kernels_per_batched_step")}
+        sub32 = MB.run_batch(bodies=16, steps=2, warmup=1, device=device, rank=rank, world=world)
+        sub64 = MB.run_batch(bodies=16, steps=2, warmup=1, precision=Nt.PREC_FP64, device=device, rank=rank,
+                             world=world)
+        batched["fp32_vs_fp64_first16_bodies"] = sub32["body_steps_per_s"] / sub64["body_steps_per_s"]
+        return batched
+
+    batched = guarded("batched run", batched_part)
+    served = guarded("served run", MB.run_serve, requests=args.serve_requests, device=device, rank=rank,
+                     world=world)
     if world == 1:
         return batched, served
     import torch.distributed as D
     parts = [None] * world
     D.all_gather_object(parts, (batched, served))
-    b = MB.combine_batch([p[0] for p in parts])
-    b["fp32_vs_fp64_first16_bodies"] = float(np.mean([p[0]["fp32_vs_fp64_first16_bodies"] for p in parts]))
-    return b, MB.combine_serve([p[1] for p in parts])
+    bad_b = [p[0] for p in parts if "error" in p[0]]
+    bad_s = [p[1] for p in parts if "error" in p[1]]
+    if bad_b:
+        b = bad_b[0]
+    else:
+        b = MB.combine_batch([p[0] for p in parts])
+        b["fp32_vs_fp64_first16_bodies"] = float(np.mean([p[0]["fp32_vs_fp64_first16_bodies"] for p in parts]))
+    return b, (bad_s[0] if bad_s else MB.combine_serve([p[1] for p in parts]))
 
 
 def cpu_sample(x, y, g, pan, n_targets, n_panels):
