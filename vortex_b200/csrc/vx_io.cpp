@@ -4,7 +4,8 @@
 // followed by one space, anything after the value is ignored, unknown keys
 // are ignored (reference read_config, src/main.c:48-115).  Keys this library
 // adds: precision (fp64|fp32|0|1), birth_offset_mode (ref|file|half_panel|
-// 0|1|2), drop_eps, diff_cutoff, probe_grid n x0 x1 y0 y1.
+// 0|1|2), drop_eps, diff_cutoff, fmm (0|1), fmm_leaf, fmm_p (8|12|16|20),
+// gj_pivot (0..3), probe_grid n x0 x1 y0 y1.
 //
 // Profile: two header lines, the panel count, then that many records
 // "n lx ly rx ry cx cy bx by nx ny tx ty len nL nR" (src/main.c:220-256).
@@ -40,6 +41,7 @@ extern "C" vx_status vx_conf_read(const char *path, vx_conf *c) {
         B(matrix_load) D(max_ve_g) D(rel_t) B(steady_flow) U(tree_depth) D(theta) B(no_log_buf)
         D(drop_eps) D(diff_cutoff) B(fmm) B(gj_pivot)
         else if (key_is(buf, "fmm_leaf")) { int v_ = 0; if (sscanf(buf, "%*s %d", &v_) == 1 && v_ > 0) c->fmm_leaf = v_; }
+        else if (key_is(buf, "fmm_p")) { int v_ = 0; if (sscanf(buf, "%*s %d", &v_) == 1) c->fmm_p = v_; }
         else if (key_is(buf, "precision")) {
             char v[32] = {0};
             if (sscanf(buf, "%*s %31s", v) == 1)
