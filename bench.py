@@ -119,15 +119,17 @@ def workload_config(args, world: int) -> dict:
 # pair kernels are compute-bound and reported in `roofline`.
 HBM_BYTES = {
     "k_advect": (64, "read x, y, G, Vx, Vy; write x, y, G"),
-    "k_fmm_bbox": (16, "read x, y"),
+    "k_fmm_prep": (16, "read x, y"),
     "k_fmm_leafid": (24, "read x, y; write leaf key and index"),
-    "k_cg_bbox": (24, "read x, y, d"),
+    "k_cg_prep": (24, "read x, y, d"),
     "k_cg_cellid": (24, "read x, y; write cell key and index"),
     "k_bk_place": (12, "read key; write key and index at the bucket slot"),
     "k_bk_order": (8, "read and write the bucket's indices"),
     "k_fmm_gather": (48, "read order index and key, x, y, G; write float4"),
     "k_cg_gather": (56, "read order index and key, x, y, G, d; write float4"),
-    "k_fmm_p2m": (16, "read float4 source"),
+    "k_col_prep": (16, "read x, y"),
+    "k_col_count": (32, "read x, y; write cell id, in-count and the two merge flags"),
+    "k_col_scatter": (12, "read cell id and cell start; write the cell-sorted index"),
     "k_col_query<2>": (28, "read x, y, G; write COL"),
     "k_col_query<1>": (28, "read x, y, G; write COL"),
     "k_cmp_count": (8, "read G"),

@@ -370,3 +370,23 @@ def test_bucket_order_is_the_stable_sort():
         assert N.lib().vx_eval_bucket_order(C.c_void_p(dk.data_ptr()), C.c_int64(len(keys)), C.c_int64(nb),
                                             C.c_void_p(out.data_ptr())) == 0
         assert np.array_equal(out.cpu().numpy(), np.argsort(keys, kind="stable"))
+
+
+def test_step_is_at_most_60_kernels():
+    """The bulk step of the benchmark body (1000-panel cylinder, quadtree
+    velocity, neighbour-list diffusion, both collapse passes) is at most 60
+    kernel launches: grid build, scan and gather fused per grid, the force
+    sums, compaction scan and collapse bookkeeping done by the last block of
+    the kernel before them."""
+    from vortex_b200 import workloads as wl
+    sim = N.Sim(wl.cylinder_conf(N.PREC_FP32), wl.cylinder_panels())
+    sim.set_particles(*wl.warm_wake(300_000, 1234))
+    sim.step(2)
+    sim.sync()
+    l0 = sim.launches()
+    sim.step(3)
+    sim.sync()
+    per_step = (sim.launches() - l0) / 3
+    assert per_step <= 60, per_step
+    sim.close()
+

@@ -3,15 +3,21 @@ configurations' own bodies, through the C ABI: the 1000-panel cylinder of
 the benchmark and the 2576-panel rounded plate at 20 degrees of incidence,
 each with a seeded wake-like cloud of 16 000 vortices around and behind it.
 
-Bounds (as for the 200-panel circle): new-vortex positions, the 3-nearest
-distance d, convection with absorption, compaction (every slot, the dead
-tail included), collapse pairing and merges bit-exact; velocities within
-1e-12; birth strengths within 1e-10 of the largest; wall diffusion 1e-13.
+Bounds: new-vortex positions, the 3-nearest distance d, convection with
+absorption, compaction (every slot, the dead tail included), collapse
+pairing and merges bit-exact; velocities within 1e-12 of the field's
+largest component (the sums run in another order than the oracle's
+sequential ones: at 16 000 sources and fields of order 1 to 30 the
+differences are a few 1e-14 of the field); birth strengths within 1e-10 of
+the largest; wall diffusion 1e-13.
 The panel system: the device's Gauss-Jordan (the reference's pivot rule)
-against the oracle's.  For the plate that rule leaves a residual of order
-1e-4 in L M - I (the reference's own result), so the birth strengths are
-compared with the device's matrix and the matrices are compared on their
-own, to the bound their rounding differences allow.
+against the oracle's.  Both are inverses with a residual R = L M - I of
+their own (1e-14 for the circle; of order 1e-4 for the plate, the
+reference's own result with its pivot rule), so they can differ by
+|M_dev - M| <= |M|_inf (|R_dev| + |R|) (max norms, |M|_inf the largest row
+sum): the test holds the difference to twice that, and the device's
+residual to ten times the oracle's.  The birth strengths are compared with
+the device's matrix.
 """
 import numpy as np
 import pytest
@@ -23,7 +29,7 @@ from vortex_b200 import native as N
 pytestmark = pytest.mark.gpu
 
 BODIES = ["circle1000", "plate2576"]
-VEL_TOL = 1e-12
+VEL_REL = 1e-12
 N_CLOUD = 16000
 
 
@@ -40,10 +46,14 @@ def test_panel_matrix_and_birth(name):
     P = len(pan)
     L, M = O.panel_matrix(pan)
     Mg = sim.matrix()
-    # Kelvin row and column as built; the inverses agree to what the
-    # elimination's conditioning allows (1e-11 for the circle)
-    tol = 1e-11 if name == "circle1000" else 1e-6
-    assert rel_err(Mg, M) < tol, rel_err(Mg, M)
+    eye = np.eye(len(M))
+    res_o = np.abs(L @ M - eye).max()
+    res_d = np.abs(L @ Mg - eye).max()
+    bound = 2.0 * np.abs(M).sum(axis=1).max() * (res_d + res_o)
+    assert np.abs(Mg - M).max() <= bound, (np.abs(Mg - M).max(), bound)
+    assert res_d <= 10.0 * res_o + 1e-13, (res_d, res_o)
+    if name == "circle1000":
+        assert rel_err(Mg, M) < 1e-11, rel_err(Mg, M)
     x, y, g = with_tail(*body_cloud(pan, N_CLOUD, seed=1), extra=96)
     n = N_CLOUD
     sim.set_slots(x, y, g, n)
@@ -70,13 +80,13 @@ def test_velocity_nearest_and_diffusion(name):
     vx, vy, d = sim.velocity()
     ovx, ovy, od = O.velocity(p, x, y, g, n)
     assert np.array_equal(d, od), "3-nearest distance must be bit-exact"
-    assert np.abs(vx - ovx).max() < VEL_TOL and np.abs(vy - ovy).max() < VEL_TOL
+    assert rel_err(vx, ovx) < VEL_REL and rel_err(vy, ovy) < VEL_REL
     # vortex diffusion from the oracle's velocities and distances
     sim.set_velocity(ovx, ovy, od)
     sim.stage("diffusion")
     dvx, dvy, _ = sim.velocity()
     evx, evy = O.diffusion(p, x, y, g, n, od, ovx, ovy)
-    assert np.abs(dvx - evx).max() < VEL_TOL and np.abs(dvy - evy).max() < VEL_TOL
+    assert rel_err(dvx, evx) < VEL_REL and rel_err(dvy, evy) < VEL_REL
     sim.close()
 
 

@@ -4,9 +4,9 @@
 //
 // Reference: step_Kernel src/kernel.cu:1090-1143, hitting :1357-1431,
 // summ_Kernel :1144-1157.  The reference sums serially in one thread; here
-// each thread of a fixed grid accumulates a fixed strided subset, blocks
-// reduce in a fixed tree and one block adds the block sums in order, so the
-// result is run-to-run identical.
+// each thread of a fixed partition accumulates a fixed strided subset,
+// partitions reduce in a fixed tree and the launch's last block adds the
+// partition sums in order, so the result is run-to-run identical.
 #include <algorithm>
 
 #include "vx_internal.cuh"
@@ -198,10 +198,13 @@ __device__ __forceinline__ void advect_part(unsigned part, unsigned nparts, cons
 // grid of nparts blocks would take them) whatever the grid: each block takes
 // partitions blockIdx, blockIdx + grid, ...; a partition past the last
 // particle has zero sums.  The partial sums, and so the totals, do not depend
-// on the grid the kernel runs with.
-VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, const VxScalars *S,
-                           const vx_panel *pan, double *red, const int *hstart, const int *hidx, int nparts) {
+// on the grid the kernel runs with.  The block that finishes last adds the
+// partition sums: thread t adds partitions t, t + 256, ... in order, then a
+// fixed shared-memory tree, so the result is run-to-run identical.
+VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
+                           double *red, const int *hstart, const int *hidx, int sms) {
     const long long n = S->n;
+    const int nparts = vx_body_parts(n, sms, VX_RED_BLOCKS);
     for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) {
         if ((long long)q * blockDim.x >= n) {
             if (threadIdx.x < 4) red[q * 4 + threadIdx.x] = 0.0;
@@ -209,21 +212,11 @@ VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, const
         }
         advect_part(q, (unsigned)nparts, p, v, S, pan, red, hstart, hidx);
     }
-}
-__global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, const VxScalars *S,
-                                                       const vx_panel *pan, double *red, const int *hstart,
-                                                       const int *hidx, int nparts) {
-    VX_PDL_WAIT();
-    k_advect_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, red, hstart, hidx, nparts);
-}
-
-// Block sums combined by one block: thread t adds blocks t, t + 256, ... in
-// order, then a fixed shared-memory tree; the result is run-to-run identical.
-VX_DEVK void k_sums_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxScalars *S, const double *red, int nblocks) {
+    if (!vx_last_block(&S->sync_ctr, vb.n)) return;
     __shared__ double sh[VX_THREADS];
     double a[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-        for (int q = 0; q < 4; ++q) a[q] += red[b * 4 + q];
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+        for (int q = 0; q < 4; ++q) a[q] += __ldcg(&red[b * 4 + q]);
     for (int q = 0; q < 4; ++q) a[q] = vx_block_sum(a[q], sh);
     if (threadIdx.x != 0) return;
     for (int q = 0; q < 4; ++q) S->raw[q] = a[q];
@@ -232,19 +225,18 @@ VX_DEVK void k_sums_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxScalars *S, con
     S->fy = a[2] * (p.rho / p.dt);
     S->m = a[3] * (p.rho / (2 * p.dt));
 }
-__global__ void __launch_bounds__(VX_THREADS) k_sums(VxParams p, VxScalars *S, const double *red, int nblocks) {
+__global__ void __launch_bounds__(VX_THREADS) k_advect(VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
+                                                       double *red, const int *hstart, const int *hidx, int sms) {
     VX_PDL_WAIT();
-    k_sums_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, p, S, red, nblocks);
+    k_advect_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, red, hstart, hidx, sms);
 }
 
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                              VxWork &w, const vx_panel *pan, const int *hstart, const int *hidx) {
     if (p.hit_nx <= 0 || p.hit_ny <= 0) hstart = hidx = nullptr;
-    // partitions of the force sums follow the body's size (vx_part_sms), the
-    // grid follows the SMs this launch is given
-    const int nparts = std::min(vx_part_sms(L) * 4, VX_RED_BLOCKS);
-    const int grid = std::min(nparts, L.num_sms * 4);
-    vx_launch<k_advect, k_advect_body>(L, grid, VX_THREADS, 0, p, v, S, pan, w.red, hstart, hidx, nparts);
-    vx_launch<k_sums, k_sums_body>(L, 1, VX_THREADS, 0, p, S, w.red, nparts);
+    // partitions of the force sums follow the body's count on the device
+    // (vx_body_parts), the grid the SMs this launch is given
+    const int grid = std::min(VX_RED_BLOCKS, L.num_sms * 4);
+    vx_launch<k_advect, k_advect_body>(L, grid, VX_THREADS, 0, p, v, S, pan, w.red, hstart, hidx, vx_full_sms(L));
     return cudaGetLastError();
 }

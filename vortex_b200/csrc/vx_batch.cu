@@ -13,8 +13,9 @@
 // and block coordinates, so a body computes exactly what its own launches
 // would have computed.  The grids of the scaled grid-stride launches are
 // sized for a share of the GPU proportional to the body's size; the
-// partitions that fix summation orders follow the body's own size
-// (VxLaunch::part_sms), so results are bit-identical to vx_step's.
+// partitions that fix summation orders follow the body's own count on the
+// device (vx_body_parts and the like), so results are bit-identical to
+// vx_step's.
 //
 // The slot tables (block ranges and packs) live in one device arena that the
 // graph's kernels read; when a body's recording changes (its store grew, a
@@ -50,9 +51,9 @@ namespace {
 // What a body's recording depends on besides its (unchanging) parameters.
 struct BodyKey {
     long long cap;
-    int kv, rhs, sms, share, fmm, leaf, lmax;
+    int rhs, sms, share, fmm, leaf, lmax;
     bool operator==(const BodyKey &o) const {
-        return cap == o.cap && kv == o.kv && rhs == o.rhs && sms == o.sms && share == o.share && fmm == o.fmm &&
+        return cap == o.cap && rhs == o.rhs && sms == o.sms && share == o.share && fmm == o.fmm &&
                leaf == o.leaf && lmax == o.lmax;
     }
 };
@@ -364,7 +365,6 @@ static vx_status upload(vx_batch *b) {
 static BodyKey key_of(vx_batch *b, vx_sim *s) {
     BodyKey k;
     k.cap = s->cap;
-    k.kv = vx_sim_kv(s);
     k.rhs = vx_sim_rhs_chunks(s);
     k.sms = vx_sim_step_sms(s);
     k.share = std::max(1, (k.sms + b->share_div - 1) / b->share_div);

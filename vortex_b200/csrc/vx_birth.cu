@@ -305,7 +305,8 @@ struct RhsMath<float> {
 template <typename T>
 VX_DEVK void k_rhs_partial_body(VxBlkB<RHS_T, 0> vb, VxView v, const VxScalars *S,
                                 const vx_panel *pan, int P, int P32,
-                                double *part, int nchunks) {
+                                double *part, int sms) {
+    const int nchunks = vx_rhs_chunks(S->n0, P, sms);   // from the body's own count
     __shared__ T sx[RHS_T], sy[RHS_T], sg[RHS_T];
     const long long n0 = S->n0;
     const long long cs = vx_ceil_div(vx_ceil_div(n0, nchunks), RHS_T) * RHS_T;
@@ -357,9 +358,9 @@ VX_DEVK void k_rhs_partial_body(VxBlkB<RHS_T, 0> vb, VxView v, const VxScalars *
 template <typename T>
 __global__ void __launch_bounds__(RHS_T) k_rhs_partial(VxView v, const VxScalars *S,
                                                        const vx_panel *pan, int P, int P32,
-                                                       double *part, int nchunks) {
+                                                       double *part, int sms) {
     VX_PDL_WAIT();
-    k_rhs_partial_body<T>(VxBlkB<RHS_T, 0>{blockIdx.x, gridDim.x}, v, S, pan, P, P32, part, nchunks);
+    k_rhs_partial_body<T>(VxBlkB<RHS_T, 0>{blockIdx.x, gridDim.x}, v, S, pan, P, P32, part, sms);
 }
 
 // ---------------------------------------------------------------------------
@@ -384,6 +385,13 @@ static_assert(BF_P % 16 == 0, "16 far-field coefficients per pass");
 struct bcplx {
     double r, i;
 };
+
+// Source chunks of the far-field pass: two per SM's worth of the body
+// (vx_body_sms of its count after birth), at most VX_BF_MAX_BLOCKS.
+__device__ __forceinline__ int vx_bf_parts(long long n, int sms) {
+    const int q = 2 * vx_body_sms(n, sms);
+    return q < VX_BF_MAX_BLOCKS ? q : VX_BF_MAX_BLOCKS;
+}
 
 // Block b: sources [b cs, (b+1) cs) of the n0 pre-birth vortices.
 __device__ __forceinline__ void bf_chunk(const VxScalars *S, int nb, int b, long long &j0, long long &j1) {
@@ -478,9 +486,16 @@ __device__ __forceinline__ void bf_far_part(unsigned q, unsigned nparts, const V
 }
 // The sources are split into nparts fixed chunks whatever the grid; each
 // block takes chunks blockIdx, blockIdx + grid, ...; an empty chunk has zero
-// partials.  The summed coefficients do not depend on the launch's grid.
-VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S, double *part, int *cnt,
-                           int nparts) {
+// partials.  The block that finishes last then scans the chunks' near-source
+// counts into offsets and adds the coefficient partials in chunk order
+// (thread t scans the counts of chunks BF_SCAN_PER t .., then a warp and
+// block scan of the thread totals).  The summed coefficients do not depend
+// on the launch's grid.
+constexpr int BF_SCAN_PER = VX_BF_MAX_BLOCKS / BF_T;
+static_assert(BF_SCAN_PER * BF_T == VX_BF_MAX_BLOCKS, "whole chunks per scan thread");
+VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, VxScalars *S, double *part, int *cnt,
+                           int sms, long long *off, double *coef) {
+    const int nparts = vx_bf_parts(S->n0 + p.P, sms);
     for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) {
         long long j0, j1;
         bf_chunk(S, nparts, q, j0, j1);
@@ -491,27 +506,13 @@ VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxSca
         }
         bf_far_part(q, (unsigned)nparts, p, v, S, part, cnt, j0, j1);
     }
-}
-__global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, const VxScalars *S, double *part, int *cnt,
-                                                 int nparts) {
-    VX_PDL_WAIT();
-    k_bf_far_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, part, cnt, nparts);
-}
-
-// Block-count offsets and the coefficient sums (block order), one block of
-// BF_SCAN_T threads: thread t scans the counts of blocks BF_SCAN_PER t ..,
-// then a warp and block scan of the thread totals.
-constexpr int BF_SCAN_T = 256;
-constexpr int BF_SCAN_PER = VX_BF_MAX_BLOCKS / BF_SCAN_T;
-static_assert(BF_SCAN_PER * BF_SCAN_T == VX_BF_MAX_BLOCKS, "whole blocks per scan thread");
-VX_DEVK void k_bf_scan_body(VxBlkB<BF_SCAN_T, 0> vb, VxScalars *S, int nb, const int *cnt, long long *off,
-                            const double *part, double *coef) {
-    __shared__ long long wsum[BF_SCAN_T / 32];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (!vx_last_block(&S->sync_ctr, vb.n)) return;
+    __shared__ long long wsum[BF_T / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nb = nparts;
     long long c[BF_SCAN_PER], tot = 0;
     for (int q = 0; q < BF_SCAN_PER; ++q) {
         const int b = BF_SCAN_PER * t + q;
-        c[q] = b < nb ? cnt[b] : 0;
+        c[q] = b < nb ? __ldcg(&cnt[b]) : 0;
         tot += c[q];
     }
     long long inc = tot;
@@ -522,7 +523,7 @@ VX_DEVK void k_bf_scan_body(VxBlkB<BF_SCAN_T, 0> vb, VxScalars *S, int nb, const
     if (lane == 31) wsum[warp] = inc;
     __syncthreads();
     long long run = inc - tot, all = 0;
-    for (int q = 0; q < BF_SCAN_T / 32; ++q) {
+    for (int q = 0; q < BF_T / 32; ++q) {
         run += q < warp ? wsum[q] : 0;
         all += wsum[q];
     }
@@ -537,14 +538,14 @@ VX_DEVK void k_bf_scan_body(VxBlkB<BF_SCAN_T, 0> vb, VxScalars *S, int nb, const
     }
     if (t < 2 * BF_P) {
         double acc = 0.0;
-        for (int b = 0; b < nb; ++b) acc += part[(long long)b * 2 * BF_P + t];
+        for (int b = 0; b < nb; ++b) acc += __ldcg(&part[(long long)b * 2 * BF_P + t]);
         coef[t] = acc;
     }
 }
-__global__ void __launch_bounds__(BF_SCAN_T) k_bf_scan(VxScalars *S, int nb, const int *cnt, long long *off,
-                                                       const double *part, double *coef) {
+__global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, VxScalars *S, double *part, int *cnt,
+                                                 int sms, long long *off, double *coef) {
     VX_PDL_WAIT();
-    k_bf_scan_body(VxBlkB<BF_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, nb, cnt, off, part, coef);
+    k_bf_far_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, part, cnt, sms, off, coef);
 }
 
 // Near sources of each block in index order (block-wide ballot scan).
@@ -578,13 +579,14 @@ __device__ __forceinline__ void bf_scatter_part(unsigned q, unsigned nparts, con
     }
 }
 VX_DEVK void k_bf_scatter_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S,
-                               const long long *off, float4 *near, int nparts) {
+                               const long long *off, float4 *near, int sms) {
+    const int nparts = vx_bf_parts(S->n0 + p.P, sms);
     for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) bf_scatter_part(q, (unsigned)nparts, p, v, S, off, near);
 }
 __global__ void __launch_bounds__(BF_T) k_bf_scatter(VxParams p, VxView v, const VxScalars *S,
-                                                     const long long *off, float4 *near, int nparts) {
+                                                     const long long *off, float4 *near, int sms) {
     VX_PDL_WAIT();
-    k_bf_scatter_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, off, near, nparts);
+    k_bf_scatter_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, off, near, sms);
 }
 
 // atan2 in FP32 for the bulk form's near panel terms: the octant reduction
@@ -658,7 +660,8 @@ __device__ __forceinline__ float vx_half_log_ratio(float r0, float r1, float num
 
 // Direct FP32 panel terms over the near list (chunked like k_rhs_partial).
 VX_DEVK void k_rhs_near_body(VxBlkB<RHS_T, 0> vb, const VxScalars *S, const vx_panel *pan, int P, int P32,
-                             const float4 *near, double *part, int nchunks) {
+                             const float4 *near, double *part, int sms) {
+    const int nchunks = vx_rhs_chunks(S->n0, P, sms);   // from the body's own count
     __shared__ float4 sq4[RHS_T];   // (x, y, G, unused)
     const long long nn = S->bf_nnear;
     const long long cs = vx_ceil_div(vx_ceil_div(nn, nchunks), RHS_T) * RHS_T;
@@ -705,9 +708,9 @@ VX_DEVK void k_rhs_near_body(VxBlkB<RHS_T, 0> vb, const VxScalars *S, const vx_p
     }
 }
 __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx_panel *pan, int P, int P32,
-                                                    const float4 *near, double *part, int nchunks) {
+                                                    const float4 *near, double *part, int sms) {
     VX_PDL_WAIT();
-    k_rhs_near_body(VxBlkB<RHS_T, 0>{blockIdx.x, gridDim.x}, S, pan, P, P32, near, part, nchunks);
+    k_rhs_near_body(VxBlkB<RHS_T, 0>{blockIdx.x, gridDim.x}, S, pan, P, P32, near, part, sms);
 }
 
 // R_i = -(mean velocity along panel i + V_inf) . tau_i; the far field (if
@@ -716,7 +719,8 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx
 // fixed butterfly); otherwise one thread per panel in chunk order.
 template <bool WARP>
 VX_DEVK void k_rhs_final_body(VxBlkB<0, 0> vb, const VxScalars *S, const vx_panel *pan, int P, int P32,
-                              const double *part, int nchunks, double *R, VxParams p, const double *coef) {
+                              const double *part, int sms, double *R, VxParams p, const double *coef) {
+    const int nchunks = vx_rhs_chunks(S->n0, P, sms);   // from the body's own count
     const int i = WARP ? (int)((vb.x * blockDim.x + threadIdx.x) >> 5) : vb.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double y0 = 0.0, y1 = 0.0;
@@ -764,62 +768,96 @@ VX_DEVK void k_rhs_final_body(VxBlkB<0, 0> vb, const VxScalars *S, const vx_pane
 }
 template <bool WARP>
 __global__ void k_rhs_final(const VxScalars *S, const vx_panel *pan, int P, int P32,
-                            const double *part, int nchunks, double *R, VxParams p, const double *coef) {
+                            const double *part, int sms, double *R, VxParams p, const double *coef) {
     VX_PDL_WAIT();
-    k_rhs_final_body<WARP>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, pan, P, P32, part, nchunks, R, p, coef);
+    k_rhs_final_body<WARP>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, pan, P, P32, part, sms, R, p, coef);
+}
+
+// One new vortex per panel at [n0, n0+P) (src/kernel.cu:862-872), written
+// by the block that finishes the gamma solve last (a vortex takes the gamma
+// of its panel's right neighbour too, so every gamma must be final).
+__device__ void birth_place(const VxParams &p, const VxView &v, VxScalars *S, const vx_panel *pan, int P,
+                            const double *gamma) {
+    const long long n0 = S->n0;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const int in = (int)pan[i].n_of_rpanel;
+        const double mx = (pan[i].left[0] + pan[i].right[0]) / 2;
+        const double my = (pan[i].left[1] + pan[i].right[1]) / 2;
+        double bx, by;
+        if (p.birth_mode == VX_BIRTH_FILE) {
+            bx = pan[i].birth[0]; by = pan[i].birth[1];
+        } else if (p.birth_mode == VX_BIRTH_HALF_PANEL) {
+            const double h = 0.5 * pan[i].length;
+            bx = mx + h * pan[i].norm[0]; by = my + h * pan[i].norm[1];
+        } else {
+            bx = mx + 1e-6 * pan[i].norm[0]; by = my + 1e-6 * pan[i].norm[1];
+        }
+        const long long k = (n0 + i) * v.ps;
+        v.x[k] = bx;
+        v.y[k] = by;
+        v.g[k] = 0.5 * (__ldcg(&gamma[i]) * pan[i].length + __ldcg(&gamma[in]) * pan[in].length);
+    }
+    if (threadIdx.x == 0) S->n = n0 + P;
 }
 
 // gamma_i = sum_j M_ij R_j + M_iP dg, sequential in j with fma (as the
-// oracle), one thread per row; ld is the matrix row stride.
-VX_DEVK void k_gamma_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *M, long long ld, int P, const double *R,
-                          double *gamma) {
-    int i = vb.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    const double *row = M + (long long)i * ld;
-    double acc = 0.0;
-    for (int j = 0; j < P; ++j) acc = fma(row[j], R[j], acc);
-    gamma[i] = fma(row[P], S->dg, acc);
+// oracle), one thread per row; ld is the matrix row stride.  Then the
+// vortices are placed (birth_place).
+VX_DEVK void k_gamma_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan, const double *M,
+                          long long ld, int P, const double *R, double *gamma) {
+    const int i = vb.x * blockDim.x + threadIdx.x;
+    if (i < P) {
+        const double *row = M + (long long)i * ld;
+        double acc = 0.0;
+        for (int j = 0; j < P; ++j) acc = fma(row[j], R[j], acc);
+        gamma[i] = fma(row[P], S->dg, acc);
+    }
+    if (vx_last_block(&S->sync_ctr, vb.n)) birth_place(p, v, S, pan, P, gamma);
 }
-__global__ void k_gamma(const VxScalars *S, const double *M, long long ld, int P, const double *R,
-                        double *gamma) {
+__global__ void k_gamma(VxParams p, VxView v, VxScalars *S, const vx_panel *pan, const double *M, long long ld, int P,
+                        const double *R, double *gamma) {
     VX_PDL_WAIT();
-    k_gamma_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, M, ld, P, R, gamma);
+    k_gamma_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, M, ld, P, R, gamma);
 }
 
 // The same sums from the transposed inverse Mt (Mt[j ld + i] = M[i ld + j]):
 // the same order and fma per row, but a warp's 32 rows read 32 consecutive
 // doubles per step instead of 32 rows' worth of cache lines.
-VX_DEVK void k_gamma_t_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *Mt, long long ld, int P, const double *R,
-                            double *gamma) {
-    int i = vb.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    double acc = 0.0;
-    for (int j = 0; j < P; ++j) acc = fma(Mt[(long long)j * ld + i], R[j], acc);
-    gamma[i] = fma(Mt[(long long)P * ld + i], S->dg, acc);
+VX_DEVK void k_gamma_t_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
+                            const double *Mt, long long ld, int P, const double *R, double *gamma) {
+    const int i = vb.x * blockDim.x + threadIdx.x;
+    if (i < P) {
+        double acc = 0.0;
+        for (int j = 0; j < P; ++j) acc = fma(Mt[(long long)j * ld + i], R[j], acc);
+        gamma[i] = fma(Mt[(long long)P * ld + i], S->dg, acc);
+    }
+    if (vx_last_block(&S->sync_ctr, vb.n)) birth_place(p, v, S, pan, P, gamma);
 }
-__global__ void k_gamma_t(const VxScalars *S, const double *Mt, long long ld, int P, const double *R,
-                          double *gamma) {
+__global__ void k_gamma_t(VxParams p, VxView v, VxScalars *S, const vx_panel *pan, const double *Mt, long long ld,
+                          int P, const double *R, double *gamma) {
     VX_PDL_WAIT();
-    k_gamma_t_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, Mt, ld, P, R, gamma);
+    k_gamma_t_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, Mt, ld, P, R, gamma);
 }
 
 // Bulk form: one warp per row, lanes striding the row (coalesced), FP64
 // partial sums combined by a fixed butterfly.
-VX_DEVK void k_gamma_w_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *M, long long ld, int P, const double *R,
-                            double *gamma) {
+VX_DEVK void k_gamma_w_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
+                            const double *M, long long ld, int P, const double *R, double *gamma) {
     const int lane = threadIdx.x & 31;
     const int i = (vb.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= P) return;
-    const double *row = M + (long long)i * ld;
-    double acc = 0.0;
-    for (int j = lane; j < P; j += 32) acc = fma(row[j], R[j], acc);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) gamma[i] = fma(row[P], S->dg, acc);
+    if (i < P) {
+        const double *row = M + (long long)i * ld;
+        double acc = 0.0;
+        for (int j = lane; j < P; j += 32) acc = fma(row[j], R[j], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) gamma[i] = fma(row[P], S->dg, acc);
+    }
+    if (vx_last_block(&S->sync_ctr, vb.n)) birth_place(p, v, S, pan, P, gamma);
 }
-__global__ void k_gamma_w(const VxScalars *S, const double *M, long long ld, int P, const double *R,
-                          double *gamma) {
+__global__ void k_gamma_w(VxParams p, VxView v, VxScalars *S, const vx_panel *pan, const double *M, long long ld,
+                          int P, const double *R, double *gamma) {
     VX_PDL_WAIT();
-    k_gamma_w_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, M, ld, P, R, gamma);
+    k_gamma_w_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, M, ld, P, R, gamma);
 }
 
 VX_DEVK void k_transpose_body(VxBlkB<0, 0> vb, const double *A, double *At, long long nr) {
@@ -850,73 +888,39 @@ cudaError_t vx_transpose_square(const VxLaunch &L, const double *A, double *At, 
     return cudaGetLastError();
 }
 
-// One new vortex per panel at [n0, n0+P) (src/kernel.cu:862-872).
-VX_DEVK void k_place_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan, int P,
-                          const double *gamma) {
-    int i = vb.x * blockDim.x + threadIdx.x;
-    const long long n0 = S->n0;
-    if (i < P) {
-        int in = (int)pan[i].n_of_rpanel;
-        double mx = (pan[i].left[0] + pan[i].right[0]) / 2;
-        double my = (pan[i].left[1] + pan[i].right[1]) / 2;
-        double bx, by;
-        if (p.birth_mode == VX_BIRTH_FILE) {
-            bx = pan[i].birth[0]; by = pan[i].birth[1];
-        } else if (p.birth_mode == VX_BIRTH_HALF_PANEL) {
-            double h = 0.5 * pan[i].length;
-            bx = mx + h * pan[i].norm[0]; by = my + h * pan[i].norm[1];
-        } else {
-            bx = mx + 1e-6 * pan[i].norm[0]; by = my + 1e-6 * pan[i].norm[1];
-        }
-        long long k = (n0 + i) * v.ps;
-        v.x[k] = bx;
-        v.y[k] = by;
-        v.g[k] = 0.5 * (gamma[i] * pan[i].length + gamma[in] * pan[in].length);
-    }
-    if (i == 0) S->n = n0 + P;
-}
-__global__ void k_place(VxParams p, VxView v, VxScalars *S, const vx_panel *pan, int P,
-                        const double *gamma) {
-    VX_PDL_WAIT();
-    k_place_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, pan, P, gamma);
-}
-
+// rhs_chunks: the source chunks the host expects, for the grid only (the
+// kernels take the chunk count from the body's own count, vx_rhs_chunks).
 static cudaError_t birth_impl(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S, VxWork &w,
                               const vx_panel *pan, const double *minv, long long ld, const double *minv_t,
                               int rhs_chunks) {
     const int P = p.P, P32 = (int)vx_round32(P);
     const int tiles = (P + RHS_T - 1) / RHS_T;
     const int grid = (int)min((long long)tiles * rhs_chunks, (long long)L.num_sms * 16);
+    const int sms = vx_full_sms(L);   // the device's SMs: partitions follow the body, not the launch
     const bool far = p.prec == VX_PREC_FP32 && p.birth_far;
     if (far) {
-        // source chunks follow the body's size (vx_part_sms), the grid the
-        // SMs this launch is given
-        const int nb = std::min(2 * vx_part_sms(L), VX_BF_MAX_BLOCKS);
-        const int gb = std::min(nb, 2 * L.num_sms);
-        vx_launch<k_bf_far, k_bf_far_body>(L, gb, BF_T, 0, p, v, S, w.bf_part, w.bf_cnt, nb);
-        vx_launch<k_bf_scan, k_bf_scan_body>(L, 1, BF_SCAN_T, 0, S, nb, w.bf_cnt, w.bf_off, w.bf_part, w.bf_coef);
-        vx_launch<k_bf_scatter, k_bf_scatter_body>(L, gb, BF_T, 0, p, v, S, w.bf_off, w.bf_near, nb);
-        vx_launch<k_rhs_near, k_rhs_near_body>(L, grid, RHS_T, 0, S, pan, P, P32, w.bf_near, w.rhs_part, rhs_chunks);
+        const int gb = std::min(VX_BF_MAX_BLOCKS, 2 * L.num_sms);
+        vx_launch<k_bf_far, k_bf_far_body>(L, gb, BF_T, 0, p, v, S, w.bf_part, w.bf_cnt, sms, w.bf_off, w.bf_coef);
+        vx_launch<k_bf_scatter, k_bf_scatter_body>(L, gb, BF_T, 0, p, v, S, w.bf_off, w.bf_near, sms);
+        vx_launch<k_rhs_near, k_rhs_near_body>(L, grid, RHS_T, 0, S, pan, P, P32, w.bf_near, w.rhs_part, sms);
     } else if (p.prec == VX_PREC_FP32) {
-        vx_launch<k_rhs_partial<float>, k_rhs_partial_body<float>>(L, grid, RHS_T, 0, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
+        vx_launch<k_rhs_partial<float>, k_rhs_partial_body<float>>(L, grid, RHS_T, 0, v, S, pan, P, P32, w.rhs_part, sms);
     } else {
-        vx_launch<k_rhs_partial<double>, k_rhs_partial_body<double>>(L, grid, RHS_T, 0, v, S, pan, P, P32, w.rhs_part, rhs_chunks);
+        vx_launch<k_rhs_partial<double>, k_rhs_partial_body<double>>(L, grid, RHS_T, 0, v, S, pan, P, P32, w.rhs_part, sms);
     }
 
     const int b = (P + 127) / 128;
     if (far)
-        vx_launch<k_rhs_final<true>, k_rhs_final_body<true>>(L, (P + 3) / 4, 128, 0, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, w.bf_coef);
+        vx_launch<k_rhs_final<true>, k_rhs_final_body<true>>(L, (P + 3) / 4, 128, 0, S, pan, P, P32, w.rhs_part, sms, w.R, p, w.bf_coef);
     else
-        vx_launch<k_rhs_final<false>, k_rhs_final_body<false>>(L, b, 128, 0, S, pan, P, P32, w.rhs_part, rhs_chunks, w.R, p, nullptr);
+        vx_launch<k_rhs_final<false>, k_rhs_final_body<false>>(L, b, 128, 0, S, pan, P, P32, w.rhs_part, sms, w.R, p, nullptr);
 
     if (minv_t && p.prec == VX_PREC_FP32)
-        vx_launch<k_gamma_w, k_gamma_w_body>(L, (P + 3) / 4, 128, 0, S, minv, ld, P, w.R, w.gamma);
+        vx_launch<k_gamma_w, k_gamma_w_body>(L, (P + 3) / 4, 128, 0, p, v, S, pan, minv, ld, P, w.R, w.gamma);
     else if (minv_t)
-        vx_launch<k_gamma_t, k_gamma_t_body>(L, b, 128, 0, S, minv_t, ld, P, w.R, w.gamma);
+        vx_launch<k_gamma_t, k_gamma_t_body>(L, b, 128, 0, p, v, S, pan, minv_t, ld, P, w.R, w.gamma);
     else
-        vx_launch<k_gamma, k_gamma_body>(L, b, 128, 0, S, minv, ld, P, w.R, w.gamma);
-
-    vx_launch<k_place, k_place_body>(L, b, 128, 0, p, v, S, pan, P, w.gamma);
+        vx_launch<k_gamma, k_gamma_body>(L, b, 128, 0, p, v, S, pan, minv, ld, P, w.R, w.gamma);
     return cudaGetLastError();
 }
 

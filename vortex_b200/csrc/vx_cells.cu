@@ -31,91 +31,77 @@ constexpr int CG_W = 32;       // targets per work item (one warp)
 constexpr int CG_DIV = VX_CG_DIV;      // cell side = cut-off radius at the mean d / CG_DIV
 constexpr int CG_KCAP = 2 * CG_DIV;    // widest window of a work item, in cells (twice the mean radius)
 
-VX_DEVK void k_cg_begin_body(VxBlkB<0, 0> vb, VxScalars *S) {
-    S->cb[0] = S->cb[1] = S->cb[2] = S->cb[3] = ~0ull;
-    S->cnwide = 0;
-    S->cnhuge = 0;
-    S->bk_nmid = S->bk_nbig = 0;
-}
-__global__ void k_cg_begin(VxScalars *S) {
-    VX_PDL_WAIT();
-    k_cg_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
-}
-
-// Bounding box of the live particles and per-block sums of d (fixed grid:
-// the mean below is reproducible).
-// Partition `part` of `nparts` (block-strided): its box into the running
-// minimum, its sum of d into red[part].
-__device__ __forceinline__ void cg_bbox_part(unsigned part, unsigned nparts, const VxView &v, VxScalars *S,
-                                             double *red) {
+// Start of the diffusion stage, one launch: per partition the bounding-box
+// keys (into box[]) and the sum of d (into red[]); the block that finishes
+// last combines them, resets the stage's counters and sizes the grid.  The
+// sum of d is split into nparts fixed partitions whatever the grid (a
+// partition past the last particle adds 0) and the partition sums are added
+// in a fixed tree, so the mean spacing, and the grid built from it, do not
+// depend on the launch's grid.  Cell side h = c * mean(d) / CG_DIV, grown
+// until the grid fits cells_cap.
+VX_DEVK void k_cg_prep_body(VxBlkB<CG_T, 0> vb, VxView v, VxScalars *S, double *red, unsigned long long *box,
+                            int sms, double cutoff, long long cells_cap) {
     __shared__ unsigned long long sk[4][CG_T];
     __shared__ double sd[CG_T];
     const long long n = S->n;
+    const int nparts = vx_body_parts(n, sms, VX_RED_BLOCKS);
+    for (unsigned part = vb.x; part < (unsigned)nparts; part += vb.n) {
+        if ((long long)part * blockDim.x >= n) {
+            if (threadIdx.x == 0) red[part] = 0.0;
+            continue;
+        }
+        unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+        double dsum = 0.0;
+        for (long long i = part * (long long)blockDim.x + threadIdx.x; i < n;
+             i += (long long)nparts * blockDim.x) {
+            const double x = v.x[i * v.ps], y = v.y[i * v.ps];
+            k[0] = min(k[0], vx_dkey(x));
+            k[1] = min(k[1], vx_dkey(-x));
+            k[2] = min(k[2], vx_dkey(y));
+            k[3] = min(k[3], vx_dkey(-y));
+            dsum += v.d[i];
+        }
+        for (int q = 0; q < 4; ++q) sk[q][threadIdx.x] = k[q];
+        sd[threadIdx.x] = dsum;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) {
+                for (int q = 0; q < 4; ++q) sk[q][threadIdx.x] = min(sk[q][threadIdx.x], sk[q][threadIdx.x + o]);
+                sd[threadIdx.x] += sd[threadIdx.x + o];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x < 4) box[4 * part + threadIdx.x] = sk[threadIdx.x][0];
+        if (threadIdx.x == 0) red[part] = sd[0];
+        __syncthreads();
+    }
+    if (!vx_last_block(&S->sync_ctr, vb.n)) return;
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
-    double dsum = 0.0;
-    for (long long i = part * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)nparts * blockDim.x) {
-        const double x = v.x[i * v.ps], y = v.y[i * v.ps];
-        k[0] = min(k[0], vx_dkey(x));
-        k[1] = min(k[1], vx_dkey(-x));
-        k[2] = min(k[2], vx_dkey(y));
-        k[3] = min(k[3], vx_dkey(-y));
-        dsum += v.d[i];
+    double dpart = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += CG_T) {
+        dpart += __ldcg(&red[b]);
+        if ((long long)b * CG_T < n)
+            for (int q = 0; q < 4; ++q) k[q] = min(k[q], __ldcg(&box[4 * b + q]));
     }
     for (int q = 0; q < 4; ++q) sk[q][threadIdx.x] = k[q];
-    sd[threadIdx.x] = dsum;
+    sd[threadIdx.x] = dpart;
     __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    for (int o = CG_T / 2; o > 0; o >>= 1) {
         if (threadIdx.x < o) {
             for (int q = 0; q < 4; ++q) sk[q][threadIdx.x] = min(sk[q][threadIdx.x], sk[q][threadIdx.x + o]);
             sd[threadIdx.x] += sd[threadIdx.x + o];
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < 4; ++q) atomicMin(&S->cb[q], sk[q][0]);
-        red[part] = sd[0];
-    }
-}
-// The sum of d is split into nparts fixed partitions whatever the grid (a
-// partition past the last particle adds 0), so the mean spacing, and the
-// grid built from it, do not depend on the launch's grid.
-VX_DEVK void k_cg_bbox_body(VxBlkB<CG_T, 0> vb, VxView v, VxScalars *S, double *red, int nparts) {
-    const long long n = S->n;
-    for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) {
-        if ((long long)q * blockDim.x >= n) {
-            if (threadIdx.x == 0) red[q] = 0.0;
-            continue;
-        }
-        cg_bbox_part(q, (unsigned)nparts, v, S, red);
-    }
-}
-__global__ void __launch_bounds__(CG_T) k_cg_bbox(VxView v, VxScalars *S, double *red, int nparts) {
-    VX_PDL_WAIT();
-    k_cg_bbox_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, v, S, red, nparts);
-}
-
-// Cell side h = c * mean(d) / CG_DIV, grown until the grid fits cells_cap.
-// One block of CG_T threads: the per-block sums of d are added in a fixed
-// tree (reproducible), then thread 0 sizes the grid.
-VX_DEVK void k_cg_params_body(VxBlkB<CG_T, 0> vb, VxScalars *S, const double *red, int nblocks, double cutoff,
-                              long long cells_cap) {
-    __shared__ double sd[CG_T];
-    double part = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += CG_T) part += red[b];
-    sd[threadIdx.x] = part;
-    __syncthreads();
-    for (int o = CG_T / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) sd[threadIdx.x] += sd[threadIdx.x + o];
-        __syncthreads();
-    }
     if (threadIdx.x != 0) return;
-    const long long n = S->n;
+    S->cnwide = 0;
+    S->cnhuge = 0;
+    S->bk_nmid = S->bk_nbig = 0;
     S->cnitems = 0;
     if (n == 0) { S->cncells = 0; S->cnx = S->cny = 0; return; }
     const double dsum = sd[0];
-    const double x0 = vx_dunkey(S->cb[0]), x1 = -vx_dunkey(S->cb[1]);
-    const double y0 = vx_dunkey(S->cb[2]), y1 = -vx_dunkey(S->cb[3]);
+    const double x0 = vx_dunkey(sk[0][0]), x1 = -vx_dunkey(sk[1][0]);
+    const double y0 = vx_dunkey(sk[2][0]), y1 = -vx_dunkey(sk[3][0]);
     double h = cutoff * (dsum / (double)n) / (double)CG_DIV;
     if (!(h > 0.0)) h = 1e-3;
     long long nx = -1, ny = -1;
@@ -128,10 +114,10 @@ VX_DEVK void k_cg_params_body(VxBlkB<CG_T, 0> vb, VxScalars *S, const double *re
     S->cx0 = x0; S->cy0 = y0; S->ch = h;
     S->cnx = nx; S->cny = ny; S->cncells = nx * ny;
 }
-__global__ void __launch_bounds__(CG_T) k_cg_params(VxScalars *S, const double *red, int nblocks, double cutoff,
-                                                    long long cells_cap) {
+__global__ void __launch_bounds__(CG_T) k_cg_prep(VxView v, VxScalars *S, double *red, unsigned long long *box,
+                                                  int sms, double cutoff, long long cells_cap) {
     VX_PDL_WAIT();
-    k_cg_params_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, S, red, nblocks, cutoff, cells_cap);
+    k_cg_prep_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, v, S, red, box, sms, cutoff, cells_cap);
 }
 
 __device__ __forceinline__ long long cg_cell(const VxScalars *S, double x, double y) {
@@ -142,17 +128,8 @@ __device__ __forceinline__ long long cg_cell(const VxScalars *S, double x, doubl
     return cy * S->cnx + cx;
 }
 
-VX_DEVK void k_cg_zero_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt) {
-    const long long nc = S->cncells;
-    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < nc;
-         c += (long long)vb.n * blockDim.x)
-        cnt[c] = 0;
-}
-__global__ void k_cg_zero(const VxScalars *S, int *cnt) {
-    VX_PDL_WAIT();
-    k_cg_zero_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt);
-}
-
+// Cell of every particle, counted per cell (the counts are zero between
+// steps: the bucket order leaves them at zero once the order is built).
 VX_DEVK void k_cg_cellid_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
     const long long n = S->n;
     if (S->cncells == 0) return;
@@ -169,172 +146,51 @@ __global__ void k_cg_cellid(VxView v, const VxScalars *S, unsigned *key, int *va
     k_cg_cellid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, key, val, cnt);
 }
 
-// Exclusive scan of cnt[0, len) into start[], start[len] = total: chunk
-// sums, one-block scan of the chunk sums, per-chunk apply.
-VX_DEVK void k_scan_sum_body(VxBlkB<CG_T, 0> vb, const long long *len_p, const int *cnt, int *csum) {
-    __shared__ int sh[CG_T];
-    const long long len = *len_p, nch = vx_ceil_div(len, VX_CHUNK);
-    for (long long c = vb.x; c < nch; c += vb.n) {
-        int k = 0;
-        for (long long q = c * VX_CHUNK + threadIdx.x; q < min(len, (c + 1) * VX_CHUNK); q += blockDim.x) k += cnt[q];
-        sh[threadIdx.x] = k;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) csum[c] = sh[0];
-        __syncthreads();
-    }
-}
-__global__ void __launch_bounds__(CG_T) k_scan_sum(const long long *len_p, const int *cnt, int *csum) {
-    VX_PDL_WAIT();
-    k_scan_sum_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, len_p, cnt, csum);
-}
-
-VX_DEVK void k_scan_top_body(VxBlkB<1024, 0> vb, const long long *len_p, const int *csum, long long *coff) {
-    __shared__ long long sh[1024];
-    __shared__ long long carry;
-    const long long nch = vx_ceil_div(*len_p, VX_CHUNK);
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (long long base = 0; base < nch; base += blockDim.x) {
-        const long long c = base + threadIdx.x;
-        const long long val = c < nch ? csum[c] : 0;
-        sh[threadIdx.x] = val;
-        __syncthreads();
-        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-            long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (c < nch) coff[c] = carry + sh[threadIdx.x] - val;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry += sh[threadIdx.x];
-        __syncthreads();
-    }
-}
-__global__ void __launch_bounds__(1024) k_scan_top(const long long *len_p, const int *csum, long long *coff) {
-    VX_PDL_WAIT();
-    k_scan_top_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, len_p, csum, coff);
-}
-
-VX_DEVK void k_scan_apply_body(VxBlkB<CG_T, 0> vb, const long long *len_p, const int *cnt, const long long *coff,
-                               int *start, const long long *total_p) {
-    constexpr int PER = VX_CHUNK / CG_T;
-    __shared__ int sh[CG_T];
-    const long long len = *len_p, nch = vx_ceil_div(len, VX_CHUNK);
-    if (vb.x == 0 && threadIdx.x == 0) start[len] = (int)*total_p;
-    for (long long c = vb.x; c < nch; c += vb.n) {
-        const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
-        int val[PER], loc = 0;
+// Cell starts: one-pass scan of the counts, start[cncells] = n.
+VX_DEVK void k_cg_scan_body(VxBlkB<VX_SCAN_T, 0> vb, VxScalars *S, const int *cnt, int *start,
+                            unsigned long long *tiles) {
+    const long long nc = S->cncells;
+    vx_scan_lookback<VX_CHUNK / VX_SCAN_T>(
+        vb.n, nc, S, tiles, [&](long long i) { return cnt[i]; },
+        [&](long long i0, const unsigned *val, long long run) {
 #pragma unroll
-        for (int q = 0; q < PER; ++q) { val[q] = (b + q < len) ? cnt[b + q] : 0; loc += val[q]; }
-        sh[threadIdx.x] = loc;
-        __syncthreads();
-        for (int o = 1; o < CG_T; o <<= 1) {
-            int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        long long run = coff[c] + sh[threadIdx.x] - loc;
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            if (b + q < len) start[b + q] = (int)run;
-            run += val[q];
-        }
-    }
+            for (int q = 0; q < VX_CHUNK / VX_SCAN_T; ++q) {
+                if (i0 + q < nc) start[i0 + q] = (int)run;
+                run += val[q];
+            }
+        },
+        [&](long long) { start[nc] = (int)S->n; });
 }
-__global__ void __launch_bounds__(CG_T) k_scan_apply(const long long *len_p, const int *cnt, const long long *coff,
-                                                     int *start, const long long *total_p) {
+__global__ void __launch_bounds__(VX_SCAN_T) k_cg_scan(VxScalars *S, const int *cnt, int *start,
+                                                       unsigned long long *tiles) {
     VX_PDL_WAIT();
-    k_scan_apply_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, len_p, cnt, coff, start, total_p);
+    k_cg_scan_body(VxBlkB<VX_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, cnt, start, tiles);
 }
 
-// Cell-sorted particles (x, y relative to their cell centre, G, d).  Keeping
-// FP32 positions relative to the cell keeps the pair differences accurate to
-// FP32 rounding of the local spacing rather than of the absolute position.
-VX_DEVK void k_cg_gather_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
-    const long long n = S->n, nx = S->cnx;
-    const double h = S->ch;
-    for (long long k = vb.x * (long long)blockDim.x + threadIdx.x; k < n;
-         k += (long long)vb.n * blockDim.x) {
-        const long long i = sorted[k];
-        const long long c = skey[k];
-        const double ccx = S->cx0 + ((double)(c % nx) + 0.5) * h, ccy = S->cy0 + ((double)(c / nx) + 0.5) * h;
-        srt[k] = make_float4((float)(v.x[i * v.ps] - ccx), (float)(v.y[i * v.ps] - ccy), (float)v.g[i * v.ps],
-                             (float)v.d[i]);
-    }
-}
-__global__ void k_cg_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
-    VX_PDL_WAIT();
-    k_cg_gather_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, sorted, skey, srt);
-}
-
-// Exclusive scan of the per-row item counts (single block, runs per thread).
-VX_DEVK void k_cg_row_scan_body(VxBlkB<1024, 0> vb, const VxScalars *S, const int *in, long long *out) {
-    __shared__ long long sh[1024];
-    const long long len = S->cny;
-    const long long per = vx_ceil_div(len, (long long)blockDim.x);
-    const long long b = threadIdx.x * per, e = min(len, b + per);
-    long long local = 0;
-    for (long long q = b; q < e; ++q) local += in[q];
-    sh[threadIdx.x] = local;
-    __syncthreads();
-    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-        long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-        __syncthreads();
-        sh[threadIdx.x] += t;
-        __syncthreads();
-    }
-    long long run = sh[threadIdx.x] - local;
-    for (long long q = b; q < e; ++q) {
-        out[q] = run;
-        run += in[q];
-    }
-}
-__global__ void __launch_bounds__(1024) k_cg_row_scan(const VxScalars *S, const int *in, long long *out) {
-    VX_PDL_WAIT();
-    k_cg_row_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, in, out);
-}
-
-// Work items: each row's sorted range cut into segments of CG_W targets.
-VX_DEVK void k_cg_row_items_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, int *row_items) {
+// Work items: each row's sorted range cut into segments of CG_W targets, as
+// (row, first sorted slot); one-pass scan of the rows' item counts, one row
+// per thread.
+VX_DEVK void k_cg_items_body(VxBlkB<VX_SCAN_T, 0> vb, VxScalars *S, const int *start, int2 *items, long long items_cap,
+                             unsigned long long *tiles) {
     const long long ny = S->cny, nx = S->cnx;
-    for (long long r = vb.x * (long long)blockDim.x + threadIdx.x; r < ny;
-         r += (long long)vb.n * blockDim.x) {
-        const int cnt = start[(r + 1) * nx] - start[r * nx];
-        row_items[r] = (cnt + CG_W - 1) / CG_W;
-    }
+    vx_scan_lookback<1>(
+        vb.n, ny, S, tiles,
+        [&](long long r) { return (start[(r + 1) * nx] - start[r * nx] + CG_W - 1) / CG_W; },
+        [&](long long r, const unsigned *val, long long run) {
+            if (r >= ny) return;
+            const int s0 = start[r * nx];
+            for (unsigned q = 0; q < val[0]; ++q)
+                if (run + q < items_cap) items[run + q] = make_int2((int)r, s0 + (int)q * CG_W);
+        },
+        [&](long long tot) {
+            S->cnitems = tot <= items_cap ? tot : 0;
+            if (tot > items_cap) S->err |= VX_DERR_GRID;
+        });
 }
-__global__ void k_cg_row_items(const VxScalars *S, const int *start, int *row_items) {
+__global__ void __launch_bounds__(VX_SCAN_T) k_cg_items(VxScalars *S, const int *start, int2 *items,
+                                                        long long items_cap, unsigned long long *tiles) {
     VX_PDL_WAIT();
-    k_cg_row_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items);
-}
-
-VX_DEVK void k_cg_items_body(VxBlkB<0, 0> vb, VxScalars *S, const int *start, const int *row_items, const long long *row_off,
-                             int2 *items, long long items_cap) {
-    const long long ny = S->cny, nx = S->cnx;
-    if (vb.x == 0 && threadIdx.x == 0 && ny > 0) {
-        const long long tot = row_off[ny - 1] + row_items[ny - 1];
-        S->cnitems = tot <= items_cap ? tot : 0;
-        if (tot > items_cap) S->err |= VX_DERR_GRID;
-    }
-    for (long long r = vb.x * (long long)blockDim.x + threadIdx.x; r < ny;
-         r += (long long)vb.n * blockDim.x) {
-        const long long o = row_off[r];
-        const int s0 = start[r * nx];
-        for (int q = 0; q < row_items[r]; ++q)
-            if (o + q < items_cap) items[o + q] = make_int2((int)r, s0 + q * CG_W);
-    }
-}
-__global__ void k_cg_items(VxScalars *S, const int *start, const int *row_items, const long long *row_off,
-                           int2 *items, long long items_cap) {
-    VX_PDL_WAIT();
-    k_cg_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items, row_off, items, items_cap);
+    k_cg_items_body(VxBlkB<VX_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, start, items, items_cap, tiles);
 }
 
 __device__ __forceinline__ float vx_rsqrt_approx(float x) {
@@ -748,30 +604,31 @@ __global__ void __launch_bounds__(WIDE_T) k_diff_huge(VxParams p, VxView v, VxSc
     k_diff_huge_body(VxBlkB<WIDE_T, 0>{blockIdx.x, gridDim.x}, p, v, S, srt, skey, sorted, start, huge);
 }
 
-// Build the grid and run the bulk diffusion.  Scratch from w; the collapse
-// chunk arrays are reused (the passes run one after the other on one stream).
+// Build the grid and run the bulk diffusion (scratch from w).
 cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                       VxWork &w) {
     const int grid = L.num_sms * 4;
-    vx_launch<k_cg_begin, k_cg_begin_body>(L, 1, 1, 0, S);
-    const int nparts = std::min(vx_part_sms(L) * 4, VX_RED_BLOCKS);
-    vx_launch<k_cg_bbox, k_cg_bbox_body>(L, std::min(nparts, L.num_sms * 4), CG_T, 0, v, S, w.red, nparts);
-    vx_launch<k_cg_params, k_cg_params_body>(L, 1, CG_T, 0, S, w.red, nparts, p.diff_cutoff, w.cells_cap);
-    vx_launch<k_cg_zero, k_cg_zero_body>(L, grid, CG_T, 0, S, w.cg_cnt);
+    // partitions of the mean spacing follow the body's count on the device
+    // (vx_body_parts), the grid the SMs this launch is given
+    vx_launch<k_cg_prep, k_cg_prep_body>(L, std::min(VX_RED_BLOCKS, L.num_sms * 4), CG_T, 0, v, S, w.red, w.box,
+                                         vx_full_sms(L), p.diff_cutoff, w.cells_cap);
     vx_launch<k_cg_cellid, k_cg_cellid_body>(L, grid, CG_T, 0, v, S, w.key0, w.val0, w.cg_cnt);
-    vx_launch<k_scan_sum, k_scan_sum_body>(L, grid, CG_T, 0, &S->cncells, w.cg_cnt, w.cell_chunk_cnt);
-    vx_launch<k_scan_top, k_scan_top_body>(L, 1, 1024, 0, &S->cncells, w.cell_chunk_cnt, w.cell_chunk_off);
-    vx_launch<k_scan_apply, k_scan_apply_body>(L, grid, CG_T, 0, &S->cncells, w.cg_cnt, w.cell_chunk_off, w.cg_start, &S->n);
+    vx_launch<k_cg_scan, k_cg_scan_body>(L, grid, VX_SCAN_T, 0, S, w.cg_cnt, w.cg_start, w.scan_tiles);
 
-    // cell order: each cell's vortices in index order (a stable sort by cell)
+    // cell order: each cell's vortices in index order (a stable sort by cell),
+    // the FP32 sources gathered at their slots on the way; the cell counts
+    // are left at zero for the next step's count
+    VxGather gt;
+    gt.mode = 2;
+    gt.zero_counts = 1;
+    gt.v = v;
+    gt.S = S;
+    gt.srt = w.srt;
     vx_bucket_order(L, S, &S->n, &S->cncells, w.key0, w.cg_start, w.cg_cnt, nullptr, w.key1, w.val1, w.bk_mid, w.bk_big,
-                    w.val0);
+                    w.val0, gt);
     const unsigned *skey = w.key1;
     const int *sorted = w.val1;
-    vx_launch<k_cg_gather, k_cg_gather_body>(L, grid, CG_T, 0, v, S, sorted, skey, w.srt);
-    vx_launch<k_cg_row_items, k_cg_row_items_body>(L, grid, CG_T, 0, S, w.cg_start, w.row_items);
-    vx_launch<k_cg_row_scan, k_cg_row_scan_body>(L, 1, 1024, 0, S, w.row_items, w.row_item_off);
-    vx_launch<k_cg_items, k_cg_items_body>(L, grid, CG_T, 0, S, w.cg_start, w.row_items, w.row_item_off, w.items, w.items_cap);
+    vx_launch<k_cg_items, k_cg_items_body>(L, grid, VX_SCAN_T, 0, S, w.cg_start, w.items, w.items_cap, w.scan_tiles);
 
     VX_EV(L, 2);
     vx_launch<k_diff_cells, k_diff_cells_body>(L, L.num_sms * 8, CG_T, 0, p, v, S, w.srt, skey, sorted, w.cg_start, w.items, w.cg_wide);

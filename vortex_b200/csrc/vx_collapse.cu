@@ -17,24 +17,27 @@
 //    pointing at j; later ones merge with (0, 1e10) as the serial loop does,
 //    which re-rounds their position.
 //  * Compaction then runs as after convection.
+// A round is six launches before the compaction: prep (box, bookkeeping and
+// grid in one, the last block finishing), count, a one-pass scan of the cell
+// counts, scatter, query, and settle (resolution, merge and write-back in
+// one block).
 #include <limits.h>
 
 #include "vx_internal.cuh"
 
-VX_DEVK void k_col_begin_body(VxBlkB<0, 0> vb, VxScalars *S, int reset) {
-    if (reset) S->col_done = 0;
-    if (S->col_done) return;
-    S->col_n_before = S->n;
-    S->ncand = 0;
-    S->bb[0] = S->bb[1] = S->bb[2] = S->bb[3] = ~0ull;
-}
-__global__ void k_col_begin(VxScalars *S, int reset) {
-    VX_PDL_WAIT();
-    k_col_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, reset);
-}
-
-VX_DEVK void k_col_bbox_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S) {
-    if (S->col_done) return;
+// Start of a round: the bounding box (per-block keys into part[], combined
+// by the last block), the round's bookkeeping and the cell grid.  A round
+// after one that removed nothing (or after a failed one) does nothing: the
+// pass has converged.  Cell side h = r (1 + 1e-6): any pair closer than r is
+// in neighbouring cells; when the box would need more than cells_cap cells,
+// h grows.
+VX_DEVK void k_col_prep_body(VxBlkB<VX_THREADS, 0> vb, VxView v, VxScalars *S, int reset, double r2,
+                             long long cells_cap, unsigned long long *part) {
+    const bool done = reset ? false : (S->col_done || S->n == S->col_n_before);
+    if (done) {
+        if (vb.x == 0 && threadIdx.x == 0) S->col_done = 1;
+        return;
+    }
     __shared__ unsigned long long sh[4][VX_THREADS];
     const long long n = S->n;
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
@@ -53,40 +56,43 @@ VX_DEVK void k_col_bbox_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S) {
             for (int q = 0; q < 4; ++q) sh[q][threadIdx.x] = min(sh[q][threadIdx.x], sh[q][threadIdx.x + o]);
         __syncthreads();
     }
-    if (threadIdx.x == 0)
-        for (int q = 0; q < 4; ++q) atomicMin(&S->bb[q], sh[q][0]);
-}
-__global__ void k_col_bbox(VxView v, VxScalars *S) {
-    VX_PDL_WAIT();
-    k_col_bbox_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S);
-}
-
-// Cell size h = r (1 + 1e-6): any pair closer than r is in neighbouring cells.
-// When the box would need more than cells_cap cells, h grows.
-VX_DEVK void k_col_grid_body(VxBlkB<0, 0> vb, VxScalars *S, double r2, long long cells_cap) {
-    if (S->col_done) return;
-    const long long n = S->n;
+    if (threadIdx.x < 4) part[4 * vb.x + threadIdx.x] = sh[threadIdx.x][0];
+    if (!vx_last_block(&S->sync_ctr, vb.n)) return;
+    for (int q = 0; q < 4; ++q) k[q] = ~0ull;
+    for (unsigned b = threadIdx.x; b < vb.n; b += blockDim.x)
+        for (int q = 0; q < 4; ++q) k[q] = min(k[q], __ldcg(&part[4 * b + q]));
+    for (int q = 0; q < 4; ++q) sh[q][threadIdx.x] = k[q];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int q = 0; q < 4; ++q) sh[q][threadIdx.x] = min(sh[q][threadIdx.x], sh[q][threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    S->col_done = 0;
+    S->col_n_before = n;
+    S->ncand = 0;
     if (n == 0) { S->gncells = 0; S->gnx = S->gny = 0; return; }
-    const double x0 = vx_dunkey(S->bb[0]), x1 = -vx_dunkey(S->bb[1]);
-    const double y0 = vx_dunkey(S->bb[2]), y1 = -vx_dunkey(S->bb[3]);
+    const double x0 = vx_dunkey(sh[0][0]), x1 = -vx_dunkey(sh[1][0]);
+    const double y0 = vx_dunkey(sh[2][0]), y1 = -vx_dunkey(sh[3][0]);
     // side = the collapse radius: the 3 x 3 search is exact and sees the
     // fewest candidates (a side at the mean spacing, with a quarter of the
     // cells to count and scan, was measured slower: the query dominates)
     double h = sqrt(r2) * (1.0 + 1e-6);
-    long long nx, ny;
+    long long nx = -1, ny = -1;
     for (int it = 0; it < 200; ++it) {
         double fx = floor((x1 - x0) / h) + 1.0, fy = floor((y1 - y0) / h) + 1.0;
         if (fx * fy <= (double)cells_cap) { nx = (long long)fx; ny = (long long)fy; break; }
         h *= 1.25;
-        nx = ny = -1;
     }
     if (nx < 0) { S->err |= VX_DERR_GRID; S->gncells = 0; S->col_done = 1; return; }
     S->gx0 = x0; S->gy0 = y0; S->gh = h;
     S->gnx = nx; S->gny = ny; S->gncells = nx * ny;
 }
-__global__ void k_col_grid(VxScalars *S, double r2, long long cells_cap) {
+__global__ void __launch_bounds__(VX_THREADS) k_col_prep(VxView v, VxScalars *S, int reset, double r2,
+                                                         long long cells_cap, unsigned long long *part) {
     VX_PDL_WAIT();
-    k_col_grid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, r2, cells_cap);
+    k_col_prep_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, v, S, reset, r2, cells_cap, part);
 }
 
 __device__ __forceinline__ void vx_cell_of(const VxScalars *S, double x, double y, long long &cx,
@@ -95,18 +101,6 @@ __device__ __forceinline__ void vx_cell_of(const VxScalars *S, double x, double 
     cy = (long long)floor((y - S->gy0) / S->gh);
     cx = cx < 0 ? 0 : (cx >= S->gnx ? S->gnx - 1 : cx);
     cy = cy < 0 ? 0 : (cy >= S->gny ? S->gny - 1 : cy);
-}
-
-VX_DEVK void k_col_zero_cells_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt) {
-    if (S->col_done) return;
-    const long long nc = S->gncells;
-    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < nc;
-         c += (long long)vb.n * blockDim.x)
-        cnt[c] = 0;
-}
-__global__ void k_col_zero_cells(const VxScalars *S, int *cnt) {
-    VX_PDL_WAIT();
-    k_col_zero_cells_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt);
 }
 
 VX_DEVK void k_col_count_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
@@ -131,100 +125,30 @@ __global__ void k_col_count(VxView v, const VxScalars *S, int *cellid, int *cnt,
     k_col_count_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cellid, cnt, in_cnt, has_app, first_app);
 }
 
-// Exclusive scan of cnt[0, gncells) into start[], start[gncells] = total.
-VX_DEVK void k_cell_chunk_sum_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *cnt, int *csum) {
+// Cell starts: exclusive scan of the counts in one pass, start[gncells] = n.
+VX_DEVK void k_col_scan_body(VxBlkB<VX_SCAN_T, 0> vb, VxScalars *S, const int *cnt, int *start,
+                             unsigned long long *tiles) {
     if (S->col_done) return;
-    __shared__ int sh[VX_THREADS];
     const long long nc = S->gncells;
-    const long long nch = vx_ceil_div(nc, VX_CHUNK);
-    for (long long c = vb.x; c < nch; c += vb.n) {
-        int k = 0;
-        for (long long p = c * VX_CHUNK + threadIdx.x; p < min(nc, (c + 1) * VX_CHUNK); p += blockDim.x)
-            k += cnt[p];
-        sh[threadIdx.x] = k;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) csum[c] = sh[0];
-        __syncthreads();
-    }
-}
-__global__ void k_cell_chunk_sum(const VxScalars *S, const int *cnt, int *csum) {
-    VX_PDL_WAIT();
-    k_cell_chunk_sum_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt, csum);
-}
-
-VX_DEVK void k_cell_chunk_scan_body(VxBlkB<1024, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
-    if (S->col_done) return;
-    __shared__ long long sh[1024];
-    __shared__ long long carry;
-    const long long nch = vx_ceil_div(S->gncells, VX_CHUNK);
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (long long base = 0; base < nch; base += blockDim.x) {
-        long long c = base + threadIdx.x;
-        long long val = c < nch ? csum[c] : 0;
-        sh[threadIdx.x] = val;
-        __syncthreads();
-        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-            long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (c < nch) coff[c] = carry + sh[threadIdx.x] - val;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry += sh[threadIdx.x];
-        __syncthreads();
-    }
-}
-__global__ void __launch_bounds__(1024) k_cell_chunk_scan(const VxScalars *S, const int *csum, long long *coff) {
-    VX_PDL_WAIT();
-    k_cell_chunk_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
-}
-
-VX_DEVK void k_cell_chunk_apply_body(VxBlkB<VX_THREADS, 0> vb, const VxScalars *S, const int *cnt,
-                                     const long long *coff, int *start) {
-    if (S->col_done) return;
-    constexpr int PER = VX_CHUNK / VX_THREADS;
-    __shared__ int sh[VX_THREADS];
-    const long long nc = S->gncells;
-    const long long nch = vx_ceil_div(nc, VX_CHUNK);
-    if (vb.x == 0 && threadIdx.x == 0) start[nc] = (int)S->n;   // sentinel
-    for (long long c = vb.x; c < nch; c += vb.n) {
-        const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
-        int val[PER];
-        int loc = 0;
+    vx_scan_lookback<VX_CHUNK / VX_SCAN_T>(
+        vb.n, nc, S, tiles, [&](long long i) { return cnt[i]; },
+        [&](long long i0, const unsigned *val, long long run) {
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            val[q] = (b + q < nc) ? cnt[b + q] : 0;
-            loc += val[q];
-        }
-        sh[threadIdx.x] = loc;
-        __syncthreads();
-        for (int o = 1; o < VX_THREADS; o <<= 1) {
-            int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        long long run = coff[c] + sh[threadIdx.x] - loc;
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            if (b + q < nc) start[b + q] = (int)run;
-            run += val[q];
-        }
-    }
+            for (int q = 0; q < VX_CHUNK / VX_SCAN_T; ++q) {
+                if (i0 + q < nc) start[i0 + q] = (int)run;
+                run += val[q];
+            }
+        },
+        [&](long long tot) { start[nc] = (int)tot; });
 }
-__global__ void __launch_bounds__(VX_THREADS) k_cell_chunk_apply(const VxScalars *S, const int *cnt,
-                                                                 const long long *coff, int *start) {
+__global__ void __launch_bounds__(VX_SCAN_T) k_col_scan(VxScalars *S, const int *cnt, int *start,
+                                                        unsigned long long *tiles) {
     VX_PDL_WAIT();
-    k_cell_chunk_apply_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, S, cnt, coff, start);
+    k_col_scan_body(VxBlkB<VX_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, cnt, start, tiles);
 }
 
+// Each cell's slots from its start, counting its count back down to zero
+// (the zero the next pass's count starts from).
 VX_DEVK void k_col_scatter_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *cellid, const int *start, int *cnt,
                                 int *sorted) {
     if (S->col_done) return;
@@ -293,10 +217,15 @@ __global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *celli
     k_col_query_body<PASS>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, cellid, start, sorted, col, in_cnt, cand);
 }
 
-// Rounds over the candidate list (single block).  cstate: 0 undecided,
-// 1 applied, 2 consumed before its turn.
-VX_DEVK void k_col_resolve_body(VxBlkB<1024, 0> vb, VxScalars *S, const int *cand, const int *col, int *in_cnt,
-                                int *has_app, int *first_app, int *cstate, int *cdec) {
+// Settles the candidates in one block: rounds over the candidate list decide
+// each one (cstate: 0 undecided, 1 applied, 2 consumed before its turn), then
+// every applied candidate's merged vortex is computed from the positions as
+// they were, then written (after a barrier: a merge may read a partner that
+// another merge removes).
+template <int PASS>
+VX_DEVK void k_col_settle_body(VxBlkB<1024, 0> vb, VxView v, VxScalars *S, const int *cand, const int *col,
+                               int *in_cnt, int *has_app, int *first_app, int *cstate, int *cdec, double *mx,
+                               double *my, double *mg) {
     if (S->col_done) return;
     __shared__ int undecided;
     const int nc = S->ncand;
@@ -332,24 +261,14 @@ VX_DEVK void k_col_resolve_body(VxBlkB<1024, 0> vb, VxScalars *S, const int *can
         if (undecided == 0) break;
         __syncthreads();
     }
-    if (threadIdx.x == 0 && round >= max_rounds) {
-        S->err |= VX_DERR_RESOLVE;
-        S->col_done = 1;
+    if (round >= max_rounds) {
+        if (threadIdx.x == 0) {
+            S->err |= VX_DERR_RESOLVE;
+            S->col_done = 1;
+        }
+        return;
     }
-}
-__global__ void __launch_bounds__(1024) k_col_resolve(VxScalars *S, const int *cand, const int *col, int *in_cnt,
-                              int *has_app, int *first_app, int *cstate, int *cdec) {
-    VX_PDL_WAIT();
-    k_col_resolve_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, cand, col, in_cnt, has_app, first_app, cstate, cdec);
-}
-
-template <int PASS>
-VX_DEVK void k_col_merge_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *cand, const int *col,
-                              const int *cstate, const int *first_app, double *mx, double *my,
-                              double *mg) {
-    if (S->col_done) return;
-    const int nc = S->ncand;
-    for (int k = vb.x * blockDim.x + threadIdx.x; k < nc; k += vb.n * blockDim.x) {
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
         if (cstate[k] != 1) continue;
         const long long i = cand[k], j = col[i];
         const double xi = v.x[i * v.ps], yi = v.y[i * v.ps], gi = v.g[i * v.ps];
@@ -368,71 +287,41 @@ VX_DEVK void k_col_merge_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, con
             mg[k] = ng;
         }
     }
-}
-template <int PASS>
-__global__ void k_col_merge(VxView v, const VxScalars *S, const int *cand, const int *col,
-                            const int *cstate, const int *first_app, double *mx, double *my,
-                            double *mg) {
-    VX_PDL_WAIT();
-    k_col_merge_body<PASS>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cand, col, cstate, first_app, mx, my, mg);
-}
-
-VX_DEVK void k_col_apply_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *cand, const int *col,
-                              const int *cstate, const double *mx, const double *my, const double *mg) {
-    if (S->col_done) return;
-    const int nc = S->ncand;
-    for (int k = vb.x * blockDim.x + threadIdx.x; k < nc; k += vb.n * blockDim.x) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
         if (cstate[k] != 1) continue;
         const long long i = cand[k], j = col[i];
         v.x[i * v.ps] = mx[k]; v.y[i * v.ps] = my[k]; v.g[i * v.ps] = mg[k];
         v.x[j * v.ps] = 1e10; v.y[j * v.ps] = 1e10; v.g[j * v.ps] = 0.0;
     }
 }
-__global__ void k_col_apply(VxView v, const VxScalars *S, const int *cand, const int *col,
-                            const int *cstate, const double *mx, const double *my, const double *mg) {
+template <int PASS>
+__global__ void __launch_bounds__(1024) k_col_settle(VxView v, VxScalars *S, const int *cand, const int *col,
+                                                     int *in_cnt, int *has_app, int *first_app, int *cstate,
+                                                     int *cdec, double *mx, double *my, double *mg) {
     VX_PDL_WAIT();
-    k_col_apply_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cand, col, cstate, mx, my, mg);
-}
-
-VX_DEVK void k_col_end_body(VxBlkB<0, 0> vb, VxScalars *S) {
-    if (S->col_done) return;
-    if (S->n == S->col_n_before) S->col_done = 1;
-}
-__global__ void k_col_end(VxScalars *S) {
-    VX_PDL_WAIT();
-    k_col_end_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
+    k_col_settle_body<PASS>(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, v, S, cand, col, in_cnt, has_app, first_app,
+                            cstate, cdec, mx, my, mg);
 }
 
 cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                VxWork &w, int pass, int n_col) {
     const double r2 = pass == 1 ? p.r_diff2 : p.r_same2;
     if (!(r2 > 0.0) || n_col <= 0) return cudaSuccess;   // no pair can qualify
-    const int grid = L.num_sms * 4;
+    const int grid = std::min(L.num_sms * 4, VX_RED_BLOCKS);   // 4 box keys per block
     for (int cc = 0; cc < n_col; ++cc) {
-        vx_launch<k_col_begin, k_col_begin_body>(L, 1, 1, 0, S, cc == 0);
-        vx_launch<k_col_bbox, k_col_bbox_body>(L, grid, VX_THREADS, 0, v, S);
-        vx_launch<k_col_grid, k_col_grid_body>(L, 1, 1, 0, S, r2, w.cells_cap);
-        vx_launch<k_col_zero_cells, k_col_zero_cells_body>(L, grid, VX_THREADS, 0, S, w.cell_cnt);
+        vx_launch<k_col_prep, k_col_prep_body>(L, grid, VX_THREADS, 0, v, S, cc == 0, r2, w.cells_cap, w.box);
         vx_launch<k_col_count, k_col_count_body>(L, grid, VX_THREADS, 0, v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app, w.first_app);
-        vx_launch<k_cell_chunk_sum, k_cell_chunk_sum_body>(L, grid, VX_THREADS, 0, S, w.cell_cnt, w.cell_chunk_cnt);
-        vx_launch<k_cell_chunk_scan, k_cell_chunk_scan_body>(L, 1, 1024, 0, S, w.cell_chunk_cnt, w.cell_chunk_off);
-        vx_launch<k_cell_chunk_apply, k_cell_chunk_apply_body>(L, grid, VX_THREADS, 0, S, w.cell_cnt, w.cell_chunk_off, w.cell_start);
+        vx_launch<k_col_scan, k_col_scan_body>(L, grid, VX_SCAN_T, 0, S, w.cell_cnt, w.cell_start, w.scan_tiles);
         vx_launch<k_col_scatter, k_col_scatter_body>(L, grid, VX_THREADS, 0, S, w.cellid, w.cell_start, w.cell_cnt, w.sorted);
-        if (pass == 1)
+        if (pass == 1) {
             vx_launch<k_col_query<1>, k_col_query_body<1>>(L, grid, VX_THREADS, 0, p, v, S, w.cellid, w.cell_start, w.sorted, w.col, w.in_cnt, w.cand);
-        else
+            vx_launch<k_col_settle<1>, k_col_settle_body<1>>(L, 1, 1024, 0, v, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec, w.mx, w.my, w.mg);
+        } else {
             vx_launch<k_col_query<2>, k_col_query_body<2>>(L, grid, VX_THREADS, 0, p, v, S, w.cellid, w.cell_start, w.sorted, w.col, w.in_cnt, w.cand);
-
-        vx_launch<k_col_resolve, k_col_resolve_body>(L, 1, 1024, 0, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec);
-        if (pass == 1)
-            vx_launch<k_col_merge<1>, k_col_merge_body<1>>(L, grid, VX_THREADS, 0, v, S, w.cand, w.col, w.cstate, w.first_app, w.mx, w.my, w.mg);
-        else
-            vx_launch<k_col_merge<2>, k_col_merge_body<2>>(L, grid, VX_THREADS, 0, v, S, w.cand, w.col, w.cstate, w.first_app, w.mx, w.my, w.mg);
-
-        vx_launch<k_col_apply, k_col_apply_body>(L, grid, VX_THREADS, 0, v, S, w.cand, w.col, w.cstate, w.mx, w.my, w.mg);
-
+            vx_launch<k_col_settle<2>, k_col_settle_body<2>>(L, 1, 1024, 0, v, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec, w.mx, w.my, w.mg);
+        }
         vx_launch_compact_skip(L, p, v, S, w, &S->col_done);
-        vx_launch<k_col_end, k_col_end_body>(L, 1, 1, 0, S);
     }
     return cudaGetLastError();
 }

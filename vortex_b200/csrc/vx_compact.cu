@@ -14,17 +14,21 @@
 //        k live elements above e is the k-th hole, or m itself once all
 //        holes are filled,
 //      - otherwise the element that was at e+1.
-// Five launches: chunk counts, a single-block scan, per-chunk classification,
-// gather into scratch, scatter back.  Everything outside [0, n0) is untouched.
+// Four launches: chunk counts (whose last block scans them), per-chunk
+// classification, gather into scratch, scatter back.  Everything outside
+// [0, n0) is untouched.
 #include "vx_internal.cuh"
 
 __device__ __forceinline__ bool vx_live(const VxView &v, long long p, double eps) {
     return fabs(v.g[p * v.ps]) >= eps;
 }
 
-VX_DEVK void k_cmp_count_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, double eps, int *cnt, const int *skip) {
+// Live elements per chunk; the block that finishes last then scans the
+// chunk counts and finds m, scan[m] and H.
+VX_DEVK void k_cmp_count_body(VxBlkB<VX_THREADS, 0> vb, VxView v, VxScalars *S, double eps, int *cnt,
+                              long long *off, const int *skip) {
     if (skip && *skip) return;
-    __shared__ int sh[VX_THREADS];
+    __shared__ long long sh[VX_THREADS];
     const long long n0 = S->n;
     const long long nch = vx_ceil_div(n0, VX_CHUNK);
     for (long long c = vb.x; c < nch; c += vb.n) {
@@ -37,32 +41,21 @@ VX_DEVK void k_cmp_count_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, double ep
             if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
             __syncthreads();
         }
-        if (threadIdx.x == 0) cnt[c] = sh[0];
+        if (threadIdx.x == 0) cnt[c] = (int)sh[0];
         __syncthreads();
     }
-}
-__global__ void k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt, const int *skip) {
-    VX_PDL_WAIT();
-    k_cmp_count_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, eps, cnt, skip);
-}
-
-// Single block: exclusive scan of the chunk counts, m, scan[m] and H.
-VX_DEVK void k_cmp_scan_body(VxBlkB<1024, 0> vb, VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
-                             const int *skip) {
-    if (skip && *skip) return;
-    __shared__ long long sh[1024];
+    if (!vx_last_block(&S->sync_ctr, vb.n)) return;
+    // exclusive scan of the chunk counts, VX_THREADS at a time
     __shared__ long long carry;
-    const long long n0 = S->n;
-    const long long nch = vx_ceil_div(n0, VX_CHUNK);
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (long long base = 0; base < nch; base += blockDim.x) {
-        long long c = base + threadIdx.x;
-        long long val = c < nch ? cnt[c] : 0;
+        const long long c = base + threadIdx.x;
+        const long long val = c < nch ? __ldcg(&cnt[c]) : 0;
         sh[threadIdx.x] = val;
         __syncthreads();
         for (int o = 1; o < (int)blockDim.x; o <<= 1) {       // inclusive Hillis-Steele
-            long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+            const long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
             __syncthreads();
             sh[threadIdx.x] += t;
             __syncthreads();
@@ -74,19 +67,18 @@ VX_DEVK void k_cmp_scan_body(VxBlkB<1024, 0> vb, VxView v, VxScalars *S, double 
     }
     const long long m = carry;
     // live elements in [0, m)
-    __shared__ long long part[1024];
     long long scan_m = m;
     if (m < n0) {
         const long long cm = m / VX_CHUNK;
         long long k = 0;
         for (long long p = cm * VX_CHUNK + threadIdx.x; p < m; p += blockDim.x) k += vx_live(v, p, eps);
-        part[threadIdx.x] = k;
+        sh[threadIdx.x] = k;
         __syncthreads();
         for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
             __syncthreads();
         }
-        scan_m = off[cm] + part[0];
+        scan_m = off[cm] + sh[0];
     }
     if (threadIdx.x == 0) {
         S->c_n0 = n0;
@@ -95,10 +87,10 @@ VX_DEVK void k_cmp_scan_body(VxBlkB<1024, 0> vb, VxView v, VxScalars *S, double 
         S->c_H = m - scan_m;
     }
 }
-__global__ void __launch_bounds__(1024) k_cmp_scan(VxView v, VxScalars *S, double eps, const int *cnt, long long *off,
-                           const int *skip) {
+__global__ void __launch_bounds__(VX_THREADS) k_cmp_count(VxView v, VxScalars *S, double eps, int *cnt,
+                                                          long long *off, const int *skip) {
     VX_PDL_WAIT();
-    k_cmp_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, v, S, eps, cnt, off, skip);
+    k_cmp_count_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, v, S, eps, cnt, off, skip);
 }
 
 // Per chunk: local scan, then hole positions, hole sources and tail sources.
@@ -191,9 +183,12 @@ __global__ void k_cmp_gather(VxView v, const VxScalars *S, const int *hole_pos, 
     k_cmp_gather_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, hole_pos, hole_src, tail_src, hx, hy, hg, tx, ty, skip);
 }
 
+// count_step: this compaction closes a whole step, which it counts (no
+// kernel after it in the step reads the step index).
 VX_DEVK void k_cmp_scatter_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const int *hole_pos, const double *hx,
                                 const double *hy, const double *hg, const double *tx, const double *ty,
-                                const int *skip) {
+                                const int *skip, int count_step) {
+    if (count_step && vb.x == 0 && threadIdx.x == 0) S->step += 1;
     if (skip && *skip) return;
     const long long n0 = S->c_n0, m = S->c_m, H = S->c_H;
     if (m != n0) {
@@ -214,24 +209,23 @@ VX_DEVK void k_cmp_scatter_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const i
 }
 __global__ void k_cmp_scatter(VxView v, VxScalars *S, const int *hole_pos, const double *hx,
                               const double *hy, const double *hg, const double *tx, const double *ty,
-                              const int *skip) {
+                              const int *skip, int count_step) {
     VX_PDL_WAIT();
-    k_cmp_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, hole_pos, hx, hy, hg, tx, ty, skip);
+    k_cmp_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, hole_pos, hx, hy, hg, tx, ty, skip, count_step);
 }
 
 cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const VxView &v,
-                                   VxScalars *S, VxWork &w, const int *skip) {
+                                   VxScalars *S, VxWork &w, const int *skip, bool count_step) {
     const int grid = L.num_sms * 4;
-    vx_launch<k_cmp_count, k_cmp_count_body>(L, grid, VX_THREADS, 0, v, S, p.drop_eps, w.cmp_cnt, skip);
-    vx_launch<k_cmp_scan, k_cmp_scan_body>(L, 1, 1024, 0, v, S, p.drop_eps, w.cmp_cnt, w.cmp_off, skip);
+    vx_launch<k_cmp_count, k_cmp_count_body>(L, grid, VX_THREADS, 0, v, S, p.drop_eps, w.cmp_cnt, w.cmp_off, skip);
     vx_launch<k_cmp_classify, k_cmp_classify_body>(L, grid, VX_THREADS, 0, v, S, p.drop_eps, w.cmp_off, w.hole_pos, w.hole_src, w.tail_src, skip);
     vx_launch<k_cmp_gather, k_cmp_gather_body>(L, grid, VX_THREADS, 0, v, S, w.hole_pos, w.hole_src, w.tail_src, w.hx, w.hy, w.hg, w.tx, w.ty, skip);
-    vx_launch<k_cmp_scatter, k_cmp_scatter_body>(L, grid, VX_THREADS, 0, v, S, w.hole_pos, w.hx, w.hy, w.hg, w.tx, w.ty, skip);
+    vx_launch<k_cmp_scatter, k_cmp_scatter_body>(L, grid, VX_THREADS, 0, v, S, w.hole_pos, w.hx, w.hy, w.hg, w.tx, w.ty, skip, count_step ? 1 : 0);
 
     return cudaGetLastError();
 }
 
 cudaError_t vx_launch_compact(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                              VxWork &w) {
-    return vx_launch_compact_skip(L, p, v, S, w, nullptr);
+                              VxWork &w, bool count_step) {
+    return vx_launch_compact_skip(L, p, v, S, w, nullptr, count_step);
 }

@@ -180,6 +180,16 @@ static vx_status dalloc(std::vector<void *> *allocs, long long *bytes, T **p, lo
     return VX_OK;
 }
 
+// dalloc, then zeroed in stream order.
+template <typename T>
+static vx_status dalloc_zero(std::vector<void *> *allocs, long long *bytes, T **p, long long count,
+                             cudaStream_t stream) {
+    vx_status st = dalloc(allocs, bytes, p, count, stream);
+    if (st != VX_OK || !allocs) return st;
+    CU(cudaMemsetAsync(*p, 0, sizeof(T) * (size_t)(count < 1 ? 1 : count), stream));
+    return VX_OK;
+}
+
 void vx_work_free(VxWork &w, std::vector<void *> &allocs, cudaStream_t stream) {
     for (void *q : allocs) {
         if (stream)
@@ -205,11 +215,13 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.hole_pos, cap); A(w.hole_src, cap); A(w.tail_src, cap);
     A(w.hx, cap); A(w.hy, cap); A(w.hg, cap); A(w.tx, cap); A(w.ty, cap);
     w.cells_cap = std::max(4 * cap, 65536LL);
-    A(w.cellid, cap); A(w.cell_cnt, w.cells_cap); A(w.cell_start, w.cells_cap + 1); A(w.sorted, cap);
+    A(w.cellid, cap); A(w.cell_start, w.cells_cap + 1); A(w.sorted, cap);
+    // the collapse grid's cell counts are zero between passes (the scatter
+    // that consumes them counts them back down), so they start at zero
+    if ((st = dalloc_zero(allocs, &w.bytes, &w.cell_cnt, w.cells_cap, stream)) != VX_OK) return st;
     A(w.col, cap); A(w.in_cnt, cap); A(w.has_app, cap); A(w.first_app, cap);
     A(w.cand, cap); A(w.cstate, cap); A(w.cdec, cap);
     A(w.mx, cap); A(w.my, cap); A(w.mg, cap);
-    A(w.cell_chunk_cnt, w.cells_cap / VX_CHUNK + 2); A(w.cell_chunk_off, w.cells_cap / VX_CHUNK + 2);
     // pair partials: K * n <= num_sms*8*tile + n for the split K the launchers pick
     w.part_cap = 5LL * ((long long)num_sms * 8 * 1024 + cap + 1024);
     A(w.part, w.part_cap);
@@ -219,15 +231,17 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.R, P32); A(w.gamma, P32);
     A(w.bf_part, 2LL * VX_BF_P * VX_BF_MAX_BLOCKS); A(w.bf_cnt, VX_BF_MAX_BLOCKS);
     A(w.bf_off, VX_BF_MAX_BLOCKS + 1); A(w.bf_near, cap); A(w.bf_coef, 2 * VX_BF_P);
-    A(w.red, VX_RED_BLOCKS * 4);
+    A(w.red, VX_RED_BLOCKS * 4); A(w.box, VX_RED_BLOCKS * 4);
     // neighbour-list grid of the bulk form
     A(w.key0, cap); A(w.key1, cap); A(w.val0, cap); A(w.val1, cap);
-    A(w.cg_cnt, w.cells_cap); A(w.cg_start, w.cells_cap + 1);
+    A(w.cg_start, w.cells_cap + 1);
+    // the diffusion grid's cell counts are zero between steps (its bucket
+    // order leaves them so), so they start at zero
+    if ((st = dalloc_zero(allocs, &w.bytes, &w.cg_cnt, w.cells_cap, stream)) != VX_OK) return st;
     A(w.srt, cap);
     w.items_cap = cap / 32 + w.cells_cap + 2;
     A(w.items, w.items_cap);
     A(w.cg_wide, cap); A(w.cg_huge, cap); A(w.bk_mid, cap / 16 + 2); A(w.bk_big, cap / 128 + 2);
-    A(w.row_items, w.cells_cap + 1); A(w.row_item_off, w.cells_cap + 1);
     // quadtree of the bulk-form Biot-Savart
     w.fmm_lmax = vx_fmm_max_level(cap);
     A(w.fmm_cnt, vx_fmm_cells(w.fmm_lmax));
@@ -237,6 +251,9 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.fmm_sub_start, (1LL << (2 * (w.fmm_lmax + 1))) + 1);
     A(w.fmm_M, 2LL * fmm_p * vx_fmm_cells(w.fmm_lmax));
     A(w.fmm_L, 2LL * fmm_p * vx_fmm_cells(w.fmm_lmax));
+    // the longest scan: cells of a grid, quarter-leaves, or rows at one per thread
+    w.scan_tiles_cap = std::max(std::max(w.cells_cap, 1LL << (2 * (w.fmm_lmax + 1))), cap) / VX_SCAN_T + 2;
+    if ((st = dalloc_zero(allocs, &w.bytes, &w.scan_tiles, w.scan_tiles_cap, stream)) != VX_OK) return st;
 #undef A
     return VX_OK;
 }
@@ -321,44 +338,22 @@ static vx_status ensure_capacity(vx_sim *s) {
     return grow(s, need_for(s, s->n_upper));
 }
 
-// Source chunks of the birth right-hand side: enough (panel tile, chunk)
-// items for every SM to hold several blocks, within the partial-sum buffer
-// (at most num_sms * 4 chunks).
-// The launch shapes below follow the host's upper bound of the source count
+// Launch shapes of a step follow the host's upper bound of the source count
 // rounded up to a power of two, so that they (and the step graph holding
-// them) change only when that bound crosses one, not every few steps.
-static long long pow2_ceil(long long n) {
-    long long q = 1;
-    while (q < n) q <<= 1;
-    return q;
-}
-
-static int rhs_chunks_for(vx_sim *s) {
-    const int tiles = (s->P + 127) / 128;
-    long long want = std::max(1LL, (long long)s->num_sms * 16 / tiles);
-    want = std::min<long long>(want, (long long)s->num_sms * 4);
-    long long bysrc = std::max(1LL, vx_ceil_div(pow2_ceil(s->n_upper), 1024));
-    return (int)std::min(want, bysrc);
-}
+// them) change only when that bound crosses one, not every few steps.  They
+// are grids only: the partitions that fix summation orders are derived on
+// the device from the body's own count.
+static int rhs_chunks_for(vx_sim *s) { return vx_rhs_chunks(s->n_upper, s->P, s->num_sms); }
 
 // SMs a step's grid-stride launches are sized for: one per 2048 sources of
 // the rounded bound, at least 4, at most the device's.
-static int step_sms_for(vx_sim *s) {
-    const long long q = pow2_ceil(s->n_upper + s->P) / 2048;
-    return (int)std::max(4LL, std::min((long long)s->num_sms, q));
-}
-
-static int kv_for(vx_sim *s) {
-    const int tile = s->prm.prec == VX_PREC_FP32 ? 1024 : 512;
-    return vx_pick_ksplit(pow2_ceil(s->n_upper + s->P), tile, s->num_sms);
-}
+static int step_sms_for(vx_sim *s) { return vx_body_sms(s->n_upper + s->P, s->num_sms); }
 
 VxLaunch vx_sim_launch(vx_sim *s) { return launch_of(s); }
 long long vx_sim_need(vx_sim *s, long long n) { return need_for(s, n); }
 vx_status vx_sim_grow(vx_sim *s, long long need) { return grow(s, need); }
 vx_status vx_sim_read_scalars(vx_sim *s) { return read_scalars(s); }
 int vx_sim_step_sms(vx_sim *s) { return step_sms_for(s); }
-int vx_sim_kv(vx_sim *s) { return kv_for(s); }
 int vx_sim_rhs_chunks(vx_sim *s) { return rhs_chunks_for(s); }
 
 // ---------------------------------------------------------------------------
@@ -840,7 +835,6 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step, VxRe
                                  int share = 0) {
     VxLaunch L = launch_of(s);
     L.num_sms = step_sms_for(s);
-    L.part_sms = L.num_sms;     // result-defining partitions: the body's own size
     if (share > 0) L.num_sms = std::min(share, L.num_sms);
     L.full_sms = s->num_sms;
     L.rec = rec;
@@ -849,7 +843,6 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step, VxRe
     VxView v = view_of(s);
     const VxParams &p = s->prm;
     cudaError_t e = cudaSuccess;
-    const int kv = kv_for(s);
     const bool timed = s->timing && !whole_step && !rec;
     if (timed)
         for (int k = 0; k < 4; ++k) L.pair_ev[k] = s->pev[k];
@@ -865,12 +858,12 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step, VxRe
         if (p.prec == VX_PREC_FP32 && s->conf.fmm)
             e = vx_launch_velocity_fmm(L, p, v, s->d_S, s->w);
         else
-            e = vx_launch_velocity(L, p, v, s->d_S, s->w, kv);
+            e = vx_launch_velocity(L, p, v, s->d_S, s->w);
         if (e != cudaSuccess) return e;
     }
     ev(2);
     if (mask & VX_STAGE_DIFFUSION)
-        if ((e = vx_launch_diffusion(L, p, v, s->d_S, s->w, kv)) != cudaSuccess) return e;
+        if ((e = vx_launch_diffusion(L, p, v, s->d_S, s->w)) != cudaSuccess) return e;
     ev(3);
     if (mask & VX_STAGE_WALL)
         if ((e = vx_launch_wall(L, p, v, s->d_S, s->d_pan, s->d_wstart, s->d_widx)) != cudaSuccess) return e;
@@ -878,12 +871,14 @@ static cudaError_t launch_stages(vx_sim *s, unsigned mask, bool whole_step, VxRe
     if (mask & VX_STAGE_ADVECT)
         if ((e = vx_launch_advect(L, p, v, s->d_S, s->w, s->d_pan, s->d_hstart, s->d_hidx)) != cudaSuccess) return e;
     if (mask & VX_STAGE_COMPACT)
-        if ((e = vx_launch_compact(L, p, v, s->d_S, s->w)) != cudaSuccess) return e;
+        if ((e = vx_launch_compact(L, p, v, s->d_S, s->w, whole_step)) != cudaSuccess) return e;
     if (mask & VX_STAGE_COLLAPSE1)
         if ((e = vx_launch_collapse(L, p, v, s->d_S, s->w, 1, (int)s->conf.n_col)) != cudaSuccess) return e;
     if (mask & VX_STAGE_COLLAPSE2)
         if ((e = vx_launch_collapse(L, p, v, s->d_S, s->w, 2, (int)s->conf.n_col)) != cudaSuccess) return e;
-    if (whole_step) e = vx_launch_step_end(L, s->d_S);
+    // a whole step is counted by its main compaction (no kernel after it
+    // reads the step index), else by a kernel of its own
+    if (whole_step && !(mask & VX_STAGE_COMPACT)) e = vx_launch_step_end(L, s->d_S);
     ev(5);
     return e;
 }
@@ -918,10 +913,10 @@ static vx_status step_once(vx_sim *s) {
         s->n_upper += s->P;
         return VX_OK;
     }
-    const int kv = kv_for(s), rc = rhs_chunks_for(s), sms = step_sms_for(s);
+    const int rc = rhs_chunks_for(s), sms = step_sms_for(s);
     vx_sim::StepGraph *sg = nullptr;
     for (auto &g : s->graphs)
-        if (g.exec && g.kv == kv && g.rhs == rc && g.sms == sms) sg = &g;
+        if (g.exec && g.rhs == rc && g.sms == sms) sg = &g;
     if (!sg) {
         sg = &s->graphs[0];
         for (auto &g : s->graphs)
@@ -946,7 +941,6 @@ static vx_status step_once(vx_sim *s) {
             vx_set_error("graph instantiate: %s", cudaGetErrorString(e));
             return VX_ERR_CUDA;
         }
-        sg->kv = kv;
         sg->rhs = rc;
         sg->sms = sms;
     }
@@ -1195,7 +1189,7 @@ extern "C" vx_status vx_probe(vx_sim *s, const double *px, const double *py, int
     CU(cudaMemcpyAsync(dpx, px, sizeof(double) * np, cudaMemcpyHostToDevice, s->stream));
     CU(cudaMemcpyAsync(dpy, py, sizeof(double) * np, cudaMemcpyHostToDevice, s->stream));
     const int tile = s->prm.prec == VX_PREC_FP32 ? 1024 : 512;
-    const int K = vx_pick_ksplit(np, tile, s->num_sms);
+    const int K = vx_ksplit(np, tile, s->num_sms);
     CU(vx_launch_probe(launch_of(s), s->prm, view_of(s), s->d_S, s->w, dpx, dpy, 1, np, dvx, dvy, 1, K));
     CU(cudaMemcpyAsync(ovx, dvx, sizeof(double) * np, cudaMemcpyDeviceToHost, s->stream));
     CU(cudaMemcpyAsync(ovy, dvy, sizeof(double) * np, cudaMemcpyDeviceToHost, s->stream));

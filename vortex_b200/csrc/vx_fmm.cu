@@ -62,20 +62,20 @@ __constant__ double c_fmm_inv[FMM_PMAX + 1] = {0.0,      1.0,      1.0 / 2,  1.0
 extern __shared__ __align__(16) unsigned char vx_fmm_dyn[];
 
 // ---------------------------------------------------------------------------
-VX_DEVK void k_fmm_begin_body(VxBlkB<0, 0> vb, VxScalars *S) {
-    S->fb[0] = S->fb[1] = S->fb[2] = S->fb[3] = ~0ull;
-    S->fnflag = 0;
-    S->fnbrute = 0;
-    S->bk_nmid = S->bk_nbig = 0;
-}
-__global__ void k_fmm_begin(VxScalars *S) {
-    VX_PDL_WAIT();
-    k_fmm_begin_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S);
-}
-
-VX_DEVK void k_fmm_bbox_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S) {
+// Start of the velocity stage, one launch: the count arrays zeroed to their
+// capacity, the bounding box (per-block keys into part[], combined by the
+// last block), then, in the last block, the stage's counters and the tree:
+// square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], reduced until
+// the leaf side is at least eps.
+VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S, double eps, int Lmax, int leaf, int *cnt,
+                             long long ncnt, int *subcnt, long long nsub, unsigned long long *part) {
     __shared__ unsigned long long sk[4][FMM_T];
     const long long n = S->n;
+    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < ncnt + nsub;
+         c += (long long)vb.n * blockDim.x) {
+        if (c < ncnt) cnt[c] = 0;
+        else subcnt[c - ncnt] = 0;
+    }
     unsigned long long k[4] = {~0ull, ~0ull, ~0ull, ~0ull};
     for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)vb.n * blockDim.x) {
@@ -90,20 +90,24 @@ VX_DEVK void k_fmm_bbox_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S) {
             for (int q = 0; q < 4; ++q) sk[q][threadIdx.x] = min(sk[q][threadIdx.x], sk[q][threadIdx.x + o]);
         __syncthreads();
     }
-    if (threadIdx.x == 0)
-        for (int q = 0; q < 4; ++q) atomicMin(&S->fb[q], sk[q][0]);
-}
-__global__ void __launch_bounds__(FMM_T) k_fmm_bbox(VxView v, VxScalars *S) {
-    VX_PDL_WAIT();
-    k_fmm_bbox_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, v, S);
-}
-
-// Square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], reduced until
-// the leaf side is at least eps.
-VX_DEVK void k_fmm_params_body(VxBlkB<0, 0> vb, VxScalars *S, double eps, int Lmax, int leaf) {
-    const long long n = S->n;
-    const double x0 = vx_dunkey(S->fb[0]), x1 = -vx_dunkey(S->fb[1]);
-    const double y0 = vx_dunkey(S->fb[2]), y1 = -vx_dunkey(S->fb[3]);
+    if (threadIdx.x < 4) part[4 * vb.x + threadIdx.x] = sk[threadIdx.x][0];
+    if (!vx_last_block(&S->sync_ctr, vb.n)) return;
+    for (int q = 0; q < 4; ++q) k[q] = ~0ull;
+    for (unsigned b = threadIdx.x; b < vb.n; b += blockDim.x)
+        for (int q = 0; q < 4; ++q) k[q] = min(k[q], __ldcg(&part[4 * b + q]));
+    for (int q = 0; q < 4; ++q) sk[q][threadIdx.x] = k[q];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int q = 0; q < 4; ++q) sk[q][threadIdx.x] = min(sk[q][threadIdx.x], sk[q][threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    S->fnflag = 0;
+    S->fnbrute = 0;
+    S->bk_nmid = S->bk_nbig = 0;
+    const double x0 = vx_dunkey(sk[0][0]), x1 = -vx_dunkey(sk[1][0]);
+    const double y0 = vx_dunkey(sk[2][0]), y1 = -vx_dunkey(sk[3][0]);
     double side = fmax(x1 - x0, y1 - y0);
     side = side * (1.0 + 1e-9) + 1e-12;
     int L = 2;
@@ -120,22 +124,11 @@ VX_DEVK void k_fmm_params_body(VxBlkB<0, 0> vb, VxScalars *S, double eps, int Lm
     S->fnsub = 4 * S->fnleaves;
     S->fs = vx_round32(n);   // sources include the round-32 padding (3-nearest)
 }
-__global__ void k_fmm_params(VxScalars *S, double eps, int Lmax, int leaf) {
+__global__ void __launch_bounds__(FMM_T) k_fmm_prep(VxView v, VxScalars *S, double eps, int Lmax, int leaf, int *cnt,
+                                                    long long ncnt, int *subcnt, long long nsub,
+                                                    unsigned long long *part) {
     VX_PDL_WAIT();
-    k_fmm_params_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, eps, Lmax, leaf);
-}
-
-VX_DEVK void k_fmm_zero_cnt_body(VxBlkB<0, 0> vb, const VxScalars *S, int *cnt, int *subcnt) {
-    const long long tot = fmm_level_off(S->fL + 1), nsub = S->fnsub;
-    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c < tot + nsub;
-         c += (long long)vb.n * blockDim.x) {
-        if (c < tot) cnt[c] = 0;
-        else subcnt[c - tot] = 0;
-    }
-}
-__global__ void k_fmm_zero_cnt(const VxScalars *S, int *cnt, int *subcnt) {
-    VX_PDL_WAIT();
-    k_fmm_zero_cnt_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cnt, subcnt);
+    k_fmm_prep_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, v, S, eps, Lmax, leaf, cnt, ncnt, subcnt, nsub, part);
 }
 
 __device__ __forceinline__ long long fmm_leaf(const VxScalars *S, double x, double y) {
@@ -177,197 +170,39 @@ __global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *v
     k_fmm_leafid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, key, val, subcnt);
 }
 
-// Leaf counts (the tree's leaf level) and leaf starts from the quarters'.
-VX_DEVK void k_fmm_leaf_from_sub_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *subcnt, const int *substart,
-                                      int *cnt, int *start) {
-    const long long nl = S->fnleaves;
+// Starts of the quarters (one-pass scan of their counts), and with them the
+// leaf counts (the tree's leaf level: the sum of a leaf's four quarters) and
+// the leaf starts (its first quarter's); both end with the sources' total.
+VX_DEVK void k_fmm_scan_body(VxBlkB<VX_SCAN_T, 0> vb, VxScalars *S, const int *subcnt, int *substart, int *cnt,
+                             int *start, unsigned long long *tiles) {
+    constexpr int PER = VX_CHUNK / VX_SCAN_T;   // a multiple of 4: a thread holds whole leaves
+    const long long len = S->fnsub, nl = S->fnleaves;
     int *leafcnt = cnt + fmm_level_off(S->fL);
-    for (long long c = vb.x * (long long)blockDim.x + threadIdx.x; c <= nl; c += (long long)vb.n * blockDim.x) {
-        if (c == nl) {
-            start[nl] = substart[4 * nl];
-            continue;
-        }
-        leafcnt[c] = subcnt[4 * c] + subcnt[4 * c + 1] + subcnt[4 * c + 2] + subcnt[4 * c + 3];
-        start[c] = substart[4 * c];
-    }
-}
-__global__ void k_fmm_leaf_from_sub(const VxScalars *S, const int *subcnt, const int *substart, int *cnt,
-                                    int *start) {
-    VX_PDL_WAIT();
-    k_fmm_leaf_from_sub_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, subcnt, substart, cnt, start);
-}
-
-// Starts of the quarters: exclusive scan of their counts (chunked, device
-// length).
-VX_DEVK void k_fmm_scan_sum_body(VxBlkB<FMM_T, 0> vb, const VxScalars *S, const int *cnt, int *csum) {
-    __shared__ int sh[FMM_T];
-    const long long len = S->fnsub, nch = vx_ceil_div(len, VX_CHUNK);
-    const int *c0 = cnt;
-    for (long long c = vb.x; c < nch; c += vb.n) {
-        int k = 0;
-        for (long long q = c * VX_CHUNK + threadIdx.x; q < min(len, (c + 1) * VX_CHUNK); q += blockDim.x) k += c0[q];
-        sh[threadIdx.x] = k;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) csum[c] = sh[0];
-        __syncthreads();
-    }
-}
-__global__ void __launch_bounds__(FMM_T) k_fmm_scan_sum(const VxScalars *S, const int *cnt, int *csum) {
-    VX_PDL_WAIT();
-    k_fmm_scan_sum_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, S, cnt, csum);
-}
-
-VX_DEVK void k_fmm_scan_top_body(VxBlkB<1024, 0> vb, const VxScalars *S, const int *csum, long long *coff) {
-    __shared__ long long sh[1024];
-    __shared__ long long carry;
-    const long long nch = vx_ceil_div(S->fnsub, VX_CHUNK);
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (long long base = 0; base < nch; base += blockDim.x) {
-        const long long c = base + threadIdx.x;
-        const long long val = c < nch ? csum[c] : 0;
-        sh[threadIdx.x] = val;
-        __syncthreads();
-        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-            long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (c < nch) coff[c] = carry + sh[threadIdx.x] - val;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry += sh[threadIdx.x];
-        __syncthreads();
-    }
-}
-__global__ void __launch_bounds__(1024) k_fmm_scan_top(const VxScalars *S, const int *csum, long long *coff) {
-    VX_PDL_WAIT();
-    k_fmm_scan_top_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, csum, coff);
-}
-
-VX_DEVK void k_fmm_scan_apply_body(VxBlkB<FMM_T, 0> vb, const VxScalars *S, const int *cnt, const long long *coff,
-                                   int *start) {
-    constexpr int PER = VX_CHUNK / FMM_T;
-    __shared__ int sh[FMM_T];
-    const long long len = S->fnsub, nch = vx_ceil_div(len, VX_CHUNK);
-    const int *c0 = cnt;
-    if (vb.x == 0 && threadIdx.x == 0) start[len] = (int)S->fs;
-    for (long long c = vb.x; c < nch; c += vb.n) {
-        const long long b = c * VX_CHUNK + (long long)threadIdx.x * PER;
-        int val[PER], loc = 0;
+    vx_scan_lookback<PER>(
+        vb.n, len, S, tiles, [&](long long i) { return subcnt[i]; },
+        [&](long long i0, const unsigned *val, long long run) {
 #pragma unroll
-        for (int q = 0; q < PER; ++q) { val[q] = (b + q < len) ? c0[b + q] : 0; loc += val[q]; }
-        sh[threadIdx.x] = loc;
-        __syncthreads();
-        for (int o = 1; o < FMM_T; o <<= 1) {
-            int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        long long run = coff[c] + sh[threadIdx.x] - loc;
-        __syncthreads();
+            for (int q = 0; q < PER; q += 4) {
+                if (i0 + q >= len) break;
+                const long long leaf = (i0 + q) >> 2;
+                leafcnt[leaf] = (int)(val[q] + val[q + 1] + val[q + 2] + val[q + 3]);
+                start[leaf] = (int)run;
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            if (b + q < len) start[b + q] = (int)run;
-            run += val[q];
-        }
-    }
-}
-__global__ void __launch_bounds__(FMM_T) k_fmm_scan_apply(const VxScalars *S, const int *cnt, const long long *coff,
-                                                          int *start) {
-    VX_PDL_WAIT();
-    k_fmm_scan_apply_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, S, cnt, coff, start);
-}
-
-// Leaf-sorted sources: position relative to the leaf centre (FP32 keeps the
-// local spacing accurate), G masked beyond n, leaf column.
-VX_DEVK void k_fmm_gather_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
-    const long long s = S->fs, n = S->n;
-    const unsigned m = 1u << S->fL;
-    const double h = S->fside / (double)m;
-    for (long long k = vb.x * (long long)blockDim.x + threadIdx.x; k < s;
-         k += (long long)vb.n * blockDim.x) {
-        const long long j = sorted[k];
-        const unsigned leaf = skey[k] >> 2, col = leaf % m, row = leaf / m;
-        const double ccx = S->fx0 + ((double)col + 0.5) * h, ccy = S->fy0 + ((double)row + 0.5) * h;
-        srt[k] = make_float4((float)(v.x[j * v.ps] - ccx), (float)(v.y[j * v.ps] - ccy),
-                             j < n ? (float)v.g[j * v.ps] : 0.0f, (float)col);
-    }
-}
-__global__ void k_fmm_gather(VxView v, const VxScalars *S, const int *sorted, const unsigned *skey, float4 *srt) {
-    VX_PDL_WAIT();
-    k_fmm_gather_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, sorted, skey, srt);
-}
-
-// P2M at the leaves, one warp per leaf: each lane expands its own vortices
-// (FP64 positions), then a fixed butterfly sums the lanes.  Empty leaves are
-// not written (nothing reads their expansion).
-template <int P>
-VX_DEVK void k_fmm_p2m_body(VxBlkB<128, 0> vb, VxView v, const VxScalars *S, const int *start, const int *sorted,
-                            cplx *M) {
-    const int L = S->fL;
-    const long long m = 1LL << L, nl = m * m, n = S->n;
-    const double h = S->fside / (double)m;
-    cplx *ML = M + fmm_level_off(L) * P;
-    const int lane = threadIdx.x & 31;
-    const long long nw = ((long long)vb.n * blockDim.x) >> 5;
-    for (long long c = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5; c < nl; c += nw) {
-        const int j0 = start[c], j1 = start[c + 1];
-        if (j0 == j1) continue;
-        cplx b[P];
-#pragma unroll
-        for (int k = 0; k < P; ++k) b[k] = {0.0, 0.0};
-        const double cx = S->fx0 + ((double)(c % m) + 0.5) * h, cy = S->fy0 + ((double)(c / m) + 0.5) * h;
-        for (int q = j0 + lane; q < j1; q += 32) {
-            const long long j = sorted[q];
-            if (j >= n) continue;
-            const double gj = v.g[j * v.ps];
-            const cplx w = {(v.x[j * v.ps] - cx) / h, (v.y[j * v.ps] - cy) / h};
-            cplx pw = {gj, 0.0};   // G w^k / k!
-#pragma unroll
-            for (int k = 0; k < P; ++k) {
-                b[k] = cadd(b[k], pw);
-                pw = cscale(cmul(pw, w), c_fmm_inv[k + 1]);
-            }
-        }
-        // reduce-scatter over the warp: at each halving the lane keeps the half
-        // of its values selected by its lane bit and adds the partner's copy of
-        // it (31 shuffles instead of 160 for an all-reduce of 32 values);
-        // afterwards lane q holds value q = coefficient q/2, part q&1
-        // (in groups of 16 coefficients, the last one padded with zeros)
-#pragma unroll
-        for (int g0 = 0; g0 < P; g0 += 16) {
-            double vv[32];
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const int kk = min(g0 + k, P - 1);
-                vv[2 * k] = g0 + k < P ? b[kk].r : 0.0;
-                vv[2 * k + 1] = g0 + k < P ? b[kk].i : 0.0;
-            }
-#pragma unroll
-            for (int half = 16; half > 0; half >>= 1) {
-                const bool up = (lane & half) != 0;
-#pragma unroll
-                for (int i = 0; i < half; ++i) {
-                    const double send = up ? vv[i] : vv[i + half];
-                    const double keep = up ? vv[i + half] : vv[i];
-                    vv[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+                for (int e = 0; e < 4; ++e) {
+                    substart[i0 + q + e] = (int)run;
+                    run += val[q + e];
                 }
             }
-            if (g0 + (lane >> 1) < P) reinterpret_cast<double *>(ML + c * P)[2 * g0 + lane] = vv[0];
-        }
-    }
+        },
+        [&](long long) {
+            substart[len] = (int)S->fs;
+            start[nl] = (int)S->fs;
+        });
 }
-template <int P>
-__global__ void __launch_bounds__(128) k_fmm_p2m(VxView v, const VxScalars *S, const int *start, const int *sorted,
-                                                 cplx *M) {
+__global__ void __launch_bounds__(VX_SCAN_T) k_fmm_scan(VxScalars *S, const int *subcnt, int *substart, int *cnt,
+                                                        int *start, unsigned long long *tiles) {
     VX_PDL_WAIT();
-    k_fmm_p2m_body<P>(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, v, S, start, sorted, M);
+    k_fmm_scan_body(VxBlkB<VX_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, subcnt, substart, cnt, start, tiles);
 }
 
 // Shift table shared by M2M and L2L, built per block in shared memory:
@@ -383,48 +218,164 @@ __device__ __forceinline__ void fmm_shift_table(cplx (*se)[P]) {
     }
 }
 
-// M2M: parent at level l from its 4 children at level l+1, one thread per
-// (parent, coefficient k); the thread of coefficient 0 also writes the
-// parent's vortex count (the sum of its children's).
+// P2M of leaf c (level L, m leaves a side), by one warp: each lane expands
+// its own vortices (FP64 positions), then a fixed butterfly sums the lanes.
+// An empty leaf is not written (nothing reads its expansion).
 template <int P>
-VX_DEVK void k_fmm_m2m_body(VxBlkB<128, 0> vb, const VxScalars *S, int *cnt, cplx *M, int l) {
-    __shared__ cplx se[4][P];
-    if (l + 1 > S->fL) return;
-    fmm_shift_table<P>(se);
-    __syncthreads();
+__device__ __forceinline__ void fmm_p2m_leaf(const VxView &v, const VxScalars *S, const int *start,
+                                             const int *sorted, cplx *ML, long long c, long long m, int lane) {
+    const int j0 = start[c], j1 = start[c + 1];
+    if (j0 == j1) return;
+    const long long n = S->n;
+    const double h = S->fside / (double)m;
+    cplx b[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k) b[k] = {0.0, 0.0};
+    const double cx = S->fx0 + ((double)(c % m) + 0.5) * h, cy = S->fy0 + ((double)(c / m) + 0.5) * h;
+    for (int q = j0 + lane; q < j1; q += 32) {
+        const long long j = sorted[q];
+        if (j >= n) continue;
+        const double gj = v.g[j * v.ps];
+        const cplx w = {(v.x[j * v.ps] - cx) / h, (v.y[j * v.ps] - cy) / h};
+        cplx pw = {gj, 0.0};   // G w^k / k!
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            b[k] = cadd(b[k], pw);
+            pw = cscale(cmul(pw, w), c_fmm_inv[k + 1]);
+        }
+    }
+    // reduce-scatter over the warp: at each halving the lane keeps the half
+    // of its values selected by its lane bit and adds the partner's copy of
+    // it (31 shuffles instead of 160 for an all-reduce of 32 values);
+    // afterwards lane q holds value q = coefficient q/2, part q&1
+    // (in groups of 16 coefficients, the last one padded with zeros)
+#pragma unroll
+    for (int g0 = 0; g0 < P; g0 += 16) {
+        double vv[32];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int kk = min(g0 + k, P - 1);
+            vv[2 * k] = g0 + k < P ? b[kk].r : 0.0;
+            vv[2 * k + 1] = g0 + k < P ? b[kk].i : 0.0;
+        }
+#pragma unroll
+        for (int half = 16; half > 0; half >>= 1) {
+            const bool up = (lane & half) != 0;
+#pragma unroll
+            for (int i = 0; i < half; ++i) {
+                const double send = up ? vv[i] : vv[i + half];
+                const double keep = up ? vv[i + half] : vv[i];
+                vv[i] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+            }
+        }
+        if (g0 + (lane >> 1) < P) reinterpret_cast<double *>(ML + c * P)[2 * g0 + lane] = vv[0];
+    }
+}
+
+// M2M of coefficient k of cell c of level l from its 4 children at level
+// l+1; the thread of coefficient 0 also writes the cell's vortex count (the
+// sum of its children's).  Children are read through L2: in the fused
+// upward kernels another block of the same launch may have written them.
+template <int P>
+__device__ __forceinline__ void fmm_m2m_cell(const cplx (*se)[P], int *cnt, cplx *M, int l, long long c, int k) {
     const long long m = 1LL << l, m2 = 2 * m;
     cplx *Mp = M + fmm_level_off(l) * P;
     const cplx *Mc = M + fmm_level_off(l + 1) * P;
     int *cp = cnt + fmm_level_off(l);
     const int *cc = cnt + fmm_level_off(l + 1);
-    const long long tot = m * m * P;
-    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < tot;
-         e += (long long)vb.n * blockDim.x) {
-        const long long c = e / P;
-        const int k = (int)(e % P);
-        const long long ix = c % m, iy = c / m;
-        const int np = cc[(2 * iy) * m2 + 2 * ix] + cc[(2 * iy) * m2 + 2 * ix + 1] +
-                       cc[(2 * iy + 1) * m2 + 2 * ix] + cc[(2 * iy + 1) * m2 + 2 * ix + 1];
-        if (k == 0) cp[c] = np;
-        cplx b = {0.0, 0.0};
-        if (np > 0) {
-            for (int q = 0; q < 4; ++q) {
-                const long long child = (2 * iy + (q >> 1)) * m2 + 2 * ix + (q & 1);
-                if (cc[child] == 0) continue;
-                double sc = 1.0;   // 2^-mm
-                for (int mm = 0; mm <= k; ++mm) {
-                    b = cadd(b, cscale(cmul(se[q][k - mm], Mc[child * P + mm]), sc));
-                    sc *= 0.5;
-                }
+    const long long ix = c % m, iy = c / m;
+    int nq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) nq[q] = __ldcg(&cc[(2 * iy + (q >> 1)) * m2 + 2 * ix + (q & 1)]);
+    const int np = nq[0] + nq[1] + nq[2] + nq[3];
+    if (k == 0) cp[c] = np;
+    cplx b = {0.0, 0.0};
+    if (np > 0) {
+        for (int q = 0; q < 4; ++q) {
+            const long long child = (2 * iy + (q >> 1)) * m2 + 2 * ix + (q & 1);
+            if (nq[q] == 0) continue;
+            double sc = 1.0;   // 2^-mm
+            for (int mm = 0; mm <= k; ++mm) {
+                const double2 t = __ldcg(reinterpret_cast<const double2 *>(&Mc[child * P + mm]));
+                b = cadd(b, cscale(cmul(se[q][k - mm], cplx{t.x, t.y}), sc));
+                sc *= 0.5;
             }
         }
-        Mp[e] = b;
+    }
+    Mp[c * P + k] = b;
+}
+
+// M2M of levels hi-1 down to lo inside the subtree of cell r of level lo (one
+// block; a barrier between levels).
+template <int P>
+__device__ __forceinline__ void fmm_m2m_subtree(const cplx (*se)[P], int *cnt, cplx *M, int lo, int hi, long long r) {
+    const long long mlo = 1LL << lo, rx = r % mlo, ry = r / mlo;
+    for (int l = hi - 1; l >= lo; --l) {
+        const long long sl = 1LL << (l - lo), m = 1LL << l;
+        for (long long e = threadIdx.x; e < sl * sl * P; e += blockDim.x) {
+            const long long q = e / P;
+            const long long c = (ry * sl + q / sl) * m + rx * sl + q % sl;
+            fmm_m2m_cell<P>(se, cnt, M, l, c, (int)(e % P));
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int FMM_UP = 3;   // levels of the upward pass per fused launch
+constexpr int FMM_TOP = 3;  // levels below this one are left to the last block of the upward pass
+
+// Upward pass, first part: a block takes a cell r of level lo = max(L - 3, 0),
+// computes P2M at the leaves of its subtree (one warp per leaf), then M2M of
+// the 3 levels above them.
+template <int P>
+VX_DEVK void k_fmm_up_body(VxBlkB<128, 0> vb, VxView v, const VxScalars *S, const int *start, const int *sorted,
+                           int *cnt, cplx *M) {
+    __shared__ cplx se[4][P];
+    const int L = S->fL;
+    const int lo = max(L - FMM_UP, 0);
+    const long long m = 1LL << L, mlo = 1LL << lo, sl = 1LL << (L - lo);
+    cplx *ML = M + fmm_level_off(L) * P;
+    fmm_shift_table<P>(se);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (long long r = vb.x; r < mlo * mlo; r += vb.n) {
+        const long long rx = r % mlo, ry = r / mlo;
+        for (long long q = warp; q < sl * sl; q += nw)
+            fmm_p2m_leaf<P>(v, S, start, sorted, ML, (ry * sl + q / sl) * m + rx * sl + q % sl, m, lane);
+        __syncthreads();
+        fmm_m2m_subtree<P>(se, cnt, M, lo, L, r);
     }
 }
 template <int P>
-__global__ void __launch_bounds__(128) k_fmm_m2m(const VxScalars *S, int *cnt, cplx *M, int l) {
+__global__ void __launch_bounds__(128) k_fmm_up(VxView v, const VxScalars *S, const int *start, const int *sorted,
+                                                int *cnt, cplx *M) {
     VX_PDL_WAIT();
-    k_fmm_m2m_body<P>(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, S, cnt, M, l);
+    k_fmm_up_body<P>(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, v, S, start, sorted, cnt, M);
+}
+
+// Upward pass, the rest: M2M of the levels from L - 4 up to 3 by subtrees
+// as above (a block per cell of level 3), then the block that finishes last
+// runs levels 2, 1 and 0.
+template <int P>
+VX_DEVK void k_fmm_up_top_body(VxBlkB<128, 0> vb, VxScalars *S, int *cnt, cplx *M) {
+    __shared__ cplx se[4][P];
+    const int hi = max(S->fL - FMM_UP, 0);
+    const int lo = min(FMM_TOP, hi);
+    if (hi == 0) return;
+    fmm_shift_table<P>(se);
+    __syncthreads();
+    for (long long r = vb.x; r < (1LL << (2 * lo)); r += vb.n) fmm_m2m_subtree<P>(se, cnt, M, lo, hi, r);
+    if (lo == 0 || !vx_last_block(&S->sync_ctr, vb.n)) return;
+    for (int l = lo - 1; l >= 0; --l) {
+        for (long long e = threadIdx.x; e < (1LL << (2 * l)) * P; e += blockDim.x)
+            fmm_m2m_cell<P>(se, cnt, M, l, e / P, (int)(e % P));
+        __syncthreads();
+    }
+}
+template <int P>
+__global__ void __launch_bounds__(128) k_fmm_up_top(VxScalars *S, int *cnt, cplx *M) {
+    VX_PDL_WAIT();
+    k_fmm_up_top_body<P>(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, S, cnt, M);
 }
 
 // M2L at level l (2 <= l <= L) plus L2L from level l-1.  A block takes a
@@ -617,29 +568,37 @@ __global__ void __launch_bounds__(M2L_TILE * M2L_TILE * P) k_fmm_m2l_small(const
     k_fmm_m2l_small_body<P>(VxBlkB<M2L_TILE * M2L_TILE * P, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc);
 }
 
-// L2L into level l (3 <= l <= min(M2L_SMALL, L)) from level l-1, one thread
-// per (cell, coefficient); one launch per level.
+// L2L into levels 3 .. min(M2L_SMALL, L), one launch: a block takes a cell
+// of level 3 and walks down its subtree level by level (a barrier between
+// levels), one thread per (cell, coefficient).
 template <int P>
-VX_DEVK void k_fmm_l2l_small_body(VxBlkB<256, 0> vb, const VxScalars *S, const int *cnt, cplx *Loc, int l) {
+VX_DEVK void k_fmm_l2l_small_body(VxBlkB<256, 0> vb, const VxScalars *S, const int *cnt, cplx *Loc) {
     __shared__ cplx se[4][P];
-    if (l > min(S->fL, M2L_SMALL)) return;
+    const int hi = min(S->fL, M2L_SMALL);
+    if (hi < 3) return;
     fmm_shift_table<P>(se);
     __syncthreads();
-    const long long m = 1LL << l;
-    const int *cl = cnt + fmm_level_off(l);
-    cplx *Ll = Loc + fmm_level_off(l) * P;
-    const cplx *Lp = Loc + fmm_level_off(l - 1) * P;
-    for (long long e = vb.x * (long long)blockDim.x + threadIdx.x; e < m * m * P;
-         e += (long long)vb.n * blockDim.x) {
-        const long long c = e / P;
-        const int lc = (int)(e % P);
-        if (cl[c] > 0) Ll[e] = cadd(Ll[e], l2l_term<P>(Lp, se, m, c % m, c / m, lc));
+    for (long long r = vb.x; r < 64; r += vb.n) {
+        const long long rx = r % 8, ry = r / 8;
+        for (int l = 3; l <= hi; ++l) {
+            const long long sl = 1LL << (l - 3), m = 1LL << l;
+            const int *cl = cnt + fmm_level_off(l);
+            cplx *Ll = Loc + fmm_level_off(l) * P;
+            const cplx *Lp = Loc + fmm_level_off(l - 1) * P;
+            for (long long e = threadIdx.x; e < sl * sl * P; e += blockDim.x) {
+                const long long q = e / P;
+                const int lc = (int)(e % P);
+                const long long c = (ry * sl + q / sl) * m + rx * sl + q % sl;
+                if (cl[c] > 0) Ll[c * P + lc] = cadd(Ll[c * P + lc], l2l_term<P>(Lp, se, m, c % m, c / m, lc));
+            }
+            __syncthreads();
+        }
     }
 }
 template <int P>
-__global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const int *cnt, cplx *Loc, int l) {
+__global__ void __launch_bounds__(256) k_fmm_l2l_small(const VxScalars *S, const int *cnt, cplx *Loc) {
     VX_PDL_WAIT();
-    k_fmm_l2l_small_body<P>(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, S, cnt, Loc, l);
+    k_fmm_l2l_small_body<P>(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, S, cnt, Loc);
 }
 
 // Near field (FP32, core smoothing) + far field (L2P, FP64): one warp per
@@ -857,6 +816,44 @@ __device__ __forceinline__ void fmm_ring_cell(int k, int q, int &dx, int &dy) {
     dx = k; dy = q - k + 1;
 }
 
+// The targets the ring search left over, by one block: each scans every
+// source slot (FP64 differences, as the direct pass).
+__device__ void fmm_nn3_brute_block(VxView v, VxScalars *S, const int *brute_list) {
+    __shared__ float sd[3][FMM_T / 32];
+    const int nb = __ldcg(&S->fnbrute);
+    const long long fs = S->fs;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = 0; b < nb; ++b) {
+        const long long i = __ldcg(&brute_list[b]);
+        const double xi = v.x[i * v.ps], yi = v.y[i * v.ps];
+        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
+        for (long long j = threadIdx.x; j < fs; j += blockDim.x) {
+            if (j == i) continue;
+            const double dx = xi - v.x[j * v.ps], dy = yi - v.y[j * v.ps];
+            vx_nn3_insert_bf(d1, d2, d3, (float)fma(dx, dx, dy * dy));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float e1 = __shfl_xor_sync(0xffffffffu, d1, o);
+            const float e2 = __shfl_xor_sync(0xffffffffu, d2, o);
+            const float e3 = __shfl_xor_sync(0xffffffffu, d3, o);
+            vx_nn3_insert_bf(d1, d2, d3, e1);
+            vx_nn3_insert_bf(d1, d2, d3, e2);
+            vx_nn3_insert_bf(d1, d2, d3, e3);
+        }
+        if (lane == 0) { sd[0][warp] = d1; sd[1][warp] = d2; sd[2][warp] = d3; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < FMM_T / 32; ++w) {
+                vx_nn3_insert_bf(d1, d2, d3, sd[0][w]);
+                vx_nn3_insert_bf(d1, d2, d3, sd[1][w]);
+                vx_nn3_insert_bf(d1, d2, d3, sd[2][w]);
+            }
+            v.d[i] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
+        }
+        __syncthreads();
+    }
+}
+
 VX_DEVK void k_fmm_nn3_fix_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const float4 *srt, const int *sorted,
                                 const int *start, const int *flag_list, int *brute_list) {
     const int nf = S->fnflag;
@@ -909,6 +906,9 @@ VX_DEVK void k_fmm_nn3_fix_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const f
             else brute_list[atomicAdd(&S->fnbrute, 1)] = (int)i;
         }
     }
+    // the rare targets no ring settled: the block that finishes last scans
+    // every source for them
+    if (vx_last_block(&S->sync_ctr, vb.n)) fmm_nn3_brute_block(v, S, brute_list);
 }
 __global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const int *sorted,
                               const int *start, const int *flag_list, int *brute_list) {
@@ -920,120 +920,36 @@ __global__ void k_fmm_nn3_fix(VxView v, VxScalars *S, const float4 *srt, const i
 // brute_list) over every source slot [0, fs): one block per target, each
 // thread keeping the three smallest of its stride, merged over the warp and
 // the block (the same set of sources as the ring search, so the same three).
-VX_DEVK void k_fmm_nn3_brute_body(VxBlkB<256, 0> vb, VxView v, const VxScalars *S, const int *brute_list) {
-    __shared__ float sd[3][256 / 32];
-    const int nb = S->fnbrute;
-    const long long fs = S->fs;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int b = vb.x; b < nb; b += vb.n) {
-        const long long i = brute_list[b];
-        const double xi = v.x[i * v.ps], yi = v.y[i * v.ps];
-        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
-        for (long long j = threadIdx.x; j < fs; j += blockDim.x) {
-            if (j == i) continue;
-            const double dx = xi - v.x[j * v.ps], dy = yi - v.y[j * v.ps];
-            vx_nn3_insert_bf(d1, d2, d3, (float)fma(dx, dx, dy * dy));
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const float e1 = __shfl_xor_sync(0xffffffffu, d1, o);
-            const float e2 = __shfl_xor_sync(0xffffffffu, d2, o);
-            const float e3 = __shfl_xor_sync(0xffffffffu, d3, o);
-            vx_nn3_insert_bf(d1, d2, d3, e1);
-            vx_nn3_insert_bf(d1, d2, d3, e2);
-            vx_nn3_insert_bf(d1, d2, d3, e3);
-        }
-        if (lane == 0) { sd[0][warp] = d1; sd[1][warp] = d2; sd[2][warp] = d3; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 1; w < 256 / 32; ++w) {
-                vx_nn3_insert_bf(d1, d2, d3, sd[0][w]);
-                vx_nn3_insert_bf(d1, d2, d3, sd[1][w]);
-                vx_nn3_insert_bf(d1, d2, d3, sd[2][w]);
+
+// Near-field work items: every leaf's targets in chunks of FMM_W, leaves in
+// index order (row-major), as (leaf, first target slot); one-pass scan of
+// the leaves' item counts, each thread writing its leaves' items.
+VX_DEVK void k_fmm_items_body(VxBlkB<VX_SCAN_T, 0> vb, VxScalars *S, const int *start, int2 *items,
+                              long long items_cap, unsigned long long *tiles) {
+    constexpr int PER = 4;
+    const long long nl = S->fnleaves;
+    vx_scan_lookback<PER>(
+        vb.n, nl, S, tiles, [&](long long c) { return (start[c + 1] - start[c] + FMM_W - 1) / FMM_W; },
+        [&](long long c0, const unsigned *val, long long run) {
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                const long long c = c0 + q;
+                if (c >= nl) break;
+                const int j0 = start[c];
+                for (unsigned k = 0; k < val[q]; ++k, ++run)
+                    if (run < items_cap) items[run] = make_int2((int)c, j0 + (int)k * FMM_W);
             }
-            v.d[i] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
-        }
-        __syncthreads();
-    }
+        },
+        [&](long long tot) {
+            // the item buffer holds s/32 + cells items, so this never truncates
+            if (tot > items_cap) S->err |= VX_DERR_GRID;
+            S->cnitems = tot <= items_cap ? tot : items_cap;
+        });
 }
-__global__ void __launch_bounds__(256) k_fmm_nn3_brute(VxView v, const VxScalars *S, const int *brute_list) {
+__global__ void __launch_bounds__(VX_SCAN_T) k_fmm_items(VxScalars *S, const int *start, int2 *items,
+                                                         long long items_cap, unsigned long long *tiles) {
     VX_PDL_WAIT();
-    k_fmm_nn3_brute_body(VxBlkB<256, 0>{blockIdx.x, gridDim.x}, v, S, brute_list);
-}
-
-// Row items over the leaf grid (m x m), as for the neighbour-list grid.
-// Near-field work items: every leaf's targets in chunks of FMM_W, counted per
-// leaf row (one warp per row, lanes over its leaves).
-VX_DEVK void k_fmm_row_items_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, int *row_items) {
-    const long long m = 1LL << S->fL;
-    const int lane = threadIdx.x & 31;
-    const long long nw = ((long long)vb.n * blockDim.x) >> 5;
-    for (long long r = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
-        int k = 0;
-        for (long long c = r * m + lane; c < (r + 1) * m; c += 32) k += (start[c + 1] - start[c] + FMM_W - 1) / FMM_W;
-        for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
-        if (lane == 0) row_items[r] = k;
-    }
-}
-__global__ void k_fmm_row_items(const VxScalars *S, const int *start, int *row_items) {
-    VX_PDL_WAIT();
-    k_fmm_row_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items);
-}
-
-VX_DEVK void k_fmm_row_scan_body(VxBlkB<1024, 0> vb, VxScalars *S, const int *in, long long *out, long long items_cap) {
-    __shared__ long long sh[1024];
-    const long long len = 1LL << S->fL;
-    const long long per = vx_ceil_div(len, (long long)blockDim.x);
-    const long long b = threadIdx.x * per, e = min(len, b + per);
-    long long local = 0;
-    for (long long q = b; q < e; ++q) local += in[q];
-    sh[threadIdx.x] = local;
-    __syncthreads();
-    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-        long long t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-        __syncthreads();
-        sh[threadIdx.x] += t;
-        __syncthreads();
-    }
-    long long run = sh[threadIdx.x] - local;
-    for (long long q = b; q < e; ++q) { out[q] = run; run += in[q]; }
-    if (threadIdx.x == blockDim.x - 1) {
-        // the item buffer holds s/32 + rows items, so this never truncates
-        if (run > items_cap) S->err |= VX_DERR_GRID;
-        S->cnitems = run <= items_cap ? run : items_cap;
-    }
-}
-__global__ void __launch_bounds__(1024) k_fmm_row_scan(VxScalars *S, const int *in, long long *out, long long items_cap) {
-    VX_PDL_WAIT();
-    k_fmm_row_scan_body(VxBlkB<1024, 0>{blockIdx.x, gridDim.x}, S, in, out, items_cap);
-}
-
-VX_DEVK void k_fmm_items_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, const int *row_items, const long long *off,
-                              int2 *items, long long items_cap) {
-    const long long m = 1LL << S->fL;
-    const int lane = threadIdx.x & 31;
-    const long long nw = ((long long)vb.n * blockDim.x) >> 5;
-    for (long long r = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
-        long long o = off[r];
-        for (long long c0 = r * m; c0 < (r + 1) * m; c0 += 32) {
-            const long long c = c0 + lane;
-            const int j0 = c < (r + 1) * m ? start[c] : 0, j1 = c < (r + 1) * m ? start[c + 1] : 0;
-            const int k = (j1 - j0 + FMM_W - 1) / FMM_W;
-            int inc = k;   // inclusive warp scan of the leaves' item counts
-            for (int d = 1; d < 32; d <<= 1) {
-                const int u = __shfl_up_sync(0xffffffffu, inc, d);
-                if (lane >= d) inc += u;
-            }
-            long long oo = o + inc - k;
-            for (int j = j0; j < j1; j += FMM_W, ++oo)
-                if (oo < items_cap) items[oo] = make_int2((int)c, j);   // (leaf, first target slot)
-            o += __shfl_sync(0xffffffffu, inc, 31);
-        }
-    }
-}
-__global__ void k_fmm_items(const VxScalars *S, const int *start, const int *row_items, const long long *off,
-                            int2 *items, long long items_cap) {
-    VX_PDL_WAIT();
-    k_fmm_items_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, row_items, off, items, items_cap);
+    k_fmm_items_body(VxBlkB<VX_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, start, items, items_cap, tiles);
 }
 
 long long vx_fmm_cells(int lmax) { return fmm_level_off(lmax + 1); }
@@ -1060,42 +976,36 @@ static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxVi
     }
     const int grid = L.num_sms * 4;
     const int Lmax = w.fmm_lmax;
-    vx_launch<k_fmm_begin, k_fmm_begin_body>(L, 1, 1, 0, S);
-    vx_launch<k_fmm_bbox, k_fmm_bbox_body>(L, grid, FMM_T, 0, v, S);
-    vx_launch<k_fmm_params, k_fmm_params_body>(L, 1, 1, 0, S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32);
-    vx_launch<k_fmm_zero_cnt, k_fmm_zero_cnt_body>(L, grid, FMM_T, 0, S, w.fmm_cnt, w.fmm_sub_cnt);
+    const int pgrid = std::min(grid, VX_RED_BLOCKS);   // 4 box keys per block
+    vx_launch<k_fmm_prep, k_fmm_prep_body>(L, pgrid, FMM_T, 0, v, S, p.eps, Lmax, p.fmm_leaf > 0 ? p.fmm_leaf : 32,
+                                           w.fmm_cnt, vx_fmm_cells(Lmax), w.fmm_sub_cnt, 1LL << (2 * (Lmax + 1)),
+                                           w.box);
     vx_launch<k_fmm_leafid, k_fmm_leafid_body>(L, grid, FMM_T, 0, v, S, w.key0, w.val0, w.fmm_sub_cnt);
-    vx_launch<k_fmm_scan_sum, k_fmm_scan_sum_body>(L, grid, FMM_T, 0, S, (const int *)w.fmm_sub_cnt, w.cell_chunk_cnt);
-    vx_launch<k_fmm_scan_top, k_fmm_scan_top_body>(L, 1, 1024, 0, S, w.cell_chunk_cnt, w.cell_chunk_off);
-    vx_launch<k_fmm_scan_apply, k_fmm_scan_apply_body>(L, grid, FMM_T, 0, S, (const int *)w.fmm_sub_cnt, w.cell_chunk_off,
-                                                       w.fmm_sub_start);
-    vx_launch<k_fmm_leaf_from_sub, k_fmm_leaf_from_sub_body>(L, grid, FMM_T, 0, S, (const int *)w.fmm_sub_cnt,
-                                                             (const int *)w.fmm_sub_start, w.fmm_cnt, w.fmm_start);
-    // leaf order: each leaf's sources in index order (a stable sort by leaf)
+    vx_launch<k_fmm_scan, k_fmm_scan_body>(L, grid, VX_SCAN_T, 0, S, (const int *)w.fmm_sub_cnt, w.fmm_sub_start,
+                                           w.fmm_cnt, w.fmm_start, w.scan_tiles);
     // source order: by quarter-leaf, each quarter's sources in index order
-    // (a stable sort by the key 4 leaf + child; each leaf stays contiguous)
+    // (a stable sort by the key 4 leaf + child; each leaf stays contiguous),
+    // the FP32 sources gathered at their slots on the way
+    VxGather gt;
+    gt.mode = 1;
+    gt.v = v;
+    gt.S = S;
+    gt.srt = w.srt;
     vx_bucket_order(L, S, &S->fs, &S->fnsub, w.key0, w.fmm_sub_start, w.fmm_sub_cnt, nullptr, w.key1, w.val1,
-                    w.bk_mid, w.bk_big, w.val0);
+                    w.bk_mid, w.bk_big, w.val0, gt);
     const unsigned *skey = w.key1;
     const int *sorted = w.val1;
-    vx_launch<k_fmm_gather, k_fmm_gather_body>(L, grid, FMM_T, 0, v, S, sorted, skey, w.srt);
-    vx_launch<k_fmm_p2m<P>, k_fmm_p2m_body<P>>(L, grid * 4, 128, 0, v, S, w.fmm_start, sorted, (cplx *)w.fmm_M);
-    // the level loops cover the deepest level this capacity allows; kernels
-    // of levels below the depth chosen on the device return at once
-    for (int l = Lmax - 1; l >= 0; --l) {
-        const int gm = (int)std::min<long long>(grid * 2, vx_ceil_div((1LL << (2 * l)) * P, 128));
-        vx_launch<k_fmm_m2m<P>, k_fmm_m2m_body<P>>(L, gm, 128, 0, S, w.fmm_cnt, (cplx *)w.fmm_M, l);
-    }
+    // upward pass: P2M + M2M of the 3 levels above the leaves by subtrees,
+    // then the levels above those (two launches whatever the depth)
+    const int gup = (int)std::min<long long>(grid * 4, 1LL << (2 * std::max(Lmax - FMM_UP, 0)));
+    vx_launch<k_fmm_up<P>, k_fmm_up_body<P>>(L, gup, 128, 0, v, S, w.fmm_start, sorted, w.fmm_cnt, (cplx *)w.fmm_M);
+    vx_launch<k_fmm_up_top<P>, k_fmm_up_top_body<P>>(L, 1 << (2 * FMM_TOP), 128, 0, S, w.fmm_cnt, (cplx *)w.fmm_M);
     {
         long long tiles = 0;
         for (int l = 2; l <= std::min(Lmax, M2L_SMALL); ++l) tiles += vx_ceil_div(1LL << (2 * l), 16LL);
         if (tiles > 0) {
             vx_launch<k_fmm_m2l_small<P>, k_fmm_m2l_small_body<P>>(L, (int)std::min<long long>(grid * 2, tiles), M2L_T, M2L_SMEM, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L);
-
-            for (int l = 3; l <= std::min(Lmax, M2L_SMALL); ++l) {
-                const int g = (int)std::min<long long>(grid, vx_ceil_div((1LL << (2 * l)) * P, 256));
-                vx_launch<k_fmm_l2l_small<P>, k_fmm_l2l_small_body<P>>(L, g, 256, 0, S, w.fmm_cnt, (cplx *)w.fmm_L, l);
-            }
+            vx_launch<k_fmm_l2l_small<P>, k_fmm_l2l_small_body<P>>(L, 64, 256, 0, S, w.fmm_cnt, (cplx *)w.fmm_L);
         }
     }
     for (int l = M2L_SMALL + 1; l <= Lmax; ++l) {
@@ -1104,9 +1014,7 @@ static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxVi
         vx_launch<k_fmm_m2l_l2l<P>, k_fmm_m2l_l2l_body<P>>(L, g, M2L_T, M2L_SMEM, S, w.fmm_cnt, (const cplx *)w.fmm_M, (cplx *)w.fmm_L, l);
 
     }
-    vx_launch<k_fmm_row_items, k_fmm_row_items_body>(L, grid, FMM_T, 0, S, w.fmm_start, w.row_items);
-    vx_launch<k_fmm_row_scan, k_fmm_row_scan_body>(L, 1, 1024, 0, S, w.row_items, w.row_item_off, w.items_cap);
-    vx_launch<k_fmm_items, k_fmm_items_body>(L, grid, FMM_T, 0, S, w.fmm_start, w.row_items, w.row_item_off, w.items, w.items_cap);
+    vx_launch<k_fmm_items, k_fmm_items_body>(L, grid, VX_SCAN_T, 0, S, w.fmm_start, w.items, w.items_cap, w.scan_tiles);
 
     VX_EV(L, 0);
     vx_launch<k_fmm_near<P>, k_fmm_near_body<P>>(L, L.num_sms * 8, FMM_T, 0, p, v, S, w.srt, sorted, w.fmm_start,
@@ -1117,7 +1025,6 @@ static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxVi
 
     vx_launch<k_fmm_nn3_fix, k_fmm_nn3_fix_body>(L, grid, FMM_T, 0, v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
 
-    vx_launch<k_fmm_nn3_brute, k_fmm_nn3_brute_body>(L, grid, 256, 0, v, S, w.fmm_brute);
 
     return cudaGetLastError();
 }

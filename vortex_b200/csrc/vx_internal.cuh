@@ -81,7 +81,6 @@ struct VxScalars {
     long long col_n_before;
     int col_done;
     int ncand;
-    unsigned long long bb[4];  // ordered keys of x_min, -x_max, y_min, -y_max
     double gx0, gy0, gh;
     long long gnx, gny, gncells;
     int err;
@@ -89,11 +88,9 @@ struct VxScalars {
     int cnhuge;            // of those, the ones whose window spans more than WIDE_ROWS rows each side
     long long bf_nnear;    // birth sources inside the far-field radius
     // neighbour-list grid of the bulk form (vortex diffusion)
-    unsigned long long cb[4];
     double cx0, cy0, ch;
     long long cnx, cny, cncells, cnitems;
     // quadtree of the bulk-form Biot-Savart (vx_fmm.cu)
-    unsigned long long fb[4];
     double fx0, fy0, fside;
     long long fnleaves, fs;
     long long fnsub;       // cells of the level below the leaves (4 per leaf): the 3-nearest grid
@@ -104,11 +101,17 @@ struct VxScalars {
     // pair evaluations executed by the bulk-form near-field and diffusion
     // kernels since the counters were last cleared
     unsigned long long pairs_bs, pairs_diff;
+    // grid-wide steps inside one launch (vx_last_block, vx_scan_lookback):
+    // the arrival counter of the last-block pattern, and the running scan's
+    // tile ticket, finished-block count and epoch (all at rest between
+    // launches: the counters at zero, the epoch advanced once per scan)
+    unsigned sync_ctr, scan_ticket, scan_done, scan_epoch;
 };
 
 enum {
     VX_DERR_RESOLVE = 1,     // collapse resolution did not converge
     VX_DERR_GRID = 2,        // collapse grid did not fit its cell capacity
+    VX_DERR_SCAN = 4,        // a look-back scan gave up waiting on a predecessor tile
 };
 
 // Device scratch of one body.  Sizes are in elements.
@@ -125,8 +128,6 @@ struct VxWork {
     int *cellid, *cell_cnt, *cell_start, *sorted;
     int *col, *in_cnt, *has_app, *first_app, *cand, *cstate, *cdec;
     double *mx, *my, *mg;
-    long long *cell_chunk_off;
-    int *cell_chunk_cnt;
     // pair partial sums
     double *part;
     long long part_cap;      // doubles
@@ -144,6 +145,7 @@ struct VxWork {
     double *bf_coef;
     // reductions
     double *red;             // [blocks][4]
+    unsigned long long *box; // [blocks][4] bounding-box keys of the grids' first pass
     // neighbour-list grid (bulk form): radix-sort buffers, cells, sorted sources
     unsigned *key0, *key1;
     int *val0, *val1;
@@ -154,14 +156,15 @@ struct VxWork {
     int *cg_wide;            // sorted slots of the diffusion targets summed one warp each
     int *cg_huge;            // sorted slots of those summed one block each
     int *bk_mid, *bk_big;    // buckets of 17..128 / more than 128 elements (vx_bucket_order)
-    int *row_items;
-    long long *row_item_off;
     // quadtree: counts and expansions of every level up to fmm_lmax
     int fmm_lmax;
     int *fmm_cnt, *fmm_start, *fmm_flags, *fmm_brute;
     int *fmm_sub_cnt, *fmm_sub_start;   // counts / starts of the level below the leaves
     int fmm_p;               // expansion terms the two arrays below were sized for
     double *fmm_M, *fmm_L;   // complex FP64 pairs, fmm_p per cell
+    // tile words of the look-back scans (zeroed when allocated)
+    unsigned long long *scan_tiles;
+    long long scan_tiles_cap;
 };
 
 constexpr int VX_FMM_P = 16;              // default expansion terms of the quadtree FMM (vx_fmm.cu)
@@ -176,6 +179,51 @@ constexpr int VX_THREADS = 256;
 // helpers
 __host__ __device__ inline long long vx_ceil_div(long long a, long long b) { return (a + b - 1) / b; }
 __host__ __device__ inline long long vx_round32(long long v) { return (v + 31) / 32 * 32; }
+__host__ __device__ inline long long vx_pow2_ceil(long long n) {
+    long long q = 1;
+    while (q < n) q <<= 1;
+    return q;
+}
+
+// Result-defining partitions.  Sums split into partitions (force sums,
+// diffusion-grid mean, birth far field and right-hand side, pair-kernel
+// source chunks) round differently for different splits, so every split is a
+// function of the body's own count, taken on the device inside the kernel
+// that uses it (never of the host's running bound of the count, which
+// depends on when the host last looked): equal states give equal bits,
+// whatever ran before or beside.  Grids stay the host's choice.
+//
+// SMs' worth of partitions for n sources: one per 2048 (n rounded up to a
+// power of two), at least 4, at most the device's sms.
+__host__ __device__ inline int vx_body_sms(long long n, int sms) {
+    const long long q = vx_pow2_ceil(n) / 2048;
+    return (int)(q < 4 ? 4 : (q > sms ? sms : q));
+}
+// Partitions of the force sums and of the diffusion-grid mean.
+__host__ __device__ inline int vx_body_parts(long long n, int sms, int cap) {
+    const int q = 4 * vx_body_sms(n, sms);
+    return q < cap ? q : cap;
+}
+// Source chunks of the pair kernels: about 8 work items per SM over tiles
+// of `tile` targets, 1 to 64.
+__host__ __device__ inline int vx_ksplit(long long n, int tile, int sms) {
+    const long long tiles = vx_ceil_div(n > 0 ? n : 1, tile);
+    long long k = vx_ceil_div(8LL * sms, tiles);
+    return (int)(k < 1 ? 1 : (k > 64 ? 64 : k));
+}
+// Source chunks of the birth right-hand side for P panels and n0 sources:
+// enough (panel tile, chunk) items for every SM to hold several blocks,
+// within the partial-sum buffer (sms * 4 chunks), one per 1024 sources (n0
+// rounded up to a power of two) at most.
+__host__ __device__ inline int vx_rhs_chunks(long long n0, int P, int sms) {
+    const long long tiles = (P + 127) / 128;
+    long long want = (long long)sms * 16 / tiles;
+    if (want < 1) want = 1;
+    if (want > (long long)sms * 4) want = (long long)sms * 4;
+    long long bysrc = vx_ceil_div(vx_pow2_ceil(n0), 1024);
+    if (bysrc < 1) bysrc = 1;
+    return (int)(want < bysrc ? want : bysrc);
+}
 
 // Keep the 3 smallest squared distances (src/kernel.cu:941-953): the result
 // is the same for any visiting order.
@@ -238,6 +286,154 @@ __device__ __forceinline__ unsigned long long vx_dkey(double v) {
 __device__ __forceinline__ double vx_dunkey(unsigned long long k) {
     unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
     return __longlong_as_double((long long)b);
+}
+
+// ---------------------------------------------------------------------------
+// Grid-wide steps inside one launch.  Both helpers count a body's own blocks
+// (nblk = the body's share of the launch), so they work the same in a single
+// body's launch and in a launch over many bodies.
+//
+// vx_last_block: true in the block that arrives last of the body's nblk
+// blocks; `ctr` counts arrivals and is left at zero.  Every block's global
+// writes before its arrival are visible to that block, which reads them
+// through L2 (__ldcg), never through an L1 line it may hold from before.
+__device__ __forceinline__ bool vx_last_block(unsigned *ctr, unsigned nblk) {
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(ctr, 1u);
+        s_last = t == nblk - 1;
+        if (s_last) atomicExch(ctr, 0u);
+    }
+    __syncthreads();
+    const bool last = s_last != 0;
+    if (last) __threadfence();
+    return last;
+}
+
+// vx_scan_lookback: one-pass exclusive scan of non-negative int counts
+// (decoupled look-back).  Blocks take tiles of VX_SCAN_T x PER consecutive
+// counts in ticket order; each tile publishes its own sum, then walks back
+// over its predecessors' published words (32 at a time, one per lane) adding
+// their sums until it meets an inclusive prefix, and publishes its own.  A
+// tile only waits on tiles whose tickets were taken before its own, so on
+// blocks that are already running: the scan needs no co-residency.
+//   tiles[t] = (stamp << 34) | (state << 32) | value, state 1 = the tile's
+//   own sum, 2 = the inclusive prefix.  The stamp (1 .. 2^30 - 1) changes
+//   with every scan of the body, so a word left by an earlier scan never
+//   counts, nor does zeroed memory.
+// A wait is bounded: after VX_SCAN_SPIN polls the scan sets VX_DERR_SCAN and
+// takes the missing sums as 0 (the step then reports the flag).
+// load(i) gives count i; store(i0, val, run) gets a thread's PER counts from
+// i0 (PER-aligned; entries at or past `count` are 0) and the scan value at i0;
+// total(sum) is called once, by one thread, with the sum of all counts.
+// The block must have VX_SCAN_T threads.  Totals below 2^32.
+constexpr int VX_SCAN_T = 256;
+constexpr int VX_SCAN_SPIN = 1 << 20;
+
+__device__ __forceinline__ void vx_scan_publish(unsigned long long *p, unsigned stamp, unsigned state,
+                                                unsigned value) {
+    const unsigned long long w = ((unsigned long long)stamp << 34) | ((unsigned long long)state << 32) | value;
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+__device__ __forceinline__ unsigned long long vx_scan_peek(const unsigned long long *p) {
+    unsigned long long w;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+    return w;
+}
+
+template <int PER, typename Load, typename Store, typename Total>
+__device__ void vx_scan_lookback(unsigned nblk, long long count, VxScalars *S, unsigned long long *tiles,
+                                 Load load, Store store, Total total) {
+    constexpr int NW = VX_SCAN_T / 32;
+    constexpr long long TILE = (long long)VX_SCAN_T * PER;
+    __shared__ long long s_tile;
+    __shared__ unsigned s_warp[NW];
+    __shared__ unsigned long long s_prefix;
+    const unsigned stamp = 1u + S->scan_epoch % 0x3fffffffu;
+    const long long ntiles = (count + TILE - 1) / TILE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long t;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(&S->scan_ticket, 1u);
+        __syncthreads();
+        t = s_tile;
+        if (t >= ntiles) break;
+        const long long i0 = t * TILE + (long long)threadIdx.x * PER;
+        unsigned val[PER];
+        unsigned loc = 0;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            val[q] = i0 + q < count ? (unsigned)load(i0 + q) : 0u;
+            loc += val[q];
+        }
+        unsigned inc = loc;   // inclusive scan over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned wv = lane < NW ? s_warp[lane] : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned u = __shfl_up_sync(0xffffffffu, wv, o);
+                if (lane >= o) wv += u;
+            }
+            if (lane < NW) s_warp[lane] = wv;
+            const unsigned agg = __shfl_sync(0xffffffffu, wv, NW - 1);
+            unsigned long long prefix = 0;
+            if (t == 0) {
+                if (lane == 0) vx_scan_publish(&tiles[0], stamp, 2u, agg);
+            } else {
+                if (lane == 0) vx_scan_publish(&tiles[t], stamp, 1u, agg);
+                long long j = t - 1;
+                int spins = 0;
+                for (;;) {
+                    const long long idx = j - lane;
+                    const unsigned long long wd =
+                        idx >= 0 ? vx_scan_peek(&tiles[idx]) : (((unsigned long long)stamp << 34) | (2ull << 32));
+                    const unsigned st = (unsigned)(wd >> 32) & 3u;
+                    const bool ready = (unsigned)(wd >> 34) == stamp && st != 0u;
+                    if (!__all_sync(0xffffffffu, ready)) {
+                        if (++spins > VX_SCAN_SPIN) {
+                            if (lane == 0) atomicOr(&S->err, VX_DERR_SCAN);
+                            break;
+                        }
+                        __nanosleep(32);
+                        continue;
+                    }
+                    const unsigned pm = __ballot_sync(0xffffffffu, st == 2u);
+                    const int stop = pm ? __ffs(pm) - 1 : 31;
+                    unsigned long long v = lane <= stop ? (wd & 0xffffffffull) : 0ull;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    prefix += v;
+                    if (pm) break;
+                    j -= 32;
+                }
+                if (lane == 0) vx_scan_publish(&tiles[t], stamp, 2u, (unsigned)(prefix + agg));
+            }
+            if (lane == 0) s_prefix = prefix;
+        }
+        __syncthreads();
+        const unsigned long long run = s_prefix + (warp ? s_warp[warp - 1] : 0u) + inc - loc;
+        store(i0, val, (long long)run);
+        if (t == ntiles - 1 && threadIdx.x == VX_SCAN_T - 1) total((long long)(run + loc));
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (ntiles == 0 && t == 0) total(0LL);
+        __threadfence();
+        if (atomicAdd(&S->scan_done, 1u) == nblk - 1) {
+            S->scan_ticket = 0;
+            S->scan_done = 0;
+            S->scan_epoch += 1;
+        }
+    }
 }
 
 // Programmatic dependent launch (sm_90+): a kernel launched by vx_launch_pdl
@@ -406,17 +602,12 @@ struct VxLaunch {
     // for a share of the GPU that follows its source count (grid-stride
     // kernels: same results, fewer idle blocks, so the kernels of many
     // small bodies on concurrent streams overlap); full_sms (0: num_sms)
-    // stays the device's count for the kernels whose work does not scale
-    // with the count (the all-pairs sums) or whose results depend on the
-    // grid (the birth far field's per-block partials).
+    // stays the device's count: the all-pairs sums' grid, and the SM count
+    // the result-defining partitions are derived from on the device
+    // (vx_body_parts, vx_ksplit, vx_rhs_chunks), so a body gets the same
+    // results whatever share of the GPU it runs on.
     int num_sms;
     int full_sms = 0;
-    // SMs the result-defining partitions of a body are sized for (0:
-    // num_sms): the force sums, the diffusion grid's mean spacing and the
-    // birth far field's partial sums split the particles into partitions
-    // whose number follows the body's size, not the grid of the launch, so
-    // a body gets the same results whatever share of the GPU it runs on.
-    int part_sms = 0;
     // optional events recorded around the Biot-Savart and diffusion pair
     // kernels: [0,1] Biot-Savart, [2,3] diffusion (null: not recorded)
     cudaEvent_t pair_ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -425,7 +616,6 @@ struct VxLaunch {
     VxKernelTimer *kt = nullptr;
 };
 inline int vx_full_sms(const VxLaunch &L) { return L.full_sms > 0 ? L.full_sms : L.num_sms; }
-inline int vx_part_sms(const VxLaunch &L) { return L.part_sms > 0 ? L.part_sms : L.num_sms; }
 #define VX_EV(L, k) do { if ((L).pair_ev[k] && !(L).rec) cudaEventRecord((L).pair_ev[k], (L).stream); } while (0)
 
 // Launch kernel K (the __global__ wrapper of body DEV) for one body: with
@@ -486,9 +676,9 @@ cudaError_t vx_launch_birth(const VxLaunch &L, const VxParams &p, const VxView &
                             int rhs_chunks);
 cudaError_t vx_transpose_square(const VxLaunch &L, const double *A, double *At, long long nr);
 cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                               VxWork &w, int ksplit);
+                               VxWork &w);
 cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                                VxWork &w, int ksplit);
+                                VxWork &w);
 // wstart/widx: per wall cell, the panels that can act on a particle in the
 // cell (CSR, ascending panel index); null: every panel is tested
 cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
@@ -496,8 +686,9 @@ cudaError_t vx_launch_wall(const VxLaunch &L, const VxParams &p, const VxView &v
 cudaError_t vx_launch_advect(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                              VxWork &w, const vx_panel *pan,
                              const int *hstart = nullptr, const int *hidx = nullptr);
+// count_step: the compaction of a whole step also advances the step index.
 cudaError_t vx_launch_compact(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                              VxWork &w);
+                              VxWork &w, bool count_step = false);
 cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                                VxWork &w, int pass, int n_col);
 cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
@@ -519,18 +710,51 @@ cudaError_t vx_launch_birth_ld(const VxLaunch &L, const VxParams &p, const VxVie
                                int rhs_chunks);
 cudaError_t vx_launch_step_end(const VxLaunch &L, VxScalars *S);
 cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const VxView &v,
-                                   VxScalars *S, VxWork &w, const int *skip);
+                                   VxScalars *S, VxWork &w, const int *skip, bool count_step = false);
 void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams *p);
 void vx_set_error(const char *fmt, ...);
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
                         cudaStream_t stream = nullptr, int fmm_p = VX_FMM_P);
 long long vx_work_bytes(long long cap, int P32, int num_sms, int fmm_p = VX_FMM_P);
-// Stable order by bucket from bucket counts (used up, then restored) and
-// starts: (okey, oval) = keys and element indices in bucket order, elements
-// of a bucket in index order (vx_sort.cu).
+// What the bucket order writes beside each element's final slot k (element
+// j, bucket key b): nothing (mode 0), the quadtree's FP32 source (mode 1:
+// position relative to the centre of leaf b / 4, G masked beyond n, the
+// leaf's column), or the diffusion grid's (mode 2: position relative to the
+// centre of cell b, G, d).  zero_counts: the bucket counts are left at zero
+// instead of restored.
+struct VxGather {
+    int mode = 0;
+    int zero_counts = 0;
+    VxView v = {};
+    const VxScalars *S = nullptr;
+    float4 *srt = nullptr;
+};
+__device__ __forceinline__ void vx_gather_slot(const VxGather &gt, long long k, long long j, unsigned b) {
+    const VxScalars *S = gt.S;
+    const VxView &v = gt.v;
+    if (gt.mode == 1) {
+        const unsigned m = 1u << S->fL;
+        const double h = S->fside / (double)m;
+        const unsigned leaf = b >> 2, col = leaf % m, row = leaf / m;
+        const double ccx = S->fx0 + ((double)col + 0.5) * h, ccy = S->fy0 + ((double)row + 0.5) * h;
+        gt.srt[k] = make_float4((float)(v.x[j * v.ps] - ccx), (float)(v.y[j * v.ps] - ccy),
+                                j < S->n ? (float)v.g[j * v.ps] : 0.0f, (float)col);
+    } else if (gt.mode == 2) {
+        const long long nx = S->cnx;
+        const double h = S->ch;
+        const double ccx = S->cx0 + ((double)(b % nx) + 0.5) * h, ccy = S->cy0 + ((double)(b / nx) + 0.5) * h;
+        gt.srt[k] = make_float4((float)(v.x[j * v.ps] - ccx), (float)(v.y[j * v.ps] - ccy), (float)v.g[j * v.ps],
+                                (float)v.d[j]);
+    }
+}
+// Stable order by bucket from bucket counts (used up, then restored or
+// zeroed) and starts: (okey, oval) = keys and element indices in bucket
+// order, elements of a bucket in index order, and the gather of gt at each
+// element's final slot (vx_sort.cu).
 cudaError_t vx_bucket_order(const VxLaunch &L, VxScalars *S, const long long *d_n, const long long *d_nbuckets,
                             const unsigned *key, const int *start, int *cnt, const long long *d_cnt_off,
-                            unsigned *okey, int *oval, int *mid, int *big, int *scratch);
+                            unsigned *okey, int *oval, int *mid, int *big, int *scratch,
+                            const VxGather &gt = VxGather());
 int vx_fmm_max_level(long long cap);
 long long vx_fmm_cells(int lmax);         // cells of all levels 0..lmax
 constexpr int VX_BF_P = 48;          // terms of the birth far-field expansion
@@ -543,4 +767,3 @@ cudaError_t vx_launch_diffusion_cells(const VxLaunch &L, const VxParams &p, cons
 void vx_work_free(VxWork &w, std::vector<void *> &allocs, cudaStream_t stream = nullptr);
 
 // Split factor so that (target tiles x source chunks) fills the GPU.
-int vx_pick_ksplit(long long n_upper, int tile, int num_sms);

@@ -20,14 +20,20 @@ constexpr int PT = 256;       // threads per block = sources per shared tile
 
 __host__ __device__ constexpr int pairs_tpt(bool fp32) { return fp32 ? 4 : 2; }
 
-int vx_pick_ksplit(long long n_upper, int tile, int num_sms) {
-    long long tiles = vx_ceil_div(n_upper > 0 ? n_upper : 1, tile);
-    long long want = (long long)num_sms * 8;
-    long long k = vx_ceil_div(want, tiles);
-    if (k < 1) k = 1;
-    if (k > 64) k = 64;
-    return (int)k;
+// Source split of the pair kernels: K source chunks; the partial sums of
+// target i and chunk sc sit at part[(sc nout + q) tstride + i], tstride =
+// cap / (nout K).  K > 0: the caller's split (probe points); K == 0: from the
+// body's own count on the device (vx_ksplit of it rounded up to a power of
+// two), so a step's sums never depend on the host's running bound.
+struct VxSplit {
+    long long cap;
+    int K, sms, tile, nout;
+};
+__device__ __forceinline__ void vx_split_of(const VxScalars *S, const VxSplit &sp, int &K, long long &tstride) {
+    K = sp.K > 0 ? sp.K : vx_ksplit(vx_pow2_ceil(S->n), sp.tile, sp.sms);
+    tstride = sp.cap / ((long long)sp.nout * K);
 }
+
 
 // ---------------------------------------------------------------------------
 // Packed FP32 sources for the bulk form: (x, y, G, 0), G masked to 0 beyond n.
@@ -82,7 +88,10 @@ template <typename T, bool NN3>
 VX_DEVK void k_bs_partial_body(VxBlkB<PT, 0> vb, VxParams p, VxView v, const VxScalars *S,
                                const float4 *src32, const double *tx,
                                const double *ty, long long tstr, long long nt_in,
-                               double *part, long long tstride, int K) {
+                               double *part, VxSplit sp) {
+    int K;
+    long long tstride;
+    vx_split_of(S, sp, K, tstride);
     constexpr int TPT = pairs_tpt(sizeof(T) == 4);
     constexpr int NOUT = NN3 ? 5 : 2;
     __shared__ SrcTile<T> st;
@@ -156,9 +165,9 @@ template <typename T, bool NN3>
 __global__ void __launch_bounds__(PT) k_bs_partial(VxParams p, VxView v, const VxScalars *S,
                                                    const float4 *src32, const double *tx,
                                                    const double *ty, long long tstr, long long nt_in,
-                                                   double *part, long long tstride, int K) {
+                                                   double *part, VxSplit sp) {
     VX_PDL_WAIT();
-    k_bs_partial_body<T, NN3>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, v, S, src32, tx, ty, tstr, nt_in, part, tstride, K);
+    k_bs_partial_body<T, NN3>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, v, S, src32, tx, ty, tstr, nt_in, part, sp);
 }
 
 // ---------------------------------------------------------------------------
@@ -204,8 +213,10 @@ __device__ __forceinline__ void bs32_tile(const float4 *sm, int cnt, int jbase, 
 template <bool NN3>
 VX_DEVK void k_bs32_partial_body(VxBlkB<PT, 0> vb, VxParams p, const VxScalars *S, const float4 *src32,
                                  const double *tx, const double *ty, long long tstr,
-                                 long long nt_in, double *part, long long tstride,
-                                 int K) {
+                                 long long nt_in, double *part, VxSplit sp) {
+    int K;
+    long long tstride;
+    vx_split_of(S, sp, K, tstride);
     constexpr int NOUT = NN3 ? 5 : 2;
     __shared__ float4 sm[PT];
     const long long n = S->n;
@@ -271,16 +282,17 @@ VX_DEVK void k_bs32_partial_body(VxBlkB<PT, 0> vb, VxParams p, const VxScalars *
 template <bool NN3>
 __global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars *S, const float4 *src32,
                                                      const double *tx, const double *ty, long long tstr,
-                                                     long long nt_in, double *part, long long tstride,
-                                                     int K) {
+                                                     long long nt_in, double *part, VxSplit sp) {
     VX_PDL_WAIT();
-    k_bs32_partial_body<NN3>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, S, src32, tx, ty, tstr, nt_in, part, tstride, K);
+    k_bs32_partial_body<NN3>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, S, src32, tx, ty, tstr, nt_in, part, sp);
 }
 
 // Combine: V = sum/(2 pi) + V_inf, d = mean of the 3 nearest distances.
 template <bool FP32>
-VX_DEVK void k_bs_combine_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const double *part, long long tstride,
-                               int K) {
+VX_DEVK void k_bs_combine_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const double *part, VxSplit sp) {
+    int K;
+    long long tstride;
+    vx_split_of(S, sp, K, tstride);
     const long long n = S->n;
     for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)vb.n * blockDim.x) {
@@ -303,14 +315,16 @@ VX_DEVK void k_bs_combine_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, co
     }
 }
 template <bool FP32>
-__global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, long long tstride,
-                             int K) {
+__global__ void k_bs_combine(VxView v, const VxScalars *S, const double *part, VxSplit sp) {
     VX_PDL_WAIT();
-    k_bs_combine_body<FP32>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, part, tstride, K);
+    k_bs_combine_body<FP32>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, part, sp);
 }
 
-VX_DEVK void k_probe_combine_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *part, long long tstride, int K,
+VX_DEVK void k_probe_combine_body(VxBlkB<0, 0> vb, const VxScalars *S, const double *part, VxSplit sp,
                                   long long np, double *ovx, double *ovy, long long ostride) {
+    int K;
+    long long tstride;
+    vx_split_of(S, sp, K, tstride);
     for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < np;
          i += (long long)vb.n * blockDim.x) {
         double sx = 0.0, sy = 0.0;
@@ -323,10 +337,10 @@ VX_DEVK void k_probe_combine_body(VxBlkB<0, 0> vb, const VxScalars *S, const dou
         ovy[i * ostride] = sy / VX_TWO_PI + S->vinf[1];
     }
 }
-__global__ void k_probe_combine(const VxScalars *S, const double *part, long long tstride, int K,
+__global__ void k_probe_combine(const VxScalars *S, const double *part, VxSplit sp,
                                 long long np, double *ovx, double *ovy, long long ostride) {
     VX_PDL_WAIT();
-    k_probe_combine_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, part, tstride, K, np, ovx, ovy, ostride);
+    k_probe_combine_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, part, sp, np, ovx, ovy, ostride);
 }
 
 // ---------------------------------------------------------------------------
@@ -354,7 +368,10 @@ template <> struct DiffMath<float> {
 template <typename T>
 VX_DEVK void k_diff_partial_body(VxBlkB<PT, 0> vb, VxParams p, VxView v, const VxScalars *S,
                                  const float4 *src32, double *part,
-                                 long long tstride, int K) {
+                                 VxSplit sp) {
+    int K;
+    long long tstride;
+    vx_split_of(S, sp, K, tstride);
     constexpr int TPT = pairs_tpt(sizeof(T) == 4);
     __shared__ SrcTile<T> st;
     const long long n = S->n;
@@ -422,13 +439,16 @@ VX_DEVK void k_diff_partial_body(VxBlkB<PT, 0> vb, VxParams p, VxView v, const V
 template <typename T>
 __global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const VxScalars *S,
                                                      const float4 *src32, double *part,
-                                                     long long tstride, int K) {
+                                                     VxSplit sp) {
     VX_PDL_WAIT();
-    k_diff_partial_body<T>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, v, S, src32, part, tstride, K);
+    k_diff_partial_body<T>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, v, S, src32, part, sp);
 }
 
 VX_DEVK void k_diff_combine_body(VxBlkB<0, 0> vb, VxParams p, VxView v, const VxScalars *S, const double *part,
-                                 long long tstride, int K) {
+                                 VxSplit sp) {
+    int K;
+    long long tstride;
+    vx_split_of(S, sp, K, tstride);
     const long long n = S->n;
     for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)vb.n * blockDim.x) {
@@ -447,9 +467,9 @@ VX_DEVK void k_diff_combine_body(VxBlkB<0, 0> vb, VxParams p, VxView v, const Vx
     }
 }
 __global__ void k_diff_combine(VxParams p, VxView v, const VxScalars *S, const double *part,
-                               long long tstride, int K) {
+                               VxSplit sp) {
     VX_PDL_WAIT();
-    k_diff_combine_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, part, tstride, K);
+    k_diff_combine_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, part, sp);
 }
 
 // ---------------------------------------------------------------------------
@@ -463,57 +483,76 @@ static cudaError_t maybe_pack(const VxLaunch &L, const VxParams &p, const VxView
     return cudaGetLastError();
 }
 
+// Source split of a step's pair sums: derived on the device from the body's
+// own count (vx_ksplit), tiles of 1024 targets in FP32, 512 in FP64.
+static VxSplit step_split(const VxLaunch &L, const VxParams &p, const VxWork &w, int nout) {
+    VxSplit sp;
+    sp.cap = w.part_cap;
+    sp.K = 0;
+    sp.sms = vx_full_sms(L);
+    sp.tile = p.prec == VX_PREC_FP32 ? 1024 : 512;
+    sp.nout = nout;
+    return sp;
+}
+
 cudaError_t vx_launch_velocity(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                               VxWork &w, int K) {
-    const long long tstride = w.part_cap / (5LL * K);
+                               VxWork &w) {
+    const VxSplit sp = step_split(L, p, w, 5);
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32) {
         VX_EV(L, 0);
-        vx_launch<k_bs32_partial<true>, k_bs32_partial_body<true>>(L, pair_grid(L), PT, 0, p, S, w.src32, v.x, v.y, v.ps, -1, w.part, tstride, K);
+        vx_launch<k_bs32_partial<true>, k_bs32_partial_body<true>>(L, pair_grid(L), PT, 0, p, S, w.src32, v.x, v.y, v.ps, -1, w.part, sp);
         VX_EV(L, 1);
 
-        vx_launch<k_bs_combine<true>, k_bs_combine_body<true>>(L, L.num_sms * 4, 256, 0, v, S, w.part, tstride, K);
+        vx_launch<k_bs_combine<true>, k_bs_combine_body<true>>(L, L.num_sms * 4, 256, 0, v, S, w.part, sp);
     } else {
         VX_EV(L, 0);
-        vx_launch<k_bs_partial<double, true>, k_bs_partial_body<double, true>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, v.x, v.y, v.ps, -1, w.part, tstride, K);
+        vx_launch<k_bs_partial<double, true>, k_bs_partial_body<double, true>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, v.x, v.y, v.ps, -1, w.part, sp);
         VX_EV(L, 1);
 
-        vx_launch<k_bs_combine<false>, k_bs_combine_body<false>>(L, L.num_sms * 4, 256, 0, v, S, w.part, tstride, K);
+        vx_launch<k_bs_combine<false>, k_bs_combine_body<false>>(L, L.num_sms * 4, 256, 0, v, S, w.part, sp);
     }
 
     return cudaGetLastError();
 }
 
 cudaError_t vx_launch_diffusion(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
-                                VxWork &w, int K) {
+                                VxWork &w) {
     // bulk form: neighbour lists within diff_cutoff * d_i (vx_cells.cu)
     if (p.prec == VX_PREC_FP32 && p.diff_cutoff > 0.0) return vx_launch_diffusion_cells(L, p, v, S, w);
-    const long long tstride = w.part_cap / (3LL * K);
+    const VxSplit sp = step_split(L, p, w, 3);
     VX_EV(L, 2);
     if (p.prec == VX_PREC_FP32) {
-        vx_launch<k_diff_partial<float>, k_diff_partial_body<float>>(L, pair_grid(L), PT, 0, p, v, S, w.src32, w.part, tstride, K);
+        vx_launch<k_diff_partial<float>, k_diff_partial_body<float>>(L, pair_grid(L), PT, 0, p, v, S, w.src32, w.part, sp);
     } else {
-        vx_launch<k_diff_partial<double>, k_diff_partial_body<double>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, w.part, tstride, K);
+        vx_launch<k_diff_partial<double>, k_diff_partial_body<double>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, w.part, sp);
     }
     VX_EV(L, 3);
 
-    vx_launch<k_diff_combine, k_diff_combine_body>(L, L.num_sms * 4, 256, 0, p, v, S, w.part, tstride, K);
+    vx_launch<k_diff_combine, k_diff_combine_body>(L, L.num_sms * 4, 256, 0, p, v, S, w.part, sp);
 
     return cudaGetLastError();
 }
 
+// Probe points: the caller's split K (chosen from the point count), at
+// least one point per partial slot.
 cudaError_t vx_launch_probe(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S,
                             VxWork &w, const double *px, const double *py, long long pstride,
                             long long np, double *ovx, double *ovy, long long ostride, int K) {
-    const long long tstride = w.part_cap / (2LL * K);
-    if (tstride < np) return cudaErrorInvalidValue;
+    if (K < 1 || w.part_cap / (2LL * K) < np) return cudaErrorInvalidValue;
+    VxSplit sp;
+    sp.cap = w.part_cap;
+    sp.K = K;
+    sp.sms = vx_full_sms(L);
+    sp.tile = p.prec == VX_PREC_FP32 ? 1024 : 512;
+    sp.nout = 2;
     if (maybe_pack(L, p, v, S, w) != cudaSuccess) return cudaGetLastError();
     if (p.prec == VX_PREC_FP32)
-        vx_launch<k_bs32_partial<false>, k_bs32_partial_body<false>>(L, pair_grid(L), PT, 0, p, S, w.src32, px, py, pstride, np, w.part, tstride, K);
+        vx_launch<k_bs32_partial<false>, k_bs32_partial_body<false>>(L, pair_grid(L), PT, 0, p, S, w.src32, px, py, pstride, np, w.part, sp);
     else
-        vx_launch<k_bs_partial<double, false>, k_bs_partial_body<double, false>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, px, py, pstride, np, w.part, tstride, K);
+        vx_launch<k_bs_partial<double, false>, k_bs_partial_body<double, false>>(L, pair_grid(L), PT, 0, p, v, S, nullptr, px, py, pstride, np, w.part, sp);
 
-    vx_launch<k_probe_combine, k_probe_combine_body>(L, (int)vx_ceil_div(np, 256), 256, 0, S, w.part, tstride, K, np, ovx, ovy, ostride);
+    vx_launch<k_probe_combine, k_probe_combine_body>(L, (int)vx_ceil_div(np, 256), 256, 0, S, w.part, sp, np, ovx, ovy, ostride);
 
     return cudaGetLastError();
 }

@@ -35,6 +35,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -386,18 +387,22 @@ static void collect_flight(vx_server *S) {
     cudaEventElapsedTime(&ms, f.e0, f.e1);
     S->ev_pool.push_back(f.e0);
     S->ev_pool.push_back(f.e1);
-    std::vector<vx_sim *> mem(f.members.size());
-    std::vector<double> out(5 * f.members.size());
+    const size_t room = f.members.size() + S->active.size();   // at least the batch's members at that step
+    std::vector<vx_sim *> mem(room);
+    std::vector<double> out(5 * room);
     int cnt = 0;
     const vx_status st = vx_batch_results(S->batch, f.step, mem.data(), out.data(), (int)mem.size(), &cnt);
-    for (size_t i = 0; i < f.members.size(); ++i) {
-        Request *r = f.members[i];
+    // the batch lists its members in its own order: match them by body
+    std::unordered_map<const vx_sim *, int> at;
+    for (int j = 0; st == VX_OK && j < cnt; ++j) at[mem[j]] = j;
+    for (Request *r : f.members) {
         if (r->state != 1) continue;
-        if (st != VX_OK || (int)i >= cnt || mem[i] != r->sim) {
+        const auto it = at.find(r->sim);
+        if (it == at.end()) {
             r->state = 3;
             continue;
         }
-        const double *o = out.data() + 5 * i;
+        const double *o = out.data() + 5 * it->second;
         S->step_ms.push_back(ms);
         S->body_steps += 1;
         S->particle_steps += o[0];

@@ -31,7 +31,7 @@ struct vx_sim {
     bool use_graph = true;
     struct StepGraph {
         cudaGraphExec_t exec = nullptr;
-        int kv = -1, rhs = -1, sms = -1;
+        int rhs = -1, sms = -1;
         long long launches = 0, used = 0;
     };
     StepGraph graphs[4];
@@ -65,7 +65,6 @@ long long vx_sim_need(vx_sim *s, long long n);     // slots a step starting with
 vx_status vx_sim_grow(vx_sim *s, long long need);
 vx_status vx_sim_read_scalars(vx_sim *s);
 int vx_sim_step_sms(vx_sim *s);
-int vx_sim_kv(vx_sim *s);
 int vx_sim_rhs_chunks(vx_sim *s);
 // Launch (or, with rec, record) the stages of one step; share > 0: the SMs
 // the scaled grid-stride launches are sized for (at most the body's own).

@@ -15,7 +15,8 @@
 // order), then each bucket's slots are put back in element-index order, the
 // order a stable sort by bucket gives (rank of an element = the number of
 // the bucket's elements with a lower index).  A bucket of up to 16 elements
-// takes one thread, one of up to 128 a warp, a larger one a block.  The
+// takes one thread, one of up to 128 a warp, a larger one a block (the warps
+// and blocks in one launch after the threads').  The
 // counts are used up by the placement and written back by the ordering.
 VX_DEVK void k_bk_place_body(VxBlkB<0, 0> vb, const long long *d_n, const unsigned *key, const int *start, int *cnt0,
                              const long long *d_off, unsigned *okey, int *oval) {
@@ -42,14 +43,17 @@ constexpr int BK_E = 4;   // elements per lane: a warp orders buckets of up to 3
 // BK_S elements itself (ranks by counting, in registers) and lists larger
 // ones for a warp (mid) or a block (big).
 VX_DEVK void k_bk_order_body(VxBlkB<0, 0> vb, VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
-                             int *oval, int *mid, int *big) {
+                             int *oval, int *mid, int *big, VxGather gt) {
     const long long nb = *d_nb;
     int *cnt = cnt0 + (d_off ? *d_off : 0);
     for (long long b = vb.x * (long long)blockDim.x + threadIdx.x; b < nb;
          b += (long long)vb.n * blockDim.x) {
         const int a = start[b], m = start[b + 1] - a;
-        cnt[b] = m;
-        if (m <= 1) continue;
+        cnt[b] = gt.zero_counts ? 0 : m;
+        if (m <= 1) {
+            if (m == 1 && gt.mode) vx_gather_slot(gt, a, oval[a], (unsigned)b);
+            continue;
+        }
         if (m > BK_S) {
             if (m > 32 * BK_E) big[atomicAdd(&S->bk_nbig, 1)] = (int)b;
             else mid[atomicAdd(&S->bk_nmid, 1)] = (int)b;
@@ -63,23 +67,49 @@ VX_DEVK void k_bk_order_body(VxBlkB<0, 0> vb, VxScalars *S, const long long *d_n
             int r = 0;
 #pragma unroll
             for (int k = 0; k < BK_S; ++k) r += v[k] < v[e];
-            if (e < m) oval[a + r] = v[e];
+            if (e < m) {
+                oval[a + r] = v[e];
+                if (gt.mode) vx_gather_slot(gt, a + r, v[e], (unsigned)b);
+            }
         }
     }
 }
 __global__ void k_bk_order(VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
-                           int *oval, int *mid, int *big) {
+                           int *oval, int *mid, int *big, VxGather gt) {
     VX_PDL_WAIT();
-    k_bk_order_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, d_nb, start, cnt0, d_off, oval, mid, big);
+    k_bk_order_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, d_nb, start, cnt0, d_off, oval, mid, big, gt);
 }
 
-// One warp per listed bucket of BK_S < m <= 32 BK_E elements: lane holds
-// elements lane, lane + 32, ...; each counts the smaller ones.
-VX_DEVK void k_bk_order_mid_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *start, const int *mid, int *oval) {
+// The listed buckets, one launch: a block per bucket of more than 32 BK_E
+// elements (each element counts the smaller ones, the bucket staged in
+// shared memory when it fits), then a warp per bucket of BK_S < m <= 32 BK_E
+// elements (lane holds elements lane, lane + 32, ...).
+constexpr int BK_T = 512;
+constexpr int BK_SH = 4096;   // elements of a bucket held in shared memory; larger ones go through scratch
+VX_DEVK void k_bk_order_rest_body(VxBlkB<BK_T, 0> vb, const VxScalars *S, const int *start, const int *mid,
+                                  const int *big, int *oval, int *scratch, VxGather gt) {
+    __shared__ int sv[BK_SH];
+    const int nbig = S->bk_nbig;
+    for (int q = vb.x; q < nbig; q += vb.n) {
+        const int b = big[q];
+        const int a = start[b], m = start[b + 1] - a;
+        const bool sh = m <= BK_SH;
+        int *src = sh ? sv : scratch + a;
+        for (int e = threadIdx.x; e < m; e += BK_T) src[e] = oval[a + e];
+        __syncthreads();
+        for (int e = threadIdx.x; e < m; e += BK_T) {
+            const int v = src[e];
+            int r = 0;
+            for (int k = 0; k < m; ++k) r += src[k] < v;
+            oval[a + r] = v;
+            if (gt.mode) vx_gather_slot(gt, a + r, v, (unsigned)b);
+        }
+        __syncthreads();
+    }
     const int nmid = S->bk_nmid;
     const int lane = threadIdx.x & 31;
-    const int nw = (vb.n * blockDim.x) >> 5;
-    for (int q = (vb.x * blockDim.x + threadIdx.x) >> 5; q < nmid; q += nw) {
+    const int nw = (vb.n * BK_T) >> 5;
+    for (int q = (vb.x * BK_T + threadIdx.x) >> 5; q < nmid; q += nw) {
         const int b = mid[q];
         const int a = start[b], m = start[b + 1] - a;
         int v[BK_E], r[BK_E];
@@ -102,52 +132,26 @@ VX_DEVK void k_bk_order_mid_body(VxBlkB<0, 0> vb, const VxScalars *S, const int 
         __syncwarp();
 #pragma unroll
         for (int e = 0; e < BK_E; ++e)
-            if (lane + 32 * e < m) oval[a + r[e]] = v[e];
+            if (lane + 32 * e < m) {
+                oval[a + r[e]] = v[e];
+                if (gt.mode) vx_gather_slot(gt, a + r[e], v[e], (unsigned)b);
+            }
     }
 }
-__global__ void k_bk_order_mid(const VxScalars *S, const int *start, const int *mid, int *oval) {
+__global__ void __launch_bounds__(BK_T) k_bk_order_rest(const VxScalars *S, const int *start, const int *mid,
+                                                        const int *big, int *oval, int *scratch, VxGather gt) {
     VX_PDL_WAIT();
-    k_bk_order_mid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, start, mid, oval);
-}
-
-constexpr int BK_T = 512;
-constexpr int BK_SH = 4096;   // elements of a bucket held in shared memory; larger ones go through scratch
-VX_DEVK void k_bk_order_big_body(VxBlkB<BK_T, 0> vb, const VxScalars *S, const int *start, const int *big,
-                                 int *oval, int *scratch) {
-    __shared__ int sv[BK_SH];
-    const int nbig = S->bk_nbig;
-    for (int q = vb.x; q < nbig; q += vb.n) {
-        const int b = big[q];
-        const int a = start[b], m = start[b + 1] - a;
-        const bool sh = m <= BK_SH;
-        int *src = sh ? sv : scratch + a;
-        for (int e = threadIdx.x; e < m; e += BK_T) src[e] = oval[a + e];
-        __syncthreads();
-        for (int e = threadIdx.x; e < m; e += BK_T) {
-            const int v = src[e];
-            int r = 0;
-            for (int k = 0; k < m; ++k) r += src[k] < v;
-            oval[a + r] = v;
-        }
-        __syncthreads();
-    }
-}
-__global__ void __launch_bounds__(BK_T) k_bk_order_big(const VxScalars *S, const int *start, const int *big,
-                                                       int *oval, int *scratch) {
-    VX_PDL_WAIT();
-    k_bk_order_big_body(VxBlkB<BK_T, 0>{blockIdx.x, gridDim.x}, S, start, big, oval, scratch);
+    k_bk_order_rest_body(VxBlkB<BK_T, 0>{blockIdx.x, gridDim.x}, S, start, mid, big, oval, scratch, gt);
 }
 
 cudaError_t vx_bucket_order(const VxLaunch &L, VxScalars *S, const long long *d_n, const long long *d_nbuckets,
                             const unsigned *key, const int *start, int *cnt, const long long *d_cnt_off,
-                            unsigned *okey, int *oval, int *mid, int *big, int *scratch) {
+                            unsigned *okey, int *oval, int *mid, int *big, int *scratch, const VxGather &gt) {
     vx_launch<k_bk_place, k_bk_place_body>(L, L.num_sms * 4, 256, 0, d_n, key, start, cnt, d_cnt_off, okey, oval);
 
-    vx_launch<k_bk_order, k_bk_order_body>(L, L.num_sms * 4, 256, 0, S, d_nbuckets, start, cnt, d_cnt_off, oval, mid, big);
+    vx_launch<k_bk_order, k_bk_order_body>(L, L.num_sms * 4, 256, 0, S, d_nbuckets, start, cnt, d_cnt_off, oval, mid, big, gt);
 
-    vx_launch<k_bk_order_mid, k_bk_order_mid_body>(L, L.num_sms * 8, 256, 0, S, start, mid, oval);
-
-    vx_launch<k_bk_order_big, k_bk_order_big_body>(L, L.num_sms, BK_T, 0, S, start, big, oval, scratch);
+    vx_launch<k_bk_order_rest, k_bk_order_rest_body>(L, L.num_sms * 4, BK_T, 0, S, start, mid, big, oval, scratch, gt);
 
     return cudaGetLastError();
 }

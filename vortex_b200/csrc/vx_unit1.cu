@@ -343,10 +343,8 @@ int Speed(vxu_vortex *pos, double (*v_inf)[2], size_t s, vxu_velocity *v, double
     ++U.launches;
     const VxLaunch L = launch0();
     const VxView vw = aos_view(pos, v, d);
-    const int tile = U.prm.prec == VX_PREC_FP32 ? 1024 : 512;
-    const int K = vx_pick_ksplit((long long)s, tile, U.num_sms);
-    CK(vx_launch_velocity(L, U.prm, vw, U.d_S, U.w, K));
-    CK(vx_launch_diffusion(L, U.prm, vw, U.d_S, U.w, K));
+    CK(vx_launch_velocity(L, U.prm, vw, U.d_S, U.w));
+    CK(vx_launch_diffusion(L, U.prm, vw, U.d_S, U.w));
     CK(vx_launch_wall(L, U.prm, vw, U.d_S, panels));
     CK(cudaDeviceSynchronize());
     return 0;
@@ -389,7 +387,7 @@ int velocity_control(vxu_vortex *pos, double (*V_inf)[2], size_t n, vxu_vortex *
     const double *px = (const double *)Contr_points;
     double *ov = (double *)V;
     const int tile = U.prm.prec == VX_PREC_FP32 ? 1024 : 512;
-    const int K = vx_pick_ksplit((long long)n_contr, tile, U.num_sms);
+    const int K = vx_ksplit((long long)n_contr, tile, U.num_sms);
     CK(vx_launch_probe(launch0(), U.prm, aos_view(pos, nullptr, nullptr), U.d_S, U.w, px, px + 1, 3,
                        (long long)n_contr, ov, ov + 1, 2, K));
     CK(cudaDeviceSynchronize());
@@ -502,7 +500,7 @@ int64_t vxu_launch_count(void) { return U.launches; }
 //     array and must be serialised by the caller.
 namespace {
 constexpr long long NA_MAX_POINTS = 4096;   // control points per call
-constexpr int NA_MAX_SPLIT = 64;            // source splits (vx_pick_ksplit's cap)
+constexpr int NA_MAX_SPLIT = 64;            // source splits (vx_ksplit's cap)
 constexpr long long NA_HEAD = ((long long)sizeof(VxScalars) + 255) / 256 * 256 / (long long)sizeof(double);
 constexpr long long NA_PART = 2LL * NA_MAX_SPLIT * NA_MAX_POINTS;
 constexpr long long NA_WORDS = NA_HEAD + NA_PART;   // 4 MiB + the scalars
@@ -575,7 +573,7 @@ extern "C" int velocity_control_noalloc(vxu_vortex *pos, double (*V_inf)[2], siz
     ++U.launches;
     const double *px = (const double *)Contr_points;
     double *ov = (double *)V;
-    const int K = vx_pick_ksplit((long long)n_contr, 512, d->num_sms);
+    const int K = vx_ksplit((long long)n_contr, 512, d->num_sms);
     CK(vx_launch_probe(L, prm, aos_view(pos, nullptr, nullptr), S, w, px, px + 1, 3, (long long)n_contr, ov,
                        ov + 1, 2, K));
     CK(cudaDeviceSynchronize());
