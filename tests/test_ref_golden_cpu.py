@@ -2,13 +2,22 @@
 build (tests/golden/ref_*.npz, made by tests/golden/make_ref_goldens.py on a
 B200 with oracle/_ref/libvortex_ref.so).
 
-Each recorded step is replayed stage by stage from the reference's own state:
-  * birth: positions exact; strengths within 1e-6 relative (the reference
-    sums the right-hand side in FP32);
+Cases: the 200-panel circle of configuration 1 (steps 1, 4, 30), a mixed
+run (steps 2, 20) and the reference's own 1000-panel circle profile
+(krug_1000, steps 2 and 6).  Each recorded step is replayed stage by stage
+from the reference's own state:
+  * birth: positions exact; strengths within 1e-6 of the largest, or, where
+    the reference's FP32 right-hand side is further from the FP64 one (at
+    1000 panels its sums over the wake differ from FP64 by up to 2e-3 of the
+    largest strength), at least three times closer to the reference than the
+    FP64 evaluation (the oracle repeats the reference's FP32 terms; only the
+    order of accumulation differs);
   * velocity in the oracle's reference-precision mode: 3-nearest distance d
     bit-exact, velocity within 5e-5 absolute (FP32 sums, exp/atan differences);
     in FP64 mode within 2e-3 (the reference's FP32 rounding, amplified by the
-    diffusion quotient I2/I1 near cancellations);
+    diffusion quotient I2/I1 near cancellations), and d within the FP32
+    rounding of the coordinates it is computed from, 4 eps32 (|x| + |y|) plus
+    1e-7 of d;
   * convection, sums, compaction and both collapse passes from the
     reference's own velocities: the same count, identical strengths,
     positions within 2 ulp (the reference's compiler fuses some products),
@@ -24,7 +33,8 @@ from oracle import oracle as O
 from vortex_b200 import profiles
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-CASES = [("cfg1", k) for k in (1, 4, 30)] + [("mixed", k) for k in (2, 20)]
+CASES = ([("cfg1", k) for k in (1, 4, 30)] + [("mixed", k) for k in (2, 20)]
+         + [("krug1000", k) for k in (2, 6)])
 
 
 def load(name):
@@ -56,7 +66,11 @@ def test_birth_matches_reference(name, k):
     R = O.birth_rhs(p, pan, pre[:n0, 0], pre[:n0, 1], pre[:n0, 2])
     bx, by, bg = O.birth_place(p, pan, O.birth_gamma(M, R, dg))
     assert np.array_equal(bx, born[n0:n0 + P, 0]) and np.array_equal(by, born[n0:n0 + P, 1])
-    assert np.abs(bg - born[n0:n0 + P, 2]).max() <= 1e-6 * np.abs(born[n0:n0 + P, 2]).max()
+    ref = born[n0:n0 + P, 2]
+    R64 = O.birth_rhs(params(c, O.PREC_FP64), pan, pre[:n0, 0], pre[:n0, 1], pre[:n0, 2])
+    bg64 = O.birth_place(params(c, O.PREC_FP64), pan, O.birth_gamma(M, R64, dg))[2]
+    bound = max(1e-6 * np.abs(ref).max(), np.abs(bg64 - ref).max() / 3)
+    assert np.abs(bg - ref).max() <= bound, (np.abs(bg - ref).max(), bound)
     assert np.array_equal(born[:n0], pre[:n0])
 
 
@@ -77,7 +91,8 @@ def test_velocity_matches_reference(name, k, prec):
         assert np.array_equal(dd, d[:n]), "FP32 3-nearest distance must match the reference bit for bit"
         assert err < 5e-5
     else:
-        assert np.abs(dd - d[:n]).max() < 2e-6 * d[:n].max()
+        eps32 = 2.0 ** -24
+        assert np.all(np.abs(dd - d[:n]) <= 4 * eps32 * (np.abs(x[:n]) + np.abs(y[:n])) + 1e-7 * d[:n])
         assert err < 2e-3
 
 

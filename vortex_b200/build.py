@@ -26,6 +26,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "-I" + os.path.join(HERE, "..", "include")]
+# Build knobs for measuring kernel variants, e.g.
+#   VX_NVCC_DEFS="-DVX_DIFF_POLY_EVERY=4" python -m vortex_b200.build --force
+FLAGS += os.environ.get("VX_NVCC_DEFS", "").split()
 CLI_SOURCES = {"vortex_cli.cpp"}
 
 
