@@ -245,6 +245,9 @@ vx_status vx_server_tick(vx_server *srv, int64_t *active, int64_t *queued);
  * per completed step, at most cap_steps steps copied. */
 vx_status vx_server_result(vx_server *srv, int64_t id, int *state, int64_t *steps_done, double *forces,
                            int64_t cap_steps, int64_t *n_final);
+/* Why a failed request (state 3) failed: the first error met, as text
+ * (empty otherwise), NUL-terminated within cap bytes. */
+vx_status vx_server_failure(vx_server *srv, int64_t id, char *buf, int64_t cap);
 /* out[0] finished, [1]/[2] p50/p99 body-step device ms, [3]/[4] p50/p99
  * submit-to-finish s, [5] mean resident bodies per tick, [6] body steps,
  * [7] particle steps, [8] bytes reserved now, [9] ticks. */

@@ -50,7 +50,10 @@ class FakeServer:
 
     def result(self, rid):
         r = self.res[rid]
-        return {"state": r["state"], "steps": r["steps"], "forces": np.zeros((r["steps"], 4)), "n_final": 0}
+        out = {"state": r["state"], "steps": r["steps"], "forces": np.zeros((r["steps"], 4)), "n_final": 0}
+        if r["state"] == "failed":
+            out["error"] = "creation: out of memory"
+        return out
 
     def stats(self):
         return {"finished": sum(r["state"] == "done" for r in self.res.values()), "step_ms_p50": 1.0,

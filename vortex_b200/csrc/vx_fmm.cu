@@ -634,7 +634,7 @@ __device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gsl
 }
 
 #ifndef VX_NEAR_MINB
-#define VX_NEAR_MINB 1   // minimum resident blocks per SM requested for k_fmm_near
+#define VX_NEAR_MINB 2   // minimum resident blocks per SM requested for k_fmm_near (at most 128 registers)
 #endif
 template <int P>
 VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
@@ -684,16 +684,29 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
             rpre[r + 1] = rpre[r] + len;
         }
         const int total = rpre[3];
+        // source f of the stream: its slot in the leaf-sorted array and the
+        // y offset of its row; the x offset of its column, (column - col) h
+        // with the difference -1, 0 or 1, is exact in FP32
+        const float hf = (float)h, colf = (float)col;
+        auto src_of = [&](int f, float &oy) {
+            const bool in0 = f < rpre[1], in1 = f < rpre[2];
+            oy = in0 ? roy[0] : (in1 ? roy[1] : roy[2]);
+            return in0 ? rj0[0] + f : (in1 ? rj0[1] + (f - rpre[1]) : rj0[2] + (f - rpre[2]));
+        };
+        // the next chunk's source is loaded before the current chunk's pairs run
+        float4 qn = make_float4(1e12f, 1e12f, 0.f, colf);
+        float oyn = 0.f;
+        if (lane < total) qn = srt[src_of(lane, oyn)];
         for (int jt = 0; jt < total; jt += 32) {
             // padding: G = 0 sources far away add exactly 0
+            const float4 q = qn;
+            const float oy = oyn;
+            const int fnext = jt + 32 + lane;
+            if (fnext < total) qn = srt[src_of(fnext, oyn)];
             float x = 1e12f, y = 1e12f, g = 0.f;
-            const int f = jt + lane;
-            if (f < total) {
-                const bool in0 = f < rpre[1], in1 = f < rpre[2];
-                const int j = in0 ? rj0[0] + f : (in1 ? rj0[1] + (f - rpre[1]) : rj0[2] + (f - rpre[2]));
-                const float4 q = srt[j];
-                x = q.x + (float)(((double)q.w - (double)col) * h);
-                y = q.y + (in0 ? roy[0] : (in1 ? roy[1] : roy[2]));
+            if (jt + lane < total) {
+                x = q.x + (q.w - colf) * hf;
+                y = q.y + oy;
                 g = q.z;
             }
             float *slot = reinterpret_cast<float *>(wxy + (lane >> 1));

@@ -64,6 +64,7 @@ struct Request {
     bool inflight = false;    // a step launched and not yet collected
     vx_status create_st = VX_OK;   // set by the worker thread
     std::string create_err;        // the worker's error text when create_st != VX_OK
+    std::string err;               // why the request failed (state 3)
     int64_t done_steps = 0;
     int64_t launched = 0;     // steps launched (batched form)
     bool in_batch = false;
@@ -118,11 +119,17 @@ struct vx_server {
 };
 
 // Launch the next step of resident body r on its stream, between its events.
+// A request fails: state 3, with the first reason kept.
+static void fail(Request *r, const std::string &why) {
+    r->state = 3;
+    if (r->err.empty()) r->err = why;
+}
+
 static void launch_step(vx_server *S, Request *r) {
     cudaStream_t st = (cudaStream_t)vx_get_stream(r->sim);
     cudaEventRecord(r->e0, st);
     if (vx_step(r->sim, 1) != VX_OK) {
-        r->state = 3;
+        fail(r, std::string("step: ") + vx_last_error());
         return;
     }
     cudaEventRecord(r->e1, st);
@@ -136,7 +143,7 @@ static void collect_step(vx_server *S, Request *r) {
     cudaEventElapsedTime(&ms, r->e0, r->e1);
     double st9[9];
     if (vx_get_state(r->sim, st9) != VX_OK) {
-        r->state = 3;
+        fail(r, std::string("state: ") + vx_last_error());
         return;
     }
     const int64_t n = (int64_t)st9[0];
@@ -277,7 +284,7 @@ static void take_created(vx_server *S) {
             vx_set_error("request %lld: body creation failed: %s", (long long)r->id,
                          r->create_err.empty() ? vx_status_str(r->create_st) : r->create_err.c_str());
             release(S, r);
-            r->state = 3;
+            fail(r, "creation: " + (r->create_err.empty() ? std::string(vx_status_str(r->create_st)) : r->create_err));
             r->t_finish = now_s();
             continue;
         }
@@ -356,7 +363,7 @@ static void tick_streams(vx_server *S) {
                 if (r->state == 1) launch_step(S, r);
             } else if (q != cudaErrorNotReady) {
                 r->inflight = false;
-                r->state = 3;
+                fail(r, std::string("step event: ") + cudaGetErrorString(q));
             }
         }
     }
@@ -399,7 +406,8 @@ static void collect_flight(vx_server *S) {
         if (r->state != 1) continue;
         const auto it = at.find(r->sim);
         if (it == at.end()) {
-            r->state = 3;
+            fail(r, st != VX_OK ? std::string("batch results: ") + vx_last_error()
+                                : std::string("batch results: body not among the step's members"));
             continue;
         }
         const double *o = out.data() + 5 * it->second;
@@ -429,7 +437,10 @@ static vx_status tick_batched(vx_server *S) {
     while (S->flight.size() < 2) {
         for (Request *r : S->active) {
             if (r->state == 1 && !r->in_batch && r->launched < r->steps) {
-                if (vx_batch_add(S->batch, r->sim) != VX_OK) { r->state = 3; continue; }
+                if (vx_batch_add(S->batch, r->sim) != VX_OK) {
+                    fail(r, std::string("batch add: ") + vx_last_error());
+                    continue;
+                }
                 r->in_batch = true;
             }
             if (r->in_batch && (r->launched >= r->steps || r->state != 1)) {
@@ -449,7 +460,8 @@ static vx_status tick_batched(vx_server *S) {
         vx_batch_info(S->batch, info);
         f.step = (int64_t)info[0];
         if (vx_batch_step(S->batch, 1) != VX_OK) {
-            for (Request *r : f.members) r->state = 3;
+            const std::string why = std::string("batch step: ") + vx_last_error();
+            for (Request *r : f.members) fail(r, why);
             S->ev_pool.push_back(f.e0);
             S->ev_pool.push_back(f.e1);
             break;
@@ -547,6 +559,18 @@ extern "C" vx_status vx_server_result(vx_server *S, int64_t id, int *state, int6
         std::memcpy(forces, r->forces.data(), sizeof(double) * 4 * (size_t)k);
     }
     if (n_final) *n_final = r->n_final;
+    return VX_OK;
+}
+
+// Why request `id` failed ("" unless its state is 3), NUL-terminated in buf.
+extern "C" vx_status vx_server_failure(vx_server *S, int64_t id, char *buf, int64_t cap) {
+    if (!S || !buf || cap < 1) return VX_ERR_ARG;
+    auto it = S->all.find(id);
+    if (it == S->all.end()) return VX_ERR_ARG;
+    const std::string &e = it->second->err;
+    const size_t k = std::min<size_t>(e.size(), (size_t)(cap - 1));
+    std::memcpy(buf, e.data(), k);
+    buf[k] = 0;
     return VX_OK;
 }
 

@@ -193,6 +193,7 @@ def run_serve(requests: int = 32, rate: float = 50.0, budget_gb: float = 160.0, 
                          if batched else "each resident body on its own stream"),
             "seed": seed, "precision": "fp32" if precision == N.PREC_FP32 else "fp64",
             "steps_requested": int(nsteps.sum()), "failed": sum(r["state"] == "failed" for r in res),
+            "failures": sorted({r["error"] for r in res if r["state"] == "failed"})[:4],
             "wall_s": wall, "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"],
             "ttc_s_p50": st["ttc_s_p50"], "ttc_s_p99": st["ttc_s_p99"], "mean_resident": st["mean_resident"],
             "body_steps": st["body_steps"], "body_steps_per_s": st["body_steps"] / wall,

@@ -482,7 +482,12 @@ class Server:
         if k:
             _check(lib().vx_server_result(self.h, C.c_int64(rid), C.byref(st), C.byref(done), _p(f),
                                           C.c_int64(k), C.byref(nf)), "vx_server_result")
-        return {"state": self.STATES[st.value], "steps": done.value, "forces": f[:k], "n_final": nf.value}
+        out = {"state": self.STATES[st.value], "steps": done.value, "forces": f[:k], "n_final": nf.value}
+        if out["state"] == "failed":
+            buf = C.create_string_buffer(512)
+            _check(lib().vx_server_failure(self.h, C.c_int64(rid), buf, C.c_int64(512)), "vx_server_failure")
+            out["error"] = buf.value.decode(errors="replace")
+        return out
 
     def stats(self) -> dict:
         o = np.zeros(10)
