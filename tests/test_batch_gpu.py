@@ -79,10 +79,13 @@ def test_batch_matches_bodies_stepped_alone():
                 assert np.array_equal(sa[q], sm[q]), f"body {k}: {name} differs"
     # somebody outgrew its store inside the batch
     assert any(s.device_bytes() > c for s, c in zip(mine, caps0))
-    # one launch per kernel of the step for all bodies, not one per body
+    # one launch per kernel of the step for all bodies, not one per body: the
+    # plain FP64 body's direct sums and the bulk bodies' quadtree and grid
+    # passes are different kernels, so the batch's step is their union, at
+    # most two bodies' worth (four bodies alone would be four)
     assert info["steps"] == steps
-    assert info["kernels_per_step"] <= 1.5 * per_body, (info, per_body)
-    assert info["kernels"] <= steps * 1.5 * per_body
+    assert info["kernels_per_step"] <= 2 * per_body, (info, per_body)
+    assert info["kernels"] <= steps * 2 * per_body
     # back on their own streams the bodies step alone again, still in step
     for a, m in zip(alone, mine):
         a.step(2)

@@ -483,17 +483,23 @@ static void update_share(vx_batch *b) {
 }
 
 // Room for `nb` members in the gathered results (the device array is
-// stream-ordered: steps in flight still write the old one).
+// stream-ordered: steps in flight still write the old one).  The host copies
+// of the last two steps' results are carried over into the larger buffers,
+// so a step that is still to be collected keeps its results.
 static vx_status gather_room(vx_batch *b, size_t nb) {
     if (nb <= b->gather_cap && b->d_gather) return VX_OK;
     size_t cap = std::max<size_t>(std::max<size_t>(nb, 2 * b->gather_cap), 16);
     for (int k = 0; k < 2; ++k) {
         BCU(cudaEventSynchronize(b->cnt_ev[k]));   // its last copy has landed
-        if (b->h_gather[k]) cudaFreeHost(b->h_gather[k]);
-        b->h_gather[k] = nullptr;
-        b->cnt_step[k] = -1;
-        b->cnt_members[k].clear();
-        BCU(cudaMallocHost(&b->h_gather[k], sizeof(double) * GATHER * cap));
+        double *old = b->h_gather[k];
+        double *grown = nullptr;
+        BCU(cudaMallocHost(&grown, sizeof(double) * GATHER * cap));
+        if (old) {
+            const size_t keep = std::min(b->cnt_members[k].size(), b->gather_cap);
+            memcpy(grown, old, sizeof(double) * GATHER * keep);
+            cudaFreeHost(old);
+        }
+        b->h_gather[k] = grown;
     }
     if (b->d_gather) BCU(cudaFreeAsync(b->d_gather, b->stream));
     b->d_gather = nullptr;

@@ -19,8 +19,12 @@
 // array, staged through the warp's shared memory 32 sources at a time.  A
 // target whose radius exceeds CG_KCAP cells (an isolated vortex with a large
 // d) would widen its warp's window for all 32 targets; it is left out of the
-// window and summed alone by one warp (k_diff_wide).  Each target is owned by
-// one warp, so the velocity is updated in place with no partial sums.
+// window and summed alone by one warp (k_diff_wide).  So is a target more
+// than 64 d from its item's first cell (items of a row that crosses the body
+// hold targets on both sides of it): the item's frame would cost it FP32
+// digits (an error of order |offset| 6e-8 / d), its own cell's frame does
+// not.  Each target is owned by one warp, so the velocity is updated in place
+// with no partial sums.
 #include "vx_internal.cuh"
 
 constexpr int CG_T = 256;
@@ -360,7 +364,12 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
         const long long ocol = (long long)key0 - row * nx;
         if (valid) me.x += (float)(int)(skey[t] - key0) * h;   // as for the sources below
         const float R = cut * me.w;
-        const bool is_wide = valid && R > (float)CG_KCAP * h;
+        // a target far from the item's first cell (an item whose row crosses
+        // the body holds targets on both sides of it) would lose FP32 digits
+        // in the item's frame: beyond 64 d it is summed alone, in the frame
+        // of its own cell, as the wide targets are
+        const bool far_frame = valid && fabsf((float)(int)(skey[t] - key0)) * h > 64.0f * me.w;
+        const bool is_wide = valid && (R > (float)CG_KCAP * h || far_frame);
         if (is_wide) wide[atomicAdd(&S->cnwide, 1)] = (int)t;
         const bool act = valid && !is_wide;
         float rmax = act ? R : 0.0f, xlo = act ? me.x : 3e38f, xhi = act ? me.x : -3e38f;

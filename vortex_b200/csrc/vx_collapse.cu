@@ -148,31 +148,39 @@ __global__ void __launch_bounds__(VX_SCAN_T) k_col_scan(VxScalars *S, const int 
 }
 
 // Each cell's slots from its start, counting its count back down to zero
-// (the zero the next pass's count starts from).
-VX_DEVK void k_col_scatter_body(VxBlkB<0, 0> vb, const VxScalars *S, const int *cellid, const int *start, int *cnt,
-                                int *sorted) {
+// (the zero the next pass's count starts from); the slot gets the vortex's
+// index and a copy of its position and strength, so that the query reads
+// its candidates as contiguous runs.
+VX_DEVK void k_col_scatter_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *cellid, const int *start,
+                                int *cnt, int *sorted, double *xs, double *ys, double *gs) {
     if (S->col_done) return;
     const long long n = S->n;
     for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)vb.n * blockDim.x) {
         const int c = cellid[i];
-        const int k = atomicSub(&cnt[c], 1) - 1;
-        sorted[start[c] + k] = (int)i;
+        const int k = start[c] + atomicSub(&cnt[c], 1) - 1;
+        sorted[k] = (int)i;
+        xs[k] = v.x[i * v.ps];
+        ys[k] = v.y[i * v.ps];
+        gs[k] = v.g[i * v.ps];
     }
 }
-__global__ void k_col_scatter(const VxScalars *S, const int *cellid, const int *start, int *cnt,
-                              int *sorted) {
+__global__ void k_col_scatter(VxView v, const VxScalars *S, const int *cellid, const int *start, int *cnt,
+                              int *sorted, double *xs, double *ys, double *gs) {
     VX_PDL_WAIT();
-    k_col_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, cellid, start, cnt, sorted);
+    k_col_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cellid, start, cnt, sorted, xs, ys, gs);
 }
 
 // COL[i] = smallest j > i in the 3x3 cell neighbourhood that qualifies.  The
-// targets are taken in cell order (i = sorted[k]), so neighbouring threads
-// read the same cells and sources; each target's answer does not depend on
-// the order.
+// targets are taken in cell order (slot k0 of the cell-sorted copy), so
+// neighbouring threads read the same cells and sources, all as contiguous
+// runs of the copy (a row's three cells are one run); each target's answer
+// does not depend on the order.  The target's cell is recomputed from its
+// position by the count's expression.
 template <int PASS>
-VX_DEVK void k_col_query_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
-                              const int *sorted, int *col, int *in_cnt, int *cand) {
+VX_DEVK void k_col_query_body(VxBlkB<0, 0> vb, VxParams p, VxScalars *S, const int *start, const int *sorted,
+                              const double *xs, const double *ys, const double *gs, int *col, int *in_cnt,
+                              int *cand) {
     if (S->col_done) return;
     const long long n = S->n;
     const long long gnx = S->gnx, gny = S->gny;
@@ -180,24 +188,23 @@ VX_DEVK void k_col_query_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *
     for (long long k0 = vb.x * (long long)blockDim.x + threadIdx.x; k0 < n;
          k0 += (long long)vb.n * blockDim.x) {
         const long long i = sorted[k0];
-        const double xi = v.x[i * v.ps], yi = v.y[i * v.ps], gi = v.g[i * v.ps];
-        const long long c = cellid[i];
-        const long long cx = c % gnx, cy = c / gnx;
+        const double xi = xs[k0], yi = ys[k0], gi = gs[k0];
+        long long cx, cy;
+        vx_cell_of(S, xi, yi, cx, cy);
         int best = INT_MAX;
         for (long long yy = max(cy - 1, 0LL); yy <= min(cy + 1, gny - 1); ++yy) {
-            for (long long xx = max(cx - 1, 0LL); xx <= min(cx + 1, gnx - 1); ++xx) {
-                const long long cc = yy * gnx + xx;
-                for (int k = start[cc]; k < start[cc + 1]; ++k) {
-                    const int j = sorted[k];
-                    if (j <= i || j >= best) continue;
-                    const double gj = v.g[(long long)j * v.ps];
-                    const double dx = xi - v.x[(long long)j * v.ps], dy = yi - v.y[(long long)j * v.ps];
-                    const double r2 = fma(dx, dx, dy * dy);
-                    bool ok;
-                    if (PASS == 1) ok = (gi * gj < 0) && (r2 < rd2);
-                    else ok = (gi * gj > 0) && (r2 < rs2) && (fabs(gi + gj) < mvg);
-                    if (ok) best = j;
-                }
+            const long long r0 = yy * gnx;
+            const int k1 = start[r0 + min(cx + 1, gnx - 1) + 1];
+            for (int k = start[r0 + max(cx - 1, 0LL)]; k < k1; ++k) {
+                const int j = sorted[k];
+                if (j <= i || j >= best) continue;
+                const double gj = gs[k];
+                const double dx = xi - xs[k], dy = yi - ys[k];
+                const double r2 = fma(dx, dx, dy * dy);
+                bool ok;
+                if (PASS == 1) ok = (gi * gj < 0) && (r2 < rd2);
+                else ok = (gi * gj > 0) && (r2 < rs2) && (fabs(gi + gj) < mvg);
+                if (ok) best = j;
             }
         }
         if (best != INT_MAX) {
@@ -211,10 +218,10 @@ VX_DEVK void k_col_query_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *
     }
 }
 template <int PASS>
-__global__ void k_col_query(VxParams p, VxView v, VxScalars *S, const int *cellid, const int *start,
-                            const int *sorted, int *col, int *in_cnt, int *cand) {
+__global__ void k_col_query(VxParams p, VxScalars *S, const int *start, const int *sorted, const double *xs,
+                            const double *ys, const double *gs, int *col, int *in_cnt, int *cand) {
     VX_PDL_WAIT();
-    k_col_query_body<PASS>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, v, S, cellid, start, sorted, col, in_cnt, cand);
+    k_col_query_body<PASS>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, S, start, sorted, xs, ys, gs, col, in_cnt, cand);
 }
 
 // Settles the candidates in one block: rounds over the candidate list decide
@@ -313,12 +320,14 @@ cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxVie
         vx_launch<k_col_prep, k_col_prep_body>(L, grid, VX_THREADS, 0, v, S, cc == 0, r2, w.cells_cap, w.box);
         vx_launch<k_col_count, k_col_count_body>(L, grid, VX_THREADS, 0, v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app, w.first_app);
         vx_launch<k_col_scan, k_col_scan_body>(L, grid, VX_SCAN_T, 0, S, w.cell_cnt, w.cell_start, w.scan_tiles);
-        vx_launch<k_col_scatter, k_col_scatter_body>(L, grid, VX_THREADS, 0, S, w.cellid, w.cell_start, w.cell_cnt, w.sorted);
+        // the cell-sorted copy lives in the compaction's scratch (free until
+        // the round's compaction)
+        vx_launch<k_col_scatter, k_col_scatter_body>(L, grid, VX_THREADS, 0, v, S, w.cellid, w.cell_start, w.cell_cnt, w.sorted, w.hx, w.hy, w.hg);
         if (pass == 1) {
-            vx_launch<k_col_query<1>, k_col_query_body<1>>(L, grid, VX_THREADS, 0, p, v, S, w.cellid, w.cell_start, w.sorted, w.col, w.in_cnt, w.cand);
+            vx_launch<k_col_query<1>, k_col_query_body<1>>(L, grid, VX_THREADS, 0, p, S, w.cell_start, w.sorted, (const double *)w.hx, (const double *)w.hy, (const double *)w.hg, w.col, w.in_cnt, w.cand);
             vx_launch<k_col_settle<1>, k_col_settle_body<1>>(L, 1, 1024, 0, v, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec, w.mx, w.my, w.mg);
         } else {
-            vx_launch<k_col_query<2>, k_col_query_body<2>>(L, grid, VX_THREADS, 0, p, v, S, w.cellid, w.cell_start, w.sorted, w.col, w.in_cnt, w.cand);
+            vx_launch<k_col_query<2>, k_col_query_body<2>>(L, grid, VX_THREADS, 0, p, S, w.cell_start, w.sorted, (const double *)w.hx, (const double *)w.hy, (const double *)w.hg, w.col, w.in_cnt, w.cand);
             vx_launch<k_col_settle<2>, k_col_settle_body<2>>(L, 1, 1024, 0, v, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec, w.mx, w.my, w.mg);
         }
         vx_launch_compact_skip(L, p, v, S, w, &S->col_done);

@@ -294,11 +294,15 @@ __device__ __forceinline__ void fmm_m2m_cell(const cplx (*se)[P], int *cnt, cplx
         for (int q = 0; q < 4; ++q) {
             const long long child = (2 * iy + (q >> 1)) * m2 + 2 * ix + (q & 1);
             if (nq[q] == 0) continue;
-            double sc = 1.0;   // 2^-mm
-            for (int mm = 0; mm <= k; ++mm) {
-                const double2 t = __ldcg(reinterpret_cast<const double2 *>(&Mc[child * P + mm]));
-                b = cadd(b, cscale(cmul(se[q][k - mm], cplx{t.x, t.y}), sc));
-                sc *= 0.5;
+            // unrolled over the P terms (those above k predicated off), so
+            // the child's coefficients are loaded together, not one L2
+            // round trip per term
+#pragma unroll
+            for (int mm = 0; mm < P; ++mm) {
+                if (mm <= k) {
+                    const double2 t = __ldcg(reinterpret_cast<const double2 *>(&Mc[child * P + mm]));
+                    b = cadd(b, cscale(cmul(se[q][k - mm], cplx{t.x, t.y}), ldexp(1.0, -mm)));
+                }
             }
         }
     }
@@ -504,7 +508,9 @@ __device__ __forceinline__ cplx l2l_term(const cplx *Lp, const cplx (*se)[P], lo
     const long long parent = (iy >> 1) * (m >> 1) + (ix >> 1);
     const int q = (int)((iy & 1) * 2 + (ix & 1));
     cplx acc = {0.0, 0.0};
-    for (int j = lc; j < P; ++j) acc = cadd(acc, cmul(Lp[parent * P + j], se[q][j - lc]));
+#pragma unroll
+    for (int j = 0; j < P; ++j)   // unrolled, the terms below lc predicated off: the loads issue together
+        if (j >= lc) acc = cadd(acc, cmul(Lp[parent * P + j], se[q][j - lc]));
     return cscale(acc, ldexp(1.0, -lc));
 }
 
@@ -776,18 +782,21 @@ VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S, con
         float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
         const int y0 = max(iy2 - 1, 0), y1 = min(iy2 + 1, m2 - 1);
         const int x0 = max(ix2 - 1, 0), x1 = min(ix2 + 1, m2 - 1);
+        // a source's offset to the target's leaf centre: (its leaf's column -
+        // col) h and (its leaf's row - row) h, differences of -1, 0 or 1, so
+        // exact in FP32 and the same for every source of a quarter
+        const float hf = (float)h;
         for (int Y2 = y0; Y2 <= y1; ++Y2) {
             const int lr = Y2 >> 1;
-            const float oy = (float)((double)(lr - row) * h);
+            const float oy = (float)(lr - row) * hf;
             for (int X2 = x0; X2 <= x1; ++X2) {
+                const float ox = (float)((X2 >> 1) - col) * hf;
                 const int k = 4 * (lr * m + (X2 >> 1)) + 2 * (Y2 & 1) + (X2 & 1);
                 const int q1 = substart[k + 1];
                 for (int qq = substart[k]; qq < q1; ++qq) {
                     if (qq == t) continue;
-                    const float4 q = srt[qq];
-                    const float x = q.x + (float)(((double)q.w - (double)col) * h);
-                    const float y = q.y + oy;
-                    const float dx = me.x - x, dy = me.y - y;
+                    const float2 q = *reinterpret_cast<const float2 *>(srt + qq);   // x, y of the source
+                    const float dx = me.x - (q.x + ox), dy = me.y - (q.y + oy);
                     vx_nn3_insert_bf(d1, d2, d3, fmaf(dx, dx, dy * dy));
                 }
             }
