@@ -80,11 +80,11 @@ typedef struct vx_conf {
     int32_t birth_offset_mode;  /* VX_BIRTH_* ; default VX_BIRTH_REF */
     double drop_eps;            /* |G| below this is removed; default 1e-12 */
     double diff_cutoff;         /* bulk form: vortex diffusion ignores pairs
-                                   with r > diff_cutoff * d_i (default 20:
-                                   each such term weighs below e^-20 = 2e-9,
-                                   together about (c+1) e^-c = 4e-8 of the
-                                   sum in a uniform cloud, below its FP32
-                                   rounding) */
+                                   with r > diff_cutoff * d_i (default 16:
+                                   each such term weighs below e^-16 = 1.1e-7,
+                                   together about (c+1) e^-c = 2e-6 of the
+                                   sum's magnitude in a uniform cloud, within
+                                   the bulk form's per-particle bound) */
     int32_t n_probes_grid;      /* >0: probes on an n x n grid (box below) */
     int32_t pad1_;
     double probe_box[4];        /* x0, x1, y0, y1 of the probe grid */

@@ -5,7 +5,10 @@ Each golden step (tests/golden/ref_*.npz, recorded from the reference's CUDA
 build) is fed through vort_creation / Speed / Step / velocity_control on AoS
 device arrays exactly as the reference's src/main.c passes them:
   * birth: positions exact, strengths within 1e-10 of the FP64 oracle and
-    1e-5 of the reference (which sums its right-hand side in FP32);
+    1e-5 of the reference (which sums its right-hand side in FP32), or, where
+    the reference's FP32 sums depart further from FP64 (its 1000-panel
+    circle: up to 2e-3 of the largest strength), no further from the
+    reference than the FP64 oracle is;
   * Speed: d bit-exact and velocity within 1e-12 of the FP64 oracle, within
     2e-3 of the reference;
   * Step on the reference's own velocities: the reference's count, identical
@@ -156,7 +159,9 @@ def test_unit1_entry_points_replay_reference(name, k):
     assert np.array_equal(born[n0:n, 0], bx) and np.array_equal(born[n0:n, 1], by)
     assert np.abs(born[n0:n, 2] - bg).max() <= 1e-10 * np.abs(bg).max()
     # the reference sums its right-hand side in FP32
-    assert np.abs(born[n0:n, 2] - born_ref[n0:n, 2]).max() <= 1e-5 * np.abs(bg).max()
+    ref_gap = np.abs(bg - born_ref[n0:n, 2]).max()
+    assert np.abs(born[n0:n, 2] - born_ref[n0:n, 2]).max() <= max(1e-5 * np.abs(bg).max(),
+                                                                  ref_gap + 1e-10 * np.abs(bg).max())
     # --- Speed on the reference's post-birth state
     buf[:s] = born_ref
     pos.put(buf)

@@ -659,7 +659,7 @@ __device__ __forceinline__ float vx_half_log_ratio(float r0, float r1, float num
 }
 
 // Direct FP32 panel terms over the near list (chunked like k_rhs_partial).
-VX_DEVK void k_rhs_near_body(VxBlkB<RHS_T, 0> vb, const VxScalars *S, const vx_panel *pan, int P, int P32,
+VX_DEVK void k_rhs_near_body(VxBlkB<RHS_T, 8> vb, const VxScalars *S, const vx_panel *pan, int P, int P32,
                              const float4 *near, double *part, int sms) {
     const int nchunks = vx_rhs_chunks(S->n0, P, sms);   // from the body's own count
     __shared__ float4 sq4[RHS_T];   // (x, y, G, unused)
@@ -710,7 +710,7 @@ VX_DEVK void k_rhs_near_body(VxBlkB<RHS_T, 0> vb, const VxScalars *S, const vx_p
 __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx_panel *pan, int P, int P32,
                                                     const float4 *near, double *part, int sms) {
     VX_PDL_WAIT();
-    k_rhs_near_body(VxBlkB<RHS_T, 0>{blockIdx.x, gridDim.x}, S, pan, P, P32, near, part, sms);
+    k_rhs_near_body(VxBlkB<RHS_T, 8>{blockIdx.x, gridDim.x}, S, pan, P, P32, near, part, sms);
 }
 
 // R_i = -(mean velocity along panel i + V_inf) . tau_i; the far field (if

@@ -2,10 +2,10 @@
 // bulk-form vortex diffusion over it.
 //
 // The diffusive velocity (reference diffusion_Kernel, src/kernel.cu:985-1029)
-// sums G_j exp(-r/d_i) terms; beyond r = c d_i (c = diff_cutoff, default 20)
+// sums G_j exp(-r/d_i) terms; beyond r = c d_i (c = diff_cutoff, default 16)
 // a term is below e^-c of its strength, and in a uniform cloud all of them
-// together about (c+1) e^-c = 4e-8 of the sum (below its FP32 rounding), so
-// the bulk form sums only the pairs within c d_i.  Particles are binned into
+// together about (c+1) e^-c = 2e-6 of the sum's magnitude, so the bulk form
+// sums only the pairs within c d_i.  Particles are binned into
 // square cells of side h (h tracks the mean 3-nearest distance), put in cell
 // order with each cell's particles in index order (vx_bucket_order: every
 // sum then has a fixed order), and gathered into one float4 per particle

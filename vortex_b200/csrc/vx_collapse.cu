@@ -178,7 +178,7 @@ __global__ void k_col_scatter(VxView v, const VxScalars *S, const int *cellid, c
 // does not depend on the order.  The target's cell is recomputed from its
 // position by the count's expression.
 template <int PASS>
-VX_DEVK void k_col_query_body(VxBlkB<0, 0> vb, VxParams p, VxScalars *S, const int *start, const int *sorted,
+VX_DEVK void k_col_query_body(VxBlkB<VX_THREADS, 4> vb, VxParams p, VxScalars *S, const int *start, const int *sorted,
                               const double *xs, const double *ys, const double *gs, int *col, int *in_cnt,
                               int *cand) {
     if (S->col_done) return;
@@ -221,7 +221,7 @@ template <int PASS>
 __global__ void k_col_query(VxParams p, VxScalars *S, const int *start, const int *sorted, const double *xs,
                             const double *ys, const double *gs, int *col, int *in_cnt, int *cand) {
     VX_PDL_WAIT();
-    k_col_query_body<PASS>(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, p, S, start, sorted, xs, ys, gs, col, in_cnt, cand);
+    k_col_query_body<PASS>(VxBlkB<VX_THREADS, 4>{blockIdx.x, gridDim.x}, p, S, start, sorted, xs, ys, gs, col, in_cnt, cand);
 }
 
 // Settles the candidates in one block: rounds over the candidate list decide

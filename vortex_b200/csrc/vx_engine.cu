@@ -142,7 +142,7 @@ extern "C" vx_status vx_conf_default(vx_conf *c) {
     c->precision = VX_PREC_FP64;
     c->birth_offset_mode = VX_BIRTH_REF;
     c->drop_eps = 1e-12;
-    c->diff_cutoff = 20.0;
+    c->diff_cutoff = 16.0;
     c->fmm = 1;
     c->fmm_leaf = 32;
     return VX_OK;

@@ -332,7 +332,7 @@ constexpr int FMM_TOP = 3;  // levels below this one are left to the last block 
 // computes P2M at the leaves of its subtree (one warp per leaf), then M2M of
 // the 3 levels above them.
 template <int P>
-VX_DEVK void k_fmm_up_body(VxBlkB<128, 0> vb, VxView v, const VxScalars *S, const int *start, const int *sorted,
+VX_DEVK void k_fmm_up_body(VxBlkB<128, 4> vb, VxView v, const VxScalars *S, const int *start, const int *sorted,
                            int *cnt, cplx *M) {
     __shared__ cplx se[4][P];
     const int L = S->fL;
@@ -354,7 +354,7 @@ template <int P>
 __global__ void __launch_bounds__(128) k_fmm_up(VxView v, const VxScalars *S, const int *start, const int *sorted,
                                                 int *cnt, cplx *M) {
     VX_PDL_WAIT();
-    k_fmm_up_body<P>(VxBlkB<128, 0>{blockIdx.x, gridDim.x}, v, S, start, sorted, cnt, M);
+    k_fmm_up_body<P>(VxBlkB<128, 4>{blockIdx.x, gridDim.x}, v, S, start, sorted, cnt, M);
 }
 
 // Upward pass, the rest: M2M of the levels from L - 4 up to 3 by subtrees

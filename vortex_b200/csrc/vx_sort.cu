@@ -42,7 +42,7 @@ constexpr int BK_E = 4;   // elements per lane: a warp orders buckets of up to 3
 // One thread per bucket: writes the count back, orders a bucket of up to
 // BK_S elements itself (ranks by counting, in registers) and lists larger
 // ones for a warp (mid) or a block (big).
-VX_DEVK void k_bk_order_body(VxBlkB<0, 0> vb, VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
+VX_DEVK void k_bk_order_body(VxBlkB<256, 3> vb, VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
                              int *oval, int *mid, int *big, VxGather gt) {
     const long long nb = *d_nb;
     int *cnt = cnt0 + (d_off ? *d_off : 0);
@@ -77,7 +77,7 @@ VX_DEVK void k_bk_order_body(VxBlkB<0, 0> vb, VxScalars *S, const long long *d_n
 __global__ void k_bk_order(VxScalars *S, const long long *d_nb, const int *start, int *cnt0, const long long *d_off,
                            int *oval, int *mid, int *big, VxGather gt) {
     VX_PDL_WAIT();
-    k_bk_order_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, S, d_nb, start, cnt0, d_off, oval, mid, big, gt);
+    k_bk_order_body(VxBlkB<256, 3>{blockIdx.x, gridDim.x}, S, d_nb, start, cnt0, d_off, oval, mid, big, gt);
 }
 
 // The listed buckets, one launch: a block per bucket of more than 32 BK_E

@@ -209,11 +209,12 @@ def main():
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--mode", default="graph", choices=["graph", "streams"])
+    ap.add_argument("--stepping", default="graph", choices=["graph", "streams"],
+                    help="batch: one batched graph per step (graph) or every body's graph on its own stream")
     a = ap.parse_args()
     prec = N.PREC_FP32 if a.precision == "fp32" else N.PREC_FP64
     if a.mode == "batch":
-        print(json.dumps(run_batch(a.bodies, a.steps, a.warmup, precision=prec, mode=a.mode)))
+        print(json.dumps(run_batch(a.bodies, a.steps, a.warmup, precision=prec, mode=a.stepping)))
     else:
         print(json.dumps(run_serve(a.requests, a.rate, precision=prec)))
 
