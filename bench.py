@@ -129,9 +129,9 @@ HBM_BYTES = {
     "k_cg_gather": (56, "read order index and key, x, y, G, d; write float4"),
     "k_col_prep": (16, "read x, y"),
     "k_col_count": (32, "read x, y; write cell id, in-count and the two merge flags"),
-    "k_col_scatter": (60, "read cell id, cell start, x, y, G; write the cell-sorted index and copy"),
-    "k_col_query<2>": (32, "read the cell-sorted copy (index, x, y, G); write COL"),
-    "k_col_query<1>": (32, "read the cell-sorted copy (index, x, y, G); write COL"),
+    "k_col_scatter": (64, "read cell id, cell start, x, y, G; write the 32-byte cell-sorted record"),
+    "k_col_query<2>": (36, "read the cell-sorted record (x, y, G, index); write COL"),
+    "k_col_query<1>": (36, "read the cell-sorted record (x, y, G, index); write COL"),
     "k_cmp_count": (8, "read G"),
     "k_cmp_classify": (8, "read G"),
 }

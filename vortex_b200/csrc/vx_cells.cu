@@ -34,6 +34,9 @@ constexpr int CG_W = 32;       // targets per work item (one warp)
 #endif
 constexpr int CG_DIV = VX_CG_DIV;      // cell side = cut-off radius at the mean d / CG_DIV
 constexpr int CG_KCAP = 2 * CG_DIV;    // widest window of a work item, in cells (twice the mean radius)
+#ifndef VX_DIFF_FRAME_D
+#define VX_DIFF_FRAME_D 64.0f          // farthest a target may sit from its item's frame, in units of its d
+#endif
 
 // Start of the diffusion stage, one launch: per partition the bounding-box
 // keys (into box[]) and the sum of d (into red[]); the block that finishes
@@ -368,7 +371,7 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
         // the body holds targets on both sides of it) would lose FP32 digits
         // in the item's frame: beyond 64 d it is summed alone, in the frame
         // of its own cell, as the wide targets are
-        const bool far_frame = valid && fabsf((float)(int)(skey[t] - key0)) * h > 64.0f * me.w;
+        const bool far_frame = valid && fabsf((float)(int)(skey[t] - key0)) * h > VX_DIFF_FRAME_D * me.w;
         const bool is_wide = valid && (R > (float)CG_KCAP * h || far_frame);
         if (is_wide) wide[atomicAdd(&S->cnwide, 1)] = (int)t;
         const bool act = valid && !is_wide;

@@ -147,28 +147,33 @@ __global__ void __launch_bounds__(VX_SCAN_T) k_col_scan(VxScalars *S, const int 
     k_col_scan_body(VxBlkB<VX_SCAN_T, 0>{blockIdx.x, gridDim.x}, S, cnt, start, tiles);
 }
 
+// A slot of the cell-sorted copy: position, strength and index of the vortex
+// (32 bytes, one DRAM sector, written by one thread).
+struct __align__(32) ColRec {
+    double x, y, g;
+    long long i;
+};
+
 // Each cell's slots from its start, counting its count back down to zero
-// (the zero the next pass's count starts from); the slot gets the vortex's
-// index and a copy of its position and strength, so that the query reads
-// its candidates as contiguous runs.
+// (the zero the next pass's count starts from); the slot gets a copy of the
+// vortex (ColRec), so that the query reads its candidates as contiguous runs.
 VX_DEVK void k_col_scatter_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *cellid, const int *start,
-                                int *cnt, int *sorted, double *xs, double *ys, double *gs) {
+                                int *cnt, ColRec *rec) {
     if (S->col_done) return;
     const long long n = S->n;
     for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)vb.n * blockDim.x) {
         const int c = cellid[i];
         const int k = start[c] + atomicSub(&cnt[c], 1) - 1;
-        sorted[k] = (int)i;
-        xs[k] = v.x[i * v.ps];
-        ys[k] = v.y[i * v.ps];
-        gs[k] = v.g[i * v.ps];
+        double2 *r = reinterpret_cast<double2 *>(rec + k);
+        r[0] = make_double2(v.x[i * v.ps], v.y[i * v.ps]);
+        r[1] = make_double2(v.g[i * v.ps], __longlong_as_double(i));
     }
 }
 __global__ void k_col_scatter(VxView v, const VxScalars *S, const int *cellid, const int *start, int *cnt,
-                              int *sorted, double *xs, double *ys, double *gs) {
+                              ColRec *rec) {
     VX_PDL_WAIT();
-    k_col_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cellid, start, cnt, sorted, xs, ys, gs);
+    k_col_scatter_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, cellid, start, cnt, rec);
 }
 
 // COL[i] = smallest j > i in the 3x3 cell neighbourhood that qualifies.  The
@@ -178,17 +183,18 @@ __global__ void k_col_scatter(VxView v, const VxScalars *S, const int *cellid, c
 // does not depend on the order.  The target's cell is recomputed from its
 // position by the count's expression.
 template <int PASS>
-VX_DEVK void k_col_query_body(VxBlkB<VX_THREADS, 4> vb, VxParams p, VxScalars *S, const int *start, const int *sorted,
-                              const double *xs, const double *ys, const double *gs, int *col, int *in_cnt,
-                              int *cand) {
+VX_DEVK void k_col_query_body(VxBlkB<VX_THREADS, 4> vb, VxParams p, VxScalars *S, const int *start, const ColRec *rec,
+                              int *col, int *in_cnt, int *cand) {
     if (S->col_done) return;
     const long long n = S->n;
     const long long gnx = S->gnx, gny = S->gny;
     const double rd2 = p.r_diff2, rs2 = p.r_same2, mvg = p.max_ve_g;
     for (long long k0 = vb.x * (long long)blockDim.x + threadIdx.x; k0 < n;
          k0 += (long long)vb.n * blockDim.x) {
-        const long long i = sorted[k0];
-        const double xi = xs[k0], yi = ys[k0], gi = gs[k0];
+        const double2 m0 = reinterpret_cast<const double2 *>(rec + k0)[0];
+        const double2 m1 = reinterpret_cast<const double2 *>(rec + k0)[1];
+        const double xi = m0.x, yi = m0.y, gi = m1.x;
+        const long long i = __double_as_longlong(m1.y);
         long long cx, cy;
         vx_cell_of(S, xi, yi, cx, cy);
         int best = INT_MAX;
@@ -196,10 +202,12 @@ VX_DEVK void k_col_query_body(VxBlkB<VX_THREADS, 4> vb, VxParams p, VxScalars *S
             const long long r0 = yy * gnx;
             const int k1 = start[r0 + min(cx + 1, gnx - 1) + 1];
             for (int k = start[r0 + max(cx - 1, 0LL)]; k < k1; ++k) {
-                const int j = sorted[k];
+                const double2 q1 = reinterpret_cast<const double2 *>(rec + k)[1];
+                const int j = (int)__double_as_longlong(q1.y);
                 if (j <= i || j >= best) continue;
-                const double gj = gs[k];
-                const double dx = xi - xs[k], dy = yi - ys[k];
+                const double2 q0 = reinterpret_cast<const double2 *>(rec + k)[0];
+                const double gj = q1.x;
+                const double dx = xi - q0.x, dy = yi - q0.y;
                 const double r2 = fma(dx, dx, dy * dy);
                 bool ok;
                 if (PASS == 1) ok = (gi * gj < 0) && (r2 < rd2);
@@ -218,10 +226,10 @@ VX_DEVK void k_col_query_body(VxBlkB<VX_THREADS, 4> vb, VxParams p, VxScalars *S
     }
 }
 template <int PASS>
-__global__ void k_col_query(VxParams p, VxScalars *S, const int *start, const int *sorted, const double *xs,
-                            const double *ys, const double *gs, int *col, int *in_cnt, int *cand) {
+__global__ void k_col_query(VxParams p, VxScalars *S, const int *start, const ColRec *rec, int *col, int *in_cnt,
+                            int *cand) {
     VX_PDL_WAIT();
-    k_col_query_body<PASS>(VxBlkB<VX_THREADS, 4>{blockIdx.x, gridDim.x}, p, S, start, sorted, xs, ys, gs, col, in_cnt, cand);
+    k_col_query_body<PASS>(VxBlkB<VX_THREADS, 4>{blockIdx.x, gridDim.x}, p, S, start, rec, col, in_cnt, cand);
 }
 
 // Settles the candidates in one block: rounds over the candidate list decide
@@ -316,18 +324,19 @@ cudaError_t vx_launch_collapse(const VxLaunch &L, const VxParams &p, const VxVie
     const double r2 = pass == 1 ? p.r_diff2 : p.r_same2;
     if (!(r2 > 0.0) || n_col <= 0) return cudaSuccess;   // no pair can qualify
     const int grid = std::min(L.num_sms * 4, VX_RED_BLOCKS);   // 4 box keys per block
+    // the cell-sorted copy (32 bytes a vortex) lives in the pair kernels'
+    // partial-sum buffer, unused by collapse (at least 5 doubles a slot)
+    ColRec *rec = reinterpret_cast<ColRec *>(w.part);
     for (int cc = 0; cc < n_col; ++cc) {
         vx_launch<k_col_prep, k_col_prep_body>(L, grid, VX_THREADS, 0, v, S, cc == 0, r2, w.cells_cap, w.box);
         vx_launch<k_col_count, k_col_count_body>(L, grid, VX_THREADS, 0, v, S, w.cellid, w.cell_cnt, w.in_cnt, w.has_app, w.first_app);
         vx_launch<k_col_scan, k_col_scan_body>(L, grid, VX_SCAN_T, 0, S, w.cell_cnt, w.cell_start, w.scan_tiles);
-        // the cell-sorted copy lives in the compaction's scratch (free until
-        // the round's compaction)
-        vx_launch<k_col_scatter, k_col_scatter_body>(L, grid, VX_THREADS, 0, v, S, w.cellid, w.cell_start, w.cell_cnt, w.sorted, w.hx, w.hy, w.hg);
+        vx_launch<k_col_scatter, k_col_scatter_body>(L, grid, VX_THREADS, 0, v, S, w.cellid, w.cell_start, w.cell_cnt, rec);
         if (pass == 1) {
-            vx_launch<k_col_query<1>, k_col_query_body<1>>(L, grid, VX_THREADS, 0, p, S, w.cell_start, w.sorted, (const double *)w.hx, (const double *)w.hy, (const double *)w.hg, w.col, w.in_cnt, w.cand);
+            vx_launch<k_col_query<1>, k_col_query_body<1>>(L, grid, VX_THREADS, 0, p, S, w.cell_start, (const ColRec *)rec, w.col, w.in_cnt, w.cand);
             vx_launch<k_col_settle<1>, k_col_settle_body<1>>(L, 1, 1024, 0, v, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec, w.mx, w.my, w.mg);
         } else {
-            vx_launch<k_col_query<2>, k_col_query_body<2>>(L, grid, VX_THREADS, 0, p, S, w.cell_start, w.sorted, (const double *)w.hx, (const double *)w.hy, (const double *)w.hg, w.col, w.in_cnt, w.cand);
+            vx_launch<k_col_query<2>, k_col_query_body<2>>(L, grid, VX_THREADS, 0, p, S, w.cell_start, (const ColRec *)rec, w.col, w.in_cnt, w.cand);
             vx_launch<k_col_settle<2>, k_col_settle_body<2>>(L, 1, 1024, 0, v, S, w.cand, w.col, w.in_cnt, w.has_app, w.first_app, w.cstate, w.cdec, w.mx, w.my, w.mg);
         }
         vx_launch_compact_skip(L, p, v, S, w, &S->col_done);

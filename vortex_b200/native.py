@@ -14,7 +14,9 @@ import numpy as np
 from .profiles import PANEL_DTYPE
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libvortex_b200.so")
+# the in-tree build; VORTEX_B200_LIB names another build of the same sources
+# (a variant built with VX_NVCC_DEFS, for measuring it side by side)
+LIB_PATH = os.environ.get("VORTEX_B200_LIB") or os.path.join(HERE, "libvortex_b200.so")
 
 PREC_FP64, PREC_FP32 = 0, 1
 BIRTH_REF, BIRTH_FILE, BIRTH_HALF_PANEL = 0, 1, 2
