@@ -32,7 +32,9 @@ def _bodies():
              dict(index=2, kind="ellipse", panels=1500, b=0.45, angle=0.0, re=12000.0, n0=150000,
                   dt=0.005 * 200 / 1500, cloud_seed=13)]
     for sp in specs:
-        out.append(wl.make_body(sp, N.PREC_FP32))
+        conf, pan, x, y, g = wl.make_body(sp, N.PREC_FP32)
+        conf.inc_step = 8192          # the smallest growth margin: body 1 outgrows its store
+        out.append((conf, pan, x, y, g))
     sp = dict(index=3, kind="ellipse", panels=200, b=0.3, angle=0.0, re=1000.0, n0=1500, dt=0.005, cloud_seed=14)
     out.append(wl.make_body(sp, N.PREC_FP64))
     return out

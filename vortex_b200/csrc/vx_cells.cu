@@ -18,7 +18,9 @@
 // cut-off circle), and those columns are one contiguous range of the sorted
 // array, staged through the warp's shared memory 32 sources at a time.  A
 // target whose radius exceeds CG_KCAP cells (an isolated vortex with a large
-// d) would widen its warp's window for all 32 targets; it is left out of the
+// d) would widen its warp's window for all 32 targets; unless the item's
+// other targets are about as wide (the sparse outskirts of a cloud: the
+// window, up to CG_KMAX cells, then serves them all) it is left out of the
 // window and summed alone by one warp (k_diff_wide).  So is a target more
 // than 64 d from its item's first cell (items of a row that crosses the body
 // hold targets on both sides of it): the item's frame would cost it FP32
@@ -33,7 +35,8 @@ constexpr int CG_W = 32;       // targets per work item (one warp)
 #define VX_CG_DIV 8
 #endif
 constexpr int CG_DIV = VX_CG_DIV;      // cell side = cut-off radius at the mean d / CG_DIV
-constexpr int CG_KCAP = 2 * CG_DIV;    // widest window of a work item, in cells (twice the mean radius)
+constexpr int CG_KCAP = 2 * CG_DIV;    // a target's radius, in cells, that needs no company (twice the mean radius)
+constexpr int CG_KMAX = 3 * CG_DIV;    // widest window of a work item, in cells
 #ifndef VX_DIFF_FRAME_D
 #define VX_DIFF_FRAME_D 64.0f          // farthest a target may sit from its item's frame, in units of its d
 #endif
@@ -334,7 +337,7 @@ struct DiffRow {
     unsigned base;   // row * nx + the item's first column (cell keys wrap modulo 2^32 alike)
     float oy;        // row offset * h
 };
-constexpr int DIFF_ROWS = 2 * CG_KCAP + 2;   // rows of the widest window, and the total
+constexpr int DIFF_ROWS = 2 * CG_KMAX + 2;   // rows of the widest window, and the total
 VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView v, VxScalars *S,
                                const float4 *srt, const unsigned *skey,
                                const int *sorted, const int *start,
@@ -372,7 +375,18 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
         // in the item's frame: beyond 64 d it is summed alone, in the frame
         // of its own cell, as the wide targets are
         const bool far_frame = valid && fabsf((float)(int)(skey[t] - key0)) * h > VX_DIFF_FRAME_D * me.w;
-        const bool is_wide = valid && (R > (float)CG_KCAP * h || far_frame);
+        // a radius beyond CG_KCAP cells stays in the item (up to CG_KMAX) while
+        // it is at most twice the item's mean: the window then serves targets
+        // about as wide as itself; an outlier is summed alone
+        float rsum = valid && !far_frame ? R : 0.0f;
+        int rcnt = valid && !far_frame ? 1 : 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            rsum += __shfl_xor_sync(0xffffffffu, rsum, o);
+            rcnt += __shfl_xor_sync(0xffffffffu, rcnt, o);
+        }
+        const float rmean = rsum / (float)max(rcnt, 1);
+        const bool too_wide = R > (float)CG_KMAX * h || (R > (float)CG_KCAP * h && R > 2.0f * rmean);
+        const bool is_wide = valid && (too_wide || far_frame);
         if (is_wide) wide[atomicAdd(&S->cnwide, 1)] = (int)t;
         const bool act = valid && !is_wide;
         float rmax = act ? R : 0.0f, xlo = act ? me.x : 3e38f, xhi = act ? me.x : -3e38f;
@@ -386,8 +400,8 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
         const f2 TX = f2_pack(me.x, me.x), TY = f2_pack(me.y, me.y);
         const float nd = -log2e / me.w;
         const f2 NDD = f2_pack(nd, nd);
-        // rows -kk..kk (kk <= CG_KCAP: a non-wide target's radius is at most CG_KCAP cells)
-        const int kk = min((int)ceilf(rmax / h), CG_KCAP);
+        // rows -kk..kk (kk <= CG_KMAX: a non-wide target's radius is at most CG_KMAX cells)
+        const int kk = min((int)ceilf(rmax / h), CG_KMAX);
         const int nrows = 2 * kk + 1;
         int total = 0;
         for (int r0 = 0; r0 < nrows; r0 += 32) {

@@ -126,7 +126,8 @@ def make_body(spec: dict, precision: int):
     a panel off the wall, same-sign collapse within 0.3 eps, |G| < 1e-8
     dropped; the panel system is inverted with the reference's pivot rule,
     or with partial pivoting where that rule meets a tiny pivot (thin
-    bodies)."""
+    bodies).  The store grows by at least 16 steps' births at a time (a
+    growth re-records the body's part of a batched step)."""
     P = spec["panels"]
     if spec["kind"] == "ellipse":
         pan = profiles.ellipse(P, 0.5, spec["b"])
@@ -148,5 +149,5 @@ def make_body(spec: dict, precision: int):
                           v_inf_y=0.0, x_min=-2.0, x_max=10.0, y_min=-10.0, y_max=10.0, ve_size=eps,
                           n_of_points=20, n_col=2, r_col_diff_sign=0.0, r_col_same_sign=0.3, max_ve_g=1e30,
                           v_inf_incr_steps=0, drop_eps=1e-8, birth_offset_mode=N.BIRTH_HALF_PANEL,
-                          precision=precision, inc_step=8192, gj_pivot=2)
+                          precision=precision, inc_step=max(8192, -(-16 * P // 8192) * 8192), gj_pivot=2)
     return conf, pan, x, y, g
