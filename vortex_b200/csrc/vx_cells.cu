@@ -277,12 +277,12 @@ __device__ __forceinline__ f2 diff_exp2_fma(float xa, float xb) {
 #ifndef VX_DIFF_POLY_EVERY
 #define VX_DIFF_POLY_EVERY 0   // every k-th pair step takes its 2^x on the FMA pipe (0: none)
 #endif
+// Two diffusion pairs (one target, sources a and b: SX = (x_a, x_b), SY,
+// G likewise) in packed FP32.
 template <bool POLY = false>
-__device__ __forceinline__ void diff_pair2(const float4 *slot, const float2 *gslot, f2 TX, f2 TY, f2 NDD,
-                                           float thr2, f2 &S2X, f2 &S2Y, f2 &S1) {
-    const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(slot);
-    const f2 G = *reinterpret_cast<const f2 *>(gslot);
-    const f2 DX = f2_sub(TX, sq.x), DY = f2_sub(TY, sq.y);
+__device__ __forceinline__ void diff_pair2(f2 SX, f2 SY, f2 G, f2 TX, f2 TY, f2 NDD, float thr2, f2 &S2X, f2 &S2Y,
+                                           f2 &S1) {
+    const f2 DX = f2_sub(TX, SX), DY = f2_sub(TY, SY);
     const f2 R2 = f2_fma(DX, DX, f2_mul(DY, DY));
     float r2a, r2b;
     f2_unpack(R2, r2a, r2b);
@@ -342,12 +342,13 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
                                const float4 *srt, const unsigned *skey,
                                const int *sorted, const int *start,
                                const int2 *items, int *wide) {
-    __shared__ float4 sxy[CG_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
-    __shared__ float2 sg[CG_T / 2];    // (G_a, G_b)
+    // per warp 32 staged sources as x[32], y[32], G[32]: one 16-byte shared
+    // load brings four sources' x (or y, or G)
+    __shared__ float4 sx[CG_T / 4], sy[CG_T / 4], sg[CG_T / 4];
     __shared__ DiffRow srow[CG_T / 32][DIFF_ROWS];
     const int lane = threadIdx.x & 31;
-    float4 *wxy = sxy + ((threadIdx.x & ~31) >> 1);
-    float2 *wg = sg + ((threadIdx.x & ~31) >> 1);
+    float4 *wx = sx + ((threadIdx.x & ~31) >> 2), *wy = sy + ((threadIdx.x & ~31) >> 2),
+           *wg = sg + ((threadIdx.x & ~31) >> 2);
     DiffRow *wrow = srow[threadIdx.x >> 5];
     const long long nitems = S->cnitems, nx = S->cnx, ny = S->cny;
     const double hd = S->ch;
@@ -451,10 +452,9 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
                 y = qn.y + e.oy;
                 gq = qn.z;
             }
-            float *slot = reinterpret_cast<float *>(wxy + (lane >> 1));
-            slot[lane & 1] = x;
-            slot[2 + (lane & 1)] = y;
-            reinterpret_cast<float *>(wg + (lane >> 1))[lane & 1] = gq;
+            reinterpret_cast<float *>(wx)[lane] = x;
+            reinterpret_cast<float *>(wy)[lane] = y;
+            reinterpret_cast<float *>(wg)[lane] = gq;
             __syncwarp();
             if (f + 32 < total) {
                 while (rc < nrows - 1 && wrow[rc + 1].pre <= f + 32) ++rc;
@@ -463,13 +463,23 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView
                 kn = skey[j];
             }
             f2 S2X = 0ull, S2Y = 0ull, S1 = 0ull;   // +0.0f in both halves
+            // sources 2q and 2q + 1 are one pair step, in index order, so
+            // each packed half sums the even (odd) sources in order
             VX_UNROLL(VX_DIFF_UNROLL)
-            for (int q = 0; q < 16; ++q) {
-                if (VX_DIFF_POLY_EVERY > 0 && q % (VX_DIFF_POLY_EVERY > 0 ? VX_DIFF_POLY_EVERY : 1) ==
-                                                  VX_DIFF_POLY_EVERY - 1)
-                    diff_pair2<true>(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
-                else
-                    diff_pair2<false>(wxy + q, wg + q, TX, TY, NDD, thr2, S2X, S2Y, S1);
+            for (int q4 = 0; q4 < 8; ++q4) {
+                const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(wx + q4);
+                const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(wy + q4);
+                const ulonglong2 G = *reinterpret_cast<const ulonglong2 *>(wg + q4);
+#pragma unroll
+                for (int h2 = 0; h2 < 2; ++h2) {
+                    const int q = 2 * q4 + h2;
+                    const f2 SXp = h2 ? X.y : X.x, SYp = h2 ? Y.y : Y.x, Gp = h2 ? G.y : G.x;
+                    if (VX_DIFF_POLY_EVERY > 0 && q % (VX_DIFF_POLY_EVERY > 0 ? VX_DIFF_POLY_EVERY : 1) ==
+                                                      VX_DIFF_POLY_EVERY - 1)
+                        diff_pair2<true>(SXp, SYp, Gp, TX, TY, NDD, thr2, S2X, S2Y, S1);
+                    else
+                        diff_pair2<false>(SXp, SYp, Gp, TX, TY, NDD, thr2, S2X, S2Y, S1);
+                }
             }
             __syncwarp();
             float a, b;   // the two halves are added in FP32, then carried in FP64

@@ -624,11 +624,8 @@ __device__ __forceinline__ float vx_rcp_approx2(float x) {
 // 0 (dx = dy = 0), so no pair is skipped.  One reciprocal serves both pairs:
 // 1/a = b (1/(a b)), 1/b = a (1/(a b)) (a b stays within FP32 range: padding
 // sources sit 1e12 away, and both padded gives 1/inf = 0, G = 0).
-__device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gslot, f2 TX, f2 TY, float eps2,
-                                           f2 &SY, f2 &SXN) {
-    const ulonglong2 sq = *reinterpret_cast<const ulonglong2 *>(slot);
-    const f2 G = *reinterpret_cast<const f2 *>(gslot);
-    const f2 DX = f2_sub(TX, sq.x), DY = f2_sub(TY, sq.y);
+__device__ __forceinline__ void near_pair2(f2 SX, f2 SYs, f2 G, f2 TX, f2 TY, float eps2, f2 &SY, f2 &SXN) {
+    const f2 DX = f2_sub(TX, SX), DY = f2_sub(TY, SYs);
     const f2 R2 = f2_fma(DX, DX, f2_mul(DY, DY));
     float r2a, r2b;
     f2_unpack(R2, r2a, r2b);
@@ -645,11 +642,12 @@ __device__ __forceinline__ void near_pair2(const float4 *slot, const float2 *gsl
 template <int P>
 VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
                              const int *sorted, const int *start, const int2 *items, const cplx *Loc) {
-    __shared__ float4 sxy[FMM_T / 2];   // per warp 16 slots: (x_a, x_b, y_a, y_b) for sources a = 2k, b = 2k+1
-    __shared__ float2 sg[FMM_T / 2];    // (G_a, G_b)
+    // per warp 32 staged sources as x[32], y[32], G[32]: one 16-byte shared
+    // load brings four sources' x (or y, or G)
+    __shared__ float4 sx[FMM_T / 4], sy[FMM_T / 4], sg[FMM_T / 4];
     const int lane = threadIdx.x & 31;
-    float4 *wxy = sxy + ((threadIdx.x & ~31) >> 1);
-    float2 *wg = sg + ((threadIdx.x & ~31) >> 1);
+    float4 *wx = sx + ((threadIdx.x & ~31) >> 2), *wy = sy + ((threadIdx.x & ~31) >> 2),
+           *wg = sg + ((threadIdx.x & ~31) >> 2);
     const long long n = S->n;
     const int L = S->fL;
     const long long m = 1LL << L;
@@ -715,14 +713,19 @@ VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView 
                 y = q.y + oy;
                 g = q.z;
             }
-            float *slot = reinterpret_cast<float *>(wxy + (lane >> 1));
-            slot[lane & 1] = x;
-            slot[2 + (lane & 1)] = y;
-            reinterpret_cast<float *>(wg + (lane >> 1))[lane & 1] = g;
+            reinterpret_cast<float *>(wx)[lane] = x;
+            reinterpret_cast<float *>(wy)[lane] = y;
+            reinterpret_cast<float *>(wg)[lane] = g;
             __syncwarp();
             f2 SY = 0ull, SXN = 0ull;   // +0.0f in both halves
-#pragma unroll 16
-            for (int q = 0; q < 16; ++q) near_pair2(wxy + q, wg + q, TX, TY, eps2, SY, SXN);
+#pragma unroll
+            for (int q4 = 0; q4 < 8; ++q4) {   // sources 2q, 2q + 1 a pair step, in index order
+                const ulonglong2 X = *reinterpret_cast<const ulonglong2 *>(wx + q4);
+                const ulonglong2 Y = *reinterpret_cast<const ulonglong2 *>(wy + q4);
+                const ulonglong2 G = *reinterpret_cast<const ulonglong2 *>(wg + q4);
+                near_pair2(X.x, Y.x, G.x, TX, TY, eps2, SY, SXN);
+                near_pair2(X.y, Y.y, G.y, TX, TY, eps2, SY, SXN);
+            }
             __syncwarp();
             float a, b;   // the two halves are added in FP32, then carried in FP64
             f2_unpack(SXN, a, b); ax -= (double)(a + b);
