@@ -201,7 +201,7 @@ __device__ __forceinline__ void advect_part(unsigned part, unsigned nparts, cons
 // on the grid the kernel runs with.  The block that finishes last adds the
 // partition sums: thread t adds partitions t, t + 256, ... in order, then a
 // fixed shared-memory tree, so the result is run-to-run identical.
-VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
+VX_DEVK void k_advect_body(VxBlkB<VX_THREADS, 0> vb, const VxParams &p, const VxView &v, VxScalars *S, const vx_panel *pan,
                            double *red, const int *hstart, const int *hidx, int sms) {
     const long long n = S->n;
     const int nparts = vx_body_parts(n, sms, VX_RED_BLOCKS);

@@ -303,7 +303,7 @@ struct RhsMath<float> {
 };
 
 template <typename T>
-VX_DEVK void k_rhs_partial_body(VxBlkB<RHS_T, 0> vb, VxView v, const VxScalars *S,
+VX_DEVK void k_rhs_partial_body(VxBlkB<RHS_T, 0> vb, const VxView &v, const VxScalars *S,
                                 const vx_panel *pan, int P, int P32,
                                 double *part, int sms) {
     const int nchunks = vx_rhs_chunks(S->n0, P, sms);   // from the body's own count
@@ -493,7 +493,7 @@ __device__ __forceinline__ void bf_far_part(unsigned q, unsigned nparts, const V
 // on the launch's grid.
 constexpr int BF_SCAN_PER = VX_BF_MAX_BLOCKS / BF_T;
 static_assert(BF_SCAN_PER * BF_T == VX_BF_MAX_BLOCKS, "whole chunks per scan thread");
-VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, VxScalars *S, double *part, int *cnt,
+VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 2> vb, const VxParams &p, const VxView &v, VxScalars *S, double *part, int *cnt,
                            int sms, long long *off, double *coef) {
     const int nparts = vx_bf_parts(S->n0 + p.P, sms);
     for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) {
@@ -545,7 +545,7 @@ VX_DEVK void k_bf_far_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, VxScalars *
 __global__ void __launch_bounds__(BF_T) k_bf_far(VxParams p, VxView v, VxScalars *S, double *part, int *cnt,
                                                  int sms, long long *off, double *coef) {
     VX_PDL_WAIT();
-    k_bf_far_body(VxBlkB<BF_T, 0>{blockIdx.x, gridDim.x}, p, v, S, part, cnt, sms, off, coef);
+    k_bf_far_body(VxBlkB<BF_T, 2>{blockIdx.x, gridDim.x}, p, v, S, part, cnt, sms, off, coef);
 }
 
 // Near sources of each block in index order (block-wide ballot scan).
@@ -578,7 +578,7 @@ __device__ __forceinline__ void bf_scatter_part(unsigned q, unsigned nparts, con
         base += total;
     }
 }
-VX_DEVK void k_bf_scatter_body(VxBlkB<BF_T, 0> vb, VxParams p, VxView v, const VxScalars *S,
+VX_DEVK void k_bf_scatter_body(VxBlkB<BF_T, 0> vb, const VxParams &p, const VxView &v, const VxScalars *S,
                                const long long *off, float4 *near, int sms) {
     const int nparts = vx_bf_parts(S->n0 + p.P, sms);
     for (unsigned q = vb.x; q < (unsigned)nparts; q += vb.n) bf_scatter_part(q, (unsigned)nparts, p, v, S, off, near);
@@ -719,7 +719,7 @@ __global__ void __launch_bounds__(RHS_T) k_rhs_near(const VxScalars *S, const vx
 // fixed butterfly); otherwise one thread per panel in chunk order.
 template <bool WARP>
 VX_DEVK void k_rhs_final_body(VxBlkB<0, 0> vb, const VxScalars *S, const vx_panel *pan, int P, int P32,
-                              const double *part, int sms, double *R, VxParams p, const double *coef) {
+                              const double *part, int sms, double *R, const VxParams &p, const double *coef) {
     const int nchunks = vx_rhs_chunks(S->n0, P, sms);   // from the body's own count
     const int i = WARP ? (int)((vb.x * blockDim.x + threadIdx.x) >> 5) : vb.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
@@ -803,7 +803,7 @@ __device__ void birth_place(const VxParams &p, const VxView &v, VxScalars *S, co
 // gamma_i = sum_j M_ij R_j + M_iP dg, sequential in j with fma (as the
 // oracle), one thread per row; ld is the matrix row stride.  Then the
 // vortices are placed (birth_place).
-VX_DEVK void k_gamma_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan, const double *M,
+VX_DEVK void k_gamma_body(VxBlkB<0, 0> vb, const VxParams &p, const VxView &v, VxScalars *S, const vx_panel *pan, const double *M,
                           long long ld, int P, const double *R, double *gamma) {
     const int i = vb.x * blockDim.x + threadIdx.x;
     if (i < P) {
@@ -823,7 +823,7 @@ __global__ void k_gamma(VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
 // The same sums from the transposed inverse Mt (Mt[j ld + i] = M[i ld + j]):
 // the same order and fma per row, but a warp's 32 rows read 32 consecutive
 // doubles per step instead of 32 rows' worth of cache lines.
-VX_DEVK void k_gamma_t_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
+VX_DEVK void k_gamma_t_body(VxBlkB<0, 0> vb, const VxParams &p, const VxView &v, VxScalars *S, const vx_panel *pan,
                             const double *Mt, long long ld, int P, const double *R, double *gamma) {
     const int i = vb.x * blockDim.x + threadIdx.x;
     if (i < P) {
@@ -841,7 +841,7 @@ __global__ void k_gamma_t(VxParams p, VxView v, VxScalars *S, const vx_panel *pa
 
 // Bulk form: one warp per row, lanes striding the row (coalesced), FP64
 // partial sums combined by a fixed butterfly.
-VX_DEVK void k_gamma_w_body(VxBlkB<0, 0> vb, VxParams p, VxView v, VxScalars *S, const vx_panel *pan,
+VX_DEVK void k_gamma_w_body(VxBlkB<0, 0> vb, const VxParams &p, const VxView &v, VxScalars *S, const vx_panel *pan,
                             const double *M, long long ld, int P, const double *R, double *gamma) {
     const int lane = threadIdx.x & 31;
     const int i = (vb.x * blockDim.x + threadIdx.x) >> 5;

@@ -49,7 +49,7 @@ constexpr int CG_KMAX = 3 * CG_DIV;    // widest window of a work item, in cells
 // in a fixed tree, so the mean spacing, and the grid built from it, do not
 // depend on the launch's grid.  Cell side h = c * mean(d) / CG_DIV, grown
 // until the grid fits cells_cap.
-VX_DEVK void k_cg_prep_body(VxBlkB<CG_T, 0> vb, VxView v, VxScalars *S, double *red, unsigned long long *box,
+VX_DEVK void k_cg_prep_body(VxBlkB<CG_T, 0> vb, const VxView &v, VxScalars *S, double *red, unsigned long long *box,
                             int sms, double cutoff, long long cells_cap) {
     __shared__ unsigned long long sk[4][CG_T];
     __shared__ double sd[CG_T];
@@ -140,7 +140,7 @@ __device__ __forceinline__ long long cg_cell(const VxScalars *S, double x, doubl
 
 // Cell of every particle, counted per cell (the counts are zero between
 // steps: the bucket order leaves them at zero once the order is built).
-VX_DEVK void k_cg_cellid_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
+VX_DEVK void k_cg_cellid_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, unsigned *key, int *val, int *cnt) {
     const long long n = S->n;
     if (S->cncells == 0) return;
     for (long long i = vb.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -338,7 +338,7 @@ struct DiffRow {
     float oy;        // row offset * h
 };
 constexpr int DIFF_ROWS = 2 * CG_KMAX + 2;   // rows of the widest window, and the total
-VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, VxParams p, VxView v, VxScalars *S,
+VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, const VxParams &p, const VxView &v, VxScalars *S,
                                const float4 *srt, const unsigned *skey,
                                const int *sorted, const int *start,
                                const int2 *items, int *wide) {
@@ -552,7 +552,7 @@ __device__ __forceinline__ void wide_apply(const VxParams &p, VxView v, const in
     }
 }
 
-VX_DEVK void k_diff_wide_body(VxBlkB<CG_T, 0> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
+VX_DEVK void k_diff_wide_body(VxBlkB<CG_T, 0> vb, const VxParams &p, const VxView &v, VxScalars *S, const float4 *srt,
                               const unsigned *skey, const int *sorted, const int *start,
                               const int *wide, int *huge) {
     const int lane = threadIdx.x & 31;
@@ -594,7 +594,7 @@ __global__ void __launch_bounds__(CG_T) k_diff_wide(VxParams p, VxView v, VxScal
     k_diff_wide_body(VxBlkB<CG_T, 0>{blockIdx.x, gridDim.x}, p, v, S, srt, skey, sorted, start, wide, huge);
 }
 
-VX_DEVK void k_diff_huge_body(VxBlkB<WIDE_T, 0> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
+VX_DEVK void k_diff_huge_body(VxBlkB<WIDE_T, 0> vb, const VxParams &p, const VxView &v, VxScalars *S, const float4 *srt,
                               const unsigned *skey, const int *sorted, const int *start,
                               const int *huge) {
     constexpr int NWARP = WIDE_T / 32;

@@ -31,7 +31,7 @@
 // pass has converged.  Cell side h = r (1 + 1e-6): any pair closer than r is
 // in neighbouring cells; when the box would need more than cells_cap cells,
 // h grows.
-VX_DEVK void k_col_prep_body(VxBlkB<VX_THREADS, 0> vb, VxView v, VxScalars *S, int reset, double r2,
+VX_DEVK void k_col_prep_body(VxBlkB<VX_THREADS, 0> vb, const VxView &v, VxScalars *S, int reset, double r2,
                              long long cells_cap, unsigned long long *part) {
     const bool done = reset ? false : (S->col_done || S->n == S->col_n_before);
     if (done) {
@@ -103,7 +103,7 @@ __device__ __forceinline__ void vx_cell_of(const VxScalars *S, double x, double 
     cy = cy < 0 ? 0 : (cy >= S->gny ? S->gny - 1 : cy);
 }
 
-VX_DEVK void k_col_count_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
+VX_DEVK void k_col_count_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, int *cellid, int *cnt, int *in_cnt,
                               int *has_app, int *first_app) {
     if (S->col_done) return;
     const long long n = S->n;
@@ -157,7 +157,7 @@ struct __align__(32) ColRec {
 // Each cell's slots from its start, counting its count back down to zero
 // (the zero the next pass's count starts from); the slot gets a copy of the
 // vortex (ColRec), so that the query reads its candidates as contiguous runs.
-VX_DEVK void k_col_scatter_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *cellid, const int *start,
+VX_DEVK void k_col_scatter_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, const int *cellid, const int *start,
                                 int *cnt, ColRec *rec) {
     if (S->col_done) return;
     const long long n = S->n;
@@ -183,7 +183,7 @@ __global__ void k_col_scatter(VxView v, const VxScalars *S, const int *cellid, c
 // does not depend on the order.  The target's cell is recomputed from its
 // position by the count's expression.
 template <int PASS>
-VX_DEVK void k_col_query_body(VxBlkB<VX_THREADS, 4> vb, VxParams p, VxScalars *S, const int *start, const ColRec *rec,
+VX_DEVK void k_col_query_body(VxBlkB<VX_THREADS, 4> vb, const VxParams &p, VxScalars *S, const int *start, const ColRec *rec,
                               int *col, int *in_cnt, int *cand) {
     if (S->col_done) return;
     const long long n = S->n;
@@ -238,7 +238,7 @@ __global__ void k_col_query(VxParams p, VxScalars *S, const int *start, const Co
 // they were, then written (after a barrier: a merge may read a partner that
 // another merge removes).
 template <int PASS>
-VX_DEVK void k_col_settle_body(VxBlkB<1024, 0> vb, VxView v, VxScalars *S, const int *cand, const int *col,
+VX_DEVK void k_col_settle_body(VxBlkB<1024, 0> vb, const VxView &v, VxScalars *S, const int *cand, const int *col,
                                int *in_cnt, int *has_app, int *first_app, int *cstate, int *cdec, double *mx,
                                double *my, double *mg) {
     if (S->col_done) return;

@@ -25,7 +25,7 @@ __device__ __forceinline__ bool vx_live(const VxView &v, long long p, double eps
 
 // Live elements per chunk; the block that finishes last then scans the
 // chunk counts and finds m, scan[m] and H.
-VX_DEVK void k_cmp_count_body(VxBlkB<VX_THREADS, 0> vb, VxView v, VxScalars *S, double eps, int *cnt,
+VX_DEVK void k_cmp_count_body(VxBlkB<VX_THREADS, 0> vb, const VxView &v, VxScalars *S, double eps, int *cnt,
                               long long *off, const int *skip) {
     if (skip && *skip) return;
     __shared__ long long sh[VX_THREADS];
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_cmp_count(VxView v, VxScalars *S
 
 // Per chunk: local scan, then hole positions, hole sources and tail sources.
 // tail_src < 0 encodes "the position of hole -(value+1)".
-VX_DEVK void k_cmp_classify_body(VxBlkB<VX_THREADS, 0> vb, VxView v, const VxScalars *S, double eps,
+VX_DEVK void k_cmp_classify_body(VxBlkB<VX_THREADS, 0> vb, const VxView &v, const VxScalars *S, double eps,
                                  const long long *off, int *hole_pos,
                                  int *hole_src, int *tail_src,
                                  const int *skip) {
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(VX_THREADS) k_cmp_classify(VxView v, const VxS
     k_cmp_classify_body(VxBlkB<VX_THREADS, 0>{blockIdx.x, gridDim.x}, v, S, eps, off, hole_pos, hole_src, tail_src, skip);
 }
 
-VX_DEVK void k_cmp_gather_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const int *hole_pos, const int *hole_src,
+VX_DEVK void k_cmp_gather_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, const int *hole_pos, const int *hole_src,
                                const int *tail_src, double *hx, double *hy, double *hg, double *tx,
                                double *ty, const int *skip) {
     if (skip && *skip) return;
@@ -185,7 +185,7 @@ __global__ void k_cmp_gather(VxView v, const VxScalars *S, const int *hole_pos, 
 
 // count_step: this compaction closes a whole step, which it counts (no
 // kernel after it in the step reads the step index).
-VX_DEVK void k_cmp_scatter_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const int *hole_pos, const double *hx,
+VX_DEVK void k_cmp_scatter_body(VxBlkB<0, 0> vb, const VxView &v, VxScalars *S, const int *hole_pos, const double *hx,
                                 const double *hy, const double *hg, const double *tx, const double *ty,
                                 const int *skip, int count_step) {
     if (count_step && vb.x == 0 && threadIdx.x == 0) S->step += 1;

@@ -67,7 +67,7 @@ extern __shared__ __align__(16) unsigned char vx_fmm_dyn[];
 // last block), then, in the last block, the stage's counters and the tree:
 // square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], reduced until
 // the leaf side is at least eps.
-VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S, double eps, int Lmax, int leaf, int *cnt,
+VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S, double eps, int Lmax, int leaf, int *cnt,
                              long long ncnt, int *subcnt, long long nsub, unsigned long long *part) {
     __shared__ unsigned long long sk[4][FMM_T];
     const long long n = S->n;
@@ -155,7 +155,7 @@ __device__ __forceinline__ unsigned fmm_subkey(const VxScalars *S, double x, dou
     return (unsigned)(4 * leaf + 2 * (iy & 1) + (ix & 1));
 }
 
-VX_DEVK void k_fmm_leafid_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, unsigned *key, int *val, int *subcnt) {
+VX_DEVK void k_fmm_leafid_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, unsigned *key, int *val, int *subcnt) {
     const long long s = S->fs;
     for (long long j = vb.x * (long long)blockDim.x + threadIdx.x; j < s;
          j += (long long)vb.n * blockDim.x) {
@@ -332,7 +332,7 @@ constexpr int FMM_TOP = 3;  // levels below this one are left to the last block 
 // computes P2M at the leaves of its subtree (one warp per leaf), then M2M of
 // the 3 levels above them.
 template <int P>
-VX_DEVK void k_fmm_up_body(VxBlkB<128, 4> vb, VxView v, const VxScalars *S, const int *start, const int *sorted,
+VX_DEVK void k_fmm_up_body(VxBlkB<128, 4> vb, const VxView &v, const VxScalars *S, const int *start, const int *sorted,
                            int *cnt, cplx *M) {
     __shared__ cplx se[4][P];
     const int L = S->fL;
@@ -640,7 +640,7 @@ __device__ __forceinline__ void near_pair2(f2 SX, f2 SYs, f2 G, f2 TX, f2 TY, fl
 #define VX_NEAR_MINB 2   // minimum resident blocks per SM requested for k_fmm_near (at most 128 registers)
 #endif
 template <int P>
-VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, VxParams p, VxView v, VxScalars *S, const float4 *srt,
+VX_DEVK void k_fmm_near_body(VxBlkB<FMM_T, VX_NEAR_MINB> vb, const VxParams &p, const VxView &v, VxScalars *S, const float4 *srt,
                              const int *sorted, const int *start, const int2 *items, const cplx *Loc) {
     // per warp 32 staged sources as x[32], y[32], G[32]: one 16-byte shared
     // load brings four sources' x (or y, or G)
@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, Vx
 // computed as the near field computes them).  Exact when the third distance
 // is below the quarter's side (every source outside the 3 x 3 block is
 // farther); the others go to the ring search over leaves (k_fmm_nn3_fix).
-VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, VxView v, VxScalars *S, const float4 *srt, const unsigned *skey,
+VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S, const float4 *srt, const unsigned *skey,
                                 const int *sorted, const int *substart, int *flag_list) {
     const long long s = S->fs, n = S->n;
     const int m = 1 << S->fL, m2 = 2 * m;
@@ -879,7 +879,7 @@ __device__ void fmm_nn3_brute_block(VxView v, VxScalars *S, const int *brute_lis
     }
 }
 
-VX_DEVK void k_fmm_nn3_fix_body(VxBlkB<0, 0> vb, VxView v, VxScalars *S, const float4 *srt, const int *sorted,
+VX_DEVK void k_fmm_nn3_fix_body(VxBlkB<0, 0> vb, const VxView &v, VxScalars *S, const float4 *srt, const int *sorted,
                                 const int *start, const int *flag_list, int *brute_list) {
     const int nf = S->fnflag;
     const long long m = 1LL << S->fL;

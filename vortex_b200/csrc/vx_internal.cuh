@@ -15,6 +15,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <type_traits>
 #include <vector>
 
 #include "../../include/vortex_b200.h"
@@ -623,18 +624,24 @@ inline int vx_full_sms(const VxLaunch &L) { return L.full_sms > 0 ? L.full_sms :
 // timing events into L.kt.
 template <auto K, auto DEV, typename SigD = decltype(DEV)>
 struct VxLauncher;
-template <auto K, auto DEV, int MAXT, int MINB, typename... A>
-struct VxLauncher<K, DEV, void (*)(VxBlkB<MAXT, MINB>, A...)> {
+// The argument a body takes by reference (a large parameter struct) is
+// stored and passed by value in the pack and to the single kernel; the
+// body then reads the pack (or the kernel's parameter space) in place
+// instead of holding a copy in registers.
+template <typename T>
+using vx_arg_t = std::remove_cv_t<std::remove_reference_t<T>>;
+template <auto K, auto DEV, int MAXT, int MINB, typename... A0>
+struct VxLauncher<K, DEV, void (*)(VxBlkB<MAXT, MINB>, A0...)> {
     static const void *many() {
-        if constexpr (MAXT > 0 && MINB > 0) return (const void *)&k_many_tb<DEV, MAXT, MINB, A...>;
-        else if constexpr (MAXT > 0) return (const void *)&k_many_t<DEV, MAXT, A...>;
-        else return (const void *)&k_many<DEV, A...>;
+        if constexpr (MAXT > 0 && MINB > 0) return (const void *)&k_many_tb<DEV, MAXT, MINB, vx_arg_t<A0>...>;
+        else if constexpr (MAXT > 0) return (const void *)&k_many_t<DEV, MAXT, vx_arg_t<A0>...>;
+        else return (const void *)&k_many<DEV, vx_arg_t<A0>...>;
     }
     template <typename... Args>
     static cudaError_t go(const VxLaunch &L, dim3 grid, dim3 block, size_t smem, Args &&...args) {
         if (L.launches) ++*L.launches;
         if (L.rec) {
-            const VxPack<A...> p = VxPackMake<A...>::make(static_cast<A>(args)...);
+            const VxPack<vx_arg_t<A0>...> p = VxPackMake<vx_arg_t<A0>...>::make(static_cast<vx_arg_t<A0>>(args)...);
             L.rec->add((const void *)K, many(), grid, block, smem, &p, sizeof(p));
             return cudaSuccess;
         }
@@ -654,7 +661,7 @@ struct VxLauncher<K, DEV, void (*)(VxBlkB<MAXT, MINB>, A...)> {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        const cudaError_t e = cudaLaunchKernelEx(&cfg, K, static_cast<A>(args)...);
+        const cudaError_t e = cudaLaunchKernelEx(&cfg, K, static_cast<vx_arg_t<A0>>(args)...);
         if (L.kt) {
             cudaEventRecord(eb, L.stream);
             L.kt->recs.push_back(VxKernelTimer::Rec{(const void *)K, ea, eb});

@@ -37,7 +37,7 @@ __device__ __forceinline__ void vx_split_of(const VxScalars *S, const VxSplit &s
 
 // ---------------------------------------------------------------------------
 // Packed FP32 sources for the bulk form: (x, y, G, 0), G masked to 0 beyond n.
-VX_DEVK void k_pack32_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, float4 *src, long long upto) {
+VX_DEVK void k_pack32_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, float4 *src, long long upto) {
     const long long n = S->n;
     const long long s = vx_round32(n);
     for (long long j = vb.x * (long long)blockDim.x + threadIdx.x; j < s;
@@ -85,7 +85,7 @@ __device__ __forceinline__ void load_src(SrcTile<T> &t, const VxView &v, const f
 // Biot-Savart (+ 3 nearest when NN3).  Targets: particles (nt < 0 -> n) or
 // probe points (tx/ty with stride tstr).  Partials: [sc][5][tstride].
 template <typename T, bool NN3>
-VX_DEVK void k_bs_partial_body(VxBlkB<PT, 0> vb, VxParams p, VxView v, const VxScalars *S,
+VX_DEVK void k_bs_partial_body(VxBlkB<PT, 0> vb, const VxParams &p, const VxView &v, const VxScalars *S,
                                const float4 *src32, const double *tx,
                                const double *ty, long long tstr, long long nt_in,
                                double *part, VxSplit sp) {
@@ -211,7 +211,7 @@ __device__ __forceinline__ void bs32_tile(const float4 *sm, int cnt, int jbase, 
 }
 
 template <bool NN3>
-VX_DEVK void k_bs32_partial_body(VxBlkB<PT, 0> vb, VxParams p, const VxScalars *S, const float4 *src32,
+VX_DEVK void k_bs32_partial_body(VxBlkB<PT, 0> vb, const VxParams &p, const VxScalars *S, const float4 *src32,
                                  const double *tx, const double *ty, long long tstr,
                                  long long nt_in, double *part, VxSplit sp) {
     int K;
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(PT) k_bs32_partial(VxParams p, const VxScalars
 
 // Combine: V = sum/(2 pi) + V_inf, d = mean of the 3 nearest distances.
 template <bool FP32>
-VX_DEVK void k_bs_combine_body(VxBlkB<0, 0> vb, VxView v, const VxScalars *S, const double *part, VxSplit sp) {
+VX_DEVK void k_bs_combine_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, const double *part, VxSplit sp) {
     int K;
     long long tstride;
     vx_split_of(S, sp, K, tstride);
@@ -366,7 +366,7 @@ template <> struct DiffMath<float> {
 };
 
 template <typename T>
-VX_DEVK void k_diff_partial_body(VxBlkB<PT, 0> vb, VxParams p, VxView v, const VxScalars *S,
+VX_DEVK void k_diff_partial_body(VxBlkB<PT, 0> vb, const VxParams &p, const VxView &v, const VxScalars *S,
                                  const float4 *src32, double *part,
                                  VxSplit sp) {
     int K;
@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(PT) k_diff_partial(VxParams p, VxView v, const
     k_diff_partial_body<T>(VxBlkB<PT, 0>{blockIdx.x, gridDim.x}, p, v, S, src32, part, sp);
 }
 
-VX_DEVK void k_diff_combine_body(VxBlkB<0, 0> vb, VxParams p, VxView v, const VxScalars *S, const double *part,
+VX_DEVK void k_diff_combine_body(VxBlkB<0, 0> vb, const VxParams &p, const VxView &v, const VxScalars *S, const double *part,
                                  VxSplit sp) {
     int K;
     long long tstride;

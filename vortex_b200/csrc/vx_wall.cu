@@ -73,7 +73,7 @@ __device__ __forceinline__ void vx_wall_integral_bulk(float Ra0, float Ra1, floa
 }
 
 template <typename T>
-VX_DEVK void k_wall_body(VxBlkB<128, sizeof(T) == 4 ? 8 : 0> vb, VxParams p, VxView v, const VxScalars *S, const vx_panel *pan, const int *wstart,
+VX_DEVK void k_wall_body(VxBlkB<128, sizeof(T) == 4 ? 8 : 0> vb, const VxParams &p, const VxView &v, const VxScalars *S, const vx_panel *pan, const int *wstart,
                          const int *widx) {
     const long long n = S->n;
     const T nu = (T)p.nu;
