@@ -519,6 +519,7 @@ extern "C" vx_status vx_batch_new(int device, vx_batch **out) {
         delete b;
         return st;
     };
+    vx_keep_pool(device);
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VX_ERR_CUDA);
     for (int k = 0; k < 2; ++k)
@@ -698,6 +699,7 @@ extern "C" vx_status vx_batch_destroy(vx_batch *b) {
     if (!b) return VX_OK;
     cudaSetDevice(b->device);
     release(b);
+    vx_trim_pool(b->device);
     delete b;
     return VX_OK;
 }

@@ -34,6 +34,26 @@ void vx_set_error(const char *fmt, ...) {
 
 extern "C" const char *vx_last_error(void) { return g_err.c_str(); }
 
+// Stream-ordered allocations (growth of the particle arrays, the batch's
+// gather buffer) come from the device's default pool.  With the pool's
+// default release threshold of 0, every stream or event synchronize hands the
+// pool's free memory back to the driver, so the next growth maps fresh pages
+// inside a step; keeping the freed memory in the pool makes a regrowth reuse it.
+void vx_keep_pool(int device) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) { cudaGetLastError(); return; }
+    unsigned long long keep = ~0ull;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) cudaGetLastError();
+}
+
+// A destroyed handle's stream-ordered memory goes back to the driver (the
+// pool keeps it otherwise, out of reach of plain cudaMalloc callers).
+void vx_trim_pool(int device) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) { cudaGetLastError(); return; }
+    if (cudaMemPoolTrimTo(pool, 0) != cudaSuccess) cudaGetLastError();
+}
+
 extern "C" const char *vx_status_str(vx_status s) {
     switch (s) {
     case VX_OK: return "ok";
@@ -471,6 +491,7 @@ extern "C" vx_status vx_create(const vx_conf *conf, const vx_panel *pan, int64_t
     *out = nullptr;
     auto fail = [&](vx_status st) { vx_destroy(s); return st; };
     if (cudaSetDevice(device) != cudaSuccess) { vx_set_error("cudaSetDevice(%d) failed", device); return fail(VX_ERR_CUDA); }
+    vx_keep_pool(device);
     cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(VX_ERR_CUDA);
     vx_params_from_conf(conf, pan, (int)P, &s->prm);
@@ -553,6 +574,7 @@ extern "C" vx_status vx_destroy(vx_sim *s) {
     for (auto &e : s->ev) if (e) cudaEventDestroy(e);
     for (auto &e : s->pev) if (e) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
+    vx_trim_pool(s->device);
     delete s;
     return VX_OK;
 }

@@ -720,6 +720,8 @@ cudaError_t vx_launch_compact_skip(const VxLaunch &L, const VxParams &p, const V
                                    VxScalars *S, VxWork &w, const int *skip, bool count_step = false);
 void vx_params_from_conf(const vx_conf *c, const vx_panel *pan, int P, VxParams *p);
 void vx_set_error(const char *fmt, ...);
+void vx_keep_pool(int device);
+void vx_trim_pool(int device);
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
                         cudaStream_t stream = nullptr, int fmm_p = VX_FMM_P);
 long long vx_work_bytes(long long cap, int P32, int num_sms, int fmm_p = VX_FMM_P);

@@ -140,7 +140,7 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
            "panels_total": int(sum(sp["panels"] for sp in specs)),
            "batched_steps_per_s": steps / total_s, "body_steps_per_s": bodies * steps / total_s,
            "ms_per_batched_step": float(np.mean(ms)), "ms_p50": float(np.percentile(ms, 50)),
-           "ms_p99": float(np.percentile(ms, 99)),
+           "ms_p99": float(np.percentile(ms, 99)), "ms_steps": [round(float(m), 3) for m in ms],
            "particle_steps_per_s": float(nmean.sum()) * steps / total_s,
            "interactions_per_s_effective": inter * steps / total_s,
            "gpu_launches": int(launches), "kernels_per_batched_step": launches / steps, "setup_s": setup_s}
