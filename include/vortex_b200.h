@@ -174,7 +174,8 @@ vx_status vx_probe(vx_sim *sim, const double *px, const double *py, int64_t np,
 /* Binary checkpoint of a body at full precision (no counterpart in the
  * reference, whose restart frames, src/main.c:175-188 and 558-605, keep six
  * decimals and lose d_g, the forces and the V_inf ramp): the vortices, the
- * step index, the current V_inf, d_g and the last forces.  A body continued
+ * step index, the current V_inf, d_g, the last forces and the last quadtree
+ * build's occupancy record (the next depth follows from it).  A body continued
  * from a checkpoint steps exactly as the one that wrote it.  Loading checks
  * the panel count, the form and a hash of the panels (VX_ERR_ARG on a
  * mismatch or a damaged file). */

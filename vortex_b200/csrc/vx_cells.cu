@@ -13,10 +13,12 @@
 //
 // Cell side h = c mean(d) / 8.  Work item = one warp's 32 consecutive
 // cell-sorted targets of one grid row.  The warp scans the rows within its
-// largest cut-off radius R; in row offset dy it needs only the columns within
-// sqrt(R^2 - ((|dy|-1) h)^2) of its targets' x range (the window follows the
-// cut-off circle), and those columns are one contiguous range of the sorted
-// array, staged through the warp's shared memory 32 sources at a time.  A
+// largest cut-off radius; in each row it needs only the union of its targets'
+// own column ranges (target i reaches the columns within sqrt(R_i^2 - gy^2)
+// of its x, gy its vertical gap to the row: the window follows the targets'
+// own cut-off circles, not the largest one), and those columns are one
+// contiguous range of the sorted array, staged through the warp's shared
+// memory 32 sources at a time.  A
 // target whose radius exceeds CG_KCAP cells (an isolated vortex with a large
 // d) would widen its warp's window for all 32 targets; unless the item's
 // other targets are about as wide (the sparse outskirts of a cloud: the
@@ -31,12 +33,16 @@
 
 constexpr int CG_T = 256;
 constexpr int CG_W = 32;       // targets per work item (one warp)
-#ifndef VX_CG_DIV
-#define VX_CG_DIV 8
+#ifndef VX_CG_DIV_X
+#define VX_CG_DIV_X 8
 #endif
-constexpr int CG_DIV = VX_CG_DIV;      // cell side = cut-off radius at the mean d / CG_DIV
-constexpr int CG_KCAP = 2 * CG_DIV;    // a target's radius, in cells, that needs no company (twice the mean radius)
-constexpr int CG_KMAX = 3 * CG_DIV;    // widest window of a work item, in cells
+#ifndef VX_CG_DIV_Y
+#define VX_CG_DIV_Y 8
+#endif
+constexpr int CG_DIV_X = VX_CG_DIV_X;    // cell width = cut-off radius at the mean d / CG_DIV_X
+constexpr int CG_DIV_Y = VX_CG_DIV_Y;    // cell height = cut-off radius at the mean d / CG_DIV_Y
+constexpr int CG_KCAP = 2 * CG_DIV_Y;    // a target's radius, in rows, that needs no company (twice the mean radius)
+constexpr int CG_KMAX = 3 * CG_DIV_Y;    // widest window of a work item, in rows
 #ifndef VX_DIFF_FRAME_D
 #define VX_DIFF_FRAME_D 64.0f          // farthest a target may sit from its item's frame, in units of its d
 #endif
@@ -47,8 +53,8 @@ constexpr int CG_KMAX = 3 * CG_DIV;    // widest window of a work item, in cells
 // sum of d is split into nparts fixed partitions whatever the grid (a
 // partition past the last particle adds 0) and the partition sums are added
 // in a fixed tree, so the mean spacing, and the grid built from it, do not
-// depend on the launch's grid.  Cell side h = c * mean(d) / CG_DIV, grown
-// until the grid fits cells_cap.
+// depend on the launch's grid.  Cell width c * mean(d) / CG_DIV_X, height
+// c * mean(d) / CG_DIV_Y, both grown until the grid fits cells_cap.
 VX_DEVK void k_cg_prep_body(VxBlkB<CG_T, 0> vb, const VxView &v, VxScalars *S, double *red, unsigned long long *box,
                             int sms, double cutoff, long long cells_cap) {
     __shared__ unsigned long long sk[4][CG_T];
@@ -112,16 +118,18 @@ VX_DEVK void k_cg_prep_body(VxBlkB<CG_T, 0> vb, const VxView &v, VxScalars *S, d
     const double dsum = sd[0];
     const double x0 = vx_dunkey(sk[0][0]), x1 = -vx_dunkey(sk[1][0]);
     const double y0 = vx_dunkey(sk[2][0]), y1 = -vx_dunkey(sk[3][0]);
-    double h = cutoff * (dsum / (double)n) / (double)CG_DIV;
-    if (!(h > 0.0)) h = 1e-3;
+    double hy = cutoff * (dsum / (double)n) / (double)CG_DIV_Y;
+    if (!(hy > 0.0)) hy = 1e-3;
+    double hx = hy * ((double)CG_DIV_Y / (double)CG_DIV_X);
     long long nx = -1, ny = -1;
     for (int it = 0; it < 400; ++it) {
-        const double fx = floor((x1 - x0) / h) + 1.0, fy = floor((y1 - y0) / h) + 1.0;
+        const double fx = floor((x1 - x0) / hx) + 1.0, fy = floor((y1 - y0) / hy) + 1.0;
         if (fx * fy <= (double)cells_cap) { nx = (long long)fx; ny = (long long)fy; break; }
-        h *= 1.25;
+        hx *= 1.25;
+        hy *= 1.25;
     }
     if (nx < 0) { S->err |= VX_DERR_GRID; S->cncells = 0; return; }
-    S->cx0 = x0; S->cy0 = y0; S->ch = h;
+    S->cx0 = x0; S->cy0 = y0; S->ch = hx; S->chy = hy;
     S->cnx = nx; S->cny = ny; S->cncells = nx * ny;
 }
 __global__ void __launch_bounds__(CG_T) k_cg_prep(VxView v, VxScalars *S, double *red, unsigned long long *box,
@@ -132,7 +140,7 @@ __global__ void __launch_bounds__(CG_T) k_cg_prep(VxView v, VxScalars *S, double
 
 __device__ __forceinline__ long long cg_cell(const VxScalars *S, double x, double y) {
     long long cx = (long long)floor((x - S->cx0) / S->ch);
-    long long cy = (long long)floor((y - S->cy0) / S->ch);
+    long long cy = (long long)floor((y - S->cy0) / S->chy);
     cx = cx < 0 ? 0 : (cx >= S->cnx ? S->cnx - 1 : cx);
     cy = cy < 0 ? 0 : (cy >= S->cny ? S->cny - 1 : cy);
     return cy * S->cnx + cx;
@@ -232,15 +240,16 @@ __device__ __forceinline__ void diff_pair(float tx, float ty, float R2, float nd
 }
 
 // Cells of row offset dy that can hold a source within R of a target whose x
-// (relative to the centre of column `ocol`) lies in [xlo, xhi]; false if none.
-__device__ __forceinline__ bool diff_window(int dy, float R, float xlo, float xhi, float h, long long ocol,
-                                            long long nx, long long &c0, long long &c1) {
-    const float gy = (float)max(abs(dy) - 1, 0) * h;   // vertical gap to that row
+// (relative to the centre of column `ocol`) lies in [xlo, xhi]; false if none
+// (cells hx wide and hy high).
+__device__ __forceinline__ bool diff_window(int dy, float R, float xlo, float xhi, float hx, float hy,
+                                            long long ocol, long long nx, long long &c0, long long &c1) {
+    const float gy = (float)max(abs(dy) - 1, 0) * hy;   // vertical gap to that row
     const float hw2 = R * R - gy * gy;
     if (!(hw2 >= 0.0f)) return false;
-    const float hw = sqrtf(hw2) * 1.0001f + 1e-3f * h;  // margin over FP32 rounding
-    c0 = max(ocol + (long long)floorf((xlo - hw) / h + 0.5f), 0LL);
-    c1 = min(ocol + (long long)floorf((xhi + hw) / h + 0.5f), nx - 1);
+    const float hw = sqrtf(hw2) * 1.0001f + 1e-3f * hx;  // margin over FP32 rounding
+    c0 = max(ocol + (long long)floorf((xlo - hw) / hx + 0.5f), 0LL);
+    c1 = min(ocol + (long long)floorf((xhi + hw) / hx + 0.5f), nx - 1);
     return c0 <= c1;
 }
 
@@ -335,7 +344,7 @@ struct DiffRow {
     int j0;          // first source of the row's column range
     int pre;         // sources of the rows before it (the entry after the last row holds the total)
     unsigned base;   // row * nx + the item's first column (cell keys wrap modulo 2^32 alike)
-    float oy;        // row offset * h
+    float oy;        // row offset * cell height
 };
 constexpr int DIFF_ROWS = 2 * CG_KMAX + 2;   // rows of the widest window, and the total
 VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, const VxParams &p, const VxView &v, VxScalars *S,
@@ -351,8 +360,8 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, const VxParams &p,
            *wg = sg + ((threadIdx.x & ~31) >> 2);
     DiffRow *wrow = srow[threadIdx.x >> 5];
     const long long nitems = S->cnitems, nx = S->cnx, ny = S->cny;
-    const double hd = S->ch;
-    const float h = (float)hd;
+    const double hyd = S->chy;
+    const float hx = (float)S->ch, hy = (float)hyd;
     const float cut = (float)p.diff_cutoff;
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
     const float log2e = 1.4426950408889634f;
@@ -369,13 +378,13 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, const VxParams &p,
         // coordinates relative to the centre of the item's first cell
         const unsigned key0 = skey[item.y];
         const long long ocol = (long long)key0 - row * nx;
-        if (valid) me.x += (float)(int)(skey[t] - key0) * h;   // as for the sources below
+        if (valid) me.x += (float)(int)(skey[t] - key0) * hx;   // as for the sources below
         const float R = cut * me.w;
         // a target far from the item's first cell (an item whose row crosses
         // the body holds targets on both sides of it) would lose FP32 digits
         // in the item's frame: beyond 64 d it is summed alone, in the frame
         // of its own cell, as the wide targets are
-        const bool far_frame = valid && fabsf((float)(int)(skey[t] - key0)) * h > VX_DIFF_FRAME_D * me.w;
+        const bool far_frame = valid && fabsf((float)(int)(skey[t] - key0)) * hx > VX_DIFF_FRAME_D * me.w;
         // a radius beyond CG_KCAP cells stays in the item (up to CG_KMAX) while
         // it is at most twice the item's mean: the window then serves targets
         // about as wide as itself; an outlier is summed alone
@@ -386,38 +395,56 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, const VxParams &p,
             rcnt += __shfl_xor_sync(0xffffffffu, rcnt, o);
         }
         const float rmean = rsum / (float)max(rcnt, 1);
-        const bool too_wide = R > (float)CG_KMAX * h || (R > (float)CG_KCAP * h && R > 2.0f * rmean);
+        const bool too_wide = R > (float)CG_KMAX * hy || (R > (float)CG_KCAP * hy && R > 2.0f * rmean);
         const bool is_wide = valid && (too_wide || far_frame);
         if (is_wide) wide[atomicAdd(&S->cnwide, 1)] = (int)t;
         const bool act = valid && !is_wide;
-        float rmax = act ? R : 0.0f, xlo = act ? me.x : 3e38f, xhi = act ? me.x : -3e38f;
-        for (int o = 16; o > 0; o >>= 1) {
-            rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-            xlo = fminf(xlo, __shfl_xor_sync(0xffffffffu, xlo, o));
-            xhi = fmaxf(xhi, __shfl_xor_sync(0xffffffffu, xhi, o));
-        }
+        float rmax = act ? R : 0.0f;
+        for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
         const int nact = __popc(__ballot_sync(0xffffffffu, act));
         if (nact == 0) continue;
         const f2 TX = f2_pack(me.x, me.x), TY = f2_pack(me.y, me.y);
         const float nd = -log2e / me.w;
         const f2 NDD = f2_pack(nd, nd);
         // rows -kk..kk (kk <= CG_KMAX: a non-wide target's radius is at most CG_KMAX cells)
-        const int kk = min((int)ceilf(rmax / h), CG_KMAX);
+        const int kk = min((int)ceilf(rmax / hy), CG_KMAX);
         const int nrows = 2 * kk + 1;
         int total = 0;
         for (int r0 = 0; r0 < nrows; r0 += 32) {
+            // columns of row r0 + lane: the union of the active targets' own
+            // ranges in that row, each within sqrt(R^2 - gy^2) of the
+            // target's x (gy its vertical gap to the row, less a margin over
+            // FP32 rounding), column offsets from the item's first column
+            int mc0 = 0, mc1 = -1;
+            const int rn = min(32, nrows - r0);
+            for (int q = 0; q < rn; ++q) {
+                const float fy = (float)(r0 + q - kk) * hy;
+                int lo = 0x7fffffff, hi = -0x7fffffff;
+                if (act) {
+                    const float gy = fmaxf(fmaxf(fy - 0.5f * hy - me.y, me.y - fy - 0.5f * hy) - 1e-3f * hy, 0.0f);
+                    const float w2 = R * R - gy * gy;
+                    if (w2 >= 0.0f) {
+                        const float hw = sqrtf(w2) * 1.0001f + 1e-3f * hx;
+                        lo = (int)floorf((me.x - hw) / hx + 0.5f);
+                        hi = (int)floorf((me.x + hw) / hx + 0.5f);
+                    }
+                }
+                lo = __reduce_min_sync(0xffffffffu, lo);
+                hi = __reduce_max_sync(0xffffffffu, hi);
+                if (lane == q) { mc0 = lo; mc1 = hi; }
+            }
             const int r = r0 + lane;
             DiffRow e = {0, 0, 0u, 0.0f};
             int len = 0;
-            if (r < nrows) {
+            if (r < nrows && mc0 <= mc1) {
                 const int dy = r - kk;
                 const long long rr = row + dy;
-                long long c0, c1;
-                if (rr >= 0 && rr < ny && diff_window(dy, rmax, xlo, xhi, h, ocol, nx, c0, c1)) {
+                const long long c0 = max(ocol + mc0, 0LL), c1 = min(ocol + (long long)mc1, nx - 1);
+                if (rr >= 0 && rr < ny && c0 <= c1) {
                     e.j0 = start[rr * nx + c0];
                     len = start[rr * nx + c1 + 1] - e.j0;
                     e.base = (unsigned)(rr * nx + ocol);
-                    e.oy = (float)((double)dy * hd);
+                    e.oy = (float)((double)dy * hyd);
                 }
             }
             int inc = len;
@@ -448,7 +475,7 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, const VxParams &p,
             float x = 0.f, y = 0.f, gq = 0.f;
             if (f < total) {
                 const DiffRow e = wrow[rc];
-                x = qn.x + (float)(int)(kn - e.base) * h;
+                x = qn.x + (float)(int)(kn - e.base) * hx;
                 y = qn.y + e.oy;
                 gq = qn.z;
             }
@@ -513,7 +540,7 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
 // grid), is passed on to k_diff_huge: one block of WIDE_T threads each, its
 // warps taking every (WIDE_T / 32)-th row.  FP32 pair sums per row and lane,
 // FP64 across rows, lanes and warps (fixed order).
-constexpr int WIDE_ROWS = 24;
+constexpr int WIDE_ROWS = 3 * CG_DIV_Y;   // three mean cut-off radii
 constexpr int WIDE_T = 512;
 
 __device__ __forceinline__ void wide_row(const VxParams &p, const VxScalars *S, const float4 *srt,
@@ -522,20 +549,20 @@ __device__ __forceinline__ void wide_row(const VxParams &p, const VxScalars *S, 
                                          int lane, double &I2x, double &I2y, double &I1,
                                          unsigned long long &pairs) {
     const long long nx = S->cnx, ny = S->cny;
-    const double hd = S->ch;
-    const float h = (float)hd;
+    const double hyd = S->chy;
+    const float hx = (float)S->ch, hy = (float)hyd;
     const long long rr = row + dy;
     if (rr < 0 || rr >= ny) return;
     long long c0, c1;
-    if (!diff_window((int)dy, R, me.x, me.x, h, ocol, nx, c0, c1)) return;
+    if (!diff_window((int)dy, R, me.x, me.x, hx, hy, ocol, nx, c0, c1)) return;
     const long long j0 = start[rr * nx + c0], j1 = start[rr * nx + c1 + 1];
     pairs += j1 - j0;
-    const float oy = (float)((double)dy * hd);
+    const float oy = (float)((double)dy * hyd);
     const unsigned base = (unsigned)(rr * nx + ocol);   // cell keys wrap modulo 2^32 alike
     float s2x = 0.f, s2y = 0.f, s1 = 0.f;
     for (long long j = j0 + lane; j < j1; j += 32) {
         float4 q = srt[j];
-        q.x += (float)(int)(skey[j] - base) * h;
+        q.x += (float)(int)(skey[j] - base) * hx;
         q.y += oy;
         diff_pair(me.x, me.y, R2, ndd, thr2, q, s2x, s2y, s1);
     }
@@ -557,7 +584,7 @@ VX_DEVK void k_diff_wide_body(VxBlkB<CG_T, 0> vb, const VxParams &p, const VxVie
                               const int *wide, int *huge) {
     const int lane = threadIdx.x & 31;
     const long long nx = S->cnx, ny = S->cny;
-    const float h = (float)S->ch;
+    const float hy = (float)S->chy;
     const unsigned unx = (unsigned)nx;
     const float cut = (float)p.diff_cutoff;
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
@@ -570,7 +597,7 @@ VX_DEVK void k_diff_wide_body(VxBlkB<CG_T, 0> vb, const VxParams &p, const VxVie
         const float4 me = srt[t];
         const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
         const float R = cut * me.w, R2 = R * R, ndd = -log2e / me.w;
-        const long long kk = min((long long)ceilf(R / h), max(nx, ny));
+        const long long kk = min((long long)ceilf(R / hy), ny);
         if (kk > WIDE_ROWS) {
             if (lane == 0) huge[atomicAdd(&S->cnhuge, 1)] = (int)t;
             continue;
@@ -601,7 +628,7 @@ VX_DEVK void k_diff_huge_body(VxBlkB<WIDE_T, 0> vb, const VxParams &p, const VxV
     __shared__ double sred[3][NWARP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long nx = S->cnx, ny = S->cny;
-    const float h = (float)S->ch;
+    const float hy = (float)S->chy;
     const unsigned unx = (unsigned)nx;
     const float cut = (float)p.diff_cutoff;
     const float thr2 = (float)(0.001 * p.eps) * (float)(0.001 * p.eps);
@@ -613,7 +640,7 @@ VX_DEVK void k_diff_huge_body(VxBlkB<WIDE_T, 0> vb, const VxParams &p, const VxV
         const float4 me = srt[t];
         const long long ocol = (long long)(skey[t] % unx), row = (long long)(skey[t] / unx);
         const float R = cut * me.w, R2 = R * R, ndd = -log2e / me.w;
-        const long long kk = min((long long)ceilf(R / h), max(nx, ny));
+        const long long kk = min((long long)ceilf(R / hy), ny);
         double I2x = 0.0, I2y = 0.0, I1 = 0.0;
         for (long long dy = -kk + warp; dy <= kk; dy += NWARP)
             wide_row(p, S, srt, skey, start, me, row, ocol, R, R2, ndd, thr2, dy, lane, I2x, I2y, I1, pairs);

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <map>
 #include <string>
+#include <cstddef>
 #include <vector>
 
 #include "vx_sim.cuh"
@@ -585,6 +586,7 @@ static vx_status set_count(vx_sim *s, long long n) {
     CU(cudaStreamSynchronize(s->stream));
     s->h_S->n = n;
     s->h_S->n0 = n >= s->P ? n - s->P : 0;   // the last P count as this step's newborns
+    s->h_S->fsq = 0;                          // a new cloud: the quadtree depth starts from the box rule
     CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     s->n_upper = n;
@@ -752,8 +754,11 @@ extern "C" vx_status vx_set_matrix(vx_sim *s, const double *minv) {
 // to the capacity, the tail beyond the live vortices included (the plain
 // form's 3-nearest search reads the round-up slots after the live ones, as
 // the reference's does), the step index, the current V_inf, d_g and the
-// last forces with their raw sums.  The file names the body it belongs to by its panel count, its form
-// (FP64 / FP32) and a hash of its panels; loading into another body fails.
+// last forces with their raw sums, and the last quadtree build's occupancy
+// record (the bulk form's next depth follows from it).  The file names the
+// body it belongs to by its panel count, its form (FP64 / FP32) and a hash of
+// its panels; loading into another body fails.  Version 1 files (no
+// quadtree record) load with the depth rule starting afresh.
 namespace {
 struct CkptHead {
     char magic[8];           // "VXCKPT1"
@@ -761,7 +766,14 @@ struct CkptHead {
     int64_t n, n0, step, slots;
     double vinf[2], dg, fx, fy, m, raw[4];
     uint64_t panel_hash;     // FNV-1a of the panel records
+    // version 2: the last quadtree build (sum of count^2 over its quarter
+    // cells, its sources, box side and depth)
+    uint64_t tree_sq;
+    int64_t tree_s;
+    double tree_side;
+    int32_t tree_L, pad2;
 };
+constexpr size_t kCkptHeadV1 = offsetof(CkptHead, tree_sq);
 const char kCkptMagic[8] = {'V', 'X', 'C', 'K', 'P', 'T', '1', 0};
 
 vx_status panel_hash(vx_sim *s, uint64_t *h) {
@@ -784,7 +796,8 @@ extern "C" vx_status vx_checkpoint_save(vx_sim *s, const char *path) {
     CkptHead hd;
     memset(&hd, 0, sizeof(hd));
     memcpy(hd.magic, kCkptMagic, 8);
-    hd.version = 1; hd.P = s->P; hd.prec = s->prm.prec;
+    hd.version = 2; hd.P = s->P; hd.prec = s->prm.prec;
+    hd.tree_sq = h.fsq; hd.tree_s = h.fs; hd.tree_side = h.fside; hd.tree_L = h.fL;
     hd.n = h.n; hd.n0 = h.n0; hd.step = h.step; hd.slots = s->cap;
     hd.vinf[0] = h.vinf[0]; hd.vinf[1] = h.vinf[1];
     hd.dg = h.dg; hd.fx = h.fx; hd.fy = h.fy; hd.m = h.m;
@@ -811,8 +824,12 @@ extern "C" vx_status vx_checkpoint_load(vx_sim *s, const char *path) {
     FILE *f = fopen(path, "rb");
     if (!f) { vx_set_error("cannot open %s", path); return VX_ERR_ARG; }
     CkptHead hd;
-    if (fread(&hd, sizeof(hd), 1, f) != 1 || memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1 ||
-        hd.n < 0 || hd.slots < hd.n) {
+    memset(&hd, 0, sizeof(hd));
+    bool head_ok = fread(&hd, kCkptHeadV1, 1, f) == 1 && memcmp(hd.magic, kCkptMagic, 8) == 0 &&
+                   (hd.version == 1 || hd.version == 2) && hd.n >= 0 && hd.slots >= hd.n;
+    if (head_ok && hd.version == 2)
+        head_ok = fread(reinterpret_cast<char *>(&hd) + kCkptHeadV1, sizeof(hd) - kCkptHeadV1, 1, f) == 1;
+    if (!head_ok) {
         fclose(f);
         vx_set_error("%s is not a checkpoint of this library", path);
         return VX_ERR_ARG;
@@ -839,6 +856,8 @@ extern "C" vx_status vx_checkpoint_load(vx_sim *s, const char *path) {
     h->vinf[0] = hd.vinf[0]; h->vinf[1] = hd.vinf[1];
     h->dg = hd.dg; h->fx = hd.fx; h->fy = hd.fy; h->m = hd.m;
     for (int q = 0; q < 4; ++q) h->raw[q] = hd.raw[q];
+    h->fsq = hd.tree_sq;
+    if (hd.tree_sq) { h->fs = hd.tree_s; h->fside = hd.tree_side; h->fL = hd.tree_L; }
     CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     return VX_OK;

@@ -65,8 +65,15 @@ extern __shared__ __align__(16) unsigned char vx_fmm_dyn[];
 // Start of the velocity stage, one launch: the count arrays zeroed to their
 // capacity, the bounding box (per-block keys into part[], combined by the
 // last block), then, in the last block, the stage's counters and the tree:
-// square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], reduced until
-// the leaf side is at least eps.
+// square box, depth L = ceil(log4(n / leaf)) within [2, Lmax], deepened while
+// the leaf occupancy a vortex sees would reach 2 leaf, reduced until the leaf
+// side is at least eps.  The occupancy a vortex sees is sum(c^2) / n over the
+// cells; the last build measured it over its quarter-leaf cells (k_fmm_leafid),
+// and at the density it implies, a leaf of side a holds rho a^2.  A clustered
+// cloud (a dense wall layer, a Gaussian core) then gets the depth its dense
+// part needs rather than the one its bounding box implies; a uniform one
+// keeps ceil(log4(n / leaf)).  The first build of a body (no measurement yet)
+// uses the box rule alone.
 VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S, double eps, int Lmax, int leaf, int *cnt,
                              long long ncnt, int *subcnt, long long nsub, unsigned long long *part) {
     __shared__ unsigned long long sk[4][FMM_T];
@@ -103,6 +110,12 @@ VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S,
         __syncthreads();
     }
     if (threadIdx.x != 0) return;
+    // the last build's quarter-cell occupancy, sources and box
+    const unsigned long long q2 = S->fsq;
+    const long long s_prev = S->fs;
+    const double side_prev = S->fside;
+    const int L_prev = S->fL;
+    S->fsq = 0;
     S->fnflag = 0;
     S->fnbrute = 0;
     S->bk_nmid = S->bk_nbig = 0;
@@ -112,6 +125,15 @@ VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S,
     side = side * (1.0 + 1e-9) + 1e-12;
     int L = 2;
     while (L < Lmax && (double)(1LL << (2 * L)) * (double)leaf < (double)n) ++L;
+    if (q2 > 0 && s_prev > 0 && side_prev > 0.0 && L_prev >= 1) {
+        const double qa = side_prev / (double)(2LL << L_prev);                      // quarter side then
+        const double rho = (double)q2 / (double)s_prev / (qa * qa) * ((double)vx_round32(n) / (double)s_prev);
+        while (L < Lmax) {
+            const double a = side / (double)(1LL << L);
+            if (rho * a * a < 2.0 * (double)leaf) break;
+            ++L;
+        }
+    }
     while (L > 2 && side / (double)(1LL << L) < eps) --L;
     // a box smaller than 4 eps: no pair may use an expansion, all near field
     if (side / 4.0 < eps) L = 1;
@@ -155,17 +177,22 @@ __device__ __forceinline__ unsigned fmm_subkey(const VxScalars *S, double x, dou
     return (unsigned)(4 * leaf + 2 * (iy & 1) + (ix & 1));
 }
 
-VX_DEVK void k_fmm_leafid_body(VxBlkB<0, 0> vb, const VxView &v, const VxScalars *S, unsigned *key, int *val, int *subcnt) {
+// The sum of count^2 over the cells (the next build's depth rule) comes from
+// the same increments: a cell's count going from c to c + 1 adds 2 c + 1.
+VX_DEVK void k_fmm_leafid_body(VxBlkB<0, 0> vb, const VxView &v, VxScalars *S, unsigned *key, int *val, int *subcnt) {
     const long long s = S->fs;
+    unsigned long long sq = 0;
     for (long long j = vb.x * (long long)blockDim.x + threadIdx.x; j < s;
          j += (long long)vb.n * blockDim.x) {
         const unsigned k = fmm_subkey(S, v.x[j * v.ps], v.y[j * v.ps]);
         key[j] = k;
         val[j] = (int)j;
-        atomicAdd(&subcnt[k], 1);
+        sq += 2ull * (unsigned)atomicAdd(&subcnt[k], 1) + 1ull;
     }
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    if ((threadIdx.x & 31) == 0 && sq) atomicAdd(&S->fsq, sq);
 }
-__global__ void k_fmm_leafid(VxView v, const VxScalars *S, unsigned *key, int *val, int *subcnt) {
+__global__ void k_fmm_leafid(VxView v, VxScalars *S, unsigned *key, int *val, int *subcnt) {
     VX_PDL_WAIT();
     k_fmm_leafid_body(VxBlkB<0, 0>{blockIdx.x, gridDim.x}, v, S, key, val, subcnt);
 }

@@ -89,7 +89,7 @@ struct VxScalars {
     int cnhuge;            // of those, the ones whose window spans more than WIDE_ROWS rows each side
     long long bf_nnear;    // birth sources inside the far-field radius
     // neighbour-list grid of the bulk form (vortex diffusion)
-    double cx0, cy0, ch;
+    double cx0, cy0, ch, chy;   // origin, cell width and cell height
     long long cnx, cny, cncells, cnitems;
     // quadtree of the bulk-form Biot-Savart (vx_fmm.cu)
     double fx0, fy0, fside;
@@ -99,6 +99,7 @@ struct VxScalars {
     int fnbrute;           // flagged targets left to the whole-set 3-nearest scan
     int bk_nmid, bk_nbig;  // buckets of 17..128 / more elements in the running bucket order (vx_sort.cu)
     long long fcnt_off;    // offset of the leaf level in the quadtree's count array
+    unsigned long long fsq;   // sum over the quarter-leaf cells of count^2 at the last tree build (depth rule)
     // pair evaluations executed by the bulk-form near-field and diffusion
     // kernels since the counters were last cleared
     unsigned long long pairs_bs, pairs_diff;
@@ -750,8 +751,7 @@ __device__ __forceinline__ void vx_gather_slot(const VxGather &gt, long long k, 
                                 j < S->n ? (float)v.g[j * v.ps] : 0.0f, (float)col);
     } else if (gt.mode == 2) {
         const long long nx = S->cnx;
-        const double h = S->ch;
-        const double ccx = S->cx0 + ((double)(b % nx) + 0.5) * h, ccy = S->cy0 + ((double)(b / nx) + 0.5) * h;
+        const double ccx = S->cx0 + ((double)(b % nx) + 0.5) * S->ch, ccy = S->cy0 + ((double)(b / nx) + 0.5) * S->chy;
         gt.srt[k] = make_float4((float)(v.x[j * v.ps] - ccx), (float)(v.y[j * v.ps] - ccy), (float)v.g[j * v.ps],
                                 (float)v.d[j]);
     }
