@@ -295,6 +295,10 @@ vx_status vx_batch_sync(vx_batch *batch);
 /* out[0] batched steps, [1] kernels they launched, [2] kernels per batched
  * step now, [3] slot-table rebuilds, [4] graph instantiations, [5] bodies. */
 vx_status vx_batch_info(vx_batch *batch, double out6[6]);
+/* Host time spent preparing the batched steps so far: out[0] / [1] the
+ * longest / total capacity growth, [2] / [3] the longest / total
+ * re-recording, merge and upload of the slot tables (ms). */
+vx_status vx_batch_host_times(vx_batch *batch, double out4[4]);
 /* The CUDA stream (cudaStream_t) the batch launches on. */
 void *vx_batch_stream(vx_batch *batch);
 /* Ends the batch (waits for its steps); the bodies return to their own

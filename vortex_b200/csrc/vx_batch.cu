@@ -31,6 +31,7 @@
 // Step / vort_creation (src/unit_1.cu:963-1218); the reference runs one body
 // per process.
 #include <algorithm>
+#include <chrono>
 #include <map>
 #include <string>
 #include <vector>
@@ -140,6 +141,9 @@ struct vx_batch {
     long long launched = 0;       // batched steps launched
     long long kernels = 0;        // kernels launched by the batched steps
     long long rebuilds = 0, reinstantiations = 0;
+    // host time spent in vx_batch_step's preparation of a step: capacity
+    // growth, then re-recording / merging / uploading (max and total, ms)
+    double grow_ms_max = 0.0, grow_ms_sum = 0.0, refresh_ms_max = 0.0, refresh_ms_sum = 0.0;
     bool dirty = true;
 };
 
@@ -617,9 +621,18 @@ extern "C" vx_status vx_batch_step(vx_batch *b, int64_t nsteps) {
     BCU(cudaSetDevice(b->device));
     if (b->bodies.empty()) return VX_OK;
     for (int64_t t = 0; t < nsteps; ++t) {
+        const auto t0 = std::chrono::steady_clock::now();
         vx_status st = ensure_capacities(b);
         if (st != VX_OK) return st;
+        const auto t1 = std::chrono::steady_clock::now();
         if ((st = refresh(b)) != VX_OK) return st;
+        const auto t2 = std::chrono::steady_clock::now();
+        const double gm = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        const double rm = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        b->grow_ms_max = std::max(b->grow_ms_max, gm);
+        b->grow_ms_sum += gm;
+        b->refresh_ms_max = std::max(b->refresh_ms_max, rm);
+        b->refresh_ms_sum += rm;
         const int k = (int)(b->launched & 1);
         BCU(cudaEventSynchronize(b->cnt_ev[k]));   // the host buffer of two steps ago has been read
         BCU(cudaGraphLaunch(b->exec, b->stream));
@@ -690,6 +703,18 @@ extern "C" vx_status vx_batch_info(vx_batch *b, double out6[6]) {
     out6[3] = (double)b->rebuilds;
     out6[4] = (double)b->reinstantiations;
     out6[5] = (double)b->bodies.size();
+    return VX_OK;
+}
+
+// Host time of the steps' preparation: out[0] / [1] the longest / total
+// capacity growth, [2] / [3] the longest / total re-recording, merge and
+// upload (ms).
+extern "C" vx_status vx_batch_host_times(vx_batch *b, double out4[4]) {
+    if (!b || !out4) return VX_ERR_ARG;
+    out4[0] = b->grow_ms_max;
+    out4[1] = b->grow_ms_sum;
+    out4[2] = b->refresh_ms_max;
+    out4[3] = b->refresh_ms_sum;
     return VX_OK;
 }
 
