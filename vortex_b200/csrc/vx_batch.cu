@@ -12,7 +12,7 @@
 // grids laid end to end, and k_many gives each block its body's arguments
 // and block coordinates, so a body computes exactly what its own launches
 // would have computed.  The grids of the scaled grid-stride launches are
-// sized for a share of the GPU proportional to the body's size; the
+// sized for a share of the GPU proportional to the body's capacity; the
 // partitions that fix summation orders follow the body's own count on the
 // device (vx_body_parts and the like), so results are bit-identical to
 // vx_step's.
@@ -366,12 +366,25 @@ static vx_status upload(vx_batch *b) {
     return VX_OK;
 }
 
+// A body's claim on the GPU in a batched step: its store's capacity in
+// units of 2048 vortices (the work of every stage grows with the count; the
+// capacity changes only when the store grows, which re-records the body
+// anyway).  Its share is that claim over the batch's divisor, at most the
+// SMs its own step would use: a stage's blocks then carry about the same
+// work in every body, and the biggest bodies do not run on alone at the end
+// of each stage.
+#ifndef VX_BATCH_FILL
+#define VX_BATCH_FILL 2   // times the members' scaled launches fill the GPU
+#endif
+static long long share_demand(const vx_sim *s) { return std::max(1LL, s->cap / 2048); }
+static void update_share(vx_batch *b);
+
 static BodyKey key_of(vx_batch *b, vx_sim *s) {
     BodyKey k;
     k.cap = s->cap;
     k.rhs = vx_sim_rhs_chunks(s);
     k.sms = vx_sim_step_sms(s);
-    k.share = std::max(1, (k.sms + b->share_div - 1) / b->share_div);
+    k.share = std::max(1, std::min(k.sms, (int)((share_demand(s) + b->share_div - 1) / b->share_div)));
     k.fmm = s->conf.fmm;
     k.leaf = s->prm.fmm_leaf;
     k.lmax = s->w.fmm_lmax;
@@ -381,6 +394,7 @@ static BodyKey key_of(vx_batch *b, vx_sim *s) {
 // Re-record the bodies whose recordings are stale, then merge, lay out,
 // upload and (if needed) re-instantiate.
 static vx_status refresh(vx_batch *b) {
+    update_share(b);   // growth moves the members' claims (the divisor has hysteresis)
     bool changed = b->dirty;
     for (Body &bd : b->bodies) {
         const BodyKey k = key_of(b, bd.s);
@@ -476,13 +490,13 @@ static void release(vx_batch *b) {
 }
 
 // Members' shares of the GPU: the scaled launches of all members together
-// fill it about twice; the divisor is kept while the total demand stays
-// within a factor of two of the one it was set for (a new divisor changes
-// every member's launch shapes, so all are recorded again).
+// fill it VX_BATCH_FILL times; the divisor is kept while the total demand
+// stays within a factor of two of the one it was set for (a new divisor
+// changes every member's launch shapes, so all are recorded again).
 static void update_share(vx_batch *b) {
     long long demand = 0;
-    for (const Body &bd : b->bodies) demand += vx_sim_step_sms(bd.s);
-    const int want = (int)std::max(1LL, demand / (2LL * b->num_sms));
+    for (const Body &bd : b->bodies) demand += share_demand(bd.s);
+    const int want = (int)std::max(1LL, demand / ((long long)VX_BATCH_FILL * b->num_sms));
     if (want > 2 * b->share_div || 2 * want < b->share_div) b->share_div = want;
 }
 
