@@ -157,51 +157,90 @@ static vx_status free_graph(vx_batch *b) {
     return VX_OK;
 }
 
-// Greedy merge of the bodies' launch sequences into slots: repeatedly take
-// the (kernel, block) pair at the head of the most sequences (ties: the one
-// heading the longest remaining sequence) and advance those sequences.
+// Merge of the bodies' launch sequences into slots: a common supersequence
+// of them, built body by body (longest recordings first) by aligning each
+// body's (kernel, block) sequence with the merged one along a longest common
+// subsequence; a slot is one entry of the merged sequence, run by every body
+// aligned to it.  Bodies whose steps differ (direct or quadtree velocity, a
+// quadtree with more levels, the collapse passes) then share every kernel
+// their sequences have in common, in order; a greedy merge (the kernel at
+// the head of the most sequences first) let a minority group fall behind and
+// run the rest of its step in slots of its own (140 slots for the seeded
+// 256-body population instead of about 60).
 static vx_status merge(vx_batch *b) {
     const int nb = (int)b->bodies.size();
-    std::vector<size_t> head((size_t)nb, 0);
-    b->slots.clear();
-    for (;;) {
-        std::map<std::pair<const void *, unsigned>, int> count;
-        std::pair<const void *, unsigned> best{nullptr, 0};
-        int best_n = 0;
-        size_t best_left = 0;
-        for (int i = 0; i < nb; ++i) {
-            const auto &L = b->bodies[(size_t)i].rec.launches;
-            if (head[(size_t)i] >= L.size()) continue;
-            const VxRecLaunch &r = L[head[(size_t)i]];
-            const auto k = std::make_pair(r.key, r.block.x);
-            count[k] += 1;
+    using Key = std::pair<const void *, unsigned>;
+    auto key_at = [&](int i, size_t q) {
+        const VxRecLaunch &r = b->bodies[(size_t)i].rec.launches[q];
+        return Key(r.key, r.block.x);
+    };
+    // the merged sequence (each entry a slot key with a stable id) and, per
+    // body, the slot id of each of its launches
+    std::vector<Key> seq;
+    std::vector<int> seq_id;
+    std::vector<std::vector<int>> at((size_t)nb);
+    int next_id = 0;
+    std::vector<int> order((size_t)nb);
+    for (int i = 0; i < nb; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return b->bodies[(size_t)a].rec.launches.size() > b->bodies[(size_t)c].rec.launches.size();
+    });
+    std::vector<int> dp;
+    // bodies with the same sequence take the same slots (aligned once)
+    std::map<std::vector<Key>, int> seen;
+    for (int i : order) {
+        const size_t m = seq.size(), n = b->bodies[(size_t)i].rec.launches.size();
+        std::vector<Key> mykeys(n);
+        for (size_t c = 0; c < n; ++c) mykeys[c] = key_at(i, c);
+        const auto hit = seen.find(mykeys);
+        if (hit != seen.end()) {
+            at[(size_t)i] = at[(size_t)hit->second];
+            continue;
         }
-        if (count.empty()) break;
-        for (int i = 0; i < nb; ++i) {
-            const auto &L = b->bodies[(size_t)i].rec.launches;
-            if (head[(size_t)i] >= L.size()) continue;
-            const VxRecLaunch &r = L[head[(size_t)i]];
-            const auto k = std::make_pair(r.key, r.block.x);
-            const int c = count[k];
-            const size_t left = L.size() - head[(size_t)i];
-            if (c > best_n || (c == best_n && left > best_left)) {
-                best = k;
-                best_n = c;
-                best_left = left;
+        seen.emplace(std::move(mykeys), i);
+        // longest common subsequence of seq[a..] and the body's launches[c..]
+        dp.assign((m + 1) * (n + 1), 0);
+        for (size_t a = m; a-- > 0;)
+            for (size_t c = n; c-- > 0;)
+                dp[a * (n + 1) + c] = seq[a] == key_at(i, c)
+                                          ? dp[(a + 1) * (n + 1) + c + 1] + 1
+                                          : std::max(dp[(a + 1) * (n + 1) + c], dp[a * (n + 1) + c + 1]);
+        std::vector<Key> ns;
+        std::vector<int> nid;
+        std::vector<int> &mine = at[(size_t)i];
+        mine.assign(n, -1);
+        size_t a = 0, c = 0;
+        while (a < m || c < n) {
+            if (a < m && c < n && seq[a] == key_at(i, c)) {
+                ns.push_back(seq[a]); nid.push_back(seq_id[a]);
+                mine[c] = seq_id[a];
+                ++a; ++c;
+            } else if (c == n || (a < m && dp[(a + 1) * (n + 1) + c] >= dp[a * (n + 1) + c + 1])) {
+                ns.push_back(seq[a]); nid.push_back(seq_id[a]);
+                ++a;
+            } else {
+                ns.push_back(key_at(i, c)); nid.push_back(next_id);
+                mine[c] = next_id++;
+                ++c;
             }
         }
-        Slot sl;
-        sl.key = best.first;
-        for (int i = 0; i < nb; ++i) {
-            const auto &L = b->bodies[(size_t)i].rec.launches;
-            if (head[(size_t)i] >= L.size()) continue;
-            const VxRecLaunch &r = L[head[(size_t)i]];
-            if (r.key != best.first || r.block.x != best.second) continue;
+        seq.swap(ns);
+        seq_id.swap(nid);
+    }
+    std::vector<int> slot_of((size_t)next_id, -1);
+    for (size_t j = 0; j < seq_id.size(); ++j) slot_of[(size_t)seq_id[j]] = (int)j;
+    b->slots.assign(seq.size(), Slot());
+    for (int i = 0; i < nb; ++i) {
+        const auto &L = b->bodies[(size_t)i].rec.launches;
+        for (size_t q = 0; q < L.size(); ++q) {
+            const VxRecLaunch &r = L[q];
+            Slot &sl = b->slots[(size_t)slot_of[(size_t)at[(size_t)i][q]]];
             if (r.grid.y != 1 || r.grid.z != 1 || r.block.y != 1 || r.block.z != 1) {
                 vx_set_error("batch: a step kernel with a multi-dimensional launch cannot be batched");
                 return VX_ERR_ARG;
             }
             if (sl.bodies.empty()) {
+                sl.key = r.key;
                 sl.many = r.many;
                 sl.block = r.block;
                 sl.pack = r.size;
@@ -211,11 +250,9 @@ static vx_status merge(vx_batch *b) {
             }
             sl.smem = std::max(sl.smem, r.smem);
             sl.bodies.push_back(i);
-            sl.launch.push_back((int)head[(size_t)i]);
+            sl.launch.push_back((int)q);
             sl.total += r.grid.x;
-            head[(size_t)i] += 1;
         }
-        b->slots.push_back(std::move(sl));
     }
     return VX_OK;
 }
@@ -374,7 +411,7 @@ static vx_status upload(vx_batch *b) {
 // work in every body, and the biggest bodies do not run on alone at the end
 // of each stage.
 #ifndef VX_BATCH_FILL
-#define VX_BATCH_FILL 2   // times the members' scaled launches fill the GPU
+#define VX_BATCH_FILL 8   // times the members' scaled launches fill the GPU
 #endif
 static long long share_demand(const vx_sim *s) { return std::max(1LL, s->cap / 2048); }
 static void update_share(vx_batch *b);
