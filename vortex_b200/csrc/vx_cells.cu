@@ -539,13 +539,15 @@ __global__ void __launch_bounds__(CG_T, VX_DIFF_MINB) k_diff_cells(VxParams p, V
 }
 
 // Targets left out of the work items (radius beyond CG_KCAP rows).  Most
-// have windows of a few thousand sources: one warp each (k_diff_wide), the
-// lanes taking the concatenated sources of 32 rows at a time.  An isolated
-// vortex, whose window spans more than WIDE_ROWS rows each side (up to the
-// whole grid), is passed on to k_diff_huge: one block of WIDE_T threads each,
-// its warps taking every (WIDE_T / 32)-th batch of 32 rows.  FP32 pair sums
-// per lane over at most 16 sources, FP64 beyond (fixed order).
-constexpr int WIDE_ROWS = 3 * CG_DIV_Y;   // three mean cut-off radii
+// have windows of about a thousand sources inside their circles (the sparse
+// edge of a Gaussian cloud: about 1 % of its vortices): one warp each
+// (k_diff_wide), the lanes taking the concatenated sources of 32 rows at a
+// time.  A vortex whose window spans more than WIDE_ROWS rows each side (up
+// to the whole grid: a vortex flung far from the cloud) is passed on to
+// k_diff_huge: one block of WIDE_T threads each, its warps taking the rows in
+// batches of equal height.  FP32 pair sums per lane over at most 16 sources,
+// FP64 beyond (fixed order).
+constexpr int WIDE_ROWS = 16 * CG_DIV_Y;   // sixteen mean cut-off radii
 constexpr int WIDE_T = 512;
 
 // Rows dy0 .. dy0 + nr - 1 (nr <= 32) of one target's window: lane l lists
@@ -684,8 +686,10 @@ VX_DEVK void k_diff_huge_body(VxBlkB<WIDE_T, 0> vb, const VxParams &p, const VxV
         const float R = cut * me.w, R2 = R * R, ndd = -log2e / me.w;
         const long long kk = min((long long)ceilf(R / hy), ny);
         double I2x = 0.0, I2y = 0.0, I1 = 0.0;
-        for (long long dy0 = -kk + 32 * warp; dy0 <= kk; dy0 += 32 * NWARP)
-            wide_rows32(S, srt, skey, start, me, row, ocol, R, R2, ndd, thr2, dy0, (int)min(32LL, kk - dy0 + 1),
+        // every warp takes batches of rpw rows (all warps busy whatever the window's height)
+        const long long rpw = min(32LL, (2 * kk + 1 + NWARP - 1) / NWARP);
+        for (long long dy0 = -kk + rpw * warp; dy0 <= kk; dy0 += rpw * NWARP)
+            wide_rows32(S, srt, skey, start, me, row, ocol, R, R2, ndd, thr2, dy0, (int)min(rpw, kk - dy0 + 1),
                         lane, stab[warp], I2x, I2y, I1, pairs);
         for (int o = 16; o > 0; o >>= 1) {
             I2x += __shfl_xor_sync(0xffffffffu, I2x, o);

@@ -469,7 +469,16 @@ __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int 
     const int lc = 4 * cg + pt;
     const long long tx0 = (t % tiles1) * M2L_TILE, ty0 = (t / tiles1) * M2L_TILE;
     const long long sx0 = tx0 - 2, sy0 = ty0 - 2;   // staged region origin
-    __syncthreads();   // the previous tile is done with sm / sc; tables are built
+    const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
+    const bool live = ix < m && iy < m;
+    c = live ? iy * m + ix : 0;
+    // the barrier: the previous tile is done with sm / sc, tables are built;
+    // a tile with no vortex under any of its cells is skipped (an empty
+    // cell's local expansion is never read: L2L and L2P read busy cells only)
+    if (!__syncthreads_or(live && cl[c] > 0)) {
+        busy = false;
+        return false;
+    }
     for (int e = threadIdx.x; e < M2L_SRC * M2L_SRC * P; e += blockDim.x) {
         const int q = e / P, k = e % P;
         const long long qx = sx0 + q % M2L_SRC, qy = sy0 + q / M2L_SRC;
@@ -480,9 +489,6 @@ __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int 
         T.sm[q][k] = n > 0 ? Ml[src * P + k] : cplx{0.0, 0.0};
     }
     __syncthreads();
-    const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
-    const bool live = ix < m && iy < m;
-    c = live ? iy * m + ix : 0;
     busy = live && cl[c] > 0;
     const long long px = ix >> 1, py = iy >> 1;
     double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // (re, im) of coefficients 4 cg + j
