@@ -297,8 +297,9 @@ vx_status vx_batch_sync(vx_batch *batch);
 vx_status vx_batch_info(vx_batch *batch, double out6[6]);
 /* Host time spent preparing the batched steps so far: out[0] / [1] the
  * longest / total capacity growth, [2] / [3] the longest / total
- * re-recording, merge and upload of the slot tables (ms). */
-vx_status vx_batch_host_times(vx_batch *batch, double out4[4]);
+ * re-recording, merge and upload of the slot tables, [4..7] the longest
+ * re-recording, merge + layout, upload and graph build (ms). */
+vx_status vx_batch_host_times(vx_batch *batch, double out8[8]);
 /* The CUDA stream (cudaStream_t) the batch launches on. */
 void *vx_batch_stream(vx_batch *batch);
 /* Ends the batch (waits for its steps); the bodies return to their own

@@ -144,6 +144,8 @@ struct vx_batch {
     // host time spent in vx_batch_step's preparation of a step: capacity
     // growth, then re-recording / merging / uploading (max and total, ms)
     double grow_ms_max = 0.0, grow_ms_sum = 0.0, refresh_ms_max = 0.0, refresh_ms_sum = 0.0;
+    // the longest of refresh's phases: re-recording, merge + layout, upload, graph build (ms)
+    double phase_ms_max[4] = {0.0, 0.0, 0.0, 0.0};
     bool dirty = true;
 };
 
@@ -430,7 +432,16 @@ static BodyKey key_of(vx_batch *b, vx_sim *s) {
 
 // Re-record the bodies whose recordings are stale, then merge, lay out,
 // upload and (if needed) re-instantiate.
+static double ms_since(std::chrono::steady_clock::time_point &t) {
+    const auto now = std::chrono::steady_clock::now();
+    const double ms = std::chrono::duration<double, std::milli>(now - t).count();
+    t = now;
+    return ms;
+}
+
 static vx_status refresh(vx_batch *b) {
+    auto tp = std::chrono::steady_clock::now();
+    auto phase = [&](int q) { b->phase_ms_max[q] = std::max(b->phase_ms_max[q], ms_since(tp)); };
     update_share(b);   // growth moves the members' claims (the divisor has hysteresis)
     bool changed = b->dirty;
     for (Body &bd : b->bodies) {
@@ -447,6 +458,7 @@ static vx_status refresh(vx_batch *b) {
         bd.recorded = true;
         changed = true;
     }
+    phase(0);
     if (!changed) return VX_OK;
     vx_status st = merge(b);
     if (st != VX_OK) return st;
@@ -460,8 +472,11 @@ static vx_status refresh(vx_batch *b) {
         b->arena_cap = cap;
         need = layout(b, b->d_arena);
     }
+    phase(1);
     if ((st = upload(b)) != VX_OK) return st;
+    phase(2);
     if (!graph_fits(b) && (st = build_graph(b)) != VX_OK) return st;
+    phase(3);
     b->rebuilds += 1;
     b->dirty = false;
     return VX_OK;
@@ -759,13 +774,15 @@ extern "C" vx_status vx_batch_info(vx_batch *b, double out6[6]) {
 
 // Host time of the steps' preparation: out[0] / [1] the longest / total
 // capacity growth, [2] / [3] the longest / total re-recording, merge and
-// upload (ms).
-extern "C" vx_status vx_batch_host_times(vx_batch *b, double out4[4]) {
-    if (!b || !out4) return VX_ERR_ARG;
-    out4[0] = b->grow_ms_max;
-    out4[1] = b->grow_ms_sum;
-    out4[2] = b->refresh_ms_max;
-    out4[3] = b->refresh_ms_sum;
+// upload, [4..7] the longest re-recording, merge + layout, upload and graph
+// build (ms).
+extern "C" vx_status vx_batch_host_times(vx_batch *b, double out8[8]) {
+    if (!b || !out8) return VX_ERR_ARG;
+    out8[0] = b->grow_ms_max;
+    out8[1] = b->grow_ms_sum;
+    out8[2] = b->refresh_ms_max;
+    out8[3] = b->refresh_ms_sum;
+    for (int q = 0; q < 4; ++q) out8[4 + q] = b->phase_ms_max[q];
     return VX_OK;
 }
 

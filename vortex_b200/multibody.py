@@ -147,7 +147,8 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
     if info:
         out["graph_instantiations"] = info["graph_instantiations"]
         out["slot_table_rebuilds"] = info["rebuilds"]
-        for k in ("host_grow_ms_max", "host_grow_ms_total", "host_refresh_ms_max", "host_refresh_ms_total"):
+        for k in ("host_grow_ms_max", "host_grow_ms_total", "host_refresh_ms_max", "host_refresh_ms_total",
+                  "host_phase_ms_max"):
             out[k] = info[k]
         batch.close()
     if own:

@@ -416,12 +416,14 @@ class Batch:
     def info(self) -> dict:
         o = np.zeros(6)
         _check(lib().vx_batch_info(self.h, _p(o)), "vx_batch_info")
-        t = np.zeros(4)
+        t = np.zeros(8)
         _check(lib().vx_batch_host_times(self.h, _p(t)), "vx_batch_host_times")
         return {"steps": int(o[0]), "kernels": int(o[1]), "kernels_per_step": int(o[2]), "rebuilds": int(o[3]),
                 "graph_instantiations": int(o[4]), "bodies": int(o[5]),
                 "host_grow_ms_max": float(t[0]), "host_grow_ms_total": float(t[1]),
-                "host_refresh_ms_max": float(t[2]), "host_refresh_ms_total": float(t[3])}
+                "host_refresh_ms_max": float(t[2]), "host_refresh_ms_total": float(t[3]),
+                "host_phase_ms_max": {"record": float(t[4]), "merge": float(t[5]), "upload": float(t[6]),
+                                      "graph": float(t[7])}}
 
     def close(self):
         if self.h:
