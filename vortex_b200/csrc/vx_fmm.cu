@@ -872,13 +872,10 @@ VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars 
         if (lane < 12) run[lane] = e;
         if (lane == 12) run[12].pre = total;
         __syncwarp();
-        // two independent triples (even and odd staged sources) halve the
-        // insertion's dependency chain; merged at the end (the 3 smallest of
-        // a set do not depend on the order of insertion)
-        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f, e1 = 1e5f, e2 = 1e5f, e3 = 1e5f;
+        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
         int rc = 0;
-        // the next chunk's source is loaded before the current chunk's tests run
-        auto fetch = [&](int f) {
+        for (int f0 = 0; f0 < total; f0 += 32) {
+            const int f = f0 + lane;
             float4 q = make_float4(1e18f, 1e18f, 0.f, __int_as_float(-1));   // padding: never among the 3
             if (f < total) {
                 while (run[rc + 1].pre <= f) ++rc;
@@ -887,27 +884,17 @@ VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars 
                 const float2 s2 = *reinterpret_cast<const float2 *>(srt + slot);   // x, y of the source
                 q = make_float4(s2.x + r.ox, s2.y + r.oy, 0.f, __int_as_float(slot));
             }
-            return q;
-        };
-        float4 qn = fetch(lane);
-        for (int f0 = 0; f0 < total; f0 += 32) {
-            wq[lane] = qn;
+            wq[lane] = q;
             __syncwarp();
-            qn = fetch(f0 + 32 + lane);
 #pragma unroll 8
-            for (int k = 0; k < 32; k += 2) {
-                const float4 sa = wq[k], sb = wq[k + 1];
-                const float dxa = me.x - sa.x, dya = me.y - sa.y;
-                const float dxb = me.x - sb.x, dyb = me.y - sb.y;
-                const float ra = fmaf(dxa, dxa, dya * dya), rb = fmaf(dxb, dxb, dyb * dyb);
-                vx_nn3_insert_bf(d1, d2, d3, __float_as_int(sa.w) == t ? 1e30f : ra);
-                vx_nn3_insert_bf(e1, e2, e3, __float_as_int(sb.w) == t ? 1e30f : rb);
+            for (int k = 0; k < 32; ++k) {
+                const float4 s = wq[k];
+                const float dx = me.x - s.x, dy = me.y - s.y;
+                const float r2 = fmaf(dx, dx, dy * dy);
+                vx_nn3_insert_bf(d1, d2, d3, __float_as_int(s.w) == t ? 1e30f : r2);
             }
             __syncwarp();
         }
-        vx_nn3_insert_bf(d1, d2, d3, e1);
-        vx_nn3_insert_bf(d1, d2, d3, e2);
-        vx_nn3_insert_bf(d1, d2, d3, e3);
         if (act) {
             v.d[j] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
             if (!(d3 < sq2)) {   // a closer source could lie outside the target's 3x3 quarters
