@@ -796,114 +796,14 @@ __global__ void __launch_bounds__(FMM_T, VX_NEAR_MINB) k_fmm_near(VxParams p, Vx
 
 // The 3 nearest sources of every live target (the reference's padded
 // launch: sources include the round-32 slots after the live ones; the
-// target itself excluded) over the quarter leaves around its own quarter
-// (each quarter a contiguous run of the sorted sources; coordinates relative
-// to the target's leaf centre, computed as the near field computes them).
-// Exact when the third distance is below the quarter's side (every source
-// outside the target's 3 x 3 quarters is farther); the others go to the ring
-// search over leaves (k_fmm_nn3_fix).
-//
-// One warp per near-field work item (up to 32 targets of one leaf): the
-// 4 x 4 quarters around the leaf (its own four and a ring of quarters of the
-// neighbouring leaves: 12 runs, every target's 3 x 3 among them) are staged
-// 32 sources at a time in the warp's shared memory, and every lane tests its
-// target against each staged source (a broadcast load).  The extra
-// candidates lie outside the target's own 3 x 3, so with d3 below the
-// quarter side they cannot be among the 3 nearest and the result is the
-// one the 3 x 3 gives; a target the 3 x 3 alone would have flagged is not
-// flagged when the 4 x 4 brings its third distance below the quarter side,
-// and is then exact all the same.  A thread per target over its own 3 x 3
-// (VX_NN3_WARP 0) diverges across the quarters of a warp's targets and
-// waits on dependent global loads.
-#ifndef VX_NN3_WARP
-#define VX_NN3_WARP 1
-#endif
-struct Nn3Run {
-    int j0, pre;     // first slot; sources of the runs before it (entry 12 holds the total)
-    float ox, oy;    // offset of the run's leaf centre from the item's
-};
+// target itself excluded), one thread per target, over the 3 x 3 quarter
+// leaves around its own quarter (each quarter a contiguous run of the
+// sorted sources; coordinates relative to the target's leaf centre,
+// computed as the near field computes them).  Exact when the third distance
+// is below the quarter's side (every source outside the 3 x 3 block is
+// farther); the others go to the ring search over leaves (k_fmm_nn3_fix).
 VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S, const float4 *srt, const unsigned *skey,
-                                const int *sorted, const int *substart, const int2 *items, int *flag_list) {
-#if VX_NN3_WARP
-    __shared__ Nn3Run srun[FMM_T / 32][13];
-    __shared__ float4 sq[FMM_T];   // staged sources: x, y (item frame), slot (as bits)
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    Nn3Run *run = srun[wid];
-    float4 *wq = sq + 32 * wid;
-    const long long n = S->n;
-    const int m = 1 << S->fL, m2 = 2 * m;
-    const double h = S->fside / (double)m;
-    const float hf = (float)h;
-    const float sq2 = (float)(0.25 * h * h);   // (quarter side)^2
-    const long long nitems = S->cnitems;
-    const long long wpb = FMM_T / 32;
-    for (long long it = vb.x * wpb + wid; it < nitems; it += vb.n * wpb) {
-        const int2 item = items[it];
-        const int leaf = item.x, row = leaf / m, col = leaf % m;
-        const int last = min(item.y + FMM_W, substart[4 * leaf + 4]);
-        const int t = item.y + lane;
-        const int j = t < last ? sorted[t] : -1;
-        const bool act = j >= 0 && j < n;
-        const float4 me = act ? srt[t] : make_float4(0.f, 0.f, 0.f, 0.f);
-        // lane r < 12: quarter row Y2 = 2 row - 1 + r / 3, part r % 3 (the
-        // left leaf's right quarter, the leaf's own two, the right leaf's
-        // left quarter)
-        Nn3Run e = {0, 0, 0.f, 0.f};
-        int len = 0;
-        if (lane < 12) {
-            const int Y2 = 2 * row - 1 + lane / 3, part = lane % 3, lc = col + part - 1;
-            if (Y2 >= 0 && Y2 < m2 && lc >= 0 && lc < m) {
-                const int lr = Y2 >> 1;
-                const int base = 4 * (lr * m + lc) + 2 * (Y2 & 1);
-                const int k0 = part == 0 ? base + 1 : base, k1 = part == 2 ? base : base + 1;
-                e.j0 = substart[k0];
-                len = substart[k1 + 1] - e.j0;
-                e.ox = (float)(lc - col) * hf;
-                e.oy = (float)(lr - row) * hf;
-            }
-        }
-        int inc = len;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += u;
-        }
-        const int total = __shfl_sync(0xffffffffu, inc, 31);
-        e.pre = inc - len;
-        if (lane < 12) run[lane] = e;
-        if (lane == 12) run[12].pre = total;
-        __syncwarp();
-        float d1 = 1e5f, d2 = 1e5f, d3 = 1e5f;
-        int rc = 0;
-        for (int f0 = 0; f0 < total; f0 += 32) {
-            const int f = f0 + lane;
-            float4 q = make_float4(1e18f, 1e18f, 0.f, __int_as_float(-1));   // padding: never among the 3
-            if (f < total) {
-                while (run[rc + 1].pre <= f) ++rc;
-                const Nn3Run r = run[rc];
-                const int slot = r.j0 + (f - r.pre);
-                const float2 s2 = *reinterpret_cast<const float2 *>(srt + slot);   // x, y of the source
-                q = make_float4(s2.x + r.ox, s2.y + r.oy, 0.f, __int_as_float(slot));
-            }
-            wq[lane] = q;
-            __syncwarp();
-#pragma unroll 8
-            for (int k = 0; k < 32; ++k) {
-                const float4 s = wq[k];
-                const float dx = me.x - s.x, dy = me.y - s.y;
-                const float r2 = fmaf(dx, dx, dy * dy);
-                vx_nn3_insert_bf(d1, d2, d3, __float_as_int(s.w) == t ? 1e30f : r2);
-            }
-            __syncwarp();
-        }
-        if (act) {
-            v.d[j] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
-            if (!(d3 < sq2)) {   // a closer source could lie outside the target's 3x3 quarters
-                const int slot = atomicAdd(&S->fnflag, 1);
-                flag_list[slot] = t;
-            }
-        }
-    }
-#else
+                                const int *sorted, const int *substart, int *flag_list) {
     const long long s = S->fs, n = S->n;
     const int m = 1 << S->fL, m2 = 2 * m;
     const double h = S->fside / (double)m;
@@ -943,13 +843,11 @@ VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars 
             flag_list[slot] = (int)t;
         }
     }
-#endif
 }
 __global__ void __launch_bounds__(FMM_T) k_fmm_nn3_sub(VxView v, VxScalars *S, const float4 *srt, const unsigned *skey,
-                                                      const int *sorted, const int *substart, const int2 *items,
-                                                      int *flag_list) {
+                                                      const int *sorted, const int *substart, int *flag_list) {
     VX_PDL_WAIT();
-    k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, v, S, srt, skey, sorted, substart, items, flag_list);
+    k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0>{blockIdx.x, gridDim.x}, v, S, srt, skey, sorted, substart, flag_list);
 }
 
 // Targets whose third-nearest distance reached the leaf side: exact 3
@@ -1180,9 +1078,8 @@ static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxVi
     vx_launch<k_fmm_near<P>, k_fmm_near_body<P>>(L, L.num_sms * 8, FMM_T, 0, p, v, S, w.srt, sorted, w.fmm_start,
                                                  w.items, (const cplx *)w.fmm_L);
     VX_EV(L, 1);
-    vx_launch<k_fmm_nn3_sub, k_fmm_nn3_sub_body>(L, VX_NN3_WARP ? L.num_sms * 8 : grid, FMM_T, 0, v, S, w.srt, skey,
-                                                 sorted, (const int *)w.fmm_sub_start, (const int2 *)w.items,
-                                                 w.fmm_flags);
+    vx_launch<k_fmm_nn3_sub, k_fmm_nn3_sub_body>(L, grid, FMM_T, 0, v, S, w.srt, skey, sorted,
+                                                 (const int *)w.fmm_sub_start, w.fmm_flags);
 
     vx_launch<k_fmm_nn3_fix, k_fmm_nn3_fix_body>(L, grid, FMM_T, 0, v, S, w.srt, sorted, w.fmm_start, w.fmm_flags, w.fmm_brute);
 
