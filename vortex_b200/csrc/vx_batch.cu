@@ -146,6 +146,10 @@ struct vx_batch {
     double grow_ms_max = 0.0, grow_ms_sum = 0.0, refresh_ms_max = 0.0, refresh_ms_sum = 0.0;
     // the longest of refresh's phases: re-recording, merge + layout, upload, graph build (ms)
     double phase_ms_max[4] = {0.0, 0.0, 0.0, 0.0};
+    // pinned buffers outgrown while steps were in flight: freed at destroy
+    // (cudaFreeHost waits for the whole device, which would drain the
+    // pipeline of batched steps)
+    std::vector<void *> retired;
     bool dirty = true;
 };
 
@@ -393,11 +397,12 @@ static vx_status upload(vx_batch *b) {
     b->stage_idx ^= 1;
     BCU(cudaEventSynchronize(b->stage_ev[k]));
     if (b->stage_cap[k] < size) {
-        if (b->h_stage[k]) cudaFreeHost(b->h_stage[k]);
+        if (b->h_stage[k]) b->retired.push_back(b->h_stage[k]);
         b->h_stage[k] = nullptr;
         b->stage_cap[k] = 0;
-        BCU(cudaMallocHost(&b->h_stage[k], size));
-        b->stage_cap[k] = size;
+        const size_t cap = size + size / 2;   // headroom: members' tables grow with them
+        BCU(cudaMallocHost(&b->h_stage[k], cap));
+        b->stage_cap[k] = cap;
     }
     memcpy(b->h_stage[k], b->h_arena.data(), size);
     BCU(cudaMemcpyAsync(b->d_arena, b->h_stage[k], size, cudaMemcpyHostToDevice, b->stream));
@@ -538,6 +543,8 @@ static void release(vx_batch *b) {
         if (b->stage_ev[k]) cudaEventDestroy(b->stage_ev[k]);
         if (b->cnt_ev[k]) cudaEventDestroy(b->cnt_ev[k]);
     }
+    for (void *h : b->retired) cudaFreeHost(h);
+    b->retired.clear();
     if (b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -567,7 +574,7 @@ static vx_status gather_room(vx_batch *b, size_t nb) {
         if (old) {
             const size_t keep = std::min(b->cnt_members[k].size(), b->gather_cap);
             memcpy(grown, old, sizeof(double) * GATHER * keep);
-            cudaFreeHost(old);
+            b->retired.push_back(old);
         }
         b->h_gather[k] = grown;
     }
