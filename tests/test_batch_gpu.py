@@ -25,9 +25,10 @@ def _bodies():
     out = []
     specs = [dict(index=0, kind="ellipse", panels=260, b=0.2, angle=0.0, re=800.0, n0=3000, dt=0.005 * 200 / 260,
                   cloud_seed=11),
-             # a store of 24 576 slots (the smallest growth margin, 8192) that
-             # 900 births a step outgrow within the test's 14 steps
-             dict(index=1, kind="plate", panels=900, b=0.1, angle=25.0, re=5000.0, n0=15420, dt=0.005 * 200 / 900,
+             # a store of 32 768 slots (the cloud's need and the smallest
+             # growth margin, 8192) that 900 births a step outgrow within the
+             # test's 14 steps
+             dict(index=1, kind="plate", panels=900, b=0.1, angle=25.0, re=5000.0, n0=23500, dt=0.005 * 200 / 900,
                   cloud_seed=12),
              dict(index=2, kind="ellipse", panels=1500, b=0.45, angle=0.0, re=12000.0, n0=150000,
                   dt=0.005 * 200 / 1500, cloud_seed=13)]

@@ -308,7 +308,11 @@ static void drop_graph(vx_sim *s) {
 // Grow the particle store to at least `need` slots, keeping every slot's
 // content (the dead tail matters: it enters the next 3-nearest search).
 static vx_status grow(vx_sim *s, long long need) {
-    long long ncap = std::max(need, s->cap + std::max<long long>(s->conf.inc_step, 8192));
+    // a growth adds at least one increment (inc_step, 8192 at least) or a
+    // quarter; the first store also gets one increment beyond what its
+    // cloud needs, so a new body does not grow at its second step
+    const long long inc = std::max<long long>(s->conf.inc_step, 8192);
+    long long ncap = s->cap > 0 ? std::max(need, s->cap + inc) : need + inc;
     ncap = std::max(ncap, (long long)(s->cap * 1.25));
     ncap = vx_ceil_div(ncap, 8192) * 8192;
     double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};

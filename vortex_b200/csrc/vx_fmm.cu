@@ -123,6 +123,12 @@ VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S,
     const double y0 = vx_dunkey(sk[2][0]), y1 = -vx_dunkey(sk[3][0]);
     double side = fmax(x1 - x0, y1 - y0);
     side = side * (1.0 + 1e-9) + 1e-12;
+    // the depth's ceiling follows the count, not the store's capacity (the
+    // arrays are sized for the capacity's ceiling, which is never lower), so
+    // the tree does not depend on when the store grew
+    int Lc = 2;
+    while (Lc < 10 && (double)(1LL << (2 * Lc)) * 8.0 < (double)vx_round32(n)) ++Lc;
+    Lmax = min(Lmax, Lc);
     int L = 2;
     while (L < Lmax && (double)(1LL << (2 * L)) * (double)leaf < (double)n) ++L;
     if (q2 > 0 && s_prev > 0 && side_prev > 0.0 && L_prev >= 1) {
