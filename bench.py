@@ -470,7 +470,7 @@ def multibody_runs(args, device, rank, world):
                                    mode="graph", population=pop)
             # the same bodies (a few steps later) as concurrent per-body step
             # graphs, for comparison
-            streams = MB.run_batch(steps=3, warmup=1, device=device, rank=rank, world=world, mode="streams",
+            streams = MB.run_batch(steps=5, warmup=1, device=device, rank=rank, world=world, mode="streams",
                                    population=pop)
         finally:
             for s in pop[1]:
@@ -668,7 +668,7 @@ def main():
     ap.add_argument("--no-multibody", dest="multibody", action="store_false",
                     help="skip the seeded multi-body population batched and served")
     ap.add_argument("--batch-bodies", type=int, default=256)
-    ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--serve-requests", type=int, default=32)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

@@ -309,10 +309,10 @@ static void drop_graph(vx_sim *s) {
 // content (the dead tail matters: it enters the next 3-nearest search).
 static vx_status grow(vx_sim *s, long long need) {
     // a growth adds at least one increment (inc_step, 8192 at least) or a
-    // quarter; the first store also gets one increment beyond what its
-    // cloud needs, so a new body does not grow at its second step
+    // quarter; the first store gets the same margin beyond what its cloud
+    // needs, so a new body does not grow within its first steps
     const long long inc = std::max<long long>(s->conf.inc_step, 8192);
-    long long ncap = s->cap > 0 ? std::max(need, s->cap + inc) : need + inc;
+    long long ncap = s->cap > 0 ? std::max(need, s->cap + inc) : std::max(need + inc, (long long)(need * 1.25));
     ncap = std::max(ncap, (long long)(s->cap * 1.25));
     ncap = vx_ceil_div(ncap, 8192) * 8192;
     double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};
