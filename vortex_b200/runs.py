@@ -1,6 +1,7 @@
-"""Long runs of two configurations, FP32-bulk form, on one GPU:
+"""Long runs of two configurations on one GPU (FP32-bulk form; config2 also
+in the plain FP64 form):
 
-    python -m vortex_b200.runs config2 [--steps 3000]
+    python -m vortex_b200.runs config2 [--steps 3000] [--precision fp64]
     python -m vortex_b200.runs config3 [--steps 5000] [--n0 3000000]
 
 config2: the 1000-panel cylinder of radius 0.5 (the benchmark's body),
@@ -66,10 +67,11 @@ def _stats(f, window, scale):
             "cl_rms": float(cl.std())}
 
 
-def config2(steps: int = 3000, every: int = 100, device: int = 0) -> dict:
+def config2(steps: int = 3000, every: int = 100, device: int = 0, precision: int = N.PREC_FP32) -> dict:
     pan = wl.cylinder_panels(1000)
-    sim = N.Sim(wl.cylinder_conf(N.PREC_FP32, 1000), pan, device=device)
-    rec = {"config": "cylinder R=0.5, 1000 panels, impulsive start, Re 2000, dt 0.002, FP32-bulk",
+    sim = N.Sim(wl.cylinder_conf(precision, 1000), pan, device=device)
+    form = "FP32-bulk" if precision == N.PREC_FP32 else "plain FP64"
+    rec = {"config": f"cylinder R=0.5, 1000 panels, impulsive start, Re 2000, dt 0.002, {form}",
            "steps": steps}
     t0 = time.perf_counter()
     f = _timed_steps(sim, steps, every, rec)
@@ -141,9 +143,12 @@ def main():
     ap.add_argument("which", choices=["config2", "config3"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--n0", type=int, default=3_000_000)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
+                    help="config2: the FP32-bulk form (default) or the plain FP64 form")
     a = ap.parse_args()
     if a.which == "config2":
-        print(json.dumps(config2(a.steps or 3000)))
+        prec = N.PREC_FP32 if a.precision == "fp32" else N.PREC_FP64
+        print(json.dumps(config2(a.steps or 3000, precision=prec)))
     else:
         print(json.dumps(config3(a.steps or 5000, a.n0)))
 
