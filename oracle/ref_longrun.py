@@ -6,10 +6,18 @@ src/main.c + src/unit_1.cu + src/kernel.cu, built with -DNO_TREE by
 oracle/build_ref.sh) with the configuration of the 1000-panel cylinder at
 Re 2000, dt 0.002 (core radius = panel length, same-sign collapse within
 0.3 eps, window [-2, 10] x [-10, 10]; src/main.c:60-110 reads these keys),
-no restart frame, and reads the count it logs every step in its timings
+started from a restart frame that holds one vortex of zero strength outside
+the window (killed at the first step, and adding exactly zero to every sum
+before that), and reads the count it logs every step in its timings
 file (src/main.c:689, "<step>\tN = <count>\t...").  The count is the
 checker for the library's own long run of the same configuration
 (`python -m vortex_b200.runs config2`).
+
+Why the frame: a start without one goes through incr_vort_quant, which
+returns randomize_tail's value (src/unit_1.cu:554), and randomize_tail ends
+without a return statement (src/unit_1.cu:488-510), so the program may stop
+with "Increase ERROR!" before its first step (it did here); the restart
+path calls randomize_tail without looking at its value (src/main.c:564).
 
     python -m oracle.ref_longrun [--steps 3000] [--every 100]
 """
@@ -52,6 +60,7 @@ rc_x 0.0
 rc_y 0.0
 matrix_load 0
 timings_file output/timings.txt
+kadr_file Kadr000000.txt
 """
 
 
@@ -64,11 +73,14 @@ def run(steps: int, every: int) -> dict:
         profiles.write_profile(os.path.join(wd, "circle1000.txt"), profiles.circle(1000))
         with open(os.path.join(wd, "run.conf"), "w") as fh:
             fh.write(CONF.format(steps=steps, eps=2 * math.pi * 0.5 / 1000))
+        with open(os.path.join(wd, "Kadr000000.txt"), "w") as fh:   # the frame src/main.c:190-203 reads
+            fh.write("1\n0 0.008000 50 0 0 0 0 0\n")
         t0 = time.perf_counter()
-        r = subprocess.run([EXE, "-c", "run.conf", "-l", "1"], cwd=wd, capture_output=True, text=True)
+        r = subprocess.run([EXE, "-c", "run.conf", "-l", "3"], cwd=wd, capture_output=True, text=True)
         wall = time.perf_counter() - t0
         if r.returncode != 0:
-            return {"unavailable": f"reference program exited {r.returncode}: {r.stderr[-300:]}"}
+            return {"unavailable": f"reference program exited {r.returncode}",
+                    "output_tail": (r.stdout[-1500:] + r.stderr[-500:])}
         counts = {}
         for line in open(os.path.join(wd, "output", "timings.txt")):
             parts = line.strip().split("\t")
