@@ -591,6 +591,7 @@ static vx_status set_count(vx_sim *s, long long n) {
     s->h_S->n = n;
     s->h_S->n0 = n >= s->P ? n - s->P : 0;   // the last P count as this step's newborns
     s->h_S->fsq = 0;                          // a new cloud: the quadtree depth starts from the box rule
+    s->h_S->fLcap = 0;
     CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
     CU(cudaStreamSynchronize(s->stream));
     s->n_upper = n;
@@ -771,11 +772,11 @@ struct CkptHead {
     double vinf[2], dg, fx, fy, m, raw[4];
     uint64_t panel_hash;     // FNV-1a of the panel records
     // version 2: the last quadtree build (sum of count^2 over its quarter
-    // cells, its sources, box side and depth)
+    // cells, its sources, box side and depth) and the depth rule's ceiling
     uint64_t tree_sq;
     int64_t tree_s;
     double tree_side;
-    int32_t tree_L, pad2;
+    int32_t tree_L, tree_Lcap;
 };
 constexpr size_t kCkptHeadV1 = offsetof(CkptHead, tree_sq);
 const char kCkptMagic[8] = {'V', 'X', 'C', 'K', 'P', 'T', '1', 0};
@@ -801,7 +802,7 @@ extern "C" vx_status vx_checkpoint_save(vx_sim *s, const char *path) {
     memset(&hd, 0, sizeof(hd));
     memcpy(hd.magic, kCkptMagic, 8);
     hd.version = 2; hd.P = s->P; hd.prec = s->prm.prec;
-    hd.tree_sq = h.fsq; hd.tree_s = h.fs; hd.tree_side = h.fside; hd.tree_L = h.fL;
+    hd.tree_sq = h.fsq; hd.tree_s = h.fs; hd.tree_side = h.fside; hd.tree_L = h.fL; hd.tree_Lcap = h.fLcap;
     hd.n = h.n; hd.n0 = h.n0; hd.step = h.step; hd.slots = s->cap;
     hd.vinf[0] = h.vinf[0]; hd.vinf[1] = h.vinf[1];
     hd.dg = h.dg; hd.fx = h.fx; hd.fy = h.fy; hd.m = h.m;
@@ -861,6 +862,7 @@ extern "C" vx_status vx_checkpoint_load(vx_sim *s, const char *path) {
     h->dg = hd.dg; h->fx = hd.fx; h->fy = hd.fy; h->m = hd.m;
     for (int q = 0; q < 4; ++q) h->raw[q] = hd.raw[q];
     h->fsq = hd.tree_sq;
+    h->fLcap = hd.tree_Lcap;
     if (hd.tree_sq) { h->fs = hd.tree_s; h->fside = hd.tree_side; h->fL = hd.tree_L; }
     CU(cudaMemcpyAsync(s->d_S, s->h_S, sizeof(VxScalars), cudaMemcpyHostToDevice, s->stream));
     CU(cudaStreamSynchronize(s->stream));

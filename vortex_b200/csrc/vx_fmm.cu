@@ -73,7 +73,8 @@ extern __shared__ __align__(16) unsigned char vx_fmm_dyn[];
 // cloud (a dense wall layer, a Gaussian core) then gets the depth its dense
 // part needs rather than the one its bounding box implies; a uniform one
 // keeps ceil(log4(n / leaf)).  The first build of a body (no measurement yet)
-// uses the box rule alone.
+// uses the box rule alone.  Deepening stops one level above a build whose
+// 3-nearest pass left more than 0.5 % of its targets to the exact search.
 VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S, double eps, int Lmax, int leaf, int *cnt,
                              long long ncnt, int *subcnt, long long nsub, unsigned long long *part) {
     __shared__ unsigned long long sk[4][FMM_T];
@@ -110,11 +111,13 @@ VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S,
         __syncthreads();
     }
     if (threadIdx.x != 0) return;
-    // the last build's quarter-cell occupancy, sources and box
+    // the last build's quarter-cell occupancy, sources, box, depth and the
+    // targets its 3-nearest pass left to the exact search
     const unsigned long long q2 = S->fsq;
     const long long s_prev = S->fs;
     const double side_prev = S->fside;
     const int L_prev = S->fL;
+    const long long flags_prev = S->fnflag;
     S->fsq = 0;
     S->fnflag = 0;
     S->fnbrute = 0;
@@ -131,10 +134,17 @@ VX_DEVK void k_fmm_prep_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars *S,
     Lmax = min(Lmax, Lc);
     int L = 2;
     while (L < Lmax && (double)(1LL << (2 * L)) * (double)leaf < (double)n) ++L;
+    // a tree deep enough for a dense region leaves the sparse rest of the
+    // cloud with quarters too small for their 3 nearest: once a build left
+    // more than 0.5 % of its targets to the exact search, the depth rule
+    // deepens no further than one level above that build, from then on
+    if (q2 > 0 && s_prev > 0 && L_prev >= 3 && flags_prev * 200 > s_prev)
+        S->fLcap = S->fLcap > 0 ? min(S->fLcap, L_prev - 1) : L_prev - 1;
+    const int Ldeep = S->fLcap > 0 ? max(L, min(Lmax, S->fLcap)) : Lmax;
     if (q2 > 0 && s_prev > 0 && side_prev > 0.0 && L_prev >= 1) {
         const double qa = side_prev / (double)(2LL << L_prev);                      // quarter side then
         const double rho = (double)q2 / (double)s_prev / (qa * qa) * ((double)vx_round32(n) / (double)s_prev);
-        while (L < Lmax) {
+        while (L < Ldeep) {
             const double a = side / (double)(1LL << L);
             if (rho * a * a < 2.0 * (double)leaf) break;
             ++L;

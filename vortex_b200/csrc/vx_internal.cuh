@@ -100,6 +100,8 @@ struct VxScalars {
     int bk_nmid, bk_nbig;  // buckets of 17..128 / more elements in the running bucket order (vx_sort.cu)
     long long fcnt_off;    // offset of the leaf level in the quadtree's count array
     unsigned long long fsq;   // sum over the quarter-leaf cells of count^2 at the last tree build (depth rule)
+    int fLcap;                // deepest level the depth rule may deepen to (0: none): set when a deepened tree
+                              // left too many targets to the exact 3-nearest search
     // pair evaluations executed by the bulk-form near-field and diffusion
     // kernels since the counters were last cleared
     unsigned long long pairs_bs, pairs_diff;

@@ -1,7 +1,7 @@
 """Long runs of two configurations on one GPU (FP32-bulk form; config2 also
 in the plain FP64 form):
 
-    python -m vortex_b200.runs config2 [--steps 3000] [--precision fp64]
+    python -m vortex_b200.runs config2 [--steps 3000] [--precision fp64] [--rules reference]
     python -m vortex_b200.runs config3 [--steps 5000] [--n0 3000000]
 
 config2: the 1000-panel cylinder of radius 0.5 (the benchmark's body),
@@ -67,11 +67,19 @@ def _stats(f, window, scale):
             "cl_rms": float(cl.std())}
 
 
-def config2(steps: int = 3000, every: int = 100, device: int = 0, precision: int = N.PREC_FP32) -> dict:
+def config2(steps: int = 3000, every: int = 100, device: int = 0, precision: int = N.PREC_FP32,
+            reference_rules: bool = False) -> dict:
+    """reference_rules: new vortices where the reference's program puts them
+    (panel midpoint + 1e-6 n, include/kernel.cuh:109-116) and |G| < 1e-12
+    dropped (its DELT, include/definitions.h:36), instead of the
+    configuration's half a panel off the wall and 1e-8."""
     pan = wl.cylinder_panels(1000)
-    sim = N.Sim(wl.cylinder_conf(precision, 1000), pan, device=device)
+    kw = dict(birth_offset_mode=N.BIRTH_REF, drop_eps=1e-12) if reference_rules else {}
+    sim = N.Sim(wl.cylinder_conf(precision, 1000, **kw), pan, device=device)
     form = "FP32-bulk" if precision == N.PREC_FP32 else "plain FP64"
-    rec = {"config": f"cylinder R=0.5, 1000 panels, impulsive start, Re 2000, dt 0.002, {form}",
+    rules = ("the reference program's birth offset and drop threshold" if reference_rules
+             else "birth half a panel off the wall, |G| < 1e-8 dropped")
+    rec = {"config": f"cylinder R=0.5, 1000 panels, impulsive start, Re 2000, dt 0.002, {form}, {rules}",
            "steps": steps}
     t0 = time.perf_counter()
     f = _timed_steps(sim, steps, every, rec)
@@ -145,10 +153,13 @@ def main():
     ap.add_argument("--n0", type=int, default=3_000_000)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                     help="config2: the FP32-bulk form (default) or the plain FP64 form")
+    ap.add_argument("--rules", default="config", choices=["config", "reference"],
+                    help="config2: the configuration's birth offset and drop threshold (default) or the "
+                         "reference program's")
     a = ap.parse_args()
     if a.which == "config2":
         prec = N.PREC_FP32 if a.precision == "fp32" else N.PREC_FP64
-        print(json.dumps(config2(a.steps or 3000, precision=prec)))
+        print(json.dumps(config2(a.steps or 3000, precision=prec, reference_rules=a.rules == "reference")))
     else:
         print(json.dumps(config3(a.steps or 5000, a.n0)))
 
