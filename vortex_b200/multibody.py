@@ -107,11 +107,14 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
     counts0 = np.array([s.count() for s in sims], dtype=np.float64)
     ms = []
     launches0 = batch.info()["kernels"] if batch else sum(s.launches() for s in sims)
+    host_ms = []
     for _ in range(steps):
         a, b = N.Event(), N.Event()
         if batch:
             a.record(stream)
+            t0 = time.perf_counter()
             batch.step(1)
+            host_ms.append(round(1e3 * (time.perf_counter() - t0), 3))
             b.record(stream)
         else:
             a.record(stream)
@@ -145,6 +148,7 @@ def run_batch(bodies: int = 256, steps: int = 20, warmup: int = 3, seed: int = 7
            "interactions_per_s_effective": inter * steps / total_s,
            "gpu_launches": int(launches), "kernels_per_batched_step": launches / steps, "setup_s": setup_s}
     if info:
+        out["host_ms_steps"] = host_ms   # host time of each batch.step(1) call (preparation and launch)
         out["graph_instantiations"] = info["graph_instantiations"]
         out["slot_table_rebuilds"] = info["rebuilds"]
         for k in ("host_grow_ms_max", "host_grow_ms_total", "host_refresh_ms_max", "host_refresh_ms_total",
