@@ -181,16 +181,28 @@ __global__ void k_fill_tail(double *x, double *y, double *g, long long from, lon
 }
 
 // Device allocation of `count` elements, counted (rounded to the 256-byte
-// allocation granularity) into *bytes; with allocs == nullptr only counted.
-// With a stream the allocation is stream-ordered (cudaMallocAsync): growing
-// one body's store then never waits for the other bodies' streams, as a
-// cudaFree would.
+// allocation granularity) into *bytes; with allocs == nullptr only counted,
+// or, with a carving cursor, taken from one block allocated before (a
+// body's scratch is one allocation: a growth that re-sizes it costs two
+// allocator calls, not forty, which matters when a batch of bodies grows at
+// once).  With a stream the allocation is stream-ordered (cudaMallocAsync):
+// growing one body's store then never waits for the other bodies' streams,
+// as a cudaFree would.
+struct WorkCarve {
+    char *next;
+};
 template <typename T>
 static vx_status dalloc(std::vector<void *> *allocs, long long *bytes, T **p, long long count,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, WorkCarve *cv = nullptr) {
     void *q = nullptr;
     if (count < 1) count = 1;
-    *bytes += ((long long)sizeof(T) * count + 255) / 256 * 256;
+    const long long nb = ((long long)sizeof(T) * count + 255) / 256 * 256;
+    *bytes += nb;
+    if (cv) {
+        *p = reinterpret_cast<T *>(cv->next);
+        cv->next += nb;
+        return VX_OK;
+    }
     if (!allocs) { *p = nullptr; return VX_OK; }
     if (stream)
         CU(cudaMallocAsync(&q, sizeof(T) * (size_t)count, stream));
@@ -204,9 +216,9 @@ static vx_status dalloc(std::vector<void *> *allocs, long long *bytes, T **p, lo
 // dalloc, then zeroed in stream order.
 template <typename T>
 static vx_status dalloc_zero(std::vector<void *> *allocs, long long *bytes, T **p, long long count,
-                             cudaStream_t stream) {
-    vx_status st = dalloc(allocs, bytes, p, count, stream);
-    if (st != VX_OK || !allocs) return st;
+                             cudaStream_t stream, WorkCarve *cv = nullptr) {
+    vx_status st = dalloc(allocs, bytes, p, count, stream, cv);
+    if (st != VX_OK || (!allocs && !cv)) return st;
     CU(cudaMemsetAsync(*p, 0, sizeof(T) * (size_t)(count < 1 ? 1 : count), stream));
     return VX_OK;
 }
@@ -225,13 +237,13 @@ void vx_work_free(VxWork &w, std::vector<void *> &allocs, cudaStream_t stream) {
 // Scratch for a particle capacity `cap` and a panel count padded to P32
 // (allocs == nullptr: only count the bytes into w.bytes).
 static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long long cap, int P32, int num_sms,
-                                 cudaStream_t stream, int fmm_p) {
+                                 cudaStream_t stream, int fmm_p, WorkCarve *cv = nullptr) {
     w.cap = cap;
     w.fmm_p = fmm_p;
     w.bytes = 0;
     const long long nch = cap / VX_CHUNK + 2;
     vx_status st;
-#define A(ptr, n) if ((st = dalloc(allocs, &w.bytes, &(ptr), (n), stream)) != VX_OK) return st
+#define A(ptr, n) if ((st = dalloc(allocs, &w.bytes, &(ptr), (n), stream, cv)) != VX_OK) return st
     A(w.cmp_cnt, nch); A(w.cmp_off, nch);
     A(w.hole_pos, cap); A(w.hole_src, cap); A(w.tail_src, cap);
     A(w.hx, cap); A(w.hy, cap); A(w.hg, cap); A(w.tx, cap); A(w.ty, cap);
@@ -239,7 +251,7 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.cellid, cap); A(w.cell_start, w.cells_cap + 1); A(w.sorted, cap);
     // the collapse grid's cell counts are zero between passes (the scatter
     // that consumes them counts them back down), so they start at zero
-    if ((st = dalloc_zero(allocs, &w.bytes, &w.cell_cnt, w.cells_cap, stream)) != VX_OK) return st;
+    if ((st = dalloc_zero(allocs, &w.bytes, &w.cell_cnt, w.cells_cap, stream, cv)) != VX_OK) return st;
     A(w.col, cap); A(w.in_cnt, cap); A(w.has_app, cap); A(w.first_app, cap);
     A(w.cand, cap); A(w.cstate, cap); A(w.cdec, cap);
     A(w.mx, cap); A(w.my, cap); A(w.mg, cap);
@@ -258,7 +270,7 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.cg_start, w.cells_cap + 1);
     // the diffusion grid's cell counts are zero between steps (its bucket
     // order leaves them so), so they start at zero
-    if ((st = dalloc_zero(allocs, &w.bytes, &w.cg_cnt, w.cells_cap, stream)) != VX_OK) return st;
+    if ((st = dalloc_zero(allocs, &w.bytes, &w.cg_cnt, w.cells_cap, stream, cv)) != VX_OK) return st;
     A(w.srt, cap);
     w.items_cap = cap / 32 + w.cells_cap + 2;
     A(w.items, w.items_cap);
@@ -274,7 +286,7 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
     A(w.fmm_L, 2LL * fmm_p * vx_fmm_cells(w.fmm_lmax));
     // the longest scan: cells of a grid, quarter-leaves, or rows at one per thread
     w.scan_tiles_cap = std::max(std::max(w.cells_cap, 1LL << (2 * (w.fmm_lmax + 1))), cap) / VX_SCAN_T + 2;
-    if ((st = dalloc_zero(allocs, &w.bytes, &w.scan_tiles, w.scan_tiles_cap, stream)) != VX_OK) return st;
+    if ((st = dalloc_zero(allocs, &w.bytes, &w.scan_tiles, w.scan_tiles_cap, stream, cv)) != VX_OK) return st;
 #undef A
     return VX_OK;
 }
@@ -282,7 +294,15 @@ static vx_status work_alloc_impl(VxWork &w, std::vector<void *> *allocs, long lo
 vx_status vx_work_alloc(VxWork &w, std::vector<void *> &allocs, long long cap, int P32, int num_sms,
                         cudaStream_t stream, int fmm_p) {
     vx_work_free(w, allocs, stream);
-    return work_alloc_impl(w, &allocs, cap, P32, num_sms, stream, fmm_p);
+    const long long bytes = vx_work_bytes(cap, P32, num_sms, fmm_p);
+    void *block = nullptr;
+    if (stream)
+        CU(cudaMallocAsync(&block, (size_t)bytes, stream));
+    else
+        CU(cudaMalloc(&block, (size_t)bytes));
+    allocs.push_back(block);
+    WorkCarve cv{static_cast<char *>(block)};
+    return work_alloc_impl(w, nullptr, cap, P32, num_sms, stream, fmm_p, &cv);
 }
 
 long long vx_work_bytes(long long cap, int P32, int num_sms, int fmm_p) {
