@@ -430,11 +430,15 @@ __global__ void __launch_bounds__(128) k_fmm_up_top(VxScalars *S, int *cnt, cplx
 // tile draw on the 8 x 8 source cells around it (children of the parents'
 // neighbours), whose multipoles are staged once in shared memory.  The
 // Hankel entries H_j = j! t^-(j+1) of the 40 integer offsets t are tabulated
-// per block.  Thread (cell, coefficient group cg, part pt) sums coefficients
-// 4 cg .. 4 cg + 3 over the interactions u = pt, pt + 4, ... of the cell's
-// list, with a sliding window over the Hankel entries (one shared load per
-// term for four coefficients); the four parts (adjacent lanes) are then
-// reduce-scattered, so part pt ends with coefficient lc = 4 cg + pt.
+// per block.  Thread (cell, coefficient group cg, part pt) sums the G
+// coefficients G cg .. G cg + G - 1 (G = 8 where it divides the order, else
+// 4) over the interactions u = pt, pt + 4, ... of the cell's list, with a
+// sliding window over the Hankel entries: per term one shared load of the
+// source coefficient and one of the window's new entry serve 4 G FP64 FMAs
+// (with G = 4 the two shared loads per 16 FMAs bound the loop).  The four
+// parts (adjacent lanes) are then reduce-scattered in a fixed tree, so part
+// pt ends with coefficients G cg + (G / 4) pt onwards; every coefficient is
+// the same sum, in the same order, whatever G.
 //
 // The levels up to M2L_SMALL have few cells each: their M2L parts are
 // independent of one another and run in one launch over all their tiles
@@ -443,6 +447,8 @@ __global__ void __launch_bounds__(128) k_fmm_up_top(VxScalars *S, int *cnt, cplx
 constexpr int M2L_TILE = 4;
 constexpr int M2L_SRC = 2 * M2L_TILE;   // 8 x 8 staged source cells
 constexpr int M2L_SMALL = 6;
+template <int P> __host__ __device__ constexpr int m2l_group() { return P % 8 == 0 ? 8 : 4; }   // coefficients a thread sums
+template <int P> __host__ __device__ constexpr int m2l_threads() { return M2L_TILE * M2L_TILE * 4 * (P / m2l_group<P>()); }
 
 template <int P>
 struct M2LShared {
@@ -474,15 +480,16 @@ __device__ void m2l_tables(M2LShared<P> &T) {
 // whether it holds vortices, *a its scaled M2L coefficient lc.
 template <int P>
 __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int l, long long t, M2LShared<P> &T,
-                         long long &c, bool &busy, cplx &a) {
+                         long long &c, bool &busy, int &lc0, cplx (&a)[2]) {
+    constexpr int G = m2l_group<P>(), NC = G / 4, TPC = 4 * (P / G);   // threads per cell
     const long long m = 1LL << l;
     const long long tiles1 = vx_ceil_div(m, (long long)M2L_TILE);
     const double s = S->fside / (double)m;
     const cplx *Ml = M + fmm_level_off(l) * P;
     const int *cl = cnt + fmm_level_off(l);
-    const int cell = threadIdx.x / P;
-    const int cg = (threadIdx.x % P) >> 2, pt = threadIdx.x & 3;
-    const int lc = 4 * cg + pt;
+    const int cell = threadIdx.x / TPC;
+    const int cg = (threadIdx.x % TPC) >> 2, pt = threadIdx.x & 3;
+    lc0 = G * cg + NC * pt;
     const long long tx0 = (t % tiles1) * M2L_TILE, ty0 = (t / tiles1) * M2L_TILE;
     const long long sx0 = tx0 - 2, sy0 = ty0 - 2;   // staged region origin
     const long long ix = tx0 + cell % M2L_TILE, iy = ty0 + cell / M2L_TILE;
@@ -507,7 +514,9 @@ __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int 
     __syncthreads();
     busy = live && cl[c] > 0;
     const long long px = ix >> 1, py = iy >> 1;
-    double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};   // (re, im) of coefficients 4 cg + j
+    double v[2 * G];   // (re, im) of coefficients G cg + j
+#pragma unroll
+    for (int j = 0; j < 2 * G; ++j) v[j] = 0.0;
     if (busy) {
         for (int u = pt; u < 36; u += 4) {
             const long long qy = 2 * (py - 1) + u / 6, qx = 2 * (px - 1) + u % 6;
@@ -515,37 +524,46 @@ __device__ bool m2l_tile(const VxScalars *S, const int *cnt, const cplx *M, int 
             if (llabs(qx - ix) <= 1 && llabs(qy - iy) <= 1) continue;   // neighbours: near field
             const int q = (int)((qy - sy0) * M2L_SRC + (qx - sx0));
             if (T.sc[q] == 0) continue;
-            const cplx *H = T.sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + 4 * cg;   // H_{k + 4 cg + j}
+            const cplx *H = T.sh[(int)(iy - qy + 3) * 7 + (int)(ix - qx + 3)] + G * cg;   // H_{k + G cg + j}
             const cplx *B = T.sm[q];
-            cplx h0 = H[0], h1 = H[1], h2 = H[2], h3 = H[3];
+            cplx h[G];
+#pragma unroll
+            for (int j = 0; j < G; ++j) h[j] = H[j];
 #pragma unroll
             for (int k = 0; k < P; ++k) {
                 const cplx b = B[k];
-                v[0] = fma(b.r, h0.r, fma(-b.i, h0.i, v[0]));
-                v[1] = fma(b.r, h0.i, fma(b.i, h0.r, v[1]));
-                v[2] = fma(b.r, h1.r, fma(-b.i, h1.i, v[2]));
-                v[3] = fma(b.r, h1.i, fma(b.i, h1.r, v[3]));
-                v[4] = fma(b.r, h2.r, fma(-b.i, h2.i, v[4]));
-                v[5] = fma(b.r, h2.i, fma(b.i, h2.r, v[5]));
-                v[6] = fma(b.r, h3.r, fma(-b.i, h3.i, v[6]));
-                v[7] = fma(b.r, h3.i, fma(b.i, h3.r, v[7]));
-                if (k + 1 < P) { h0 = h1; h1 = h2; h2 = h3; h3 = H[k + 4]; }
+#pragma unroll
+                for (int j = 0; j < G; ++j) {
+                    v[2 * j] = fma(b.r, h[j].r, fma(-b.i, h[j].i, v[2 * j]));
+                    v[2 * j + 1] = fma(b.r, h[j].i, fma(b.i, h[j].r, v[2 * j + 1]));
+                }
+                if (k + 1 < P) {
+#pragma unroll
+                    for (int j = 0; j + 1 < G; ++j) h[j] = h[j + 1];
+                    h[G - 1] = H[k + G];
+                }
             }
         }
     }
-    // reduce-scatter over the four parts (all lanes take part)
+    // reduce-scatter over the four parts (all lanes take part): first with
+    // the part two lanes away (halves of the G coefficients), then with the
+    // neighbouring part (halves of those): (p0 + p2) + (p1 + p3) for each
 #pragma unroll
-    for (int half = 4; half >= 2; half >>= 1) {
-        const bool up = (pt & (half >> 1)) != 0;
+    for (int lvl = 0; lvl < 2; ++lvl) {
+        const int half = G >> lvl, x = 2 >> lvl;
+        const bool up = (pt & x) != 0;
 #pragma unroll
         for (int i = 0; i < half; ++i) {
             const double send = up ? v[i] : v[i + half];
             const double keep = up ? v[i + half] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, half >> 1);
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, x);
         }
     }
-    a = {v[0], v[1]};
-    if (busy) a = cscale(a, ((lc & 1) ? -1.0 : 1.0) / s);
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+        a[i] = {v[2 * i], v[2 * i + 1]};
+        if (busy) a[i] = cscale(a[i], (((lc0 + i) & 1) ? -1.0 : 1.0) / s);
+    }
     return live;
 }
 
@@ -564,8 +582,9 @@ __device__ __forceinline__ cplx l2l_term(const cplx *Lp, const cplx (*se)[P], lo
 }
 
 template <int P>
-VX_DEVK void k_fmm_m2l_l2l_body(VxBlkB<M2L_TILE * M2L_TILE * P, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
+VX_DEVK void k_fmm_m2l_l2l_body(VxBlkB<m2l_threads<P>(), 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
                                 cplx *Loc, int l) {
+    constexpr int NC = m2l_group<P>() / 4;
     M2LShared<P> &T = *reinterpret_cast<M2LShared<P> *>(vx_fmm_dyn);
     if (l > S->fL) return;
     m2l_tables<P>(T);
@@ -573,35 +592,38 @@ VX_DEVK void k_fmm_m2l_l2l_body(VxBlkB<M2L_TILE * M2L_TILE * P, 0> vb, const VxS
     const long long tiles1 = vx_ceil_div(m, (long long)M2L_TILE);
     cplx *Ll = Loc + fmm_level_off(l) * P;
     const cplx *Lp = Loc + fmm_level_off(l - 1) * P;
-    const int lc = threadIdx.x % P;   // = 4 cg + pt
     for (long long t = vb.x; t < tiles1 * tiles1; t += vb.n) {
         long long c;
         bool busy;
-        cplx a;
-        if (!m2l_tile<P>(S, cnt, M, l, t, T, c, busy, a)) continue;
-        if (busy && l > 2) a = cadd(a, l2l_term<P>(Lp, T.se, m, c % m, c / m, lc));
-        Ll[c * P + lc] = a;
+        int lc0;
+        cplx a[2];
+        if (!m2l_tile<P>(S, cnt, M, l, t, T, c, busy, lc0, a)) continue;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+            if (busy && l > 2) a[i] = cadd(a[i], l2l_term<P>(Lp, T.se, m, c % m, c / m, lc0 + i));
+            Ll[c * P + lc0 + i] = a[i];
+        }
     }
 }
 template <int P>
-__global__ void __launch_bounds__(M2L_TILE * M2L_TILE * P) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
+__global__ void __launch_bounds__(m2l_threads<P>()) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
                                                        cplx *Loc, int l) {
     VX_PDL_WAIT();
-    k_fmm_m2l_l2l_body<P>(VxBlkB<M2L_TILE * M2L_TILE * P, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc, l);
+    k_fmm_m2l_l2l_body<P>(VxBlkB<m2l_threads<P>(), 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc, l);
 }
 
 // M2L (without L2L) of levels 2 .. min(M2L_SMALL, L): blocks over the tiles
 // of all of them.
 template <int P>
-VX_DEVK void k_fmm_m2l_small_body(VxBlkB<M2L_TILE * M2L_TILE * P, 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
+VX_DEVK void k_fmm_m2l_small_body(VxBlkB<m2l_threads<P>(), 0> vb, const VxScalars *S, const int *cnt, const cplx *M,
                                   cplx *Loc) {
+    constexpr int NC = m2l_group<P>() / 4;
     M2LShared<P> &T = *reinterpret_cast<M2LShared<P> *>(vx_fmm_dyn);
     const int hi = min(S->fL, M2L_SMALL);
     if (hi < 2) return;
     m2l_tables<P>(T);
     long long total = 0;
     for (int l = 2; l <= hi; ++l) total += vx_ceil_div(1LL << (2 * l), (long long)(M2L_TILE * M2L_TILE));
-    const int lc = threadIdx.x % P;
     for (long long b = vb.x; b < total; b += vb.n) {
         int l = 2;
         long long t = b;
@@ -611,16 +633,18 @@ VX_DEVK void k_fmm_m2l_small_body(VxBlkB<M2L_TILE * M2L_TILE * P, 0> vb, const V
         }
         long long c;
         bool busy;
-        cplx a;
-        if (!m2l_tile<P>(S, cnt, M, l, t, T, c, busy, a)) continue;
-        Loc[(fmm_level_off(l) + c) * P + lc] = a;
+        int lc0;
+        cplx a[2];
+        if (!m2l_tile<P>(S, cnt, M, l, t, T, c, busy, lc0, a)) continue;
+#pragma unroll
+        for (int i = 0; i < NC; ++i) Loc[(fmm_level_off(l) + c) * P + lc0 + i] = a[i];
     }
 }
 template <int P>
-__global__ void __launch_bounds__(M2L_TILE * M2L_TILE * P) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
+__global__ void __launch_bounds__(m2l_threads<P>()) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
                                                          cplx *Loc) {
     VX_PDL_WAIT();
-    k_fmm_m2l_small_body<P>(VxBlkB<M2L_TILE * M2L_TILE * P, 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc);
+    k_fmm_m2l_small_body<P>(VxBlkB<m2l_threads<P>(), 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc);
 }
 
 // L2L into levels 3 .. min(M2L_SMALL, L), one launch: a block takes a cell
@@ -1036,7 +1060,7 @@ int vx_fmm_max_level(long long cap) {
 
 template <int P>
 static cudaError_t velocity_fmm(const VxLaunch &L, const VxParams &p, const VxView &v, VxScalars *S, VxWork &w) {
-    constexpr int M2L_T = M2L_TILE * M2L_TILE * P;
+    constexpr int M2L_T = m2l_threads<P>();
     constexpr size_t M2L_SMEM = sizeof(M2LShared<P>);
     if (M2L_SMEM > 48 * 1024 && !L.rec) {   // opt in to more than 48 KB of shared memory (once per device)
         static bool done[64] = {};
