@@ -449,6 +449,9 @@ constexpr int M2L_SRC = 2 * M2L_TILE;   // 8 x 8 staged source cells
 constexpr int M2L_SMALL = 6;
 template <int P> __host__ __device__ constexpr int m2l_group() { return P % 8 == 0 ? 8 : 4; }   // coefficients a thread sums
 template <int P> __host__ __device__ constexpr int m2l_threads() { return M2L_TILE * M2L_TILE * 4 * (P / m2l_group<P>()); }
+#ifndef VX_M2L_MINB
+#define VX_M2L_MINB 0   // minimum resident blocks per SM requested for the M2L kernels (0: none)
+#endif
 
 template <int P>
 struct M2LShared {
@@ -606,7 +609,7 @@ VX_DEVK void k_fmm_m2l_l2l_body(VxBlkB<m2l_threads<P>(), 0> vb, const VxScalars 
     }
 }
 template <int P>
-__global__ void __launch_bounds__(m2l_threads<P>()) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
+__global__ void __launch_bounds__(m2l_threads<P>(), VX_M2L_MINB) k_fmm_m2l_l2l(const VxScalars *S, const int *cnt, const cplx *M,
                                                        cplx *Loc, int l) {
     VX_PDL_WAIT();
     k_fmm_m2l_l2l_body<P>(VxBlkB<m2l_threads<P>(), 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc, l);
@@ -641,7 +644,7 @@ VX_DEVK void k_fmm_m2l_small_body(VxBlkB<m2l_threads<P>(), 0> vb, const VxScalar
     }
 }
 template <int P>
-__global__ void __launch_bounds__(m2l_threads<P>()) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
+__global__ void __launch_bounds__(m2l_threads<P>(), VX_M2L_MINB) k_fmm_m2l_small(const VxScalars *S, const int *cnt, const cplx *M,
                                                          cplx *Loc) {
     VX_PDL_WAIT();
     k_fmm_m2l_small_body<P>(VxBlkB<m2l_threads<P>(), 0>{blockIdx.x, gridDim.x}, S, cnt, M, Loc);
