@@ -513,6 +513,24 @@ static vx_status ensure_capacities(vx_batch *b) {
             if (bound < s->n_upper) s->n_upper = bound;
         }
     }
+    // the members that grow now take their new stores and scratch from the
+    // device's pool: one allocation of their total, given back at once,
+    // leaves that memory in the pool (its release threshold keeps it), so
+    // their own allocations are served from it instead of each mapping new
+    // memory (hundreds of ms when a batch of bodies grows together)
+    long long grow_bytes = 0;
+    for (Body &bd : b->bodies) {
+        vx_sim *s = bd.s;
+        const long long need = vx_sim_need(s, s->n_upper);
+        if (need > s->cap) grow_bytes += vx_sim_grow_bytes(s, need);
+    }
+    if (grow_bytes > 0) {
+        void *reserve = nullptr;
+        if (cudaMallocAsync(&reserve, (size_t)grow_bytes, b->stream) == cudaSuccess)
+            cudaFreeAsync(reserve, b->stream);
+        else
+            cudaGetLastError();   // no room for the whole at once: the members allocate one by one
+    }
     for (Body &bd : b->bodies) {
         vx_sim *s = bd.s;
         const long long need = vx_sim_need(s, s->n_upper);

@@ -327,14 +327,19 @@ static void drop_graph(vx_sim *s) {
 
 // Grow the particle store to at least `need` slots, keeping every slot's
 // content (the dead tail matters: it enters the next 3-nearest search).
-static vx_status grow(vx_sim *s, long long need) {
-    // a growth adds at least one increment (inc_step, 8192 at least) or a
-    // quarter; the first store gets the same margin beyond what its cloud
-    // needs, so a new body does not grow within its first steps
+// The capacity a growth to at least `need` slots gives: it adds at least
+// one increment (inc_step, 8192 at least) or a quarter; the first store gets
+// the same margin beyond what its cloud needs, so a new body does not grow
+// within its first steps.
+static long long grown_cap(const vx_sim *s, long long need) {
     const long long inc = std::max<long long>(s->conf.inc_step, 8192);
     long long ncap = s->cap > 0 ? std::max(need, s->cap + inc) : std::max(need + inc, (long long)(need * 1.25));
     ncap = std::max(ncap, (long long)(s->cap * 1.25));
-    ncap = vx_ceil_div(ncap, 8192) * 8192;
+    return vx_ceil_div(ncap, 8192) * 8192;
+}
+
+static vx_status grow(vx_sim *s, long long need) {
+    const long long ncap = grown_cap(s, need);
     double *arr[6] = {s->x, s->y, s->g, s->vx, s->vy, s->d};
     double *nar[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     for (int k = 0; k < 6; ++k) {
@@ -396,6 +401,10 @@ static int step_sms_for(vx_sim *s) { return vx_body_sms(s->n_upper + s->P, s->nu
 
 VxLaunch vx_sim_launch(vx_sim *s) { return launch_of(s); }
 long long vx_sim_need(vx_sim *s, long long n) { return need_for(s, n); }
+long long vx_sim_grow_bytes(vx_sim *s, long long need) {
+    const long long ncap = grown_cap(s, need);
+    return 6LL * 8 * ncap + vx_work_bytes(ncap, s->P32, s->num_sms, s->prm.fmm_p) + 6 * 256;
+}
 vx_status vx_sim_grow(vx_sim *s, long long need) { return grow(s, need); }
 vx_status vx_sim_read_scalars(vx_sim *s) { return read_scalars(s); }
 int vx_sim_step_sms(vx_sim *s) { return step_sms_for(s); }

@@ -63,6 +63,7 @@ struct vx_sim {
 VxLaunch vx_sim_launch(vx_sim *s);
 long long vx_sim_need(vx_sim *s, long long n);     // slots a step starting with n vortices needs
 vx_status vx_sim_grow(vx_sim *s, long long need);
+long long vx_sim_grow_bytes(vx_sim *s, long long need);   // device bytes the store and scratch of that growth take
 vx_status vx_sim_read_scalars(vx_sim *s);
 int vx_sim_step_sms(vx_sim *s);
 int vx_sim_rhs_chunks(vx_sim *s);
