@@ -864,20 +864,35 @@ VX_DEVK void k_fmm_nn3_sub_body(VxBlkB<FMM_T, 0> vb, const VxView &v, VxScalars 
         // a source's offset to the target's leaf centre: (its leaf's column -
         // col) h and (its leaf's row - row) h, differences of -1, 0 or 1, so
         // exact in FP32 and the same for every source of a quarter
-        const float hf = (float)h;
-        for (int Y2 = y0; Y2 <= y1; ++Y2) {
+        const float hf = (float)h, hq = 0.5f * hf;
+        // the target's own quarter first, then its four edge neighbours, then
+        // the corners; a quarter whose box lies farther than the third
+        // distance found so far (with a margin over FP32 rounding) cannot
+        // hold one of the 3 nearest and is not read: in a dense region the
+        // own quarter alone usually settles them.  (A quarter X2 spans
+        // [(X2 - 2 col - 1) hq, (X2 - 2 col) hq] in the leaf frame.)
+#pragma unroll 1
+        for (int o = 0; o < 9; ++o) {
+            const int ddx = (o == 1 || o == 5 || o == 7) ? -1 : ((o == 2 || o == 6 || o == 8) ? 1 : 0);
+            const int ddy = (o == 3 || o == 5 || o == 6) ? -1 : ((o == 4 || o == 7 || o == 8) ? 1 : 0);
+            const int X2 = ix2 + ddx, Y2 = iy2 + ddy;
+            if (X2 < x0 || X2 > x1 || Y2 < y0 || Y2 > y1) continue;
+            if (o > 0) {
+                const float qx = (float)(X2 - 2 * col), qy = (float)(Y2 - 2 * row);
+                const float gx = fmaxf(fmaxf((qx - 1.0f) * hq - me.x, me.x - qx * hq), 0.0f);
+                const float gy = fmaxf(fmaxf((qy - 1.0f) * hq - me.y, me.y - qy * hq), 0.0f);
+                if (fmaf(gx, gx, gy * gy) > 1.0001f * d3) continue;
+            }
             const int lr = Y2 >> 1;
             const float oy = (float)(lr - row) * hf;
-            for (int X2 = x0; X2 <= x1; ++X2) {
-                const float ox = (float)((X2 >> 1) - col) * hf;
-                const int k = 4 * (lr * m + (X2 >> 1)) + 2 * (Y2 & 1) + (X2 & 1);
-                const int q1 = substart[k + 1];
-                for (int qq = substart[k]; qq < q1; ++qq) {
-                    if (qq == t) continue;
-                    const float2 q = *reinterpret_cast<const float2 *>(srt + qq);   // x, y of the source
-                    const float dx = me.x - (q.x + ox), dy = me.y - (q.y + oy);
-                    vx_nn3_insert_bf(d1, d2, d3, fmaf(dx, dx, dy * dy));
-                }
+            const float ox = (float)((X2 >> 1) - col) * hf;
+            const int k = 4 * (lr * m + (X2 >> 1)) + 2 * (Y2 & 1) + (X2 & 1);
+            const int q1 = substart[k + 1];
+            for (int qq = substart[k]; qq < q1; ++qq) {
+                if (qq == t) continue;
+                const float2 q = *reinterpret_cast<const float2 *>(srt + qq);   // x, y of the source
+                const float dx = me.x - (q.x + ox), dy = me.y - (q.y + oy);
+                vx_nn3_insert_bf(d1, d2, d3, fmaf(dx, dx, dy * dy));
             }
         }
         v.d[j] = (double)((sqrtf(d1) + sqrtf(d2) + sqrtf(d3)) / 3);
