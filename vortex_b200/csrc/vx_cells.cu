@@ -119,7 +119,6 @@ VX_DEVK void k_cg_prep_body(VxBlkB<CG_T, 0> vb, const VxView &v, VxScalars *S, d
     S->cnhuge = 0;
     S->bk_nmid = S->bk_nbig = 0;
     S->cnitems = 0;
-    S->cg_next = 0;
     if (n == 0) { S->cncells = 0; S->cnx = S->cny = 0; return; }
     const double dsum = sd[0];
     const double x0 = vx_dunkey(sk[0][0]), x1 = -vx_dunkey(sk[1][0]);
@@ -373,20 +372,7 @@ VX_DEVK void k_diff_cells_body(VxBlkB<CG_T, VX_DIFF_MINB> vb, const VxParams &p,
     const float log2e = 1.4426950408889634f;
     const long long wpb = CG_T / 32;
     unsigned long long pairs = 0;
-    // items are handed out in turn (one atomic per item and warp): their
-    // costs differ by orders of magnitude once a wake has evolved (a window
-    // over dense rows holds thousands of sources, one in a sparse region a
-    // few), and a fixed share of items per warp left the kernel waiting on
-    // the warps that drew the dense ones (the same pairs took 1.28 instead
-    // of 0.89 ms on the benchmark wake after 40 steps).  Each item is still
-    // summed by one warp in its fixed order, so results do not depend on
-    // which warp takes it.
-    (void)wpb;
-    for (;;) {
-        unsigned long long got = 0;
-        if (lane == 0) got = atomicAdd(&S->cg_next, 1ull);
-        const long long it = (long long)__shfl_sync(0xffffffffu, got, 0);
-        if (it >= nitems) break;
+    for (long long it = vb.x * wpb + (threadIdx.x >> 5); it < nitems; it += vb.n * wpb) {
         const int2 item = items[it];
         const long long row = item.x;
         const long long row_end = start[(row + 1) * nx];

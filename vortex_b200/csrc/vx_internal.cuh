@@ -91,7 +91,6 @@ struct VxScalars {
     // neighbour-list grid of the bulk form (vortex diffusion)
     double cx0, cy0, ch, chy;   // origin, cell width and cell height
     long long cnx, cny, cncells, cnitems;
-    unsigned long long cg_next;   // next diffusion work item to hand out (k_diff_cells takes them in turn)
     // quadtree of the bulk-form Biot-Savart (vx_fmm.cu)
     double fx0, fy0, fside;
     long long fnleaves, fs;
